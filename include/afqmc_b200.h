@@ -1,0 +1,171 @@
+/* afqmc_b200.h - C ABI of the B200 (sm_100a) walker propagation and measurement path.
+ *
+ * A drop-in for the operation calls the miniAFQMC driver makes on its walker set
+ * (QMCPACK miniAFQMC, src/miniapps/miniafqmc_base.cpp:249-345).  Every entry point
+ * takes plain pointers and sizes; complex numbers are interleaved FP64 pairs
+ * (std::complex<double> / double _Complex compatible), arrays are row-major with the
+ * reference's index orders:
+ *
+ *   W       [nwalk][2][NMO][NAEA]       walker Slater matrices   (miniafqmc_base.cpp:222)
+ *   W_data  [nwalk][8]                  0 eloc, 1 weight, 2/3 overlap alpha/beta,
+ *                                       4 hybrid energy, 5 previous 4, 6/7 previous 2/3
+ *                                                                  (miniafqmc_base.cpp:223-224)
+ *   Gc      [2*NAEA*NMO][nwalk]         compact mixed density matrix (walker fastest)
+ *   vbias   [nchol][nwalk], X [nchol][nwalk], vHS [NMO*NMO][nwalk]
+ *
+ * The handle owns all device memory; walker state stays on the GPU between calls and
+ * only the host arrays passed to set/get/copy calls cross PCIe.  A handle is used by one
+ * host thread at a time and runs its work on its own CUDA stream.  All calls return an
+ * afq_status; none of them aborts the process.
+ */
+#ifndef AFQMC_B200_H
+#define AFQMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AFQ_OK = 0,
+  AFQ_ERR_ARG = 1,          /* null pointer, inconsistent or out-of-range size          */
+  AFQ_ERR_STATE = 2,        /* call out of order (e.g. no Hamiltonian loaded yet)        */
+  AFQ_ERR_CUDA = 3,         /* a CUDA runtime call failed; see afq_last_error            */
+  AFQ_ERR_OOM = 4,          /* device allocation failed                                  */
+  AFQ_ERR_UNSUPPORTED = 5,  /* size or option not supported by this build                */
+  AFQ_ERR_SINGULAR = 6      /* some walker had an exactly singular overlap matrix;
+                               its overlap is 0 and its flags are in afq_get_info        */
+} afq_status;
+
+typedef enum {
+  AFQ_PREC_FP64 = 0,        /* every contraction in FP64 (the plain form)                */
+  AFQ_PREC_MIXED = 1        /* tensor-core contractions, FP64 LU/QR/weights              */
+} afq_precision;
+
+typedef enum {
+  AFQ_ENERGY_VAKBL = 0,     /* eloc = 1/2 Gc.(Vakbl Gc) + Gc.haj (energy.hpp:66-102)     */
+  AFQ_ENERGY_CHOLESKY = 1   /* same energy from the half-rotated Cholesky factors        */
+} afq_energy_mode;
+
+typedef enum {
+  AFQ_BUF_GC = 0, AFQ_BUF_VBIAS = 1, AFQ_BUF_X = 2, AFQ_BUF_VHS = 3, AFQ_BUF_HYBRIDW = 4,
+  AFQ_BUF_XRAW = 5,         /* real normals [nchol][nwalk] (double)                      */
+  AFQ_BUF_INFO = 6,         /* int32 [nwalk][2], nonzero = singular overlap matrix      */
+  AFQ_BUF_ENERGY_PARTS = 7  /* double [nwalk][3] = (E1, EJ, EK) of the last Cholesky
+                               energy evaluation                                         */
+} afq_buffer;
+
+typedef struct {
+  int nmo;                  /* NMO                                                       */
+  int naea, naeb;           /* electrons per spin; the reference requires naea == naeb
+                               (initialize_serial.hpp:67-71)                              */
+  int nchol;                /* number of Cholesky vectors                                */
+  int nwalk;                /* walkers held by this handle                               */
+  double dt;                /* time step; Spvn passed in is already scaled by sqrt(dt)   */
+  int taylor_order;         /* terms of exp(vHS) (the reference fixes 6, vHS.hpp:65)     */
+  int precision;            /* afq_precision                                             */
+  int device;               /* CUDA device ordinal                                       */
+} afq_system_desc;
+
+/* Zero-based CSR with int32 indices, rows sorted and columns sorted within each row,
+ * as SparseMatrix::compress leaves them (src/Matrix/SparseMatrix.hpp:295-319). */
+typedef struct {
+  int nrows, ncols;
+  const int32_t* rowIndex;  /* [nrows+1]                                                 */
+  const int32_t* cols;      /* [nnz]                                                     */
+  const double* vals;       /* [2*nnz] interleaved complex                               */
+} afq_csr_z;
+
+typedef struct afq_handle afq_handle;
+
+/* Set-up: replaces base::afqmc_sys::setup (afqmc_sys.hpp:61-93) and the data
+ * afqmc::Initialize + base::halfrotate_cholesky produce (miniafqmc_base.cpp:176-185). */
+afq_status afq_create(const afq_system_desc* desc, afq_handle** out);
+void afq_destroy(afq_handle* h);
+const char* afq_status_string(afq_status s);
+const char* afq_last_error(const afq_handle* h);
+
+/* Spvn: [NMO^2 x nchol] scaled by sqrt(dt) (initialize_serial.hpp:221);
+ * SpvnT: [nchol x 2*NAEA*NMO] half-rotated (rotate.hpp:69-169);
+ * Propg1 [NMO][NMO]; haj [2*NAEA][NMO]; trial [2][NMO][NAEA] = conj(Wavefun)
+ * (afqmc_sys.hpp:58-59); Vakbl [2*NAEA*NMO]^2 or NULL; Lhalf [nchol][2][NAEA][NMO]
+ * unscaled half-rotated factors without cutoff, or NULL.  At least one of Vakbl and
+ * Lhalf is needed for afq_energy. */
+afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_csr_z* SpvnT,
+                               const double* Propg1, const double* haj, const double* trial,
+                               const afq_csr_z* Vakbl, const double* Lhalf);
+
+afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data);
+afq_status afq_get_walkers(afq_handle* h, double* W, double* W_data);
+
+/* afqmc_sys::calculate_mixed_density_matrix(W, W_data, Gc, compact=true)
+ * (afqmc_sys.hpp:98-116): Gc and W_data[:,2..3] on the device. */
+afq_status afq_mixed_density_matrix(afq_handle* h);
+/* afqmc_sys::calculate_overlaps (afqmc_sys.hpp:136-144).  save_old != 0 first does the
+ * driver's W_data[5,6,7] <- W_data[4,2,3] copy (miniafqmc_base.cpp:305-309). */
+afq_status afq_overlaps(afq_handle* h, int save_old);
+/* base::get_vbias(SpvnT, Gc, vbias, true) (vbias.hpp:49-63). */
+afq_status afq_vbias(afq_handle* h);
+/* Driver step 2 (miniafqmc_base.cpp:281-289) with x ~ N(0,1) from Philox4x32-10
+ * keyed by seed, counter (pair index, step).  afq_sigma_from takes x from the host. */
+afq_status afq_sigma(afq_handle* h, uint64_t seed, uint64_t step);
+afq_status afq_sigma_from(afq_handle* h, const double* x);
+/* base::get_vHS(Spvn, X, vHS) (vHS.hpp:47-56). */
+afq_status afq_vhs(afq_handle* h);
+/* afqmc_sys::propagate(W, Propg1, vHS) (afqmc_sys.hpp:150-173), Taylor order from desc. */
+afq_status afq_propagate(afq_handle* h);
+/* Driver step 6 (miniafqmc_base.cpp:316-327); Eshift lives on the device. */
+afq_status afq_update_weights(afq_handle* h);
+/* Same weight update with the current Eshift but without replacing it; returns the
+ * local sum of Re W_data[:,4] so a walker-sharded caller can all-reduce it and call
+ * afq_set_eshift(global_sum / global_nwalk). */
+afq_status afq_update_weights_partial(afq_handle* h, double* e4_sum);
+afq_status afq_get_eshift(afq_handle* h, double* eshift);
+afq_status afq_set_eshift(afq_handle* h, double eshift);
+/* Places this handle's walkers at [offset, offset+nwalk) of an ensemble of nwalk_global
+ * walkers, so that the Philox stream (indexed by the global walker) gives every shard
+ * the auxiliary fields the unsharded ensemble would draw.  No reference counterpart:
+ * the reference runs one ensemble in one process (miniafqmc_base.cpp:282). */
+afq_status afq_set_walker_offset(afq_handle* h, int offset, int nwalk_global);
+/* afqmc_sys::orthogonalize (afqmc_sys.hpp:176-207): zgelqf + zunglq conventions. */
+afq_status afq_orthogonalize(afq_handle* h);
+/* afqmc_sys::calculate_energy (afqmc_sys.hpp:121-133) on the current Gc:
+ * W_data[:,0] = eloc and *eav = sum Re(eloc) Re(w) / sum Re(w). */
+afq_status afq_energy(afq_handle* h, int mode, double* eav);
+/* As afq_energy, returning the two weighted sums instead of their ratio (for sharded
+ * callers): sums[0] = sum Re(eloc) Re(w), sums[1] = sum Re(w). */
+afq_status afq_energy_sums(afq_handle* h, int mode, double* sums);
+
+/* One whole substep of the driver loop (miniafqmc_base.cpp:251-337) as one CUDA graph
+ * launch: mixed density matrix, vbias, sigma (Philox, counter `step_tot`), vHS,
+ * propagation, overlaps, weights, and orthogonalization + overlaps when
+ * step_tot > 0 && step_tot % northo == 0.  Asynchronous. */
+afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int northo);
+
+afq_status afq_synchronize(afq_handle* h);
+
+/* Stage timers, the counterpart of the reference's NewTimer stages
+ * (miniafqmc_base.cpp:50-77): with profiling on, every op-by-op call records CUDA events
+ * on the handle's stream around its kernels (graph substeps are not split). */
+typedef enum {
+  AFQ_STAGE_DM = 0, AFQ_STAGE_VBIAS = 1, AFQ_STAGE_SIGMA = 2, AFQ_STAGE_VHS = 3,
+  AFQ_STAGE_PROPAGATE = 4, AFQ_STAGE_OVERLAP = 5, AFQ_STAGE_WEIGHTS = 6,
+  AFQ_STAGE_ORTHO = 7, AFQ_STAGE_ENERGY = 8, AFQ_NSTAGES = 9
+} afq_stage;
+afq_status afq_profile(afq_handle* h, int enable);
+/* Synchronizes, then writes accumulated GPU milliseconds and kernel launches per stage
+ * ([AFQ_NSTAGES] each, either may be NULL); reset != 0 clears the accumulators.
+ * Launch counts include graph substeps. */
+afq_status afq_stage_times(afq_handle* h, double* ms, long long* launches, int reset);
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
+ * or events against the library's. */
+afq_status afq_get_stream(afq_handle* h, void** stream);
+/* Copies a device buffer to host memory in the reference layout (see afq_buffer). */
+afq_status afq_copy_out(afq_handle* h, int which, void* host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFQMC_B200_H */

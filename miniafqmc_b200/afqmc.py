@@ -1,0 +1,280 @@
+"""Host-side mirror of the miniapp's AFQMC operation interface over libafqmc_b200.
+
+`AfqmcSys` carries the same operation names as the reference's `base::afqmc_sys` and
+free functions (src/AFQMC/afqmc_sys.hpp, vbias.hpp, vHS.hpp, energy.hpp), but the walker
+set lives on the GPU inside the handle; every call goes through the C ABI declared in
+include/afqmc_b200.h.  Errors come back as `AfqmcError` carrying the library's status.
+
+The library must be built (`python -m miniafqmc_b200.build`); there is no CPU
+fallback, and loading fails loudly when the shared object is missing."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libafqmc_b200.so")
+
+AFQ_PREC_FP64, AFQ_PREC_MIXED = 0, 1
+AFQ_ENERGY_VAKBL, AFQ_ENERGY_CHOLESKY = 0, 1
+BUFFERS = {"Gc": 0, "vbias": 1, "X": 2, "vHS": 3, "hybridW": 4, "xraw": 5, "info": 6,
+           "energy_parts": 7}
+STATUS = {0: "AFQ_OK", 1: "AFQ_ERR_ARG", 2: "AFQ_ERR_STATE", 3: "AFQ_ERR_CUDA",
+          4: "AFQ_ERR_OOM", 5: "AFQ_ERR_UNSUPPORTED", 6: "AFQ_ERR_SINGULAR"}
+
+EXPORTS = [
+    "afq_create", "afq_destroy", "afq_status_string", "afq_last_error", "afq_set_hamiltonian",
+    "afq_set_walkers", "afq_get_walkers", "afq_mixed_density_matrix", "afq_overlaps",
+    "afq_vbias", "afq_sigma", "afq_sigma_from", "afq_vhs", "afq_propagate",
+    "afq_update_weights", "afq_update_weights_partial", "afq_get_eshift", "afq_set_eshift",
+    "afq_orthogonalize", "afq_energy", "afq_energy_sums", "afq_substep", "afq_synchronize",
+    "afq_copy_out", "afq_set_walker_offset", "afq_profile", "afq_stage_times", "afq_get_stream",
+]
+STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
+
+
+class AfqmcError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [("nmo", ctypes.c_int), ("naea", ctypes.c_int), ("naeb", ctypes.c_int),
+                ("nchol", ctypes.c_int), ("nwalk", ctypes.c_int), ("dt", ctypes.c_double),
+                ("taylor_order", ctypes.c_int), ("precision", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class CsrZ(ctypes.Structure):
+    _fields_ = [("nrows", ctypes.c_int), ("ncols", ctypes.c_int),
+                ("rowIndex", ctypes.c_void_p), ("cols", ctypes.c_void_p),
+                ("vals", ctypes.c_void_p)]
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m miniafqmc_b200.build`")
+    lib = ctypes.CDLL(path)
+    P, I, D, U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_uint64
+    sigs = {
+        "afq_create": ([P, P], I), "afq_destroy": ([P], None),
+        "afq_status_string": ([I], ctypes.c_char_p), "afq_last_error": ([P], ctypes.c_char_p),
+        "afq_set_hamiltonian": ([P, P, P, P, P, P, P, P], I),
+        "afq_set_walkers": ([P, P, P], I), "afq_get_walkers": ([P, P, P], I),
+        "afq_mixed_density_matrix": ([P], I), "afq_overlaps": ([P, I], I),
+        "afq_vbias": ([P], I), "afq_sigma": ([P, U64, U64], I), "afq_sigma_from": ([P, P], I),
+        "afq_vhs": ([P], I), "afq_propagate": ([P], I), "afq_update_weights": ([P], I),
+        "afq_update_weights_partial": ([P, P], I), "afq_get_eshift": ([P, P], I),
+        "afq_set_eshift": ([P, D], I), "afq_orthogonalize": ([P], I),
+        "afq_energy": ([P, I, P], I), "afq_energy_sums": ([P, I, P], I),
+        "afq_substep": ([P, U64, U64, I], I), "afq_synchronize": ([P], I),
+        "afq_copy_out": ([P, I, P], I), "afq_set_walker_offset": ([P, I, I], I),
+        "afq_profile": ([P, I], I), "afq_stage_times": ([P, P, P, I], I),
+        "afq_get_stream": ([P, P], I),
+    }
+    for name, (args, res) in sigs.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = lib
+    return lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def _csr(m):
+    if m is None:
+        return None, ()
+    ri = np.ascontiguousarray(m.rowIndex, np.int32)
+    ci = np.ascontiguousarray(m.cols, np.int32)
+    v = np.ascontiguousarray(m.vals, np.complex128)
+    s = CsrZ(m.nrows, m.ncols, _p(ri), _p(ci), _p(v))
+    return s, (ri, ci, v)
+
+
+class AfqmcSys:
+    """One device-resident walker set with its Hamiltonian (mirrors base::afqmc_sys)."""
+
+    def __init__(self, system, nwalk: int, precision: int = AFQ_PREC_FP64, device: int = 0,
+                 use_vakbl: bool = True, use_chol: bool = True, walkers=None):
+        self.lib = load_library()
+        self.sys = system
+        self.N, self.n, self.nchol, self.nw = system.N, system.n, system.nchol, nwalk
+        self.precision = precision
+        desc = SystemDesc(system.N, system.n, system.n, system.nchol, nwalk, system.cfg.dt,
+                          system.cfg.taylor_order, precision, device)
+        h = ctypes.c_void_p()
+        st = self.lib.afq_create(ctypes.byref(desc), ctypes.byref(h))
+        if st != 0:
+            raise AfqmcError(st, "afq_create failed")
+        self.h = h
+        sp, k1 = _csr(system.Spvn)
+        spT, k2 = _csr(system.SpvnT)
+        vk, k3 = _csr(system.Vakbl if use_vakbl else None)
+        P = np.ascontiguousarray(system.Propg1, np.complex128)
+        haj = np.ascontiguousarray(system.haj, np.complex128)
+        tr = np.ascontiguousarray(system.trial, np.complex128)
+        Lh = np.ascontiguousarray(system.Lh, np.complex128) if (use_chol and system.Lh is not None) else None
+        self._check(self.lib.afq_set_hamiltonian(
+            self.h, ctypes.byref(sp), ctypes.byref(spT), _p(P), _p(haj), _p(tr),
+            ctypes.byref(vk) if vk is not None else None, _p(Lh) if Lh is not None else None))
+        del k1, k2, k3
+        self.has_vakbl = vk is not None
+        self.has_chol = Lh is not None
+        W, Wd = walkers if walkers is not None else system.initial_walkers(nwalk)
+        self.set_walkers(W, Wd)
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = self.lib.afq_last_error(self.h)
+            raise AfqmcError(st, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.afq_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # state -------------------------------------------------------------------------
+    def set_walkers(self, W, Wd):
+        W = np.ascontiguousarray(W, np.complex128)
+        Wd = np.ascontiguousarray(Wd, np.complex128)
+        self._check(self.lib.afq_set_walkers(self.h, _p(W), _p(Wd)))
+
+    def get_walkers(self):
+        W = np.empty((self.nw, 2, self.N, self.n), np.complex128)
+        Wd = np.empty((self.nw, 8), np.complex128)
+        self._check(self.lib.afq_get_walkers(self.h, _p(W), _p(Wd)))
+        return W, Wd
+
+    def get_walker_data(self):
+        Wd = np.empty((self.nw, 8), np.complex128)
+        self._check(self.lib.afq_get_walkers(self.h, None, _p(Wd)))
+        return Wd
+
+    def copy_out(self, which: str) -> np.ndarray:
+        nw, N, n, nc = self.nw, self.N, self.n, self.nchol
+        shapes = {"Gc": ((2 * n * N, nw), np.complex128), "vbias": ((nc, nw), np.complex128),
+                  "X": ((nc, nw), np.complex128), "vHS": ((N * N, nw), np.complex128),
+                  "hybridW": ((nw,), np.complex128), "xraw": ((nc, nw), np.float64),
+                  "info": ((nw, 2), np.int32), "energy_parts": ((nw, 3), np.float64)}
+        shape, dt = shapes[which]
+        out = np.empty(shape, dt)
+        self._check(self.lib.afq_copy_out(self.h, BUFFERS[which], _p(out)))
+        return out
+
+    @property
+    def eshift(self) -> float:
+        v = ctypes.c_double()
+        self._check(self.lib.afq_get_eshift(self.h, ctypes.byref(v)))
+        return v.value
+
+    @eshift.setter
+    def eshift(self, value: float):
+        self._check(self.lib.afq_set_eshift(self.h, float(value)))
+
+    # operations (reference names) ------------------------------------------------
+    def calculate_mixed_density_matrix(self):
+        self._check(self.lib.afq_mixed_density_matrix(self.h))
+
+    def calculate_overlaps(self, save_old: bool = False):
+        self._check(self.lib.afq_overlaps(self.h, int(save_old)))
+
+    def get_vbias(self):
+        self._check(self.lib.afq_vbias(self.h))
+
+    def sigma(self, seed: int, step: int):
+        self._check(self.lib.afq_sigma(self.h, seed, step))
+
+    def sigma_from(self, x: np.ndarray):
+        x = np.ascontiguousarray(x, np.float64)
+        self._check(self.lib.afq_sigma_from(self.h, _p(x)))
+
+    def get_vHS(self):
+        self._check(self.lib.afq_vhs(self.h))
+
+    def propagate(self):
+        self._check(self.lib.afq_propagate(self.h))
+
+    def update_weights(self):
+        self._check(self.lib.afq_update_weights(self.h))
+
+    def update_weights_partial(self) -> float:
+        v = ctypes.c_double()
+        self._check(self.lib.afq_update_weights_partial(self.h, ctypes.byref(v)))
+        return v.value
+
+    def orthogonalize(self):
+        self._check(self.lib.afq_orthogonalize(self.h))
+
+    def set_walker_offset(self, offset: int, nwalk_global: int):
+        self._check(self.lib.afq_set_walker_offset(self.h, offset, nwalk_global))
+
+    def calculate_energy(self, mode: str = "auto") -> float:
+        m = self._mode(mode)
+        v = ctypes.c_double()
+        self._check(self.lib.afq_energy(self.h, m, ctypes.byref(v)))
+        return v.value
+
+    def energy_sums(self, mode: str = "auto"):
+        m = self._mode(mode)
+        buf = np.zeros(2)
+        self._check(self.lib.afq_energy_sums(self.h, m, _p(buf)))
+        return buf
+
+    def _mode(self, mode: str) -> int:
+        if mode == "auto":
+            mode = "chol" if self.has_chol else "vakbl"
+        return AFQ_ENERGY_VAKBL if mode == "vakbl" else AFQ_ENERGY_CHOLESKY
+
+    def substep(self, seed: int, step_tot: int, northo: int, graph: bool = True):
+        """One substep of the driver loop (miniafqmc_base.cpp:251-337)."""
+        if graph:
+            self._check(self.lib.afq_substep(self.h, seed, step_tot, northo))
+            return
+        self.calculate_mixed_density_matrix()
+        self.get_vbias()
+        self.sigma(seed, step_tot)
+        self.get_vHS()
+        self.propagate()
+        self.calculate_overlaps(save_old=True)
+        self.update_weights()
+        if step_tot > 0 and step_tot % northo == 0:
+            self.orthogonalize()
+            self.calculate_overlaps(save_old=False)
+
+    def synchronize(self):
+        self._check(self.lib.afq_synchronize(self.h))
+
+    def profile(self, enable: bool = True):
+        self._check(self.lib.afq_profile(self.h, int(enable)))
+
+    def stage_times(self, reset: bool = True):
+        """{stage: (gpu_ms, kernel_launches)} accumulated since the last reset."""
+        ms = np.zeros(len(STAGES))
+        nl = np.zeros(len(STAGES), np.int64)
+        self._check(self.lib.afq_stage_times(self.h, _p(ms), _p(nl), int(reset)))
+        return {k: (float(ms[i]), int(nl[i])) for i, k in enumerate(STAGES)}
+
+    @property
+    def stream(self) -> int:
+        v = ctypes.c_void_p()
+        self._check(self.lib.afq_get_stream(self.h, ctypes.byref(v)))
+        return v.value or 0

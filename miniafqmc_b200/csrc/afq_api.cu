@@ -1,0 +1,803 @@
+// C ABI of libafqmc_b200 (declared in include/afqmc_b200.h): the handle, device buffers,
+// one entry point per reference operation, and the CUDA-graph substep.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/afqmc_b200.h"
+#include "afq_kernels.h"
+#include "afq_mixed.h"
+#include "zgemm_fp64.cuh"
+
+using afq::launch_csr_gather;
+
+struct afq_handle {
+  afq_system_desc d{};
+  int N = 0, n = 0, nc = 0, nw = 0;
+  long long NAK = 0;
+  cudaStream_t st = nullptr;
+  std::string err;
+  bool have_ham = false;
+  bool have_walkers = false;
+  std::vector<void*> allocs;
+
+  z_t *W = nullptr, *Wd = nullptr, *tw = nullptr, *P = nullptr, *haj = nullptr;
+  z_t *Gc = nullptr, *vbias = nullptr, *X = nullptr, *hybridW = nullptr, *vHS = nullptr;
+  z_t *S = nullptr, *T1 = nullptr, *T2 = nullptr;
+  double* xraw = nullptr;
+  int* info = nullptr;
+  DevScalars* sc = nullptr;
+  DevScalars* h_sc = nullptr;  // pinned mirror
+
+  int *sp_ri = nullptr, *sp_ci = nullptr;
+  z_t* sp_v = nullptr;
+  double* sp_rv = nullptr;
+  z_t* spT_dense = nullptr;
+  int *spT_ri = nullptr, *spT_ci = nullptr;
+  z_t* spT_v = nullptr;
+  z_t* vk_dense = nullptr;
+  int *vk_ri = nullptr, *vk_ci = nullptr;
+  z_t* vk_v = nullptr;
+  bool have_vakbl = false;
+  z_t* Lh = nullptr;
+
+  z_t *Gcloc = nullptr, *cvec = nullptr, *Kpart = nullptr;
+  int nblk = 0;
+  double* parts = nullptr;
+
+  afq::MixedState* mixed = nullptr;
+
+  cudaGraphExec_t g_plain = nullptr, g_ortho = nullptr;
+  long long g_plain_launches[AFQ_NSTAGES] = {0}, g_ortho_launches[AFQ_NSTAGES] = {0};
+  unsigned long long host_seed = ~0ull, host_step = ~0ull;
+
+  // stage timers
+  struct Rec {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  bool profiling = false;
+  bool capturing = false;
+  std::vector<Rec> recs;
+  size_t nrec = 0;
+  double stage_ms[AFQ_NSTAGES] = {0};
+  long long stage_launches[AFQ_NSTAGES] = {0};
+  long long* launch_sink = nullptr;   // where launch counts go (capture counts per graph)
+};
+
+namespace {
+
+const double kDenseThreshold = 0.25;  // CSR operand above this density is densified
+
+afq_status fail(afq_handle* h, afq_status s, const std::string& msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+#define AFQ_CUDA(h, call)                                                               \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(h, e_ == cudaErrorMemoryAllocation ? AFQ_ERR_OOM : AFQ_ERR_CUDA,      \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(afq_handle* h, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
+  if (e != cudaSuccess) return e;
+  h->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return cudaSuccess;
+}
+
+void dfree(afq_handle* h, void* p) {
+  if (!p) return;
+  for (auto& q : h->allocs)
+    if (q == p) {
+      cudaFree(q);
+      q = nullptr;
+    }
+}
+
+__global__ void csr_to_dense_kernel(const int* ri, const int* ci, const z_t* v, int nrows,
+                                    long long ncols, z_t* out) {
+  int r = blockIdx.x * blockDim.y + threadIdx.y;
+  if (r >= nrows) return;
+  for (int p = ri[r] + threadIdx.x; p < ri[r + 1]; p += blockDim.x)
+    out[(long long)r * ncols + ci[p]] = v[p];
+}
+
+afq_status check_csr(afq_handle* h, const afq_csr_z* m, int nrows, int ncols, const char* name) {
+  if (!m || !m->rowIndex || !m->cols || !m->vals)
+    return fail(h, AFQ_ERR_ARG, std::string(name) + ": null CSR");
+  if (m->nrows != nrows || m->ncols != ncols)
+    return fail(h, AFQ_ERR_ARG, std::string(name) + ": wrong shape");
+  if (m->rowIndex[0] != 0) return fail(h, AFQ_ERR_ARG, std::string(name) + ": rowIndex[0] != 0");
+  long long nnz = m->rowIndex[nrows];
+  for (int r = 0; r < nrows; r++)
+    if (m->rowIndex[r + 1] < m->rowIndex[r])
+      return fail(h, AFQ_ERR_ARG, std::string(name) + ": rowIndex not monotone");
+  for (long long p = 0; p < nnz; p++)
+    if (m->cols[p] < 0 || m->cols[p] >= ncols)
+      return fail(h, AFQ_ERR_ARG, std::string(name) + ": column index out of range");
+  return AFQ_OK;
+}
+
+// Uploads a CSR; when dense_out is non-null and the density reaches the threshold, a
+// dense row-major copy is built on the device instead and the CSR arrays are released.
+afq_status upload_csr(afq_handle* h, const afq_csr_z* m, int** ri, int** ci, z_t** v,
+                      z_t** dense_out, bool allow_dense) {
+  long long nnz = m->rowIndex[m->nrows];
+  AFQ_CUDA(h, dalloc(h, ri, m->nrows + 1));
+  AFQ_CUDA(h, dalloc(h, ci, nnz));
+  AFQ_CUDA(h, dalloc(h, v, nnz));
+  AFQ_CUDA(h, cudaMemcpy(*ri, m->rowIndex, sizeof(int) * (m->nrows + 1), cudaMemcpyHostToDevice));
+  AFQ_CUDA(h, cudaMemcpy(*ci, m->cols, sizeof(int) * nnz, cudaMemcpyHostToDevice));
+  AFQ_CUDA(h, cudaMemcpy(*v, m->vals, sizeof(z_t) * nnz, cudaMemcpyHostToDevice));
+  double dens = (double)nnz / ((double)m->nrows * (double)m->ncols);
+  if (dense_out) *dense_out = nullptr;
+  if (allow_dense && dense_out && dens >= kDenseThreshold) {
+    size_t cnt = (size_t)m->nrows * m->ncols;
+    AFQ_CUDA(h, dalloc(h, dense_out, cnt));
+    AFQ_CUDA(h, cudaMemsetAsync(*dense_out, 0, sizeof(z_t) * cnt, h->st));
+    csr_to_dense_kernel<<<(m->nrows + 7) / 8, dim3(32, 8), 0, h->st>>>(*ri, *ci, *v, m->nrows,
+                                                                       m->ncols, *dense_out);
+    AFQ_CUDA(h, cudaGetLastError());
+    AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+    dfree(h, *ri); dfree(h, *ci); dfree(h, *v);
+    *ri = nullptr; *ci = nullptr; *v = nullptr;
+  }
+  return AFQ_OK;
+}
+
+cudaError_t collect_stage_times(afq_handle* h) {
+  if (h->nrec == 0) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return e;
+  for (size_t i = 0; i < h->nrec; i++) {
+    float ms = 0.f;
+    e = cudaEventElapsedTime(&ms, h->recs[i].a, h->recs[i].b);
+    if (e != cudaSuccess) return e;
+    h->stage_ms[h->recs[i].stage] += ms;
+  }
+  h->nrec = 0;
+  return cudaSuccess;
+}
+
+// Runs one stage body, counting its kernel launches and, with profiling on (and outside
+// stream capture), bracketing it with CUDA events on the handle's stream.
+template <class F>
+cudaError_t staged(afq_handle* h, int stage, int nlaunch, F&& body) {
+  (h->launch_sink ? h->launch_sink : h->stage_launches)[stage] += nlaunch;
+  if (!h->profiling || h->capturing) return body();
+  if (h->nrec == 4096) {
+    cudaError_t e = collect_stage_times(h);
+    if (e != cudaSuccess) return e;
+  }
+  if (h->nrec == h->recs.size()) {
+    afq_handle::Rec r{};
+    cudaError_t e = cudaEventCreate(&r.a);
+    if (e == cudaSuccess) e = cudaEventCreate(&r.b);
+    if (e != cudaSuccess) return e;
+    h->recs.push_back(r);
+  }
+  afq_handle::Rec& r = h->recs[h->nrec++];
+  r.stage = stage;
+  cudaError_t e = cudaEventRecord(r.a, h->st);
+  if (e != cudaSuccess) return e;
+  e = body();
+  if (e != cudaSuccess) return e;
+  return cudaEventRecord(r.b, h->st);
+}
+
+afq_status need_ready(afq_handle* h) {
+  if (!h) return AFQ_ERR_ARG;
+  if (!h->have_ham) return fail(h, AFQ_ERR_STATE, "Hamiltonian not set");
+  if (!h->have_walkers) return fail(h, AFQ_ERR_STATE, "walkers not set");
+  return AFQ_OK;
+}
+
+// ------------------------------------------------------------ stage bodies (async)
+cudaError_t body_dm(afq_handle* h, int want_gc, int save_old) {
+  return afq::launch_dm(h->W, h->tw, h->N, h->n, h->nw, h->Gc, h->Wd, h->info, want_gc, save_old,
+                        h->st);
+}
+
+cudaError_t body_vbias(afq_handle* h) {
+  if (h->mixed) return afq::mixed_vbias(h->mixed, h->Gc, h->vbias, h->st);
+  if (h->spT_dense) {
+    ZGemmDesc g{h->nc, h->nw, (int)h->NAK, h->spT_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+    EpiStore e{h->vbias, h->nw, 0, zmk(0, 0), 0};
+    return zgemm_launch<true, true>(g, 1, e, h->st);
+  }
+  return launch_csr_gather(h->spT_ri, h->spT_ci, h->spT_v, h->Gc, h->NAK, h->nc, h->nw, h->vbias,
+                           h->st);
+}
+
+cudaError_t body_sigma(afq_handle* h, int use_xraw) {
+  return afq::launch_sigma(h->vbias, h->X, h->xraw, h->hybridW, h->nc, h->nw, h->sc, use_xraw,
+                           h->st);
+}
+
+cudaError_t body_vhs(afq_handle* h) {
+  if (h->mixed) return afq::mixed_vhs(h->mixed, h->X, h->vHS, h->st);
+  return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, h->N * h->N, h->nw,
+                                h->vHS, (long long)h->N * h->N, h->st);
+}
+
+cudaError_t body_propagate(afq_handle* h) {
+  if (h->mixed) return afq::mixed_propagate(h->mixed, h->W, h->vHS, h->st);
+  const int N = h->N, n2 = 2 * h->n, nw = h->nw;
+  const long long sWN = (long long)N * n2, sV = (long long)N * N;
+  cudaError_t e;
+  {  // S = P W, T1 = S
+    ZGemmDesc g{N, n2, N, h->P, N, 0, h->W, n2, sWN, zmk(1, 0)};
+    EpiDual ep{h->T1, h->S, n2, sWN};
+    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st)) != cudaSuccess) return e;
+  }
+  z_t* cur = h->T1;
+  z_t* nxt = h->T2;
+  for (int k = 1; k <= h->d.taylor_order; k++) {  // T = (i/k) V T; S += T
+    ZGemmDesc g{N, n2, N, h->vHS, N, sV, cur, n2, sWN, zmk(0.0, 1.0 / (double)k)};
+    EpiTaylor ep{nxt, h->S, n2, sWN};
+    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st)) != cudaSuccess) return e;
+    std::swap(cur, nxt);
+  }
+  {  // W = P S
+    ZGemmDesc g{N, n2, N, h->P, N, 0, h->S, n2, sWN, zmk(1, 0)};
+    EpiStore ep{h->W, n2, sWN, zmk(0, 0), 0};
+    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t body_weights(afq_handle* h, int update_eshift) {
+  return afq::launch_weights(h->Wd, h->hybridW, h->nw, h->d.dt, h->sc, update_eshift, h->st);
+}
+
+cudaError_t body_ortho(afq_handle* h) { return afq::launch_ortho(h->W, h->N, h->n, h->nw, h->st); }
+
+cudaError_t body_energy(afq_handle* h, int mode) {
+  cudaError_t e;
+  const int nak = (int)h->NAK;
+  if (mode == AFQ_ENERGY_VAKBL) {
+    if (h->vk_dense) {
+      ZGemmDesc g{nak, h->nw, nak, h->vk_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+      EpiStore ep{h->Gcloc, h->nw, 0, zmk(0, 0), 0};
+      if ((e = zgemm_launch<true, true>(g, 1, ep, h->st)) != cudaSuccess) return e;
+    } else {
+      if ((e = launch_csr_gather(h->vk_ri, h->vk_ci, h->vk_v, h->Gc, h->NAK, nak, h->nw, h->Gcloc,
+                                 h->st)) != cudaSuccess)
+        return e;
+    }
+    if ((e = afq::launch_energy_reduce(h->Gc, h->haj, nak, h->Gcloc, nullptr, 0, nullptr, 0, h->nw,
+                                       0, h->Wd, nullptr, h->st)) != cudaSuccess)
+      return e;
+  } else {
+    if (h->mixed) {
+      if ((e = afq::mixed_energy_chol(h->mixed, h->Gc, h->cvec, h->Kpart, h->nblk, h->st)) !=
+          cudaSuccess)
+        return e;
+    } else {
+      ZGemmDesc g{h->nc, h->nw, nak, h->Lh, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+      EpiStore ep{h->cvec, h->nw, 0, zmk(0, 0), 0};
+      if ((e = zgemm_launch<true, true>(g, 1, ep, h->st)) != cudaSuccess) return e;
+      int nb = 0;
+      if ((e = afq::launch_exchange(h->Lh, h->Gc, h->N, h->n, h->nc, h->nw, h->Kpart, &nb,
+                                    h->st)) != cudaSuccess)
+        return e;
+    }
+    if ((e = afq::launch_energy_reduce(h->Gc, h->haj, nak, nullptr, h->cvec, h->nc, h->Kpart,
+                                       h->nblk, h->nw, 1, h->Wd, h->parts, h->st)) != cudaSuccess)
+      return e;
+  }
+  return afq::launch_eav(h->Wd, h->nw, h->sc, h->st);
+}
+
+// Timed / counted stages.  The launch counts are the kernels each body issues.
+cudaError_t st_dm(afq_handle* h, int want_gc, int save_old) {
+  return staged(h, want_gc ? AFQ_STAGE_DM : AFQ_STAGE_OVERLAP, 1,
+                [&] { return body_dm(h, want_gc, save_old); });
+}
+cudaError_t st_vbias(afq_handle* h) {
+  int nl = h->mixed ? afq::mixed_launches(h->mixed, AFQ_STAGE_VBIAS) : 1;
+  return staged(h, AFQ_STAGE_VBIAS, nl, [&] { return body_vbias(h); });
+}
+cudaError_t st_sigma(afq_handle* h, int use_xraw) {
+  return staged(h, AFQ_STAGE_SIGMA, 1, [&] { return body_sigma(h, use_xraw); });
+}
+cudaError_t st_vhs(afq_handle* h) {
+  int nl = h->mixed ? afq::mixed_launches(h->mixed, AFQ_STAGE_VHS) : 1;
+  return staged(h, AFQ_STAGE_VHS, nl, [&] { return body_vhs(h); });
+}
+cudaError_t st_propagate(afq_handle* h) {
+  int nl = h->mixed ? afq::mixed_launches(h->mixed, AFQ_STAGE_PROPAGATE) : h->d.taylor_order + 2;
+  return staged(h, AFQ_STAGE_PROPAGATE, nl, [&] { return body_propagate(h); });
+}
+cudaError_t st_weights(afq_handle* h, int update_eshift) {
+  return staged(h, AFQ_STAGE_WEIGHTS, 1, [&] { return body_weights(h, update_eshift); });
+}
+cudaError_t st_ortho(afq_handle* h) {
+  return staged(h, AFQ_STAGE_ORTHO, 1, [&] { return body_ortho(h); });
+}
+cudaError_t st_energy(afq_handle* h, int mode) {
+  int nl = mode == AFQ_ENERGY_VAKBL ? 3
+           : (h->mixed ? afq::mixed_launches(h->mixed, AFQ_STAGE_ENERGY) + 2 : 5);
+  return staged(h, AFQ_STAGE_ENERGY, nl, [&] { return body_energy(h, mode); });
+}
+
+cudaError_t st_substep(afq_handle* h, bool ortho) {
+  cudaError_t e;
+  if ((e = st_dm(h, 1, 0)) != cudaSuccess) return e;
+  if ((e = st_vbias(h)) != cudaSuccess) return e;
+  if ((e = st_sigma(h, 0)) != cudaSuccess) return e;
+  if ((e = st_vhs(h)) != cudaSuccess) return e;
+  if ((e = st_propagate(h)) != cudaSuccess) return e;
+  if ((e = st_dm(h, 0, 1)) != cudaSuccess) return e;
+  if ((e = st_weights(h, 1)) != cudaSuccess) return e;
+  if (ortho) {
+    if ((e = st_ortho(h)) != cudaSuccess) return e;
+    if ((e = st_dm(h, 0, 0)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+afq_status set_scalars(afq_handle* h, uint64_t seed, uint64_t step) {
+  AFQ_CUDA(h, afq::launch_set_scalars(h->sc, seed, step, 0, 0.0, h->st));
+  h->host_seed = seed;
+  h->host_step = step;
+  return AFQ_OK;
+}
+
+void drop_graphs(afq_handle* h) {
+  if (h->g_plain) cudaGraphExecDestroy(h->g_plain);
+  if (h->g_ortho) cudaGraphExecDestroy(h->g_ortho);
+  h->g_plain = h->g_ortho = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* afq_status_string(afq_status s) {
+  switch (s) {
+    case AFQ_OK: return "ok";
+    case AFQ_ERR_ARG: return "invalid argument";
+    case AFQ_ERR_STATE: return "call out of order";
+    case AFQ_ERR_CUDA: return "CUDA error";
+    case AFQ_ERR_OOM: return "out of device memory";
+    case AFQ_ERR_UNSUPPORTED: return "unsupported size or option";
+    case AFQ_ERR_SINGULAR: return "singular overlap matrix";
+  }
+  return "unknown status";
+}
+
+const char* afq_last_error(const afq_handle* h) { return h ? h->err.c_str() : ""; }
+
+afq_status afq_create(const afq_system_desc* desc, afq_handle** out) {
+  if (!desc || !out) return AFQ_ERR_ARG;
+  *out = nullptr;
+  if (desc->nmo <= 0 || desc->naea <= 0 || desc->nchol <= 0 || desc->nwalk <= 0 ||
+      desc->taylor_order < 0 || !(desc->dt > 0.0))
+    return AFQ_ERR_ARG;
+  if (desc->naea != desc->naeb) return AFQ_ERR_UNSUPPORTED;   // initialize_serial.hpp:67-71
+  if (desc->naea > 64 || desc->naea > desc->nmo) return AFQ_ERR_UNSUPPORTED;
+  if (desc->precision != AFQ_PREC_FP64 && desc->precision != AFQ_PREC_MIXED)
+    return AFQ_ERR_ARG;
+  afq_handle* h = new afq_handle();
+  h->d = *desc;
+  h->N = desc->nmo; h->n = desc->naea; h->nc = desc->nchol; h->nw = desc->nwalk;
+  h->NAK = 2LL * h->n * h->N;
+  cudaError_t e = cudaSetDevice(desc->device);
+  if (e != cudaSuccess) { delete h; return AFQ_ERR_CUDA; }
+  e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete h; return AFQ_ERR_CUDA; }
+  const size_t N = h->N, n = h->n, nw = h->nw, nc = h->nc;
+  afq_status s = AFQ_OK;
+  auto A = [&](cudaError_t r) { if (r != cudaSuccess && s == AFQ_OK) s = (r == cudaErrorMemoryAllocation) ? AFQ_ERR_OOM : AFQ_ERR_CUDA; };
+  A(dalloc(h, &h->W, nw * N * 2 * n));
+  A(dalloc(h, &h->Wd, nw * 8));
+  A(dalloc(h, &h->tw, N * 2 * n));
+  A(dalloc(h, &h->P, N * N));
+  A(dalloc(h, &h->haj, 2 * n * N));
+  A(dalloc(h, &h->Gc, nw * 2 * n * N));
+  A(dalloc(h, &h->vbias, nc * nw));
+  A(dalloc(h, &h->X, nc * nw));
+  A(dalloc(h, &h->xraw, nc * nw));
+  A(dalloc(h, &h->hybridW, nw));
+  A(dalloc(h, &h->vHS, nw * N * N));
+  A(dalloc(h, &h->S, nw * N * 2 * n));
+  A(dalloc(h, &h->T1, nw * N * 2 * n));
+  A(dalloc(h, &h->T2, nw * N * 2 * n));
+  A(dalloc(h, &h->info, nw * 2));
+  A(dalloc(h, &h->sc, 1));
+  A(dalloc(h, &h->cvec, nc * nw));
+  A(dalloc(h, &h->parts, nw * 3));
+  if (s == AFQ_OK) {
+    int nb = 0;
+    afq::launch_exchange(nullptr, nullptr, h->N, h->n, h->nc, h->nw, nullptr, &nb, h->st);
+    h->nblk = nb;
+    A(dalloc(h, &h->Kpart, nw * 2 * (size_t)nb));
+    A(cudaMallocHost(&h->h_sc, sizeof(DevScalars)));
+  }
+  if (s == AFQ_OK) {
+    A(cudaMemsetAsync(h->sc, 0, sizeof(DevScalars), h->st));
+    A(cudaMemsetAsync(h->Wd, 0, sizeof(z_t) * nw * 8, h->st));
+    A(cudaMemsetAsync(h->parts, 0, sizeof(double) * nw * 3, h->st));
+    A(cudaStreamSynchronize(h->st));
+  }
+  if (s != AFQ_OK) {
+    afq_destroy(h);
+    return s;
+  }
+  *out = h;
+  return AFQ_OK;
+}
+
+void afq_destroy(afq_handle* h) {
+  if (!h) return;
+  drop_graphs(h);
+  for (auto& r : h->recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  if (h->mixed) afq::mixed_destroy(h->mixed);
+  if (h->st) cudaStreamSynchronize(h->st);
+  for (void* p : h->allocs)
+    if (p) cudaFree(p);
+  if (h->h_sc) cudaFreeHost(h->h_sc);
+  if (h->st) cudaStreamDestroy(h->st);
+  delete h;
+}
+
+afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_csr_z* SpvnT,
+                               const double* Propg1, const double* haj, const double* trial,
+                               const afq_csr_z* Vakbl, const double* Lhalf) {
+  if (!h) return AFQ_ERR_ARG;
+  if (h->have_ham) return fail(h, AFQ_ERR_STATE, "Hamiltonian already set");
+  if (!Propg1 || !haj || !trial) return fail(h, AFQ_ERR_ARG, "null dense operand");
+  if (!Vakbl && !Lhalf) return fail(h, AFQ_ERR_ARG, "need Vakbl or Lhalf for the energy");
+  const int N = h->N, n = h->n, nc = h->nc;
+  const int NAK = (int)h->NAK;
+  afq_status s;
+  if ((s = check_csr(h, Spvn, N * N, nc, "Spvn")) != AFQ_OK) return s;
+  if ((s = check_csr(h, SpvnT, nc, NAK, "SpvnT")) != AFQ_OK) return s;
+  if (Vakbl && (s = check_csr(h, Vakbl, NAK, NAK, "Vakbl")) != AFQ_OK) return s;
+  cudaSetDevice(h->d.device);
+  // Spvn: keep real values only when every imaginary part is zero
+  {
+    long long nnz = Spvn->rowIndex[N * N];
+    bool real = true;
+    for (long long p = 0; p < nnz && real; p++) real = Spvn->vals[2 * p + 1] == 0.0;
+    AFQ_CUDA(h, dalloc(h, &h->sp_ri, (size_t)N * N + 1));
+    AFQ_CUDA(h, dalloc(h, &h->sp_ci, nnz));
+    AFQ_CUDA(h, cudaMemcpy(h->sp_ri, Spvn->rowIndex, sizeof(int) * ((size_t)N * N + 1),
+                           cudaMemcpyHostToDevice));
+    AFQ_CUDA(h, cudaMemcpy(h->sp_ci, Spvn->cols, sizeof(int) * nnz, cudaMemcpyHostToDevice));
+    if (real) {
+      std::vector<double> rv(nnz);
+      for (long long p = 0; p < nnz; p++) rv[p] = Spvn->vals[2 * p];
+      AFQ_CUDA(h, dalloc(h, &h->sp_rv, nnz));
+      AFQ_CUDA(h, cudaMemcpy(h->sp_rv, rv.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice));
+    } else {
+      AFQ_CUDA(h, dalloc(h, &h->sp_v, nnz));
+      AFQ_CUDA(h, cudaMemcpy(h->sp_v, Spvn->vals, sizeof(z_t) * nnz, cudaMemcpyHostToDevice));
+    }
+  }
+  if ((s = upload_csr(h, SpvnT, &h->spT_ri, &h->spT_ci, &h->spT_v, &h->spT_dense, true)) != AFQ_OK)
+    return s;
+  if (Vakbl) {
+    if ((s = upload_csr(h, Vakbl, &h->vk_ri, &h->vk_ci, &h->vk_v, &h->vk_dense, true)) != AFQ_OK)
+      return s;
+    AFQ_CUDA(h, dalloc(h, &h->Gcloc, (size_t)NAK * h->nw));
+    h->have_vakbl = true;
+  }
+  if (Lhalf) {
+    AFQ_CUDA(h, dalloc(h, &h->Lh, (size_t)nc * NAK));
+    AFQ_CUDA(h, cudaMemcpy(h->Lh, Lhalf, sizeof(z_t) * (size_t)nc * NAK, cudaMemcpyHostToDevice));
+  }
+  AFQ_CUDA(h, cudaMemcpy(h->P, Propg1, sizeof(z_t) * (size_t)N * N, cudaMemcpyHostToDevice));
+  AFQ_CUDA(h, cudaMemcpy(h->haj, haj, sizeof(z_t) * (size_t)NAK, cudaMemcpyHostToDevice));
+  {  // trial [2][N][n] -> [N][2n]
+    std::vector<z_t> t((size_t)N * 2 * n);
+    const z_t* src = reinterpret_cast<const z_t*>(trial);
+    for (int s2 = 0; s2 < 2; s2++)
+      for (int i = 0; i < N; i++)
+        for (int a = 0; a < n; a++) t[(size_t)i * 2 * n + s2 * n + a] = src[((size_t)s2 * N + i) * n + a];
+    AFQ_CUDA(h, cudaMemcpy(h->tw, t.data(), sizeof(z_t) * t.size(), cudaMemcpyHostToDevice));
+  }
+  if (h->d.precision == AFQ_PREC_MIXED) {
+    afq::MixedInit mi{};
+    mi.N = N; mi.n = n; mi.nchol = nc; mi.nw = h->nw; mi.order = h->d.taylor_order;
+    mi.P = h->P; mi.Lh = h->Lh; mi.SpvnT_dense = h->spT_dense;
+    mi.sp_ri = h->sp_ri; mi.sp_ci = h->sp_ci; mi.sp_v = h->sp_v; mi.sp_rv = h->sp_rv;
+    std::string msg;
+    cudaError_t e = afq::mixed_create(&mi, &h->mixed, &msg, h->st);
+    if (e != cudaSuccess || !h->mixed)
+      return fail(h, e == cudaSuccess ? AFQ_ERR_UNSUPPORTED : AFQ_ERR_CUDA, "mixed: " + msg);
+  }
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  h->have_ham = true;
+  return AFQ_OK;
+}
+
+afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data) {
+  if (!h || !W || !W_data) return AFQ_ERR_ARG;
+  const size_t N = h->N, n = h->n, nw = h->nw;
+  std::vector<z_t> t(nw * N * 2 * n);
+  const z_t* src = reinterpret_cast<const z_t*>(W);
+  for (size_t w = 0; w < nw; w++)
+    for (int s = 0; s < 2; s++)
+      for (size_t i = 0; i < N; i++)
+        for (size_t a = 0; a < n; a++)
+          t[(w * N + i) * 2 * n + s * n + a] = src[((w * 2 + s) * N + i) * n + a];
+  cudaSetDevice(h->d.device);
+  AFQ_CUDA(h, cudaMemcpyAsync(h->W, t.data(), sizeof(z_t) * t.size(), cudaMemcpyHostToDevice, h->st));
+  AFQ_CUDA(h, cudaMemcpyAsync(h->Wd, W_data, sizeof(z_t) * nw * 8, cudaMemcpyHostToDevice, h->st));
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  h->have_walkers = true;
+  return AFQ_OK;
+}
+
+afq_status afq_get_walkers(afq_handle* h, double* W, double* W_data) {
+  if (!h) return AFQ_ERR_ARG;
+  const size_t N = h->N, n = h->n, nw = h->nw;
+  cudaSetDevice(h->d.device);
+  if (W) {
+    std::vector<z_t> t(nw * N * 2 * n);
+    AFQ_CUDA(h, cudaMemcpyAsync(t.data(), h->W, sizeof(z_t) * t.size(), cudaMemcpyDeviceToHost, h->st));
+    AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+    z_t* dst = reinterpret_cast<z_t*>(W);
+    for (size_t w = 0; w < nw; w++)
+      for (int s = 0; s < 2; s++)
+        for (size_t i = 0; i < N; i++)
+          for (size_t a = 0; a < n; a++)
+            dst[((w * 2 + s) * N + i) * n + a] = t[(w * N + i) * 2 * n + s * n + a];
+  }
+  if (W_data) {
+    AFQ_CUDA(h, cudaMemcpyAsync(W_data, h->Wd, sizeof(z_t) * nw * 8, cudaMemcpyDeviceToHost, h->st));
+    AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  }
+  return AFQ_OK;
+}
+
+afq_status afq_mixed_density_matrix(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_dm(h, 1, 0));
+  return AFQ_OK;
+}
+
+afq_status afq_overlaps(afq_handle* h, int save_old) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_dm(h, 0, save_old ? 1 : 0));
+  return AFQ_OK;
+}
+
+afq_status afq_vbias(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_vbias(h));
+  return AFQ_OK;
+}
+
+afq_status afq_sigma(afq_handle* h, uint64_t seed, uint64_t step) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if ((s = set_scalars(h, seed, step)) != AFQ_OK) return s;
+  AFQ_CUDA(h, st_sigma(h, 0));
+  return AFQ_OK;
+}
+
+afq_status afq_sigma_from(afq_handle* h, const double* x) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (!x) return fail(h, AFQ_ERR_ARG, "null x");
+  AFQ_CUDA(h, cudaMemcpyAsync(h->xraw, x, sizeof(double) * (size_t)h->nc * h->nw,
+                              cudaMemcpyHostToDevice, h->st));
+  AFQ_CUDA(h, st_sigma(h, 1));
+  return AFQ_OK;
+}
+
+afq_status afq_vhs(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_vhs(h));
+  return AFQ_OK;
+}
+
+afq_status afq_propagate(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_propagate(h));
+  return AFQ_OK;
+}
+
+afq_status afq_update_weights(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_weights(h, 1));
+  h->host_step++;
+  return AFQ_OK;
+}
+
+afq_status afq_update_weights_partial(afq_handle* h, double* e4_sum) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (!e4_sum) return fail(h, AFQ_ERR_ARG, "null e4_sum");
+  AFQ_CUDA(h, st_weights(h, 0));
+  h->host_step++;
+  AFQ_CUDA(h, cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  *e4_sum = h->h_sc->e4sum;
+  return AFQ_OK;
+}
+
+afq_status afq_get_eshift(afq_handle* h, double* eshift) {
+  if (!h || !eshift) return AFQ_ERR_ARG;
+  AFQ_CUDA(h, cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  *eshift = h->h_sc->eshift;
+  return AFQ_OK;
+}
+
+afq_status afq_set_eshift(afq_handle* h, double eshift) {
+  if (!h) return AFQ_ERR_ARG;
+  uint64_t seed = h->host_seed == ~0ull ? 0 : h->host_seed;
+  uint64_t step = h->host_step == ~0ull ? 0 : h->host_step;
+  AFQ_CUDA(h, afq::launch_set_scalars(h->sc, seed, step, 1, eshift, h->st));
+  h->host_seed = seed;
+  h->host_step = step;
+  return AFQ_OK;
+}
+
+afq_status afq_set_walker_offset(afq_handle* h, int offset, int nwalk_global) {
+  if (!h || offset < 0 || nwalk_global < offset + h->nw) return AFQ_ERR_ARG;
+  uint64_t seed = h->host_seed == ~0ull ? 0 : h->host_seed;
+  uint64_t step = h->host_step == ~0ull ? 0 : h->host_step;
+  AFQ_CUDA(h, afq::launch_set_scalars(h->sc, seed, step, 0, 0.0, h->st, offset, nwalk_global));
+  h->host_seed = seed;
+  h->host_step = step;
+  return AFQ_OK;
+}
+
+afq_status afq_orthogonalize(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  AFQ_CUDA(h, st_ortho(h));
+  return AFQ_OK;
+}
+
+afq_status afq_energy_sums(afq_handle* h, int mode, double* sums) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (!sums) return fail(h, AFQ_ERR_ARG, "null sums");
+  if (mode == AFQ_ENERGY_VAKBL && !h->have_vakbl) return fail(h, AFQ_ERR_STATE, "no Vakbl loaded");
+  if (mode == AFQ_ENERGY_CHOLESKY && !h->Lh) return fail(h, AFQ_ERR_STATE, "no Lhalf loaded");
+  if (mode != AFQ_ENERGY_VAKBL && mode != AFQ_ENERGY_CHOLESKY) return fail(h, AFQ_ERR_ARG, "mode");
+  AFQ_CUDA(h, st_energy(h, mode));
+  AFQ_CUDA(h, cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  sums[0] = h->h_sc->esum[0];
+  sums[1] = h->h_sc->esum[1];
+  return AFQ_OK;
+}
+
+afq_status afq_energy(afq_handle* h, int mode, double* eav) {
+  double sums[2];
+  afq_status s = afq_energy_sums(h, mode, sums);
+  if (s != AFQ_OK) return s;
+  if (eav) *eav = sums[0] / sums[1];
+  return AFQ_OK;
+}
+
+afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int northo) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (northo <= 0) return fail(h, AFQ_ERR_ARG, "northo must be positive");
+  if (seed != h->host_seed || step_tot != h->host_step)
+    if ((s = set_scalars(h, seed, step_tot)) != AFQ_OK) return s;
+  const bool ortho = step_tot > 0 && step_tot % (uint64_t)northo == 0;
+  cudaGraphExec_t* slot = ortho ? &h->g_ortho : &h->g_plain;
+  long long* counts = ortho ? h->g_ortho_launches : h->g_plain_launches;
+  if (!*slot) {
+    cudaGraph_t g = nullptr;
+    AFQ_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
+    h->capturing = true;
+    for (int i = 0; i < AFQ_NSTAGES; i++) counts[i] = 0;
+    h->launch_sink = counts;
+    cudaError_t e = st_substep(h, ortho);
+    h->launch_sink = nullptr;
+    h->capturing = false;
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(h, AFQ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    }
+    AFQ_CUDA(h, e2);
+    e = cudaGraphInstantiate(slot, g, 0);
+    cudaGraphDestroy(g);
+    AFQ_CUDA(h, e);
+  }
+  AFQ_CUDA(h, cudaGraphLaunch(*slot, h->st));
+  for (int i = 0; i < AFQ_NSTAGES; i++) h->stage_launches[i] += counts[i];
+  h->host_step = step_tot + 1;
+  return AFQ_OK;
+}
+
+afq_status afq_profile(afq_handle* h, int enable) {
+  if (!h) return AFQ_ERR_ARG;
+  h->profiling = enable != 0;
+  return AFQ_OK;
+}
+
+afq_status afq_stage_times(afq_handle* h, double* ms, long long* launches, int reset) {
+  if (!h) return AFQ_ERR_ARG;
+  AFQ_CUDA(h, collect_stage_times(h));
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  for (int i = 0; i < AFQ_NSTAGES; i++) {
+    if (ms) ms[i] = h->stage_ms[i];
+    if (launches) launches[i] = h->stage_launches[i];
+    if (reset) {
+      h->stage_ms[i] = 0.0;
+      h->stage_launches[i] = 0;
+    }
+  }
+  return AFQ_OK;
+}
+
+afq_status afq_get_stream(afq_handle* h, void** stream) {
+  if (!h || !stream) return AFQ_ERR_ARG;
+  *stream = (void*)h->st;
+  return AFQ_OK;
+}
+
+afq_status afq_synchronize(afq_handle* h) {
+  if (!h) return AFQ_ERR_ARG;
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  return AFQ_OK;
+}
+
+afq_status afq_copy_out(afq_handle* h, int which, void* host) {
+  if (!h || !host) return AFQ_ERR_ARG;
+  const size_t N = h->N, nw = h->nw, nc = h->nc, NAK = h->NAK;
+  cudaSetDevice(h->d.device);
+  auto d2h = [&](void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    return e;
+  };
+  switch (which) {
+    case AFQ_BUF_GC: {
+      std::vector<z_t> t(nw * NAK);
+      AFQ_CUDA(h, d2h(t.data(), h->Gc, sizeof(z_t) * t.size()));
+      z_t* dst = static_cast<z_t*>(host);
+      for (size_t w = 0; w < nw; w++)
+        for (size_t i = 0; i < NAK; i++) dst[i * nw + w] = t[w * NAK + i];
+      break;
+    }
+    case AFQ_BUF_VHS: {
+      std::vector<z_t> t(nw * N * N);
+      AFQ_CUDA(h, d2h(t.data(), h->vHS, sizeof(z_t) * t.size()));
+      z_t* dst = static_cast<z_t*>(host);
+      for (size_t w = 0; w < nw; w++)
+        for (size_t i = 0; i < N * N; i++) dst[i * nw + w] = t[w * N * N + i];
+      break;
+    }
+    case AFQ_BUF_VBIAS: AFQ_CUDA(h, d2h(host, h->vbias, sizeof(z_t) * nc * nw)); break;
+    case AFQ_BUF_X: AFQ_CUDA(h, d2h(host, h->X, sizeof(z_t) * nc * nw)); break;
+    case AFQ_BUF_HYBRIDW: AFQ_CUDA(h, d2h(host, h->hybridW, sizeof(z_t) * nw)); break;
+    case AFQ_BUF_XRAW: AFQ_CUDA(h, d2h(host, h->xraw, sizeof(double) * nc * nw)); break;
+    case AFQ_BUF_INFO: AFQ_CUDA(h, d2h(host, h->info, sizeof(int) * nw * 2)); break;
+    case AFQ_BUF_ENERGY_PARTS: AFQ_CUDA(h, d2h(host, h->parts, sizeof(double) * nw * 3)); break;
+    default: return fail(h, AFQ_ERR_ARG, "unknown buffer");
+  }
+  return AFQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,33 @@
+// Launch wrappers of the walker-step kernels (internal to libafqmc_b200).
+#pragma once
+#include <algorithm>
+#include <cstddef>
+#include "afq_common.cuh"
+
+namespace afq {
+
+size_t dm_smem_bytes(int n);
+cudaError_t launch_dm(const z_t* W, const z_t* tw, int N, int n, int nw, z_t* Gc, z_t* Wd,
+                      int* info, int want_gc, int save_old, cudaStream_t st);
+cudaError_t launch_sigma(const z_t* vbias, z_t* X, double* xraw, z_t* hybridW, int nchol,
+                         int nw, const DevScalars* sc, int use_xraw, cudaStream_t st);
+cudaError_t launch_csr_walker(const int* rowIndex, const int* cols, const z_t* zvals,
+                              const double* rvals, const z_t* B, int nrows, int nw, z_t* out,
+                              long long out_ld, cudaStream_t st);
+cudaError_t launch_csr_gather(const int* rowIndex, const int* cols, const z_t* vals, const z_t* G,
+                              long long ldg, int nrows, int nw, z_t* out, cudaStream_t st);
+cudaError_t launch_weights(z_t* Wd, const z_t* hybridW, int nw, double dt, DevScalars* sc,
+                           int update_eshift, cudaStream_t st);
+cudaError_t launch_set_scalars(DevScalars* sc, unsigned long long seed, unsigned long long step,
+                               int set_eshift, double eshift, cudaStream_t st,
+                               int walker_offset = 0, long long nwalk_global = 0);
+cudaError_t launch_ortho(z_t* W, int N, int n, int nw, cudaStream_t st);
+size_t exch_smem_bytes();
+cudaError_t launch_exchange(const z_t* Lh, const z_t* Gc, int N, int n, int nchol, int nw,
+                            z_t* Kpart, int* nblk_out, cudaStream_t st);
+cudaError_t launch_energy_reduce(const z_t* Gc, const z_t* haj, int nak, const z_t* Gcloc,
+                                 const z_t* cv, int nchol, const z_t* Kpart, int nblk, int nw,
+                                 int mode, z_t* Wd, double* parts, cudaStream_t st);
+cudaError_t launch_eav(const z_t* Wd, int nw, DevScalars* sc, cudaStream_t st);
+
+}  // namespace afq

@@ -1,0 +1,34 @@
+// Mixed-precision (tensor-core) form of the contraction stages.  FP64 stays in the
+// LU/overlaps, QR and weights; these entry points replace vbias, vHS, the propagation
+// chain and the Cholesky energy when the handle is created with AFQ_PREC_MIXED.
+#pragma once
+#include <string>
+#include "afq_common.cuh"
+
+namespace afq {
+
+struct MixedState;
+
+struct MixedInit {
+  int N, n, nchol, nw, order;
+  const z_t* P;             // Propg1 [N][N]
+  const z_t* Lh;            // [nchol][2nN] unscaled (may be null)
+  const z_t* SpvnT_dense;   // [nchol][2nN] or null
+  const int* sp_ri;         // Spvn CSR
+  const int* sp_ci;
+  const z_t* sp_v;
+  const double* sp_rv;
+};
+
+cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* msg,
+                         cudaStream_t st);
+void mixed_destroy(MixedState* m);
+cudaError_t mixed_vbias(MixedState* m, const z_t* Gc, z_t* vbias, cudaStream_t st);
+cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t* vHS, cudaStream_t st);
+cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t* vHS, cudaStream_t st);
+cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpart, int nblk,
+                              cudaStream_t st);
+// Kernels one call of a stage issues (afq_stage numbering), for the launch counters.
+int mixed_launches(const MixedState* m, int stage);
+
+}  // namespace afq

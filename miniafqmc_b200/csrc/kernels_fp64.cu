@@ -1,0 +1,755 @@
+// FP64 kernels of the walker step (the plain form): mixed density matrix and overlaps,
+// sigma (Philox), CSR SpMM for vHS / vbias / Vakbl, weight update, Householder
+// re-orthogonalisation and the local energy.  Internal device layouts:
+//   W   [nw][N][2n]   (spin s occupies columns s*n .. s*n+n-1 of each row)
+//   tw  [N][2n]       trial, same interleave
+//   Gc  [nw][2][n][N] per-walker compact density matrices (linear index s*n*N + a*N + k)
+//   vHS [nw][N][N], vbias / X / xraw [nchol][nw] (reference layout)
+#include "afq_kernels.h"
+#include "afq_common.cuh"
+
+namespace afq {
+
+// ============================================================ mixed density matrix
+// One CTA per (walker, spin).  T1 = W_s^T tw_s (n x n, mixed_density_matrix.hpp:83);
+// Gauss-Jordan with partial pivoting (max |re|+|im|, as izamax) gives det(T1) and
+// T1^-1 (ma_operations.hpp:244-260); Gc_s = T1^-1 W_s^T (mixed_density_matrix.hpp:91).
+// want_gc == 0 runs only the LU elimination for the determinant (Overlap, :124-138).
+constexpr int DM_KC = 32;
+constexpr int DM_THREADS = 256;
+
+size_t dm_smem_bytes(int n) {
+  size_t ldT = n + 1;
+  size_t buf = std::max((size_t)2 * DM_KC * n, (size_t)n * (DM_KC + 1));
+  return sizeof(z_t) * (n * ldT + buf + n) + sizeof(int) * n;
+}
+
+__global__ void __launch_bounds__(DM_THREADS)
+dm_kernel(const z_t* __restrict__ W, const z_t* __restrict__ tw, int N, int n,
+          z_t* __restrict__ Gc, z_t* __restrict__ Wd, int* __restrict__ info, int want_gc,
+          int save_old) {
+  extern __shared__ __align__(16) unsigned char dm_smem[];
+  const int w = blockIdx.x >> 1, s = blockIdx.x & 1;
+  const int ldT = n + 1;
+  z_t* T = reinterpret_cast<z_t*>(dm_smem);
+  z_t* buf = T + n * ldT;
+  const int bufsz = max(2 * DM_KC * n, n * (DM_KC + 1));
+  z_t* fcol = buf + bufsz;
+  int* perm = reinterpret_cast<int*>(fcol + n);
+  __shared__ int s_piv, s_sing;
+  const long long ldw = 2 * n;
+  const z_t* Ws = W + (long long)w * N * ldw + s * n;
+  const z_t* ts = tw + s * n;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int nout = n * n;
+
+  // ---- phase 1: T1 = W_s^T tw_s
+  z_t acc[16];
+#pragma unroll
+  for (int r = 0; r < 16; r++) acc[r] = zmk(0, 0);
+  for (int k0 = 0; k0 < N; k0 += DM_KC) {
+    const int kc = min(DM_KC, N - k0);
+    for (int e = tid; e < kc * n; e += nt) {
+      int kk = e / n, a = e % n;
+      buf[kk * n + a] = Ws[(long long)(k0 + kk) * ldw + a];
+      buf[DM_KC * n + kk * n + a] = ts[(long long)(k0 + kk) * ldw + a];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+      int o = tid + r * DM_THREADS;
+      if (o < nout) {
+        int a = o / n, b = o % n;
+        z_t t = acc[r];
+        for (int kk = 0; kk < kc; kk++) zfma(t, buf[kk * n + a], buf[DM_KC * n + kk * n + b]);
+        acc[r] = t;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 16; r++) {
+    int o = tid + r * DM_THREADS;
+    if (o < nout) T[(o / n) * ldT + (o % n)] = acc[r];
+  }
+  if (tid == 0) s_sing = 0;
+  __syncthreads();
+
+  // ---- phase 2: pivoted elimination
+  z_t det = zmk(1.0, 0.0);
+  for (int j = 0; j < n; j++) {
+    if (tid < 32) {
+      double best = -1.0;
+      int bi = n;
+      for (int i = j + tid; i < n; i += 32) {
+        double v = zabs1(T[i * ldT + j]);
+        if (v > best) { best = v; bi = i; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (tid == 0) { s_piv = bi; perm[j] = bi; }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != j)
+      for (int c = tid; c < n; c += nt) {
+        z_t t = T[j * ldT + c];
+        T[j * ldT + c] = T[p * ldT + c];
+        T[p * ldT + c] = t;
+      }
+    __syncthreads();
+    const z_t pv = T[j * ldT + j];
+    if (pv.x == 0.0 && pv.y == 0.0) {  // exactly singular: uniform across the CTA
+      if (tid == 0) s_sing = 1;
+      break;
+    }
+    if (tid == 0) {
+      det = zmul(det, pv);
+      if (p != j) det = zmk(-det.x, -det.y);
+    }
+    const z_t inv = zrecip(pv);
+    if (!want_gc) {
+      const int m = n - j - 1;
+      for (int e = tid; e < m * m; e += nt) {
+        int i = j + 1 + e / m, c = j + 1 + e % m;
+        z_t f = zmul(T[i * ldT + j], inv);
+        T[i * ldT + c] = zsub(T[i * ldT + c], zmul(f, T[j * ldT + c]));
+      }
+      __syncthreads();
+    } else {
+      for (int i = tid; i < n; i += nt) fcol[i] = T[i * ldT + j];
+      __syncthreads();
+      for (int c = tid; c < n; c += nt)
+        T[j * ldT + c] = (c == j) ? inv : zmul(T[j * ldT + c], inv);
+      __syncthreads();
+      for (int e = tid; e < nout; e += nt) {
+        int i = e / n, c = e % n;
+        if (i == j) continue;
+        z_t base = (c == j) ? zmk(0, 0) : T[i * ldT + c];
+        T[i * ldT + c] = zsub(base, zmul(fcol[i], T[j * ldT + c]));
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  const int sing = s_sing;
+  if (sing) det = zmk(0, 0);
+
+  // ---- phase 3: Gc_s = T1^-1 W_s^T
+  if (want_gc) {
+    z_t* Gout = Gc + ((long long)w * 2 + s) * n * N;
+    if (!sing) {
+      for (int j = n - 1; j >= 0; j--) {   // undo the row interchanges on the columns
+        int p = perm[j];
+        if (p != j)
+          for (int r = tid; r < n; r += nt) {
+            z_t t = T[r * ldT + j];
+            T[r * ldT + j] = T[r * ldT + p];
+            T[r * ldT + p] = t;
+          }
+        __syncthreads();
+      }
+    }
+    for (int k0 = 0; k0 < N; k0 += DM_KC) {
+      const int kc = min(DM_KC, N - k0);
+      for (int e = tid; e < kc * n; e += nt) {
+        int kk = e / n, b = e % n;
+        buf[b * (DM_KC + 1) + kk] = Ws[(long long)(k0 + kk) * ldw + b];
+      }
+      __syncthreads();
+      for (int e = tid; e < n * DM_KC; e += nt) {
+        int a = e / DM_KC, kk = e % DM_KC;
+        if (kk < kc) {
+          z_t t = zmk(0, 0);
+          if (!sing)
+            for (int b = 0; b < n; b++) zfma(t, T[a * ldT + b], buf[b * (DM_KC + 1) + kk]);
+          Gout[(long long)a * N + k0 + kk] = t;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) {
+    z_t* d = Wd + (long long)w * 8;
+    if (save_old) {
+      if (s == 0) d[5] = d[4];
+      d[6 + s] = d[2 + s];
+    }
+    d[2 + s] = det;
+    info[w * 2 + s] = sing;
+  }
+}
+
+cudaError_t launch_dm(const z_t* W, const z_t* tw, int N, int n, int nw, z_t* Gc, z_t* Wd,
+                      int* info, int want_gc, int save_old, cudaStream_t st) {
+  size_t smem = dm_smem_bytes(n);
+  static size_t attr = 0;
+  if (smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  dm_kernel<<<2 * nw, DM_THREADS, smem, st>>>(W, tw, N, n, Gc, Wd, info, want_gc, save_old);
+  return cudaGetLastError();
+}
+
+// ============================================================ sigma
+// X = x + i vbias, hybridW[w] = -sum_c i vb (x + i/2 vb)  (miniafqmc_base.cpp:281-289).
+// Block (32 walkers) x (32 groups of Cholesky rows); fixed-order reduction over groups.
+__global__ void __launch_bounds__(1024)
+sigma_kernel(const z_t* __restrict__ vbias, z_t* __restrict__ X, double* __restrict__ xraw,
+             z_t* __restrict__ hybridW, int nchol, int nw, const DevScalars* __restrict__ sc,
+             int use_xraw) {
+  __shared__ z_t red[32][33];
+  const int lane = threadIdx.x, g = threadIdx.y;
+  const int w = blockIdx.x * 32 + lane;
+  const unsigned long long seed = sc->seed, step = sc->step;
+  const long long nwg = sc->nwalk_global > 0 ? sc->nwalk_global : nw;
+  const long long woff = sc->walker_offset;
+  z_t hw = zmk(0, 0);
+  if (w < nw) {
+    for (int c = g; c < nchol; c += 32) {
+      long long e = (long long)c * nw + w;
+      double x;
+      if (use_xraw) {
+        x = xraw[e];
+      } else {
+        // the stream is indexed by the global walker so shards reproduce one ensemble
+        long long eg = (long long)c * nwg + woff + w;
+        double x0, x1;
+        normal_pair(seed, step, (unsigned long long)eg >> 1, &x0, &x1);
+        x = (eg & 1) ? x1 : x0;
+        xraw[e] = x;
+      }
+      z_t vb = vbias[e];
+      z_t ivb = zmk(-vb.y, vb.x);                      // i vb
+      z_t t = zmk(x - 0.5 * vb.y, 0.5 * vb.x);         // x + (i/2) vb
+      hw = zsub(hw, zmul(ivb, t));
+      X[e] = zmk(x - vb.y, vb.x);                      // x + i vb
+    }
+  }
+  red[g][lane] = hw;
+  __syncthreads();
+  if (g == 0 && w < nw) {
+    z_t s = zmk(0, 0);
+    for (int q = 0; q < 32; q++) s = zadd(s, red[q][lane]);
+    hybridW[w] = s;
+  }
+}
+
+cudaError_t launch_sigma(const z_t* vbias, z_t* X, double* xraw, z_t* hybridW, int nchol,
+                         int nw, const DevScalars* sc, int use_xraw, cudaStream_t st) {
+  sigma_kernel<<<(nw + 31) / 32, dim3(32, 32), 0, st>>>(vbias, X, xraw, hybridW, nchol, nw, sc,
+                                                         use_xraw);
+  return cudaGetLastError();
+}
+
+// ============================================================ CSR x dense (walker-fast B)
+// out[w][r] = sum_p A[p] B[col(p)][w] for the rows r of a CSR, B [ncols][nw] walker
+// fastest (vHS = Spvn X, vHS.hpp:47-56).  A warp owns a row; its lanes own walkers;
+// the nonzeros of a row are fetched 32 at a time and broadcast with shuffles.  The CTA
+// stages its [rows x walkers] results in shared memory and writes them walker-major.
+constexpr int VHS_ROWS = 16;      // warps (rows) per CTA
+constexpr int VHS_WALK = 64;      // walkers per CTA (2 per lane)
+
+template <bool REALV>
+__global__ void __launch_bounds__(VHS_ROWS * 32)
+csr_walker_kernel(const int* __restrict__ rowIndex, const int* __restrict__ cols,
+                  const z_t* __restrict__ zvals, const double* __restrict__ rvals,
+                  const z_t* __restrict__ B, int nrows, int nw, z_t* __restrict__ out,
+                  long long out_ld) {
+  __shared__ z_t tile[VHS_ROWS][VHS_WALK + 1];
+  const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
+  const int r0 = blockIdx.x * VHS_ROWS, r = r0 + wy;
+  const int w0 = blockIdx.y * VHS_WALK;
+  const int wa = w0 + lane, wb = w0 + 32 + lane;
+  z_t acc0 = zmk(0, 0), acc1 = zmk(0, 0);
+  if (r < nrows) {
+    const int beg = rowIndex[r], end = rowIndex[r + 1];
+    for (int p0 = beg; p0 < end; p0 += 32) {
+      const int cnt = min(32, end - p0);
+      int myc = 0;
+      z_t myv = zmk(0, 0);
+      double myr = 0.0;
+      if (lane < cnt) {
+        myc = cols[p0 + lane];
+        if (REALV) myr = rvals[p0 + lane];
+        else myv = zvals[p0 + lane];
+      }
+      for (int q = 0; q < cnt; q++) {
+        const int c = __shfl_sync(0xffffffffu, myc, q);
+        const z_t* br = B + (long long)c * nw;
+        if (REALV) {
+          const double v = __shfl_sync(0xffffffffu, myr, q);
+          if (wa < nw) zfma_r(acc0, v, br[wa]);
+          if (wb < nw) zfma_r(acc1, v, br[wb]);
+        } else {
+          z_t v;
+          v.x = __shfl_sync(0xffffffffu, myv.x, q);
+          v.y = __shfl_sync(0xffffffffu, myv.y, q);
+          if (wa < nw) zfma(acc0, v, br[wa]);
+          if (wb < nw) zfma(acc1, v, br[wb]);
+        }
+      }
+    }
+  }
+  tile[wy][lane] = acc0;
+  tile[wy][lane + 32] = acc1;
+  __syncthreads();
+  for (int e = threadIdx.x; e < VHS_ROWS * VHS_WALK; e += VHS_ROWS * 32) {
+    const int wl = e / VHS_ROWS, rr = e % VHS_ROWS;
+    const int w = w0 + wl, rw = r0 + rr;
+    if (w < nw && rw < nrows) out[(long long)w * out_ld + rw] = tile[rr][wl];
+  }
+}
+
+cudaError_t launch_csr_walker(const int* rowIndex, const int* cols, const z_t* zvals,
+                              const double* rvals, const z_t* B, int nrows, int nw, z_t* out,
+                              long long out_ld, cudaStream_t st) {
+  dim3 grid((nrows + VHS_ROWS - 1) / VHS_ROWS, (nw + VHS_WALK - 1) / VHS_WALK);
+  if (rvals)
+    csr_walker_kernel<true><<<grid, VHS_ROWS * 32, 0, st>>>(rowIndex, cols, nullptr, rvals, B,
+                                                            nrows, nw, out, out_ld);
+  else
+    csr_walker_kernel<false><<<grid, VHS_ROWS * 32, 0, st>>>(rowIndex, cols, zvals, nullptr, B,
+                                                             nrows, nw, out, out_ld);
+  return cudaGetLastError();
+}
+
+// ============================================================ CSR x walker-major G
+// out[r][w] = sum_p A[p] G[w][col(p)] (vbias = SpvnT Gc when SpvnT is sparse,
+// vbias.hpp:63; Gcloc = Vakbl Gc, energy.hpp:89).  Warp per row, lanes over walkers.
+__global__ void __launch_bounds__(256)
+csr_gather_kernel(const int* __restrict__ rowIndex, const int* __restrict__ cols,
+                  const z_t* __restrict__ vals, const z_t* __restrict__ G, long long ldg,
+                  int nrows, int nw, z_t* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (r >= nrows) return;
+  const int beg = rowIndex[r], end = rowIndex[r + 1];
+  for (int w0 = 0; w0 < nw; w0 += 32) {
+    const int w = w0 + lane;
+    z_t acc = zmk(0, 0);
+    for (int p0 = beg; p0 < end; p0 += 32) {
+      const int cnt = min(32, end - p0);
+      int myc = 0;
+      z_t myv = zmk(0, 0);
+      if (lane < cnt) { myc = cols[p0 + lane]; myv = vals[p0 + lane]; }
+      for (int q = 0; q < cnt; q++) {
+        const int c = __shfl_sync(0xffffffffu, myc, q);
+        z_t v;
+        v.x = __shfl_sync(0xffffffffu, myv.x, q);
+        v.y = __shfl_sync(0xffffffffu, myv.y, q);
+        if (w < nw) zfma(acc, v, G[(long long)w * ldg + c]);
+      }
+    }
+    if (w < nw) out[(long long)r * nw + w] = acc;
+  }
+}
+
+cudaError_t launch_csr_gather(const int* rowIndex, const int* cols, const z_t* vals, const z_t* G,
+                              long long ldg, int nrows, int nw, z_t* out, cudaStream_t st) {
+  csr_gather_kernel<<<(nrows + 7) / 8, 256, 0, st>>>(rowIndex, cols, vals, G, ldg, nrows, nw, out);
+  return cudaGetLastError();
+}
+
+// ============================================================ weights
+// miniafqmc_base.cpp:316-327; one CTA, fixed-order reduction of sum Re e4.
+__global__ void __launch_bounds__(1024)
+weights_kernel(z_t* __restrict__ Wd, const z_t* __restrict__ hybridW, int nw, double dt,
+               DevScalars* __restrict__ sc, int update_eshift) {
+  __shared__ z_t red[32];
+  const double eshift = sc->eshift;
+  double sum = 0.0;
+  for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+    z_t* d = Wd + (long long)w * 8;
+    z_t ratio = zdiv(zmul(d[2], d[3]), zmul(d[6], d[7]));
+    double ang = atan2(ratio.y, ratio.x);
+    double scale = fmax(0.0, cos(ang));
+    z_t lr = zmk(log(hypot(ratio.x, ratio.y)), ang);
+    z_t hw = hybridW[w];
+    z_t e4 = zmk(-(hw.x + lr.x) / dt, -(hw.y + lr.y) / dt);
+    double f = scale * exp(-dt * (0.5 * (e4.x + d[5].x) - eshift));
+    d[4] = e4;
+    d[1] = zmk(d[1].x * f, d[1].y * f);
+    sum += e4.x;
+  }
+  z_t t = block_zsum(zmk(sum, 0.0), red);
+  if (threadIdx.x == 0) {
+    sc->e4sum = t.x;
+    if (update_eshift) sc->eshift = t.x / nw;
+    sc->step += 1;
+  }
+}
+
+cudaError_t launch_weights(z_t* Wd, const z_t* hybridW, int nw, double dt, DevScalars* sc,
+                           int update_eshift, cudaStream_t st) {
+  weights_kernel<<<1, 1024, 0, st>>>(Wd, hybridW, nw, dt, sc, update_eshift);
+  return cudaGetLastError();
+}
+
+__global__ void set_scalars_kernel(DevScalars* sc, unsigned long long seed,
+                                   unsigned long long step, int set_eshift, double eshift,
+                                   int walker_offset, long long nwalk_global) {
+  sc->seed = seed;
+  sc->step = step;
+  if (set_eshift) sc->eshift = eshift;
+  if (nwalk_global > 0) {
+    sc->walker_offset = walker_offset;
+    sc->nwalk_global = nwalk_global;
+  }
+}
+
+cudaError_t launch_set_scalars(DevScalars* sc, unsigned long long seed, unsigned long long step,
+                               int set_eshift, double eshift, cudaStream_t st,
+                               int walker_offset, long long nwalk_global) {
+  set_scalars_kernel<<<1, 1, 0, st>>>(sc, seed, step, set_eshift, eshift, walker_offset,
+                                      nwalk_global);
+  return cudaGetLastError();
+}
+
+// ============================================================ orthogonalisation
+// LQ of W_s seen column-major (zgelqf + zunglq, afqmc_sys.hpp:200-204) is the QR of
+// B = conj(W_s) (N x n): Householder reflectors with zlarfg's conventions (real beta
+// of sign -sign(Re alpha); tau = (beta - alpha)/beta; v = x/(alpha - beta)), each
+// H^H = I - conj(tau) v v^H applied from the left (zgeqr2), then Q = H(1)..H(n) formed
+// by backward accumulation (zung2r) and W_s = conj(Q).  One CTA per (walker, spin)
+// works in place on the walker buffer (L2 resident); threads are laid out as
+// (column, row-group) so row segments are read contiguously.
+constexpr int QR_THREADS = 256;
+
+__global__ void __launch_bounds__(QR_THREADS)
+ortho_kernel(z_t* __restrict__ W, int N, int n) {
+  __shared__ z_t tau_s[64];
+  __shared__ z_t sdot[4][65];
+  __shared__ z_t red[QR_THREADS / 32];
+  __shared__ z_t s_ctau, s_scal;
+  __shared__ double s_beta;
+  __shared__ int s_skip;
+  const int w = blockIdx.x >> 1, s = blockIdx.x & 1;
+  const long long ld = 2 * n;
+  z_t* B = W + (long long)w * N * ld + s * n;
+  const int tid = threadIdx.x;
+  const int lc = tid % 64, rg = tid / 64;   // column lane, row group (4 groups)
+
+  for (long long e = tid; e < (long long)N * n; e += QR_THREADS) {
+    long long i = e / n, c = e % n;
+    z_t v = B[i * ld + c];
+    B[i * ld + c] = zconj(v);
+  }
+  __syncthreads();
+
+  for (int j = 0; j < n; j++) {
+    // xnorm^2 over rows j+1..N-1 of column j
+    double part = 0.0;
+    for (int i = j + 1 + tid; i < N; i += QR_THREADS) {
+      z_t v = B[(long long)i * ld + j];
+      part += v.x * v.x + v.y * v.y;
+    }
+    z_t tot = block_zsum(zmk(part, 0.0), red);
+    if (tid == 0) {
+      z_t alpha = B[(long long)j * ld + j];
+      double xn2 = tot.x;
+      if (xn2 == 0.0 && alpha.y == 0.0) {
+        s_skip = 1;
+        tau_s[j] = zmk(0, 0);
+      } else {
+        double nrm = sqrt(alpha.x * alpha.x + alpha.y * alpha.y + xn2);
+        double beta = -copysign(nrm, alpha.x);
+        z_t tau = zmk((beta - alpha.x) / beta, -alpha.y / beta);
+        tau_s[j] = tau;
+        s_ctau = zconj(tau);
+        s_scal = zrecip(zmk(alpha.x - beta, alpha.y));
+        s_beta = beta;
+        s_skip = 0;
+      }
+    }
+    __syncthreads();
+    if (s_skip) continue;
+    const z_t scal = s_scal;
+    for (int i = j + 1 + tid; i < N; i += QR_THREADS) {
+      long long o = (long long)i * ld + j;
+      B[o] = zmul(B[o], scal);
+    }
+    __syncthreads();
+    if (tid == 0) B[(long long)j * ld + j] = zmk(s_beta, 0.0);
+    // s_l = v^H B[j:, l] for l > j (v_j = 1)
+    const int l = j + 1 + lc;
+    z_t acc = zmk(0, 0);
+    if (l < n) {
+      if (rg == 0) acc = B[(long long)j * ld + l];
+      for (int i = j + 1 + rg; i < N; i += 4)
+        zfma_conj(acc, B[(long long)i * ld + j], B[(long long)i * ld + l]);
+    }
+    sdot[rg][lc] = acc;
+    __syncthreads();
+    if (rg == 0 && l < n)
+      sdot[0][lc] = zadd(zadd(sdot[0][lc], sdot[1][lc]), zadd(sdot[2][lc], sdot[3][lc]));
+    __syncthreads();
+    if (l < n) {
+      const z_t f = zmul(s_ctau, sdot[0][lc]);
+      if (rg == 0) {
+        long long o = (long long)j * ld + l;
+        B[o] = zsub(B[o], f);
+      }
+      for (int i = j + 1 + rg; i < N; i += 4) {
+        long long o = (long long)i * ld + l;
+        B[o] = zsub(B[o], zmul(B[(long long)i * ld + j], f));
+      }
+    }
+    __syncthreads();
+  }
+
+  // Q = H(1) ... H(n) applied to the first n columns of the identity (zung2r)
+  for (int i = n - 1; i >= 0; i--) {
+    const z_t tau = tau_s[i];
+    if (i < n - 1) {
+      const int l = i + 1 + lc;
+      z_t acc = zmk(0, 0);
+      if (l < n) {
+        if (rg == 0) acc = B[(long long)i * ld + l];   // v_i = 1
+        for (int r = i + 1 + rg; r < N; r += 4)
+          zfma_conj(acc, B[(long long)r * ld + i], B[(long long)r * ld + l]);
+      }
+      sdot[rg][lc] = acc;
+      __syncthreads();
+      if (rg == 0 && l < n)
+        sdot[0][lc] = zadd(zadd(sdot[0][lc], sdot[1][lc]), zadd(sdot[2][lc], sdot[3][lc]));
+      __syncthreads();
+      if (l < n) {
+        const z_t f = zmul(tau, sdot[0][lc]);
+        if (rg == 0) {
+          long long o = (long long)i * ld + l;
+          B[o] = zsub(B[o], f);
+        }
+        for (int r = i + 1 + rg; r < N; r += 4) {
+          long long o = (long long)r * ld + l;
+          B[o] = zsub(B[o], zmul(B[(long long)r * ld + i], f));
+        }
+      }
+      __syncthreads();
+    }
+    const z_t mt = zmk(-tau.x, -tau.y);
+    for (int r = i + 1 + tid; r < N; r += QR_THREADS) {
+      long long o = (long long)r * ld + i;
+      B[o] = zmul(B[o], mt);
+    }
+    if (tid == 0) B[(long long)i * ld + i] = zmk(1.0 - tau.x, -tau.y);
+    for (int r = tid; r < i; r += QR_THREADS) B[(long long)r * ld + i] = zmk(0, 0);
+    __syncthreads();
+  }
+
+  for (long long e = tid; e < (long long)N * n; e += QR_THREADS) {
+    long long i = e / n, c = e % n;
+    z_t v = B[i * ld + c];
+    B[i * ld + c] = zconj(v);
+  }
+}
+
+cudaError_t launch_ortho(z_t* W, int N, int n, int nw, cudaStream_t st) {
+  ortho_kernel<<<2 * nw, QR_THREADS, 0, st>>>(W, N, n);
+  return cudaGetLastError();
+}
+
+// ============================================================ exchange energy
+// K_w = 1/2 sum_{s,c} tr(T T), T = Lh_s[c] Gc_s^T (n x n), for Gn Cholesky vectors x Gw
+// walkers per CTA: a (Gn*n) x (Gw*n) complex tile over K = N, then the trace of each
+// n x n block squared from shared memory.  Partial sums per (walker, spin, c-block).
+constexpr int EX_T = 96, EX_BK = 16, EX_TM = 6, EX_TN = 6, EX_THREADS = 256;
+
+size_t exch_smem_bytes() {
+  size_t main = sizeof(z_t) * 2 * EX_BK * 2 * (EX_T + 1);
+  size_t epi = sizeof(z_t) * EX_T * (EX_T + 1);
+  return std::max(main, epi);
+}
+
+__global__ void __launch_bounds__(EX_THREADS)
+exchange_kernel(const z_t* __restrict__ Lh, const z_t* __restrict__ Gc, int N, int n, int nchol,
+                int nw, int Gn, int Gw, z_t* __restrict__ Kpart, int nblk) {
+  extern __shared__ __align__(16) unsigned char ex_smem[];
+  z_t* As = reinterpret_cast<z_t*>(ex_smem);          // [2][BK][T+1]
+  z_t* Bs = As + 2 * EX_BK * (EX_T + 1);
+  const int s = blockIdx.z;
+  const int c0 = blockIdx.x * Gn, w0 = blockIdx.y * Gw;
+  const long long NAK = 2LL * n * N;
+  const int Mr = Gn * n, Nc = Gw * n;
+  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
+
+  auto load = [&](int stage, int k0) {
+    z_t* as = As + stage * EX_BK * (EX_T + 1);
+    z_t* bs = Bs + stage * EX_BK * (EX_T + 1);
+    for (int e = tid; e < EX_T * EX_BK; e += EX_THREADS) {
+      int m = e / EX_BK, k = e % EX_BK, gk = k0 + k;
+      int cv = m / n, a = m % n;
+      const z_t* src = Lh;
+      int bytes = 0;
+      if (m < Mr && c0 + cv < nchol && gk < N) {
+        src = Lh + (long long)(c0 + cv) * NAK + (long long)s * n * N + (long long)a * N + gk;
+        bytes = 16;
+      }
+      cp_async16(as + k * (EX_T + 1) + m, src, bytes);
+      const z_t* srcb = Gc;
+      int bb = 0;
+      if (m < Nc && w0 + m / n < nw && gk < N) {
+        int wl = m / n, b = m % n;
+        srcb = Gc + (long long)(w0 + wl) * NAK + (long long)s * n * N + (long long)b * N + gk;
+        bb = 16;
+      }
+      cp_async16(bs + k * (EX_T + 1) + m, srcb, bb);
+    }
+    cp_async_commit();
+  };
+
+  z_t acc[EX_TM][EX_TN];
+#pragma unroll
+  for (int i = 0; i < EX_TM; i++)
+#pragma unroll
+    for (int j = 0; j < EX_TN; j++) acc[i][j] = zmk(0, 0);
+  const int nk = (N + EX_BK - 1) / EX_BK;
+  load(0, 0);
+  for (int kt = 0; kt < nk; kt++) {
+    if (kt + 1 < nk) {
+      load((kt + 1) & 1, (kt + 1) * EX_BK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const z_t* as = As + (kt & 1) * EX_BK * (EX_T + 1);
+    const z_t* bs = Bs + (kt & 1) * EX_BK * (EX_T + 1);
+#pragma unroll 4
+    for (int kk = 0; kk < EX_BK; kk++) {
+      z_t a[EX_TM], b[EX_TN];
+#pragma unroll
+      for (int i = 0; i < EX_TM; i++) a[i] = as[kk * (EX_T + 1) + ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < EX_TN; j++) b[j] = bs[kk * (EX_T + 1) + tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < EX_TM; i++)
+#pragma unroll
+        for (int j = 0; j < EX_TN; j++) zfma(acc[i][j], a[i], b[j]);
+    }
+    __syncthreads();
+  }
+  z_t* Ts = reinterpret_cast<z_t*>(ex_smem);             // [T][T+1], reuses the slabs
+#pragma unroll
+  for (int i = 0; i < EX_TM; i++)
+#pragma unroll
+    for (int j = 0; j < EX_TN; j++) Ts[(ty + 16 * i) * (EX_T + 1) + tx + 16 * j] = acc[i][j];
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int wl = warp; wl < Gw; wl += EX_THREADS / 32) {
+    z_t sum = zmk(0, 0);
+    for (int cv = 0; cv < Gn; cv++)
+      for (int t = lane; t < n * n; t += 32) {
+        int a = t / n, b = t % n;
+        zfma(sum, Ts[(cv * n + a) * (EX_T + 1) + wl * n + b], Ts[(cv * n + b) * (EX_T + 1) + wl * n + a]);
+      }
+    sum = warp_zsum(sum);
+    if (lane == 0 && w0 + wl < nw) Kpart[((long long)(w0 + wl) * 2 + s) * nblk + blockIdx.x] = sum;
+  }
+}
+
+cudaError_t launch_exchange(const z_t* Lh, const z_t* Gc, int N, int n, int nchol, int nw,
+                            z_t* Kpart, int* nblk_out, cudaStream_t st) {
+  if (n > EX_T) return cudaErrorInvalidValue;
+  const int Gn = EX_T / n, Gw = EX_T / n;
+  const int nblk = (nchol + Gn - 1) / Gn;
+  *nblk_out = nblk;
+  if (!Kpart) return cudaSuccess;
+  size_t smem = exch_smem_bytes();
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(exchange_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  dim3 grid(nblk, (nw + Gw - 1) / Gw, 2);
+  exchange_kernel<<<grid, EX_THREADS, smem, st>>>(Lh, Gc, N, n, nchol, nw, Gn, Gw, Kpart, nblk);
+  return cudaGetLastError();
+}
+
+// ============================================================ energy reductions
+// Per walker: E1 = sum Gc.haj (energy.hpp:100); mode 0 (Vakbl): E2 = 1/2 sum Gc.Gcloc
+// (energy.hpp:93-97); mode 1 (Cholesky): EJ = 1/2 sum_c cv^2, EK = 1/2 sum Kpart.
+__global__ void __launch_bounds__(256)
+energy_reduce_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, int nak,
+                     const z_t* __restrict__ Gcloc, const z_t* __restrict__ cv, int nchol,
+                     const z_t* __restrict__ Kpart, int nblk, int nw, int mode,
+                     z_t* __restrict__ Wd, double* __restrict__ parts) {
+  __shared__ z_t red[8];
+  const int w = blockIdx.x;
+  const z_t* g = Gc + (long long)w * nak;
+  z_t e1 = zmk(0, 0), e2 = zmk(0, 0);
+  for (int i = threadIdx.x; i < nak; i += blockDim.x) {
+    z_t gi = g[i];
+    zfma(e1, gi, haj[i]);
+    if (mode == 0) zfma(e2, gi, Gcloc[(long long)i * nw + w]);
+  }
+  e1 = block_zsum(e1, red);
+  z_t ej = zmk(0, 0), ek = zmk(0, 0);
+  if (mode == 0) {
+    e2 = block_zsum(e2, red);
+  } else {
+    for (int c = threadIdx.x; c < nchol; c += blockDim.x) {
+      z_t v = cv[(long long)c * nw + w];
+      zfma(ej, v, v);
+    }
+    for (int q = threadIdx.x; q < 2 * nblk; q += blockDim.x)
+      ek = zadd(ek, Kpart[(long long)w * 2 * nblk + q]);
+    ej = block_zsum(ej, red);
+    ek = block_zsum(ek, red);
+  }
+  if (threadIdx.x == 0) {
+    z_t e;
+    if (mode == 0) {
+      e = zadd(zscale(e2, 0.5), e1);
+    } else {
+      ej = zscale(ej, 0.5);
+      ek = zscale(ek, 0.5);
+      e = zsub(zadd(e1, ej), ek);
+      if (parts) {
+        parts[3 * w] = e1.x; parts[3 * w + 1] = ej.x; parts[3 * w + 2] = ek.x;
+      }
+    }
+    Wd[(long long)w * 8] = e;
+  }
+}
+
+cudaError_t launch_energy_reduce(const z_t* Gc, const z_t* haj, int nak, const z_t* Gcloc,
+                                 const z_t* cv, int nchol, const z_t* Kpart, int nblk, int nw,
+                                 int mode, z_t* Wd, double* parts, cudaStream_t st) {
+  energy_reduce_kernel<<<nw, 256, 0, st>>>(Gc, haj, nak, Gcloc, cv, nchol, Kpart, nblk, nw, mode,
+                                           Wd, parts);
+  return cudaGetLastError();
+}
+
+// sum Re(eloc) Re(w) and sum Re(w) (afqmc_sys.hpp:127-132), fixed-order reduction.
+__global__ void __launch_bounds__(1024)
+eav_kernel(const z_t* __restrict__ Wd, int nw, DevScalars* __restrict__ sc) {
+  __shared__ z_t red[32];
+  double a = 0.0, b = 0.0;
+  for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+    const z_t* d = Wd + (long long)w * 8;
+    a += d[0].x * d[1].x;
+    b += d[1].x;
+  }
+  z_t t = block_zsum(zmk(a, b), red);
+  if (threadIdx.x == 0) {
+    sc->esum[0] = t.x;
+    sc->esum[1] = t.y;
+  }
+}
+
+cudaError_t launch_eav(const z_t* Wd, int nw, DevScalars* sc, cudaStream_t st) {
+  eav_kernel<<<1, 1024, 0, st>>>(Wd, nw, sc);
+  return cudaGetLastError();
+}
+
+}  // namespace afq

@@ -164,6 +164,8 @@ struct orc_handle {
   std::vector<int> info;
   double Eshift = 0.0;
   int nthreads = 1;
+  int walker_offset = 0;     // global index of walker 0 (sharded ensembles)
+  long long nwalk_global = 0;
 };
 
 extern "C" {
@@ -358,14 +360,28 @@ static void sigma_core(orc_handle* h) {
     }
 }
 
+// x[c][w] is element c*nwg + woff + w of one stream over the global ensemble, so a
+// sharded ensemble draws the same fields as the unsharded one.
 void orc_generate_x(orc_handle* h, uint64_t seed, uint64_t step) {
-  size_t tot = (size_t)h->nchol * h->nw;
-  for (size_t j = 0; 2 * j < tot; j++) {
-    double a, b;
-    normal_pair(seed, step, j, &a, &b);
-    h->xraw[2 * j] = a;
-    if (2 * j + 1 < tot) h->xraw[2 * j + 1] = b;
-  }
+  const long long nwg = h->nwalk_global > 0 ? h->nwalk_global : h->nw;
+  for (int c = 0; c < h->nchol; c++)
+    for (int w = 0; w < h->nw; w++) {
+      long long eg = (long long)c * nwg + h->walker_offset + w;
+      double a, b;
+      normal_pair(seed, step, (uint64_t)eg >> 1, &a, &b);
+      h->xraw[(size_t)c * h->nw + w] = (eg & 1) ? b : a;
+    }
+}
+
+void orc_set_walker_offset(orc_handle* h, int offset, long long nwalk_global) {
+  h->walker_offset = offset;
+  h->nwalk_global = nwalk_global;
+}
+
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+  uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+  philox4x32_10(c, key[0], key[1]);
+  for (int i = 0; i < 4; i++) out[i] = c[i];
 }
 
 void orc_sigma(orc_handle* h, uint64_t seed, uint64_t step) {

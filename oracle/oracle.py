@@ -91,6 +91,8 @@ def load(fast: bool = False) -> ctypes.CDLL:
         "orc_rm_gemm": ([ctypes.c_char, ctypes.c_char, I, I, I, P, I, P, I, P, I], None),
         "orc_invert": ([I, P, P], I),
         "orc_normals": ([U64, U64, ctypes.c_longlong, P], None),
+        "orc_set_walker_offset": ([P, I, ctypes.c_longlong], None),
+        "orc_philox": ([P, P, P], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -164,6 +166,9 @@ class Oracle:
         self.lib.orc_copy_out(self.h, code, _p(out))
         return out
 
+    def set_walker_offset(self, offset: int, nwalk_global: int):
+        self.lib.orc_set_walker_offset(self.h, offset, nwalk_global)
+
     @property
     def eshift(self) -> float:
         return self.lib.orc_get_eshift(self.h)
@@ -201,6 +206,19 @@ class Oracle:
     def sum_e4(self) -> float:
         return self.lib.orc_sum_e4(self.h)
 
+    def update_weights_partial(self) -> float:
+        """Weights with the current Eshift; returns the local sum of Re W_data[:,4]
+        and leaves Eshift for the caller to set from the global sum."""
+        e = self.eshift
+        self.update_weights()
+        self.eshift = e
+        return self.sum_e4()
+
+    def energy_sums(self, mode: str = "auto"):
+        self.calculate_energy(mode)
+        _, Wd = self.get_walkers()
+        return np.array([np.sum(Wd[:, 0].real * Wd[:, 1].real), np.sum(Wd[:, 1].real)])
+
     def orthogonalize(self):
         self.lib.orc_orthogonalize(self.h)
 
@@ -214,7 +232,8 @@ class Oracle:
         return (e, buf) if parts else e
 
     # the driver's substep (miniafqmc_base.cpp:251-337) ------------------------------
-    def substep(self, seed: int, step_tot: int, northo: int, x: np.ndarray | None = None):
+    def substep(self, seed: int, step_tot: int, northo: int, x: np.ndarray | None = None,
+                graph: bool = False):
         self.calculate_mixed_density_matrix()
         self.get_vbias()
         if x is None:
@@ -233,6 +252,14 @@ class Oracle:
 def normals(seed: int, step: int, count: int) -> np.ndarray:
     out = np.empty(count, np.float64)
     load().orc_normals(seed, step, count, _p(out))
+    return out
+
+
+def philox(ctr, key) -> np.ndarray:
+    c = np.asarray(ctr, np.uint32)
+    k = np.asarray(key, np.uint32)
+    out = np.empty(4, np.uint32)
+    load().orc_philox(_p(c), _p(k), _p(out))
     return out
 
 

@@ -1,0 +1,43 @@
+"""The C-ABI library loads without a GPU and exports every entry point the header
+declares (no compute calls here)."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "afqmc_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:afq_status|void|const char\*)\s+(afq_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_the_operation_set():
+    names = declared_functions()
+    for op in ("afq_mixed_density_matrix", "afq_overlaps", "afq_vbias", "afq_sigma", "afq_vhs",
+               "afq_propagate", "afq_update_weights", "afq_orthogonalize", "afq_energy",
+               "afq_substep", "afq_create", "afq_set_hamiltonian"):
+        assert op in names
+
+
+def test_library_exports_every_declared_symbol():
+    from miniafqmc_b200 import build
+    build.build()
+    lib = ctypes.CDLL(build.LIB)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    from miniafqmc_b200.afqmc import EXPORTS
+    assert set(declared_functions()) <= set(EXPORTS)
+
+
+def test_status_strings_without_gpu():
+    from miniafqmc_b200.afqmc import load_library
+    lib = load_library()
+    assert lib.afq_status_string(0) == b"ok"
+    assert lib.afq_status_string(6) == b"singular overlap matrix"
