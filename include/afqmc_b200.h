@@ -165,6 +165,14 @@ afq_status afq_get_stream(afq_handle* h, void** stream);
 /* Copies a device buffer to host memory in the reference layout (see afq_buffer). */
 afq_status afq_copy_out(afq_handle* h, int which, void* host);
 
+/* Self-test of the tensor-core GEMM used by the mixed form (no reference counterpart):
+ * C[b][m][n] = sum_k A[b][m][k] B[b][n][k] for host fp32 arrays, computed on the current
+ * device with bf16 operands (tf32 == 0, inputs rounded to nearest bf16) or tf32 operands,
+ * fp32 accumulation, tile width bn in {64, 128, 192}; K must be a multiple of 8.
+ * *kernel_err receives the kernel's timeout flags (0 when clean). */
+afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn, const float* A,
+                                const float* B, float* C, int* kernel_err);
+
 #ifdef __cplusplus
 }
 #endif

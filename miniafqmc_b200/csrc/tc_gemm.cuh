@@ -1,0 +1,343 @@
+// tcgen05 (5th-generation tensor core) GEMM for sm_100a with TMA staging.
+//
+// D[b][m][n] = sum_k A[b][m][k] * B[b][n][k]      (both operands K-major, fp32 accumulate)
+//
+// One CTA computes a 128 x BN tile: warp 4 issues TMA loads of 128-byte-wide K slabs
+// (SWIZZLE_128B) into a STAGES-deep shared-memory ring guarded by mbarriers; one thread
+// of warp 5 issues tcgen05.mma (kind::f16 for bf16 operands, kind::tf32 for fp32 operands)
+// into a TMEM accumulator and frees each stage with tcgen05.commit; warps 0-3 then read
+// the accumulator with tcgen05.ld (one TMEM lane per output row) and hand 32-column
+// chunks (or the whole tile, staged in shared memory) to the epilogue functor.
+// The split form loads hi and lo parts of both operands per stage and accumulates
+// hi*hi + hi*lo + lo*hi: with bf16 parts that carries ~16 significant bits per operand
+// (bf16x3), with tf32 parts ~21 bits (3xTF32).
+//
+// Every mbarrier wait is bounded (about one second of SM clocks); on timeout the CTA
+// records an error code in *err, skips its remaining work and still frees its TMEM.
+#pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+#include "afq_common.cuh"
+
+namespace tc {
+
+enum : int { ERR_TIMEOUT_PRODUCER = 1, ERR_TIMEOUT_MMA = 2, ERR_TIMEOUT_EPILOGUE = 4 };
+
+AFQ_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+AFQ_D void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+AFQ_D void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Waits for the phase with the given parity to complete; false after ~1 s of clocks.
+AFQ_D bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > 2000000000LL) return false;
+  }
+}
+AFQ_D void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+AFQ_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+AFQ_D void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+AFQ_D void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(slot)),
+               "r"(ncols));
+}
+AFQ_D void tmem_relinquish() {
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+AFQ_D void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+AFQ_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+AFQ_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+template <bool TF32>
+AFQ_D void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  if (TF32)
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+  else
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+AFQ_D void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// 32 consecutive fp32 columns of this thread's TMEM lane.
+AFQ_D void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Shared-memory matrix descriptor: K-major operand tile written by TMA with
+// SWIZZLE_128B (rows of 128 bytes, 8-row groups 1024 bytes apart).
+AFQ_D uint64_t sdesc_k128(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);   // start address
+  d |= (uint64_t)1 << 16;                     // leading byte offset (unused when swizzled)
+  d |= (uint64_t)(1024 >> 4) << 32;           // stride byte offset: one 8-row group
+  d |= (uint64_t)1 << 46;                     // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;                     // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor: fp32 accumulator, bf16 or tf32 operands, both K-major.
+constexpr uint32_t idesc(int M, int N, bool tf32) {
+  return (1u << 4) | ((tf32 ? 2u : 1u) << 7) | ((tf32 ? 2u : 1u) << 10) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+template <int BN, int STAGES, bool TF32, bool SPLIT>
+struct Cfg {
+  static constexpr int BM = 128;
+  static constexpr int ELEM = TF32 ? 4 : 2;
+  static constexpr int BK = 128 / ELEM;          // elements per 128-byte K slab
+  static constexpr int UK = 32 / ELEM;           // K of one tcgen05.mma
+  static constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128;
+  static constexpr int PARTS = SPLIT ? 2 : 1;    // hi (and lo) parts of each operand
+  static constexpr uint32_t STAGE_BYTES = PARTS * (A_BYTES + B_BYTES);
+  static constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  static constexpr size_t SMEM = 1024 + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 1) + 16;
+  static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "UMMA N for M=128");
+  static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+// Operand tensor maps; the lo parts are used only by the split form.
+struct Maps {
+  CUtensorMap a, b, a_lo, b_lo;
+};
+
+// Named barrier among the 128 epilogue threads (warps 0-3).
+AFQ_D void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Epilogue interface.  Row-wise functors (Epi::kTile == false) get
+//   epi(batch, tile_row, m, n_first, v[32])
+// for each 32-column chunk of each of the 128 rows.  Tile functors (kTile == true) get
+// the whole fp32 tile in shared memory (row stride BN + 1) after the epilogue barrier:
+//   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi>
+__global__ void __launch_bounds__(192, 1)
+tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched, int b_batched,
+               int k_split, Epi epi, int* err) {
+  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  // stage s: [A_hi | B_hi | A_lo | B_lo]
+  auto stA = [&](int s, int part) { return smem + s * C::STAGE_BYTES + part * (C::A_BYTES + C::B_BYTES); };
+  auto stB = [&](int s, int part) { return stA(s, part) + C::A_BYTES; };
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * m_step, n0 = blockIdx.x * BN;
+  const int batch = blockIdx.z;
+  // split-K: z selects the K range [z*k_split, (z+1)*k_split) of an unbatched product
+  const int kbase = k_split ? batch * k_split : 0;
+  const int klen = k_split ? min(k_split, K - kbase) : K;
+  const int nk = (klen + C::BK - 1) / C::BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, C::TMEM_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 4 && lane == 0) {
+    // ---- TMA producer
+    const int za = (a_batched && !k_split) ? batch : 0, zb = (b_batched && !k_split) ? batch : 0;
+    for (int kb = 0; kb < nk; kb++) {
+      const int kx = kbase + kb * C::BK;
+      const int s = kb % STAGES;
+      const uint32_t ph = (kb / STAGES) & 1;
+      if (!mbar_wait(&empty[s], ph ^ 1)) {
+        atomicOr(err, ERR_TIMEOUT_PRODUCER);
+        break;
+      }
+      mbar_expect_tx(&full[s], C::STAGE_BYTES);
+      tma_load_3d(stA(s, 0), &maps.a, &full[s], kx, m0, za);
+      tma_load_3d(stB(s, 0), &maps.b, &full[s], kx, n0, zb);
+      if (SPLIT) {
+        tma_load_3d(stA(s, 1), &maps.a_lo, &full[s], kx, m0, za);
+        tma_load_3d(stB(s, 1), &maps.b_lo, &full[s], kx, n0, zb);
+      }
+    }
+  } else if (warp == 5 && lane == 0) {
+    // ---- MMA issuer
+    constexpr uint32_t ID = idesc(128, BN, TF32);
+    bool ok = true;
+    for (int kb = 0; kb < nk; kb++) {
+      const int s = kb % STAGES;
+      const uint32_t ph = (kb / STAGES) & 1;
+      if (!mbar_wait(&full[s], ph)) {
+        atomicOr(err, ERR_TIMEOUT_MMA);
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint64_t ad = sdesc_k128(smem_u32(stA(s, 0)));
+      const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
+#pragma unroll
+      for (int k = 0; k < C::BK / C::UK; k++)   // advance 32 bytes along K per MMA
+        umma<TF32>(tmem, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
+      if (SPLIT) {
+        const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
+        const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
+#pragma unroll
+        for (int k = 0; k < C::BK / C::UK; k++) {
+          umma<TF32>(tmem, ad + 2 * k, bl + 2 * k, ID, 1u);   // hi * lo
+          umma<TF32>(tmem, al + 2 * k, bd + 2 * k, ID, 1u);   // lo * hi
+        }
+      }
+      umma_commit(&empty[s]);
+    }
+    if (ok) umma_commit(done);
+  }
+
+  if (warp < 4) {
+    // ---- epilogue: TMEM lane = tile row
+    const bool ok = mbar_wait(done, 0);
+    if (!ok) {
+      if (lane == 0) atomicOr(err, ERR_TIMEOUT_EPILOGUE);
+    } else {
+      tc_fence_after();
+      const int row = warp * 32 + lane;
+      const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+      float v[32];
+      if constexpr (Epi::kTile) {
+        // the operand ring is idle once `done` has fired: reuse it for the fp32 tile
+        float* tile = reinterpret_cast<float*>(smem);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          tmem_ld32(trow + c0, v);
+#pragma unroll
+          for (int i = 0; i < 32; i++) tile[row * (BN + 1) + c0 + i] = v[i];
+        }
+        epi_bar();
+        epi.tile(batch, blockIdx.y, blockIdx.x, tile, BN + 1, threadIdx.x);
+      } else {
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          tmem_ld32(trow + c0, v);
+          epi(batch, row, m0 + row, n0 + c0, v);
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, C::TMEM_COLS);
+}
+
+// ------------------------------------------------------------------ host side
+// Tensor map of a [batch][rows][K] K-major operand (rows strided by ld elements, batches
+// by sbatch elements), tiles of box_rows x 128 bytes, SWIZZLE_128B, zero fill outside.
+inline CUresult make_kmajor_map(CUtensorMap* map, const void* base, bool fp32, uint64_t K,
+                                uint64_t rows, uint64_t batch, uint64_t ld, uint64_t sbatch,
+                                uint32_t box_rows) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&encode, cudaEnableDefault,
+                                &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !encode)
+      return CUDA_ERROR_NOT_FOUND;
+  }
+  const uint32_t esz = fp32 ? 4 : 2;
+  cuuint64_t dims[3] = {K, rows, batch};
+  cuuint64_t strides[2] = {ld * esz, (batch > 1 ? sbatch : rows * ld) * esz};
+  cuuint32_t box[3] = {128 / esz, box_rows, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return encode(map, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
+                const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+
+struct GemmShape {
+  int M, N, K, batch;  // batch = number of z slices (batches, or K splits when k_split > 0)
+  int m_step;          // rows between consecutive M tiles (128 unless aligned to row groups)
+  int m_tiles;         // number of M tiles
+  bool a_batched, b_batched;
+  int k_split;         // 0, or the K extent of each z slice (a multiple of the K slab)
+};
+
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi>
+cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
+                   cudaStream_t st) {
+  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
+                "tile epilogue needs the operand ring to hold the fp32 tile");
+  auto kern = tc_gemm_kernel<BN, STAGES, TF32, SPLIT, Epi>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  dim3 grid((g.N + BN - 1) / BN, g.m_tiles, g.batch);
+  kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, g.a_batched, g.b_batched, g.k_split, epi,
+                                    err);
+  return cudaGetLastError();
+}
+
+}  // namespace tc

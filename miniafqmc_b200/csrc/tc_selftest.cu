@@ -1,0 +1,91 @@
+// Self-test entry of the tcgen05 GEMM: host fp32 operands in, fp32 product out.
+// Used by the numerics tests to compare the tensor-core kernel with a plain fp32
+// reference of the same operation on bf16- or tf32-representable inputs.
+#include <cuda_bf16.h>
+#include <vector>
+
+#include "../../include/afqmc_b200.h"
+#include "tc_gemm.cuh"
+
+namespace {
+
+struct EpiStoreF32 {
+  static constexpr bool kTile = false;
+  float* C;
+  int M, N;
+  long long sC;
+  AFQ_D void operator()(int b, int, int m, int n0, const float* v) const {
+    if (m >= M) return;
+    float* row = C + (long long)b * sC + (long long)m * N;
+#pragma unroll
+    for (int i = 0; i < 32; i++)
+      if (n0 + i < N) row[n0 + i] = v[i];
+  }
+};
+
+template <int BN, bool TF32>
+cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, int batch,
+                int* derr, cudaStream_t st) {
+  tc::Maps maps;
+  if (tc::make_kmajor_map(&maps.a, dA, TF32, K, M, batch, K, (uint64_t)M * K, 128) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  if (tc::make_kmajor_map(&maps.b, dB, TF32, K, N, batch, K, (uint64_t)N * K, BN) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  maps.a_lo = maps.a;
+  maps.b_lo = maps.b;
+  tc::GemmShape g{M, N, K, batch, 128, (M + 127) / 128, true, true, 0};
+  EpiStoreF32 epi{dC, M, N, (long long)M * N};
+  return tc::launch<BN, 4, TF32, false>(maps, g, epi, derr, st);
+}
+
+}  // namespace
+
+extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn,
+                                          const float* A, const float* B, float* C,
+                                          int* kernel_err) {
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C) return AFQ_ERR_ARG;
+  if (K % 8 != 0) return AFQ_ERR_UNSUPPORTED;   // 16-byte row strides for TMA
+  const size_t na = (size_t)batch * M * K, nb = (size_t)batch * N * K, nc = (size_t)batch * M * N;
+  void *dA = nullptr, *dB = nullptr;
+  float* dC = nullptr;
+  int* derr = nullptr;
+  cudaStream_t st = nullptr;
+  afq_status s = AFQ_OK;
+  const size_t esz = tf32 ? 4 : 2;
+  if (cudaMalloc(&dA, na * esz) != cudaSuccess || cudaMalloc(&dB, nb * esz) != cudaSuccess ||
+      cudaMalloc(&dC, nc * 4) != cudaSuccess || cudaMalloc(&derr, sizeof(int)) != cudaSuccess ||
+      cudaStreamCreate(&st) != cudaSuccess) {
+    s = AFQ_ERR_OOM;
+  }
+  if (s == AFQ_OK) {
+    if (tf32) {
+      cudaMemcpy(dA, A, na * 4, cudaMemcpyHostToDevice);
+      cudaMemcpy(dB, B, nb * 4, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<__nv_bfloat16> ha(na), hb(nb);
+      for (size_t i = 0; i < na; i++) ha[i] = __float2bfloat16_rn(A[i]);
+      for (size_t i = 0; i < nb; i++) hb[i] = __float2bfloat16_rn(B[i]);
+      cudaMemcpy(dA, ha.data(), na * 2, cudaMemcpyHostToDevice);
+      cudaMemcpy(dB, hb.data(), nb * 2, cudaMemcpyHostToDevice);
+    }
+    cudaMemset(dC, 0, nc * 4);
+    cudaMemset(derr, 0, sizeof(int));
+    cudaError_t e;
+    if (bn == 64) e = tf32 ? run<64, true>(dA, dB, dC, M, N, K, batch, derr, st)
+                           : run<64, false>(dA, dB, dC, M, N, K, batch, derr, st);
+    else if (bn == 192) e = tf32 ? run<192, true>(dA, dB, dC, M, N, K, batch, derr, st)
+                                 : run<192, false>(dA, dB, dC, M, N, K, batch, derr, st);
+    else e = tf32 ? run<128, true>(dA, dB, dC, M, N, K, batch, derr, st)
+                  : run<128, false>(dA, dB, dC, M, N, K, batch, derr, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) s = AFQ_ERR_CUDA;
+    cudaMemcpy(C, dC, nc * 4, cudaMemcpyDeviceToHost);
+    if (kernel_err) cudaMemcpy(kernel_err, derr, sizeof(int), cudaMemcpyDeviceToHost);
+  }
+  if (st) cudaStreamDestroy(st);
+  cudaFree(dA);
+  cudaFree(dB);
+  cudaFree(dC);
+  cudaFree(derr);
+  return s;
+}
