@@ -518,7 +518,13 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
     std::string msg;
     cudaError_t e = afq::mixed_create(&mi, &h->mixed, &msg, h->st);
     if (e != cudaSuccess || !h->mixed)
-      return fail(h, e == cudaSuccess ? AFQ_ERR_UNSUPPORTED : AFQ_ERR_CUDA, "mixed: " + msg);
+      return fail(h, e == cudaErrorInvalidValue ? AFQ_ERR_UNSUPPORTED : AFQ_ERR_CUDA,
+                  "mixed: " + msg);
+    if (h->Lh) {   // the tensor-core exchange uses its own Cholesky blocking
+      int nb = afq::mixed_nblk(h->mixed);
+      if (nb > h->nblk) AFQ_CUDA(h, dalloc(h, &h->Kpart, (size_t)h->nw * 2 * nb));
+      h->nblk = nb;
+    }
   }
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
   h->have_ham = true;
@@ -760,6 +766,12 @@ afq_status afq_get_stream(afq_handle* h, void** stream) {
 afq_status afq_synchronize(afq_handle* h) {
   if (!h) return AFQ_ERR_ARG;
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->mixed) {
+    int flags = 0;
+    AFQ_CUDA(h, afq::mixed_error(h->mixed, &flags));
+    if (flags) return fail(h, AFQ_ERR_CUDA, "tensor-core pipeline wait timed out (flags " +
+                                                std::to_string(flags) + ")");
+  }
   return AFQ_OK;
 }
 
@@ -782,6 +794,7 @@ afq_status afq_copy_out(afq_handle* h, int which, void* host) {
       break;
     }
     case AFQ_BUF_VHS: {
+      if (h->mixed) AFQ_CUDA(h, afq::mixed_unpack_vhs(h->mixed, h->vHS, h->st));
       std::vector<z_t> t(nw * N * N);
       AFQ_CUDA(h, d2h(t.data(), h->vHS, sizeof(z_t) * t.size()));
       z_t* dst = static_cast<z_t*>(host);

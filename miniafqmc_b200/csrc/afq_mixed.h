@@ -30,5 +30,11 @@ cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpar
                               cudaStream_t st);
 // Kernels one call of a stage issues (afq_stage numbering), for the launch counters.
 int mixed_launches(const MixedState* m, int stage);
+// Cholesky-vector blocks of the exchange partial sums (Kpart[nw][2][nblk]).
+int mixed_nblk(const MixedState* m);
+// Timeout flags raised by the tensor-core kernels (0 when clean).
+cudaError_t mixed_error(MixedState* m, int* flags);
+// FP64 copy of the V operand ([nw][N*N]), for copy-out.
+cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st);
 
 }  // namespace afq

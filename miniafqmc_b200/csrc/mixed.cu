@@ -1,25 +1,603 @@
-// Mixed-precision stages (tensor cores).  Placeholder until the tcgen05 kernels land:
-// creating a mixed handle reports the form as unavailable.
+// Mixed-precision form of the contraction stages on tcgen05 tensor cores.
+//
+// Complex products C = A B run as real GEMMs D[m][n] = sum_k A'[m][k] B'[n][k] (both
+// operands K-major bf16, fp32 accumulation in TMEM):
+//   A' rows are A's rows with real and imaginary parts interleaved along K;
+//   B' has two rows per column j of B: (Re b, -Im b) interleaved -> D = Re C[:, j],
+//                                      (Im b,  Re b) interleaved -> D = Im C[:, j].
+// Each operand is stored as bf16 hi and lo parts (x = hi + lo); a stage runs either plain
+// bf16 (hi only) or the split form hi*hi + hi*lo + lo*hi (~16 significant bits).
+//
+//   vHS   : D[(w,re|im)][ik] = sum_c X[c][w] Spvn[ik][c]        -> V_w operand (epilogue)
+//   prop  : S = P W; T_k = (i/k) V T_{k-1}, S += T_k; W = P S    (fused Taylor epilogues)
+//   vbias : D[c][(w,re|im)] = sum_ak SpvnT[c][ak] Gc_w[ak]       (split K, fixed-order sum)
+//   E_J   : same product with the unscaled half-rotated factors
+//   E_K   : T_cw = Lh_c Gc_w^T per spin, trace of T^2 from the tile in shared memory
+// LU/overlaps, orthogonalisation, weights and the energy assembly stay FP64.
+#include <cuda_bf16.h>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "afq_kernels.h"
 #include "afq_mixed.h"
+#include "tc_gemm.cuh"
 
 namespace afq {
 
-struct MixedState {
-  int dummy;
+typedef __nv_bfloat16 bf16;
+typedef __nv_bfloat162 bf162;
+
+enum { PREC_BF16 = 0, PREC_SPLIT = 1 };
+
+struct Op {
+  bf16* hi = nullptr;
+  bf16* lo = nullptr;
 };
 
-cudaError_t mixed_create(const MixedInit*, MixedState** out, std::string* msg, cudaStream_t) {
+AFQ_D void put2(const Op& o, long long idx, float a, float b) {
+  bf162 h = __floats2bfloat162_rn(a, b);
+  float2 hf = __bfloat1622float2(h);
+  bf162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  *reinterpret_cast<bf162*>(o.hi + idx) = h;
+  *reinterpret_cast<bf162*>(o.lo + idx) = l;
+}
+AFQ_D void put1(const Op& o, long long idx, float a) {
+  bf16 h = __float2bfloat16_rn(a);
+  o.hi[idx] = h;
+  o.lo[idx] = __float2bfloat16_rn(a - __bfloat162float(h));
+}
+AFQ_D float2 get2(const Op& o, long long idx) {
+  float2 h = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.hi + idx));
+  float2 l = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.lo + idx));
+  return make_float2(h.x + l.x, h.y + l.y);
+}
+
+struct MixedState {
+  MixedInit in{};
+  int N = 0, n = 0, nc = 0, nw = 0;
+  long long NAK = 0;
+  bool s_real = true;
+  int Kv = 0;                  // K of the vHS product (nchol, or 2*nchol for complex Spvn)
+  int prec_vhs = PREC_SPLIT, prec_p = PREC_SPLIT, prec_v1 = PREC_SPLIT, prec_vk = PREC_BF16;
+  int prec_vbias = PREC_SPLIT, prec_ej = PREC_SPLIT, prec_ek = PREC_SPLIT;
+  int bn_prop = 0;             // tile width >= 4n of the propagation products
+  Op Sd, Pf, SpT, LhJ, LhX;    // static operands
+  Op Xf, Vf, F[2], Gb, Gx;     // per-step operands
+  float2* S = nullptr;         // Taylor sum [nw][N][2n]
+  float* part = nullptr;       // split-K partial products
+  int splits = 1, ksplit = 0;
+  int* err = nullptr;
+  int ex_Gn = 0, ex_Gw = 0, ex_bn = 0, ex_mtiles = 0;
+  std::vector<void*> allocs;
+  tc::Maps m_vhs, m_pw[2], m_v[2], m_vbias, m_ej, m_ek;
+};
+
+namespace {
+
+template <class T>
+cudaError_t malloc_track(MixedState* m, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * (count ? count : 1));
+  if (e == cudaSuccess) {
+    m->allocs.push_back(q);
+    *p = static_cast<T*>(q);
+  }
+  return e;
+}
+cudaError_t alloc_op(MixedState* m, Op& o, size_t count) {
+  cudaError_t e = malloc_track(m, &o.hi, count);
+  if (e == cudaSuccess) e = malloc_track(m, &o.lo, count);
+  return e;
+}
+
+// ------------------------------------------------------------ static operand packing
+// interleaved complex rows: dst[r][2q + {0,1}] = (Re, Im) src[r][q]
+__global__ void pack_complex_kernel(const z_t* __restrict__ src, long long count, Op dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x) {
+    z_t v = src[e];
+    put2(dst, 2 * e, (float)v.x, (float)v.y);
+  }
+}
+// Lh [c][s][a][k] -> LhX [s][c][a][2k]
+__global__ void pack_lhx_kernel(const z_t* __restrict__ Lh, int nc, int n, int N, Op dst) {
+  const long long per = (long long)n * N, tot = 2LL * nc * per;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long s = e / (nc * per), r = e % (nc * per), c = r / per, q = r % per;
+    z_t v = Lh[c * 2 * per + s * per + q];
+    put2(dst, 2 * e, (float)v.x, (float)v.y);
+  }
+}
+// dense Spvn from CSR: real values -> [ik][c]; complex -> [ik][2c + {0,1}]
+__global__ void pack_spvn_kernel(const int* __restrict__ ri, const int* __restrict__ ci,
+                                 const z_t* __restrict__ zv, const double* __restrict__ rv,
+                                 int nrows, int Kv, int real, Op dst) {
+  int r = blockIdx.x * blockDim.y + threadIdx.y;
+  if (r >= nrows) return;
+  for (int p = ri[r] + threadIdx.x; p < ri[r + 1]; p += blockDim.x) {
+    long long base = (long long)r * Kv;
+    if (real) put1(dst, base + ci[p], (float)(rv ? rv[p] : zv[p].x));
+    else put2(dst, base + 2LL * ci[p], (float)zv[p].x, (float)zv[p].y);
+  }
+}
+
+// ------------------------------------------------------------ per-step operand packing
+// X [nc][nw] -> Xf rows (w, re|im): real Spvn: (Re X[:,w]) and (Im X[:,w]);
+// complex Spvn: (Re, -Im) and (Im, Re) interleaved along c.
+__global__ void pack_x_kernel(const z_t* __restrict__ X, int nc, int nw, int Kv, int real, Op dst) {
+  __shared__ z_t t[32][33];
+  const int c0 = blockIdx.x * 32, w0 = blockIdx.y * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    int c = c0 + i, w = w0 + threadIdx.x;
+    t[i][threadIdx.x] = (c < nc && w < nw) ? X[(long long)c * nw + w] : zmk(0, 0);
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    int w = w0 + i, c = c0 + threadIdx.x;
+    if (w >= nw || c >= nc) continue;
+    z_t v = t[threadIdx.x][i];
+    long long r0 = (2LL * w) * Kv, r1 = (2LL * w + 1) * Kv;
+    if (real) {
+      put1(dst, r0 + c, (float)v.x);
+      put1(dst, r1 + c, (float)v.y);
+    } else {
+      put2(dst, r0 + 2 * c, (float)v.x, (float)-v.y);
+      put2(dst, r1 + 2 * c, (float)v.y, (float)v.x);
+    }
+  }
+}
+// W [nw][N][2n] -> B form F [nw][4n][2N]: row j: (Re W[:,j], -Im W[:,j]); row 2n+j: (Im, Re)
+__global__ void pack_w_kernel(const z_t* __restrict__ W, int N, int n2, Op dst) {
+  __shared__ z_t t[32][33];
+  const int w = blockIdx.z, k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+  const z_t* Ww = W + (long long)w * N * n2;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    int k = k0 + i, j = j0 + threadIdx.x;
+    t[i][threadIdx.x] = (k < N && j < n2) ? Ww[(long long)k * n2 + j] : zmk(0, 0);
+  }
+  __syncthreads();
+  const long long base = (long long)w * 2 * n2 * 2 * N;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    int j = j0 + i, k = k0 + threadIdx.x;
+    if (j >= n2 || k >= N) continue;
+    z_t v = t[threadIdx.x][i];
+    put2(dst, base + (long long)j * 2 * N + 2 * k, (float)v.x, (float)-v.y);
+    put2(dst, base + (long long)(n2 + j) * 2 * N + 2 * k, (float)v.y, (float)v.x);
+  }
+}
+// Gc [nw][2][n][N] -> Gb [2nw][2*NAK] (vbias / Coulomb B form) and, when Gx.hi is set,
+// Gx [2][nw][2n][2N] (exchange B form, rows (w, re|im, b) per spin).
+__global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N, Op Gb, Op Gx) {
+  const long long NAK = 2LL * n * N, tot = (long long)nw * NAK;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long w = e / NAK, q = e % NAK;
+    const z_t g = Gc[e];
+    put2(Gb, w * 2 * NAK + 2 * q, (float)g.x, (float)-g.y);
+    put2(Gb, (nw + w) * 2 * NAK + 2 * q, (float)g.y, (float)g.x);
+    if (Gx.hi) {
+      const long long s = q / ((long long)n * N), r = q % ((long long)n * N);
+      const long long b = r / N, k = r % N;
+      const long long row0 = (s * nw + w) * 2 * n + b, row1 = row0 + n;
+      put2(Gx, row0 * 2 * N + 2 * k, (float)g.x, (float)-g.y);
+      put2(Gx, row1 * 2 * N + 2 * k, (float)g.y, (float)g.x);
+    }
+  }
+}
+// sum of split-K partials: out[c][w] = sum_z part[z][c][w] + i part[z][c][nw + w]
+__global__ void reduce_part_kernel(const float* __restrict__ part, int splits, int M, int nw,
+                                   z_t* __restrict__ out) {
+  const long long tot = (long long)M * nw, sz = (long long)M * 2 * nw;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long c = e / nw, w = e % nw;
+    double re = 0.0, im = 0.0;
+    for (int z = 0; z < splits; z++) {
+      re += part[z * sz + c * 2 * nw + w];
+      im += part[z * sz + c * 2 * nw + nw + w];
+    }
+    out[e] = zmk(re, im);
+  }
+}
+// V operand back to FP64 vHS [nw][N*N] (for copy-out only)
+__global__ void unpack_v_kernel(Op V, long long count, z_t* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x) {
+    float2 v = get2(V, 2 * e);
+    out[e] = zmk(v.x, v.y);
+  }
+}
+
+int grid_for(long long n) { return (int)std::min<long long>((n + 255) / 256, 148LL * 16); }
+
+// ------------------------------------------------------------ epilogues
+// vHS: rows (w, re|im) are adjacent lanes; the even lane writes columns 0-15 of the
+// chunk, the odd lane columns 16-31, as (re, im) pairs of V_w[ik].
+struct EpiVhs {
+  static constexpr bool kTile = false;
+  Op V;
+  int nw;
+  long long nik;
+  AFQ_D void operator()(int, int, int m, int n0, const float* v) const {
+    const bool odd = threadIdx.x & 1;
+    float o[32];
+#pragma unroll
+    for (int i = 0; i < 32; i++) o[i] = __shfl_xor_sync(0xffffffffu, v[i], 1);
+    const int w = m >> 1;
+    if (w >= nw) return;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      if ((i < 16) == odd) continue;
+      const long long ik = n0 + i;
+      if (ik >= nik) continue;
+      const float re = odd ? o[i] : v[i], im = odd ? v[i] : o[i];
+      put2(V, ((long long)w * nik + ik) * 2, re, im);
+    }
+  }
+};
+
+// split-K partial products part[z][m][n]
+struct EpiPart {
+  static constexpr bool kTile = false;
+  float* part;
+  int M, Ncol;
+  long long sz;
+  AFQ_D void operator()(int z, int, int m, int n0, const float* v) const {
+    if (m >= M) return;
+    float* row = part + z * sz + (long long)m * Ncol;
+#pragma unroll
+    for (int i = 0; i < 32; i++)
+      if (n0 + i < Ncol) row[n0 + i] = v[i];
+  }
+};
+
+// Propagation products: tile rows i (orbital), columns [Re C | Im C] over the 2n walker
+// columns.  mode 0: S = C (P W); mode 1: T = (i/k) C, S += T (Taylor term k; the last
+// term forms S); mode 2: W = C (P S).  Modes 0 and 1 write the next B operand.
+struct EpiProp {
+  static constexpr bool kTile = true;
+  int mode, k, last, N, n2;
+  float2* S;
+  z_t* W;
+  Op F;          // B form of the next product [nw][2*n2][2N]
+  AFQ_D void tile(int w, int mt, int, float* t, int ld, int tid) const {
+    const int i0 = mt * 128;
+    const long long sW = (long long)N * n2;
+    for (int e = tid; e < 128 * n2; e += 128) {
+      const int r = e / n2, j = e % n2, i = i0 + r;
+      if (i >= N) continue;
+      const float cr = t[r * ld + j], ci = t[r * ld + n2 + j];
+      const long long o = w * sW + (long long)i * n2 + j;
+      if (mode == 0) {
+        S[o] = make_float2(cr, ci);
+      } else if (mode == 1) {
+        const float inv = 1.0f / (float)k;
+        const float tr = -ci * inv, ti = cr * inv;
+        float2 s = S[o];
+        s.x += tr;
+        s.y += ti;
+        S[o] = s;
+        t[r * ld + j] = last ? s.x : tr;
+        t[r * ld + n2 + j] = last ? s.y : ti;
+      } else {
+        W[o] = zmk(cr, ci);
+      }
+    }
+    if (mode == 2) return;
+    tc::epi_bar();
+    const long long base = (long long)w * 2 * n2 * 2 * N;
+    for (int e = tid; e < 128 * n2; e += 128) {
+      const int j = e / 128, r = e % 128, i = i0 + r;
+      if (i >= N) continue;
+      const float vr = t[r * ld + j], vi = t[r * ld + n2 + j];
+      put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
+      put2(F, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
+    }
+  }
+};
+
+// Exchange: rows (cv, a), columns (wl, re|im, b); per (cv, wl) the trace of T^2 with
+// T[a][b] = tile[cv*n + a][wl*2n + b] + i tile[cv*n + a][wl*2n + n + b].
+struct EpiExchange {
+  static constexpr bool kTile = true;
+  int n, Gn, Gw, nc, nw, nblk;
+  z_t* Kpart;
+  AFQ_D void tile(int s, int mt, int nt, float* t, int ld, int tid) const {
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int wl = warp; wl < Gw; wl += 4) {
+      const int w = nt * Gw + wl;
+      double sr = 0.0, si = 0.0;
+      for (int cv = 0; cv < Gn; cv++) {
+        if (mt * Gn + cv >= nc) break;
+        const float* rows = t + (long long)cv * n * ld + wl * 2 * n;
+        for (int q = lane; q < n * n; q += 32) {
+          const int a = q / n, b = q % n;
+          const double ar = rows[a * ld + b], ai = rows[a * ld + n + b];
+          const double br = rows[b * ld + a], bi = rows[b * ld + n + a];
+          sr += ar * br - ai * bi;
+          si += ar * bi + ai * br;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+      }
+      if (lane == 0 && w < nw) Kpart[((long long)w * 2 + s) * nblk + mt] = zmk(sr, si);
+    }
+  }
+};
+
+// ------------------------------------------------------------ dispatch helpers
+template <int BN, int ST, bool SPLIT, class Epi>
+cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
+                     cudaStream_t st) {
+  return tc::launch<BN, ST, false, SPLIT>(mp, g, e, err, st);
+}
+
+template <int BN, class Epi>
+cudaError_t run_prec(int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
+                     cudaStream_t st) {
+  // 4 stages for plain bf16, 2 for the split form (each stage carries hi and lo parts)
+  if (prec == PREC_SPLIT) return run_gemm<BN, 2, true>(mp, g, e, err, st);
+  return run_gemm<BN, 4, false>(mp, g, e, err, st);
+}
+
+template <class Epi>
+cudaError_t run_bn(int bn, int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e,
+                   int* err, cudaStream_t st) {
+  switch (bn) {
+    case 64: return run_prec<64>(prec, mp, g, e, err, st);
+    case 128: return run_prec<128>(prec, mp, g, e, err, st);
+    case 192: return run_prec<192>(prec, mp, g, e, err, st);
+    case 256: return run_prec<256>(prec, mp, g, e, err, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int pick_bn(int cols) {
+  if (cols <= 64) return 64;
+  if (cols <= 128) return 128;
+  if (cols <= 192) return 192;
+  if (cols <= 256) return 256;
+  return 0;
+}
+
+bool map2(tc::Maps& mp, const Op& a, uint64_t Ka, uint64_t ra, uint64_t ba, uint64_t lda,
+          uint64_t sa, const Op& b, uint64_t Kb, uint64_t rb, uint64_t bb, uint64_t ldb,
+          uint64_t sb, uint32_t bn) {
+  return tc::make_kmajor_map(&mp.a, a.hi, false, Ka, ra, ba, lda, sa, 128) == CUDA_SUCCESS &&
+         tc::make_kmajor_map(&mp.a_lo, a.lo, false, Ka, ra, ba, lda, sa, 128) == CUDA_SUCCESS &&
+         tc::make_kmajor_map(&mp.b, b.hi, false, Kb, rb, bb, ldb, sb, bn) == CUDA_SUCCESS &&
+         tc::make_kmajor_map(&mp.b_lo, b.lo, false, Kb, rb, bb, ldb, sb, bn) == CUDA_SUCCESS;
+}
+
+void parse_prec(MixedState* m) {
+  const char* env = getenv("AFQ_MIXED_PREC");   // e.g. "vhs=1,p=1,v1=1,vk=0,vbias=1,ej=1,ek=1"
+  if (!env) return;
+  std::string s(env);
+  auto get = [&](const char* key, int& dst) {
+    std::string k = std::string(key) + "=";
+    size_t p = s.find(k);
+    if (p != std::string::npos) dst = atoi(s.c_str() + p + k.size()) ? PREC_SPLIT : PREC_BF16;
+  };
+  get("vhs", m->prec_vhs); get("p", m->prec_p); get("v1", m->prec_v1); get("vk", m->prec_vk);
+  get("vbias", m->prec_vbias); get("ej", m->prec_ej); get("ek", m->prec_ek);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ public entry points
+cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* msg,
+                         cudaStream_t st) {
   *out = nullptr;
-  if (msg) *msg = "mixed-precision form not built";
+  MixedState* m = new MixedState();
+  m->in = *init;
+  m->N = init->N; m->n = init->n; m->nc = init->nchol; m->nw = init->nw;
+  m->NAK = 2LL * m->n * m->N;
+  const int N = m->N, n = m->n, nc = m->nc, nw = m->nw;
+  const long long NAK = m->NAK;
+  parse_prec(m);
+  auto bail = [&](cudaError_t e, const std::string& why) {
+    if (msg) *msg = why;
+    mixed_destroy(m);
+    return e == cudaSuccess ? cudaErrorInvalidValue : e;
+  };
+  m->bn_prop = pick_bn(4 * n);
+  if (!m->bn_prop) return bail(cudaSuccess, "4*NAEA exceeds 256");
+  if (!init->SpvnT_dense) return bail(cudaSuccess, "SpvnT below the dense threshold");
+  if ((2 * N) % 8 || (2 * NAK) % 8) return bail(cudaSuccess, "operand rows must be 16-byte multiples");
+  m->s_real = init->sp_rv != nullptr;
+  m->Kv = m->s_real ? nc : 2 * nc;
+  if (m->Kv % 8) return bail(cudaSuccess, "nchol must be a multiple of 8 (4 for complex Spvn)");
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  A(alloc_op(m, m->Sd, (size_t)N * N * m->Kv));
+  A(alloc_op(m, m->Pf, (size_t)N * 2 * N));
+  A(alloc_op(m, m->SpT, (size_t)nc * 2 * NAK));
+  A(alloc_op(m, m->Xf, (size_t)2 * nw * m->Kv));
+  A(alloc_op(m, m->Vf, (size_t)nw * N * 2 * N));
+  A(alloc_op(m, m->F[0], (size_t)nw * 4 * n * 2 * N));
+  A(alloc_op(m, m->F[1], (size_t)nw * 4 * n * 2 * N));
+  A(alloc_op(m, m->Gb, (size_t)2 * nw * 2 * NAK));
+  A(malloc_track(m, &m->S, (size_t)nw * N * 2 * n));
+  A(malloc_track(m, &m->err, 1));
+  if (init->Lh) {
+    A(alloc_op(m, m->LhJ, (size_t)nc * 2 * NAK));
+    A(alloc_op(m, m->LhX, (size_t)nc * 2 * NAK));
+    A(alloc_op(m, m->Gx, (size_t)nw * 2 * NAK * 2));
+  }
+  // split K of the vbias / Coulomb products so the grid covers the GPU
+  {
+    const long long Kq = 2 * NAK;
+    const int tiles = ((nc + 127) / 128) * ((2 * nw + 127) / 128);
+    int sp = std::max(1, std::min(16, (int)((4 * 148 + tiles - 1) / tiles)));
+    long long ks = (Kq + sp - 1) / sp;
+    ks = (ks + 63) / 64 * 64;
+    sp = (int)((Kq + ks - 1) / ks);
+    m->splits = sp;
+    m->ksplit = (int)ks;
+    A(malloc_track(m, &m->part, (size_t)sp * nc * 2 * nw));
+  }
+  if (e != cudaSuccess) return bail(e, "allocation");
+  A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+  A(cudaMemsetAsync(m->Sd.hi, 0, sizeof(bf16) * (size_t)N * N * m->Kv, st));
+  A(cudaMemsetAsync(m->Sd.lo, 0, sizeof(bf16) * (size_t)N * N * m->Kv, st));
+  pack_spvn_kernel<<<(N * N + 7) / 8, dim3(32, 8), 0, st>>>(init->sp_ri, init->sp_ci, init->sp_v,
+                                                            init->sp_rv, N * N, m->Kv, m->s_real,
+                                                            m->Sd);
+  pack_complex_kernel<<<grid_for((long long)N * N), 256, 0, st>>>(init->P, (long long)N * N, m->Pf);
+  pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->SpvnT_dense,
+                                                                    (long long)nc * NAK, m->SpT);
+  if (init->Lh) {
+    pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, (long long)nc * NAK,
+                                                                      m->LhJ);
+    pack_lhx_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, nc, n, N, m->LhX);
+  }
+  A(cudaGetLastError());
+  A(cudaStreamSynchronize(st));
+  if (e != cudaSuccess) return bail(e, "packing");
+  // tensor maps
+  bool ok = true;
+  const int bnv = 256;
+  ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, (uint64_t)N * N, 1, m->Kv,
+             0, bnv);
+  const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
+  for (int i = 0; i < 2; i++) {
+    ok &= map2(m->m_pw[i], m->Pf, 2 * N, N, 1, 2 * N, 0, m->F[i], 2 * N, fr, nw, 2 * N, fsz,
+               m->bn_prop);
+    ok &= map2(m->m_v[i], m->Vf, 2 * N, N, nw, 2 * N, (uint64_t)N * 2 * N, m->F[i], 2 * N, fr, nw,
+               2 * N, fsz, m->bn_prop);
+  }
+  ok &= map2(m->m_vbias, m->SpT, 2 * NAK, nc, 1, 2 * NAK, 0, m->Gb, 2 * NAK, 2 * nw, 1, 2 * NAK, 0,
+             128);
+  if (init->Lh) {
+    ok &= map2(m->m_ej, m->LhJ, 2 * NAK, nc, 1, 2 * NAK, 0, m->Gb, 2 * NAK, 2 * nw, 1, 2 * NAK, 0,
+               128);
+    m->ex_Gn = 128 / n;
+    m->ex_Gw = std::max(1, 256 / (2 * n));
+    while (m->ex_Gw > 1 && !pick_bn(m->ex_Gw * 2 * n)) m->ex_Gw--;
+    m->ex_bn = pick_bn(m->ex_Gw * 2 * n);
+    // the tile must hold whole walkers: use the exact width when it is a compiled size
+    if (m->ex_bn != m->ex_Gw * 2 * n) {
+      int gw = m->ex_Gw;
+      while (gw > 1 && pick_bn(gw * 2 * n) != gw * 2 * n) gw--;
+      if (pick_bn(gw * 2 * n) == gw * 2 * n) { m->ex_Gw = gw; m->ex_bn = gw * 2 * n; }
+    }
+    m->ex_mtiles = (nc + m->ex_Gn - 1) / m->ex_Gn;
+    ok &= map2(m->m_ek, m->LhX, 2 * N, (uint64_t)nc * n, 2, 2 * N, (uint64_t)nc * n * 2 * N, m->Gx,
+               2 * N, (uint64_t)nw * 2 * n, 2, 2 * N, (uint64_t)nw * 2 * n * 2 * N, m->ex_bn);
+  }
+  if (!ok) return bail(cudaSuccess, "tensor map encoding failed");
+  *out = m;
   return cudaSuccess;
 }
-void mixed_destroy(MixedState* m) { delete m; }
-cudaError_t mixed_vbias(MixedState*, const z_t*, z_t*, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t mixed_vhs(MixedState*, const z_t*, z_t*, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t mixed_propagate(MixedState*, z_t*, const z_t*, cudaStream_t) { return cudaErrorNotSupported; }
-cudaError_t mixed_energy_chol(MixedState*, const z_t*, z_t*, z_t*, int, cudaStream_t) {
-  return cudaErrorNotSupported;
+
+void mixed_destroy(MixedState* m) {
+  if (!m) return;
+  for (void* p : m->allocs) cudaFree(p);
+  delete m;
 }
-int mixed_launches(const MixedState*, int) { return 0; }
+
+int mixed_nblk(const MixedState* m) { return m ? m->ex_mtiles : 0; }
+
+cudaError_t mixed_error(MixedState* m, int* flags) {
+  return cudaMemcpy(flags, m->err, sizeof(int), cudaMemcpyDeviceToHost);
+}
+
+int mixed_launches(const MixedState* m, int stage) {
+  switch (stage) {
+    case 1: return 3;                                  // pack, GEMM, reduce (vbias)
+    case 3: return 2;                                  // pack, GEMM (vHS)
+    case 4: return 2 + m->in.order + 1;                // pack, P W, order terms, P S
+    case 8: return m->in.Lh ? 4 : 0;                   // pack, E_J GEMM, reduce, E_K GEMM
+  }
+  return 0;
+}
+
+cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
+  const int nc = m->nc, nw = m->nw, N = m->N;
+  pack_x_kernel<<<dim3((nc + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(X, nc, nw, m->Kv,
+                                                                             m->s_real, m->Xf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  tc::GemmShape g{2 * nw, N * N, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0};
+  EpiVhs epi{m->Vf, nw, (long long)N * N};
+  return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
+}
+
+cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st) {
+  const long long cnt = (long long)m->nw * m->N * m->N;
+  unpack_v_kernel<<<grid_for(cnt), 256, 0, st>>>(m->Vf, cnt, vHS);
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) {
+  const int N = m->N, n2 = 2 * m->n, nw = m->nw;
+  pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0]);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int mt = (N + 127) / 128;
+  int cur = 0;
+  {  // S = P W
+    tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, false, true, 0};
+    EpiProp ep{0, 0, 0, N, n2, m->S, nullptr, m->F[1]};
+    if ((e = run_bn(m->bn_prop, m->prec_p, m->m_pw[0], g, ep, m->err, st)) != cudaSuccess) return e;
+    cur = 1;
+  }
+  for (int k = 1; k <= m->in.order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
+    tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, true, true, 0};
+    EpiProp ep{1, k, k == m->in.order, N, n2, m->S, nullptr, m->F[cur ^ 1]};
+    int prec = k == 1 ? m->prec_v1 : m->prec_vk;
+    if ((e = run_bn(m->bn_prop, prec, m->m_v[cur], g, ep, m->err, st)) != cudaSuccess) return e;
+    cur ^= 1;
+  }
+  if (m->in.order == 0) {   // no Taylor terms: S itself feeds P S
+    // F[cur] already holds the B form of S = P W
+  }
+  {  // W = P S
+    tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, false, true, 0};
+    EpiProp ep{2, 0, 0, N, n2, m->S, W, Op{}};
+    if ((e = run_bn(m->bn_prop, m->prec_p, m->m_pw[cur], g, ep, m->err, st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, z_t* out,
+                                  cudaStream_t st) {
+  const int nc = m->nc, nw = m->nw;
+  tc::GemmShape g{nc, 2 * nw, (int)(2 * m->NAK), m->splits, 128, (nc + 127) / 128, false, false,
+                  m->ksplit};
+  EpiPart ep{m->part, nc, 2 * nw, (long long)nc * 2 * nw};
+  cudaError_t e = run_bn(128, prec, mp, g, ep, m->err, st);
+  if (e != cudaSuccess) return e;
+  reduce_part_kernel<<<grid_for((long long)nc * nw), 256, 0, st>>>(m->part, m->splits, nc, nw, out);
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_vbias(MixedState* m, const z_t* Gc, z_t* vbias, cudaStream_t st) {
+  pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
+                                                                      Op{});
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return splitk_product(m, m->m_vbias, m->prec_vbias, vbias, st);
+}
+
+cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpart, int nblk,
+                              cudaStream_t st) {
+  if (!m->in.Lh) return cudaErrorInvalidValue;
+  pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
+                                                                      m->Gx);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if ((e = splitk_product(m, m->m_ej, m->prec_ej, cvec, st)) != cudaSuccess) return e;
+  const int n = m->n;
+  tc::GemmShape g{m->nc * n, m->nw * 2 * n, 2 * m->N, 2, m->ex_Gn * n, m->ex_mtiles, true, true, 0};
+  EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, m->nw, nblk, Kpart};
+  return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g, ep, m->err, st);
+}
 
 }  // namespace afq

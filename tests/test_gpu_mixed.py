@@ -1,0 +1,99 @@
+"""The mixed-precision (tcgen05) form against the FP64 form on identical inputs.
+
+Stage tolerances (relative to the largest magnitude of the quantity):
+  split bf16 (hi*hi + hi*lo + lo*hi) stages: 1e-4    plain bf16 stages: 2e-2
+Trajectory: per-step mixed energy within 1e-4 relative of the FP64 energy on the same
+auxiliary fields.  Measured errors are written to gpurun_out/mixed_errors.json."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, system
+
+pytestmark = pytest.mark.gpu
+OUT = os.path.join(ROOT, "gpurun_out", "mixed_errors.json")
+ERRS = {}
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def record(key, val):
+    ERRS[key] = val
+    os.makedirs(os.path.dirname(OUT), exist_ok=True)
+    with open(OUT, "w") as f:
+        json.dump(ERRS, f, indent=1)
+
+
+def pair(s, nw, walkers):
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
+    d = AfqmcSys(s, nw, precision=AFQ_PREC_FP64, walkers=walkers)
+    m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=walkers)
+    return d, m
+
+
+def perturbed(s, nw, seed=0, amp=0.05):
+    rng = np.random.default_rng(seed)
+    W, Wd = s.initial_walkers(nw)
+    W = W + amp * (rng.normal(size=W.shape) + 1j * rng.normal(size=W.shape))
+    Wd[:, 1] = rng.uniform(0.5, 1.5, nw)
+    return W, Wd
+
+
+@pytest.mark.parametrize("name,kw,nw", [("C1", {}, 16),
+                                        ("C1", dict(complex_trial=True, complex_chol=True,
+                                                    nchol=96, seed=5), 16),
+                                        ("C2", dict(with_vakbl=False), 64)])
+def test_mixed_stages(name, kw, nw):
+    s = system(name, **kw)
+    tag = name + ("c" if kw.get("complex_chol") else "")
+    d, m = pair(s, nw, perturbed(s, nw))
+    for e in (d, m):
+        e.calculate_mixed_density_matrix()
+        e.get_vbias()
+    ev = rel(m.copy_out("vbias"), d.copy_out("vbias"))
+    for e in (d, m):
+        e.sigma(3, 1)
+        e.get_vHS()
+    eh = rel(m.copy_out("vHS"), d.copy_out("vHS"))
+    for e in (d, m):
+        e.propagate()
+    ew = rel(m.get_walkers()[0], d.get_walkers()[0])
+    for e in (d, m):
+        e.calculate_mixed_density_matrix()
+    ed, em = d.calculate_energy("chol"), m.calculate_energy("chol")
+    pd, pm = d.copy_out("energy_parts"), m.copy_out("energy_parts")
+    m.synchronize()
+    res = {"vbias": ev, "vHS": eh, "W_after_propagate": ew, "E": abs(em - ed) / abs(ed),
+           "E1": rel(pm[:, 0], pd[:, 0]), "EJ": rel(pm[:, 1], pd[:, 1]), "EK": rel(pm[:, 2], pd[:, 2]),
+           "E_abs_Ha": abs(em - ed)}
+    record(f"stages_{tag}", res)
+    assert ev < 1e-4 and eh < 1e-4
+    assert ew < 2e-2
+    assert res["EJ"] < 1e-4 and res["EK"] < 1e-4
+    d.close()
+    m.close()
+
+
+def test_mixed_trajectory_C1():
+    s = system("C1")
+    nw = 16
+    d, m = pair(s, nw, None)
+    dE = []
+    for e in (d, m):
+        e.calculate_mixed_density_matrix()
+    for st in range(20):
+        for e in (d, m):
+            e.substep(0, st, 5, graph=True)
+            e.calculate_mixed_density_matrix()
+        ed, em = d.calculate_energy("chol"), m.calculate_energy("chol")
+        dE.append(abs(em - ed))
+    m.synchronize()
+    record("trajectory_C1", {"max_abs_dE_Ha": max(dE), "dE_per_step": dE,
+                             "E_last": ed})
+    assert max(dE) / abs(ed) < 1e-4
+    d.close()
+    m.close()
