@@ -165,6 +165,24 @@ afq_status afq_get_stream(afq_handle* h, void** stream);
 /* Copies a device buffer to host memory in the reference layout (see afq_buffer). */
 afq_status afq_copy_out(afq_handle* h, int which, void* host);
 
+/* Exchange energy of a batch of walkers without allocating any device memory.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc: work recorded
+ * into a CUDA graph under stream capture (an allocation there breaks the capture) and
+ * host frameworks that own all device memory through their own pool.
+ *   Lh  [nchol][2][naea][nmo] complex, unscaled half-rotated factors (device memory)
+ *   Gc  [nwalk][2][naea][nmo] complex, compact density matrices, walker-major (device)
+ *   ek  [nwalk] complex output (device): EK_w = 1/2 sum_{s,n} tr(T T), T = Lh_s[n] Gc_s^T
+ * Asynchronous on `stream` (a cudaStream_t, NULL for the default stream).  The partial
+ * sums live in one file-scope device array of 2^18 complex values (4 MiB, held by every
+ * GPU that loads the library until exit): calls with 2 * nwalk * ceil(nchol / (96 /
+ * naea)) above that are rejected with AFQ_ERR_UNSUPPORTED (split the walkers into
+ * batches); naea must be <= 96.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture.  All calls share the array, so calls that overlap on the GPU (on
+ * different streams) race; serialise them. */
+afq_status afq_exchange_energy_noalloc(const double* Lh, const double* Gc, int nmo, int naea,
+                                       int nchol, int nwalk, double* ek, void* stream);
+
 /* Self-test of the tensor-core GEMM used by the mixed form (no reference counterpart):
  * C[b][m][n] = sum_k A[b][m][k] B[b][n][k] for host fp32 arrays, computed on the current
  * device with bf16 operands (tf32 == 0, inputs rounded to nearest bf16) or tf32 operands,

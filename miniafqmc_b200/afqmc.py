@@ -31,7 +31,7 @@ EXPORTS = [
     "afq_update_weights", "afq_update_weights_partial", "afq_get_eshift", "afq_set_eshift",
     "afq_orthogonalize", "afq_energy", "afq_energy_sums", "afq_substep", "afq_synchronize",
     "afq_copy_out", "afq_set_walker_offset", "afq_profile", "afq_stage_times", "afq_get_stream",
-    "afq_selftest_tc_gemm",
+    "afq_selftest_tc_gemm", "afq_exchange_energy_noalloc",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -83,6 +83,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_profile": ([P, I], I), "afq_stage_times": ([P, P, P, I], I),
         "afq_get_stream": ([P, P], I),
         "afq_selftest_tc_gemm": ([I, I, I, I, I, I, P, P, P, P], I),
+        "afq_exchange_energy_noalloc": ([P, P, I, I, I, I, P, P], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
