@@ -259,7 +259,12 @@ cudaError_t body_weights(afq_handle* h, int update_eshift) {
   return afq::launch_weights(h->Wd, h->hybridW, h->nw, h->d.dt, h->sc, update_eshift, h->st);
 }
 
-cudaError_t body_ortho(afq_handle* h) { return afq::launch_ortho(h->W, h->N, h->n, h->nw, h->st); }
+// The FP64 form keeps LAPACK's Householder convention (raw overlaps match the
+// reference); the mixed form uses CholeskyQR2, equal up to column signs.
+cudaError_t body_ortho(afq_handle* h) {
+  if (h->mixed) return afq::launch_ortho_cholqr(h->W, h->N, h->n, h->nw, h->info, h->st);
+  return afq::launch_ortho(h->W, h->N, h->n, h->nw, h->st);
+}
 
 cudaError_t body_energy(afq_handle* h, int mode) {
   cudaError_t e;

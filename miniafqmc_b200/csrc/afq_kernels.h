@@ -22,6 +22,7 @@ cudaError_t launch_set_scalars(DevScalars* sc, unsigned long long seed, unsigned
                                int set_eshift, double eshift, cudaStream_t st,
                                int walker_offset = 0, long long nwalk_global = 0);
 cudaError_t launch_ortho(z_t* W, int N, int n, int nw, cudaStream_t st);
+cudaError_t launch_ortho_cholqr(z_t* W, int N, int n, int nw, int* info, cudaStream_t st);
 size_t exch_smem_bytes();
 cudaError_t launch_exchange(const z_t* Lh, const z_t* Gc, int N, int n, int nchol, int nw,
                             z_t* Kpart, int* nblk_out, cudaStream_t st);

@@ -556,6 +556,131 @@ cudaError_t launch_ortho(z_t* W, int N, int n, int nw, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// CholeskyQR2 re-orthogonalisation (FP64): G = W_s^H W_s, G = R^H R (R upper, positive
+// real diagonal), W_s <- W_s R^-1, done twice.  The columns span the same space as the
+// Householder result and differ from it by a diagonal of +-1, so G, overlap ratios,
+// weights and energies are unchanged; only raw overlaps may change sign.  One CTA per
+// (walker, spin); the n x n factors live in shared memory, W streams through it in
+// 32-row chunks.  A walker whose Gram matrix is not positive definite is left as is
+// and flagged in info.
+constexpr int CQ_KC = 32;
+
+size_t cholqr_smem_bytes(int n) {
+  return sizeof(z_t) * ((size_t)2 * n * (n + 1) + (size_t)CQ_KC * (n + 1));
+}
+
+__global__ void __launch_bounds__(256)
+ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
+  extern __shared__ __align__(16) unsigned char cq_smem[];
+  const int w = blockIdx.x >> 1, s = blockIdx.x & 1;
+  const int ld = n + 1;
+  z_t* G = reinterpret_cast<z_t*>(cq_smem);     // Gram matrix, then R
+  z_t* Ri = G + n * ld;                          // R^-1
+  z_t* buf = Ri + n * ld;                        // W chunk [KC][n+1]
+  __shared__ int s_bad;
+  const long long ldw = 2 * n;
+  z_t* B = W + (long long)w * N * ldw + s * n;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid == 0) s_bad = 0;
+  for (int pass = 0; pass < 2; pass++) {
+    // ---- Gram matrix G[a][b] = sum_k conj(B[k][a]) B[k][b]
+    z_t acc[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) acc[r] = zmk(0, 0);
+    for (int k0 = 0; k0 < N; k0 += CQ_KC) {
+      const int kc = min(CQ_KC, N - k0);
+      for (int e = tid; e < kc * n; e += nt) {
+        int kk = e / n, a = e % n;
+        buf[kk * ld + a] = B[(long long)(k0 + kk) * ldw + a];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < 16; r++) {
+        int o = tid + r * 256;
+        if (o < n * n) {
+          int a = o / n, b = o % n;
+          z_t t = acc[r];
+          for (int kk = 0; kk < kc; kk++) zfma_conj(t, buf[kk * ld + a], buf[kk * ld + b]);
+          acc[r] = t;
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int r = 0; r < 16; r++) {
+      int o = tid + r * 256;
+      if (o < n * n) G[(o / n) * ld + (o % n)] = acc[r];
+    }
+    __syncthreads();
+    // ---- Cholesky G = R^H R in place (upper triangle)
+    for (int j = 0; j < n; j++) {
+      const double dj = G[j * ld + j].x;
+      if (!(dj > 0.0)) {
+        if (tid == 0) s_bad = 1;
+        break;
+      }
+      const double d = sqrt(dj), inv = 1.0 / d;
+      __syncthreads();
+      for (int l = j + tid; l < n; l += nt)
+        G[j * ld + l] = (l == j) ? zmk(d, 0.0) : zscale(G[j * ld + l], inv);
+      __syncthreads();
+      const int m = n - j - 1;
+      for (int e = tid; e < m * m; e += nt) {
+        int a = j + 1 + e / m, b = j + 1 + e % m;
+        if (b < a) continue;   // upper triangle only
+        z_t t = G[a * ld + b];
+        zfma(t, zmk(-G[j * ld + a].x, G[j * ld + a].y), G[j * ld + b]);   // -= conj(R_ja) R_jb
+        G[a * ld + b] = t;
+      }
+      __syncthreads();
+    }
+    __syncthreads();
+    if (s_bad) break;
+    // ---- R^-1 (upper) by back substitution, one column per thread
+    for (int j = tid; j < n; j += nt) {
+      for (int i = n - 1; i >= 0; i--) {
+        z_t t = (i == j) ? zmk(1.0, 0.0) : zmk(0.0, 0.0);
+        if (i <= j) {
+          for (int l = i + 1; l <= j; l++) t = zsub(t, zmul(G[i * ld + l], Ri[l * ld + j]));
+          t = zscale(t, 1.0 / G[i * ld + i].x);
+        }
+        Ri[i * ld + j] = t;
+      }
+    }
+    __syncthreads();
+    // ---- B <- B R^-1 in 32-row chunks
+    for (int k0 = 0; k0 < N; k0 += CQ_KC) {
+      const int kc = min(CQ_KC, N - k0);
+      for (int e = tid; e < kc * n; e += nt) {
+        int kk = e / n, a = e % n;
+        buf[kk * ld + a] = B[(long long)(k0 + kk) * ldw + a];
+      }
+      __syncthreads();
+      for (int e = tid; e < kc * n; e += nt) {
+        int kk = e / n, b = e % n;
+        z_t t = zmk(0, 0);
+        for (int a = 0; a <= b; a++) zfma(t, buf[kk * ld + a], Ri[a * ld + b]);
+        B[(long long)(k0 + kk) * ldw + b] = t;
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) info[w * 2 + s] |= s_bad ? 2 : 0;
+}
+
+cudaError_t launch_ortho_cholqr(z_t* W, int N, int n, int nw, int* info, cudaStream_t st) {
+  size_t smem = cholqr_smem_bytes(n);
+  static size_t attr = 0;
+  if (smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(ortho_cholqr_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = smem;
+  }
+  ortho_cholqr_kernel<<<2 * nw, 256, smem, st>>>(W, N, n, info);
+  return cudaGetLastError();
+}
+
 // ============================================================ exchange energy
 // K_w = 1/2 sum_{s,c} tr(T T), T = Lh_s[c] Gc_s^T (n x n), for Gn Cholesky vectors x Gw
 // walkers per CTA: a (Gn*n) x (Gw*n) complex tile over K = N, then the trace of each

@@ -217,7 +217,7 @@ int grid_for(long long n) { return (int)std::min<long long>((n + 255) / 256, 148
 // vHS: rows (w, re|im) are adjacent lanes; the even lane writes columns 0-15 of the
 // chunk, the odd lane columns 16-31, as (re, im) pairs of V_w[ik].
 struct EpiVhs {
-  static constexpr bool kTile = false;
+  static constexpr bool kTile = false, kPair = false;
   Op V;
   int nw;
   long long nik;
@@ -241,7 +241,7 @@ struct EpiVhs {
 
 // split-K partial products part[z][m][n]
 struct EpiPart {
-  static constexpr bool kTile = false;
+  static constexpr bool kTile = false, kPair = false;
   float* part;
   int M, Ncol;
   long long sz;
@@ -258,7 +258,7 @@ struct EpiPart {
 // columns.  mode 0: S = C (P W); mode 1: T = (i/k) C, S += T (Taylor term k; the last
 // term forms S); mode 2: W = C (P S).  Modes 0 and 1 write the next B operand.
 struct EpiProp {
-  static constexpr bool kTile = true;
+  static constexpr bool kTile = true, kPair = false;
   int mode, k, last, N, n2;
   float2* S;
   z_t* W;
@@ -299,10 +299,49 @@ struct EpiProp {
   }
 };
 
+// The same propagation epilogue without a shared-memory tile, for 2n a multiple of 32:
+// each thread receives Re C and Im C of 32 columns of its row.  S is updated in place
+// and the next B operand is written with lanes on consecutive orbitals (coalesced).
+struct EpiPropPair {
+  static constexpr bool kTile = false, kPair = true;
+  int mode, k, last, N, n2;
+  float2* S;
+  z_t* W;
+  Op F;
+  AFQ_D int pair_stride() const { return n2; }
+  AFQ_D void pair(int w, int, int i, int j0, const float* cr, const float* ci) const {
+    if (i >= N) return;
+    const long long row = (long long)w * N * n2 + (long long)i * n2;
+    const long long base = (long long)w * 2 * n2 * 2 * N;
+    const float inv = mode == 1 ? 1.0f / (float)k : 0.0f;
+#pragma unroll
+    for (int jj = 0; jj < 32; jj++) {
+      const int j = j0 + jj;
+      float vr = cr[jj], vi = ci[jj];
+      if (mode == 0) {
+        S[row + j] = make_float2(vr, vi);
+      } else if (mode == 1) {
+        const float tr = -vi * inv, ti = vr * inv;
+        float2 s = S[row + j];
+        s.x += tr;
+        s.y += ti;
+        S[row + j] = s;
+        vr = last ? s.x : tr;
+        vi = last ? s.y : ti;
+      } else {
+        W[row + j] = zmk(vr, vi);
+        continue;
+      }
+      put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
+      put2(F, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
+    }
+  }
+};
+
 // Exchange: rows (cv, a), columns (wl, re|im, b); per (cv, wl) the trace of T^2 with
 // T[a][b] = tile[cv*n + a][wl*2n + b] + i tile[cv*n + a][wl*2n + n + b].
 struct EpiExchange {
-  static constexpr bool kTile = true;
+  static constexpr bool kTile = true, kPair = false;
   int n, Gn, Gw, nc, nw, nblk;
   z_t* Kpart;
   AFQ_D void tile(int s, int mt, int nt, float* t, int ld, int tid) const {
@@ -338,24 +377,38 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
   return tc::launch<BN, ST, false, SPLIT>(mp, g, e, err, st);
 }
 
-template <int BN, class Epi>
+// Stage counts: the default ring (4 plain / 2 split stages) keeps one CTA per SM busy;
+// the lean ring (2 plain / 1 split) lets two CTAs share an SM so one's epilogue overlaps
+// the other's main loop (used when the epilogue needs no shared-memory tile).
+template <int BN, bool LEAN, class Epi>
 cudaError_t run_prec(int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
                      cudaStream_t st) {
-  // 4 stages for plain bf16, 2 for the split form (each stage carries hi and lo parts)
-  if (prec == PREC_SPLIT) return run_gemm<BN, 2, true>(mp, g, e, err, st);
-  return run_gemm<BN, 4, false>(mp, g, e, err, st);
+  if (prec == PREC_SPLIT) return run_gemm<BN, (LEAN ? 1 : 2), true>(mp, g, e, err, st);
+  return run_gemm<BN, (LEAN ? 2 : 4), false>(mp, g, e, err, st);
 }
 
-template <class Epi>
+template <bool LEAN = false, class Epi>
 cudaError_t run_bn(int bn, int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e,
                    int* err, cudaStream_t st) {
   switch (bn) {
-    case 64: return run_prec<64>(prec, mp, g, e, err, st);
-    case 128: return run_prec<128>(prec, mp, g, e, err, st);
-    case 192: return run_prec<192>(prec, mp, g, e, err, st);
-    case 256: return run_prec<256>(prec, mp, g, e, err, st);
+    case 64: return run_prec<64, LEAN>(prec, mp, g, e, err, st);
+    case 128: return run_prec<128, LEAN>(prec, mp, g, e, err, st);
+    case 192: return run_prec<192, LEAN>(prec, mp, g, e, err, st);
+    case 256: return run_prec<256, LEAN>(prec, mp, g, e, err, st);
   }
   return cudaErrorInvalidValue;
+}
+
+// propagation product with the pair epilogue when 2n is a multiple of 32
+cudaError_t run_prop(MixedState* m, int prec, const tc::Maps& mp, const tc::GemmShape& g, int mode,
+                     int k, int last, z_t* W, const Op& F, cudaStream_t st) {
+  const int n2 = 2 * m->n;
+  if (n2 % 32 == 0) {
+    EpiPropPair ep{mode, k, last, m->N, n2, m->S, W, F};
+    return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st);
+  }
+  EpiProp ep{mode, k, last, m->N, n2, m->S, W, F};
+  return run_bn(m->bn_prop, prec, mp, g, ep, m->err, st);
 }
 
 int pick_bn(int cols) {
@@ -544,24 +597,21 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
   int cur = 0;
   {  // S = P W
     tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, false, true, 0};
-    EpiProp ep{0, 0, 0, N, n2, m->S, nullptr, m->F[1]};
-    if ((e = run_bn(m->bn_prop, m->prec_p, m->m_pw[0], g, ep, m->err, st)) != cudaSuccess) return e;
+    if ((e = run_prop(m, m->prec_p, m->m_pw[0], g, 0, 0, 0, nullptr, m->F[1], st)) != cudaSuccess)
+      return e;
     cur = 1;
   }
   for (int k = 1; k <= m->in.order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
     tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, true, true, 0};
-    EpiProp ep{1, k, k == m->in.order, N, n2, m->S, nullptr, m->F[cur ^ 1]};
     int prec = k == 1 ? m->prec_v1 : m->prec_vk;
-    if ((e = run_bn(m->bn_prop, prec, m->m_v[cur], g, ep, m->err, st)) != cudaSuccess) return e;
+    if ((e = run_prop(m, prec, m->m_v[cur], g, 1, k, k == m->in.order, nullptr, m->F[cur ^ 1],
+                      st)) != cudaSuccess)
+      return e;
     cur ^= 1;
   }
-  if (m->in.order == 0) {   // no Taylor terms: S itself feeds P S
-    // F[cur] already holds the B form of S = P W
-  }
-  {  // W = P S
+  {  // W = P S (with order 0 the B operand of S = P W is already in F[cur])
     tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, false, true, 0};
-    EpiProp ep{2, 0, 0, N, n2, m->S, W, Op{}};
-    if ((e = run_bn(m->bn_prop, m->prec_p, m->m_pw[cur], g, ep, m->err, st)) != cudaSuccess) return e;
+    if ((e = run_prop(m, m->prec_p, m->m_pw[cur], g, 2, 0, 0, W, Op{}, st)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

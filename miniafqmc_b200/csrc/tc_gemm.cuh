@@ -155,10 +155,12 @@ struct Maps {
 // Named barrier among the 128 epilogue threads (warps 0-3).
 AFQ_D void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
-// Epilogue interface.  Row-wise functors (Epi::kTile == false) get
+// Epilogue interface.  Row-wise functors (Epi::kTile == Epi::kPair == false) get
 //   epi(batch, tile_row, m, n_first, v[32])
-// for each 32-column chunk of each of the 128 rows.  Tile functors (kTile == true) get
-// the whole fp32 tile in shared memory (row stride BN + 1) after the epilogue barrier:
+// for each 32-column chunk of each of the 128 rows.  Pair functors (kPair) get chunks
+// c0 and c0 + P of a row together, epi.pair(batch, tile_row, m, c0, v[32], u[32]), for
+// c0 < P = epi.pair_stride().  Tile functors (kTile) get the whole fp32 tile in shared
+// memory (row stride BN + 1) after the epilogue barrier:
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
 template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi>
 __global__ void __launch_bounds__(192, 1)
@@ -262,7 +264,18 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
       const int row = warp * 32 + lane;
       const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
       float v[32];
-      if constexpr (Epi::kTile) {
+      if constexpr (Epi::kPair) {
+        // columns [0, P) pair with [P, 2P): chunk c0 and chunk c0 + P reach the functor
+        // together (P = epi.pair_stride(), a multiple of 32)
+        const int P = epi.pair_stride();
+        float u[32];
+#pragma unroll 1
+        for (int c0 = 0; c0 < P && c0 + P < BN + 1; c0 += 32) {
+          tmem_ld32(trow + c0, v);
+          tmem_ld32(trow + c0 + P, u);
+          epi.pair(batch, row, m0 + row, c0, v, u);
+        }
+      } else if constexpr (Epi::kTile) {
         // the operand ring is idle once `done` has fired: reuse it for the fp32 tile
         float* tile = reinterpret_cast<float*>(smem);
 #pragma unroll 1

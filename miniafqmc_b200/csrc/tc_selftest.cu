@@ -10,7 +10,7 @@
 namespace {
 
 struct EpiStoreF32 {
-  static constexpr bool kTile = false;
+  static constexpr bool kTile = false, kPair = false;
   float* C;
   int M, N;
   long long sC;

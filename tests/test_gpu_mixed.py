@@ -97,3 +97,25 @@ def test_mixed_trajectory_C1():
     assert max(dE) / abs(ed) < 1e-4
     d.close()
     m.close()
+
+
+def test_cholqr2_ortho_matches_householder_up_to_signs():
+    """The mixed form re-orthogonalises with CholeskyQR2: same column space as the FP64
+    form's LAPACK-convention Householder QR, columns equal up to +-1, so the density
+    matrix is identical and overlaps agree in magnitude."""
+    s = system("C1", complex_trial=True, complex_chol=True, nchol=96, seed=5)
+    nw = 8
+    d, m = pair(s, nw, perturbed(s, nw, amp=0.3))
+    for e in (d, m):
+        e.orthogonalize()
+        e.calculate_mixed_density_matrix()
+    Wd_, Wm = d.get_walkers()[0], m.get_walkers()[0]
+    for w in range(nw):
+        for sp in range(2):
+            M = Wm[w, sp].conj().T @ Wd_[w, sp]
+            assert np.max(np.abs(np.abs(M) - np.eye(s.n))) < 1e-11
+    assert rel(m.copy_out("Gc"), d.copy_out("Gc")) < 1e-11
+    od, om = d.get_walker_data()[:, 2:4], m.get_walker_data()[:, 2:4]
+    assert rel(np.abs(om), np.abs(od)) < 1e-11
+    d.close()
+    m.close()
