@@ -46,15 +46,20 @@ typedef enum {
 
 typedef enum {
   AFQ_ENERGY_VAKBL = 0,     /* eloc = 1/2 Gc.(Vakbl Gc) + Gc.haj (energy.hpp:66-102)     */
-  AFQ_ENERGY_CHOLESKY = 1   /* same energy from the half-rotated Cholesky factors        */
+  AFQ_ENERGY_CHOLESKY = 1,  /* same energy from the half-rotated Cholesky factors        */
+  AFQ_ENERGY_CV = 2         /* Cholesky energy with the exchange term estimated by the
+                               learned control variate (afq_cv_configure); unbiased     */
 } afq_energy_mode;
 
 typedef enum {
   AFQ_BUF_GC = 0, AFQ_BUF_VBIAS = 1, AFQ_BUF_X = 2, AFQ_BUF_VHS = 3, AFQ_BUF_HYBRIDW = 4,
   AFQ_BUF_XRAW = 5,         /* real normals [nchol][nwalk] (double)                      */
   AFQ_BUF_INFO = 6,         /* int32 [nwalk][2], nonzero = singular overlap matrix      */
-  AFQ_BUF_ENERGY_PARTS = 7  /* double [nwalk][3] = (E1, EJ, EK) of the last Cholesky
+  AFQ_BUF_ENERGY_PARTS = 7, /* double [nwalk][3] = (E1, EJ, EK) of the last Cholesky
                                energy evaluation                                         */
+  AFQ_BUF_CV_PRED = 8       /* double [nwalk] surrogate exchange energy of every walker
+                               from the last AFQ_ENERGY_CV measurement (0 before the
+                               estimator is active)                                      */
 } afq_buffer;
 
 typedef struct {
@@ -145,6 +150,37 @@ afq_status afq_energy_sums(afq_handle* h, int mode, double* sums);
 afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int northo);
 
 afq_status afq_synchronize(afq_handle* h);
+
+/* Learned control variate for the exchange energy (no reference counterpart).  A
+ * 36 -> hidden -> hidden -> 1 GELU network (BF16 weights, FP32 Adam at rate lr) predicts
+ * each walker's exchange energy from the Coulomb vector's fixed random projection (32),
+ * E_J, E_1, log|overlap| and its phase.  AFQ_ENERGY_CV evaluates the exact exchange on
+ * every walker until train_walker_steps exact samples have been gathered, then on a
+ * seeded random 1/subset_den of the walkers per measurement, correcting the surrogate
+ * with a Horvitz-Thompson term so the weighted energy stays unbiased; the network keeps
+ * training online on the exact samples.  Call after afq_set_hamiltonian with Lhalf. */
+afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
+                            long long train_walker_steps, int subset_den);
+/* stats[5] = exact samples so far, subset size of the last measurement, last training
+ * loss (normalised units), estimator active (0/1), measurements. */
+afq_status afq_cv_stats(afq_handle* h, double* stats);
+
+/* The surrogate network on its own (used by the control variate; exposed for testing
+ * and for callers that train it offline).  Parameters are one flat fp32 vector:
+ * W1[hidden][nin], b1[hidden], W2[hidden][hidden], b2[hidden], w3[hidden], b3.
+ * Host arrays: x[B][nin], t[B], y[B]; B <= capacity.  The loss is
+ * L = 1/(2B) sum_b (y_b - t_b)^2. */
+typedef struct afq_mlp afq_mlp;
+afq_status afq_mlp_create(int nin, int hidden, int capacity, uint64_t seed, afq_mlp** out);
+void afq_mlp_destroy(afq_mlp* m);
+long long afq_mlp_num_params(const afq_mlp* m);
+afq_status afq_mlp_set_params(afq_mlp* m, const float* params);
+afq_status afq_mlp_get_params(afq_mlp* m, float* params);
+afq_status afq_mlp_forward(afq_mlp* m, int B, const float* x, float* y);
+afq_status afq_mlp_gradient(afq_mlp* m, int B, const float* x, const float* t, float* grad,
+                            float* loss);
+afq_status afq_mlp_train(afq_mlp* m, int B, const float* x, const float* t, int iters, float lr,
+                         float* loss);
 
 /* Stage timers, the counterpart of the reference's NewTimer stages
  * (miniafqmc_base.cpp:50-77): with profiling on, every op-by-op call records CUDA events

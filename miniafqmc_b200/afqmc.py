@@ -18,9 +18,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafqmc_b200.so")
 
 AFQ_PREC_FP64, AFQ_PREC_MIXED = 0, 1
-AFQ_ENERGY_VAKBL, AFQ_ENERGY_CHOLESKY = 0, 1
+AFQ_ENERGY_VAKBL, AFQ_ENERGY_CHOLESKY, AFQ_ENERGY_CV = 0, 1, 2
 BUFFERS = {"Gc": 0, "vbias": 1, "X": 2, "vHS": 3, "hybridW": 4, "xraw": 5, "info": 6,
-           "energy_parts": 7}
+           "energy_parts": 7, "cv_pred": 8}
 STATUS = {0: "AFQ_OK", 1: "AFQ_ERR_ARG", 2: "AFQ_ERR_STATE", 3: "AFQ_ERR_CUDA",
           4: "AFQ_ERR_OOM", 5: "AFQ_ERR_UNSUPPORTED", 6: "AFQ_ERR_SINGULAR"}
 
@@ -31,7 +31,9 @@ EXPORTS = [
     "afq_update_weights", "afq_update_weights_partial", "afq_get_eshift", "afq_set_eshift",
     "afq_orthogonalize", "afq_energy", "afq_energy_sums", "afq_substep", "afq_synchronize",
     "afq_copy_out", "afq_set_walker_offset", "afq_profile", "afq_stage_times", "afq_get_stream",
-    "afq_selftest_tc_gemm", "afq_exchange_energy_noalloc",
+    "afq_selftest_tc_gemm", "afq_exchange_energy_noalloc", "afq_cv_configure", "afq_cv_stats",
+    "afq_mlp_create", "afq_mlp_destroy", "afq_mlp_num_params", "afq_mlp_set_params",
+    "afq_mlp_get_params", "afq_mlp_forward", "afq_mlp_gradient", "afq_mlp_train",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -84,6 +86,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_get_stream": ([P, P], I),
         "afq_selftest_tc_gemm": ([I, I, I, I, I, I, P, P, P, P], I),
         "afq_exchange_energy_noalloc": ([P, P, I, I, I, I, P, P], I),
+        "afq_cv_configure": ([P, I, D, U64, ctypes.c_longlong, I], I),
+        "afq_cv_stats": ([P, P], I),
+        "afq_mlp_create": ([I, I, I, U64, P], I), "afq_mlp_destroy": ([P], None),
+        "afq_mlp_num_params": ([P], ctypes.c_longlong), "afq_mlp_set_params": ([P, P], I),
+        "afq_mlp_get_params": ([P, P], I), "afq_mlp_forward": ([P, I, P, P], I),
+        "afq_mlp_gradient": ([P, I, P, P, P, P], I),
+        "afq_mlp_train": ([P, I, P, P, I, ctypes.c_float, P], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -177,7 +186,8 @@ class AfqmcSys:
         shapes = {"Gc": ((2 * n * N, nw), np.complex128), "vbias": ((nc, nw), np.complex128),
                   "X": ((nc, nw), np.complex128), "vHS": ((N * N, nw), np.complex128),
                   "hybridW": ((nw,), np.complex128), "xraw": ((nc, nw), np.float64),
-                  "info": ((nw, 2), np.int32), "energy_parts": ((nw, 3), np.float64)}
+                  "info": ((nw, 2), np.int32), "energy_parts": ((nw, 3), np.float64),
+                  "cv_pred": ((nw,), np.float64)}
         shape, dt = shapes[which]
         out = np.empty(shape, dt)
         self._check(self.lib.afq_copy_out(self.h, BUFFERS[which], _p(out)))
@@ -245,7 +255,19 @@ class AfqmcSys:
     def _mode(self, mode: str) -> int:
         if mode == "auto":
             mode = "chol" if self.has_chol else "vakbl"
-        return AFQ_ENERGY_VAKBL if mode == "vakbl" else AFQ_ENERGY_CHOLESKY
+        return {"vakbl": AFQ_ENERGY_VAKBL, "chol": AFQ_ENERGY_CHOLESKY, "cv": AFQ_ENERGY_CV}[mode]
+
+    def cv_configure(self, hidden: int = 256, lr: float = 1e-3, seed: int = 12345,
+                     train_walker_steps: int = 2000, subset_den: int = 8):
+        """Learned control variate for the exchange energy (used by mode "cv")."""
+        self._check(self.lib.afq_cv_configure(self.h, hidden, lr, seed, train_walker_steps,
+                                              subset_den))
+
+    def cv_stats(self) -> dict:
+        v = np.zeros(5)
+        self._check(self.lib.afq_cv_stats(self.h, _p(v)))
+        return {"samples": int(v[0]), "subset": int(v[1]), "loss": float(v[2]),
+                "active": bool(v[3]), "measurements": int(v[4])}
 
     def substep(self, seed: int, step_tot: int, northo: int, graph: bool = True):
         """One substep of the driver loop (miniafqmc_base.cpp:251-337)."""
@@ -281,3 +303,63 @@ class AfqmcSys:
         v = ctypes.c_void_p()
         self._check(self.lib.afq_get_stream(self.h, ctypes.byref(v)))
         return v.value or 0
+
+
+class Mlp:
+    """The control variate's surrogate network on its own (afq_mlp_* entry points)."""
+
+    def __init__(self, nin: int = 36, hidden: int = 256, capacity: int = 4096, seed: int = 1):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        st = self.lib.afq_mlp_create(nin, hidden, capacity, seed, ctypes.byref(h))
+        if st != 0:
+            raise AfqmcError(st, "afq_mlp_create failed")
+        self.h, self.nin, self.hidden = h, nin, hidden
+        self.nparams = int(self.lib.afq_mlp_num_params(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.afq_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st):
+        if st != 0:
+            raise AfqmcError(st, "mlp call failed")
+
+    def get_params(self) -> np.ndarray:
+        p = np.empty(self.nparams, np.float32)
+        self._chk(self.lib.afq_mlp_get_params(self.h, _p(p)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        self._chk(self.lib.afq_mlp_set_params(self.h, _p(p)))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty(x.shape[0], np.float32)
+        self._chk(self.lib.afq_mlp_forward(self.h, x.shape[0], _p(x), _p(y)))
+        return y
+
+    def gradient(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.empty(self.nparams, np.float32)
+        loss = ctypes.c_float()
+        self._chk(self.lib.afq_mlp_gradient(self.h, x.shape[0], _p(x), _p(t), _p(g),
+                                            ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, x: np.ndarray, t: np.ndarray, iters: int, lr: float = 1e-3) -> float:
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = ctypes.c_float()
+        self._chk(self.lib.afq_mlp_train(self.h, x.shape[0], _p(x), _p(t), iters, lr,
+                                         ctypes.byref(loss)))
+        return loss.value

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/afqmc_b200.h"
+#include "afq_cv.h"
 #include "afq_kernels.h"
 #include "afq_mixed.h"
 #include "zgemm_fp64.cuh"
@@ -48,6 +49,8 @@ struct afq_handle {
   double* parts = nullptr;
 
   afq::MixedState* mixed = nullptr;
+  afq::CvState* cv = nullptr;
+  afq::CvConfig cv_cfg;
 
   cudaGraphExec_t g_plain = nullptr, g_ortho = nullptr;
   long long g_plain_launches[AFQ_NSTAGES] = {0}, g_ortho_launches[AFQ_NSTAGES] = {0};
@@ -451,6 +454,7 @@ void afq_destroy(afq_handle* h) {
     cudaEventDestroy(r.b);
   }
   if (h->mixed) afq::mixed_destroy(h->mixed);
+  if (h->cv) afq::cv_destroy(h->cv);
   if (h->st) cudaStreamSynchronize(h->st);
   for (void* p : h->allocs)
     if (p) cudaFree(p);
@@ -684,10 +688,54 @@ afq_status afq_orthogonalize(afq_handle* h) {
   return AFQ_OK;
 }
 
+// Control-variate measurement: exact E_1 and E_J for every walker, surrogate + exact
+// exchange on a subset (cv_energy.cu).
+afq_status energy_cv(afq_handle* h, double* sums) {
+  if (!h->Lh) return fail(h, AFQ_ERR_STATE, "no Lhalf loaded");
+  if (!h->cv) {
+    cudaError_t e = afq::cv_create(h->cv_cfg, h->nw, h->nc, h->NAK, &h->cv, h->st);
+    if (e != cudaSuccess) return fail(h, AFQ_ERR_CUDA, "control variate set-up failed");
+  }
+  afq::CvInputs in;
+  in.Gc = h->Gc;
+  in.haj = h->haj;
+  in.cvec = h->cvec;
+  in.Wd = h->Wd;
+  in.Kpart = h->Kpart;
+  in.nblk = h->nblk;
+  in.exact_exchange = [h](const z_t* gsub, int m, z_t* kp) -> cudaError_t {
+    if (h->mixed) return afq::mixed_exchange(h->mixed, gsub, m, kp, h->nblk, h->st);
+    int nb = 0;
+    return afq::launch_exchange(h->Lh, gsub, h->N, h->n, h->nc, m, kp, &nb, h->st);
+  };
+  cudaError_t e = staged(h, AFQ_STAGE_ENERGY, 0, [&]() -> cudaError_t {
+    cudaError_t r;
+    if (h->mixed) {
+      r = afq::mixed_coulomb(h->mixed, h->Gc, h->cvec, h->st);
+    } else {
+      const int nak = (int)h->NAK;
+      ZGemmDesc g{h->nc, h->nw, nak, h->Lh, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+      EpiStore ep{h->cvec, h->nw, 0, zmk(0, 0), 0};
+      r = zgemm_launch<true, true>(g, 1, ep, h->st);
+    }
+    if (r != cudaSuccess) return r;
+    return afq::cv_energy(h->cv, in, sums, h->st);
+  });
+  if (e != cudaSuccess) return fail(h, AFQ_ERR_CUDA, std::string("cv energy: ") + cudaGetErrorString(e));
+  double st5[5];
+  afq::cv_stats(h->cv, st5);
+  // coulomb (2 or 3), features, normalise, forward, gather, exchange (1-2), reduce, mark,
+  // assemble, append, and 5 kernels per training iteration
+  h->stage_launches[AFQ_STAGE_ENERGY] +=
+      12 + 5LL * (st5[3] > 0 ? h->cv_cfg.iters_online : h->cv_cfg.iters_warm);
+  return AFQ_OK;
+}
+
 afq_status afq_energy_sums(afq_handle* h, int mode, double* sums) {
   afq_status s = need_ready(h);
   if (s != AFQ_OK) return s;
   if (!sums) return fail(h, AFQ_ERR_ARG, "null sums");
+  if (mode == AFQ_ENERGY_CV) return energy_cv(h, sums);
   if (mode == AFQ_ENERGY_VAKBL && !h->have_vakbl) return fail(h, AFQ_ERR_STATE, "no Vakbl loaded");
   if (mode == AFQ_ENERGY_CHOLESKY && !h->Lh) return fail(h, AFQ_ERR_STATE, "no Lhalf loaded");
   if (mode != AFQ_ENERGY_VAKBL && mode != AFQ_ENERGY_CHOLESKY) return fail(h, AFQ_ERR_ARG, "mode");
@@ -738,6 +786,33 @@ afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int nort
   AFQ_CUDA(h, cudaGraphLaunch(*slot, h->st));
   for (int i = 0; i < AFQ_NSTAGES; i++) h->stage_launches[i] += counts[i];
   h->host_step = step_tot + 1;
+  return AFQ_OK;
+}
+
+afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
+                            long long train_walker_steps, int subset_den) {
+  if (!h || hidden <= 0 || hidden % 32 || hidden > 1024 || !(lr > 0.0) || subset_den < 1 ||
+      train_walker_steps < 0)
+    return AFQ_ERR_ARG;
+  if (h->cv) {
+    afq::cv_destroy(h->cv);
+    h->cv = nullptr;
+  }
+  h->cv_cfg.hidden = hidden;
+  h->cv_cfg.lr = (float)lr;
+  h->cv_cfg.seed = seed;
+  h->cv_cfg.train_walker_steps = train_walker_steps;
+  h->cv_cfg.subset_den = subset_den;
+  return AFQ_OK;
+}
+
+afq_status afq_cv_stats(afq_handle* h, double* stats) {
+  if (!h || !stats) return AFQ_ERR_ARG;
+  if (!h->cv) {
+    for (int i = 0; i < 5; i++) stats[i] = 0.0;
+    return AFQ_OK;
+  }
+  afq::cv_stats(h->cv, stats);
   return AFQ_OK;
 }
 
@@ -813,6 +888,13 @@ afq_status afq_copy_out(afq_handle* h, int which, void* host) {
     case AFQ_BUF_XRAW: AFQ_CUDA(h, d2h(host, h->xraw, sizeof(double) * nc * nw)); break;
     case AFQ_BUF_INFO: AFQ_CUDA(h, d2h(host, h->info, sizeof(int) * nw * 2)); break;
     case AFQ_BUF_ENERGY_PARTS: AFQ_CUDA(h, d2h(host, h->parts, sizeof(double) * nw * 3)); break;
+    case AFQ_BUF_CV_PRED:
+      if (!h->cv) {
+        for (size_t w = 0; w < nw; w++) static_cast<double*>(host)[w] = 0.0;
+        break;
+      }
+      AFQ_CUDA(h, afq::cv_predictions(h->cv, static_cast<double*>(host), h->st));
+      break;
     default: return fail(h, AFQ_ERR_ARG, "unknown buffer");
   }
   return AFQ_OK;

@@ -1,0 +1,60 @@
+// Learned control variate for the exchange energy (internal interface).
+#pragma once
+#include <functional>
+#include "afq_common.cuh"
+
+namespace afq {
+
+struct Mlp;
+cudaError_t mlp_create(int nin, int H, int cap, unsigned long long seed, Mlp** out,
+                       cudaStream_t st);
+void mlp_destroy(Mlp* m);
+long long mlp_nparams(const Mlp* m);
+int mlp_capacity(const Mlp* m);
+float* mlp_x(Mlp* m);
+float* mlp_t(Mlp* m);
+float* mlp_y(Mlp* m);
+cudaError_t mlp_set_params(Mlp* m, const float* host, cudaStream_t st);
+cudaError_t mlp_get_params(Mlp* m, float* host, cudaStream_t st);
+cudaError_t mlp_forward(Mlp* m, const float* x, int B, float* y, bool keep, cudaStream_t st);
+cudaError_t mlp_gradient(Mlp* m, const float* x, const float* t, int B, cudaStream_t st);
+cudaError_t mlp_train(Mlp* m, const float* x, const float* t, int B, int iters, float lr,
+                      float* last_loss, cudaStream_t st);
+
+struct CvConfig {
+  int hidden = 256;
+  float lr = 1e-3f;
+  unsigned long long seed = 12345;
+  long long train_walker_steps = 2000;   // exact samples gathered before the estimator
+  int subset_den = 8;                     // exact exchange on nw / subset_den walkers
+  int iters_warm = 200, iters_online = 20;
+};
+
+struct CvState;
+
+// Device inputs of one measurement.  exact_exchange(Gc_sub, m, Kpart) must write the
+// exchange partial sums [m][2][nblk] of the m walkers whose compact density matrices
+// are packed in Gc_sub.
+struct CvInputs {
+  const z_t* Gc;        // [nw][NAK]
+  const z_t* haj;       // [NAK]
+  const z_t* cvec;      // [nchol][nw], Coulomb vector of every walker
+  z_t* Wd;              // [nw][8] walker data (overlaps in 2, 3; eloc written to 0)
+  z_t* Kpart;           // [nw][2][nblk] scratch for the exact exchange
+  int nblk;
+  std::function<cudaError_t(const z_t*, int, z_t*)> exact_exchange;
+};
+
+cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvState** out,
+                      cudaStream_t st);
+void cv_destroy(CvState* s);
+// Runs one measurement; writes W_data[:,0] and the two weighted sums (sum Re(e) Re(w),
+// sum Re(w)) of the estimator.  Synchronises the stream.
+cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t st);
+// stats: [exact samples seen, subset size of the last measurement, last training loss,
+//         estimator active (0/1), measurements]
+void cv_stats(const CvState* s, double* stats);
+// Surrogate exchange energy of every walker from the last measurement (host doubles).
+cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st);
+
+}  // namespace afq

@@ -28,6 +28,9 @@ cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t* vHS, cudaStream_t st);
 cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t* vHS, cudaStream_t st);
 cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpart, int nblk,
                               cudaStream_t st);
+cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t st);
+cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
+                           cudaStream_t st);
 // Kernels one call of a stage issues (afq_stage numbering), for the launch counters.
 int mixed_launches(const MixedState* m, int stage);
 // Cholesky-vector blocks of the exchange partial sums (Kpart[nw][2][nblk]).

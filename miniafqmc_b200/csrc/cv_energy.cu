@@ -1,0 +1,370 @@
+// Control-variate energy estimator with the learned exchange surrogate.
+//
+// Per measurement (after the mixed density matrix):
+//   features of every walker from quantities the step already has: a fixed Gaussian
+//     projection (32 rows) of the Coulomb vector c_w = Lh Gc_w, E_J = 1/2 c_w.c_w,
+//     E_1 = Gc_w.haj, log|ovlp_a ovlp_b| and its phase;
+//   surrogate f_w = MLP(features) on every walker;
+//   exact exchange E_K on a seeded random subset S of m = ceil(nw / subset_den) walkers
+//     (all walkers while the network is being warmed up);
+//   sum_w w_w eloc_w = sum_w w_w (E1 + EJ)_w - [sum_w w_w f_w + (nw/m) sum_{w in S} w_w (EK_w - f_w)]
+//     which is unbiased for the exact weighted energy (Horvitz-Thompson correction of the
+//     surrogate on a without-replacement sample with inclusion probability m/nw);
+//   W_data[:,0] holds exact energies on S and E1 + EJ - f elsewhere;
+//   the exact (features, E_K) pairs of S enter a replay buffer and the network takes a
+//     few Adam steps on it -- after the estimate, so the estimate never sees its own data.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "afq_cv.h"
+
+namespace afq {
+
+constexpr int CV_NIN = 36, CV_NPROJ = 32;
+
+struct CvState {
+  CvConfig cfg;
+  int nw = 0, nc = 0;
+  long long nak = 0;
+  Mlp* mlp = nullptr;
+  float *R = nullptr, *feats = nullptr, *featn = nullptr, *fpred = nullptr;
+  float *d_mu = nullptr, *d_sd = nullptr, *buf_x = nullptr, *buf_t = nullptr;
+  double *e1ej = nullptr, *ek_sub = nullptr, *d_sums = nullptr;
+  int *d_sub = nullptr, *member = nullptr, *h_sub = nullptr;
+  z_t* Gc_sub = nullptr;
+  int sub_cap = 0, cap = 0, buf_n = 0, buf_head = 0;
+  float mu_t = 0.0f, sd_t = 1.0f;
+  bool have_norm = false, active = false;
+  long long seen = 0, meas = 0;
+  int last_m = 0;
+  float last_loss = 0.0f;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+template <class T>
+cudaError_t cmal(CvState* s, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * (n ? n : 1));
+  if (e == cudaSuccess) {
+    s->allocs.push_back(q);
+    *p = static_cast<T*>(q);
+  }
+  return e;
+}
+int gridn(long long n, int t) { return (int)std::min<long long>((n + t - 1) / t, 148LL * 32); }
+
+__global__ void cv_proj_init_kernel(float* R, long long count, int twonc,
+                                    unsigned long long seed) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x) {
+    double a, b;
+    normal_pair(seed ^ 0x9e3779b97f4a7c15ull, 7, (unsigned long long)e, &a, &b);
+    R[e] = (float)(a / sqrt((double)twonc));
+  }
+}
+
+// One CTA (256 threads) per walker.
+__global__ void __launch_bounds__(256)
+cv_features_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, long long nak,
+                   const z_t* __restrict__ cvec, int nc, int nw, const z_t* __restrict__ Wd,
+                   const float* __restrict__ R, float* __restrict__ feats,
+                   double* __restrict__ e1ej) {
+  __shared__ z_t red[8];
+  __shared__ float proj[CV_NPROJ];
+  const int w = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  z_t e1 = zmk(0, 0), ej = zmk(0, 0);
+  for (long long i = tid; i < nak; i += blockDim.x) zfma(e1, Gc[(long long)w * nak + i], haj[i]);
+  for (int c = tid; c < nc; c += blockDim.x) {
+    z_t v = cvec[(long long)c * nw + w];
+    zfma(ej, v, v);
+  }
+  e1 = block_zsum(e1, red);
+  ej = block_zsum(ej, red);
+  for (int q = warp; q < CV_NPROJ; q += 8) {
+    const float* Rq = R + (long long)q * 2 * nc;
+    float s = 0.0f;
+    for (int c = lane; c < nc; c += 32) {
+      z_t v = cvec[(long long)c * nw + w];
+      s = fmaf(Rq[c], (float)v.x, s);
+      s = fmaf(Rq[nc + c], (float)v.y, s);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) proj[q] = s;
+  }
+  __syncthreads();
+  if (tid < CV_NPROJ) feats[(long long)w * CV_NIN + tid] = proj[tid];
+  if (tid == 0) {
+    const z_t ov = zmul(Wd[(long long)w * 8 + 2], Wd[(long long)w * 8 + 3]);
+    float* f = feats + (long long)w * CV_NIN;
+    f[32] = (float)(0.5 * ej.x);
+    f[33] = (float)e1.x;
+    f[34] = (float)log(fmax(hypot(ov.x, ov.y), 1e-300));
+    f[35] = (float)atan2(ov.y, ov.x);
+    double* o = e1ej + (long long)w * 4;
+    o[0] = e1.x; o[1] = e1.y; o[2] = 0.5 * ej.x; o[3] = 0.5 * ej.y;
+  }
+}
+
+__global__ void cv_normalize_kernel(const float* __restrict__ f, long long count,
+                                    const float* __restrict__ mu, const float* __restrict__ sd,
+                                    float* __restrict__ out) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(e % CV_NIN);
+    out[e] = (f[e] - mu[q]) / sd[q];
+  }
+}
+
+__global__ void cv_gather_kernel(const z_t* __restrict__ Gc, long long nak,
+                                 const int* __restrict__ sub, int m, z_t* __restrict__ out) {
+  const long long tot = (long long)m * nak;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e / nak, q = e % nak;
+    out[e] = Gc[(long long)sub[i] * nak + q];
+  }
+}
+
+__global__ void __launch_bounds__(128)
+cv_ek_kernel(const z_t* __restrict__ Kpart, int nblk, double* __restrict__ ek) {
+  __shared__ z_t red[4];
+  const int i = blockIdx.x;
+  z_t s = zmk(0, 0);
+  for (int q = threadIdx.x; q < 2 * nblk; q += blockDim.x)
+    s = zadd(s, Kpart[(long long)i * 2 * nblk + q]);
+  s = block_zsum(s, red);
+  if (threadIdx.x == 0) {
+    ek[2 * i] = 0.5 * s.x;
+    ek[2 * i + 1] = 0.5 * s.y;
+  }
+}
+
+__global__ void cv_mark_kernel(const int* __restrict__ sub, int m, int* __restrict__ member) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m; i += gridDim.x * blockDim.x)
+    member[sub[i]] = i;
+}
+
+// Replay buffer append: (normalised features, normalised exact E_K) of the subset.
+__global__ void cv_append_kernel(const float* __restrict__ featn, const int* __restrict__ sub,
+                                 int m, const double* __restrict__ ek, float mu_t, float sd_t,
+                                 float* __restrict__ bx, float* __restrict__ bt, int head,
+                                 int cap) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m * CV_NIN;
+       e += gridDim.x * blockDim.x) {
+    const int i = e / CV_NIN, q = e % CV_NIN, slot = (head + i) % cap;
+    bx[(long long)slot * CV_NIN + q] = featn[(long long)sub[i] * CV_NIN + q];
+    if (q == 0) bt[slot] = (float)((ek[2 * i] - mu_t) / sd_t);
+  }
+}
+
+// Assembles W_data[:,0] and the weighted sums of the estimator (one CTA, fixed order).
+__global__ void __launch_bounds__(1024)
+cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
+                   const double* __restrict__ e1ej, const double* __restrict__ ek,
+                   const float* __restrict__ fpred, float mu_t, float sd_t, z_t* __restrict__ Wd,
+                   double* __restrict__ sums) {
+  __shared__ z_t red[32];
+  double A = 0.0, Bc = 0.0, Wt = 0.0;
+  for (int w = threadIdx.x; w < nw; w += blockDim.x) {
+    const double* p = e1ej + (long long)w * 4;
+    const int i = member[w];
+    const double f = active ? (double)fpred[w] * sd_t + mu_t : 0.0;
+    z_t e;
+    if (i >= 0) e = zmk(p[0] + p[2] - ek[2 * i], p[1] + p[3] - ek[2 * i + 1]);
+    else e = zmk(p[0] + p[2] - f, p[1] + p[3]);
+    Wd[(long long)w * 8] = e;
+    const double om = Wd[(long long)w * 8 + 1].x;
+    if (active) {
+      A += om * (p[0] + p[2] - f);
+      if (i >= 0) Bc += om * (ek[2 * i] - f);
+    } else {
+      A += om * e.x;
+    }
+    Wt += om;
+  }
+  z_t ab = block_zsum(zmk(A, Bc), red);
+  z_t wt = block_zsum(zmk(Wt, 0.0), red);
+  if (threadIdx.x == 0) {
+    sums[0] = active ? ab.x - ((double)nw / (double)m) * ab.y : ab.x;
+    sums[1] = wt.x;
+  }
+}
+
+// Seeded simple random sample of m walkers out of nw (partial Fisher-Yates on Philox).
+void sample_subset(unsigned long long seed, long long meas, int nw, int m, int* out) {
+  std::vector<int> idx(nw);
+  for (int i = 0; i < nw; i++) idx[i] = i;
+  for (int i = 0; i < m; i++) {
+    uint32_t c[4] = {(uint32_t)i, 0x53554253u, (uint32_t)meas, (uint32_t)(meas >> 32)};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t r = ((uint64_t)c[0] << 32) | c[1];
+    const int j = i + (int)(r % (uint64_t)(nw - i));
+    std::swap(idx[i], idx[j]);
+  }
+  std::sort(idx.begin(), idx.begin() + m);
+  for (int i = 0; i < m; i++) out[i] = idx[i];
+}
+
+}  // namespace
+
+cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvState** out,
+                      cudaStream_t st) {
+  *out = nullptr;
+  if (cfg.subset_den < 1 || cfg.hidden % 32 || cfg.hidden > 1024) return cudaErrorInvalidValue;
+  CvState* s = new CvState();
+  s->cfg = cfg;
+  s->nw = nw; s->nc = nchol; s->nak = nak;
+  s->sub_cap = (nw + cfg.subset_den - 1) / cfg.subset_den;
+  s->cap = std::max(4096, nw);
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  A(cmal(s, &s->R, (size_t)CV_NPROJ * 2 * nchol));
+  A(cmal(s, &s->feats, (size_t)nw * CV_NIN));
+  A(cmal(s, &s->featn, (size_t)nw * CV_NIN));
+  A(cmal(s, &s->fpred, nw));
+  A(cmal(s, &s->d_mu, CV_NIN));
+  A(cmal(s, &s->d_sd, CV_NIN));
+  A(cmal(s, &s->buf_x, (size_t)s->cap * CV_NIN));
+  A(cmal(s, &s->buf_t, s->cap));
+  A(cmal(s, &s->e1ej, (size_t)nw * 4));
+  A(cmal(s, &s->ek_sub, (size_t)nw * 2));
+  A(cmal(s, &s->d_sums, 2));
+  A(cmal(s, &s->d_sub, nw));
+  A(cmal(s, &s->member, nw));
+  A(cmal(s, &s->Gc_sub, (size_t)s->sub_cap * nak));
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
+  if (e == cudaSuccess) e = mlp_create(CV_NIN, cfg.hidden, s->cap, cfg.seed, &s->mlp, st);
+  if (e == cudaSuccess) {
+    cv_proj_init_kernel<<<gridn((long long)CV_NPROJ * 2 * nchol, 256), 256, 0, st>>>(
+        s->R, (long long)CV_NPROJ * 2 * nchol, 2 * nchol, cfg.seed);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    cv_destroy(s);
+    return e;
+  }
+  *out = s;
+  return cudaSuccess;
+}
+
+void cv_destroy(CvState* s) {
+  if (!s) return;
+  mlp_destroy(s->mlp);
+  if (s->h_sub) cudaFreeHost(s->h_sub);
+  for (void* p : s->allocs) cudaFree(p);
+  delete s;
+}
+
+void cv_stats(const CvState* s, double* o) {
+  o[0] = (double)s->seen;
+  o[1] = (double)s->last_m;
+  o[2] = (double)s->last_loss;
+  o[3] = s->active ? 1.0 : 0.0;
+  o[4] = (double)s->meas;
+}
+
+cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st) {
+  std::vector<float> f(s->nw, 0.0f);
+  if (s->active) {
+    cudaError_t e = cudaMemcpyAsync(f.data(), s->fpred, sizeof(float) * s->nw,
+                                    cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+  }
+  for (int w = 0; w < s->nw; w++) host[w] = s->active ? (double)f[w] * s->sd_t + s->mu_t : 0.0;
+  return cudaSuccess;
+}
+
+cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t st) {
+  const int nw = s->nw;
+  cudaError_t e;
+  s->meas++;
+  cv_features_kernel<<<nw, 256, 0, st>>>(in.Gc, in.haj, s->nak, in.cvec, s->nc, nw, in.Wd, s->R,
+                                         s->feats, s->e1ej);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  s->active = s->have_norm && s->seen >= s->cfg.train_walker_steps;
+  const int m = s->active ? s->sub_cap : nw;
+  if (s->active) {
+    sample_subset(s->cfg.seed, s->meas, nw, m, s->h_sub);
+  } else {
+    for (int i = 0; i < nw; i++) s->h_sub[i] = i;
+  }
+  s->last_m = m;
+  if ((e = cudaMemcpyAsync(s->d_sub, s->h_sub, sizeof(int) * m, cudaMemcpyHostToDevice, st)) !=
+      cudaSuccess)
+    return e;
+  if (s->have_norm) {
+    cv_normalize_kernel<<<gridn((long long)nw * CV_NIN, 256), 256, 0, st>>>(
+        s->feats, (long long)nw * CV_NIN, s->d_mu, s->d_sd, s->featn);
+    if ((e = mlp_forward(s->mlp, s->featn, nw, s->fpred, false, st)) != cudaSuccess) return e;
+  }
+  // exact exchange on the subset
+  const z_t* gsub = in.Gc;
+  if (s->active) {
+    cv_gather_kernel<<<gridn((long long)m * s->nak, 256), 256, 0, st>>>(in.Gc, s->nak, s->d_sub, m,
+                                                                        s->Gc_sub);
+    gsub = s->Gc_sub;
+  }
+  if ((e = in.exact_exchange(gsub, m, in.Kpart)) != cudaSuccess) return e;
+  cv_ek_kernel<<<m, 128, 0, st>>>(in.Kpart, in.nblk, s->ek_sub);
+  if ((e = cudaMemsetAsync(s->member, 0xFF, sizeof(int) * nw, st)) != cudaSuccess) return e;
+  cv_mark_kernel<<<gridn(m, 256), 256, 0, st>>>(s->d_sub, m, s->member);
+  cv_assemble_kernel<<<1, 1024, 0, st>>>(nw, m, s->active ? 1 : 0, s->member, s->e1ej, s->ek_sub,
+                                          s->fpred, s->mu_t, s->sd_t, in.Wd, s->d_sums);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = cudaMemcpyAsync(sums, s->d_sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return e;
+  // feature / target scales from the first (all-walker) measurement
+  if (!s->have_norm) {
+    std::vector<float> f((size_t)nw * CV_NIN);
+    std::vector<double> ek((size_t)nw * 2);
+    if ((e = cudaMemcpyAsync(f.data(), s->feats, sizeof(float) * f.size(), cudaMemcpyDeviceToHost,
+                             st)) != cudaSuccess)
+      return e;
+    if ((e = cudaMemcpyAsync(ek.data(), s->ek_sub, sizeof(double) * ek.size(),
+                             cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    float mu[CV_NIN], sd[CV_NIN];
+    for (int q = 0; q < CV_NIN; q++) {
+      double a = 0, b = 0;
+      for (int w = 0; w < nw; w++) a += f[(size_t)w * CV_NIN + q];
+      a /= nw;
+      for (int w = 0; w < nw; w++) b += (f[(size_t)w * CV_NIN + q] - a) * (f[(size_t)w * CV_NIN + q] - a);
+      mu[q] = (float)a;
+      sd[q] = (float)std::max(sqrt(b / nw), 1e-6);
+    }
+    double a = 0, b = 0;
+    for (int w = 0; w < nw; w++) a += ek[2 * w];
+    a /= nw;
+    for (int w = 0; w < nw; w++) b += (ek[2 * w] - a) * (ek[2 * w] - a);
+    s->mu_t = (float)a;
+    s->sd_t = (float)std::max(sqrt(b / nw), 1e-6);
+    if ((e = cudaMemcpyAsync(s->d_mu, mu, sizeof(mu), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return e;
+    if ((e = cudaMemcpyAsync(s->d_sd, sd, sizeof(sd), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return e;
+    cv_normalize_kernel<<<gridn((long long)nw * CV_NIN, 256), 256, 0, st>>>(
+        s->feats, (long long)nw * CV_NIN, s->d_mu, s->d_sd, s->featn);
+    s->have_norm = true;
+  }
+  // online training on the replay buffer
+  cv_append_kernel<<<gridn((long long)m * CV_NIN, 256), 256, 0, st>>>(
+      s->featn, s->d_sub, m, s->ek_sub, s->mu_t, s->sd_t, s->buf_x, s->buf_t, s->buf_head, s->cap);
+  s->buf_head = (s->buf_head + m) % s->cap;
+  s->buf_n = std::min(s->cap, s->buf_n + m);
+  s->seen += m;
+  const int iters = s->active ? s->cfg.iters_online : s->cfg.iters_warm;
+  if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, &s->last_loss, st)) !=
+      cudaSuccess)
+    return e;
+  return cudaStreamSynchronize(st);
+}
+
+}  // namespace afq

@@ -176,8 +176,10 @@ __global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N,
        e += (long long)gridDim.x * blockDim.x) {
     const long long w = e / NAK, q = e % NAK;
     const z_t g = Gc[e];
-    put2(Gb, w * 2 * NAK + 2 * q, (float)g.x, (float)-g.y);
-    put2(Gb, (nw + w) * 2 * NAK + 2 * q, (float)g.y, (float)g.x);
+    if (Gb.hi) {
+      put2(Gb, w * 2 * NAK + 2 * q, (float)g.x, (float)-g.y);
+      put2(Gb, (nw + w) * 2 * NAK + 2 * q, (float)g.y, (float)g.x);
+    }
     if (Gx.hi) {
       const long long s = q / ((long long)n * N), r = q % ((long long)n * N);
       const long long b = r / N, k = r % N;
@@ -636,18 +638,35 @@ cudaError_t mixed_vbias(MixedState* m, const z_t* Gc, z_t* vbias, cudaStream_t s
   return splitk_product(m, m->m_vbias, m->prec_vbias, vbias, st);
 }
 
-cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpart, int nblk,
-                              cudaStream_t st) {
+// Coulomb vector cvec[c][w] = sum_ak Lh[c][ak] Gc_w[ak] of every walker.
+cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t st) {
   if (!m->in.Lh) return cudaErrorInvalidValue;
   pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
-                                                                      m->Gx);
+                                                                      Op{});
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  if ((e = splitk_product(m, m->m_ej, m->prec_ej, cvec, st)) != cudaSuccess) return e;
+  return splitk_product(m, m->m_ej, m->prec_ej, cvec, st);
+}
+
+// Exchange partial sums Kpart[w][s][block] of the first nsub walkers packed in Gc.
+cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
+                           cudaStream_t st) {
+  if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
+  pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(Gc, nsub, m->n, m->N, Op{},
+                                                                     m->Gx);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   const int n = m->n;
-  tc::GemmShape g{m->nc * n, m->nw * 2 * n, 2 * m->N, 2, m->ex_Gn * n, m->ex_mtiles, true, true, 0};
-  EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, m->nw, nblk, Kpart};
+  tc::GemmShape g{m->nc * n, nsub * 2 * n, 2 * m->N, 2, m->ex_Gn * n, m->ex_mtiles, true, true, 0};
+  EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart};
   return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g, ep, m->err, st);
+}
+
+cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpart, int nblk,
+                              cudaStream_t st) {
+  cudaError_t e = mixed_coulomb(m, Gc, cvec, st);
+  if (e != cudaSuccess) return e;
+  return mixed_exchange(m, Gc, m->nw, Kpart, nblk, st);
 }
 
 }  // namespace afq

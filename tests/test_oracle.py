@@ -186,3 +186,30 @@ def test_trajectory_is_deterministic_and_threads_agree():
         res.append(o.get_walkers())
     np.testing.assert_array_equal(res[0][0], res[1][0])
     np.testing.assert_array_equal(res[0][1], res[1][1])
+
+
+def test_mlp_oracle_gradient_by_finite_differences():
+    """Pins the network oracle: analytic gradient vs central differences (float64,
+    unrounded weights)."""
+    from oracle import mlp as M
+    rng = np.random.default_rng(0)
+    nin, H, B = 5, 32, 7
+    P = M.layout(nin, H)["b3"][1]
+    p = rng.normal(scale=0.3, size=P)
+    x = rng.normal(size=(B, nin))
+    t = rng.normal(size=B)
+    g, _ = M.gradient(p, x, t, nin, H, round_weights=False)
+    loss = lambda q: 0.5 * np.mean((M.forward(q, x, nin, H, round_weights=False)[0] - t) ** 2)
+    for i in rng.choice(P, 40, replace=False):
+        e = np.zeros(P)
+        e[i] = 1e-6
+        fd = (loss(p + e) - loss(p - e)) / 2e-6
+        assert abs(fd - g[i]) < 1e-6 + 1e-5 * abs(g[i])
+
+
+def test_bf16_rounding_matches_torch():
+    import torch
+    from oracle import mlp as M
+    x = np.random.default_rng(1).normal(size=10000).astype(np.float32) * 100
+    ref = torch.from_numpy(x).bfloat16().float().numpy()
+    np.testing.assert_array_equal(M.bf16(x), ref)
