@@ -1,25 +1,33 @@
 """Walker-steps/s of the miniAFQMC walker hot path on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--config C4] [--precision fp64|mixed]
+                  [--config C4] [--form mixed-cv|mixed|fp64] [--no-fp64]
 
 A step is one substep of the driver loop (miniafqmc_base.cpp:251-337: mixed density
 matrix, vbias, sigma, vHS, propagation, overlaps, weights; orthogonalisation every
-`northo` substeps) plus, every `energy_every` substeps, the mixed density matrix and
-local energy (miniafqmc_base.cpp:341-345).  The default workload is the target system:
-NMO=384, 48+48 electrons, nchol=1536 Cholesky vectors (20% nonzero), 1024 walkers per
-GPU, synthetic (seeded) inputs.  Multi-GPU runs shard walkers (weak scaling): each
-rank holds its own 1024 walkers and the per-step Eshift sum is all-reduced.
+`northo` substeps) plus, every `energy_every` substeps, the mixed density matrix and the
+local energy (miniafqmc_base.cpp:341-345).  The workload is the target system: NMO=384,
+48+48 electrons, nchol=1536 Cholesky vectors (20% nonzero), 1024 walkers per GPU,
+synthetic seeded inputs.  Multi-GPU runs shard walkers (weak scaling): each rank holds
+its own 1024 walkers and the per-step Eshift sum and the energy sums are all-reduced.
+
+The headline form is mixed precision with the learned control variate (tensor-core
+contractions, FP64 LU/QR/weights, exact exchange on 1/8 of the walkers); at N=1 the plain
+FP64 form runs the same steps on the same auxiliary fields for the comparison the metric
+asks for: speed-up, |dE| between the two forms' mean energies, and energy error per
+wall-second sigma_E * sqrt(T) of each (sigma_E from the walker-population variance of
+the weighted mean at each measurement, combined over measurements).
 
 Rank 0 prints one JSON line.  `value` is whole-job walker-steps/s with the walker set
 resident in HBM; `e2e` is the same rate through the C ABI with host buffers (the normals
 of every step copied host->device, W_data copied back every step).  `--impl reference`
-times the FP64 CPU restatement of the reference (the oracle, with the reference's call
-granularity and Release flags) on the host cores, on a bounded sample of walkers.
+times the FP64 CPU restatement of the reference (the oracle: the reference's call
+granularity and GNU Release flags) on the host cores, on a bounded sample of walkers.
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -42,12 +50,14 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--config", default="C4")
-    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    p.add_argument("--energy-every", type=int, default=10)
+    p.add_argument("--form", default="mixed-cv", choices=["mixed-cv", "mixed", "fp64"])
+    p.add_argument("--energy-every", type=int, default=5)
     p.add_argument("--northo", type=int, default=5)
+    p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-walkers", type=int, default=0)
+    p.add_argument("--walkers", type=int, default=0, help="walkers per GPU (default: config)")
     return p.parse_args()
 
 
@@ -56,8 +66,8 @@ def workload(cfg, args, nw):
         "workload": (f"{args.config}: NMO={cfg.nmo}, {cfg.nel}+{cfg.nel} electrons, "
                      f"nchol={cfg.nchol} ({cfg.density:.0%} nonzero), {nw} walkers/GPU, "
                      f"dt={cfg.dt}, Taylor order {cfg.taylor_order}, ortho every {args.northo}, "
-                     f"energy every {args.energy_every} substeps (Cholesky form)"),
-        "precision": args.precision,
+                     f"energy every {args.energy_every} substeps"),
+        "form": args.form,
         "l2": "inputs larger than L2 (vHS, walkers, Spvn, SpvnT each > 126 MB); no flush",
         "seed": cfg.seed,
     }
@@ -103,6 +113,7 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
         def num(x):
             try:
                 return float(x)
@@ -111,8 +122,8 @@ class ClockSampler:
         sm = [num(r[0]) for r in self.rows if num(r[0]) is not None]
         mx = [num(r[1]) for r in self.rows if num(r[1]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if "Active" in r[3 + i]
-                          and "Not" not in r[3 + i]})
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if "Active" in r[3 + i] and "Not" not in r[3 + i]})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
                 "samples": len(self.rows)}
@@ -126,8 +137,8 @@ def measured_peaks():
 
 
 def fp64_peak_tflops(torch):
-    """The FP64 roofline denominator: cuBLAS DGEMM 8192^3 via torch.matmul, best of 5
-    (no FP64 figure is provided in MEASURED_PEAKS.json)."""
+    """FP64 roofline denominator: cuBLAS DGEMM 8192^3 via torch.matmul, best of 6
+    (MEASURED_PEAKS.json has no FP64 entry)."""
     a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
     b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
     best = 1e9
@@ -142,28 +153,47 @@ def fp64_peak_tflops(torch):
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def stage_flops(cfg, nw, stage, order=6):
-    """Algorithmic FLOPs (complex multiply-add = 8 FLOP) of one call of a stage."""
+def fp64_stage_flops(cfg, nw, stage, order=6):
+    """Algorithmic FLOPs of one call of an FP64 stage (complex multiply-add = 8 FLOP)."""
     N, n, nc = cfg.nmo, cfg.nel, cfg.nchol
-    d = cfg.density
-    if stage == "propagate":     # (order + 2) GEMMs of N x N x 2n per walker
+    if stage == "propagate":
         return 8.0 * nw * (order + 2) * N * N * 2 * n
-    if stage == "vbias":         # dense SpvnT: nchol x 2nN per walker
+    if stage == "vbias":
         return 8.0 * nw * nc * 2 * n * N
-    if stage == "vHS":           # real Spvn (nnz) x complex X
-        return 4.0 * nw * d * N * N * nc
+    if stage == "vHS":
+        return 4.0 * nw * cfg.density * N * N * nc
     if stage == "DM":
         return 8.0 * nw * 2 * (2 * n * n * N + n ** 3)
-    if stage == "energy":        # Coulomb + exchange per walker
+    if stage == "energy":
         return 8.0 * nw * (2 * n * N * nc + 2 * nc * n * n * N)
     return 0.0
+
+
+def mixed_propagate_bytes(cfg, nw, order=6):
+    """HBM bytes one mixed-form propagation stage must move with its operand layouts:
+    the FP64 walkers in and out, and per product the bf16 operands read once (hi, plus lo
+    for the split products), the fp32 Taylor sum read and written, and the next bf16
+    operand written (hi and lo)."""
+    N, n = cfg.nmo, cfg.nel
+    W64 = nw * N * 2 * n * 16            # FP64 walkers
+    F = nw * 4 * n * 2 * N * 2           # one bf16 part of a B operand
+    V = nw * N * 2 * N * 2               # one bf16 part of the V operand
+    S = nw * N * 2 * n * 8               # fp32 Taylor sum
+    split = {"P": True, "V1": True, "Vk": False}
+    tot = W64 + 2 * F                    # pack W
+    tot += 2 * F + S + 2 * F             # S = P W (split): B hi+lo in, S out, next B out
+    for k in range(1, order + 1):
+        sp = split["V1"] if k == 1 else split["Vk"]
+        tot += V * (2 if sp else 1) + F * (2 if sp else 1) + 2 * S + 2 * F
+    tot += 2 * F + W64                   # W = P S (split)
+    return float(tot)
 
 
 # --------------------------------------------------------------------------- CPU leg
 def cpu_rate(system, cfg, args, nwalk_sample, threads):
     """walker-steps/s of the oracle (reference-structured FP64 CPU path, Release flags)
-    on `nwalk_sample` walkers: 2 substeps + one energy evaluation, amortised like the
-    GPU run (one energy every energy_every substeps)."""
+    on `nwalk_sample` walkers: 2 substeps + one exact energy evaluation amortised over
+    energy_every substeps, OpenMP over walkers."""
     from oracle import oracle as O
     try:
         from threadpoolctl import threadpool_limits
@@ -180,20 +210,17 @@ def cpu_rate(system, cfg, args, nwalk_sample, threads):
     o.calculate_mixed_density_matrix()
     o.calculate_energy("chol")
     t2 = time.perf_counter()
-    if lim is not None:
-        lim.unregister() if hasattr(lim, "unregister") else None
+    del lim
     per_step = (t1 - t0) / ksub + (t2 - t1) / args.energy_every
     return nwalk_sample / per_step, {
-        "substep_s": (t1 - t0) / ksub, "energy_s": t2 - t1,
-        "sample": f"{nwalk_sample} walkers of the same system, {ksub} substeps + 1 energy "
+        "sample": f"{nwalk_sample} walkers of the same system, {ksub} substeps + 1 exact energy "
                   f"(amortised over {args.energy_every} substeps), OpenMP over walkers"}
 
 
 def run_reference(args):
     from miniafqmc_b200.synthetic import CONFIGS, make_system
     import dataclasses
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    if int(os.environ.get("RANK", "0")) != 0:
         return
     cfg = dataclasses.replace(CONFIGS[args.config], with_vakbl=False)
     s = make_system(cfg)
@@ -217,6 +244,71 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------- GPU leg
+class Form:
+    """One walker set in one numerical form, with its step loop."""
+
+    def __init__(self, system, cfg, args, form, device, comm, torch):
+        from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
+        self.cfg, self.args, self.form, self.comm = cfg, args, form, comm
+        prec = AFQ_PREC_FP64 if form == "fp64" else AFQ_PREC_MIXED
+        self.eng = AfqmcSys(system, cfg.nwalk, precision=prec, device=device, use_vakbl=False)
+        if comm is not None:
+            self.eng.set_walker_offset(comm.offset, comm.nwalk_global)
+        self.mode = "cv" if form == "mixed-cv" else "chol"
+        if self.mode == "cv":
+            self.eng.cv_configure(hidden=256, lr=1e-3, seed=cfg.seed, train_walker_steps=2000,
+                                  subset_den=8)
+        self.stream = torch.cuda.ExternalStream(self.eng.stream)
+        self.energies, self.sig2 = [], []
+
+    def measure(self, record=True):
+        from miniafqmc_b200 import driver
+        e = self.eng
+        e.calculate_mixed_density_matrix()
+        E = driver.energy(e, self.mode, self.comm)
+        if record:
+            Wd = e.get_walker_data()
+            w = Wd[:, 1].real
+            el = Wd[:, 0].real
+            self.energies.append(E)
+            self.sig2.append(float(np.sum(w * w * (el - E) ** 2) / np.sum(w) ** 2))
+        return E
+
+    def step(self, st, record=True, graph=True):
+        from miniafqmc_b200 import driver
+        driver.substep(self.eng, self.cfg.seed, st, self.args.northo, self.comm,
+                       graph=graph and self.comm is None)
+        if (st + 1) % self.args.energy_every == 0:
+            self.measure(record)
+
+
+def timed(form, steps, start, torch, dist, world, profile=False):
+    e = form.eng
+    e.synchronize()
+    e.stage_times(reset=True)
+    e.profile(profile)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(form.stream)
+    for st in range(start, start + steps):
+        form.step(st, graph=not profile)   # stage events need the op-by-op calls
+    e1.record(form.stream)
+    e.synchronize()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    e.profile(False)
+    ms = e0.elapsed_time(e1)
+    stages = e.stage_times(reset=True)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, wall, stages
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -225,21 +317,20 @@ def main():
     import torch
     import torch.distributed as dist
     from datetime import timedelta
+    import dataclasses
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
     from miniafqmc_b200.synthetic import CONFIGS, make_system
     from miniafqmc_b200 import driver
-    import dataclasses
     cfg = dataclasses.replace(CONFIGS[args.config], with_vakbl=False)
+    if args.walkers:
+        cfg = dataclasses.replace(cfg, nwalk=args.walkers)
     s = make_system(cfg)
     nw = cfg.nwalk
-    prec = AFQ_PREC_MIXED if args.precision == "mixed" else AFQ_PREC_FP64
-    eng = AfqmcSys(s, nw, precision=prec, device=local, use_vakbl=False)
     comm = None
     if world > 1:
         def allreduce(vals):
@@ -247,54 +338,31 @@ def main():
             dist.all_reduce(t)
             return t.tolist()
         comm = driver.Comm(rank * nw, world * nw, allreduce)
-        eng.set_walker_offset(rank * nw, world * nw)
-    stream = torch.cuda.ExternalStream(eng.stream)
 
-    def one_step(st):
-        driver.substep(eng, cfg.seed, st, args.northo, comm, graph=False)
-        if (st + 1) % args.energy_every == 0:
-            eng.calculate_mixed_density_matrix()
-            driver.energy(eng, "chol", comm)
-
-    eng.calculate_mixed_density_matrix()
-    driver.energy(eng, "chol", comm)
+    head = Form(s, cfg, args, args.form, local, comm, torch)
+    head.measure(record=False)
+    # warm-up: W substeps, and for the control variate the exact-exchange measurements
+    # that gather its 2000 training walker-steps before the estimator switches on
     for st in range(args.warmup):
-        one_step(st)
-    eng.synchronize()
-    eng.stage_times(reset=True)
-    eng.profile(True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        head.step(st, record=False)
+    if head.mode == "cv":
+        while not head.eng.cv_stats()["active"]:
+            head.measure(record=False)
+        head.measure(record=False)
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        for st in range(args.warmup, args.warmup + args.steps):
-            one_step(st)
-        e1.record(stream)
-        eng.synchronize()
-        torch.cuda.synchronize()
-    eng.profile(False)
-    ms = e0.elapsed_time(e1)
-    stages = eng.stage_times(reset=True)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+        ms, wall, stages = timed(head, args.steps, args.warmup, torch, dist, world, profile=True)
     value = world * nw * args.steps / (ms * 1e-3)
     launches = int(sum(v[1] for v in stages.values()))
 
     # ---- end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
+        eng = head.eng
         K = args.steps
         xs = torch.empty((K, cfg.nchol, nw), dtype=torch.float64, pin_memory=True)
-        g = torch.Generator().manual_seed(cfg.seed)
-        xs.normal_(generator=g)
+        xs.normal_(generator=torch.Generator().manual_seed(cfg.seed))
         wd = torch.empty((nw, 8, 2), dtype=torch.float64, pin_memory=True)
         xnp, wdnp = xs.numpy(), wd.numpy()
-        import ctypes
         eng.synchronize()
         if world > 1:
             dist.barrier()
@@ -317,8 +385,7 @@ def main():
                 eng.orthogonalize()
                 eng.calculate_overlaps()
             if (k + 1) % args.energy_every == 0:
-                eng.calculate_mixed_density_matrix()
-                driver.energy(eng, "chol", comm)
+                head.measure(record=False)
             eng._check(eng.lib.afq_get_walkers(eng.h, None, ctypes.c_void_p(wdnp.ctypes.data)))
         eng.synchronize()
         t_e2e = time.perf_counter() - t0
@@ -329,7 +396,34 @@ def main():
         e2e = {"value": world * nw * K / t_e2e, "unit": METRIC,
                "h2d_bytes_per_step": int(cfg.nchol * nw * 8),
                "d2h_bytes_per_step": int(nw * 8 * 16),
-               "note": "per step: normals H2D (pinned) via afq_sigma_from, W_data D2H via afq_get_walkers"}
+               "note": "per step: normals H2D (pinned) via afq_sigma_from, W_data D2H via "
+                       "afq_get_walkers; energy every energy_every steps"}
+
+    # ---- the plain FP64 form on the same steps and auxiliary fields (N=1)
+    cmp = None
+    if not args.no_fp64 and args.form != "fp64" and world == 1:
+        ref = Form(s, cfg, args, "fp64", local, None, torch)
+        ref.measure(record=False)
+        for st in range(args.warmup):
+            ref.step(st, record=False)
+        ms64, wall64, stages64 = timed(ref, args.steps, args.warmup, torch, dist, world, profile=True)
+        Em, E6 = np.array(head.energies), np.array(ref.energies)
+        T_m, T_6 = ms * 1e-3, ms64 * 1e-3
+        sig_m = float(np.sqrt(np.mean(head.sig2) / len(head.sig2)))
+        sig_6 = float(np.sqrt(np.mean(ref.sig2) / len(ref.sig2)))
+        eps_m, eps_6 = sig_m * np.sqrt(T_m), sig_6 * np.sqrt(T_6)
+        cmp = {
+            "fp64_plain": {"value": nw * args.steps / T_6, "unit": METRIC,
+                           "ms_per_step": ms64 / args.steps,
+                           "stages_ms": {k: round(v[0], 3) for k, v in stages64.items()}},
+            "speedup_vs_fp64_plain": T_6 / T_m,
+            "energy": {"measurements": len(Em), "mean_E_form": float(Em.mean()),
+                       "mean_E_fp64": float(E6.mean()), "abs_dE_Ha": float(abs(Em.mean() - E6.mean())),
+                       "max_abs_dE_per_measurement_Ha": float(np.max(np.abs(Em - E6))),
+                       "err_per_wall_s": {"form": eps_m, "fp64": eps_6,
+                                          "fp64_over_form": eps_6 / eps_m}},
+        }
+        ref.eng.close()
 
     if rank != 0:
         if world > 1:
@@ -341,45 +435,55 @@ def main():
     peaks, src = measured_peaks()
     dom = max(stages, key=lambda k: stages[k][0])
     dom_ms, dom_launch = stages[dom]
-    calls = {"propagate": args.steps, "vbias": args.steps, "vHS": args.steps,
-             "DM": args.steps + args.steps // args.energy_every,
-             "energy": args.steps // args.energy_every}.get(dom, args.steps)
-    flops = stage_flops(cfg, nw, dom) * calls
-    if args.precision == "fp64":
+    if args.form == "fp64":
+        calls = {"DM": args.steps + args.steps // args.energy_every,
+                 "energy": args.steps // args.energy_every}.get(dom, args.steps)
         peak = fp64_peak_tflops(torch)
-        peak_src = "FP64 cuBLAS DGEMM 8192^3 measured in this run (no FP64 entry in MEASURED_PEAKS.json)"
+        achieved = fp64_stage_flops(cfg, nw, dom) * calls / (dom_ms * 1e-3) / 1e12
+        roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run "
+                               "(no FP64 entry in MEASURED_PEAKS.json)"}
+    elif dom == "propagate":
+        byt = mixed_propagate_bytes(cfg, nw) * args.steps
+        achieved = byt / (dom_ms * 1e-3) / 1e9
+        roof = {"kernel": "propagate (tcgen05 GEMM chain)", "bound": "hbm", "achieved": achieved,
+                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "peak_source": f"hbm_gbs, {src}"}
     else:
-        peak = peaks["bf16_tflops_sustained"]
-        peak_src = f"bf16 sustained, {src}"
-    achieved = flops / (dom_ms * 1e-3) / 1e12 if dom_ms > 0 else 0.0
+        calls = args.steps if dom != "energy" else args.steps // args.energy_every
+        achieved = fp64_stage_flops(cfg, nw, dom) * calls / (dom_ms * 1e-3) / 1e12
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved,
+                "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
+                "frac": achieved / peaks["bf16_tflops_sustained"],
+                "peak_source": f"bf16_tflops_sustained, {src}"}
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"{args.config}:{args.precision}:{dom}")
-    roof = {"kernel": dom, "bound": "tensor" if args.precision == "mixed" else "fp64",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_source": peak_src,
-            "avg_launch_ms": dom_ms / max(dom_launch, 1), "launches": dom_launch}
+        traffic = json.load(open(tpath)).get(f"{args.config}:{args.form}:{dom}")
+    roof.update({"traffic": traffic, "stage_ms": dom_ms, "launches": dom_launch,
+                 "avg_launch_ms": dom_ms / max(dom_launch, 1)})
 
     cpu = None
     if not args.no_cpu and world == 1:
         threads = os.cpu_count() or 1
         r, info = cpu_rate(s, cfg, args, args.cpu_walkers or max(threads, 8), threads)
-        cpu = {"value": r, "unit": METRIC, "cores": threads, "kind": "port",
-               "sample": info["sample"]}
+        cpu = {"value": r, "unit": METRIC, "cores": threads, "kind": "port", "sample": info["sample"]}
 
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "bf16/tf32+f64",
+        "dtype": "f64" if args.form == "fp64" else "bf16 split/plain tensor-core + f64 LU/QR/weights",
         "data": "synthetic", "config": workload(cfg, args, nw),
         "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clk.summary(),
-        "stages_ms": {k: round(v[0], 3) for k, v in stages.items()},
+        "clocks": clk.summary(), "stages_ms": {k: round(v[0], 3) for k, v in stages.items()},
     }
+    if cmp:
+        line.update(cmp)
+    if head.mode == "cv":
+        line["control_variate"] = head.eng.cv_stats()
     print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -337,15 +337,17 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
       for (int w = 0; w < nw; w++) a += f[(size_t)w * CV_NIN + q];
       a /= nw;
       for (int w = 0; w < nw; w++) b += (f[(size_t)w * CV_NIN + q] - a) * (f[(size_t)w * CV_NIN + q] - a);
+      // the first measurement's walkers are close to each other: floor the spread at a
+      // small fraction of the mean so later, more spread-out walkers stay O(1)
       mu[q] = (float)a;
-      sd[q] = (float)std::max(sqrt(b / nw), 1e-6);
+      sd[q] = (float)std::max(sqrt(b / nw), 1e-2 * fabs(a) + 1e-6);
     }
     double a = 0, b = 0;
     for (int w = 0; w < nw; w++) a += ek[2 * w];
     a /= nw;
     for (int w = 0; w < nw; w++) b += (ek[2 * w] - a) * (ek[2 * w] - a);
     s->mu_t = (float)a;
-    s->sd_t = (float)std::max(sqrt(b / nw), 1e-6);
+    s->sd_t = (float)std::max(sqrt(b / nw), 1e-3 * fabs(a) + 1e-6);
     if ((e = cudaMemcpyAsync(s->d_mu, mu, sizeof(mu), cudaMemcpyHostToDevice, st)) != cudaSuccess)
       return e;
     if ((e = cudaMemcpyAsync(s->d_sd, sd, sizeof(sd), cudaMemcpyHostToDevice, st)) != cudaSuccess)
