@@ -19,7 +19,8 @@ plus `base::halfrotate_cholesky` leave behind (`miniafqmc_base.cpp:176-185`):
   Vakbl  CSR [2*NAEA*NMO]^2 half-rotated two-body matrix     (initialize_serial.hpp:134-164)
 
 System model (all configs): h1 = sym(N(0,0.1)) + diag(linspace(-2,2,N)); nchol real
-symmetric Cholesky vectors L_n with the requested fraction of nonzeros drawn N(0,0.05);
+symmetric Cholesky vectors L_n with the requested fraction of nonzeros drawn
+N(0, sigma), sigma = 0.05 at NMO=64/nchol=256/10% and size-scaled (Config.sigma);
 trial = the lowest NAEA eigenvectors of h1 for both spins; Propg1 =
 expm(-dt/2 (h1 - 1/2 sum_n L_n L_n)).  Everything is drawn from numpy's Philox
 bit generator seeded with `seed`.
@@ -93,6 +94,18 @@ class Config:
     with_vakbl: bool = True
     complex_trial: bool = False   # rotate the trial by a random unitary (tests conj paths)
     complex_chol: bool = False    # give the Cholesky vectors an imaginary part
+    chol_sigma: float | None = None  # std of the nonzeros (default: size-scaled, see below)
+
+    @property
+    def sigma(self) -> float:
+        """Standard deviation of the Cholesky nonzeros: 0.05 at the 64-orbital,
+        256-vector, 10%-dense system, scaled by sqrt(64*256*0.1 / (nmo*nchol*density))
+        elsewhere so the two-body diagonal sum_n L_n(i,k)^2 is the same at every size
+        (with a fixed 0.05 it grows ~70x at NMO=384, nchol=1536, 20% and the propagator
+        becomes unstable: overlaps overflow within a few substeps)."""
+        if self.chol_sigma is not None:
+            return self.chol_sigma
+        return 0.05 * math.sqrt(64 * 256 * 0.1 / (self.nmo * self.nchol * self.density))
 
     @property
     def name(self) -> str:
@@ -117,7 +130,8 @@ CONFIGS = {
 }
 
 
-def _sym_chol_coo(rng, N: int, nchol: int, density: float, complex_chol: bool):
+def _sym_chol_coo(rng, N: int, nchol: int, density: float, complex_chol: bool,
+                  sigma: float = 0.05):
     """COO (row = i*N+k, col = n, value) of nchol symmetric N x N matrices."""
     iu, ju = np.triu_indices(N)
     npos = iu.shape[0]
@@ -127,7 +141,7 @@ def _sym_chol_coo(rng, N: int, nchol: int, density: float, complex_chol: bool):
         n1 = min(nchol, n0 + chunk)
         mask = rng.random((n1 - n0, npos)) < density
         vec, pos = np.nonzero(mask)
-        v = rng.normal(0.0, 0.05, vec.shape[0])
+        v = rng.normal(0.0, sigma, vec.shape[0])
         if complex_chol:
             v = v + 1j * rng.normal(0.0, 0.02, vec.shape[0])
         i, k = iu[pos], ju[pos]
@@ -251,7 +265,7 @@ def make_system(cfg: Config, build_vakbl: bool | None = None) -> System:
     rng = np.random.Generator(np.random.Philox(cfg.seed))
     A = rng.normal(0.0, 0.1, (N, N))
     h1 = 0.5 * (A + A.T) + np.diag(np.linspace(-2.0, 2.0, N))
-    rows, cols, vals = _sym_chol_coo(rng, N, nchol, cfg.density, cfg.complex_chol)
+    rows, cols, vals = _sym_chol_coo(rng, N, nchol, cfg.density, cfg.complex_chol, cfg.sigma)
     evals, evecs = np.linalg.eigh(h1)
     wf = evecs[:, :n].astype(np.complex128)
     if cfg.complex_trial:
