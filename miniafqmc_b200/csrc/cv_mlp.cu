@@ -6,7 +6,7 @@
 // Kernels (CUDA cores; the network is ~75k parameters, far below tensor-core sizes):
 //   mlp_fwd    8 samples per CTA, one hidden unit per thread; keeps z1, z2 for backward
 //   mlp_bwd_x  per-sample backward through the layers (dz2, dz1)
-//   mlp_gradw  one thread per weight: fixed-order sums over the batch (deterministic)
+//   mlp_atb    tiled weight gradients (dz^T x), mlp_colsum bias gradients; fixed order
 //   mlp_adam   Adam update of the FP32 master weights and refresh of the BF16 copies
 #include <cuda_bf16.h>
 #include <cmath>
@@ -151,38 +151,54 @@ __global__ void mlp_bwd_x_kernel(const float* __restrict__ y, const float* __res
   }
 }
 
-// Weight gradients, one output per thread, fixed-order sums over the batch:
-//   gW1[j][i] = sum_b dz1[b][j] x[b][i]   gb1[j] = sum_b dz1[b][j]
-//   gW2[j][k] = sum_b dz2[b][j] h1[b][k]  gb2[j] = sum_b dz2[b][j]
-//   gw3[j]    = sum_b dy[b] h2[b][j]      gb3    = sum_b dy[b]
-__global__ void mlp_gradw_kernel(int B, int nin, int H, const float* __restrict__ x,
-                                 const float* __restrict__ h1, const float* __restrict__ h2,
-                                 const float* __restrict__ dy, const float* __restrict__ dz1,
-                                 const float* __restrict__ dz2, float* __restrict__ g,
-                                 MlpLayout L) {
-  const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (e >= L.total) return;
-  float s = 0.0f;
-  if (e < L.ob1) {
-    const int j = (int)(e / nin), i = (int)(e % nin);
-    for (int b = 0; b < B; b++) s = fmaf(dz1[(long long)b * H + j], x[(long long)b * nin + i], s);
-  } else if (e < L.oW2) {
-    const int j = (int)(e - L.ob1);
-    for (int b = 0; b < B; b++) s += dz1[(long long)b * H + j];
-  } else if (e < L.ob2) {
-    const long long q = e - L.oW2;
-    const int j = (int)(q / H), k = (int)(q % H);
-    for (int b = 0; b < B; b++) s = fmaf(dz2[(long long)b * H + j], h1[(long long)b * H + k], s);
-  } else if (e < L.ow3) {
-    const int j = (int)(e - L.ob2);
-    for (int b = 0; b < B; b++) s += dz2[(long long)b * H + j];
-  } else if (e < L.ob3) {
-    const int j = (int)(e - L.ow3);
-    for (int b = 0; b < B; b++) s = fmaf(dy[b], h2[(long long)b * H + j], s);
-  } else {
-    for (int b = 0; b < B; b++) s += dy[b];
+// Tiled weight gradient C[i][j] = sum_b A[b][i] B[b][j] (A [Bn][M], B [Bn][N], row-major)
+// for gW1 = dz1^T x, gW2 = dz2^T h1 and gw3 = h2^T dy: 64 x 64 outputs per CTA, 4 x 4 per
+// thread, 16-sample slabs staged in shared memory; fixed summation order.
+constexpr int GW_T = 64, GW_K = 16;
+__global__ void __launch_bounds__(256)
+mlp_atb_kernel(const float* __restrict__ A, const float* __restrict__ B, int Bn, int M, int N,
+               float* __restrict__ C) {
+  __shared__ float As[GW_K][GW_T], Bs[GW_K][GW_T];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int i0 = blockIdx.y * GW_T, j0 = blockIdx.x * GW_T;
+  float acc[4][4] = {};
+  for (int b0 = 0; b0 < Bn; b0 += GW_K) {
+    for (int e = threadIdx.x; e < GW_K * GW_T; e += 256) {
+      const int kk = e / GW_T, c = e % GW_T, b = b0 + kk;
+      As[kk][c] = (b < Bn && i0 + c < M) ? A[(long long)b * M + i0 + c] : 0.0f;
+      Bs[kk][c] = (b < Bn && j0 + c < N) ? B[(long long)b * N + j0 + c] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GW_K; kk++) {
+      float a[4], bb[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) a[r] = As[kk][ty + 16 * r];
+#pragma unroll
+      for (int c = 0; c < 4; c++) bb[c] = Bs[kk][tx + 16 * c];
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[r][c] = fmaf(a[r], bb[c], acc[r][c]);
+    }
+    __syncthreads();
   }
-  g[e] = s;
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int i = i0 + ty + 16 * r, j = j0 + tx + 16 * c;
+      if (i < M && j < N) C[(long long)i * N + j] = acc[r][c];
+    }
+}
+
+// column sums s[j] = sum_b A[b][j] (bias gradients), fixed order
+__global__ void mlp_colsum_kernel(const float* __restrict__ A, int Bn, int N, float* __restrict__ s) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  float t = 0.0f;
+  for (int b = 0; b < Bn; b++) t += A[(long long)b * N + j];
+  s[j] = t;
 }
 
 // Adam on the FP32 master weights, then BF16 copies: W1t [nin][H], W2 [H][H], W2t, w3.
@@ -365,8 +381,16 @@ cudaError_t mlp_gradient(Mlp* m, const float* x, const float* t, int B, cudaStre
   if (e != cudaSuccess) return e;
   mlp_bwd_x_kernel<<<nblk(B, MLP_SB), H, sizeof(float) * MLP_SB * H, st>>>(
       m->y, t, B, m->W2, m->w3, m->z1, m->z2, m->dy, m->dz1, m->dz2);
-  mlp_gradw_kernel<<<nblk(m->L.total, 256), 256, 0, st>>>(B, m->L.nin, H, x, m->h1, m->h2, m->dy,
-                                                         m->dz1, m->dz2, m->g, m->L);
+  const MlpLayout& L = m->L;
+  const int nin = L.nin;
+  mlp_atb_kernel<<<dim3(nblk(nin, GW_T), nblk(H, GW_T)), 256, 0, st>>>(m->dz1, x, B, H, nin,
+                                                                      m->g + L.oW1);
+  mlp_atb_kernel<<<dim3(nblk(H, GW_T), nblk(H, GW_T)), 256, 0, st>>>(m->dz2, m->h1, B, H, H,
+                                                                    m->g + L.oW2);
+  mlp_atb_kernel<<<dim3(1, nblk(H, GW_T)), 256, 0, st>>>(m->h2, m->dy, B, H, 1, m->g + L.ow3);
+  mlp_colsum_kernel<<<nblk(H, 128), 128, 0, st>>>(m->dz1, B, H, m->g + L.ob1);
+  mlp_colsum_kernel<<<nblk(H, 128), 128, 0, st>>>(m->dz2, B, H, m->g + L.ob2);
+  mlp_colsum_kernel<<<1, 32, 0, st>>>(m->dy, B, 1, m->g + L.ob3);
   mlp_loss_kernel<<<1, 256, 0, st>>>(m->y, t, B, m->loss);
   return cudaGetLastError();
 }

@@ -20,7 +20,7 @@ constexpr int DM_THREADS = 256;
 
 size_t dm_smem_bytes(int n) {
   size_t ldT = n + 1;
-  size_t buf = std::max((size_t)2 * DM_KC * n, (size_t)n * (DM_KC + 1));
+  size_t buf = std::max((size_t)2 * DM_KC * n, (size_t)n * 65);   // phase 1 slabs | W^T chunk
   return sizeof(z_t) * (n * ldT + buf + n) + sizeof(int) * n;
 }
 
@@ -33,7 +33,7 @@ dm_kernel(const z_t* __restrict__ W, const z_t* __restrict__ tw, int N, int n,
   const int ldT = n + 1;
   z_t* T = reinterpret_cast<z_t*>(dm_smem);
   z_t* buf = T + n * ldT;
-  const int bufsz = max(2 * DM_KC * n, n * (DM_KC + 1));
+  const int bufsz = max(2 * DM_KC * n, n * 65);
   z_t* fcol = buf + bufsz;
   int* perm = reinterpret_cast<int*>(fcol + n);
   __shared__ int s_piv, s_sing;
@@ -43,34 +43,48 @@ dm_kernel(const z_t* __restrict__ W, const z_t* __restrict__ tw, int N, int n,
   const int tid = threadIdx.x, nt = blockDim.x;
   const int nout = n * n;
 
-  // ---- phase 1: T1 = W_s^T tw_s
-  z_t acc[16];
+  // ---- phase 1: T1 = W_s^T tw_s; thread (ta, tb) of a 16 x 16 grid owns rows
+  // a = ta + 16i and columns b = tb + 16j (i, j < R = ceil(n/16)), a register block that
+  // reuses each shared-memory operand R times
+  const int R = (n + 15) / 16;
+  const int ta = tid / 16, tb = tid % 16;
+  {
+    z_t acc[4][4];
 #pragma unroll
-  for (int r = 0; r < 16; r++) acc[r] = zmk(0, 0);
-  for (int k0 = 0; k0 < N; k0 += DM_KC) {
-    const int kc = min(DM_KC, N - k0);
-    for (int e = tid; e < kc * n; e += nt) {
-      int kk = e / n, a = e % n;
-      buf[kk * n + a] = Ws[(long long)(k0 + kk) * ldw + a];
-      buf[DM_KC * n + kk * n + a] = ts[(long long)(k0 + kk) * ldw + a];
-    }
-    __syncthreads();
+    for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
-      int o = tid + r * DM_THREADS;
-      if (o < nout) {
-        int a = o / n, b = o % n;
-        z_t t = acc[r];
-        for (int kk = 0; kk < kc; kk++) zfma(t, buf[kk * n + a], buf[DM_KC * n + kk * n + b]);
-        acc[r] = t;
+      for (int j = 0; j < 4; j++) acc[i][j] = zmk(0, 0);
+    for (int k0 = 0; k0 < N; k0 += DM_KC) {
+      const int kc = min(DM_KC, N - k0);
+      for (int e = tid; e < kc * n; e += nt) {
+        int kk = e / n, a = e % n;
+        buf[kk * n + a] = Ws[(long long)(k0 + kk) * ldw + a];
+        buf[DM_KC * n + kk * n + a] = ts[(long long)(k0 + kk) * ldw + a];
       }
-    }
-    __syncthreads();
-  }
+      __syncthreads();
+      for (int kk = 0; kk < kc; kk++) {
+        z_t av[4], bv[4];
 #pragma unroll
-  for (int r = 0; r < 16; r++) {
-    int o = tid + r * DM_THREADS;
-    if (o < nout) T[(o / n) * ldT + (o % n)] = acc[r];
+        for (int i = 0; i < 4; i++) {
+          const int a = ta + 16 * i, b = tb + 16 * i;
+          av[i] = (i < R && a < n) ? buf[kk * n + a] : zmk(0, 0);
+          bv[i] = (i < R && b < n) ? buf[DM_KC * n + kk * n + b] : zmk(0, 0);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (i < R && j < R) zfma(acc[i][j], av[i], bv[j]);
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int a = ta + 16 * i, b = tb + 16 * j;
+        if (i < R && j < R && a < n && b < n) T[a * ldT + b] = acc[i][j];
+      }
   }
   if (tid == 0) s_sing = 0;
   __syncthreads();
@@ -154,22 +168,44 @@ dm_kernel(const z_t* __restrict__ W, const z_t* __restrict__ tw, int N, int n,
         __syncthreads();
       }
     }
-    for (int k0 = 0; k0 < N; k0 += DM_KC) {
-      const int kc = min(DM_KC, N - k0);
+    // Gc[a][k] = sum_b Tinv[a][b] W[k][b] over 64-row chunks of W: thread (ta, tk) owns
+    // rows a = ta + 16i (i < R) and chunk columns k = tk + 16j (j < 4)
+    constexpr int KC3 = 64;
+    const int tk = tb;
+    for (int k0 = 0; k0 < N; k0 += KC3) {
+      const int kc = min(KC3, N - k0);
       for (int e = tid; e < kc * n; e += nt) {
         int kk = e / n, b = e % n;
-        buf[b * (DM_KC + 1) + kk] = Ws[(long long)(k0 + kk) * ldw + b];
+        buf[b * (KC3 + 1) + kk] = Ws[(long long)(k0 + kk) * ldw + b];
       }
       __syncthreads();
-      for (int e = tid; e < n * DM_KC; e += nt) {
-        int a = e / DM_KC, kk = e % DM_KC;
-        if (kk < kc) {
-          z_t t = zmk(0, 0);
-          if (!sing)
-            for (int b = 0; b < n; b++) zfma(t, T[a * ldT + b], buf[b * (DM_KC + 1) + kk]);
-          Gout[(long long)a * N + k0 + kk] = t;
+      z_t acc[4][4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = zmk(0, 0);
+      if (!sing)
+        for (int b = 0; b < n; b++) {
+          z_t tv[4], wv[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int a = ta + 16 * i;
+            tv[i] = (i < R && a < n) ? T[a * ldT + b] : zmk(0, 0);
+            wv[i] = buf[b * (KC3 + 1) + tk + 16 * i];
+          }
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+              if (i < R) zfma(acc[i][j], tv[i], wv[j]);
         }
-      }
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int a = ta + 16 * i, kk = tk + 16 * j;
+          if (i < R && a < n && kk < kc) Gout[(long long)a * N + k0 + kk] = acc[i][j];
+        }
       __syncthreads();
     }
   }
