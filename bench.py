@@ -271,7 +271,10 @@ class Form:
             w = Wd[:, 1].real
             el = Wd[:, 0].real
             self.energies.append(E)
-            self.sig2.append(float(np.sum(w * w * (el - E) ** 2) / np.sum(w) ** 2))
+            s2 = float(np.sum(w * w * (el - E) ** 2) / np.sum(w) ** 2)
+            if self.mode == "cv":   # plus the sampling variance of the subset correction
+                s2 += e.cv_stats()["subset_var"]
+            self.sig2.append(s2)
         return E
 
     def step(self, st, record=True, graph=True):
@@ -292,10 +295,12 @@ def timed(form, steps, start, torch, dist, world, profile=False):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
+    torch.cuda.nvtx.range_push("timed")   # `ncu --nvtx --nvtx-include timed/` selects it
     e0.record(form.stream)
     for st in range(start, start + steps):
         form.step(st, graph=not profile)   # stage events need the op-by-op calls
     e1.record(form.stream)
+    torch.cuda.nvtx.range_pop()
     e.synchronize()
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
@@ -341,16 +346,18 @@ def main():
 
     head = Form(s, cfg, args, args.form, local, comm, torch)
     head.measure(record=False)
-    # warm-up: W substeps, and for the control variate the exact-exchange measurements
-    # that gather its 2000 training walker-steps before the estimator switches on
-    for st in range(args.warmup):
+    # warm-up: W substeps, and for the control variate as many more as its first 2000
+    # exact-exchange walker-steps take (walkers propagate in between, so the training set
+    # spans the walkers' spread), until the estimator is on for the next measurement
+    nwarm = args.warmup
+    for st in range(nwarm):
         head.step(st, record=False)
     if head.mode == "cv":
-        while not head.eng.cv_stats()["active"]:
-            head.measure(record=False)
-        head.measure(record=False)
+        while not head.eng.cv_stats()["samples"] >= 2000 or nwarm % args.energy_every:
+            head.step(nwarm, record=False)
+            nwarm += 1
     with ClockSampler(local) as clk:
-        ms, wall, stages = timed(head, args.steps, args.warmup, torch, dist, world, profile=True)
+        ms, wall, stages = timed(head, args.steps, nwarm, torch, dist, world, profile=True)
     value = world * nw * args.steps / (ms * 1e-3)
     launches = int(sum(v[1] for v in stages.values()))
 
@@ -369,7 +376,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for k in range(K):
-            st = args.warmup + args.steps + k
+            st = nwarm + args.steps + k
             eng.calculate_mixed_density_matrix()
             eng.get_vbias()
             eng._check(eng.lib.afq_sigma_from(eng.h, ctypes.c_void_p(xnp[k].ctypes.data)))
@@ -404,9 +411,9 @@ def main():
     if not args.no_fp64 and args.form != "fp64" and world == 1:
         ref = Form(s, cfg, args, "fp64", local, None, torch)
         ref.measure(record=False)
-        for st in range(args.warmup):
+        for st in range(nwarm):
             ref.step(st, record=False)
-        ms64, wall64, stages64 = timed(ref, args.steps, args.warmup, torch, dist, world, profile=True)
+        ms64, wall64, stages64 = timed(ref, args.steps, nwarm, torch, dist, world, profile=True)
         Em, E6 = np.array(head.energies), np.array(ref.energies)
         T_m, T_6 = ms * 1e-3, ms64 * 1e-3
         sig_m = float(np.sqrt(np.mean(head.sig2) / len(head.sig2)))

@@ -161,8 +161,11 @@ afq_status afq_synchronize(afq_handle* h);
  * training online on the exact samples.  Call after afq_set_hamiltonian with Lhalf. */
 afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
                             long long train_walker_steps, int subset_den);
-/* stats[5] = exact samples so far, subset size of the last measurement, last training
- * loss (normalised units), estimator active (0/1), measurements. */
+/* stats[8] = exact samples so far, subset size of the last measurement, last training
+ * loss (standardised units), estimator active (0/1), measurements, sampling variance
+ * (Ha^2) that the subset correction adds to the last weighted mean energy,
+ * re-standardisations of the network so far, fallback to exact exchange on every walker
+ * after a non-finite training loss (0/1). */
 afq_status afq_cv_stats(afq_handle* h, double* stats);
 
 /* The surrogate network on its own (used by the control variate; exposed for testing
@@ -223,9 +226,10 @@ afq_status afq_exchange_energy_noalloc(const double* Lh, const double* Gc, int n
  * C[b][m][n] = sum_k A[b][m][k] B[b][n][k] for host fp32 arrays, computed on the current
  * device with bf16 operands (tf32 == 0, inputs rounded to nearest bf16) or tf32 operands,
  * fp32 accumulation, tile width bn in {64, 128, 192}; K must be a multiple of 8.
- * *kernel_err receives the kernel's timeout flags (0 when clean). */
-afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn, const float* A,
-                                const float* B, float* C, int* kernel_err);
+ * mode 0 = one CTA per tile, 1 / 2 = persistent kernel with one / two epilogue
+ * warpgroups.  *kernel_err receives the kernel's timeout flags (0 when clean). */
+afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn, int mode,
+                                const float* A, const float* B, float* C, int* kernel_err);
 
 #ifdef __cplusplus
 }

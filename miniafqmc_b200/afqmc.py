@@ -84,7 +84,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_copy_out": ([P, I, P], I), "afq_set_walker_offset": ([P, I, I], I),
         "afq_profile": ([P, I], I), "afq_stage_times": ([P, P, P, I], I),
         "afq_get_stream": ([P, P], I),
-        "afq_selftest_tc_gemm": ([I, I, I, I, I, I, P, P, P, P], I),
+        "afq_selftest_tc_gemm": ([I, I, I, I, I, I, I, P, P, P, P], I),
         "afq_exchange_energy_noalloc": ([P, P, I, I, I, I, P, P], I),
         "afq_cv_configure": ([P, I, D, U64, ctypes.c_longlong, I], I),
         "afq_cv_stats": ([P, P], I),
@@ -264,10 +264,11 @@ class AfqmcSys:
                                               subset_den))
 
     def cv_stats(self) -> dict:
-        v = np.zeros(5)
+        v = np.zeros(8)
         self._check(self.lib.afq_cv_stats(self.h, _p(v)))
         return {"samples": int(v[0]), "subset": int(v[1]), "loss": float(v[2]),
-                "active": bool(v[3]), "measurements": int(v[4])}
+                "active": bool(v[3]), "measurements": int(v[4]), "subset_var": float(v[5]),
+                "restandardisations": int(v[6]), "fallback": bool(v[7])}
 
     def substep(self, seed: int, step_tot: int, northo: int, graph: bool = True):
         """One substep of the driver loop (miniafqmc_base.cpp:251-337)."""

@@ -206,6 +206,8 @@ afq_status need_ready(afq_handle* h) {
 
 // ------------------------------------------------------------ stage bodies (async)
 cudaError_t body_dm(afq_handle* h, int want_gc, int save_old) {
+  if (h->mixed && afq::mixed_has_dm(h->mixed))
+    return afq::mixed_dm(h->mixed, h->W, h->Gc, h->Wd, h->info, want_gc, save_old, h->st);
   return afq::launch_dm(h->W, h->tw, h->N, h->n, h->nw, h->Gc, h->Wd, h->info, want_gc, save_old,
                         h->st);
 }
@@ -308,8 +310,9 @@ cudaError_t body_energy(afq_handle* h, int mode) {
 
 // Timed / counted stages.  The launch counts are the kernels each body issues.
 cudaError_t st_dm(afq_handle* h, int want_gc, int save_old) {
-  return staged(h, want_gc ? AFQ_STAGE_DM : AFQ_STAGE_OVERLAP, 1,
-                [&] { return body_dm(h, want_gc, save_old); });
+  const int stage = want_gc ? AFQ_STAGE_DM : AFQ_STAGE_OVERLAP;
+  const int nl = (h->mixed && afq::mixed_has_dm(h->mixed)) ? afq::mixed_launches(h->mixed, stage) : 1;
+  return staged(h, stage, nl, [&] { return body_dm(h, want_gc, save_old); });
 }
 cudaError_t st_vbias(afq_handle* h) {
   int nl = h->mixed ? afq::mixed_launches(h->mixed, AFQ_STAGE_VBIAS) : 1;
@@ -524,6 +527,7 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
     mi.N = N; mi.n = n; mi.nchol = nc; mi.nw = h->nw; mi.order = h->d.taylor_order;
     mi.P = h->P; mi.Lh = h->Lh; mi.SpvnT_dense = h->spT_dense;
     mi.sp_ri = h->sp_ri; mi.sp_ci = h->sp_ci; mi.sp_v = h->sp_v; mi.sp_rv = h->sp_rv;
+    mi.trial = getenv("AFQ_MIXED_DM_FP64") ? nullptr : h->tw;
     std::string msg;
     cudaError_t e = afq::mixed_create(&mi, &h->mixed, &msg, h->st);
     if (e != cudaSuccess || !h->mixed)
@@ -722,12 +726,8 @@ afq_status energy_cv(afq_handle* h, double* sums) {
     return afq::cv_energy(h->cv, in, sums, h->st);
   });
   if (e != cudaSuccess) return fail(h, AFQ_ERR_CUDA, std::string("cv energy: ") + cudaGetErrorString(e));
-  double st5[5];
-  afq::cv_stats(h->cv, st5);
-  // coulomb (2 or 3), features, normalise, forward, gather, exchange (1-2), reduce, mark,
-  // assemble, append, and 5 kernels per training iteration
-  h->stage_launches[AFQ_STAGE_ENERGY] +=
-      12 + 5LL * (st5[3] > 0 ? h->cv_cfg.iters_online : h->cv_cfg.iters_warm);
+  // coulomb and exact exchange (2-3 launches each) plus the estimator's own kernels
+  h->stage_launches[AFQ_STAGE_ENERGY] += 5 + afq::cv_launches(h->cv);
   return AFQ_OK;
 }
 
@@ -809,7 +809,7 @@ afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
 afq_status afq_cv_stats(afq_handle* h, double* stats) {
   if (!h || !stats) return AFQ_ERR_ARG;
   if (!h->cv) {
-    for (int i = 0; i < 5; i++) stats[i] = 0.0;
+    for (int i = 0; i < 8; i++) stats[i] = 0.0;
     return AFQ_OK;
   }
   afq::cv_stats(h->cv, stats);

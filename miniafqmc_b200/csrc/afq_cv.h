@@ -20,6 +20,11 @@ cudaError_t mlp_forward(Mlp* m, const float* x, int B, float* y, bool keep, cuda
 cudaError_t mlp_gradient(Mlp* m, const float* x, const float* t, int B, cudaStream_t st);
 cudaError_t mlp_train(Mlp* m, const float* x, const float* t, int B, int iters, float lr,
                       float* last_loss, cudaStream_t st);
+// Rescales the network so that it computes the same function of new input / output
+// coordinates: x_old = a * x_new + c (device arrays [nin]), y_new = alpha y_old + gamma.
+// Restarts the Adam moments.
+cudaError_t mlp_restandardize(Mlp* m, const float* a, const float* c, float alpha, float gamma,
+                              cudaStream_t st);
 
 struct CvConfig {
   int hidden = 256;
@@ -52,8 +57,11 @@ void cv_destroy(CvState* s);
 // sum Re(w)) of the estimator.  Synchronises the stream.
 cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t st);
 // stats: [exact samples seen, subset size of the last measurement, last training loss,
-//         estimator active (0/1), measurements]
+//         estimator active (0/1), measurements, sampling variance of the last estimate
+//         from the subset correction, re-standardisations, fallback to exact (0/1)]
 void cv_stats(const CvState* s, double* stats);
+// Kernels launched by the last cv_energy call (training included).
+long long cv_launches(const CvState* s);
 // Surrogate exchange energy of every walker from the last measurement (host doubles).
 cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st);
 

@@ -18,6 +18,7 @@ struct MixedInit {
   const int* sp_ci;
   const z_t* sp_v;
   const double* sp_rv;
+  const z_t* trial;         // [N][2n] (null: the density matrix stays FP64)
 };
 
 cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* msg,
@@ -31,6 +32,12 @@ cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpar
 cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t st);
 cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
                            cudaStream_t st);
+// Mixed density matrix: T1 = W^T tw in split bf16 on tensor cores, FP64 Gauss-Jordan for
+// det(T1) (-> W_data overlaps, info) and T1^-1, Gc = T1^-1 W^T on tensor cores.
+// want_gc == 0 computes the overlaps only.
+bool mixed_has_dm(const MixedState* m);
+cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, int want_gc,
+                     int save_old, cudaStream_t st);
 // Kernels one call of a stage issues (afq_stage numbering), for the launch counters.
 int mixed_launches(const MixedState* m, int stage);
 // Cholesky-vector blocks of the exchange partial sums (Kpart[nw][2][nblk]).

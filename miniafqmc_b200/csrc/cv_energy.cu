@@ -6,13 +6,23 @@
 //     E_1 = Gc_w.haj, log|ovlp_a ovlp_b| and its phase;
 //   surrogate f_w = MLP(features) on every walker;
 //   exact exchange E_K on a seeded random subset S of m = ceil(nw / subset_den) walkers
-//     (all walkers while the network is being warmed up);
+//     (all walkers until the first train_walker_steps exact samples are in);
 //   sum_w w_w eloc_w = sum_w w_w (E1 + EJ)_w - [sum_w w_w f_w + (nw/m) sum_{w in S} w_w (EK_w - f_w)]
 //     which is unbiased for the exact weighted energy (Horvitz-Thompson correction of the
-//     surrogate on a without-replacement sample with inclusion probability m/nw);
+//     surrogate on a without-replacement sample with inclusion probability m/nw), whatever
+//     the network predicts;
 //   W_data[:,0] holds exact energies on S and E1 + EJ - f elsewhere;
-//   the exact (features, E_K) pairs of S enter a replay buffer and the network takes a
-//     few Adam steps on it -- after the estimate, so the estimate never sees its own data.
+//   the exact (features, E_K) pairs of S enter a replay buffer of raw values and the
+//     network takes a few Adam steps on it -- after the estimate, so the estimate never
+//     sees its own data.
+//
+// Scales.  Walkers start identical and spread out as the run goes on, so feature and
+// target scales come from the whole replay buffer, not one measurement: the network works
+// on standardised inputs (x - mu) / sd clipped to +-8 and standardised targets clipped to
+// +-16.  When the buffer's statistics drift (a scale off by 1.5x or a mean shifted by half
+// a scale) the network is rescaled so it computes the same function of the new
+// coordinates (mlp_restandardize) and training continues.  A non-finite training loss
+// switches the estimator off for good: exact exchange on every walker, the fallback.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -22,6 +32,7 @@
 namespace afq {
 
 constexpr int CV_NIN = 36, CV_NPROJ = 32;
+constexpr float CV_CLIP_X = 8.0f, CV_CLIP_T = 16.0f;
 
 struct CvState {
   CvConfig cfg;
@@ -29,16 +40,20 @@ struct CvState {
   long long nak = 0;
   Mlp* mlp = nullptr;
   float *R = nullptr, *feats = nullptr, *featn = nullptr, *fpred = nullptr;
-  float *d_mu = nullptr, *d_sd = nullptr, *buf_x = nullptr, *buf_t = nullptr;
-  double *e1ej = nullptr, *ek_sub = nullptr, *d_sums = nullptr;
+  float *d_mu = nullptr, *d_sd = nullptr, *d_a = nullptr, *d_c = nullptr, *d_stat = nullptr;
+  float *raw_x = nullptr, *raw_t = nullptr, *buf_x = nullptr, *buf_t = nullptr;
+  double *e1ej = nullptr, *ek_sub = nullptr, *d_sums = nullptr, *h_sums = nullptr;
   int *d_sub = nullptr, *member = nullptr, *h_sub = nullptr;
   z_t* Gc_sub = nullptr;
   int sub_cap = 0, cap = 0, buf_n = 0, buf_head = 0;
-  float mu_t = 0.0f, sd_t = 1.0f;
-  bool have_norm = false, active = false;
-  long long seen = 0, meas = 0;
+  // standardisation: features (mu, sd); targets E_K = ref + mu_r + sd_r * y
+  float mu[CV_NIN] = {}, sd[CV_NIN] = {};
+  double ref = 0.0, mu_r = 0.0, sd_r = 1.0;
+  bool have_ref = false, trained = false, active = false, failed = false;
+  long long seen = 0, meas = 0, restd = 0, launches = 0;
   int last_m = 0;
   float last_loss = 0.0f;
+  double ht_var = 0.0;
   std::vector<void*> allocs;
 };
 
@@ -109,13 +124,56 @@ cv_features_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, long
   }
 }
 
+// Standardised, clipped features: out = clip((f - mu) / sd, +-CV_CLIP_X).
 __global__ void cv_normalize_kernel(const float* __restrict__ f, long long count,
                                     const float* __restrict__ mu, const float* __restrict__ sd,
                                     float* __restrict__ out) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
        e += (long long)gridDim.x * blockDim.x) {
     const int q = (int)(e % CV_NIN);
-    out[e] = (f[e] - mu[q]) / sd[q];
+    out[e] = fminf(fmaxf((f[e] - mu[q]) / sd[q], -CV_CLIP_X), CV_CLIP_X);
+  }
+}
+
+// Training copy of the replay buffer: standardised features and targets.
+__global__ void cv_normalize_buffer_kernel(const float* __restrict__ rx,
+                                           const float* __restrict__ rt, int n,
+                                           const float* __restrict__ mu,
+                                           const float* __restrict__ sd, float mu_r, float sd_r,
+                                           float* __restrict__ bx, float* __restrict__ bt) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * CV_NIN;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int q = (int)(e % CV_NIN);
+    bx[e] = fminf(fmaxf((rx[e] - mu[q]) / sd[q], -CV_CLIP_X), CV_CLIP_X);
+    if (q == 0) {
+      const long long b = e / CV_NIN;
+      bt[b] = fminf(fmaxf((rt[b] - mu_r) / sd_r, -CV_CLIP_T), CV_CLIP_T);
+    }
+  }
+}
+
+// Column means and standard deviations of the raw buffer (36 features, then the target):
+// one CTA per column, two passes in double, fixed reduction order.
+__global__ void __launch_bounds__(256)
+cv_buffer_stats_kernel(const float* __restrict__ rx, const float* __restrict__ rt, int n,
+                       float* __restrict__ stat) {
+  __shared__ z_t red[8];
+  const int q = blockIdx.x;
+  auto val = [&](int b) -> double {
+    return q < CV_NIN ? (double)rx[(long long)b * CV_NIN + q] : (double)rt[b];
+  };
+  double s = 0.0;
+  for (int b = threadIdx.x; b < n; b += blockDim.x) s += val(b);
+  const double mean = block_zsum(zmk(s, 0.0), red).x / n;
+  double v = 0.0;
+  for (int b = threadIdx.x; b < n; b += blockDim.x) {
+    const double d = val(b) - mean;
+    v += d * d;
+  }
+  const double var = block_zsum(zmk(v, 0.0), red).x / n;
+  if (threadIdx.x == 0) {
+    stat[q] = (float)mean;
+    stat[CV_NIN + 1 + q] = (float)sqrt(var);
   }
 }
 
@@ -148,31 +206,33 @@ __global__ void cv_mark_kernel(const int* __restrict__ sub, int m, int* __restri
     member[sub[i]] = i;
 }
 
-// Replay buffer append: (normalised features, normalised exact E_K) of the subset.
-__global__ void cv_append_kernel(const float* __restrict__ featn, const int* __restrict__ sub,
-                                 int m, const double* __restrict__ ek, float mu_t, float sd_t,
-                                 float* __restrict__ bx, float* __restrict__ bt, int head,
+// Replay buffer append of raw values: features of the subset and E_K - ref.
+__global__ void cv_append_kernel(const float* __restrict__ feats, const int* __restrict__ sub,
+                                 int m, const double* __restrict__ ek, double ref,
+                                 float* __restrict__ rx, float* __restrict__ rt, int head,
                                  int cap) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m * CV_NIN;
        e += gridDim.x * blockDim.x) {
     const int i = e / CV_NIN, q = e % CV_NIN, slot = (head + i) % cap;
-    bx[(long long)slot * CV_NIN + q] = featn[(long long)sub[i] * CV_NIN + q];
-    if (q == 0) bt[slot] = (float)((ek[2 * i] - mu_t) / sd_t);
+    rx[(long long)slot * CV_NIN + q] = feats[(long long)sub[i] * CV_NIN + q];
+    if (q == 0) rt[slot] = (float)(ek[2 * i] - ref);
   }
 }
 
 // Assembles W_data[:,0] and the weighted sums of the estimator (one CTA, fixed order).
+// sums = [numerator, sum of weights, sum_S x, sum_S x^2] with x = w (E_K - f) on the
+// subset (the terms of the Horvitz-Thompson correction, for its sampling variance).
 __global__ void __launch_bounds__(1024)
 cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
                    const double* __restrict__ e1ej, const double* __restrict__ ek,
-                   const float* __restrict__ fpred, float mu_t, float sd_t, z_t* __restrict__ Wd,
-                   double* __restrict__ sums) {
+                   const float* __restrict__ fpred, double f0, double fs,
+                   z_t* __restrict__ Wd, double* __restrict__ sums) {
   __shared__ z_t red[32];
-  double A = 0.0, Bc = 0.0, Wt = 0.0;
+  double A = 0.0, Bc = 0.0, Wt = 0.0, B2 = 0.0;
   for (int w = threadIdx.x; w < nw; w += blockDim.x) {
     const double* p = e1ej + (long long)w * 4;
     const int i = member[w];
-    const double f = active ? (double)fpred[w] * sd_t + mu_t : 0.0;
+    const double f = active ? f0 + fs * (double)fpred[w] : 0.0;
     z_t e;
     if (i >= 0) e = zmk(p[0] + p[2] - ek[2 * i], p[1] + p[3] - ek[2 * i + 1]);
     else e = zmk(p[0] + p[2] - f, p[1] + p[3]);
@@ -180,17 +240,23 @@ cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
     const double om = Wd[(long long)w * 8 + 1].x;
     if (active) {
       A += om * (p[0] + p[2] - f);
-      if (i >= 0) Bc += om * (ek[2 * i] - f);
+      if (i >= 0) {
+        const double x = om * (ek[2 * i] - f);
+        Bc += x;
+        B2 += x * x;
+      }
     } else {
       A += om * e.x;
     }
     Wt += om;
   }
-  z_t ab = block_zsum(zmk(A, Bc), red);
-  z_t wt = block_zsum(zmk(Wt, 0.0), red);
+  const z_t ab = block_zsum(zmk(A, Bc), red);
+  const z_t wt = block_zsum(zmk(Wt, B2), red);
   if (threadIdx.x == 0) {
     sums[0] = active ? ab.x - ((double)nw / (double)m) * ab.y : ab.x;
     sums[1] = wt.x;
+    sums[2] = active ? ab.y : 0.0;
+    sums[3] = active ? wt.y : 0.0;
   }
 }
 
@@ -207,6 +273,59 @@ void sample_subset(unsigned long long seed, long long meas, int nw, int m, int* 
   }
   std::sort(idx.begin(), idx.begin() + m);
   for (int i = 0; i < m; i++) out[i] = idx[i];
+}
+
+// Scale of a column: its standard deviation, floored so constant columns (identical
+// walkers at the start of a run) do not divide by zero.
+float floor_sd(float sd, float mu) { return std::max(sd, 1e-6f * (fabsf(mu) + 1.0f)); }
+
+// New buffer statistics; (re)standardises the network when they drifted.
+cudaError_t cv_restandardize(CvState* s, cudaStream_t st) {
+  cudaError_t e;
+  cv_buffer_stats_kernel<<<CV_NIN + 1, 256, 0, st>>>(s->raw_x, s->raw_t, s->buf_n, s->d_stat);
+  s->launches++;
+  float hs[2 * (CV_NIN + 1)];
+  if ((e = cudaMemcpyAsync(hs, s->d_stat, sizeof(hs), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  float mu[CV_NIN], sd[CV_NIN];
+  bool drift = false;
+  for (int q = 0; q < CV_NIN; q++) {
+    mu[q] = hs[q];
+    sd[q] = floor_sd(hs[CV_NIN + 1 + q], mu[q]);
+    if (s->trained)
+      drift = drift || fabsf(logf(sd[q] / s->sd[q])) > logf(1.5f) ||
+              fabsf(mu[q] - s->mu[q]) > 0.5f * s->sd[q];
+  }
+  const double mu_r = hs[CV_NIN];
+  const double sd_r = floor_sd(hs[2 * CV_NIN + 1], (float)mu_r);
+  if (s->trained)
+    drift = drift || fabs(log(sd_r / s->sd_r)) > log(1.5) || fabs(mu_r - s->mu_r) > 0.5 * s->sd_r;
+  if (s->trained && !drift) return cudaSuccess;
+  if (s->trained) {
+    float a[CV_NIN], c[CV_NIN];
+    for (int q = 0; q < CV_NIN; q++) {
+      a[q] = sd[q] / s->sd[q];
+      c[q] = (mu[q] - s->mu[q]) / s->sd[q];
+    }
+    if ((e = cudaMemcpyAsync(s->d_a, a, sizeof(a), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(s->d_c, c, sizeof(c), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+      return e;
+    const float alpha = (float)(s->sd_r / sd_r), gamma = (float)((s->mu_r - mu_r) / sd_r);
+    if ((e = mlp_restandardize(s->mlp, s->d_a, s->d_c, alpha, gamma, st)) != cudaSuccess) return e;
+    s->launches += 2;
+    s->restd++;
+    // the host arrays a, c must outlive the copies
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  }
+  std::copy(mu, mu + CV_NIN, s->mu);
+  std::copy(sd, sd + CV_NIN, s->sd);
+  s->mu_r = mu_r;
+  s->sd_r = sd_r;
+  if ((e = cudaMemcpyAsync(s->d_mu, s->mu, sizeof(s->mu), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(s->d_sd, s->sd, sizeof(s->sd), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return e;
+  return cudaStreamSynchronize(st);
 }
 
 }  // namespace
@@ -228,15 +347,21 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   A(cmal(s, &s->fpred, nw));
   A(cmal(s, &s->d_mu, CV_NIN));
   A(cmal(s, &s->d_sd, CV_NIN));
+  A(cmal(s, &s->d_a, CV_NIN));
+  A(cmal(s, &s->d_c, CV_NIN));
+  A(cmal(s, &s->d_stat, 2 * (CV_NIN + 1)));
+  A(cmal(s, &s->raw_x, (size_t)s->cap * CV_NIN));
+  A(cmal(s, &s->raw_t, s->cap));
   A(cmal(s, &s->buf_x, (size_t)s->cap * CV_NIN));
   A(cmal(s, &s->buf_t, s->cap));
   A(cmal(s, &s->e1ej, (size_t)nw * 4));
   A(cmal(s, &s->ek_sub, (size_t)nw * 2));
-  A(cmal(s, &s->d_sums, 2));
+  A(cmal(s, &s->d_sums, 4));
   A(cmal(s, &s->d_sub, nw));
   A(cmal(s, &s->member, nw));
   A(cmal(s, &s->Gc_sub, (size_t)s->sub_cap * nak));
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_sums, sizeof(double) * 4);
   if (e == cudaSuccess) e = mlp_create(CV_NIN, cfg.hidden, s->cap, cfg.seed, &s->mlp, st);
   if (e == cudaSuccess) {
     cv_proj_init_kernel<<<gridn((long long)CV_NPROJ * 2 * nchol, 256), 256, 0, st>>>(
@@ -256,6 +381,7 @@ void cv_destroy(CvState* s) {
   if (!s) return;
   mlp_destroy(s->mlp);
   if (s->h_sub) cudaFreeHost(s->h_sub);
+  if (s->h_sums) cudaFreeHost(s->h_sums);
   for (void* p : s->allocs) cudaFree(p);
   delete s;
 }
@@ -266,7 +392,12 @@ void cv_stats(const CvState* s, double* o) {
   o[2] = (double)s->last_loss;
   o[3] = s->active ? 1.0 : 0.0;
   o[4] = (double)s->meas;
+  o[5] = s->ht_var;
+  o[6] = (double)s->restd;
+  o[7] = s->failed ? 1.0 : 0.0;
 }
+
+long long cv_launches(const CvState* s) { return s->launches; }
 
 cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st) {
   std::vector<float> f(s->nw, 0.0f);
@@ -276,7 +407,8 @@ cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
   }
-  for (int w = 0; w < s->nw; w++) host[w] = s->active ? (double)f[w] * s->sd_t + s->mu_t : 0.0;
+  for (int w = 0; w < s->nw; w++)
+    host[w] = s->active ? s->ref + s->mu_r + s->sd_r * (double)f[w] : 0.0;
   return cudaSuccess;
 }
 
@@ -284,10 +416,12 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   const int nw = s->nw;
   cudaError_t e;
   s->meas++;
+  s->launches = 0;
   cv_features_kernel<<<nw, 256, 0, st>>>(in.Gc, in.haj, s->nak, in.cvec, s->nc, nw, in.Wd, s->R,
                                          s->feats, s->e1ej);
+  s->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  s->active = s->have_norm && s->seen >= s->cfg.train_walker_steps;
+  s->active = s->trained && !s->failed;
   const int m = s->active ? s->sub_cap : nw;
   if (s->active) {
     sample_subset(s->cfg.seed, s->meas, nw, m, s->h_sub);
@@ -298,16 +432,18 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   if ((e = cudaMemcpyAsync(s->d_sub, s->h_sub, sizeof(int) * m, cudaMemcpyHostToDevice, st)) !=
       cudaSuccess)
     return e;
-  if (s->have_norm) {
+  if (s->active) {
     cv_normalize_kernel<<<gridn((long long)nw * CV_NIN, 256), 256, 0, st>>>(
         s->feats, (long long)nw * CV_NIN, s->d_mu, s->d_sd, s->featn);
     if ((e = mlp_forward(s->mlp, s->featn, nw, s->fpred, false, st)) != cudaSuccess) return e;
+    s->launches += 2;
   }
   // exact exchange on the subset
   const z_t* gsub = in.Gc;
   if (s->active) {
     cv_gather_kernel<<<gridn((long long)m * s->nak, 256), 256, 0, st>>>(in.Gc, s->nak, s->d_sub, m,
                                                                         s->Gc_sub);
+    s->launches++;
     gsub = s->Gc_sub;
   }
   if ((e = in.exact_exchange(gsub, m, in.Kpart)) != cudaSuccess) return e;
@@ -315,58 +451,56 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   if ((e = cudaMemsetAsync(s->member, 0xFF, sizeof(int) * nw, st)) != cudaSuccess) return e;
   cv_mark_kernel<<<gridn(m, 256), 256, 0, st>>>(s->d_sub, m, s->member);
   cv_assemble_kernel<<<1, 1024, 0, st>>>(nw, m, s->active ? 1 : 0, s->member, s->e1ej, s->ek_sub,
-                                          s->fpred, s->mu_t, s->sd_t, in.Wd, s->d_sums);
+                                          s->fpred, s->ref + s->mu_r, s->sd_r, in.Wd, s->d_sums);
+  s->launches += 3;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  if ((e = cudaMemcpyAsync(sums, s->d_sums, 2 * sizeof(double), cudaMemcpyDeviceToHost, st)) !=
-      cudaSuccess)
+  if ((e = cudaMemcpyAsync(s->h_sums, s->d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                           st)) != cudaSuccess)
     return e;
-  // feature / target scales from the first (all-walker) measurement
-  if (!s->have_norm) {
-    std::vector<float> f((size_t)nw * CV_NIN);
-    std::vector<double> ek((size_t)nw * 2);
-    if ((e = cudaMemcpyAsync(f.data(), s->feats, sizeof(float) * f.size(), cudaMemcpyDeviceToHost,
-                             st)) != cudaSuccess)
+  if (!s->have_ref) {
+    // offset of the stored targets: the first walker's exact exchange energy
+    double ek0[2];
+    if ((e = cudaMemcpyAsync(ek0, s->ek_sub, sizeof(ek0), cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
       return e;
-    if ((e = cudaMemcpyAsync(ek.data(), s->ek_sub, sizeof(double) * ek.size(),
-                             cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-      return e;
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    float mu[CV_NIN], sd[CV_NIN];
-    for (int q = 0; q < CV_NIN; q++) {
-      double a = 0, b = 0;
-      for (int w = 0; w < nw; w++) a += f[(size_t)w * CV_NIN + q];
-      a /= nw;
-      for (int w = 0; w < nw; w++) b += (f[(size_t)w * CV_NIN + q] - a) * (f[(size_t)w * CV_NIN + q] - a);
-      // the first measurement's walkers are close to each other: floor the spread at a
-      // small fraction of the mean so later, more spread-out walkers stay O(1)
-      mu[q] = (float)a;
-      sd[q] = (float)std::max(sqrt(b / nw), 1e-2 * fabs(a) + 1e-6);
-    }
-    double a = 0, b = 0;
-    for (int w = 0; w < nw; w++) a += ek[2 * w];
-    a /= nw;
-    for (int w = 0; w < nw; w++) b += (ek[2 * w] - a) * (ek[2 * w] - a);
-    s->mu_t = (float)a;
-    s->sd_t = (float)std::max(sqrt(b / nw), 1e-3 * fabs(a) + 1e-6);
-    if ((e = cudaMemcpyAsync(s->d_mu, mu, sizeof(mu), cudaMemcpyHostToDevice, st)) != cudaSuccess)
-      return e;
-    if ((e = cudaMemcpyAsync(s->d_sd, sd, sizeof(sd), cudaMemcpyHostToDevice, st)) != cudaSuccess)
-      return e;
-    cv_normalize_kernel<<<gridn((long long)nw * CV_NIN, 256), 256, 0, st>>>(
-        s->feats, (long long)nw * CV_NIN, s->d_mu, s->d_sd, s->featn);
-    s->have_norm = true;
+    s->ref = ek0[0];
+    s->have_ref = true;
   }
-  // online training on the replay buffer
+  // replay buffer of raw (features, E_K - ref) pairs
   cv_append_kernel<<<gridn((long long)m * CV_NIN, 256), 256, 0, st>>>(
-      s->featn, s->d_sub, m, s->ek_sub, s->mu_t, s->sd_t, s->buf_x, s->buf_t, s->buf_head, s->cap);
+      s->feats, s->d_sub, m, s->ek_sub, s->ref, s->raw_x, s->raw_t, s->buf_head, s->cap);
+  s->launches++;
   s->buf_head = (s->buf_head + m) % s->cap;
   s->buf_n = std::min(s->cap, s->buf_n + m);
   s->seen += m;
-  const int iters = s->active ? s->cfg.iters_online : s->cfg.iters_warm;
-  if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, &s->last_loss, st)) !=
-      cudaSuccess)
-    return e;
-  return cudaStreamSynchronize(st);
+  if (!s->failed && s->seen >= s->cfg.train_walker_steps) {
+    const bool first = !s->trained;
+    if ((e = cv_restandardize(s, st)) != cudaSuccess) return e;
+    s->trained = true;
+    cv_normalize_buffer_kernel<<<gridn((long long)s->buf_n * CV_NIN, 256), 256, 0, st>>>(
+        s->raw_x, s->raw_t, s->buf_n, s->d_mu, s->d_sd, (float)s->mu_r, (float)s->sd_r, s->buf_x,
+        s->buf_t);
+    s->launches++;
+    const int iters = first ? s->cfg.iters_warm : s->cfg.iters_online;
+    if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, &s->last_loss,
+                       st)) != cudaSuccess)
+      return e;
+    s->launches += 10LL * iters;
+    if (!std::isfinite(s->last_loss)) s->failed = true;
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  const double* hs = s->h_sums;
+  sums[0] = hs[0];
+  sums[1] = hs[1];
+  // sampling variance of the weighted mean from the subset correction (without
+  // replacement): nw^2 (1 - m/nw) S_x^2 / m / (sum w)^2
+  s->ht_var = 0.0;
+  if (s->active && m > 1 && hs[1] != 0.0) {
+    const double S2 = (hs[3] - hs[2] * hs[2] / m) / (m - 1);
+    s->ht_var = (double)nw * nw * (1.0 - (double)m / nw) * std::max(S2, 0.0) / m / (hs[1] * hs[1]);
+  }
+  return cudaSuccess;
 }
 
 }  // namespace afq

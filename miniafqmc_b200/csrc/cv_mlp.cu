@@ -6,9 +6,11 @@
 // Kernels (CUDA cores; the network is ~75k parameters, far below tensor-core sizes):
 //   mlp_fwd    8 samples per CTA, one hidden unit per thread; keeps z1, z2 for backward
 //   mlp_bwd_x  per-sample backward through the layers (dz2, dz1)
-//   mlp_atb    tiled weight gradients (dz^T x), mlp_colsum bias gradients; fixed order
+//   mlp_atb    tiled weight + bias gradients (dz^T [x|1]) over sample chunks, mlp_gsum
+//              adds the chunks; fixed order
 //   mlp_adam   Adam update of the FP32 master weights and refresh of the BF16 copies
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -151,22 +153,26 @@ __global__ void mlp_bwd_x_kernel(const float* __restrict__ y, const float* __res
   }
 }
 
-// Tiled weight gradient C[i][j] = sum_b A[b][i] B[b][j] (A [Bn][M], B [Bn][N], row-major)
-// for gW1 = dz1^T x, gW2 = dz2^T h1 and gw3 = h2^T dy: 64 x 64 outputs per CTA, 4 x 4 per
-// thread, 16-sample slabs staged in shared memory; fixed summation order.
+// Weight and bias gradients of one layer, C[i][j] = sum_b A[b][i] B[b][j] for j < N and
+// C[i][N] = sum_b A[b][i] (B extended by a column of ones): gW1 = dz1^T [x|1],
+// gW2 = dz2^T [h1|1], [gw3|gb3] = dy^T [h2|1].  64 x 64 outputs per CTA, 4 x 4 per thread,
+// 16-sample slabs in shared memory; grid z splits the samples into chunks whose partial
+// sums part[z][M][N+1] are added in fixed order by mlp_gsum_kernel.
 constexpr int GW_T = 64, GW_K = 16;
 __global__ void __launch_bounds__(256)
 mlp_atb_kernel(const float* __restrict__ A, const float* __restrict__ B, int Bn, int M, int N,
-               float* __restrict__ C) {
+               int chunk, float* __restrict__ part) {
   __shared__ float As[GW_K][GW_T], Bs[GW_K][GW_T];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  const int i0 = blockIdx.y * GW_T, j0 = blockIdx.x * GW_T;
+  const int i0 = blockIdx.y * GW_T, j0 = blockIdx.x * GW_T, N1 = N + 1;
+  const int bbeg = blockIdx.z * chunk, bend = min(Bn, bbeg + chunk);
   float acc[4][4] = {};
-  for (int b0 = 0; b0 < Bn; b0 += GW_K) {
+  for (int b0 = bbeg; b0 < bend; b0 += GW_K) {
     for (int e = threadIdx.x; e < GW_K * GW_T; e += 256) {
-      const int kk = e / GW_T, c = e % GW_T, b = b0 + kk;
-      As[kk][c] = (b < Bn && i0 + c < M) ? A[(long long)b * M + i0 + c] : 0.0f;
-      Bs[kk][c] = (b < Bn && j0 + c < N) ? B[(long long)b * N + j0 + c] : 0.0f;
+      const int kk = e / GW_T, c = e % GW_T, b = b0 + kk, j = j0 + c;
+      const bool in = b < bend;
+      As[kk][c] = (in && i0 + c < M) ? A[(long long)b * M + i0 + c] : 0.0f;
+      Bs[kk][c] = !in ? 0.0f : j < N ? B[(long long)b * N + j] : j == N ? 1.0f : 0.0f;
     }
     __syncthreads();
 #pragma unroll
@@ -183,23 +189,45 @@ mlp_atb_kernel(const float* __restrict__ A, const float* __restrict__ B, int Bn,
     }
     __syncthreads();
   }
+  float* P = part + (long long)blockIdx.z * M * N1;
 #pragma unroll
   for (int r = 0; r < 4; r++)
 #pragma unroll
     for (int c = 0; c < 4; c++) {
       const int i = i0 + ty + 16 * r, j = j0 + tx + 16 * c;
-      if (i < M && j < N) C[(long long)i * N + j] = acc[r][c];
+      if (i < M && j < N1) P[(long long)i * N1 + j] = acc[r][c];
     }
 }
 
-// column sums s[j] = sum_b A[b][j] (bias gradients), fixed order
-__global__ void mlp_colsum_kernel(const float* __restrict__ A, int Bn, int N, float* __restrict__ s) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= N) return;
-  float t = 0.0f;
-  for (int b = 0; b < Bn; b++) t += A[(long long)b * N + j];
-  s[j] = t;
+// gW[i][j] = sum_z part[z][i][j] (j < N), gb[i] = sum_z part[z][i][N]; fixed order.
+__global__ void mlp_gsum_kernel(const float* __restrict__ part, int nz, int M, int N,
+                                float* __restrict__ gW, float* __restrict__ gb) {
+  const int N1 = N + 1;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < M * N1; e += gridDim.x * blockDim.x) {
+    float t = 0.0f;
+    for (int z = 0; z < nz; z++) t += part[(long long)z * M * N1 + e];
+    const int i = e / N1, j = e % N1;
+    if (j < N) gW[(long long)i * N + j] = t;
+    else gb[i] = t;
+  }
 }
+
+// Sample chunking of one layer's gradient: enough CTAs to cover the GPU twice.
+struct GradSplit {
+  int nz, chunk;
+  static int target(int Bn, int M, int N) {
+    const int tiles = ((N + 1 + GW_T - 1) / GW_T) * ((M + GW_T - 1) / GW_T);
+    return std::min(std::max(1, (Bn + GW_K - 1) / GW_K), std::max(1, (2 * 148 + tiles - 1) / tiles));
+  }
+  GradSplit(int Bn, int M, int N) {
+    const int z = target(Bn, M, N);
+    chunk = ((Bn + z - 1) / z + GW_K - 1) / GW_K * GW_K;
+    nz = std::max(1, (Bn + chunk - 1) / chunk);   // <= target(cap, M, N) for Bn <= cap
+  }
+  static long long max_part(int cap, int M, int N) {
+    return (long long)target(cap, M, N) * M * (N + 1);
+  }
+};
 
 // Adam on the FP32 master weights, then BF16 copies: W1t [nin][H], W2 [H][H], W2t, w3.
 __global__ void mlp_adam_kernel(float* __restrict__ p, const float* __restrict__ g,
@@ -268,7 +296,8 @@ struct Mlp {
   float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;
   bf16 *W1t = nullptr, *W2 = nullptr, *W2t = nullptr, *w3 = nullptr;
   float *x = nullptr, *t = nullptr, *y = nullptr, *z1 = nullptr, *z2 = nullptr, *h1 = nullptr,
-        *h2 = nullptr, *dy = nullptr, *dz1 = nullptr, *dz2 = nullptr, *loss = nullptr;
+        *h2 = nullptr, *dy = nullptr, *dz1 = nullptr, *dz2 = nullptr, *loss = nullptr,
+        *part = nullptr;   // per-chunk gradient partial sums
   long long step = 0;
   std::vector<void*> allocs;
   Mlp(int nin, int H) : L(nin, H) {}
@@ -305,6 +334,9 @@ cudaError_t mlp_create(int nin, int H, int cap, unsigned long long seed, Mlp** o
   A(mal(m, &m->h1, (size_t)cap * H)); A(mal(m, &m->h2, (size_t)cap * H));
   A(mal(m, &m->dy, cap)); A(mal(m, &m->dz1, (size_t)cap * H)); A(mal(m, &m->dz2, (size_t)cap * H));
   A(mal(m, &m->loss, 1));
+  A(mal(m, &m->part, (size_t)std::max({GradSplit::max_part(cap, H, nin),
+                                         GradSplit::max_part(cap, H, H),
+                                         GradSplit::max_part(cap, 1, H)})));
   if (e != cudaSuccess) {
     mlp_destroy(m);
     return e;
@@ -359,6 +391,39 @@ cudaError_t mlp_get_params(Mlp* m, float* host, cudaStream_t st) {
   return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
 }
 
+// Function-preserving change of the input and output scales: with x_old = a * x_new + c
+// and y_new = alpha * y_old + gamma, W1' = W1 diag(a), b1' = b1 + W1 c, w3' = alpha w3,
+// b3' = alpha b3 + gamma.  One thread per hidden unit.
+__global__ void mlp_restd_kernel(float* __restrict__ p, MlpLayout L, const float* __restrict__ a,
+                                 const float* __restrict__ c, float alpha, float gamma) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < L.H) {
+    float* w = p + L.oW1 + (long long)j * L.nin;
+    float db = 0.0f;
+    for (int i = 0; i < L.nin; i++) {
+      db = fmaf(w[i], c[i], db);
+      w[i] *= a[i];
+    }
+    p[L.ob1 + j] += db;
+    p[L.ow3 + j] *= alpha;
+  }
+  if (j == 0) p[L.ob3] = alpha * p[L.ob3] + gamma;
+}
+
+cudaError_t mlp_restandardize(Mlp* m, const float* a, const float* c, float alpha, float gamma,
+                              cudaStream_t st) {
+  const long long P = m->L.total;
+  mlp_restd_kernel<<<nblk(m->L.H, 128), 128, 0, st>>>(m->p, m->L, a, c, alpha, gamma);
+  cudaError_t e = cudaGetLastError();
+  // the Adam moments belong to the old coordinates: restart them
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->m, 0, sizeof(float) * P, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(m->v, 0, sizeof(float) * P, st);
+  m->step = 0;
+  if (e != cudaSuccess) return e;
+  mlp_refresh_kernel<<<nblk(P, 256), 256, 0, st>>>(m->p, m->L, m->W1t, m->W2, m->W2t, m->w3);
+  return cudaGetLastError();
+}
+
 // Forward on device inputs x [B][nin] (normalised features) into y [B].
 cudaError_t mlp_forward(Mlp* m, const float* x, int B, float* y, bool keep, cudaStream_t st) {
   if (B <= 0) return cudaSuccess;
@@ -383,14 +448,15 @@ cudaError_t mlp_gradient(Mlp* m, const float* x, const float* t, int B, cudaStre
       m->y, t, B, m->W2, m->w3, m->z1, m->z2, m->dy, m->dz1, m->dz2);
   const MlpLayout& L = m->L;
   const int nin = L.nin;
-  mlp_atb_kernel<<<dim3(nblk(nin, GW_T), nblk(H, GW_T)), 256, 0, st>>>(m->dz1, x, B, H, nin,
-                                                                      m->g + L.oW1);
-  mlp_atb_kernel<<<dim3(nblk(H, GW_T), nblk(H, GW_T)), 256, 0, st>>>(m->dz2, m->h1, B, H, H,
-                                                                    m->g + L.oW2);
-  mlp_atb_kernel<<<dim3(1, nblk(H, GW_T)), 256, 0, st>>>(m->h2, m->dy, B, H, 1, m->g + L.ow3);
-  mlp_colsum_kernel<<<nblk(H, 128), 128, 0, st>>>(m->dz1, B, H, m->g + L.ob1);
-  mlp_colsum_kernel<<<nblk(H, 128), 128, 0, st>>>(m->dz2, B, H, m->g + L.ob2);
-  mlp_colsum_kernel<<<1, 32, 0, st>>>(m->dy, B, 1, m->g + L.ob3);
+  auto layer = [&](const float* A, const float* Bm, int M, int N, float* gW, float* gb) {
+    const GradSplit gs(B, M, N);
+    mlp_atb_kernel<<<dim3(nblk(N + 1, GW_T), nblk(M, GW_T), gs.nz), 256, 0, st>>>(
+        A, Bm, B, M, N, gs.chunk, m->part);
+    mlp_gsum_kernel<<<nblk((long long)M * (N + 1), 256), 256, 0, st>>>(m->part, gs.nz, M, N, gW, gb);
+  };
+  layer(m->dz1, x, H, nin, m->g + L.oW1, m->g + L.ob1);
+  layer(m->dz2, m->h1, H, H, m->g + L.oW2, m->g + L.ob2);
+  layer(m->dy, m->h2, 1, H, m->g + L.ow3, m->g + L.ob3);
   mlp_loss_kernel<<<1, 256, 0, st>>>(m->y, t, B, m->loss);
   return cudaGetLastError();
 }

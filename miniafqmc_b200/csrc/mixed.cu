@@ -15,6 +15,7 @@
 //   E_K   : T_cw = Lh_c Gc_w^T per spin, trace of T^2 from the tile in shared memory
 // LU/overlaps, orthogonalisation, weights and the energy assembly stay FP64.
 #include <cuda_bf16.h>
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -65,13 +66,23 @@ struct MixedState {
   int bn_prop = 0;             // tile width >= 4n of the propagation products
   Op Sd, Pf, SpT, LhJ, LhX;    // static operands
   Op Xf, Vf, F[2], Gb, Gx;     // per-step operands
-  float2* S = nullptr;         // Taylor sum [nw][N][2n]
+  float2* S = nullptr;         // Taylor sum [nw][2n][N]
   float* part = nullptr;       // split-K partial products
   int splits = 1, ksplit = 0;
   int* err = nullptr;
   int ex_Gn = 0, ex_Gw = 0, ex_bn = 0, ex_mtiles = 0;
   std::vector<void*> allocs;
   tc::Maps m_vhs, m_pw[2], m_v[2], m_vbias, m_ej, m_ek;
+  // symmetric Cholesky vectors (L_n(i,k) = L_n(k,i)): the vHS product covers the 16 x 16
+  // orbital blocks (ib <= jb) only and the epilogue mirrors them
+  bool vsym = false;
+  int npairs = 0;
+  int* pairs = nullptr;        // [npairs] ib << 16 | jb
+  // mixed density matrix: T1 = W^T tw (split bf16) -> FP64 LU / inverse -> Gc = T1^-1 W^T
+  Op TwB, Wn, Tinv;            // trial B form, W natural bf16, B form of T1^-1 per spin
+  float2* T1 = nullptr;        // [nw][2][n][n]
+  int bn_t1 = 0, bn_gc = 0;
+  tc::Maps m_t1, m_gc[2];
 };
 
 namespace {
@@ -124,6 +135,38 @@ __global__ void pack_spvn_kernel(const int* __restrict__ ri, const int* __restri
   }
 }
 
+// Symmetry test of the packed Spvn rows ik = i*N + k: flag = 1 if any (i,k) row differs
+// from the (k,i) row in either bf16 part.
+__global__ void check_sym_kernel(Op Sd, int N, int Kv, int* flag) {
+  const long long tot = (long long)N * N * Kv;
+  const uint16_t* hi = reinterpret_cast<const uint16_t*>(Sd.hi);
+  const uint16_t* lo = reinterpret_cast<const uint16_t*>(Sd.lo);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / Kv, c = e % Kv;
+    const int i = (int)(r / N), k = (int)(r % N);
+    if (i >= k) continue;
+    const long long t = ((long long)k * N + i) * Kv + c;
+    if (hi[e] != hi[t] || lo[e] != lo[t]) *flag = 1;
+  }
+}
+// Block-pair rows: dst row p = t*256 + ii*16 + jj <- Sd row (ib*16 + ii)*N + jb*16 + jj
+// for the t-th block pair (ib, jb); 16-byte copies (Kv is a multiple of 8).
+__global__ void pack_sym_kernel(Op Sd, int N, int Kv, const int* __restrict__ pairs, int npairs,
+                                Op dst) {
+  const int q = Kv / 8;   // uint4 per row
+  const long long tot = (long long)npairs * 256 * q;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / q;
+    const int c = (int)(e % q), t = (int)(p >> 8), ii = (int)((p >> 4) & 15), jj = (int)(p & 15);
+    const int ib = pairs[t] >> 16, jb = pairs[t] & 0xffff;
+    const long long src = ((long long)(ib * 16 + ii) * N + jb * 16 + jj) * q + c;
+    reinterpret_cast<uint4*>(dst.hi)[e] = reinterpret_cast<const uint4*>(Sd.hi)[src];
+    reinterpret_cast<uint4*>(dst.lo)[e] = reinterpret_cast<const uint4*>(Sd.lo)[src];
+  }
+}
+
 // ------------------------------------------------------------ per-step operand packing
 // X [nc][nw] -> Xf rows (w, re|im): real Spvn: (Re X[:,w]) and (Im X[:,w]);
 // complex Spvn: (Re, -Im) and (Im, Re) interleaved along c.
@@ -150,7 +193,7 @@ __global__ void pack_x_kernel(const z_t* __restrict__ X, int nc, int nw, int Kv,
   }
 }
 // W [nw][N][2n] -> B form F [nw][4n][2N]: row j: (Re W[:,j], -Im W[:,j]); row 2n+j: (Im, Re)
-__global__ void pack_w_kernel(const z_t* __restrict__ W, int N, int n2, Op dst) {
+__global__ void pack_w_kernel(const z_t* __restrict__ W, int N, int n2, Op dst, int both = 1) {
   __shared__ z_t t[32][33];
   const int w = blockIdx.z, k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
   const z_t* Ww = W + (long long)w * N * n2;
@@ -165,12 +208,147 @@ __global__ void pack_w_kernel(const z_t* __restrict__ W, int N, int n2, Op dst) 
     if (j >= n2 || k >= N) continue;
     z_t v = t[threadIdx.x][i];
     put2(dst, base + (long long)j * 2 * N + 2 * k, (float)v.x, (float)-v.y);
-    put2(dst, base + (long long)(n2 + j) * 2 * N + 2 * k, (float)v.y, (float)v.x);
+    if (both) put2(dst, base + (long long)(n2 + j) * 2 * N + 2 * k, (float)v.y, (float)v.x);
   }
 }
+// Trial B form of T1: rows 2(s n + b) = (Re tw, Im tw), 2(s n + b) + 1 = (-Im tw, Re tw)
+// interleaved along k (the conjugate-trial rows; the product then gives conj(T1)).
+__global__ void pack_trial_kernel(const z_t* __restrict__ tw, int N, int n2, Op dst) {
+  const long long tot = (long long)N * n2;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(e / n2), j = (int)(e % n2);
+    const z_t v = tw[e];
+    put2(dst, (2LL * j) * 2 * N + 2 * k, (float)v.x, (float)v.y);
+    put2(dst, (2LL * j + 1) * 2 * N + 2 * k, (float)-v.y, (float)v.x);
+  }
+}
+// W [nw][N][n2] -> bf16 hi/lo in the same layout ((re, im) pairs): A operand of Gc.
+__global__ void pack_wn_kernel(const z_t* __restrict__ W, long long count, Op dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x) {
+    const z_t v = W[e];
+    put2(dst, 2 * e, (float)v.x, (float)v.y);
+  }
+}
+
+// Batched FP64 Gauss-Jordan of the n x n overlap matrices T1 (one 128-thread CTA per
+// walker-spin, matrix in shared memory; warps take rows, lanes columns), pivoting on
+// max |re| + |im| as izamax: det(T1) for the overlap (ma_operations.hpp:244-260) and,
+// when want_inv, T1^-1 written as the B form of the Gc product: rows 2a = (Re y, -Im y),
+// 2a + 1 = (Im y, Re y) along b, y = T1^-1[a][.].
+constexpr int LU_THREADS = 128;
+size_t lu_smem_bytes(int n) { return sizeof(z_t) * ((size_t)n * (n + 1) + n); }
+
+__global__ void __launch_bounds__(LU_THREADS)
+lu_inv_kernel(const float2* __restrict__ T1, int n, int nmat, Op Tinv, z_t* __restrict__ Wd,
+              int* __restrict__ info, int want_inv, int save_old) {
+  extern __shared__ __align__(16) unsigned char lu_smem[];
+  __shared__ int perm[64], s_piv;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int NWARP = LU_THREADS / 32;
+  const int q = blockIdx.x;   // matrix (walker, spin) = w * 2 + s
+  const int ld = n + 1, nn = n * n;
+  z_t* T = reinterpret_cast<z_t*>(lu_smem);
+  z_t* fcol = T + n * ld;
+  const float2* src = T1 + (long long)q * nn;
+  for (int e = tid; e < nn; e += LU_THREADS) {
+    const float2 v = src[e];
+    T[(e / n) * ld + e % n] = zmk(v.x, v.y);
+  }
+  __syncthreads();
+  z_t det = zmk(1.0, 0.0);
+  int sing = 0;
+  for (int j = 0; j < n; j++) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = n;
+      for (int i = j + lane; i < n; i += 32) {
+        const double v = zabs1(T[i * ld + j]);
+        if (v > best) { best = v; bi = i; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) { s_piv = bi; perm[j] = bi; }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != j)
+      for (int c = tid; c < n; c += LU_THREADS) {
+        const z_t t = T[j * ld + c];
+        T[j * ld + c] = T[p * ld + c];
+        T[p * ld + c] = t;
+      }
+    __syncthreads();
+    const z_t pv = T[j * ld + j];
+    if (pv.x == 0.0 && pv.y == 0.0) { sing = 1; break; }   // uniform across the CTA
+    det = zmul(det, pv);
+    if (p != j) det = zmk(-det.x, -det.y);
+    const z_t inv = zrecip(pv);
+    if (!want_inv) {   // LU: eliminate below the pivot only
+      for (int i = j + 1 + warp; i < n; i += NWARP) {
+        const z_t f = zmul(T[i * ld + j], inv);
+        for (int c = j + 1 + lane; c < n; c += 32)
+          T[i * ld + c] = zsub(T[i * ld + c], zmul(f, T[j * ld + c]));
+      }
+    } else {
+      for (int i = tid; i < n; i += LU_THREADS) fcol[i] = T[i * ld + j];
+      __syncthreads();
+      for (int c = tid; c < n; c += LU_THREADS) T[j * ld + c] = (c == j) ? inv : zmul(T[j * ld + c], inv);
+      __syncthreads();
+      for (int i = warp; i < n; i += NWARP) {
+        if (i == j) continue;
+        const z_t f = fcol[i];
+        for (int c = lane; c < n; c += 32) {
+          const z_t base = (c == j) ? zmk(0, 0) : T[i * ld + c];
+          T[i * ld + c] = zsub(base, zmul(f, T[j * ld + c]));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (sing) det = zmk(0, 0);
+  if (want_inv) {
+    if (!sing)
+      for (int j = n - 1; j >= 0; j--) {   // undo the row interchanges on the columns
+        const int p = perm[j];
+        if (p != j)
+          for (int r = tid; r < n; r += LU_THREADS) {
+            const z_t t = T[r * ld + j];
+            T[r * ld + j] = T[r * ld + p];
+            T[r * ld + p] = t;
+          }
+        __syncthreads();
+      }
+    const long long base = (long long)q * 2 * n * 2 * n;
+    for (int e = tid; e < nn; e += LU_THREADS) {
+      const int a = e / n, b = e % n;
+      const z_t y = sing ? zmk(0, 0) : T[a * ld + b];
+      put2(Tinv, base + (2LL * a) * 2 * n + 2 * b, (float)y.x, (float)-y.y);
+      put2(Tinv, base + (2LL * a + 1) * 2 * n + 2 * b, (float)y.y, (float)y.x);
+    }
+  }
+  if (tid == 0) {
+    const int w = q >> 1, sp = q & 1;
+    z_t* d = Wd + (long long)w * 8;
+    if (save_old) {
+      if (sp == 0) d[5] = d[4];
+      d[6 + sp] = d[2 + sp];
+    }
+    d[2 + sp] = det;
+    info[q] = sing;
+  }
+}
+
 // Gc [nw][2][n][N] -> Gb [2nw][2*NAK] (vbias / Coulomb B form) and, when Gx.hi is set,
-// Gx [2][nw][2n][2N] (exchange B form, rows (w, re|im, b) per spin).
-__global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N, Op Gb, Op Gx) {
+// Gx [2][nwx][2n][2N] (exchange B form, rows (w, re|im, b) per spin; nwx = the walker
+// capacity of Gx, which fixes the spin stride the exchange product reads with).
+__global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N, Op Gb, Op Gx,
+                               int nwx = 0) {
   const long long NAK = 2LL * n * N, tot = (long long)nw * NAK;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -183,7 +361,7 @@ __global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N,
     if (Gx.hi) {
       const long long s = q / ((long long)n * N), r = q % ((long long)n * N);
       const long long b = r / N, k = r % N;
-      const long long row0 = (s * nw + w) * 2 * n + b, row1 = row0 + n;
+      const long long row0 = (s * (nwx ? nwx : nw) + w) * 2 * n + b, row1 = row0 + n;
       put2(Gx, row0 * 2 * N + 2 * k, (float)g.x, (float)-g.y);
       put2(Gx, row1 * 2 * N + 2 * k, (float)g.y, (float)g.x);
     }
@@ -241,6 +419,73 @@ struct EpiVhs {
   }
 };
 
+
+// T1 product: rows j = s n + a of the walker (first 2n rows of the tile), columns
+// 2(s' n + b) + {re, im} of conj(T1); keeps the s' == s blocks as T1[w][s][a][b].
+struct EpiT1 {
+  static constexpr bool kTile = false, kPair = false;
+  float2* T1;
+  int n;
+  AFQ_D void operator()(int w, int row, int, int n0, const float* v) const {
+    if (row >= 2 * n) return;
+    const int s = row / n, a = row % n;
+    float2* dst = T1 + (((long long)w * 2 + s) * n + a) * n;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const int col = n0 + 2 * i, sb = col / (2 * n), b = (col % (2 * n)) >> 1;
+      if (sb == s) dst[b] = make_float2(v[2 * i], -v[2 * i + 1]);
+    }
+  }
+};
+
+// Gc product of spin s: rows k, columns 2a + {re, im}: Gc[w][s][a][k].
+struct EpiGc {
+  static constexpr bool kTile = false, kPair = false;
+  z_t* Gc;
+  int n, N, s;
+  AFQ_D void operator()(int w, int, int k, int n0, const float* v) const {
+    if (k >= N) return;
+    z_t* dst = Gc + ((long long)w * 2 + s) * n * N + k;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const int a = (n0 >> 1) + i;
+      if (a < n) dst[(long long)a * N] = zmk(v[2 * i], v[2 * i + 1]);
+    }
+  }
+};
+
+// vHS of symmetric Cholesky vectors: each 256-column tile is one 16 x 16 orbital block
+// pair (ib, jb), column q = ii*16 + jj; the value goes to V[i][j] and, off the block
+// diagonal, to V[j][i].
+struct EpiVhsSym {
+  static constexpr bool kTile = false, kPair = false;
+  Op V;
+  int nw, N;
+  const int* pairs;
+  AFQ_D void operator()(int, int, int m, int n0, const float* v) const {
+    const bool odd = threadIdx.x & 1;
+    float o[32];
+#pragma unroll
+    for (int c = 0; c < 32; c++) o[c] = __shfl_xor_sync(0xffffffffu, v[c], 1);
+    const int w = m >> 1;
+    if (w >= nw) return;
+    // tile t -> block pair (ib, jb), ib <= jb, in row order (no memory access)
+    int t = n0 >> 8, ib = 0;
+    const int nb = N >> 4;
+    while (t >= nb - ib) { t -= nb - ib; ib++; }
+    const int jb = ib + t;
+    const int i = ib * 16 + ((n0 & 255) >> 4) + (odd ? 1 : 0);
+    const long long vw = (long long)w * N * N;
+#pragma unroll
+    for (int jj = 0; jj < 16; jj++) {
+      const float re = odd ? o[16 + jj] : v[jj], im = odd ? v[16 + jj] : o[jj];
+      const int j = jb * 16 + jj;
+      put2(V, (vw + (long long)i * N + j) * 2, re, im);
+      if (ib != jb) put2(V, (vw + (long long)j * N + i) * 2, re, im);
+    }
+  }
+};
+
 // split-K partial products part[z][m][n]
 struct EpiPart {
   static constexpr bool kTile = false, kPair = false;
@@ -262,39 +507,36 @@ struct EpiPart {
 struct EpiProp {
   static constexpr bool kTile = true, kPair = false;
   int mode, k, last, N, n2;
-  float2* S;
+  float2* S;     // Taylor sum [nw][n2][N] (orbital-major: lanes on consecutive rows)
   z_t* W;
   Op F;          // B form of the next product [nw][2*n2][2N]
   AFQ_D void tile(int w, int mt, int, float* t, int ld, int tid) const {
     const int i0 = mt * 128;
-    const long long sW = (long long)N * n2;
-    for (int e = tid; e < 128 * n2; e += 128) {
-      const int r = e / n2, j = e % n2, i = i0 + r;
-      if (i >= N) continue;
-      const float cr = t[r * ld + j], ci = t[r * ld + n2 + j];
-      const long long o = w * sW + (long long)i * n2 + j;
-      if (mode == 0) {
-        S[o] = make_float2(cr, ci);
-      } else if (mode == 1) {
-        const float inv = 1.0f / (float)k;
-        const float tr = -ci * inv, ti = cr * inv;
-        float2 s = S[o];
-        s.x += tr;
-        s.y += ti;
-        S[o] = s;
-        t[r * ld + j] = last ? s.x : tr;
-        t[r * ld + n2 + j] = last ? s.y : ti;
-      } else {
-        W[o] = zmk(cr, ci);
+    if (mode == 2) {   // walker layout [N][n2]: lanes on consecutive columns
+      for (int e = tid; e < 128 * n2; e += 128) {
+        const int r = e / n2, j = e % n2, i = i0 + r;
+        if (i < N) W[(long long)w * N * n2 + (long long)i * n2 + j] = zmk(t[r * ld + j], t[r * ld + n2 + j]);
       }
+      return;
     }
-    if (mode == 2) return;
-    tc::epi_bar();
     const long long base = (long long)w * 2 * n2 * 2 * N;
+    const float inv = mode == 1 ? 1.0f / (float)k : 0.0f;
     for (int e = tid; e < 128 * n2; e += 128) {
       const int j = e / 128, r = e % 128, i = i0 + r;
       if (i >= N) continue;
-      const float vr = t[r * ld + j], vi = t[r * ld + n2 + j];
+      float vr = t[r * ld + j], vi = t[r * ld + n2 + j];
+      const long long o = (long long)w * N * n2 + (long long)j * N + i;
+      if (mode == 0) {
+        S[o] = make_float2(vr, vi);
+      } else {
+        const float tr = -vi * inv, ti = vr * inv;
+        float2 sv = S[o];
+        sv.x += tr;
+        sv.y += ti;
+        S[o] = sv;
+        vr = last ? sv.x : tr;
+        vi = last ? sv.y : ti;
+      }
       put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
       put2(F, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
     }
@@ -313,21 +555,28 @@ struct EpiPropPair {
   AFQ_D int pair_stride() const { return n2; }
   AFQ_D void pair(int w, int, int i, int j0, const float* cr, const float* ci) const {
     if (i >= N) return;
-    const long long row = (long long)w * N * n2 + (long long)i * n2;
+    const long long row = (long long)w * N * n2 + (long long)i * n2;    // W[w][i][.]
+    const long long scol = (long long)w * N * n2 + i;                   // S[w][.][i]
     const long long base = (long long)w * 2 * n2 * 2 * N;
     const float inv = mode == 1 ? 1.0f / (float)k : 0.0f;
+    // the 32 loads of S first: stores to S and F below cannot be moved above them
+    float2 sv[32];
+    if (mode == 1) {
+#pragma unroll
+      for (int jj = 0; jj < 32; jj++) sv[jj] = S[scol + (long long)(j0 + jj) * N];
+    }
 #pragma unroll
     for (int jj = 0; jj < 32; jj++) {
       const int j = j0 + jj;
       float vr = cr[jj], vi = ci[jj];
       if (mode == 0) {
-        S[row + j] = make_float2(vr, vi);
+        S[scol + (long long)j * N] = make_float2(vr, vi);
       } else if (mode == 1) {
         const float tr = -vi * inv, ti = vr * inv;
-        float2 s = S[row + j];
+        float2 s = sv[jj];
         s.x += tr;
         s.y += ti;
-        S[row + j] = s;
+        S[scol + (long long)j * N] = s;
         vr = last ? s.x : tr;
         vi = last ? s.y : ti;
       } else {
@@ -372,11 +621,91 @@ struct EpiExchange {
   }
 };
 
+// Exchange from the accumulator with per-walker staging (persistent kernel): for each
+// walker of the tile its 2n columns go to shared memory, then all four warps share the
+// trace sums of the tile's Cholesky vectors, added in fixed order.
+template <int TWO_N>
+struct EpiExchangeStaged {
+  static constexpr bool kTile = false, kPair = false, kStaged = true;
+  static constexpr int LD = TWO_N + 1;
+  static constexpr int kScratchBytes = 128 * LD * 4;
+  int n, Gn, Gw, nc, nw, nblk;
+  z_t* Kpart;
+  template <class Ld>
+  AFQ_D void staged(int s, int mt, int nt, int row, Ld& ld, float* scr, int wg) const {
+    __shared__ double red[2][4][2];
+    const int lane = row & 31, warp = row >> 5;
+    const int ncv = min(Gn, nc - mt * Gn);
+    for (int wl = 0; wl < Gw; wl++) {
+      float v[32];
+#pragma unroll
+      for (int q = 0; q < TWO_N / 32; q++) {
+        ld(wl * TWO_N + q * 32, v);
+#pragma unroll
+        for (int i = 0; i < 32; i++) scr[row * LD + q * 32 + i] = v[i];
+      }
+      tc::epi_bar_group(wg);
+      double sr = 0.0, si = 0.0;
+      for (int cv = 0; cv < ncv; cv++) {
+        const float* rows = scr + cv * n * LD;
+        for (int q = row; q < n * n; q += 128) {
+          const int a = q / n, b = q % n;
+          const double ar = rows[a * LD + b], ai = rows[a * LD + n + b];
+          const double br = rows[b * LD + a], bi = rows[b * LD + n + a];
+          sr += ar * br - ai * bi;
+          si += ar * bi + ai * br;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        si += __shfl_xor_sync(0xffffffffu, si, o);
+      }
+      if (lane == 0) {
+        red[wl & 1][warp][0] = sr;
+        red[wl & 1][warp][1] = si;
+      }
+      tc::epi_bar_group(wg);
+      const int w = nt * Gw + wl;
+      if (row == 0 && w < nw) {
+        const double (*r)[2] = red[wl & 1];
+        Kpart[((long long)w * 2 + s) * nblk + mt] =
+            zmk(((r[0][0] + r[1][0]) + r[2][0]) + r[3][0], ((r[0][1] + r[1][1]) + r[2][1]) + r[3][1]);
+      }
+    }
+  }
+};
+
 // ------------------------------------------------------------ dispatch helpers
-template <int BN, int ST, bool SPLIT, class Epi>
+// The persistent kernel (double-buffered accumulator) runs every product whose epilogue
+// needs no shared-memory tile; AFQ_TC_PERSISTENT=0 selects the per-tile kernel instead.
+bool tc_persistent() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("AFQ_TC_PERSISTENT");
+    on = (e && atoi(e) == 0) ? 0 : 1;
+  }
+  return on == 1;
+}
+
+template <int BN, int ST, bool SPLIT, class Epi, int MINB = 1>
 cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
                      cudaStream_t st) {
-  return tc::launch<BN, ST, false, SPLIT>(mp, g, e, err, st);
+  if constexpr (!Epi::kTile) {
+    constexpr int PST = SPLIT ? 2 : 4;
+    constexpr int WG = tc::EpiStaged<Epi>::value ? 1 : 2;
+    if (tc_persistent() || tc::EpiStaged<Epi>::value) {
+      if constexpr (tc::PCfg<BN, PST, false, SPLIT, Epi, WG>::kFits)
+        return tc::launch_persistent<BN, PST, false, SPLIT, Epi, WG>(mp, g, e, err, st);
+      else
+        return cudaErrorInvalidValue;
+    }
+  }
+  if constexpr (tc::EpiStaged<Epi>::value) {
+    return cudaErrorInvalidValue;
+  } else {
+    return tc::launch<BN, ST, false, SPLIT, Epi, MINB>(mp, g, e, err, st);
+  }
 }
 
 // Stage counts: the default ring (4 plain / 2 split stages) keeps one CTA per SM busy;
@@ -385,8 +714,8 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
 template <int BN, bool LEAN, class Epi>
 cudaError_t run_prec(int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
                      cudaStream_t st) {
-  if (prec == PREC_SPLIT) return run_gemm<BN, (LEAN ? 1 : 2), true>(mp, g, e, err, st);
-  return run_gemm<BN, (LEAN ? 2 : 4), false>(mp, g, e, err, st);
+  if (prec == PREC_SPLIT) return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st);
+  return run_gemm<BN, (LEAN ? 2 : 4), false, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st);
 }
 
 template <bool LEAN = false, class Epi>
@@ -480,6 +809,12 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   A(alloc_op(m, m->Gb, (size_t)2 * nw * 2 * NAK));
   A(malloc_track(m, &m->S, (size_t)nw * N * 2 * n));
   A(malloc_track(m, &m->err, 1));
+  if (init->trial) {
+    A(alloc_op(m, m->TwB, (size_t)4 * n * 2 * N));
+    A(alloc_op(m, m->Wn, (size_t)nw * N * 4 * n));
+    A(alloc_op(m, m->Tinv, (size_t)nw * 2 * 2 * n * 2 * n));
+    A(malloc_track(m, &m->T1, (size_t)nw * 2 * n * n));
+  }
   if (init->Lh) {
     A(alloc_op(m, m->LhJ, (size_t)nc * 2 * NAK));
     A(alloc_op(m, m->LhX, (size_t)nc * 2 * NAK));
@@ -507,6 +842,15 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   pack_complex_kernel<<<grid_for((long long)N * N), 256, 0, st>>>(init->P, (long long)N * N, m->Pf);
   pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->SpvnT_dense,
                                                                     (long long)nc * NAK, m->SpT);
+  for (int i = 0; i < 2; i++) {   // rows the products read past their data stay finite
+    A(cudaMemsetAsync(m->F[i].hi, 0, sizeof(bf16) * (size_t)nw * 4 * n * 2 * N, st));
+    A(cudaMemsetAsync(m->F[i].lo, 0, sizeof(bf16) * (size_t)nw * 4 * n * 2 * N, st));
+  }
+  if (init->trial) {
+    A(cudaMemsetAsync(m->TwB.hi, 0, sizeof(bf16) * (size_t)4 * n * 2 * N, st));
+    A(cudaMemsetAsync(m->TwB.lo, 0, sizeof(bf16) * (size_t)4 * n * 2 * N, st));
+    pack_trial_kernel<<<grid_for((long long)N * 2 * n), 256, 0, st>>>(init->trial, N, 2 * n, m->TwB);
+  }
   if (init->Lh) {
     pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, (long long)nc * NAK,
                                                                       m->LhJ);
@@ -515,11 +859,44 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   A(cudaGetLastError());
   A(cudaStreamSynchronize(st));
   if (e != cudaSuccess) return bail(e, "packing");
+  // symmetric Cholesky vectors: keep only the 16 x 16 block pairs ib <= jb
+  if (N % 16 == 0 && !getenv("AFQ_VHS_FULL")) {
+    A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+    check_sym_kernel<<<148 * 8, 256, 0, st>>>(m->Sd, N, m->Kv, m->err);
+    int asym = 1;
+    A(cudaGetLastError());
+    A(cudaMemcpyAsync(&asym, m->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    A(cudaStreamSynchronize(st));
+    A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+    if (e == cudaSuccess && !asym) {
+      const int nb = N / 16;
+      std::vector<int> hp;
+      for (int ib = 0; ib < nb; ib++)
+        for (int jb = ib; jb < nb; jb++) hp.push_back(ib << 16 | jb);
+      m->npairs = (int)hp.size();
+      Op sym;
+      A(malloc_track(m, &m->pairs, hp.size()));
+      A(alloc_op(m, sym, (size_t)m->npairs * 256 * m->Kv));
+      A(cudaMemcpyAsync(m->pairs, hp.data(), sizeof(int) * hp.size(), cudaMemcpyHostToDevice, st));
+      if (e == cudaSuccess)
+        pack_sym_kernel<<<148 * 8, 256, 0, st>>>(m->Sd, N, m->Kv, m->pairs, m->npairs, sym);
+      A(cudaGetLastError());
+      A(cudaStreamSynchronize(st));
+      if (e != cudaSuccess) return bail(e, "symmetric Spvn packing");
+      // the full dense operand was a set-up temporary
+      for (void* q : {(void*)m->Sd.hi, (void*)m->Sd.lo}) {
+        m->allocs.erase(std::find(m->allocs.begin(), m->allocs.end(), q));
+        cudaFree(q);
+      }
+      m->Sd = sym;
+      m->vsym = true;
+    }
+  }
   // tensor maps
   bool ok = true;
   const int bnv = 256;
-  ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, (uint64_t)N * N, 1, m->Kv,
-             0, bnv);
+  const uint64_t vrows = m->vsym ? (uint64_t)m->npairs * 256 : (uint64_t)N * N;
+  ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv);
   const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
   for (int i = 0; i < 2; i++) {
     ok &= map2(m->m_pw[i], m->Pf, 2 * N, N, 1, 2 * N, 0, m->F[i], 2 * N, fr, nw, 2 * N, fsz,
@@ -546,6 +923,19 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     ok &= map2(m->m_ek, m->LhX, 2 * N, (uint64_t)nc * n, 2, 2 * N, (uint64_t)nc * n * 2 * N, m->Gx,
                2 * N, (uint64_t)nw * 2 * n, 2, 2 * N, (uint64_t)nw * 2 * n * 2 * N, m->ex_bn);
   }
+  if (init->trial && n <= 64) {
+    m->bn_t1 = pick_bn(4 * n);
+    m->bn_gc = pick_bn(2 * n);
+    const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
+    ok &= map2(m->m_t1, m->F[0], 2 * N, fr, nw, 2 * N, fsz, m->TwB, 2 * N, 4 * n, 1, 2 * N, 0,
+               m->bn_t1);
+    for (int sp = 0; sp < 2; sp++) {
+      Op a{m->Wn.hi + 2 * n * sp, m->Wn.lo + 2 * n * sp};
+      Op b{m->Tinv.hi + (size_t)sp * 2 * n * 2 * n, m->Tinv.lo + (size_t)sp * 2 * n * 2 * n};
+      ok &= map2(m->m_gc[sp], a, 2 * n, N, nw, 4 * n, (uint64_t)N * 4 * n, b, 2 * n, 2 * n, nw,
+                 2 * n, (uint64_t)2 * 2 * n * 2 * n, m->bn_gc);
+    }
+  }
   if (!ok) return bail(cudaSuccess, "tensor map encoding failed");
   *out = m;
   return cudaSuccess;
@@ -569,6 +959,8 @@ int mixed_launches(const MixedState* m, int stage) {
     case 3: return 2;                                  // pack, GEMM (vHS)
     case 4: return 2 + m->in.order + 1;                // pack, P W, order terms, P S
     case 8: return m->in.Lh ? 4 : 0;                   // pack, E_J GEMM, reduce, E_K GEMM
+    case 0: return 6;                                  // pack, T1, LU, pack, Gc x 2
+    case 5: return 3;                                  // pack, T1, LU (overlaps)
   }
   return 0;
 }
@@ -579,7 +971,13 @@ cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
                                                                              m->s_real, m->Xf);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  tc::GemmShape g{2 * nw, N * N, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0};
+  if (m->vsym) {
+    tc::GemmShape g{2 * nw, m->npairs * 256, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0,
+                    true};
+    EpiVhsSym epi{m->Vf, nw, N, m->pairs};
+    return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
+  }
+  tc::GemmShape g{2 * nw, N * N, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0, true};
   EpiVhs epi{m->Vf, nw, (long long)N * N};
   return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
 }
@@ -653,13 +1051,63 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
                            cudaStream_t st) {
   if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
   pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(Gc, nsub, m->n, m->N, Op{},
-                                                                     m->Gx);
+                                                                     m->Gx, m->nw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int n = m->n;
   tc::GemmShape g{m->nc * n, nsub * 2 * n, 2 * m->N, 2, m->ex_Gn * n, m->ex_mtiles, true, true, 0};
+  if (tc_persistent()) {
+    switch (2 * n) {   // staged exchange for the compiled walker widths
+      case 32: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
+                             EpiExchangeStaged<32>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart},
+                             m->err, st);
+      case 64: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
+                             EpiExchangeStaged<64>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart},
+                             m->err, st);
+      case 96: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
+                             EpiExchangeStaged<96>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart},
+                             m->err, st);
+    }
+  }
   EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart};
   return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g, ep, m->err, st);
+}
+
+bool mixed_has_dm(const MixedState* m) { return m && m->T1 && m->bn_t1 && m->bn_gc; }
+
+// Overlaps (want_gc == 0) or the full mixed density matrix of every walker.
+cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, int want_gc,
+                     int save_old, cudaStream_t st) {
+  if (!mixed_has_dm(m)) return cudaErrorInvalidValue;
+  const int N = m->N, n = m->n, n2 = 2 * n, nw = m->nw;
+  pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0], 0);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  {  // T1 (conjugated) of both spins: one 128-row tile per walker
+    tc::GemmShape g{128, 4 * n, 2 * N, nw, 128, 1, true, false, 0};
+    if ((e = run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st)) != cudaSuccess)
+      return e;
+  }
+  static size_t attr = 0;
+  const size_t smem = lu_smem_bytes(n);
+  if (smem > attr) {
+    if ((e = cudaFuncSetAttribute(lu_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem)) != cudaSuccess)
+      return e;
+    attr = smem;
+  }
+  lu_inv_kernel<<<2 * nw, LU_THREADS, smem, st>>>(m->T1, n, 2 * nw, m->Tinv, Wd, info, want_gc,
+                                                  save_old);
+  if ((e = cudaGetLastError()) != cudaSuccess || !want_gc) return e;
+  pack_wn_kernel<<<grid_for((long long)nw * N * n2), 256, 0, st>>>(W, (long long)nw * N * n2, m->Wn);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  for (int sp = 0; sp < 2; sp++) {
+    tc::GemmShape g{N, 2 * n, 2 * n, nw, 128, (N + 127) / 128, true, true, 0};
+    if ((e = run_bn(m->bn_gc, PREC_SPLIT, m->m_gc[sp], g, EpiGc{Gc, n, N, sp}, m->err, st)) !=
+        cudaSuccess)
+      return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpart, int nblk,

@@ -18,6 +18,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <stdint.h>
+#include <type_traits>
 #include "afq_common.cuh"
 
 namespace tc {
@@ -49,6 +50,9 @@ AFQ_D bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (done) return true;
     if (clock64() - t0 > 2000000000LL) return false;
   }
+}
+AFQ_D void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 AFQ_D void fence_barrier_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 AFQ_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -154,6 +158,18 @@ struct Maps {
 
 // Named barrier among the 128 epilogue threads (warps 0-3).
 AFQ_D void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// Named barrier of epilogue warpgroup g of the persistent kernel (ids 1, 2).
+AFQ_D void epi_bar_group(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+
+// Optional epilogue traits: kStaged functors get TMEM access and kScratchBytes of shared
+// memory per epilogue warpgroup (persistent kernel only).
+template <class E, class = void> struct EpiStaged : std::false_type {};
+template <class E>
+struct EpiStaged<E, std::void_t<decltype(E::kStaged)>> : std::integral_constant<bool, E::kStaged> {};
+template <class E, class = void> struct EpiScratch : std::integral_constant<int, 0> {};
+template <class E>
+struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
+    : std::integral_constant<int, E::kScratchBytes> {};
 
 // Epilogue interface.  Row-wise functors (Epi::kTile == Epi::kPair == false) get
 //   epi(batch, tile_row, m, n_first, v[32])
@@ -162,10 +178,12 @@ AFQ_D void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 // c0 < P = epi.pair_stride().  Tile functors (kTile) get the whole fp32 tile in shared
 // memory (row stride BN + 1) after the epilogue barrier:
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi>
-__global__ void __launch_bounds__(192, 1)
+//   MINB = CTAs per SM the launch is compiled for (2 caps registers at 170 per thread so a
+//   lean ring's CTAs pair up on an SM).
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int MINB = 1>
+__global__ void __launch_bounds__(192, MINB)
 tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched, int b_batched,
-               int k_split, Epi epi, int* err) {
+               int k_split, int m_fast, Epi epi, int* err) {
   using C = Cfg<BN, STAGES, TF32, SPLIT>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -179,7 +197,9 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * m_step, n0 = blockIdx.x * BN;
+  // m_fast: M tiles along grid x, so the CTAs that share a B tile run together
+  const int mt = m_fast ? blockIdx.x : blockIdx.y, nt = m_fast ? blockIdx.y : blockIdx.x;
+  const int m0 = mt * m_step, n0 = nt * BN;
   const int batch = blockIdx.z;
   // split-K: z selects the K range [z*k_split, (z+1)*k_split) of an unbatched product
   const int kbase = k_split ? batch * k_split : 0;
@@ -285,7 +305,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
           for (int i = 0; i < 32; i++) tile[row * (BN + 1) + c0 + i] = v[i];
         }
         epi_bar();
-        epi.tile(batch, blockIdx.y, blockIdx.x, tile, BN + 1, threadIdx.x);
+        epi.tile(batch, mt, nt, tile, BN + 1, threadIdx.x);
       } else {
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 32) {
@@ -298,6 +318,213 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, C::TMEM_COLS);
+}
+
+// ------------------------------------------------------------------ persistent form
+// One CTA per SM walks the tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...  The TMA
+// producer (one thread) and the MMA issuer (one thread) run ahead across tile boundaries
+// through the operand ring; the accumulator is double-buffered in TMEM (2 x TMEM_COLS
+// columns), so the epilogue of tile i (EPI_WG warpgroups splitting the 32-column chunks)
+// overlaps the main loop of tile i + 1.  Barriers: full/empty per ring stage, acc_full /
+// acc_empty per accumulator buffer, fin for the issuer's last MMAs.  Every wait is
+// bounded as in the per-tile kernel; a role that times out records the error and stops,
+// and the others follow at their next wait.
+struct TileSched {
+  int m_tiles, n_tiles, nbatch, m_fast;
+  AFQ_HD int total() const { return m_tiles * n_tiles * nbatch; }
+  AFQ_D void decode(int t, int& z, int& mt, int& nt) const {
+    const int per = m_tiles * n_tiles;
+    z = t / per;
+    const int r = t - z * per;
+    if (m_fast) {
+      mt = r % m_tiles;
+      nt = r / m_tiles;
+    } else {
+      nt = r % n_tiles;
+      mt = r / n_tiles;
+    }
+  }
+};
+
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int EPI_WG>
+struct PCfg {
+  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  static constexpr int NEPI = 128 * EPI_WG, THREADS = NEPI + 64;
+  static constexpr uint32_t ACC_COLS = 2 * C::TMEM_COLS;
+  static constexpr size_t SCRATCH = (size_t)EpiScratch<Epi>::value * EPI_WG;
+  static constexpr size_t BAR = 8 * (2 * STAGES + 5);
+  static constexpr size_t SMEM = 1024 + STAGES * C::STAGE_BYTES + SCRATCH + BAR + 16;
+  static constexpr bool kFits = SMEM <= 227 * 1024 && ACC_COLS <= 512;
+};
+
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int EPI_WG>
+__global__ void __launch_bounds__(128 * EPI_WG + 64, 1)
+tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched,
+                          int b_batched, int k_split, TileSched sched, Epi epi, int* err) {
+  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  using P = PCfg<BN, STAGES, TF32, SPLIT, Epi, EPI_WG>;
+  static_assert(!Epi::kTile, "tile epilogues reuse the operand ring: per-tile kernel only");
+  extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  auto stA = [&](int s, int part) { return smem + s * C::STAGE_BYTES + part * (C::A_BYTES + C::B_BYTES); };
+  auto stB = [&](int s, int part) { return stA(s, part) + C::A_BYTES; };
+  float* scratch = reinterpret_cast<float*>(smem + STAGES * C::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES + P::SCRATCH);
+  uint64_t* empty = full + STAGES;
+  uint64_t* accf = empty + STAGES;   // [2]
+  uint64_t* acce = accf + 2;         // [2]
+  uint64_t* fin = acce + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int WPROD = P::NEPI / 32, WMMA = WPROD + 1;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], P::NEPI);
+    }
+    mbar_init(fin, 1);
+    fence_barrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(tmem_slot, P::ACC_COLS);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const int total = sched.total();
+
+  if (warp == WPROD && lane == 0) {
+    // ---- TMA producer
+    int g = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+      int z, mt, nt;
+      sched.decode(t, z, mt, nt);
+      const int kbase = k_split ? z * k_split : 0;
+      const int klen = k_split ? min(k_split, K - kbase) : K;
+      const int nk = (klen + C::BK - 1) / C::BK;
+      const int za = (a_batched && !k_split) ? z : 0, zb = (b_batched && !k_split) ? z : 0;
+      const int m0 = mt * m_step, n0 = nt * BN;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g % STAGES;
+        if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1)) {
+          atomicOr(err, ERR_TIMEOUT_PRODUCER);
+          ok = false;
+          break;
+        }
+        const int kx = kbase + kb * C::BK;
+        mbar_expect_tx(&full[s], C::STAGE_BYTES);
+        tma_load_3d(stA(s, 0), &maps.a, &full[s], kx, m0, za);
+        tma_load_3d(stB(s, 0), &maps.b, &full[s], kx, n0, zb);
+        if (SPLIT) {
+          tma_load_3d(stA(s, 1), &maps.a_lo, &full[s], kx, m0, za);
+          tma_load_3d(stB(s, 1), &maps.b_lo, &full[s], kx, n0, zb);
+        }
+      }
+    }
+    // the last fills of each stage land before the CTA can exit
+    for (int q = max(0, g - STAGES); q < g; q++) mbar_wait(&full[q % STAGES], (q / STAGES) & 1);
+  } else if (warp == WMMA && lane == 0) {
+    // ---- MMA issuer
+    constexpr uint32_t ID = idesc(128, BN, TF32);
+    int g = 0, li = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, li++) {
+      int z, mt, nt;
+      sched.decode(t, z, mt, nt);
+      const int kbase = k_split ? z * k_split : 0;
+      const int klen = k_split ? min(k_split, K - kbase) : K;
+      const int nk = (klen + C::BK - 1) / C::BK;
+      const int b = li & 1;
+      if (!mbar_wait(&acce[b], ((li >> 1) & 1) ^ 1)) {   // the epilogue released buffer b
+        atomicOr(err, ERR_TIMEOUT_MMA);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t d = tmem + b * C::TMEM_COLS;
+      for (int kb = 0; kb < nk; kb++, g++) {
+        const int s = g % STAGES;
+        if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+          atomicOr(err, ERR_TIMEOUT_MMA);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t ad = sdesc_k128(smem_u32(stA(s, 0)));
+        const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
+#pragma unroll
+        for (int k = 0; k < C::BK / C::UK; k++)
+          umma<TF32>(d, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
+        if (SPLIT) {
+          const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
+          const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
+#pragma unroll
+          for (int k = 0; k < C::BK / C::UK; k++) {
+            umma<TF32>(d, ad + 2 * k, bl + 2 * k, ID, 1u);
+            umma<TF32>(d, al + 2 * k, bd + 2 * k, ID, 1u);
+          }
+        }
+        umma_commit(&empty[s]);
+      }
+      if (!ok) break;
+      umma_commit(&accf[b]);
+    }
+    umma_commit(fin);   // fires once every MMA issued above has completed
+    mbar_wait(fin, 0);
+  }
+
+  if (warp < WPROD) {
+    // ---- epilogue: warpgroup wg takes chunks wg, wg + EPI_WG, ...; TMEM lane = tile row
+    const int wg = warp >> 2, wq = warp & 3;
+    const int row = wq * 32 + lane;
+    int li = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, li++) {
+      int z, mt, nt;
+      sched.decode(t, z, mt, nt);
+      const int b = li & 1;
+      if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
+        if (lane == 0) atomicOr(err, ERR_TIMEOUT_EPILOGUE);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t trow = tmem + b * C::TMEM_COLS + ((uint32_t)(wq * 32) << 16);
+      const int m0 = mt * m_step, n0 = nt * BN;
+      float v[32];
+      if constexpr (Epi::kPair) {
+        const int Pw = epi.pair_stride();
+        float u[32];
+#pragma unroll 1
+        for (int c0 = wg * 32; c0 < Pw && c0 + Pw < BN + 1; c0 += 32 * EPI_WG) {
+          tmem_ld32(trow + c0, v);
+          tmem_ld32(trow + c0 + Pw, u);
+          epi.pair(z, row, m0 + row, c0, v, u);
+        }
+      } else if constexpr (EpiStaged<Epi>::value) {
+        float* scr = scratch + (size_t)wg * (EpiScratch<Epi>::value / 4);
+        auto ld = [&](int col, float* out) { tmem_ld32(trow + col, out); };
+        epi.staged(z, mt, nt, row, ld, scr, wg);
+      } else {
+#pragma unroll 1
+        for (int c0 = wg * 32; c0 < BN; c0 += 32 * EPI_WG) {
+          tmem_ld32(trow + c0, v);
+          epi(z, row, m0 + row, n0 + c0, v);
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[b]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, P::ACC_COLS);
 }
 
 // ------------------------------------------------------------------ host side
@@ -331,25 +558,65 @@ struct GemmShape {
   int m_tiles;         // number of M tiles
   bool a_batched, b_batched;
   int k_split;         // 0, or the K extent of each z slice (a multiple of the K slab)
+  bool m_fast = false; // raster M tiles fastest (B tiles reused from L2 across M)
 };
 
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi>
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int MINB = 1>
 cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
                    cudaStream_t st) {
   using C = Cfg<BN, STAGES, TF32, SPLIT>;
   static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
                 "tile epilogue needs the operand ring to hold the fp32 tile");
-  auto kern = tc_gemm_kernel<BN, STAGES, TF32, SPLIT, Epi>;
+  static_assert(MINB * C::SMEM <= 228 * 1024 && MINB * C::TMEM_COLS <= 512,
+                "CTAs per SM exceed shared memory or TMEM");
+  auto kern = tc_gemm_kernel<BN, STAGES, TF32, SPLIT, Epi, MINB>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)C::SMEM);
+    if (e == cudaSuccess && MINB > 1)
+      e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  dim3 grid((g.N + BN - 1) / BN, g.m_tiles, g.batch);
-  kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, g.a_batched, g.b_batched, g.k_split, epi,
-                                    err);
+  const unsigned ntiles = (g.N + BN - 1) / BN;
+  dim3 grid(g.m_fast ? g.m_tiles : ntiles, g.m_fast ? ntiles : g.m_tiles, g.batch);
+  kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, g.a_batched, g.b_batched, g.k_split,
+                                    g.m_fast ? 1 : 0, epi, err);
+  return cudaGetLastError();
+}
+
+inline int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+  }
+  return n;
+}
+
+template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int EPI_WG = 1>
+cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
+                              cudaStream_t st) {
+  using P = PCfg<BN, STAGES, TF32, SPLIT, Epi, EPI_WG>;
+  static_assert(P::kFits, "persistent configuration exceeds shared memory or TMEM");
+  auto kern = tc_gemm_persistent_kernel<BN, STAGES, TF32, SPLIT, Epi, EPI_WG>;
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)P::SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  TileSched sc{g.m_tiles, (g.N + BN - 1) / BN, g.batch, g.m_fast ? 1 : 0};
+  const int total = sc.total();
+  if (total <= 0) return cudaSuccess;
+  const int grid = total < sm_count() ? total : sm_count();
+  kern<<<grid, P::THREADS, P::SMEM, st>>>(maps, g.K, g.m_step, g.a_batched, g.b_batched,
+                                          g.k_split, sc, epi, err);
   return cudaGetLastError();
 }
 

@@ -25,7 +25,7 @@ struct EpiStoreF32 {
 
 template <int BN, bool TF32>
 cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, int batch,
-                int* derr, cudaStream_t st) {
+                int mode, int* derr, cudaStream_t st) {
   tc::Maps maps;
   if (tc::make_kmajor_map(&maps.a, dA, TF32, K, M, batch, K, (uint64_t)M * K, 128) != CUDA_SUCCESS)
     return cudaErrorInvalidValue;
@@ -35,15 +35,18 @@ cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, 
   maps.b_lo = maps.b;
   tc::GemmShape g{M, N, K, batch, 128, (M + 127) / 128, true, true, 0};
   EpiStoreF32 epi{dC, M, N, (long long)M * N};
+  if (mode == 1) return tc::launch_persistent<BN, 4, TF32, false, EpiStoreF32, 1>(maps, g, epi, derr, st);
+  if (mode == 2) return tc::launch_persistent<BN, 4, TF32, false, EpiStoreF32, 2>(maps, g, epi, derr, st);
   return tc::launch<BN, 4, TF32, false>(maps, g, epi, derr, st);
 }
 
 }  // namespace
 
 extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn,
-                                          const float* A, const float* B, float* C,
+                                          int mode, const float* A, const float* B, float* C,
                                           int* kernel_err) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C) return AFQ_ERR_ARG;
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C || mode < 0 || mode > 2)
+    return AFQ_ERR_ARG;
   if (K % 8 != 0) return AFQ_ERR_UNSUPPORTED;   // 16-byte row strides for TMA
   const size_t na = (size_t)batch * M * K, nb = (size_t)batch * N * K, nc = (size_t)batch * M * N;
   void *dA = nullptr, *dB = nullptr;
@@ -71,12 +74,12 @@ extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int t
     cudaMemset(dC, 0, nc * 4);
     cudaMemset(derr, 0, sizeof(int));
     cudaError_t e;
-    if (bn == 64) e = tf32 ? run<64, true>(dA, dB, dC, M, N, K, batch, derr, st)
-                           : run<64, false>(dA, dB, dC, M, N, K, batch, derr, st);
-    else if (bn == 192) e = tf32 ? run<192, true>(dA, dB, dC, M, N, K, batch, derr, st)
-                                 : run<192, false>(dA, dB, dC, M, N, K, batch, derr, st);
-    else e = tf32 ? run<128, true>(dA, dB, dC, M, N, K, batch, derr, st)
-                  : run<128, false>(dA, dB, dC, M, N, K, batch, derr, st);
+    if (bn == 64) e = tf32 ? run<64, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
+                           : run<64, false>(dA, dB, dC, M, N, K, batch, mode, derr, st);
+    else if (bn == 192) e = tf32 ? run<192, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
+                                 : run<192, false>(dA, dB, dC, M, N, K, batch, mode, derr, st);
+    else e = tf32 ? run<128, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
+                  : run<128, false>(dA, dB, dC, M, N, K, batch, mode, derr, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) s = AFQ_ERR_CUDA;
     cudaMemcpy(C, dC, nc * 4, cudaMemcpyDeviceToHost);

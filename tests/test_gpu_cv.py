@@ -55,7 +55,7 @@ def test_cv_energy_unbiased_with_variance_gain():
     nw = 256
     g = AfqmcSys(s, nw)
     g.cv_configure(hidden=256, lr=1e-3, seed=7, train_walker_steps=4 * nw, subset_den=8)
-    diffs, gains, exact = [], [], []
+    diffs, gains, exact, htv = [], [], [], []
     st = 0
     for meas in range(40):
         for _ in range(2):
@@ -68,19 +68,25 @@ def test_cv_energy_unbiased_with_variance_gain():
         Wd_cv = g.get_walker_data()
         e_ex = g.calculate_energy("chol")
         ek = g.copy_out("energy_parts")[:, 2]
+        Wd_ex = g.get_walker_data()
         if stats["active"]:
+            # the subset's exact local energies are the exact evaluation's, walker by walker
+            same = np.abs(Wd_cv[:, 0] - Wd_ex[:, 0]) <= 1e-9 * np.abs(Wd_ex[:, 0])
+            assert same.sum() == stats["subset"], (same.sum(), stats["subset"])
             diffs.append(e_cv - e_ex)
             om = Wd_cv[:, 1].real
             v_plain = np.var(om * ek, ddof=1)           # plain subsampling of exact E_K
             v_cv = np.var(om * (ek - pred), ddof=1)     # subsampling the residual
             gains.append(v_plain / v_cv)
             exact.append(e_ex)
+            htv.append(stats["subset_var"])
         else:
             assert e_cv == pytest.approx(e_ex, rel=1e-12)
     diffs = np.array(diffs)
     res = {"measurements_active": len(diffs), "mean_dE": float(diffs.mean()),
            "std_dE": float(diffs.std(ddof=1)), "median_variance_gain": float(np.median(gains)),
-           "last_stats": stats, "E_exact_last": exact[-1]}
+           "last_stats": stats, "E_exact_last": exact[-1],
+           "predicted_std_dE": float(np.sqrt(np.mean(htv)))}
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     with open(OUT, "w") as f:
         json.dump(res, f, indent=1)
@@ -89,4 +95,7 @@ def test_cv_energy_unbiased_with_variance_gain():
     assert abs(diffs.mean()) < 4 * diffs.std(ddof=1) / np.sqrt(len(diffs)) + 1e-12
     # the trained surrogate removes most of the exchange variance of plain subsampling
     assert np.median(gains) > 3.0
+    # the estimator's own sampling-variance estimate matches the observed scatter
+    assert 0.4 < diffs.std(ddof=1) / np.sqrt(np.mean(htv)) < 2.5
+    assert not stats["fallback"]
     g.close()

@@ -1,6 +1,7 @@
 """The mixed-precision (tcgen05) form against the FP64 form on identical inputs.
 
-Stage tolerances (relative to the largest magnitude of the quantity):
+Stage tolerances (relative to the largest magnitude of the quantity; overlaps relative
+per walker):
   split bf16 (hi*hi + hi*lo + lo*hi) stages: 1e-4    plain bf16 stages: 2e-2
 Trajectory: per-step mixed energy within 1e-4 relative of the FP64 energy on the same
 auxiliary fields.  Measured errors are written to gpurun_out/mixed_errors.json."""
@@ -54,6 +55,9 @@ def test_mixed_stages(name, kw, nw):
     for e in (d, m):
         e.calculate_mixed_density_matrix()
         e.get_vbias()
+    eg = rel(m.copy_out("Gc"), d.copy_out("Gc"))
+    od, om = d.get_walker_data()[:, 2:4], m.get_walker_data()[:, 2:4]
+    eo = float(np.max(np.abs(om - od) / np.abs(od)))
     ev = rel(m.copy_out("vbias"), d.copy_out("vbias"))
     for e in (d, m):
         e.sigma(3, 1)
@@ -67,11 +71,12 @@ def test_mixed_stages(name, kw, nw):
     ed, em = d.calculate_energy("chol"), m.calculate_energy("chol")
     pd, pm = d.copy_out("energy_parts"), m.copy_out("energy_parts")
     m.synchronize()
-    res = {"vbias": ev, "vHS": eh, "W_after_propagate": ew, "E": abs(em - ed) / abs(ed),
+    res = {"Gc": eg, "overlap": eo, "vbias": ev, "vHS": eh, "W_after_propagate": ew,
+           "E": abs(em - ed) / abs(ed),
            "E1": rel(pm[:, 0], pd[:, 0]), "EJ": rel(pm[:, 1], pd[:, 1]), "EK": rel(pm[:, 2], pd[:, 2]),
            "E_abs_Ha": abs(em - ed)}
     record(f"stages_{tag}", res)
-    assert ev < 1e-4 and eh < 1e-4
+    assert eg < 1e-4 and eo < 1e-4 and ev < 1e-4 and eh < 1e-4
     assert ew < 2e-2
     assert res["EJ"] < 1e-4 and res["EK"] < 1e-4
     d.close()
@@ -114,8 +119,9 @@ def test_cholqr2_ortho_matches_householder_up_to_signs():
         for sp in range(2):
             M = Wm[w, sp].conj().T @ Wd_[w, sp]
             assert np.max(np.abs(np.abs(M) - np.eye(s.n))) < 1e-11
-    assert rel(m.copy_out("Gc"), d.copy_out("Gc")) < 1e-11
+    # the mixed form's density matrix and overlaps are split-bf16 tensor-core products
+    assert rel(m.copy_out("Gc"), d.copy_out("Gc")) < 1e-4
     od, om = d.get_walker_data()[:, 2:4], m.get_walker_data()[:, 2:4]
-    assert rel(np.abs(om), np.abs(od)) < 1e-11
+    assert rel(np.abs(om), np.abs(od)) < 1e-4
     d.close()
     m.close()

@@ -10,7 +10,7 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def run(M, N, K, batch, tf32, bn, seed=0):
+def run(M, N, K, batch, tf32, bn, seed=0, mode=0):
     from miniafqmc_b200.afqmc import load_library
     lib = load_library()
     g = torch.Generator().manual_seed(seed)
@@ -25,7 +25,8 @@ def run(M, N, K, batch, tf32, bn, seed=0):
     C = np.zeros((batch, M, N), np.float32)
     err = ctypes.c_int(-1)
     An, Bn = A.numpy().copy(), B.numpy().copy()
-    st = lib.afq_selftest_tc_gemm(M, N, K, batch, int(tf32), bn, ctypes.c_void_p(An.ctypes.data),
+    st = lib.afq_selftest_tc_gemm(M, N, K, batch, int(tf32), bn, mode,
+                                  ctypes.c_void_p(An.ctypes.data),
                                   ctypes.c_void_p(Bn.ctypes.data), ctypes.c_void_p(C.ctypes.data),
                                   ctypes.byref(err))
     assert st == 0 and err.value == 0, (st, err.value)
@@ -37,8 +38,9 @@ def run(M, N, K, batch, tf32, bn, seed=0):
 @pytest.mark.parametrize("shape", [(128, 128, 64, 1, 128), (300, 200, 768, 3, 128),
                                    (256, 192, 1024, 2, 192), (100, 64, 72, 1, 64),
                                    (384, 192, 768, 4, 192)])
-def test_tc_gemm_matches_reference(shape, tf32):
+@pytest.mark.parametrize("mode", [0, 1, 2])   # per-tile, persistent x1 / x2 epilogue groups
+def test_tc_gemm_matches_reference(shape, tf32, mode):
     M, N, K, batch, bn = shape
-    C, ref = run(M, N, K, batch, tf32, bn)
+    C, ref = run(M, N, K, batch, tf32, bn, mode=mode)
     scale = np.abs(ref).max()
     assert np.max(np.abs(C - ref)) / scale < 2e-5
