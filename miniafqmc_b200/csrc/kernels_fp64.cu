@@ -617,35 +617,48 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
   const long long ldw = 2 * n;
   z_t* B = W + (long long)w * N * ldw + s * n;
   const int tid = threadIdx.x, nt = blockDim.x;
+  const int R = (n + 15) / 16, ta = tid / 16, tb = tid % 16;   // n <= 64, 256 threads
   if (tid == 0) s_bad = 0;
   for (int pass = 0; pass < 2; pass++) {
-    // ---- Gram matrix G[a][b] = sum_k conj(B[k][a]) B[k][b]
-    z_t acc[16];
+    // ---- Gram matrix G[a][b] = sum_k conj(B[k][a]) B[k][b]; thread (ta, tb) of a 16 x 16
+    // grid owns a = ta + 16i, b = tb + 16j (i, j < R = ceil(n/16)): R^2 products per 2R
+    // shared-memory reads
+    {
+      z_t acc[4][4];
 #pragma unroll
-    for (int r = 0; r < 16; r++) acc[r] = zmk(0, 0);
-    for (int k0 = 0; k0 < N; k0 += CQ_KC) {
-      const int kc = min(CQ_KC, N - k0);
-      for (int e = tid; e < kc * n; e += nt) {
-        int kk = e / n, a = e % n;
-        buf[kk * ld + a] = B[(long long)(k0 + kk) * ldw + a];
-      }
-      __syncthreads();
+      for (int i = 0; i < 4; i++)
 #pragma unroll
-      for (int r = 0; r < 16; r++) {
-        int o = tid + r * 256;
-        if (o < n * n) {
-          int a = o / n, b = o % n;
-          z_t t = acc[r];
-          for (int kk = 0; kk < kc; kk++) zfma_conj(t, buf[kk * ld + a], buf[kk * ld + b]);
-          acc[r] = t;
+        for (int j = 0; j < 4; j++) acc[i][j] = zmk(0, 0);
+      for (int k0 = 0; k0 < N; k0 += CQ_KC) {
+        const int kc = min(CQ_KC, N - k0);
+        for (int e = tid; e < kc * n; e += nt) {
+          int kk = e / n, a = e % n;
+          buf[kk * ld + a] = B[(long long)(k0 + kk) * ldw + a];
         }
-      }
-      __syncthreads();
-    }
+        __syncthreads();
+        for (int kk = 0; kk < kc; kk++) {
+          z_t av[4], bv[4];
 #pragma unroll
-    for (int r = 0; r < 16; r++) {
-      int o = tid + r * 256;
-      if (o < n * n) G[(o / n) * ld + (o % n)] = acc[r];
+          for (int i = 0; i < 4; i++) {
+            const int a = ta + 16 * i, b = tb + 16 * i;
+            av[i] = (i < R && a < n) ? buf[kk * ld + a] : zmk(0, 0);
+            bv[i] = (i < R && b < n) ? buf[kk * ld + b] : zmk(0, 0);
+          }
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+              if (i < R && j < R) zfma_conj(acc[i][j], av[i], bv[j]);
+        }
+        __syncthreads();
+      }
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int a = ta + 16 * i, b = tb + 16 * j;
+          if (i < R && j < R && a < n && b < n) G[a * ld + b] = acc[i][j];
+        }
     }
     __syncthreads();
     // ---- Cholesky G = R^H R in place (upper triangle)
@@ -684,7 +697,8 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
       }
     }
     __syncthreads();
-    // ---- B <- B R^-1 in 32-row chunks
+    // ---- B <- B R^-1 in 32-row chunks: thread (tk, tb) owns rows k = tk + 16i (i < 2)
+    // and columns b = tb + 16j (j < R); R^-1 is upper triangular (zeros below)
     for (int k0 = 0; k0 < N; k0 += CQ_KC) {
       const int kc = min(CQ_KC, N - k0);
       for (int e = tid; e < kc * n; e += nt) {
@@ -692,12 +706,33 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
         buf[kk * ld + a] = B[(long long)(k0 + kk) * ldw + a];
       }
       __syncthreads();
-      for (int e = tid; e < kc * n; e += nt) {
-        int kk = e / n, b = e % n;
-        z_t t = zmk(0, 0);
-        for (int a = 0; a <= b; a++) zfma(t, buf[kk * ld + a], Ri[a * ld + b]);
-        B[(long long)(k0 + kk) * ldw + b] = t;
+      z_t acc[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = zmk(0, 0);
+      for (int a = 0; a < n; a++) {
+        z_t bv[2], rv[4];
+#pragma unroll
+        for (int i = 0; i < 2; i++) bv[i] = buf[(ta + 16 * i) * ld + a];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int b = tb + 16 * j;
+          rv[j] = (j < R && b < n) ? Ri[a * ld + b] : zmk(0, 0);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (j < R) zfma(acc[i][j], bv[i], rv[j]);
       }
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const int kk = ta + 16 * i, b = tb + 16 * j;
+          if (j < R && kk < kc && b < n) B[(long long)(k0 + kk) * ldw + b] = acc[i][j];
+        }
       __syncthreads();
     }
   }
@@ -705,6 +740,7 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
 }
 
 cudaError_t launch_ortho_cholqr(z_t* W, int N, int n, int nw, int* info, cudaStream_t st) {
+  if (n > 64) return cudaErrorInvalidValue;   // the register tiles cover n <= 64
   size_t smem = cholqr_smem_bytes(n);
   static size_t attr = 0;
   if (smem > attr) {

@@ -69,6 +69,10 @@ struct MixedState {
   float2* S = nullptr;         // Taylor sum [nw][2n][N]
   float* part = nullptr;       // split-K partial products
   int splits = 1, ksplit = 0;
+  // real SpvnT and Lh (real orbitals and Cholesky vectors): A operands hold real values
+  // only and the G operands carry Re and Im in separate rows, so K is halved
+  bool greal = false;
+  bool preal = false;   // real Propg1: P W and P S take K = N with (Re | Im) B rows
   int* err = nullptr;
   int ex_Gn = 0, ex_Gw = 0, ex_bn = 0, ex_mtiles = 0;
   std::vector<void*> allocs;
@@ -110,6 +114,27 @@ __global__ void pack_complex_kernel(const z_t* __restrict__ src, long long count
        e += (long long)gridDim.x * blockDim.x) {
     z_t v = src[e];
     put2(dst, 2 * e, (float)v.x, (float)v.y);
+  }
+}
+// flag = 1 if any imaginary part of src is nonzero
+__global__ void check_imag_kernel(const z_t* __restrict__ src, long long count, int* flag) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x)
+    if (src[e].y != 0.0) *flag = 1;
+}
+// real parts: dst[e] = Re src[e]
+__global__ void pack_real_kernel(const z_t* __restrict__ src, long long count, Op dst) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x)
+    put1(dst, e, (float)src[e].x);
+}
+// Lh [c][s][a][k] -> real LhX [s][c][a][k]
+__global__ void pack_lhx_real_kernel(const z_t* __restrict__ Lh, int nc, int n, int N, Op dst) {
+  const long long per = (long long)n * N, tot = 2LL * nc * per;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    long long s = e / (nc * per), r = e % (nc * per), c = r / per, q = r % per;
+    put1(dst, e, (float)Lh[c * 2 * per + s * per + q].x);
   }
 }
 // Lh [c][s][a][k] -> LhX [s][c][a][2k]
@@ -193,6 +218,7 @@ __global__ void pack_x_kernel(const z_t* __restrict__ X, int nc, int nw, int Kv,
   }
 }
 // W [nw][N][2n] -> B form F [nw][4n][2N]: row j: (Re W[:,j], -Im W[:,j]); row 2n+j: (Im, Re)
+// both == 2: real-A form instead, row j = Re W[:, j], row n2 + j = Im W[:, j] (K = N).
 __global__ void pack_w_kernel(const z_t* __restrict__ W, int N, int n2, Op dst, int both = 1) {
   __shared__ z_t t[32][33];
   const int w = blockIdx.z, k0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
@@ -207,6 +233,11 @@ __global__ void pack_w_kernel(const z_t* __restrict__ W, int N, int n2, Op dst, 
     int j = j0 + i, k = k0 + threadIdx.x;
     if (j >= n2 || k >= N) continue;
     z_t v = t[threadIdx.x][i];
+    if (both == 2) {
+      put1(dst, base + (long long)j * 2 * N + k, (float)v.x);
+      put1(dst, base + (long long)(n2 + j) * 2 * N + k, (float)v.y);
+      continue;
+    }
     put2(dst, base + (long long)j * 2 * N + 2 * k, (float)v.x, (float)-v.y);
     if (both) put2(dst, base + (long long)(n2 + j) * 2 * N + 2 * k, (float)v.y, (float)v.x);
   }
@@ -347,13 +378,29 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, int nmat, Op Tinv, z_t* __re
 // Gc [nw][2][n][N] -> Gb [2nw][2*NAK] (vbias / Coulomb B form) and, when Gx.hi is set,
 // Gx [2][nwx][2n][2N] (exchange B form, rows (w, re|im, b) per spin; nwx = the walker
 // capacity of Gx, which fixes the spin stride the exchange product reads with).
+// real == 1 (real A operands): Gb rows w = Re Gc_w, nw + w = Im Gc_w over NAK; Gx rows
+// (w, re, b) = Re Gc_w[b][.], (w, im, b) = Im over N.
 __global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N, Op Gb, Op Gx,
-                               int nwx = 0) {
+                               int nwx = 0, int real = 0) {
   const long long NAK = 2LL * n * N, tot = (long long)nw * NAK;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
     const long long w = e / NAK, q = e % NAK;
     const z_t g = Gc[e];
+    if (real) {
+      if (Gb.hi) {
+        put1(Gb, w * NAK + q, (float)g.x);
+        put1(Gb, (nw + w) * NAK + q, (float)g.y);
+      }
+      if (Gx.hi) {
+        const long long s = q / ((long long)n * N), r = q % ((long long)n * N);
+        const long long b = r / N, k = r % N;
+        const long long row0 = (s * (nwx ? nwx : nw) + w) * 2 * n + b;
+        put1(Gx, row0 * N + k, (float)g.x);
+        put1(Gx, (row0 + n) * N + k, (float)g.y);
+      }
+      continue;
+    }
     if (Gb.hi) {
       put2(Gb, w * 2 * NAK + 2 * q, (float)g.x, (float)-g.y);
       put2(Gb, (nw + w) * 2 * NAK + 2 * q, (float)g.y, (float)g.x);
@@ -510,6 +557,7 @@ struct EpiProp {
   float2* S;     // Taylor sum [nw][n2][N] (orbital-major: lanes on consecutive rows)
   z_t* W;
   Op F;          // B form of the next product [nw][2*n2][2N]
+  int real_next; // the next product has a real A operand (P S with real P): (Re | Im) rows
   AFQ_D void tile(int w, int mt, int, float* t, int ld, int tid) const {
     const int i0 = mt * 128;
     if (mode == 2) {   // walker layout [N][n2]: lanes on consecutive columns
@@ -537,8 +585,13 @@ struct EpiProp {
         vr = last ? sv.x : tr;
         vi = last ? sv.y : ti;
       }
-      put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
-      put2(F, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
+      if (real_next) {
+        put1(F, base + (long long)j * 2 * N + i, vr);
+        put1(F, base + (long long)(n2 + j) * 2 * N + i, vi);
+      } else {
+        put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
+        put2(F, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
+      }
     }
   }
 };
@@ -552,6 +605,7 @@ struct EpiPropPair {
   float2* S;
   z_t* W;
   Op F;
+  int real_next;
   AFQ_D int pair_stride() const { return n2; }
   AFQ_D void pair(int w, int, int i, int j0, const float* cr, const float* ci) const {
     if (i >= N) return;
@@ -581,6 +635,11 @@ struct EpiPropPair {
         vi = last ? s.y : ti;
       } else {
         W[row + j] = zmk(vr, vi);
+        continue;
+      }
+      if (real_next) {
+        put1(F, base + (long long)j * 2 * N + i, vr);
+        put1(F, base + (long long)(n2 + j) * 2 * N + i, vi);
         continue;
       }
       put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
@@ -735,10 +794,10 @@ cudaError_t run_prop(MixedState* m, int prec, const tc::Maps& mp, const tc::Gemm
                      int k, int last, z_t* W, const Op& F, cudaStream_t st) {
   const int n2 = 2 * m->n;
   if (n2 % 32 == 0) {
-    EpiPropPair ep{mode, k, last, m->N, n2, m->S, W, F};
+    EpiPropPair ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
     return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st);
   }
-  EpiProp ep{mode, k, last, m->N, n2, m->S, W, F};
+  EpiProp ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
   return run_bn(m->bn_prop, prec, mp, g, ep, m->err, st);
 }
 
@@ -820,9 +879,28 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     A(alloc_op(m, m->LhX, (size_t)nc * 2 * NAK));
     A(alloc_op(m, m->Gx, (size_t)nw * 2 * NAK * 2));
   }
+  // real half-rotated operands?
+  if (e == cudaSuccess && !getenv("AFQ_MIXED_COMPLEX")) {
+    A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+    check_imag_kernel<<<148 * 8, 256, 0, st>>>(init->SpvnT_dense, (long long)nc * NAK, m->err);
+    if (init->Lh) check_imag_kernel<<<148 * 8, 256, 0, st>>>(init->Lh, (long long)nc * NAK, m->err);
+    int cplx = 1;
+    A(cudaGetLastError());
+    A(cudaMemcpyAsync(&cplx, m->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    A(cudaStreamSynchronize(st));
+    m->greal = e == cudaSuccess && !cplx;
+    A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+    check_imag_kernel<<<148 * 8, 256, 0, st>>>(init->P, (long long)N * N, m->err);
+    cplx = 1;
+    A(cudaGetLastError());
+    A(cudaMemcpyAsync(&cplx, m->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    A(cudaStreamSynchronize(st));
+    m->preal = e == cudaSuccess && !cplx && init->order >= 1;
+    A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+  }
   // split K of the vbias / Coulomb products so the grid covers the GPU
   {
-    const long long Kq = 2 * NAK;
+    const long long Kq = m->greal ? NAK : 2 * NAK;
     const int tiles = ((nc + 127) / 128) * ((2 * nw + 127) / 128);
     int sp = std::max(1, std::min(16, (int)((4 * 148 + tiles - 1) / tiles)));
     long long ks = (Kq + sp - 1) / sp;
@@ -839,9 +917,16 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   pack_spvn_kernel<<<(N * N + 7) / 8, dim3(32, 8), 0, st>>>(init->sp_ri, init->sp_ci, init->sp_v,
                                                             init->sp_rv, N * N, m->Kv, m->s_real,
                                                             m->Sd);
-  pack_complex_kernel<<<grid_for((long long)N * N), 256, 0, st>>>(init->P, (long long)N * N, m->Pf);
-  pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->SpvnT_dense,
-                                                                    (long long)nc * NAK, m->SpT);
+  if (m->preal)
+    pack_real_kernel<<<grid_for((long long)N * N), 256, 0, st>>>(init->P, (long long)N * N, m->Pf);
+  else
+    pack_complex_kernel<<<grid_for((long long)N * N), 256, 0, st>>>(init->P, (long long)N * N, m->Pf);
+  if (m->greal)
+    pack_real_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->SpvnT_dense,
+                                                                   (long long)nc * NAK, m->SpT);
+  else
+    pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->SpvnT_dense,
+                                                                      (long long)nc * NAK, m->SpT);
   for (int i = 0; i < 2; i++) {   // rows the products read past their data stay finite
     A(cudaMemsetAsync(m->F[i].hi, 0, sizeof(bf16) * (size_t)nw * 4 * n * 2 * N, st));
     A(cudaMemsetAsync(m->F[i].lo, 0, sizeof(bf16) * (size_t)nw * 4 * n * 2 * N, st));
@@ -851,7 +936,11 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     A(cudaMemsetAsync(m->TwB.lo, 0, sizeof(bf16) * (size_t)4 * n * 2 * N, st));
     pack_trial_kernel<<<grid_for((long long)N * 2 * n), 256, 0, st>>>(init->trial, N, 2 * n, m->TwB);
   }
-  if (init->Lh) {
+  if (init->Lh && m->greal) {
+    pack_real_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, (long long)nc * NAK,
+                                                                   m->LhJ);
+    pack_lhx_real_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, nc, n, N, m->LhX);
+  } else if (init->Lh) {
     pack_complex_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, (long long)nc * NAK,
                                                                       m->LhJ);
     pack_lhx_kernel<<<grid_for((long long)nc * NAK), 256, 0, st>>>(init->Lh, nc, n, N, m->LhX);
@@ -899,15 +988,17 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv);
   const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
   for (int i = 0; i < 2; i++) {
-    ok &= map2(m->m_pw[i], m->Pf, 2 * N, N, 1, 2 * N, 0, m->F[i], 2 * N, fr, nw, 2 * N, fsz,
-               m->bn_prop);
+    const uint64_t Kp = m->preal ? N : 2 * N;
+    ok &= map2(m->m_pw[i], m->Pf, Kp, N, 1, Kp, 0, m->F[i], Kp, fr, nw, 2 * N, fsz, m->bn_prop);
     ok &= map2(m->m_v[i], m->Vf, 2 * N, N, nw, 2 * N, (uint64_t)N * 2 * N, m->F[i], 2 * N, fr, nw,
                2 * N, fsz, m->bn_prop);
   }
-  ok &= map2(m->m_vbias, m->SpT, 2 * NAK, nc, 1, 2 * NAK, 0, m->Gb, 2 * NAK, 2 * nw, 1, 2 * NAK, 0,
+  const uint64_t Kg = m->greal ? NAK : 2 * NAK;   // K of the vbias / Coulomb products
+  const uint64_t Kx = m->greal ? N : 2 * N;       // K of the exchange product
+  ok &= map2(m->m_vbias, m->SpT, Kg, nc, 1, Kg, 0, m->Gb, Kg, 2 * nw, 1, Kg, 0,
              128);
   if (init->Lh) {
-    ok &= map2(m->m_ej, m->LhJ, 2 * NAK, nc, 1, 2 * NAK, 0, m->Gb, 2 * NAK, 2 * nw, 1, 2 * NAK, 0,
+    ok &= map2(m->m_ej, m->LhJ, Kg, nc, 1, Kg, 0, m->Gb, Kg, 2 * nw, 1, Kg, 0,
                128);
     m->ex_Gn = 128 / n;
     m->ex_Gw = std::max(1, 256 / (2 * n));
@@ -920,8 +1011,8 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
       if (pick_bn(gw * 2 * n) == gw * 2 * n) { m->ex_Gw = gw; m->ex_bn = gw * 2 * n; }
     }
     m->ex_mtiles = (nc + m->ex_Gn - 1) / m->ex_Gn;
-    ok &= map2(m->m_ek, m->LhX, 2 * N, (uint64_t)nc * n, 2, 2 * N, (uint64_t)nc * n * 2 * N, m->Gx,
-               2 * N, (uint64_t)nw * 2 * n, 2, 2 * N, (uint64_t)nw * 2 * n * 2 * N, m->ex_bn);
+    ok &= map2(m->m_ek, m->LhX, Kx, (uint64_t)nc * n, 2, Kx, (uint64_t)nc * n * Kx, m->Gx, Kx,
+               (uint64_t)nw * 2 * n, 2, Kx, (uint64_t)nw * 2 * n * Kx, m->ex_bn);
   }
   if (init->trial && n <= 64) {
     m->bn_t1 = pick_bn(4 * n);
@@ -990,13 +1081,16 @@ cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st) {
 
 cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) {
   const int N = m->N, n2 = 2 * m->n, nw = m->nw;
-  pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0]);
+  const bool pr = m->preal && m->in.order >= 1;
+  pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0],
+                                                                               pr ? 2 : 1);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int mt = (N + 127) / 128;
+  const int Kp = pr ? N : 2 * N;   // K of P W and P S
   int cur = 0;
   {  // S = P W
-    tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, false, true, 0};
+    tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
     if ((e = run_prop(m, m->prec_p, m->m_pw[0], g, 0, 0, 0, nullptr, m->F[1], st)) != cudaSuccess)
       return e;
     cur = 1;
@@ -1010,7 +1104,7 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
     cur ^= 1;
   }
   {  // W = P S (with order 0 the B operand of S = P W is already in F[cur])
-    tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, false, true, 0};
+    tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
     if ((e = run_prop(m, m->prec_p, m->m_pw[cur], g, 2, 0, 0, W, Op{}, st)) != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1019,8 +1113,8 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
 static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, z_t* out,
                                   cudaStream_t st) {
   const int nc = m->nc, nw = m->nw;
-  tc::GemmShape g{nc, 2 * nw, (int)(2 * m->NAK), m->splits, 128, (nc + 127) / 128, false, false,
-                  m->ksplit};
+  tc::GemmShape g{nc, 2 * nw, (int)(m->greal ? m->NAK : 2 * m->NAK), m->splits, 128,
+                  (nc + 127) / 128, false, false, m->ksplit};
   EpiPart ep{m->part, nc, 2 * nw, (long long)nc * 2 * nw};
   cudaError_t e = run_bn(128, prec, mp, g, ep, m->err, st);
   if (e != cudaSuccess) return e;
@@ -1030,7 +1124,7 @@ static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, z
 
 cudaError_t mixed_vbias(MixedState* m, const z_t* Gc, z_t* vbias, cudaStream_t st) {
   pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
-                                                                      Op{});
+                                                                      Op{}, 0, m->greal);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return splitk_product(m, m->m_vbias, m->prec_vbias, vbias, st);
@@ -1040,7 +1134,7 @@ cudaError_t mixed_vbias(MixedState* m, const z_t* Gc, z_t* vbias, cudaStream_t s
 cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t st) {
   if (!m->in.Lh) return cudaErrorInvalidValue;
   pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
-                                                                      Op{});
+                                                                      Op{}, 0, m->greal);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return splitk_product(m, m->m_ej, m->prec_ej, cvec, st);
@@ -1051,11 +1145,12 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
                            cudaStream_t st) {
   if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
   pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(Gc, nsub, m->n, m->N, Op{},
-                                                                     m->Gx, m->nw);
+                                                                     m->Gx, m->nw, m->greal);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int n = m->n;
-  tc::GemmShape g{m->nc * n, nsub * 2 * n, 2 * m->N, 2, m->ex_Gn * n, m->ex_mtiles, true, true, 0};
+  tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
+                  m->ex_mtiles, true, true, 0};
   if (tc_persistent()) {
     switch (2 * n) {   // staged exchange for the compiled walker widths
       case 32: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
