@@ -169,24 +169,48 @@ def fp64_stage_flops(cfg, nw, stage, order=6):
     return 0.0
 
 
-def mixed_propagate_bytes(cfg, nw, order=6):
+def mixed_propagate_bytes(cfg, nw, order=6, preal=True):
     """HBM bytes one mixed-form propagation stage must move with its operand layouts:
     the FP64 walkers in and out, and per product the bf16 operands read once (hi, plus lo
     for the split products), the fp32 Taylor sum read and written, and the next bf16
-    operand written (hi and lo)."""
+    operand written (hi and lo).  With a real Propg1 (preal) the P W and P S products
+    read B operands of K = N (separate Re / Im rows) instead of 2N."""
     N, n = cfg.nmo, cfg.nel
     W64 = nw * N * 2 * n * 16            # FP64 walkers
     F = nw * 4 * n * 2 * N * 2           # one bf16 part of a B operand
+    Fp = F // 2 if preal else F          # B operand of P W / P S
     V = nw * N * 2 * N * 2               # one bf16 part of the V operand
     S = nw * N * 2 * n * 8               # fp32 Taylor sum
     split = {"P": True, "V1": True, "Vk": False}
-    tot = W64 + 2 * F                    # pack W
-    tot += 2 * F + S + 2 * F             # S = P W (split): B hi+lo in, S out, next B out
+    tot = W64 + 2 * Fp                   # pack W
+    tot += 2 * Fp + S + 2 * F            # S = P W (split): B hi+lo in, S out, next B out
     for k in range(1, order + 1):
         sp = split["V1"] if k == 1 else split["Vk"]
-        tot += V * (2 if sp else 1) + F * (2 if sp else 1) + 2 * S + 2 * F
-    tot += 2 * F + W64                   # W = P S (split)
+        nxt = 2 * Fp if k == order else 2 * F
+        tot += V * (2 if sp else 1) + F * (2 if sp else 1) + 2 * S + nxt
+    tot += 2 * Fp + W64                  # W = P S (split)
     return float(tot)
+
+
+def mixed_stage_flops(cfg, nw, stage, real_ops=True, subset=None):
+    """Algorithmic FLOPs of one call of a mixed-form tensor-core stage (complex x complex
+    multiply-add = 8 FLOP, real x complex = 4).  vHS counts the N(N+1)/2 symmetric pairs
+    the dense product evaluates; the energy stage counts the exchange of `subset` walkers
+    and the Coulomb vectors of all walkers.  Split precision executes three tensor-core
+    products per algorithmic product."""
+    N, n, nc = cfg.nmo, cfg.nel, cfg.nchol
+    nak = 2 * n * N
+    f = 4.0 if real_ops else 8.0
+    if stage == "vHS":
+        return 4.0 * nw * (N * (N + 1) // 2) * nc
+    if stage == "vbias":
+        return f * nw * nc * nak
+    if stage == "energy":
+        m = subset if subset is not None else nw
+        return f * nw * nc * nak + f * m * 2 * nc * n * n * N
+    if stage in ("DM", "overlap"):
+        return 8.0 * nw * 2 * (n * n * N + (n * n * N if stage == "DM" else 0))
+    return fp64_stage_flops(cfg, nw, stage)
 
 
 # --------------------------------------------------------------------------- CPU leg
@@ -452,14 +476,19 @@ def main():
                 "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run "
                                "(no FP64 entry in MEASURED_PEAKS.json)"}
     elif dom == "propagate":
-        byt = mixed_propagate_bytes(cfg, nw) * args.steps
+        preal = bool(np.all(np.asarray(s.Propg1).imag == 0))
+        byt = mixed_propagate_bytes(cfg, nw, preal=preal) * args.steps
         achieved = byt / (dom_ms * 1e-3) / 1e9
         roof = {"kernel": "propagate (tcgen05 GEMM chain)", "bound": "hbm", "achieved": achieved,
                 "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                 "peak_source": f"hbm_gbs, {src}"}
     else:
-        calls = args.steps if dom != "energy" else args.steps // args.energy_every
-        achieved = fp64_stage_flops(cfg, nw, dom) * calls / (dom_ms * 1e-3) / 1e12
+        calls = {"DM": args.steps + args.steps // args.energy_every,
+                 "energy": args.steps // args.energy_every}.get(dom, args.steps)
+        real_ops = bool(np.all(s.SpvnT.vals.imag == 0)) and (s.Lh is None or
+                                                             bool(np.all(s.Lh.imag == 0)))
+        sub = (nw + 7) // 8 if head.mode == "cv" else nw
+        achieved = mixed_stage_flops(cfg, nw, dom, real_ops, sub) * calls / (dom_ms * 1e-3) / 1e12
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved,
                 "peak": peaks["bf16_tflops_sustained"], "unit": "TFLOP/s",
                 "frac": achieved / peaks["bf16_tflops_sustained"],

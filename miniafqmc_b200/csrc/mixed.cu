@@ -263,107 +263,139 @@ __global__ void pack_wn_kernel(const z_t* __restrict__ W, long long count, Op ds
   }
 }
 
-// Batched FP64 Gauss-Jordan of the n x n overlap matrices T1 (one 128-thread CTA per
-// walker-spin, matrix in shared memory; warps take rows, lanes columns), pivoting on
-// max |re| + |im| as izamax: det(T1) for the overlap (ma_operations.hpp:244-260) and,
-// when want_inv, T1^-1 written as the B form of the Gc product: rows 2a = (Re y, -Im y),
-// 2a + 1 = (Im y, Re y) along b, y = T1^-1[a][.].
-constexpr int LU_THREADS = 128;
-size_t lu_smem_bytes(int n) { return sizeof(z_t) * ((size_t)n * (n + 1) + n); }
-
-__global__ void __launch_bounds__(LU_THREADS)
-lu_inv_kernel(const float2* __restrict__ T1, int n, int nmat, Op Tinv, z_t* __restrict__ Wd,
+// Batched FP64 Gauss-Jordan of the n x n overlap matrices T1, one CTA per walker-spin
+// with the matrix in registers: thread (r, q) of a GR x GC grid holds the elements
+// (r + GR a, q + GC b).  Pivoting as izamax (max |re| + |im| over the rows not yet used,
+// ma_operations.hpp:244-260), without moving rows: step j pivots on (p_j, j), scales the
+// pivot row, and eliminates column j from every other row (in-place exchange form).
+// Afterwards element (i, c) holds T1^-1[invp(i)][p_c] and det(T1) = sign(p) prod pivots.
+// Writes det (overlap), the singular flag and, when want_inv, T1^-1 as the B form of the
+// Gc product: rows 2a = (Re y, -Im y), 2a + 1 = (Im y, Re y) along b, y = T1^-1[a][.].
+template <int GR, int GC, int RT, int CT>
+__global__ void __launch_bounds__(GR * GC)
+lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ Wd,
               int* __restrict__ info, int want_inv, int save_old) {
-  extern __shared__ __align__(16) unsigned char lu_smem[];
-  __shared__ int perm[64], s_piv;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr int NWARP = LU_THREADS / 32;
-  const int q = blockIdx.x;   // matrix (walker, spin) = w * 2 + s
-  const int ld = n + 1, nn = n * n;
-  z_t* T = reinterpret_cast<z_t*>(lu_smem);
-  z_t* fcol = T + n * ld;
-  const float2* src = T1 + (long long)q * nn;
-  for (int e = tid; e < nn; e += LU_THREADS) {
-    const float2 v = src[e];
-    T[(e / n) * ld + e % n] = zmk(v.x, v.y);
-  }
+  __shared__ z_t prow[64], pcol[64], cval[GR];
+  __shared__ double cmax[GR];
+  __shared__ int cidx[GR], used[64], pivrow[64], invp[64];
+  const int q = blockIdx.x, t = threadIdx.x, r = t / GC, cq = t % GC;
+  const float2* src = T1 + (long long)q * n * n;
+  z_t M[RT][CT];
+#pragma unroll
+  for (int a = 0; a < RT; a++)
+#pragma unroll
+    for (int b = 0; b < CT; b++) {
+      const int i = r + GR * a, c = cq + GC * b;
+      const float2 v = (i < n && c < n) ? src[i * n + c] : make_float2(0.f, 0.f);
+      M[a][b] = zmk(v.x, v.y);
+    }
+  for (int i = t; i < 64; i += GR * GC) used[i] = 0;
   __syncthreads();
   z_t det = zmk(1.0, 0.0);
   int sing = 0;
   for (int j = 0; j < n; j++) {
-    if (warp == 0) {
+    const int jq = j % GC, jb = j / GC;
+    if (cq == jq) {   // candidates of column j among the unused rows this thread holds
       double best = -1.0;
       int bi = n;
-      for (int i = j + lane; i < n; i += 32) {
-        const double v = zabs1(T[i * ld + j]);
-        if (v > best) { best = v; bi = i; }
-      }
+      z_t bv = zmk(0, 0);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      for (int a = 0; a < RT; a++) {
+        const int i = r + GR * a;
+        z_t v = zmk(0, 0);
+#pragma unroll
+        for (int b = 0; b < CT; b++)
+          if (b == jb) v = M[a][b];
+        if (i < n && !used[i]) {
+          const double m = zabs1(v);
+          if (m > best) { best = m; bi = i; bv = v; }
+        }
       }
-      if (lane == 0) { s_piv = bi; perm[j] = bi; }
+      cmax[r] = best;
+      cidx[r] = bi;
+      cval[r] = bv;
     }
     __syncthreads();
-    const int p = s_piv;
-    if (p != j)
-      for (int c = tid; c < n; c += LU_THREADS) {
-        const z_t t = T[j * ld + c];
-        T[j * ld + c] = T[p * ld + c];
-        T[p * ld + c] = t;
-      }
-    __syncthreads();
-    const z_t pv = T[j * ld + j];
-    if (pv.x == 0.0 && pv.y == 0.0) { sing = 1; break; }   // uniform across the CTA
+    double best = -1.0;
+    int p = n;
+    z_t pv = zmk(0, 0);
+    for (int g = 0; g < GR; g++)
+      if (cmax[g] > best || (cmax[g] == best && cidx[g] < p)) { best = cmax[g]; p = cidx[g]; pv = cval[g]; }
+    if (!(best > 0.0)) { sing = 1; break; }   // uniform: every thread read the same values
     det = zmul(det, pv);
-    if (p != j) det = zmk(-det.x, -det.y);
     const z_t inv = zrecip(pv);
-    if (!want_inv) {   // LU: eliminate below the pivot only
-      for (int i = j + 1 + warp; i < n; i += NWARP) {
-        const z_t f = zmul(T[i * ld + j], inv);
-        for (int c = j + 1 + lane; c < n; c += 32)
-          T[i * ld + c] = zsub(T[i * ld + c], zmul(f, T[j * ld + c]));
+    const int pr = p % GR, pa = p / GR;
+    if (r == pr) {
+#pragma unroll
+      for (int a = 0; a < RT; a++)
+        if (a == pa)
+#pragma unroll
+          for (int b = 0; b < CT; b++) {
+            const int c = cq + GC * b;
+            if (c < n) prow[c] = (c == j) ? inv : zmul(M[a][b], inv);
+          }
+    }
+    if (cq == jq) {
+#pragma unroll
+      for (int a = 0; a < RT; a++) {
+        const int i = r + GR * a;
+        z_t v = zmk(0, 0);
+#pragma unroll
+        for (int b = 0; b < CT; b++)
+          if (b == jb) v = M[a][b];
+        if (i < n) pcol[i] = v;
       }
-    } else {
-      for (int i = tid; i < n; i += LU_THREADS) fcol[i] = T[i * ld + j];
-      __syncthreads();
-      for (int c = tid; c < n; c += LU_THREADS) T[j * ld + c] = (c == j) ? inv : zmul(T[j * ld + c], inv);
-      __syncthreads();
-      for (int i = warp; i < n; i += NWARP) {
-        if (i == j) continue;
-        const z_t f = fcol[i];
-        for (int c = lane; c < n; c += 32) {
-          const z_t base = (c == j) ? zmk(0, 0) : T[i * ld + c];
-          T[i * ld + c] = zsub(base, zmul(f, T[j * ld + c]));
+    }
+    __syncthreads();
+    z_t rowv[CT];
+#pragma unroll
+    for (int b = 0; b < CT; b++) {
+      const int c = cq + GC * b;
+      rowv[b] = c < n ? prow[c] : zmk(0, 0);
+    }
+#pragma unroll
+    for (int a = 0; a < RT; a++) {
+      const int i = r + GR * a;
+      if (i >= n) continue;
+      if (i == p) {
+#pragma unroll
+        for (int b = 0; b < CT; b++) M[a][b] = rowv[b];
+      } else {
+        const z_t f = pcol[i];
+#pragma unroll
+        for (int b = 0; b < CT; b++) {
+          const z_t base = (cq + GC * b == j) ? zmk(0, 0) : M[a][b];
+          M[a][b] = zsub(base, zmul(f, rowv[b]));
         }
       }
     }
+    if (t == 0) { used[p] = 1; pivrow[j] = p; }
     __syncthreads();
   }
   if (sing) det = zmk(0, 0);
-  if (want_inv) {
-    if (!sing)
-      for (int j = n - 1; j >= 0; j--) {   // undo the row interchanges on the columns
-        const int p = perm[j];
-        if (p != j)
-          for (int r = tid; r < n; r += LU_THREADS) {
-            const z_t t = T[r * ld + j];
-            T[r * ld + j] = T[r * ld + p];
-            T[r * ld + p] = t;
-          }
-        __syncthreads();
-      }
-    const long long base = (long long)q * 2 * n * 2 * n;
-    for (int e = tid; e < nn; e += LU_THREADS) {
-      const int a = e / n, b = e % n;
-      const z_t y = sing ? zmk(0, 0) : T[a * ld + b];
-      put2(Tinv, base + (2LL * a) * 2 * n + 2 * b, (float)y.x, (float)-y.y);
-      put2(Tinv, base + (2LL * a + 1) * 2 * n + 2 * b, (float)y.y, (float)y.x);
-    }
+  if (t == 0 && !sing) {   // sign of the permutation j -> p_j (inversion count)
+    int inv_cnt = 0;
+    for (int a = 0; a < n; a++)
+      for (int b = a + 1; b < n; b++) inv_cnt += pivrow[a] > pivrow[b];
+    if (inv_cnt & 1) det = zmk(-det.x, -det.y);
+    for (int a = 0; a < n; a++) invp[pivrow[a]] = a;
   }
-  if (tid == 0) {
+  __syncthreads();
+  if (want_inv) {
+    const long long base = (long long)q * 2 * n * 2 * n;
+#pragma unroll
+    for (int a = 0; a < RT; a++)
+#pragma unroll
+      for (int b = 0; b < CT; b++) {
+        const int i = r + GR * a, c = cq + GC * b;
+        if (i >= n || c >= n) continue;
+        const int ra = sing ? i : invp[i], cb = sing ? c : pivrow[c];
+        const z_t y = sing ? zmk(0, 0) : M[a][b];
+        put2(Tinv, base + (2LL * ra) * 2 * n + 2 * cb, (float)y.x, (float)-y.y);
+        put2(Tinv, base + (2LL * ra + 1) * 2 * n + 2 * cb, (float)y.y, (float)y.x);
+      }
+  }
+  if (t == 0) {
     const int w = q >> 1, sp = q & 1;
     z_t* d = Wd + (long long)w * 8;
     if (save_old) {
@@ -373,6 +405,21 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, int nmat, Op Tinv, z_t* __re
     d[2 + sp] = det;
     info[q] = sing;
   }
+}
+
+cudaError_t launch_lu(const float2* T1, int n, int nmat, Op Tinv, z_t* Wd, int* info, int want_inv,
+                      int save_old, cudaStream_t st) {
+  if (n <= 16)
+    lu_inv_kernel<8, 8, 2, 2><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+  else if (n <= 32)
+    lu_inv_kernel<8, 8, 4, 4><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+  else if (n <= 48)
+    lu_inv_kernel<8, 8, 6, 6><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+  else if (n <= 64)
+    lu_inv_kernel<16, 8, 4, 8><<<nmat, 128, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+  else
+    return cudaErrorInvalidValue;
+  return cudaGetLastError();
 }
 
 // Gc [nw][2][n][N] -> Gb [2nw][2*NAK] (vbias / Coulomb B form) and, when Gx.hi is set,
@@ -1183,17 +1230,9 @@ cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, i
     if ((e = run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st)) != cudaSuccess)
       return e;
   }
-  static size_t attr = 0;
-  const size_t smem = lu_smem_bytes(n);
-  if (smem > attr) {
-    if ((e = cudaFuncSetAttribute(lu_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)smem)) != cudaSuccess)
-      return e;
-    attr = smem;
-  }
-  lu_inv_kernel<<<2 * nw, LU_THREADS, smem, st>>>(m->T1, n, 2 * nw, m->Tinv, Wd, info, want_gc,
-                                                  save_old);
-  if ((e = cudaGetLastError()) != cudaSuccess || !want_gc) return e;
+  if ((e = launch_lu(m->T1, n, 2 * nw, m->Tinv, Wd, info, want_gc, save_old, st)) != cudaSuccess ||
+      !want_gc)
+    return e;
   pack_wn_kernel<<<grid_for((long long)nw * N * n2), 256, 0, st>>>(W, (long long)nw * N * n2, m->Wn);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   for (int sp = 0; sp < 2; sp++) {
