@@ -452,8 +452,27 @@ def main():
                        "mean_E_fp64": float(E6.mean()), "abs_dE_Ha": float(abs(Em.mean() - E6.mean())),
                        "max_abs_dE_per_measurement_Ha": float(np.max(np.abs(Em - E6))),
                        "err_per_wall_s": {"form": eps_m, "fp64": eps_6,
-                                          "fp64_over_form": eps_6 / eps_m}},
+                                          "fp64_over_form": eps_6 / eps_m,
+                                          "definition": "sigma_E * sqrt(timed seconds); sigma_E "
+                                          "from the weighted walker spread of each measurement "
+                                          "(plus the subset-correction variance for the control "
+                                          "variate), combined over the measurements"}},
         }
+        # the same walkers measured by both forms: the mixed form's deterministic energy
+        # error against FP64, and the control-variate estimate against exact exchange
+        W, Wd = head.eng.get_walkers()
+        ref.eng.set_walkers(W, Wd)
+        ref.eng.calculate_mixed_density_matrix()
+        e64 = ref.eng.calculate_energy("chol")
+        head.eng.calculate_mixed_density_matrix()
+        same = {"E_fp64_Ha": e64}
+        if head.mode == "cv":
+            ecv = head.eng.calculate_energy("cv")
+            same["cv_minus_fp64_Ha"] = ecv - e64
+            same["cv_sigma_Ha"] = float(np.sqrt(head.eng.cv_stats()["subset_var"]))
+        emx = head.eng.calculate_energy("chol")
+        same["mixed_exact_minus_fp64_Ha"] = emx - e64
+        cmp["energy"]["same_walkers"] = same
         ref.eng.close()
 
     if rank != 0:

@@ -53,6 +53,9 @@ struct afq_handle {
   afq::CvConfig cv_cfg;
 
   cudaGraphExec_t g_plain = nullptr, g_ortho = nullptr;
+  // mixed form: the T1^-1 of the last overlap / density-matrix call matches the current
+  // walkers (cleared by propagate, orthogonalise and set_walkers)
+  bool dm_cache = false;
   long long g_plain_launches[AFQ_NSTAGES] = {0}, g_ortho_launches[AFQ_NSTAGES] = {0};
   unsigned long long host_seed = ~0ull, host_step = ~0ull;
 
@@ -205,9 +208,15 @@ afq_status need_ready(afq_handle* h) {
 }
 
 // ------------------------------------------------------------ stage bodies (async)
+bool mixed_dm_on(const afq_handle* h) { return h->mixed && afq::mixed_has_dm(h->mixed); }
+
 cudaError_t body_dm(afq_handle* h, int want_gc, int save_old) {
-  if (h->mixed && afq::mixed_has_dm(h->mixed))
-    return afq::mixed_dm(h->mixed, h->W, h->Gc, h->Wd, h->info, want_gc, save_old, h->st);
+  if (mixed_dm_on(h)) {
+    cudaError_t e = afq::mixed_dm(h->mixed, h->W, h->Gc, h->Wd, h->info, want_gc, save_old,
+                                  h->dm_cache ? 1 : 0, h->st);
+    h->dm_cache = e == cudaSuccess;
+    return e;
+  }
   return afq::launch_dm(h->W, h->tw, h->N, h->n, h->nw, h->Gc, h->Wd, h->info, want_gc, save_old,
                         h->st);
 }
@@ -235,6 +244,7 @@ cudaError_t body_vhs(afq_handle* h) {
 }
 
 cudaError_t body_propagate(afq_handle* h) {
+  h->dm_cache = false;
   if (h->mixed) return afq::mixed_propagate(h->mixed, h->W, h->vHS, h->st);
   const int N = h->N, n2 = 2 * h->n, nw = h->nw;
   const long long sWN = (long long)N * n2, sV = (long long)N * N;
@@ -267,6 +277,7 @@ cudaError_t body_weights(afq_handle* h, int update_eshift) {
 // The FP64 form keeps LAPACK's Householder convention (raw overlaps match the
 // reference); the mixed form uses CholeskyQR2, equal up to column signs.
 cudaError_t body_ortho(afq_handle* h) {
+  h->dm_cache = false;
   if (h->mixed) return afq::launch_ortho_cholqr(h->W, h->N, h->n, h->nw, h->info, h->st);
   return afq::launch_ortho(h->W, h->N, h->n, h->nw, h->st);
 }
@@ -311,7 +322,7 @@ cudaError_t body_energy(afq_handle* h, int mode) {
 // Timed / counted stages.  The launch counts are the kernels each body issues.
 cudaError_t st_dm(afq_handle* h, int want_gc, int save_old) {
   const int stage = want_gc ? AFQ_STAGE_DM : AFQ_STAGE_OVERLAP;
-  const int nl = (h->mixed && afq::mixed_has_dm(h->mixed)) ? afq::mixed_launches(h->mixed, stage) : 1;
+  const int nl = !mixed_dm_on(h) ? 1 : (want_gc && h->dm_cache) ? 3 : afq::mixed_launches(h->mixed, stage);
   return staged(h, stage, nl, [&] { return body_dm(h, want_gc, save_old); });
 }
 cudaError_t st_vbias(afq_handle* h) {
@@ -559,6 +570,7 @@ afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data)
   AFQ_CUDA(h, cudaMemcpyAsync(h->Wd, W_data, sizeof(z_t) * nw * 8, cudaMemcpyHostToDevice, h->st));
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
   h->have_walkers = true;
+  h->dm_cache = false;
   return AFQ_OK;
 }
 
@@ -762,6 +774,9 @@ afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int nort
   if (seed != h->host_seed || step_tot != h->host_step)
     if ((s = set_scalars(h, seed, step_tot)) != AFQ_OK) return s;
   const bool ortho = step_tot > 0 && step_tot % (uint64_t)northo == 0;
+  // the captured substep starts with a density matrix formed from the cached T1^-1 (and
+  // ends with an overlap call that leaves it valid): refresh it first when it is stale
+  if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
   cudaGraphExec_t* slot = ortho ? &h->g_ortho : &h->g_plain;
   long long* counts = ortho ? h->g_ortho_launches : h->g_plain_launches;
   if (!*slot) {

@@ -34,10 +34,11 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
                            cudaStream_t st);
 // Mixed density matrix: T1 = W^T tw in split bf16 on tensor cores, FP64 Gauss-Jordan for
 // det(T1) (-> W_data overlaps, info) and T1^-1, Gc = T1^-1 W^T on tensor cores.
-// want_gc == 0 computes the overlaps only.
+// want_gc == 0 computes the overlaps (and keeps T1^-1); cached != 0 forms Gc from the
+// T1^-1 of an earlier call on the same walkers.
 bool mixed_has_dm(const MixedState* m);
 cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, int want_gc,
-                     int save_old, cudaStream_t st);
+                     int save_old, int cached, cudaStream_t st);
 // Kernels one call of a stage issues (afq_stage numbering), for the launch counters.
 int mixed_launches(const MixedState* m, int stage);
 // Cholesky-vector blocks of the exchange partial sums (Kpart[nw][2][nblk]).

@@ -37,17 +37,19 @@ struct Op {
   bf16* lo = nullptr;
 };
 
+// (an operand whose consumer runs plain bf16 is passed with lo == nullptr: hi only)
 AFQ_D void put2(const Op& o, long long idx, float a, float b) {
   bf162 h = __floats2bfloat162_rn(a, b);
-  float2 hf = __bfloat1622float2(h);
-  bf162 l = __floats2bfloat162_rn(a - hf.x, b - hf.y);
   *reinterpret_cast<bf162*>(o.hi + idx) = h;
-  *reinterpret_cast<bf162*>(o.lo + idx) = l;
+  if (o.lo) {
+    float2 hf = __bfloat1622float2(h);
+    *reinterpret_cast<bf162*>(o.lo + idx) = __floats2bfloat162_rn(a - hf.x, b - hf.y);
+  }
 }
 AFQ_D void put1(const Op& o, long long idx, float a) {
   bf16 h = __float2bfloat16_rn(a);
   o.hi[idx] = h;
-  o.lo[idx] = __float2bfloat16_rn(a - __bfloat162float(h));
+  if (o.lo) o.lo[idx] = __float2bfloat16_rn(a - __bfloat162float(h));
 }
 AFQ_D float2 get2(const Op& o, long long idx) {
   float2 h = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.hi + idx));
@@ -1097,7 +1099,7 @@ int mixed_launches(const MixedState* m, int stage) {
     case 3: return 2;                                  // pack, GEMM (vHS)
     case 4: return 2 + m->in.order + 1;                // pack, P W, order terms, P S
     case 8: return m->in.Lh ? 4 : 0;                   // pack, E_J GEMM, reduce, E_K GEMM
-    case 0: return 6;                                  // pack, T1, LU, pack, Gc x 2
+    case 0: return 6;                                  // pack, T1, LU, pack, Gc x 2 (3 cached)
     case 5: return 3;                                  // pack, T1, LU (overlaps)
   }
   return 0;
@@ -1126,6 +1128,9 @@ cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// B operand of the next product: the lo part only when that product runs split
+static Op next_op(const Op& F, int prec) { return prec == PREC_SPLIT ? F : Op{F.hi, nullptr}; }
+
 cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) {
   const int N = m->N, n2 = 2 * m->n, nw = m->nw;
   const bool pr = m->preal && m->in.order >= 1;
@@ -1138,14 +1143,17 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
   int cur = 0;
   {  // S = P W
     tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
-    if ((e = run_prop(m, m->prec_p, m->m_pw[0], g, 0, 0, 0, nullptr, m->F[1], st)) != cudaSuccess)
+    if ((e = run_prop(m, m->prec_p, m->m_pw[0], g, 0, 0, 0, nullptr, next_op(m->F[1], m->prec_v1),
+                      st)) != cudaSuccess)
       return e;
     cur = 1;
   }
   for (int k = 1; k <= m->in.order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
     tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, true, true, 0};
     int prec = k == 1 ? m->prec_v1 : m->prec_vk;
-    if ((e = run_prop(m, prec, m->m_v[cur], g, 1, k, k == m->in.order, nullptr, m->F[cur ^ 1],
+    const int nprec = k < m->in.order ? m->prec_vk : m->prec_p;   // precision of the next product
+    if ((e = run_prop(m, prec, m->m_v[cur], g, 1, k, k == m->in.order, nullptr,
+                      next_op(m->F[cur ^ 1], nprec),
                       st)) != cudaSuccess)
       return e;
     cur ^= 1;
@@ -1217,22 +1225,25 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
 
 bool mixed_has_dm(const MixedState* m) { return m && m->T1 && m->bn_t1 && m->bn_gc; }
 
-// Overlaps (want_gc == 0) or the full mixed density matrix of every walker.
+// Overlaps (want_gc == 0) or the full mixed density matrix of every walker.  Both compute
+// T1^-1 (kept in Tinv); cached != 0 reuses the T1^-1 of an earlier call on the same W.
 cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, int want_gc,
-                     int save_old, cudaStream_t st) {
+                     int save_old, int cached, cudaStream_t st) {
   if (!mixed_has_dm(m)) return cudaErrorInvalidValue;
   const int N = m->N, n = m->n, n2 = 2 * n, nw = m->nw;
+  cudaError_t e;
+  if (cached && want_gc) goto gc;
   pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0], 0);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   {  // T1 (conjugated) of both spins: one 128-row tile per walker
     tc::GemmShape g{128, 4 * n, 2 * N, nw, 128, 1, true, false, 0};
     if ((e = run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st)) != cudaSuccess)
       return e;
   }
-  if ((e = launch_lu(m->T1, n, 2 * nw, m->Tinv, Wd, info, want_gc, save_old, st)) != cudaSuccess ||
+  if ((e = launch_lu(m->T1, n, 2 * nw, m->Tinv, Wd, info, 1, save_old, st)) != cudaSuccess ||
       !want_gc)
     return e;
+gc:
   pack_wn_kernel<<<grid_for((long long)nw * N * n2), 256, 0, st>>>(W, (long long)nw * N * n2, m->Wn);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   for (int sp = 0; sp < 2; sp++) {
