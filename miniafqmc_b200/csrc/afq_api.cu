@@ -56,6 +56,10 @@ struct afq_handle {
   // mixed form: the T1^-1 of the last overlap / density-matrix call matches the current
   // walkers (cleared by propagate, orthogonalise and set_walkers)
   bool dm_cache = false;
+  // mixed form: energies are measured on an FP64 density matrix (dm_kernel) whose
+  // overlaps go to scratch, so the walkers' W_data keeps the propagation's values
+  z_t* Wd_scr = nullptr;
+  int* info_scr = nullptr;
   long long g_plain_launches[AFQ_NSTAGES] = {0}, g_ortho_launches[AFQ_NSTAGES] = {0};
   unsigned long long host_seed = ~0ull, host_step = ~0ull;
 
@@ -743,10 +747,32 @@ afq_status energy_cv(afq_handle* h, double* sums) {
   return AFQ_OK;
 }
 
+// The E1 term of the energy is a sum of G over all orbitals: its relative error is that
+// of G (a few 1e-6 of E1 with the tensor-core G at 48+48 electrons), so the mixed form
+// measures on an FP64 G; the two-body terms keep the tensor-core contractions.
+// AFQ_MIXED_ENERGY_G=mixed keeps the tensor-core G.
+cudaError_t energy_density_matrix(afq_handle* h) {
+  static const bool keep = getenv("AFQ_MIXED_ENERGY_G") &&
+                           std::string(getenv("AFQ_MIXED_ENERGY_G")) == "mixed";
+  if (!h->mixed || keep) return cudaSuccess;
+  cudaError_t e = cudaSuccess;
+  if (!h->Wd_scr && (e = cudaMalloc(&h->Wd_scr, sizeof(z_t) * (size_t)h->nw * 8)) == cudaSuccess)
+    h->allocs.push_back(h->Wd_scr);
+  if (e == cudaSuccess && !h->info_scr &&
+      (e = cudaMalloc(&h->info_scr, sizeof(int) * 2 * (size_t)h->nw)) == cudaSuccess)
+    h->allocs.push_back(h->info_scr);
+  if (e != cudaSuccess) return e;
+  return staged(h, AFQ_STAGE_ENERGY, 1, [&] {
+    return afq::launch_dm(h->W, h->tw, h->N, h->n, h->nw, h->Gc, h->Wd_scr, h->info_scr, 1, 0,
+                          h->st);
+  });
+}
+
 afq_status afq_energy_sums(afq_handle* h, int mode, double* sums) {
   afq_status s = need_ready(h);
   if (s != AFQ_OK) return s;
   if (!sums) return fail(h, AFQ_ERR_ARG, "null sums");
+  if (mode != AFQ_ENERGY_VAKBL) AFQ_CUDA(h, energy_density_matrix(h));
   if (mode == AFQ_ENERGY_CV) return energy_cv(h, sums);
   if (mode == AFQ_ENERGY_VAKBL && !h->have_vakbl) return fail(h, AFQ_ERR_STATE, "no Vakbl loaded");
   if (mode == AFQ_ENERGY_CHOLESKY && !h->Lh) return fail(h, AFQ_ERR_STATE, "no Lhalf loaded");

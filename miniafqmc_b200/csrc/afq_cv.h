@@ -33,6 +33,7 @@ struct CvConfig {
   long long train_walker_steps = 2000;   // exact samples gathered before the estimator
   int subset_den = 8;                     // exact exchange on nw / subset_den walkers
   int iters_warm = 200, iters_online = 20;
+  int batch_online = 1024;                // samples per online Adam step (a window of the buffer)
 };
 
 struct CvState;

@@ -483,9 +483,19 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
         s->buf_t);
     s->launches++;
     const int iters = first ? s->cfg.iters_warm : s->cfg.iters_online;
-    if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, &s->last_loss,
-                       st)) != cudaSuccess)
-      return e;
+    const int bb = s->cfg.batch_online;
+    if (first || bb <= 0 || s->buf_n <= bb) {   // full-buffer steps
+      if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, &s->last_loss,
+                         st)) != cudaSuccess)
+        return e;
+    } else {   // online: each step on the next contiguous window of bb buffered samples
+      for (int it = 0; it < iters; it++) {
+        const long long off = ((s->meas * iters + it) * (long long)bb) % (s->buf_n - bb + 1);
+        if ((e = mlp_train(s->mlp, s->buf_x + off * CV_NIN, s->buf_t + off, bb, 1, s->cfg.lr,
+                           it == iters - 1 ? &s->last_loss : nullptr, st)) != cudaSuccess)
+          return e;
+      }
+    }
     s->launches += 10LL * iters;
     if (!std::isfinite(s->last_loss)) s->failed = true;
   }

@@ -266,21 +266,25 @@ __global__ void pack_wn_kernel(const z_t* __restrict__ W, long long count, Op ds
 }
 
 // Batched FP64 Gauss-Jordan of the n x n overlap matrices T1, one CTA per walker-spin
-// with the matrix in registers: thread (r, q) of a GR x GC grid holds the elements
-// (r + GR a, q + GC b).  Pivoting as izamax (max |re| + |im| over the rows not yet used,
-// ma_operations.hpp:244-260), without moving rows: step j pivots on (p_j, j), scales the
-// pivot row, and eliminates column j from every other row (in-place exchange form).
-// Afterwards element (i, c) holds T1^-1[invp(i)][p_c] and det(T1) = sign(p) prod pivots.
-// Writes det (overlap), the singular flag and, when want_inv, T1^-1 as the B form of the
-// Gc product: rows 2a = (Re y, -Im y), 2a + 1 = (Im y, Re y) along b, y = T1^-1[a][.].
+// with the matrix in registers: thread (r, q), numbered t = q * GR + r so that a column's
+// owners are consecutive lanes, holds the elements (r + GR a, q + GC b).  Pivoting as
+// izamax (max |re| + |im| over the rows not yet used, ma_operations.hpp:244-260), without
+// moving rows: step j pivots on (p_j, j), scales the pivot row and eliminates column j
+// from every other row (in-place exchange form).  Afterwards element (i, c) holds
+// T1^-1[invp(i)][p_c] and det(T1) = sign(p) prod pivots.  Writes det (overlap), the
+// singular flag and, when want_inv, T1^-1 as the B form of the Gc product:
+// rows 2a = (Re y, -Im y), 2a + 1 = (Im y, Re y) along b, y = T1^-1[a][.].
+// Per step: the column's owners (GR consecutive lanes) pick the pivot with shuffles, one
+// barrier publishes it, a second one publishes the scaled pivot row and the column.
 template <int GR, int GC, int RT, int CT>
 __global__ void __launch_bounds__(GR * GC)
 lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ Wd,
               int* __restrict__ info, int want_inv, int save_old) {
-  __shared__ z_t prow[64], pcol[64], cval[GR];
-  __shared__ double cmax[GR];
-  __shared__ int cidx[GR], used[64], pivrow[64], invp[64];
-  const int q = blockIdx.x, t = threadIdx.x, r = t / GC, cq = t % GC;
+  static_assert(GR == 8 || GR == 16, "a column's owners fill a half warp or a quarter");
+  __shared__ z_t prow[64], pcol[64];
+  __shared__ z_t s_pv;
+  __shared__ int s_p, pivrow[64], invp[64];
+  const int q = blockIdx.x, t = threadIdx.x, cq = t / GR, r = t % GR;
   const float2* src = T1 + (long long)q * n * n;
   z_t M[RT][CT];
 #pragma unroll
@@ -291,13 +295,12 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
       const float2 v = (i < n && c < n) ? src[i * n + c] : make_float2(0.f, 0.f);
       M[a][b] = zmk(v.x, v.y);
     }
-  for (int i = t; i < 64; i += GR * GC) used[i] = 0;
-  __syncthreads();
+  unsigned used = 0;   // bit a: row r + GR a is a pivot row already
   z_t det = zmk(1.0, 0.0);
   int sing = 0;
   for (int j = 0; j < n; j++) {
     const int jq = j % GC, jb = j / GC;
-    if (cq == jq) {   // candidates of column j among the unused rows this thread holds
+    if (cq == jq) {   // owners of column j: pivot among their unused rows, then shuffles
       double best = -1.0;
       int bi = n;
       z_t bv = zmk(0, 0);
@@ -308,26 +311,37 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
 #pragma unroll
         for (int b = 0; b < CT; b++)
           if (b == jb) v = M[a][b];
-        if (i < n && !used[i]) {
+        if (i < n && !((used >> a) & 1u)) {
           const double m = zabs1(v);
           if (m > best) { best = m; bi = i; bv = v; }
         }
       }
-      cmax[r] = best;
-      cidx[r] = bi;
-      cval[r] = bv;
+      // the GR owners are consecutive lanes of one warp: shuffle among them only
+      const unsigned grp = ((1u << GR) - 1u) << ((t & 31) & ~(GR - 1));
+#pragma unroll
+      for (int o = GR / 2; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(grp, best, o);
+        const int oi = __shfl_xor_sync(grp, bi, o);
+        const double ovx = __shfl_xor_sync(grp, bv.x, o);
+        const double ovy = __shfl_xor_sync(grp, bv.y, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; bv = zmk(ovx, ovy); }
+      }
+      if (r == 0) {
+        s_p = best > 0.0 ? bi : -1;   // exactly singular: no nonzero candidate
+        s_pv = bv;
+      }
     }
     __syncthreads();
-    double best = -1.0;
-    int p = n;
-    z_t pv = zmk(0, 0);
-    for (int g = 0; g < GR; g++)
-      if (cmax[g] > best || (cmax[g] == best && cidx[g] < p)) { best = cmax[g]; p = cidx[g]; pv = cval[g]; }
-    if (!(best > 0.0)) { sing = 1; break; }   // uniform: every thread read the same values
-    det = zmul(det, pv);
-    const z_t inv = zrecip(pv);
+    const int p = s_p;
+    if (p < 0) { sing = 1; break; }   // uniform across the CTA
+    const z_t pv = s_pv;
+    if (t == 0) {
+      det = zmul(det, pv);
+      pivrow[j] = p;
+    }
     const int pr = p % GR, pa = p / GR;
-    if (r == pr) {
+    if (r == pr) {   // pivot-row owners publish the scaled row
+      const z_t inv = zrecip(pv);
 #pragma unroll
       for (int a = 0; a < RT; a++)
         if (a == pa)
@@ -336,8 +350,9 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
             const int c = cq + GC * b;
             if (c < n) prow[c] = (c == j) ? inv : zmul(M[a][b], inv);
           }
+      used |= 1u << pa;
     }
-    if (cq == jq) {
+    if (cq == jq) {   // column owners publish column j
 #pragma unroll
       for (int a = 0; a < RT; a++) {
         const int i = r + GR * a;
@@ -371,8 +386,8 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
         }
       }
     }
-    if (t == 0) { used[p] = 1; pivrow[j] = p; }
-    __syncthreads();
+    // prow / pcol are rewritten only after the next step's first barrier, which every
+    // thread reaches after finishing this update
   }
   if (sing) det = zmk(0, 0);
   if (t == 0 && !sing) {   // sign of the permutation j -> p_j (inversion count)
@@ -411,14 +426,15 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
 
 cudaError_t launch_lu(const float2* T1, int n, int nmat, Op Tinv, z_t* Wd, int* info, int want_inv,
                       int save_old, cudaStream_t st) {
+  // 16 x 16 threads per matrix: few registers per thread, many warps per SM
   if (n <= 16)
     lu_inv_kernel<8, 8, 2, 2><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
   else if (n <= 32)
-    lu_inv_kernel<8, 8, 4, 4><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+    lu_inv_kernel<16, 16, 2, 2><<<nmat, 256, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
   else if (n <= 48)
-    lu_inv_kernel<8, 8, 6, 6><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+    lu_inv_kernel<16, 16, 3, 3><<<nmat, 256, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
   else if (n <= 64)
-    lu_inv_kernel<16, 8, 4, 8><<<nmat, 128, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+    lu_inv_kernel<16, 16, 4, 4><<<nmat, 256, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();
@@ -494,6 +510,7 @@ int grid_for(long long n) { return (int)std::min<long long>((n + 255) / 256, 148
 // chunk, the odd lane columns 16-31, as (re, im) pairs of V_w[ik].
 struct EpiVhs {
   static constexpr bool kTile = false, kPair = false;
+  static constexpr bool kPerTile = true;
   Op V;
   int nw;
   long long nik;
@@ -555,6 +572,7 @@ struct EpiGc {
 // diagonal, to V[j][i].
 struct EpiVhsSym {
   static constexpr bool kTile = false, kPair = false;
+  static constexpr bool kPerTile = true;   // measured faster than the persistent kernel
   Op V;
   int nw, N;
   const int* pairs;
@@ -753,16 +771,23 @@ struct EpiExchangeStaged {
         for (int i = 0; i < 32; i++) scr[row * LD + q * 32 + i] = v[i];
       }
       tc::epi_bar_group(wg);
+      // thread `row` = (cv, a) sums T[a][b] T[b][a] over b: its own staged row and the
+      // column a of the same Cholesky vector (both bank-conflict free, LD = 1 mod 32);
+      // fp32 products over n terms, double across threads
       double sr = 0.0, si = 0.0;
-      for (int cv = 0; cv < ncv; cv++) {
-        const float* rows = scr + cv * n * LD;
-        for (int q = row; q < n * n; q += 128) {
-          const int a = q / n, b = q % n;
-          const double ar = rows[a * LD + b], ai = rows[a * LD + n + b];
-          const double br = rows[b * LD + a], bi = rows[b * LD + n + a];
-          sr += ar * br - ai * bi;
-          si += ar * bi + ai * br;
+      if (row < ncv * n) {
+        const int cv = row / n, a = row - cv * n;
+        const float* own = scr + row * LD;
+        const float* col = scr + cv * n * LD + a;
+        float fr = 0.0f, fi = 0.0f;
+        for (int b = 0; b < n; b++) {
+          const float ar = own[b], ai = own[n + b];
+          const float br = col[b * LD], bi = col[b * LD + n];
+          fr = fmaf(ar, br, fmaf(-ai, bi, fr));
+          fi = fmaf(ar, bi, fmaf(ai, br, fi));
         }
+        sr = fr;
+        si = fi;
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -799,7 +824,7 @@ bool tc_persistent() {
 template <int BN, int ST, bool SPLIT, class Epi, int MINB = 1>
 cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
                      cudaStream_t st) {
-  if constexpr (!Epi::kTile) {
+  if constexpr (!Epi::kTile && !tc::EpiPerTile<Epi>::value) {
     constexpr int PST = SPLIT ? 2 : 4;
     constexpr int WG = tc::EpiStaged<Epi>::value ? 1 : 2;
     if (tc_persistent() || tc::EpiStaged<Epi>::value) {

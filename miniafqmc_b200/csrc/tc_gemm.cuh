@@ -166,6 +166,10 @@ AFQ_D void epi_bar_group(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) 
 template <class E, class = void> struct EpiStaged : std::false_type {};
 template <class E>
 struct EpiStaged<E, std::void_t<decltype(E::kStaged)>> : std::integral_constant<bool, E::kStaged> {};
+// kPerTile functors run on the per-tile kernel even when the persistent one is enabled.
+template <class E, class = void> struct EpiPerTile : std::false_type {};
+template <class E>
+struct EpiPerTile<E, std::void_t<decltype(E::kPerTile)>> : std::integral_constant<bool, E::kPerTile> {};
 template <class E, class = void> struct EpiScratch : std::integral_constant<int, 0> {};
 template <class E>
 struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
