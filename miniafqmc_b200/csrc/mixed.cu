@@ -15,6 +15,7 @@
 //   E_K   : T_cw = Lh_c Gc_w^T per spin, trace of T^2 from the tile in shared memory
 // LU/overlaps, orthogonalisation, weights and the energy assembly stay FP64.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -30,15 +31,32 @@ namespace afq {
 typedef __nv_bfloat16 bf16;
 typedef __nv_bfloat162 bf162;
 
-enum { PREC_BF16 = 0, PREC_SPLIT = 1 };
+// PREC_BF16: plain bf16; PREC_SPLIT: bf16 hi + lo (hi*hi + hi*lo + lo*hi, ~16 bits);
+// PREC_SPLIT16: fp16 hi + lo of power-of-two scaled values (~22 bits)
+enum { PREC_BF16 = 0, PREC_SPLIT = 1, PREC_SPLIT16 = 2 };
 
+// A 2-byte operand in hi (+ lo) parts.  f16: the parts are fp16 and every value is
+// multiplied by `scale` (a power of two chosen from the operand's range) when written.
 struct Op {
   bf16* hi = nullptr;
   bf16* lo = nullptr;
+  int f16 = 0;
+  float scale = 1.0f;
 };
 
 // (an operand whose consumer runs plain bf16 is passed with lo == nullptr: hi only)
 AFQ_D void put2(const Op& o, long long idx, float a, float b) {
+  if (o.f16) {
+    a *= o.scale;
+    b *= o.scale;
+    const __half2 h = __floats2half2_rn(a, b);
+    *reinterpret_cast<__half2*>(o.hi + idx) = h;
+    if (o.lo) {
+      const float2 hf = __half22float2(h);
+      *reinterpret_cast<__half2*>(o.lo + idx) = __floats2half2_rn(a - hf.x, b - hf.y);
+    }
+    return;
+  }
   bf162 h = __floats2bfloat162_rn(a, b);
   *reinterpret_cast<bf162*>(o.hi + idx) = h;
   if (o.lo) {
@@ -47,11 +65,23 @@ AFQ_D void put2(const Op& o, long long idx, float a, float b) {
   }
 }
 AFQ_D void put1(const Op& o, long long idx, float a) {
+  if (o.f16) {
+    a *= o.scale;
+    const __half h = __float2half_rn(a);
+    reinterpret_cast<__half*>(o.hi)[idx] = h;
+    if (o.lo) reinterpret_cast<__half*>(o.lo)[idx] = __float2half_rn(a - __half2float(h));
+    return;
+  }
   bf16 h = __float2bfloat16_rn(a);
   o.hi[idx] = h;
   if (o.lo) o.lo[idx] = __float2bfloat16_rn(a - __bfloat162float(h));
 }
 AFQ_D float2 get2(const Op& o, long long idx) {
+  if (o.f16) {
+    const float2 h = __half22float2(*reinterpret_cast<const __half2*>(o.hi + idx));
+    const float2 l = __half22float2(*reinterpret_cast<const __half2*>(o.lo + idx));
+    return make_float2((h.x + l.x) / o.scale, (h.y + l.y) / o.scale);
+  }
   float2 h = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.hi + idx));
   float2 l = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.lo + idx));
   return make_float2(h.x + l.x, h.y + l.y);
@@ -64,7 +94,7 @@ struct MixedState {
   bool s_real = true;
   int Kv = 0;                  // K of the vHS product (nchol, or 2*nchol for complex Spvn)
   int prec_vhs = PREC_SPLIT, prec_p = PREC_SPLIT, prec_v1 = PREC_SPLIT, prec_vk = PREC_BF16;
-  int prec_vbias = PREC_SPLIT, prec_ej = PREC_SPLIT, prec_ek = PREC_SPLIT;
+  int prec_vbias = PREC_SPLIT16, prec_ej = PREC_SPLIT16, prec_ek = PREC_SPLIT16;
   int bn_prop = 0;             // tile width >= 4n of the propagation products
   Op Sd, Pf, SpT, LhJ, LhX;    // static operands
   Op Xf, Vf, F[2], Gb, Gx;     // per-step operands
@@ -75,6 +105,12 @@ struct MixedState {
   // only and the G operands carry Re and Im in separate rows, so K is halved
   bool greal = false;
   bool preal = false;   // real Propg1: P W and P S take K = N with (Re | Im) B rows
+  // fp16 split for the G products (vbias, E_J, E_K): static operands scaled by a power of
+  // two (sSpT, sLh), the G operands per walker (wscale[w], from the walker's max |G|)
+  bool f16g = false;
+  float sSpT = 1.0f, sLh = 1.0f;
+  float* wscale = nullptr;
+  double* dmax = nullptr;
   int* err = nullptr;
   int ex_Gn = 0, ex_Gw = 0, ex_bn = 0, ex_mtiles = 0;
   std::vector<void*> allocs;
@@ -118,6 +154,46 @@ __global__ void pack_complex_kernel(const z_t* __restrict__ src, long long count
     put2(dst, 2 * e, (float)v.x, (float)v.y);
   }
 }
+// max over src of max(|re|, |im|), into *out (double; atomicMax on the bit pattern of a
+// non-negative double orders like the value)
+__global__ void maxabs_kernel(const z_t* __restrict__ src, long long count,
+                              unsigned long long* out) {
+  double m = 0.0;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+       e += (long long)gridDim.x * blockDim.x)
+    m = fmax(m, fmax(fabs(src[e].x), fabs(src[e].y)));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+// power-of-two scale that brings a magnitude m to [2^11, 2^12): fp16 keeps 16x headroom
+AFQ_HD float pow2_scale(double m) {
+  if (!(m > 0.0) || !isfinite(m)) return 1.0f;
+  int ex;
+  frexp(m, &ex);   // m = f * 2^ex, f in [0.5, 1)
+  return (float)ldexp(1.0, 12 - ex);
+}
+// per-walker scale of the compact density matrices Gc [nw][NAK]
+__global__ void __launch_bounds__(256)
+gc_scale_kernel(const z_t* __restrict__ Gc, long long nak, float* __restrict__ wscale) {
+  __shared__ double red[8];
+  const int w = blockIdx.x;
+  double m = 0.0;
+  for (long long i = threadIdx.x; i < nak; i += blockDim.x) {
+    const z_t g = Gc[(long long)w * nak + i];
+    m = fmax(m, fmax(fabs(g.x), fabs(g.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mm = red[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) mm = fmax(mm, red[i]);
+    wscale[w] = pow2_scale(mm);
+  }
+}
+
 // flag = 1 if any imaginary part of src is nonzero
 __global__ void check_imag_kernel(const z_t* __restrict__ src, long long count, int* flag) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
@@ -445,13 +521,15 @@ cudaError_t launch_lu(const float2* T1, int n, int nmat, Op Tinv, z_t* Wd, int* 
 // capacity of Gx, which fixes the spin stride the exchange product reads with).
 // real == 1 (real A operands): Gb rows w = Re Gc_w, nw + w = Im Gc_w over NAK; Gx rows
 // (w, re, b) = Re Gc_w[b][.], (w, im, b) = Im over N.
+// wscale (optional): per-walker factor applied before the conversion (fp16 operands).
 __global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N, Op Gb, Op Gx,
-                               int nwx = 0, int real = 0) {
+                               int nwx = 0, int real = 0, const float* __restrict__ wscale = nullptr) {
   const long long NAK = 2LL * n * N, tot = (long long)nw * NAK;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
     const long long w = e / NAK, q = e % NAK;
-    const z_t g = Gc[e];
+    z_t g = Gc[e];
+    if (wscale) g = zscale(g, (double)wscale[w]);
     if (real) {
       if (Gb.hi) {
         put1(Gb, w * NAK + q, (float)g.x);
@@ -480,8 +558,10 @@ __global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N,
   }
 }
 // sum of split-K partials: out[c][w] = sum_z part[z][c][w] + i part[z][c][nw + w]
+// (scaled operands: the sum is divided by ascale * wscale[w])
 __global__ void reduce_part_kernel(const float* __restrict__ part, int splits, int M, int nw,
-                                   z_t* __restrict__ out) {
+                                   z_t* __restrict__ out, float ascale = 1.0f,
+                                   const float* __restrict__ wscale = nullptr) {
   const long long tot = (long long)M * nw, sz = (long long)M * 2 * nw;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
@@ -491,7 +571,8 @@ __global__ void reduce_part_kernel(const float* __restrict__ part, int splits, i
       re += part[z * sz + c * 2 * nw + w];
       im += part[z * sz + c * 2 * nw + nw + w];
     }
-    out[e] = zmk(re, im);
+    const double u = 1.0 / ((double)ascale * (wscale ? (double)wscale[w] : 1.0));
+    out[e] = zmk(re * u, im * u);
   }
 }
 // V operand back to FP64 vHS [nw][N*N] (for copy-out only)
@@ -602,7 +683,7 @@ struct EpiVhsSym {
 
 // split-K partial products part[z][m][n]
 struct EpiPart {
-  static constexpr bool kTile = false, kPair = false;
+  static constexpr bool kTile = false, kPair = false, kF16 = true;
   float* part;
   int M, Ncol;
   long long sz;
@@ -718,9 +799,11 @@ struct EpiPropPair {
 // Exchange: rows (cv, a), columns (wl, re|im, b); per (cv, wl) the trace of T^2 with
 // T[a][b] = tile[cv*n + a][wl*2n + b] + i tile[cv*n + a][wl*2n + n + b].
 struct EpiExchange {
-  static constexpr bool kTile = true, kPair = false;
+  static constexpr bool kTile = true, kPair = false, kF16 = true;
   int n, Gn, Gw, nc, nw, nblk;
   z_t* Kpart;
+  float ascale;           // scale of the Lh operand (1 for bf16)
+  const float* wscale;    // per-walker scale of the G operand (null for bf16)
   AFQ_D void tile(int s, int mt, int nt, float* t, int ld, int tid) const {
     const int lane = tid & 31, warp = tid >> 5;
     for (int wl = warp; wl < Gw; wl += 4) {
@@ -742,7 +825,10 @@ struct EpiExchange {
         sr += __shfl_xor_sync(0xffffffffu, sr, o);
         si += __shfl_xor_sync(0xffffffffu, si, o);
       }
-      if (lane == 0 && w < nw) Kpart[((long long)w * 2 + s) * nblk + mt] = zmk(sr, si);
+      if (lane == 0 && w < nw) {
+        const double u = 1.0 / ((double)ascale * (wscale ? (double)wscale[w] : 1.0));
+        Kpart[((long long)w * 2 + s) * nblk + mt] = zmk(sr * u * u, si * u * u);
+      }
     }
   }
 };
@@ -752,11 +838,13 @@ struct EpiExchange {
 // trace sums of the tile's Cholesky vectors, added in fixed order.
 template <int TWO_N>
 struct EpiExchangeStaged {
-  static constexpr bool kTile = false, kPair = false, kStaged = true;
+  static constexpr bool kTile = false, kPair = false, kStaged = true, kF16 = true;
   static constexpr int LD = TWO_N + 1;
   static constexpr int kScratchBytes = 128 * LD * 4;
   int n, Gn, Gw, nc, nw, nblk;
   z_t* Kpart;
+  float ascale;           // scale of the Lh operand (1 for bf16)
+  const float* wscale;    // per-walker scale of the G operand (null for bf16)
   template <class Ld>
   AFQ_D void staged(int s, int mt, int nt, int row, Ld& ld, float* scr, int wg) const {
     __shared__ double red[2][4][2];
@@ -802,8 +890,10 @@ struct EpiExchangeStaged {
       const int w = nt * Gw + wl;
       if (row == 0 && w < nw) {
         const double (*r)[2] = red[wl & 1];
+        const double u = 1.0 / ((double)ascale * (wscale ? (double)wscale[w] : 1.0));
         Kpart[((long long)w * 2 + s) * nblk + mt] =
-            zmk(((r[0][0] + r[1][0]) + r[2][0]) + r[3][0], ((r[0][1] + r[1][1]) + r[2][1]) + r[3][1]);
+            zmk((((r[0][0] + r[1][0]) + r[2][0]) + r[3][0]) * u * u,
+                (((r[0][1] + r[1][1]) + r[2][1]) + r[3][1]) * u * u);
       }
     }
   }
@@ -821,15 +911,20 @@ bool tc_persistent() {
   return on == 1;
 }
 
-template <int BN, int ST, bool SPLIT, class Epi, int MINB = 1>
+// Functors that may consume fp16 split operands (kF16) get that variant compiled.
+template <class E, class = void> struct EpiF16 : std::false_type {};
+template <class E>
+struct EpiF16<E, std::void_t<decltype(E::kF16)>> : std::integral_constant<bool, E::kF16> {};
+
+template <int BN, int ST, bool SPLIT, class Epi, int MINB = 1, int FMT = 1>
 cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
                      cudaStream_t st) {
   if constexpr (!Epi::kTile && !tc::EpiPerTile<Epi>::value) {
     constexpr int PST = SPLIT ? 2 : 4;
     constexpr int WG = tc::EpiStaged<Epi>::value ? 1 : 2;
     if (tc_persistent() || tc::EpiStaged<Epi>::value) {
-      if constexpr (tc::PCfg<BN, PST, false, SPLIT, Epi, WG>::kFits)
-        return tc::launch_persistent<BN, PST, false, SPLIT, Epi, WG>(mp, g, e, err, st);
+      if constexpr (tc::PCfg<BN, PST, FMT, SPLIT, Epi, WG>::kFits)
+        return tc::launch_persistent<BN, PST, FMT, SPLIT, Epi, WG>(mp, g, e, err, st);
       else
         return cudaErrorInvalidValue;
     }
@@ -837,7 +932,7 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
   if constexpr (tc::EpiStaged<Epi>::value) {
     return cudaErrorInvalidValue;
   } else {
-    return tc::launch<BN, ST, false, SPLIT, Epi, MINB>(mp, g, e, err, st);
+    return tc::launch<BN, ST, FMT, SPLIT, Epi, MINB>(mp, g, e, err, st);
   }
 }
 
@@ -847,6 +942,12 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
 template <int BN, bool LEAN, class Epi>
 cudaError_t run_prec(int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
                      cudaStream_t st) {
+  if (prec == PREC_SPLIT16) {
+    if constexpr (EpiF16<Epi>::value)
+      return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1), 0>(mp, g, e, err, st);
+    else
+      return cudaErrorInvalidValue;
+  }
   if (prec == PREC_SPLIT) return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st);
   return run_gemm<BN, (LEAN ? 2 : 4), false, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st);
 }
@@ -893,13 +994,18 @@ bool map2(tc::Maps& mp, const Op& a, uint64_t Ka, uint64_t ra, uint64_t ba, uint
 }
 
 void parse_prec(MixedState* m) {
-  const char* env = getenv("AFQ_MIXED_PREC");   // e.g. "vhs=1,p=1,v1=1,vk=0,vbias=1,ej=1,ek=1"
+  // e.g. "vhs=1,p=1,v1=1,vk=0,vbias=2,ej=2,ek=2" (0 plain bf16, 1 bf16 split, 2 fp16 split;
+  // fp16 split applies to vbias / ej / ek only)
+  const char* env = getenv("AFQ_MIXED_PREC");
   if (!env) return;
   std::string s(env);
   auto get = [&](const char* key, int& dst) {
     std::string k = std::string(key) + "=";
     size_t p = s.find(k);
-    if (p != std::string::npos) dst = atoi(s.c_str() + p + k.size()) ? PREC_SPLIT : PREC_BF16;
+    if (p != std::string::npos) {
+      const int v = atoi(s.c_str() + p + k.size());
+      dst = v == 2 ? PREC_SPLIT16 : v ? PREC_SPLIT : PREC_BF16;
+    }
   };
   get("vhs", m->prec_vhs); get("p", m->prec_p); get("v1", m->prec_v1); get("vk", m->prec_vk);
   get("vbias", m->prec_vbias); get("ej", m->prec_ej); get("ek", m->prec_ek);
@@ -923,6 +1029,9 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     mixed_destroy(m);
     return e == cudaSuccess ? cudaErrorInvalidValue : e;
   };
+  // vbias and E_J share the G operand Gb: one format for both
+  if (m->prec_vbias == PREC_SPLIT16 || m->prec_ej == PREC_SPLIT16)
+    m->prec_vbias = m->prec_ej = PREC_SPLIT16;
   m->bn_prop = pick_bn(4 * n);
   if (!m->bn_prop) return bail(cudaSuccess, "4*NAEA exceeds 256");
   if (!init->SpvnT_dense) return bail(cudaSuccess, "SpvnT below the dense threshold");
@@ -942,6 +1051,8 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   A(alloc_op(m, m->Gb, (size_t)2 * nw * 2 * NAK));
   A(malloc_track(m, &m->S, (size_t)nw * N * 2 * n));
   A(malloc_track(m, &m->err, 1));
+  A(malloc_track(m, &m->wscale, nw));
+  A(malloc_track(m, &m->dmax, 2));
   if (init->trial) {
     A(alloc_op(m, m->TwB, (size_t)4 * n * 2 * N));
     A(alloc_op(m, m->Wn, (size_t)nw * N * 4 * n));
@@ -971,6 +1082,30 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     A(cudaStreamSynchronize(st));
     m->preal = e == cudaSuccess && !cplx && init->order >= 1;
     A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+  }
+  // fp16 split G products: power-of-two scales of the static operands from their ranges
+  if (e == cudaSuccess) {
+    const bool gb16 = m->prec_vbias == PREC_SPLIT16, gx16 = m->prec_ek == PREC_SPLIT16;
+    if (gb16 || gx16) {
+      A(cudaMemsetAsync(m->dmax, 0, 2 * sizeof(double), st));
+      unsigned long long* dm = reinterpret_cast<unsigned long long*>(m->dmax);
+      maxabs_kernel<<<148 * 4, 256, 0, st>>>(init->SpvnT_dense, (long long)nc * NAK, dm);
+      if (init->Lh) maxabs_kernel<<<148 * 4, 256, 0, st>>>(init->Lh, (long long)nc * NAK, dm + 1);
+      double hm[2] = {0.0, 0.0};
+      A(cudaGetLastError());
+      A(cudaMemcpyAsync(hm, m->dmax, sizeof(hm), cudaMemcpyDeviceToHost, st));
+      A(cudaStreamSynchronize(st));
+      m->sSpT = pow2_scale(hm[0]);
+      m->sLh = pow2_scale(hm[1]);
+    }
+    m->SpT.f16 = m->Gb.f16 = gb16 ? 1 : 0;
+    m->SpT.scale = gb16 ? m->sSpT : 1.0f;
+    if (init->Lh) {
+      m->LhJ.f16 = gb16 ? 1 : 0;
+      m->LhJ.scale = gb16 ? m->sLh : 1.0f;
+      m->LhX.f16 = m->Gx.f16 = gx16 ? 1 : 0;
+      m->LhX.scale = gx16 ? m->sLh : 1.0f;
+    }
   }
   // split K of the vbias / Coulomb products so the grid covers the GPU
   {
@@ -1190,61 +1325,71 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
   return cudaSuccess;
 }
 
-static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, z_t* out,
-                                  cudaStream_t st) {
+static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, float ascale,
+                                  z_t* out, cudaStream_t st) {
   const int nc = m->nc, nw = m->nw;
   tc::GemmShape g{nc, 2 * nw, (int)(m->greal ? m->NAK : 2 * m->NAK), m->splits, 128,
                   (nc + 127) / 128, false, false, m->ksplit};
   EpiPart ep{m->part, nc, 2 * nw, (long long)nc * 2 * nw};
   cudaError_t e = run_bn(128, prec, mp, g, ep, m->err, st);
   if (e != cudaSuccess) return e;
-  reduce_part_kernel<<<grid_for((long long)nc * nw), 256, 0, st>>>(m->part, m->splits, nc, nw, out);
+  const bool f16 = prec == PREC_SPLIT16;
+  reduce_part_kernel<<<grid_for((long long)nc * nw), 256, 0, st>>>(
+      m->part, m->splits, nc, nw, out, f16 ? ascale : 1.0f, f16 ? m->wscale : nullptr);
+  return cudaGetLastError();
+}
+
+// Gb of every walker (per-walker scales first when the G products run fp16 split)
+static cudaError_t pack_gb(MixedState* m, const z_t* Gc, cudaStream_t st) {
+  if (m->Gb.f16) gc_scale_kernel<<<m->nw, 256, 0, st>>>(Gc, m->NAK, m->wscale);
+  pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(
+      Gc, m->nw, m->n, m->N, m->Gb, Op{}, 0, m->greal, m->Gb.f16 ? m->wscale : nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t mixed_vbias(MixedState* m, const z_t* Gc, z_t* vbias, cudaStream_t st) {
-  pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
-                                                                      Op{}, 0, m->greal);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = pack_gb(m, Gc, st);
   if (e != cudaSuccess) return e;
-  return splitk_product(m, m->m_vbias, m->prec_vbias, vbias, st);
+  return splitk_product(m, m->m_vbias, m->prec_vbias, m->sSpT, vbias, st);
 }
 
 // Coulomb vector cvec[c][w] = sum_ak Lh[c][ak] Gc_w[ak] of every walker.
 cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t st) {
   if (!m->in.Lh) return cudaErrorInvalidValue;
-  pack_gc_kernel<<<grid_for((long long)m->nw * m->NAK), 256, 0, st>>>(Gc, m->nw, m->n, m->N, m->Gb,
-                                                                      Op{}, 0, m->greal);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = pack_gb(m, Gc, st);
   if (e != cudaSuccess) return e;
-  return splitk_product(m, m->m_ej, m->prec_ej, cvec, st);
+  return splitk_product(m, m->m_ej, m->prec_ej, m->sLh, cvec, st);
 }
 
 // Exchange partial sums Kpart[w][s][block] of the first nsub walkers packed in Gc.
 cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
                            cudaStream_t st) {
   if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
-  pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(Gc, nsub, m->n, m->N, Op{},
-                                                                     m->Gx, m->nw, m->greal);
+  const bool f16 = m->Gx.f16;
+  if (f16) gc_scale_kernel<<<nsub, 256, 0, st>>>(Gc, m->NAK, m->wscale);
+  pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(
+      Gc, nsub, m->n, m->N, Op{}, m->Gx, m->nw, m->greal, f16 ? m->wscale : nullptr);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int n = m->n;
+  const float as = f16 ? m->sLh : 1.0f;
+  const float* ws = f16 ? m->wscale : nullptr;
   tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
                   m->ex_mtiles, true, true, 0};
   if (tc_persistent()) {
     switch (2 * n) {   // staged exchange for the compiled walker widths
       case 32: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
-                             EpiExchangeStaged<32>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart},
+                             EpiExchangeStaged<32>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
       case 64: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
-                             EpiExchangeStaged<64>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart},
+                             EpiExchangeStaged<64>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
       case 96: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
-                             EpiExchangeStaged<96>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart},
+                             EpiExchangeStaged<96>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
     }
   }
-  EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart};
+  EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws};
   return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g, ep, m->err, st);
 }
 

@@ -79,9 +79,10 @@ AFQ_D void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 AFQ_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 AFQ_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-template <bool TF32>
+// FMT: operand format of both A and B: 0 = fp16, 1 = bf16 (kind::f16), 2 = tf32.
+template <int FMT>
 AFQ_D void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
-  if (TF32)
+  if (FMT == 2)
     asm volatile(
         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
@@ -130,16 +131,17 @@ AFQ_D uint64_t sdesc_k128(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: fp32 accumulator, bf16 or tf32 operands, both K-major.
-constexpr uint32_t idesc(int M, int N, bool tf32) {
-  return (1u << 4) | ((tf32 ? 2u : 1u) << 7) | ((tf32 ? 2u : 1u) << 10) |
+// Instruction descriptor: fp32 accumulator, A and B of the same format (0 = fp16,
+// 1 = bf16 for kind::f16; 2 = tf32 for kind::tf32), both K-major.
+constexpr uint32_t idesc(int M, int N, int fmt) {
+  return (1u << 4) | ((uint32_t)fmt << 7) | ((uint32_t)fmt << 10) |
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-template <int BN, int STAGES, bool TF32, bool SPLIT>
+template <int BN, int STAGES, int FMT, bool SPLIT>
 struct Cfg {
   static constexpr int BM = 128;
-  static constexpr int ELEM = TF32 ? 4 : 2;
+  static constexpr int ELEM = FMT == 2 ? 4 : 2;
   static constexpr int BK = 128 / ELEM;          // elements per 128-byte K slab
   static constexpr int UK = 32 / ELEM;           // K of one tcgen05.mma
   static constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128;
@@ -184,11 +186,11 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
 //   MINB = CTAs per SM the launch is compiled for (2 caps registers at 170 per thread so a
 //   lean ring's CTAs pair up on an SM).
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int MINB = 1>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
 __global__ void __launch_bounds__(192, MINB)
 tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched, int b_batched,
                int k_split, int m_fast, Epi epi, int* err) {
-  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -248,7 +250,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
     }
   } else if (warp == 5 && lane == 0) {
     // ---- MMA issuer
-    constexpr uint32_t ID = idesc(128, BN, TF32);
+    constexpr uint32_t ID = idesc(128, BN, FMT);
     bool ok = true;
     for (int kb = 0; kb < nk; kb++) {
       const int s = kb % STAGES;
@@ -263,14 +265,14 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
       const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
 #pragma unroll
       for (int k = 0; k < C::BK / C::UK; k++)   // advance 32 bytes along K per MMA
-        umma<TF32>(tmem, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
+        umma<FMT>(tmem, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
       if (SPLIT) {
         const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
         const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
 #pragma unroll
         for (int k = 0; k < C::BK / C::UK; k++) {
-          umma<TF32>(tmem, ad + 2 * k, bl + 2 * k, ID, 1u);   // hi * lo
-          umma<TF32>(tmem, al + 2 * k, bd + 2 * k, ID, 1u);   // lo * hi
+          umma<FMT>(tmem, ad + 2 * k, bl + 2 * k, ID, 1u);   // hi * lo
+          umma<FMT>(tmem, al + 2 * k, bd + 2 * k, ID, 1u);   // lo * hi
         }
       }
       umma_commit(&empty[s]);
@@ -350,9 +352,9 @@ struct TileSched {
   }
 };
 
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int EPI_WG>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG>
 struct PCfg {
-  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT>;
   static constexpr int NEPI = 128 * EPI_WG, THREADS = NEPI + 64;
   static constexpr uint32_t ACC_COLS = 2 * C::TMEM_COLS;
   static constexpr size_t SCRATCH = (size_t)EpiScratch<Epi>::value * EPI_WG;
@@ -361,12 +363,12 @@ struct PCfg {
   static constexpr bool kFits = SMEM <= 227 * 1024 && ACC_COLS <= 512;
 };
 
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int EPI_WG>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG>
 __global__ void __launch_bounds__(128 * EPI_WG + 64, 1)
 tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched,
                           int b_batched, int k_split, TileSched sched, Epi epi, int* err) {
-  using C = Cfg<BN, STAGES, TF32, SPLIT>;
-  using P = PCfg<BN, STAGES, TF32, SPLIT, Epi, EPI_WG>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT>;
+  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
   static_assert(!Epi::kTile, "tile epilogues reuse the operand ring: per-tile kernel only");
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -438,7 +440,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
     for (int q = max(0, g - STAGES); q < g; q++) mbar_wait(&full[q % STAGES], (q / STAGES) & 1);
   } else if (warp == WMMA && lane == 0) {
     // ---- MMA issuer
-    constexpr uint32_t ID = idesc(128, BN, TF32);
+    constexpr uint32_t ID = idesc(128, BN, FMT);
     int g = 0, li = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x, li++) {
@@ -466,14 +468,14 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
         const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
 #pragma unroll
         for (int k = 0; k < C::BK / C::UK; k++)
-          umma<TF32>(d, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
+          umma<FMT>(d, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
         if (SPLIT) {
           const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
           const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
 #pragma unroll
           for (int k = 0; k < C::BK / C::UK; k++) {
-            umma<TF32>(d, ad + 2 * k, bl + 2 * k, ID, 1u);
-            umma<TF32>(d, al + 2 * k, bd + 2 * k, ID, 1u);
+            umma<FMT>(d, ad + 2 * k, bl + 2 * k, ID, 1u);
+            umma<FMT>(d, al + 2 * k, bd + 2 * k, ID, 1u);
           }
         }
         umma_commit(&empty[s]);
@@ -565,15 +567,15 @@ struct GemmShape {
   bool m_fast = false; // raster M tiles fastest (B tiles reused from L2 across M)
 };
 
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int MINB = 1>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
 cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
                    cudaStream_t st) {
-  using C = Cfg<BN, STAGES, TF32, SPLIT>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT>;
   static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
                 "tile epilogue needs the operand ring to hold the fp32 tile");
   static_assert(MINB * C::SMEM <= 228 * 1024 && MINB * C::TMEM_COLS <= 512,
                 "CTAs per SM exceed shared memory or TMEM");
-  auto kern = tc_gemm_kernel<BN, STAGES, TF32, SPLIT, Epi, MINB>;
+  auto kern = tc_gemm_kernel<BN, STAGES, FMT, SPLIT, Epi, MINB>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -602,12 +604,12 @@ inline int sm_count() {
   return n;
 }
 
-template <int BN, int STAGES, bool TF32, bool SPLIT, class Epi, int EPI_WG = 1>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG = 1>
 cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
                               cudaStream_t st) {
-  using P = PCfg<BN, STAGES, TF32, SPLIT, Epi, EPI_WG>;
+  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
   static_assert(P::kFits, "persistent configuration exceeds shared memory or TMEM");
-  auto kern = tc_gemm_persistent_kernel<BN, STAGES, TF32, SPLIT, Epi, EPI_WG>;
+  auto kern = tc_gemm_persistent_kernel<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,

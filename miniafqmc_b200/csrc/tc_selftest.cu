@@ -35,9 +35,9 @@ cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, 
   maps.b_lo = maps.b;
   tc::GemmShape g{M, N, K, batch, 128, (M + 127) / 128, true, true, 0};
   EpiStoreF32 epi{dC, M, N, (long long)M * N};
-  if (mode == 1) return tc::launch_persistent<BN, 4, TF32, false, EpiStoreF32, 1>(maps, g, epi, derr, st);
-  if (mode == 2) return tc::launch_persistent<BN, 4, TF32, false, EpiStoreF32, 2>(maps, g, epi, derr, st);
-  return tc::launch<BN, 4, TF32, false>(maps, g, epi, derr, st);
+  if (mode == 1) return tc::launch_persistent<BN, 4, (TF32 ? 2 : 1), false, EpiStoreF32, 1>(maps, g, epi, derr, st);
+  if (mode == 2) return tc::launch_persistent<BN, 4, (TF32 ? 2 : 1), false, EpiStoreF32, 2>(maps, g, epi, derr, st);
+  return tc::launch<BN, 4, (TF32 ? 2 : 1), false>(maps, g, epi, derr, st);
 }
 
 }  // namespace
