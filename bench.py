@@ -309,7 +309,9 @@ class Form:
             self.measure(record)
 
 
-def timed(form, steps, start, torch, dist, world, profile=False):
+def timed(form, steps, start, torch, dist, world, profile=False, record=True):
+    """Times `steps` substeps from step index `start`.  profile=False: CUDA-graph substeps
+    (the headline); profile=True: op-by-op calls with per-stage events (the breakdown)."""
     e = form.eng
     e.synchronize()
     e.stage_times(reset=True)
@@ -322,7 +324,7 @@ def timed(form, steps, start, torch, dist, world, profile=False):
     torch.cuda.nvtx.range_push("timed")   # `ncu --nvtx --nvtx-include timed/` selects it
     e0.record(form.stream)
     for st in range(start, start + steps):
-        form.step(st, graph=not profile)   # stage events need the op-by-op calls
+        form.step(st, record=record, graph=not profile)   # stage events need op-by-op calls
     e1.record(form.stream)
     torch.cuda.nvtx.range_pop()
     e.synchronize()
@@ -381,7 +383,10 @@ def main():
             head.step(nwarm, record=False)
             nwarm += 1
     with ClockSampler(local) as clk:
-        ms, wall, stages = timed(head, args.steps, nwarm, torch, dist, world, profile=True)
+        ms, wall, _ = timed(head, args.steps, nwarm, torch, dist, world)
+    # per-stage breakdown: the same number of further substeps, op by op with stage events
+    _, _, stages = timed(head, args.steps, nwarm + args.steps, torch, dist, world, profile=True,
+                         record=False)
     value = world * nw * args.steps / (ms * 1e-3)
     launches = int(sum(v[1] for v in stages.values()))
 
@@ -400,7 +405,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for k in range(K):
-            st = nwarm + args.steps + k
+            st = nwarm + 2 * args.steps + k
             eng.calculate_mixed_density_matrix()
             eng.get_vbias()
             eng._check(eng.lib.afq_sigma_from(eng.h, ctypes.c_void_p(xnp[k].ctypes.data)))
@@ -437,7 +442,10 @@ def main():
         ref.measure(record=False)
         for st in range(nwarm):
             ref.step(st, record=False)
-        ms64, wall64, stages64 = timed(ref, args.steps, nwarm, torch, dist, world, profile=True)
+        ms64, wall64, _ = timed(ref, args.steps, nwarm, torch, dist, world)
+        _, _, stages64 = timed(ref, min(args.steps, 5), nwarm + args.steps, torch, dist, world,
+                               profile=True, record=False)
+        stages64 = {k: (v[0] * args.steps / min(args.steps, 5), v[1]) for k, v in stages64.items()}
         Em, E6 = np.array(head.energies), np.array(ref.energies)
         T_m, T_6 = ms * 1e-3, ms64 * 1e-3
         sig_m = float(np.sqrt(np.mean(head.sig2) / len(head.sig2)))

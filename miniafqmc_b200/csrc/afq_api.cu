@@ -723,6 +723,9 @@ afq_status energy_cv(afq_handle* h, double* sums) {
   in.Wd = h->Wd;
   in.Kpart = h->Kpart;
   in.nblk = h->nblk;
+  in.Lh = h->Lh;
+  in.n = h->n;
+  in.N = h->N;
   in.exact_exchange = [h](const z_t* gsub, int m, z_t* kp) -> cudaError_t {
     if (h->mixed) return afq::mixed_exchange(h->mixed, gsub, m, kp, h->nblk, h->st);
     int nb = 0;

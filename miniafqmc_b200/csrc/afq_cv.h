@@ -49,6 +49,8 @@ struct CvInputs {
   z_t* Kpart;           // [nw][2][nblk] scratch for the exact exchange
   int nblk;
   std::function<cudaError_t(const z_t*, int, z_t*)> exact_exchange;
+  const z_t* Lh;        // [nchol][2][n][N] unscaled half-rotated factors (FP64)
+  int n, N;
 };
 
 cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvState** out,

@@ -3,7 +3,8 @@
 // Per measurement (after the mixed density matrix):
 //   features of every walker from quantities the step already has: a fixed Gaussian
 //     projection (32 rows) of the Coulomb vector c_w = Lh Gc_w, E_J = 1/2 c_w.c_w,
-//     E_1 = Gc_w.haj, log|ovlp_a ovlp_b| and its phase;
+//     E_1 = Gc_w.haj, log|ovlp_a ovlp_b| and its phase, and the linearised exchange
+//     Q.Gc_w (Re, Im), Q = dE_K/dG at the first measurement's mean G;
 //   surrogate f_w = MLP(features) on every walker;
 //   exact exchange E_K on a seeded random subset S of m = ceil(nw / subset_den) walkers
 //     (all walkers until the first train_walker_steps exact samples are in);
@@ -25,13 +26,14 @@
 // switches the estimator off for good: exact exchange on every walker, the fallback.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "afq_cv.h"
 
 namespace afq {
 
-constexpr int CV_NIN = 36, CV_NPROJ = 32;
+constexpr int CV_NIN = 38, CV_NPROJ = 32;
 constexpr float CV_CLIP_X = 8.0f, CV_CLIP_T = 16.0f;
 
 struct CvState {
@@ -54,6 +56,8 @@ struct CvState {
   int last_m = 0;
   float last_loss = 0.0f;
   double ht_var = 0.0;
+  z_t* Q = nullptr;      // [2][n][N] linearised exchange, set at the first measurement
+  bool have_q = false;
   std::vector<void*> allocs;
 };
 
@@ -85,13 +89,18 @@ __global__ void cv_proj_init_kernel(float* R, long long count, int twonc,
 __global__ void __launch_bounds__(256)
 cv_features_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, long long nak,
                    const z_t* __restrict__ cvec, int nc, int nw, const z_t* __restrict__ Wd,
-                   const float* __restrict__ R, float* __restrict__ feats,
-                   double* __restrict__ e1ej) {
+                   const float* __restrict__ R, const z_t* __restrict__ Q,
+                   float* __restrict__ feats, double* __restrict__ e1ej) {
   __shared__ z_t red[8];
   __shared__ float proj[CV_NPROJ];
   const int w = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  z_t e1 = zmk(0, 0), ej = zmk(0, 0);
-  for (long long i = tid; i < nak; i += blockDim.x) zfma(e1, Gc[(long long)w * nak + i], haj[i]);
+  z_t e1 = zmk(0, 0), ej = zmk(0, 0), eq = zmk(0, 0);
+  for (long long i = tid; i < nak; i += blockDim.x) {
+    const z_t g = Gc[(long long)w * nak + i];
+    zfma(e1, g, haj[i]);
+    zfma(eq, g, Q[i]);
+  }
+  eq = block_zsum(eq, red);
   for (int c = tid; c < nc; c += blockDim.x) {
     z_t v = cvec[(long long)c * nw + w];
     zfma(ej, v, v);
@@ -119,8 +128,55 @@ cv_features_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, long
     f[33] = (float)e1.x;
     f[34] = (float)log(fmax(hypot(ov.x, ov.y), 1e-300));
     f[35] = (float)atan2(ov.y, ov.x);
+    f[36] = (float)eq.x;
+    f[37] = (float)eq.y;
     double* o = e1ej + (long long)w * 4;
     o[0] = e1.x; o[1] = e1.y; o[2] = 0.5 * ej.x; o[3] = 0.5 * ej.y;
+  }
+}
+
+// Weighted mean density matrix Gm[q] = sum_w Re(W_data[w][1]) Gc[w][q] / sum_w Re(...).
+__global__ void cv_gmean_kernel(const z_t* __restrict__ Gc, long long nak, int nw,
+                                const z_t* __restrict__ Wd, z_t* __restrict__ Gm) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nak;
+       q += (long long)gridDim.x * blockDim.x) {
+    z_t s = zmk(0, 0);
+    double wt = 0.0;
+    for (int w = 0; w < nw; w++) {
+      const double om = Wd[(long long)w * 8 + 1].x;
+      s = zadd(s, zscale(Gc[(long long)w * nak + q], om));
+      wt += om;
+    }
+    Gm[q] = zscale(s, wt != 0.0 ? 1.0 / wt : 0.0);
+  }
+}
+// Tt[s][b][c][a] = sum_k Gm[s][b][k] Lh[c][s][a][k]  (T_c = Lh_c Gm^T, transposed)
+__global__ void cv_qt_kernel(const z_t* __restrict__ Lh, const z_t* __restrict__ Gm, int nc,
+                             int n, int N, z_t* __restrict__ Tt) {
+  const long long tot = 2LL * n * nc * n;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long a = e % n, c = (e / n) % nc, b = (e / ((long long)n * nc)) % n,
+                    s = e / ((long long)n * nc * n);
+    const z_t* g = Gm + (s * n + b) * N;
+    const z_t* l = Lh + ((c * 2 + s) * n + a) * N;
+    z_t t = zmk(0, 0);
+    for (int k = 0; k < N; k++) zfma(t, g[k], l[k]);
+    Tt[e] = t;
+  }
+}
+// Q[s][b][k] = dE_K/dG[s][b][k] = sum_{c,a} T_c[b][a] Lh[c][s][a][k] (E_K = 1/2 sum tr(T T))
+__global__ void cv_q_kernel(const z_t* __restrict__ Lh, const z_t* __restrict__ Tt, int nc,
+                            int n, int N, z_t* __restrict__ Q) {
+  const long long tot = 2LL * n * N;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long k = e % N, b = (e / N) % n, s = e / ((long long)n * N);
+    const z_t* t = Tt + (s * n + b) * (long long)nc * n;
+    z_t q = zmk(0, 0);
+    for (int c = 0; c < nc; c++)
+      for (int a = 0; a < n; a++) zfma(q, t[c * n + a], Lh[((long long)(c * 2 + s) * n + a) * N + k]);
+    Q[e] = q;
   }
 }
 
@@ -336,6 +392,7 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   if (cfg.subset_den < 1 || cfg.hidden % 32 || cfg.hidden > 1024) return cudaErrorInvalidValue;
   CvState* s = new CvState();
   s->cfg = cfg;
+  if (const char* it = getenv("AFQ_CV_ITERS")) s->cfg.iters_online = std::max(1, atoi(it));
   s->nw = nw; s->nc = nchol; s->nak = nak;
   s->sub_cap = (nw + cfg.subset_den - 1) / cfg.subset_den;
   s->cap = std::max(4096, nw);
@@ -360,6 +417,8 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   A(cmal(s, &s->d_sub, nw));
   A(cmal(s, &s->member, nw));
   A(cmal(s, &s->Gc_sub, (size_t)s->sub_cap * nak));
+  A(cmal(s, &s->Q, (size_t)nak));
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->Q, 0, sizeof(z_t) * nak, st);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sums, sizeof(double) * 4);
   if (e == cudaSuccess) e = mlp_create(CV_NIN, cfg.hidden, s->cap, cfg.seed, &s->mlp, st);
@@ -417,8 +476,22 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   cudaError_t e;
   s->meas++;
   s->launches = 0;
+  if (!s->have_q && in.Lh) {   // linearised exchange about the first measurement's mean G
+    z_t *Gm = nullptr, *Tt = nullptr;
+    const long long ntt = 2LL * in.n * s->nc * in.n;
+    if ((e = cudaMallocAsync(&Gm, sizeof(z_t) * s->nak, st)) != cudaSuccess) return e;
+    if ((e = cudaMallocAsync(&Tt, sizeof(z_t) * ntt, st)) != cudaSuccess) return e;
+    cv_gmean_kernel<<<gridn(s->nak, 256), 256, 0, st>>>(in.Gc, s->nak, nw, in.Wd, Gm);
+    cv_qt_kernel<<<gridn(ntt, 256), 256, 0, st>>>(in.Lh, Gm, s->nc, in.n, in.N, Tt);
+    cv_q_kernel<<<gridn(s->nak, 128), 128, 0, st>>>(in.Lh, Tt, s->nc, in.n, in.N, s->Q);
+    s->launches += 3;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    cudaFreeAsync(Gm, st);
+    cudaFreeAsync(Tt, st);
+    s->have_q = true;
+  }
   cv_features_kernel<<<nw, 256, 0, st>>>(in.Gc, in.haj, s->nak, in.cvec, s->nc, nw, in.Wd, s->R,
-                                         s->feats, s->e1ej);
+                                         s->Q, s->feats, s->e1ej);
   s->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   s->active = s->trained && !s->failed;

@@ -44,19 +44,10 @@ struct Op {
   float scale = 1.0f;
 };
 
-// (an operand whose consumer runs plain bf16 is passed with lo == nullptr: hi only)
+// bf16 writers (an operand whose consumer runs plain bf16 is passed with lo == nullptr:
+// hi only).  The epilogues of the products use these; put2f / put1f below also handle
+// fp16 operands and are used by the pack kernels of operands that may be fp16.
 AFQ_D void put2(const Op& o, long long idx, float a, float b) {
-  if (o.f16) {
-    a *= o.scale;
-    b *= o.scale;
-    const __half2 h = __floats2half2_rn(a, b);
-    *reinterpret_cast<__half2*>(o.hi + idx) = h;
-    if (o.lo) {
-      const float2 hf = __half22float2(h);
-      *reinterpret_cast<__half2*>(o.lo + idx) = __floats2half2_rn(a - hf.x, b - hf.y);
-    }
-    return;
-  }
   bf162 h = __floats2bfloat162_rn(a, b);
   *reinterpret_cast<bf162*>(o.hi + idx) = h;
   if (o.lo) {
@@ -65,23 +56,35 @@ AFQ_D void put2(const Op& o, long long idx, float a, float b) {
   }
 }
 AFQ_D void put1(const Op& o, long long idx, float a) {
-  if (o.f16) {
-    a *= o.scale;
-    const __half h = __float2half_rn(a);
-    reinterpret_cast<__half*>(o.hi)[idx] = h;
-    if (o.lo) reinterpret_cast<__half*>(o.lo)[idx] = __float2half_rn(a - __half2float(h));
-    return;
-  }
   bf16 h = __float2bfloat16_rn(a);
   o.hi[idx] = h;
   if (o.lo) o.lo[idx] = __float2bfloat16_rn(a - __bfloat162float(h));
 }
-AFQ_D float2 get2(const Op& o, long long idx) {
-  if (o.f16) {
-    const float2 h = __half22float2(*reinterpret_cast<const __half2*>(o.hi + idx));
-    const float2 l = __half22float2(*reinterpret_cast<const __half2*>(o.lo + idx));
-    return make_float2((h.x + l.x) / o.scale, (h.y + l.y) / o.scale);
+AFQ_D void put2f(const Op& o, long long idx, float a, float b) {
+  if (!o.f16) {
+    put2(o, idx, a, b);
+    return;
   }
+  a *= o.scale;
+  b *= o.scale;
+  const __half2 h = __floats2half2_rn(a, b);
+  *reinterpret_cast<__half2*>(o.hi + idx) = h;
+  if (o.lo) {
+    const float2 hf = __half22float2(h);
+    *reinterpret_cast<__half2*>(o.lo + idx) = __floats2half2_rn(a - hf.x, b - hf.y);
+  }
+}
+AFQ_D void put1f(const Op& o, long long idx, float a) {
+  if (!o.f16) {
+    put1(o, idx, a);
+    return;
+  }
+  a *= o.scale;
+  const __half h = __float2half_rn(a);
+  reinterpret_cast<__half*>(o.hi)[idx] = h;
+  if (o.lo) reinterpret_cast<__half*>(o.lo)[idx] = __float2half_rn(a - __half2float(h));
+}
+AFQ_D float2 get2(const Op& o, long long idx) {   // bf16 operands
   float2 h = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.hi + idx));
   float2 l = __bfloat1622float2(*reinterpret_cast<const bf162*>(o.lo + idx));
   return make_float2(h.x + l.x, h.y + l.y);
@@ -94,7 +97,9 @@ struct MixedState {
   bool s_real = true;
   int Kv = 0;                  // K of the vHS product (nchol, or 2*nchol for complex Spvn)
   int prec_vhs = PREC_SPLIT, prec_p = PREC_SPLIT, prec_v1 = PREC_SPLIT, prec_vk = PREC_BF16;
-  int prec_vbias = PREC_SPLIT16, prec_ej = PREC_SPLIT16, prec_ek = PREC_SPLIT16;
+  // fp16 split (PREC_SPLIT16) measured no better than bf16 split for these products: their
+  // error at C4 sizes is set by the fp32 accumulation over long K, not by the operands
+  int prec_vbias = PREC_SPLIT, prec_ej = PREC_SPLIT, prec_ek = PREC_SPLIT;
   int bn_prop = 0;             // tile width >= 4n of the propagation products
   Op Sd, Pf, SpT, LhJ, LhX;    // static operands
   Op Xf, Vf, F[2], Gb, Gx;     // per-step operands
@@ -151,7 +156,7 @@ __global__ void pack_complex_kernel(const z_t* __restrict__ src, long long count
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
        e += (long long)gridDim.x * blockDim.x) {
     z_t v = src[e];
-    put2(dst, 2 * e, (float)v.x, (float)v.y);
+    put2f(dst, 2 * e, (float)v.x, (float)v.y);
   }
 }
 // max over src of max(|re|, |im|), into *out (double; atomicMax on the bit pattern of a
@@ -204,7 +209,7 @@ __global__ void check_imag_kernel(const z_t* __restrict__ src, long long count, 
 __global__ void pack_real_kernel(const z_t* __restrict__ src, long long count, Op dst) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
        e += (long long)gridDim.x * blockDim.x)
-    put1(dst, e, (float)src[e].x);
+    put1f(dst, e, (float)src[e].x);
 }
 // Lh [c][s][a][k] -> real LhX [s][c][a][k]
 __global__ void pack_lhx_real_kernel(const z_t* __restrict__ Lh, int nc, int n, int N, Op dst) {
@@ -212,7 +217,7 @@ __global__ void pack_lhx_real_kernel(const z_t* __restrict__ Lh, int nc, int n, 
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
        e += (long long)gridDim.x * blockDim.x) {
     long long s = e / (nc * per), r = e % (nc * per), c = r / per, q = r % per;
-    put1(dst, e, (float)Lh[c * 2 * per + s * per + q].x);
+    put1f(dst, e, (float)Lh[c * 2 * per + s * per + q].x);
   }
 }
 // Lh [c][s][a][k] -> LhX [s][c][a][2k]
@@ -222,7 +227,7 @@ __global__ void pack_lhx_kernel(const z_t* __restrict__ Lh, int nc, int n, int N
        e += (long long)gridDim.x * blockDim.x) {
     long long s = e / (nc * per), r = e % (nc * per), c = r / per, q = r % per;
     z_t v = Lh[c * 2 * per + s * per + q];
-    put2(dst, 2 * e, (float)v.x, (float)v.y);
+    put2f(dst, 2 * e, (float)v.x, (float)v.y);
   }
 }
 // dense Spvn from CSR: real values -> [ik][c]; complex -> [ik][2c + {0,1}]
@@ -532,28 +537,28 @@ __global__ void pack_gc_kernel(const z_t* __restrict__ Gc, int nw, int n, int N,
     if (wscale) g = zscale(g, (double)wscale[w]);
     if (real) {
       if (Gb.hi) {
-        put1(Gb, w * NAK + q, (float)g.x);
-        put1(Gb, (nw + w) * NAK + q, (float)g.y);
+        put1f(Gb, w * NAK + q, (float)g.x);
+        put1f(Gb, (nw + w) * NAK + q, (float)g.y);
       }
       if (Gx.hi) {
         const long long s = q / ((long long)n * N), r = q % ((long long)n * N);
         const long long b = r / N, k = r % N;
         const long long row0 = (s * (nwx ? nwx : nw) + w) * 2 * n + b;
-        put1(Gx, row0 * N + k, (float)g.x);
-        put1(Gx, (row0 + n) * N + k, (float)g.y);
+        put1f(Gx, row0 * N + k, (float)g.x);
+        put1f(Gx, (row0 + n) * N + k, (float)g.y);
       }
       continue;
     }
     if (Gb.hi) {
-      put2(Gb, w * 2 * NAK + 2 * q, (float)g.x, (float)-g.y);
-      put2(Gb, (nw + w) * 2 * NAK + 2 * q, (float)g.y, (float)g.x);
+      put2f(Gb, w * 2 * NAK + 2 * q, (float)g.x, (float)-g.y);
+      put2f(Gb, (nw + w) * 2 * NAK + 2 * q, (float)g.y, (float)g.x);
     }
     if (Gx.hi) {
       const long long s = q / ((long long)n * N), r = q % ((long long)n * N);
       const long long b = r / N, k = r % N;
       const long long row0 = (s * (nwx ? nwx : nw) + w) * 2 * n + b, row1 = row0 + n;
-      put2(Gx, row0 * 2 * N + 2 * k, (float)g.x, (float)-g.y);
-      put2(Gx, row1 * 2 * N + 2 * k, (float)g.y, (float)g.x);
+      put2f(Gx, row0 * 2 * N + 2 * k, (float)g.x, (float)-g.y);
+      put2f(Gx, row1 * 2 * N + 2 * k, (float)g.y, (float)g.x);
     }
   }
 }

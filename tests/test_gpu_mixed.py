@@ -125,3 +125,25 @@ def test_cholqr2_ortho_matches_householder_up_to_signs():
     assert rel(np.abs(om), np.abs(od)) < 1e-4
     d.close()
     m.close()
+
+
+def test_fp16_split_g_products(monkeypatch):
+    """The fp16 hi/lo form (power-of-two scaled operands) of the vbias, Coulomb and
+    exchange products agrees with the FP64 form like the bf16 split form (1e-4)."""
+    monkeypatch.setenv("AFQ_MIXED_PREC", "vbias=2,ej=2,ek=2")
+    s = system("C1")
+    nw = 16
+    d, m = pair(s, nw, perturbed(s, nw))
+    for e in (d, m):
+        e.calculate_mixed_density_matrix()
+        e.get_vbias()
+    ev = rel(m.copy_out("vbias"), d.copy_out("vbias"))
+    ed, em = d.calculate_energy("chol"), m.calculate_energy("chol")
+    pd, pm = d.copy_out("energy_parts"), m.copy_out("energy_parts")
+    m.synchronize()
+    res = {"vbias": ev, "E": abs(em - ed) / abs(ed), "EJ": rel(pm[:, 1], pd[:, 1]),
+           "EK": rel(pm[:, 2], pd[:, 2])}
+    record("fp16_g_C1", res)
+    assert ev < 1e-4 and res["EJ"] < 1e-4 and res["EK"] < 1e-4 and res["E"] < 1e-5
+    d.close()
+    m.close()
