@@ -19,8 +19,13 @@ wall-second sigma_E * sqrt(T) of each (sigma_E from the walker-population varian
 the weighted mean at each measurement, combined over measurements).
 
 Rank 0 prints one JSON line.  `value` is whole-job walker-steps/s with the walker set
-resident in HBM; `e2e` is the same rate through the C ABI with host buffers (the normals
-of every step copied host->device, W_data copied back every step).  `--impl reference`
+resident in HBM, timed over K substeps launched as CUDA graphs (`afq_substep`) with the
+energy measurements op by op; `stages_ms` comes from a second pass of K further substeps
+op by op with per-stage CUDA events; `e2e` is the same rate through the C ABI with host
+buffers (the normals of every step copied host->device, W_data copied back every step).
+The control variate's warm-up (its first 2000 exact samples) runs before the timed
+region; the same-walker comparison measures the mixed form's final walkers with both
+forms.  `--impl reference`
 times the FP64 CPU restatement of the reference (the oracle: the reference's call
 granularity and GNU Release flags) on the host cores, on a bounded sample of walkers.
 """

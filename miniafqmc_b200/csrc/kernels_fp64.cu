@@ -227,6 +227,9 @@ cudaError_t launch_dm(const z_t* W, const z_t* tw, int N, int n, int nw, z_t* Gc
   if (smem > attr) {
     cudaError_t e = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
+    if (e == cudaSuccess)   // several CTAs per SM need the full shared-memory carveout
+      e = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr = smem;
   }
@@ -746,6 +749,9 @@ cudaError_t launch_ortho_cholqr(z_t* W, int N, int n, int nw, int* info, cudaStr
   if (smem > attr) {
     cudaError_t e = cudaFuncSetAttribute(ortho_cholqr_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ortho_cholqr_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr = smem;
   }

@@ -505,8 +505,130 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
   }
 }
 
+// The same Gauss-Jordan (in-place exchange form, implicit izamax pivoting) with the matrix
+// in shared memory: 128 threads per matrix (warps on rows, lanes on columns), three
+// barriers per pivot; small register footprint, so five matrices share an SM.
+constexpr int LUS_THREADS = 128;
+size_t lus_smem_bytes(int n) { return sizeof(z_t) * ((size_t)n * (n + 1) + 2 * n); }
+
+__global__ void __launch_bounds__(LUS_THREADS)
+lu_smem_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ Wd,
+               int* __restrict__ info, int want_inv, int save_old) {
+  extern __shared__ __align__(16) unsigned char lus_raw[];
+  __shared__ int s_p, pivrow[64], invp[64], used[64];
+  __shared__ z_t s_pv;
+  const int q = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int NWARP = LUS_THREADS / 32;
+  const int ld = n + 1, nn = n * n;
+  z_t* T = reinterpret_cast<z_t*>(lus_raw);
+  z_t* pcol = T + n * ld;
+  z_t* prow = pcol + n;
+  const float2* src = T1 + (long long)q * nn;
+  for (int e = tid; e < nn; e += LUS_THREADS) {
+    const float2 v = src[e];
+    T[(e / n) * ld + e % n] = zmk(v.x, v.y);
+  }
+  for (int i = tid; i < 64; i += LUS_THREADS) used[i] = 0;
+  __syncthreads();
+  z_t det = zmk(1.0, 0.0);
+  int sing = 0;
+  for (int j = 0; j < n; j++) {
+    if (warp == 0) {   // pivot: max |re| + |im| of column j over the unused rows
+      double best = -1.0;
+      int bi = n;
+      for (int i = lane; i < n; i += 32) {
+        if (used[i]) continue;
+        const double v = zabs1(T[i * ld + j]);
+        if (v > best) { best = v; bi = i; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+      }
+      if (lane == 0) {
+        s_p = best > 0.0 ? bi : -1;
+        if (bi < n) {
+          s_pv = T[bi * ld + j];
+          used[bi] = 1;
+          pivrow[j] = bi;
+        }
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p < 0) { sing = 1; break; }   // uniform across the CTA
+    const z_t pv = s_pv;
+    if (tid == 0) det = zmul(det, pv);
+    const z_t inv = zrecip(pv);
+    for (int i = tid; i < n; i += LUS_THREADS) {
+      pcol[i] = T[i * ld + j];
+      prow[i] = (i == j) ? inv : zmul(T[p * ld + i], inv);
+    }
+    __syncthreads();
+    for (int i = warp; i < n; i += NWARP) {
+      const z_t f = pcol[i];
+      for (int c = lane; c < n; c += 32) {
+        if (i == p) {
+          T[i * ld + c] = prow[c];
+        } else {
+          const z_t base = (c == j) ? zmk(0, 0) : T[i * ld + c];
+          T[i * ld + c] = zsub(base, zmul(f, prow[c]));
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (sing) det = zmk(0, 0);
+  if (tid == 0 && !sing) {
+    int inv_cnt = 0;
+    for (int a = 0; a < n; a++)
+      for (int b = a + 1; b < n; b++) inv_cnt += pivrow[a] > pivrow[b];
+    if (inv_cnt & 1) det = zmk(-det.x, -det.y);
+    for (int a = 0; a < n; a++) invp[pivrow[a]] = a;
+  }
+  __syncthreads();
+  if (want_inv) {
+    const long long base = (long long)q * 2 * n * 2 * n;
+    for (int e = tid; e < nn; e += LUS_THREADS) {
+      const int i = e / n, c = e % n;
+      const int ra = sing ? i : invp[i], cb = sing ? c : pivrow[c];
+      const z_t y = sing ? zmk(0, 0) : T[i * ld + c];
+      put2(Tinv, base + (2LL * ra) * 2 * n + 2 * cb, (float)y.x, (float)-y.y);
+      put2(Tinv, base + (2LL * ra + 1) * 2 * n + 2 * cb, (float)y.y, (float)y.x);
+    }
+  }
+  if (tid == 0) {
+    const int w = q >> 1, sp = q & 1;
+    z_t* d = Wd + (long long)w * 8;
+    if (save_old) {
+      if (sp == 0) d[5] = d[4];
+      d[6 + sp] = d[2 + sp];
+    }
+    d[2 + sp] = det;
+    info[q] = sing;
+  }
+}
+
 cudaError_t launch_lu(const float2* T1, int n, int nmat, Op Tinv, z_t* Wd, int* info, int want_inv,
                       int save_old, cudaStream_t st) {
+  static const bool regs = getenv("AFQ_LU_REGISTERS") != nullptr;
+  if (!regs && n <= 64) {   // shared-memory form (default)
+    const size_t smem = lus_smem_bytes(n);
+    static size_t attr = 0;
+    if (smem > attr) {   // and the full shared-memory carveout: five matrices per SM
+      cudaError_t e = cudaFuncSetAttribute(lu_smem_kernel,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(lu_smem_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
+      if (e != cudaSuccess) return e;
+      attr = smem;
+    }
+    lu_smem_kernel<<<nmat, LUS_THREADS, smem, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
+    return cudaGetLastError();
+  }
   // 16 x 16 threads per matrix: few registers per thread, many warps per SM
   if (n <= 16)
     lu_inv_kernel<8, 8, 2, 2><<<nmat, 64, 0, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
