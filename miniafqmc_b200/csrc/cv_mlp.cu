@@ -4,7 +4,7 @@
 // exact energy for every walker, energy.hpp:66-102).
 //
 // Kernels (CUDA cores; the network is ~75k parameters, far below tensor-core sizes):
-//   mlp_fwd    8 samples per CTA, one hidden unit per thread; keeps z1, z2 for backward
+//   mlp_fwd    MLP_SB samples per CTA, one hidden unit per thread; keeps z1, z2 for backward
 //   mlp_bwd_x  per-sample backward through the layers (dz2, dz1)
 //   mlp_atb    tiled weight + bias gradients (dz^T [x|1]) over sample chunks, mlp_gsum
 //              adds the chunks; fixed order
@@ -43,9 +43,9 @@ struct MlpLayout {
   }
 };
 
-constexpr int MLP_SB = 8;   // samples per CTA in the per-sample kernels
+constexpr int MLP_SB = 2;   // samples per CTA in the per-sample kernels (few: many CTAs per SM)
 
-// y = w3 . gelu(W2 gelu(W1 x + b1) + b2) + b3 for 8 samples per CTA; blockDim = H.
+// y = w3 . gelu(W2 gelu(W1 x + b1) + b2) + b3 for MLP_SB samples per CTA; blockDim = H.
 __global__ void mlp_fwd_kernel(const float* __restrict__ x, int B, int nin,
                                const bf16* __restrict__ W1t,   // [nin][H]
                                const float* __restrict__ b1,

@@ -647,10 +647,11 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
             av[i] = (i < R && a < n) ? buf[kk * ld + a] : zmk(0, 0);
             bv[i] = (i < R && b < n) ? buf[kk * ld + b] : zmk(0, 0);
           }
+          // blocks i > j hold only a > b: the lower triangle, which nothing reads
 #pragma unroll
           for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++)
+            for (int j = i; j < 4; j++)
               if (i < R && j < R) zfma_conj(acc[i][j], av[i], bv[j]);
         }
         __syncthreads();
@@ -658,7 +659,7 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
+        for (int j = i; j < 4; j++) {
           const int a = ta + 16 * i, b = tb + 16 * j;
           if (i < R && j < R && a < n && b < n) G[a * ld + b] = acc[i][j];
         }
@@ -714,20 +715,27 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
       for (int i = 0; i < 2; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) acc[i][j] = zmk(0, 0);
-      for (int a = 0; a < n; a++) {
-        z_t bv[2], rv[4];
+      // R^-1 is upper triangular: rows a in [16r, 16r + 16) reach columns b = tb + 16j
+      // only for j >= r
 #pragma unroll
-        for (int i = 0; i < 2; i++) bv[i] = buf[(ta + 16 * i) * ld + a];
+      for (int r = 0; r < 4; r++) {
+        if (r >= R) break;
+        const int a1 = min(16 * r + 16, n);
+        for (int a = 16 * r; a < a1; a++) {
+          z_t bv[2], rv[4];
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const int b = tb + 16 * j;
-          rv[j] = (j < R && b < n) ? Ri[a * ld + b] : zmk(0, 0);
+          for (int i = 0; i < 2; i++) bv[i] = buf[(ta + 16 * i) * ld + a];
+#pragma unroll
+          for (int j = r; j < 4; j++) {
+            const int b = tb + 16 * j;
+            rv[j] = (j < R && b < n) ? Ri[a * ld + b] : zmk(0, 0);
+          }
+#pragma unroll
+          for (int i = 0; i < 2; i++)
+#pragma unroll
+            for (int j = r; j < 4; j++)
+              if (j < R) zfma(acc[i][j], bv[i], rv[j]);
         }
-#pragma unroll
-        for (int i = 0; i < 2; i++)
-#pragma unroll
-          for (int j = 0; j < 4; j++)
-            if (j < R) zfma(acc[i][j], bv[i], rv[j]);
       }
 #pragma unroll
       for (int i = 0; i < 2; i++)

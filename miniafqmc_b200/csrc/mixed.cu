@@ -567,15 +567,26 @@ lu_smem_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ 
       prow[i] = (i == j) ? inv : zmul(T[p * ld + i], inv);
     }
     __syncthreads();
+    // lanes own columns lane and lane + 32 (n <= 64): the pivot row's values stay in
+    // registers across the rows; each element is one load, four FMAs and one store
+    const bool c0 = lane < n, c1 = lane + 32 < n;
+    const z_t pr0 = c0 ? prow[lane] : zmk(0, 0), pr1 = c1 ? prow[lane + 32] : zmk(0, 0);
     for (int i = warp; i < n; i += NWARP) {
+      z_t* Ti = T + i * ld;
+      if (i == p) {
+        if (c0) Ti[lane] = pr0;
+        if (c1) Ti[lane + 32] = pr1;
+        continue;
+      }
       const z_t f = pcol[i];
-      for (int c = lane; c < n; c += 32) {
-        if (i == p) {
-          T[i * ld + c] = prow[c];
-        } else {
-          const z_t base = (c == j) ? zmk(0, 0) : T[i * ld + c];
-          T[i * ld + c] = zsub(base, zmul(f, prow[c]));
-        }
+      if (c0) {
+        const z_t b = (lane == j) ? zmk(0, 0) : Ti[lane];
+        Ti[lane] = zmk(fma(-f.x, pr0.x, fma(f.y, pr0.y, b.x)), fma(-f.x, pr0.y, fma(-f.y, pr0.x, b.y)));
+      }
+      if (c1) {
+        const z_t b = (lane + 32 == j) ? zmk(0, 0) : Ti[lane + 32];
+        Ti[lane + 32] =
+            zmk(fma(-f.x, pr1.x, fma(f.y, pr1.y, b.x)), fma(-f.x, pr1.y, fma(-f.y, pr1.x, b.y)));
       }
     }
     __syncthreads();
@@ -1402,6 +1413,8 @@ cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
     tc::GemmShape g{2 * nw, m->npairs * 256, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0,
                     true};
     EpiVhsSym epi{m->Vf, nw, N, m->pairs};
+    static const bool lean = getenv("AFQ_VHS_LEAN") != nullptr;   // 2 CTAs/SM, 1-stage rings
+    if (lean) return run_bn<true>(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
     return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
   }
   tc::GemmShape g{2 * nw, N * N, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0, true};
