@@ -551,6 +551,8 @@ def main():
         line.update(cmp)
     if head.mode == "cv":
         line["control_variate"] = head.eng.cv_stats()
+    if args.form != "fp64":
+        line["config"]["kernel_tuning"] = head.eng.tuning()
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -198,6 +198,15 @@ afq_status afq_profile(afq_handle* h, int enable);
  * ([AFQ_NSTAGES] each, either may be NULL); reset != 0 clears the accumulators.
  * Launch counts include graph substeps. */
 afq_status afq_stage_times(afq_handle* h, double* ms, long long* launches, int reset);
+/* Kernel choices of the mixed-precision products, made when afq_set_hamiltonian times
+ * the candidates on the handle's own shapes.  No counterpart in the reference (its
+ * kernels have fixed launch shapes).  Sites, in order: vHS, propagation chain, split-K
+ * vbias / Coulomb, exchange over all walkers, exchange over a 1/8 subset, T1 = W^T trial.
+ * choice[7]: per site 0 (built-in rule), 1 (persistent kernel) or 2 (per-tile kernel),
+ * then the split-K slice count; ms[12]: per site the timed milliseconds of candidates 1
+ * and 2 (0 when not timed).  AFQ_TUNE=0 in the environment skips the timing, AFQ_TUNE=1
+ * or 2 forces one kernel.  All zeros for an FP64 handle. */
+afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */
 afq_status afq_get_stream(afq_handle* h, void** stream);
@@ -221,6 +230,24 @@ afq_status afq_copy_out(afq_handle* h, int which, void* host);
  * different streams) race; serialise them. */
 afq_status afq_exchange_energy_noalloc(const double* Lh, const double* Gc, int nmo, int naea,
                                        int nchol, int nwalk, double* ek, void* stream);
+
+/* Heterogeneous multi-system batch (no reference counterpart; the reference runs one
+ * system per process).  A batch groups handles of systems with different NMO, electron
+ * count, nchol and walker count (each set up as usual, on one device, with its own
+ * walkers, Hamiltonian and control variate).  afq_batch_substep advances every system by
+ * one substep (the afq_substep sequence of each) with ONE CUDA-graph launch: the
+ * systems' stages are parallel branches of the graph, so small systems share the GPU
+ * instead of running one after another.  seeds[i] is the Philox seed of system i;
+ * step_tot and northo are common.  Results equal afq_substep on each handle alone.
+ * Energy measurements stay per handle (afq_energy).  The handles must not be used from
+ * other threads during the call; stage profiling must be off. */
+typedef struct afq_batch afq_batch;
+afq_status afq_batch_create(afq_handle* const* handles, int count, afq_batch** out);
+void afq_batch_destroy(afq_batch* b);
+afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_tot,
+                             int northo);
+/* Waits for the batch's work and reports any handle's tensor-core timeout flags. */
+afq_status afq_batch_synchronize(afq_batch* b);
 
 /* Self-test of the tensor-core GEMM used by the mixed form (no reference counterpart):
  * C[b][m][n] = sum_k A[b][m][k] B[b][n][k] for host fp32 arrays, computed on the current

@@ -34,6 +34,8 @@ EXPORTS = [
     "afq_selftest_tc_gemm", "afq_exchange_energy_noalloc", "afq_cv_configure", "afq_cv_stats",
     "afq_mlp_create", "afq_mlp_destroy", "afq_mlp_num_params", "afq_mlp_set_params",
     "afq_mlp_get_params", "afq_mlp_forward", "afq_mlp_gradient", "afq_mlp_train",
+    "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
+    "afq_get_tuning",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -93,6 +95,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_mlp_get_params": ([P, P], I), "afq_mlp_forward": ([P, I, P, P], I),
         "afq_mlp_gradient": ([P, I, P, P, P, P], I),
         "afq_mlp_train": ([P, I, P, P, I, ctypes.c_float, P], I),
+        "afq_batch_create": ([P, I, P], I), "afq_batch_destroy": ([P], None),
+        "afq_batch_substep": ([P, P, U64, I], I), "afq_batch_synchronize": ([P], I),
+        "afq_get_tuning": ([P, P, P], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -270,6 +275,21 @@ class AfqmcSys:
                 "active": bool(v[3]), "measurements": int(v[4]), "subset_var": float(v[5]),
                 "restandardisations": int(v[6]), "fallback": bool(v[7])}
 
+    TUNE_SITES = ["vhs", "propagate", "splitk", "exchange_all", "exchange_subset", "t1"]
+
+    def tuning(self) -> dict:
+        """Kernel picked per mixed-precision product site at set-up (0 built-in rule,
+        1 persistent, 2 per-tile), the timed milliseconds of both candidates, and the
+        split-K slice count of the vbias / Coulomb products."""
+        c = np.zeros(len(self.TUNE_SITES) + 1, dtype=np.int32)
+        t = np.zeros(2 * len(self.TUNE_SITES))
+        self._check(self.lib.afq_get_tuning(self.h, _p(c), _p(t)))
+        out = {k: {"kernel": int(c[i]), "ms": [round(float(t[2 * i]), 4),
+                                               round(float(t[2 * i + 1]), 4)]}
+               for i, k in enumerate(self.TUNE_SITES)}
+        out["splitk_slices"] = int(c[-1])
+        return out
+
     def substep(self, seed: int, step_tot: int, northo: int, graph: bool = True):
         """One substep of the driver loop (miniafqmc_base.cpp:251-337)."""
         if graph:
@@ -304,6 +324,44 @@ class AfqmcSys:
         v = ctypes.c_void_p()
         self._check(self.lib.afq_get_stream(self.h, ctypes.byref(v)))
         return v.value or 0
+
+
+class AfqmcBatch:
+    """Several systems (AfqmcSys handles of any sizes, one device) advanced together:
+    one CUDA-graph launch per substep, the systems' stages as parallel graph branches."""
+
+    def __init__(self, systems):
+        self.lib = load_library()
+        self.systems = list(systems)
+        arr = (ctypes.c_void_p * len(self.systems))(*[s.h for s in self.systems])
+        self._arr = arr
+        h = ctypes.c_void_p()
+        st = self.lib.afq_batch_create(arr, len(self.systems), ctypes.byref(h))
+        if st != 0:
+            raise AfqmcError(st, "afq_batch_create failed")
+        self.b = h
+
+    def substep(self, seeds, step_tot: int, northo: int):
+        sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+        st = self.lib.afq_batch_substep(self.b, _p(sd), step_tot, northo)
+        if st != 0:
+            raise AfqmcError(st, "afq_batch_substep failed")
+
+    def synchronize(self):
+        st = self.lib.afq_batch_synchronize(self.b)
+        if st != 0:
+            raise AfqmcError(st, "afq_batch_synchronize failed")
+
+    def close(self):
+        if self.b:
+            self.lib.afq_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Mlp:

@@ -833,6 +833,138 @@ afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int nort
   return AFQ_OK;
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------------ multi-system batch
+struct afq_batch {
+  std::vector<afq_handle*> hs;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr;
+  std::vector<cudaEvent_t> pre, join;
+  cudaGraphExec_t g[2] = {nullptr, nullptr};
+  std::vector<std::vector<long long>> counts[2];   // per handle, per stage
+};
+
+namespace {
+void batch_release(afq_batch* b) {
+  for (auto& g : b->g)
+    if (g) cudaGraphExecDestroy(g);
+  for (cudaEvent_t e : b->pre) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->done) cudaEventDestroy(b->done);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+}
+}  // namespace
+
+extern "C" {
+
+afq_status afq_batch_create(afq_handle* const* handles, int count, afq_batch** out) {
+  if (!handles || count < 1 || !out) return AFQ_ERR_ARG;
+  *out = nullptr;
+  for (int i = 0; i < count; i++) {
+    if (!handles[i]) return AFQ_ERR_ARG;
+    if (handles[i]->d.device != handles[0]->d.device) return AFQ_ERR_UNSUPPORTED;
+    for (int j = 0; j < i; j++)
+      if (handles[j] == handles[i]) return AFQ_ERR_ARG;
+  }
+  afq_batch* b = new afq_batch();
+  b->hs.assign(handles, handles + count);
+  b->device = handles[0]->d.device;
+  cudaSetDevice(b->device);
+  bool ok = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
+  b->pre.assign(count, nullptr);
+  b->join.assign(count, nullptr);
+  for (int i = 0; ok && i < count; i++)
+    ok = cudaEventCreateWithFlags(&b->pre[i], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    batch_release(b);
+    return AFQ_ERR_CUDA;
+  }
+  *out = b;
+  return AFQ_OK;
+}
+
+void afq_batch_destroy(afq_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->st);
+  batch_release(b);
+}
+
+afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_tot,
+                             int northo) {
+  if (!b || !seeds || northo <= 0) return AFQ_ERR_ARG;
+  cudaSetDevice(b->device);
+  const int n = (int)b->hs.size();
+  const bool ortho = step_tot > 0 && step_tot % (uint64_t)northo == 0;
+  // per system: scalars of this step, a fresh T1^-1 for the graph's first density matrix
+  for (int i = 0; i < n; i++) {
+    afq_handle* h = b->hs[i];
+    afq_status s = need_ready(h);
+    if (s != AFQ_OK) return s;
+    if (h->profiling) return fail(h, AFQ_ERR_STATE, "stage profiling is on");
+    if (seeds[i] != h->host_seed || step_tot != h->host_step)
+      if ((s = set_scalars(h, seeds[i], step_tot)) != AFQ_OK) return s;
+    if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
+    AFQ_CUDA(h, cudaEventRecord(b->pre[i], h->st));
+    if (cudaStreamWaitEvent(b->st, b->pre[i], 0) != cudaSuccess) return AFQ_ERR_CUDA;
+  }
+  const int slot = ortho ? 1 : 0;
+  if (!b->g[slot]) {
+    // one graph: fork from the batch stream into every handle's stream, join back
+    if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return AFQ_ERR_CUDA;
+    cudaError_t e = cudaEventRecord(b->fork, b->st);
+    b->counts[slot].assign(n, std::vector<long long>(AFQ_NSTAGES, 0));
+    for (int i = 0; i < n && e == cudaSuccess; i++) {
+      afq_handle* h = b->hs[i];
+      if ((e = cudaStreamWaitEvent(h->st, b->fork, 0)) != cudaSuccess) break;
+      h->capturing = true;
+      h->launch_sink = b->counts[slot][i].data();
+      e = st_substep(h, ortho);
+      h->launch_sink = nullptr;
+      h->capturing = false;
+      if (e == cudaSuccess) e = cudaEventRecord(b->join[i], h->st);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->join[i], 0);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->g[slot], g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      b->g[slot] = nullptr;
+      return fail(b->hs[0], AFQ_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
+    }
+  }
+  if (cudaGraphLaunch(b->g[slot], b->st) != cudaSuccess || cudaEventRecord(b->done, b->st) != cudaSuccess)
+    return AFQ_ERR_CUDA;
+  for (int i = 0; i < n; i++) {   // later work on a handle's own stream follows the step
+    afq_handle* h = b->hs[i];
+    AFQ_CUDA(h, cudaStreamWaitEvent(h->st, b->done, 0));
+    for (int k = 0; k < AFQ_NSTAGES; k++) h->stage_launches[k] += b->counts[slot][i][k];
+    h->host_step = step_tot + 1;
+  }
+  return AFQ_OK;
+}
+
+afq_status afq_batch_synchronize(afq_batch* b) {
+  if (!b) return AFQ_ERR_ARG;
+  cudaSetDevice(b->device);
+  if (cudaStreamSynchronize(b->st) != cudaSuccess) return AFQ_ERR_CUDA;
+  for (afq_handle* h : b->hs) {
+    afq_status s = afq_synchronize(h);
+    if (s != AFQ_OK) return s;
+  }
+  return AFQ_OK;
+}
+
 afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
                             long long train_walker_steps, int subset_den) {
   if (!h || hidden <= 0 || hidden % 32 || hidden > 1024 || !(lr > 0.0) || subset_den < 1 ||
@@ -857,6 +989,18 @@ afq_status afq_cv_stats(afq_handle* h, double* stats) {
     return AFQ_OK;
   }
   afq::cv_stats(h->cv, stats);
+  return AFQ_OK;
+}
+
+afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms) {
+  if (!h || (!choice && !ms)) return AFQ_ERR_ARG;
+  int c[afq::TS_N + 1] = {};
+  float t[2 * afq::TS_N] = {};
+  if (h->mixed) afq::mixed_tuning(h->mixed, c, t);
+  for (int i = 0; i <= afq::TS_N; i++)
+    if (choice) choice[i] = c[i];
+  for (int i = 0; i < 2 * afq::TS_N; i++)
+    if (ms) ms[i] = t[i];
   return AFQ_OK;
 }
 

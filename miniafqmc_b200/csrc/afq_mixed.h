@@ -9,6 +9,11 @@ namespace afq {
 
 struct MixedState;
 
+// Product sites whose kernel (persistent or per-tile) is chosen at set-up by timing:
+// vHS, the propagation chain, the split-K vbias / Coulomb products, the exchange over all
+// walkers and over a 1/8 subset, and T1.
+enum TuneSite { TS_VHS, TS_PROP, TS_PART, TS_EXF, TS_EXS, TS_T1, TS_N };
+
 struct MixedInit {
   int N, n, nchol, nw, order;
   const z_t* P;             // Propg1 [N][N]
@@ -45,6 +50,9 @@ int mixed_launches(const MixedState* m, int stage);
 int mixed_nblk(const MixedState* m);
 // Timeout flags raised by the tensor-core kernels (0 when clean).
 cudaError_t mixed_error(MixedState* m, int* flags);
+// Kernel choices: choice[TS_N + 1] (0 built-in rule, 1 persistent, 2 per-tile; the last
+// entry is the split-K slice count), ms[TS_N][2] the set-up timings (0 when not timed).
+void mixed_tuning(const MixedState* m, int* choice, float* ms);
 // FP64 copy of the V operand ([nw][N*N]), for copy-out.
 cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st);
 

@@ -17,8 +17,13 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -130,6 +135,11 @@ struct MixedState {
   float2* T1 = nullptr;        // [nw][2][n][n]
   int bn_t1 = 0, bn_gc = 0;
   tc::Maps m_t1, m_gc[2];
+  // kernel of each product site (0 built-in rule, 1 persistent, 2 per-tile), chosen at
+  // set-up by timing the candidates on the real shapes; part_cap = split-K slots allocated
+  int tune[TS_N] = {};
+  float tune_ms[TS_N][2] = {};
+  int splits0 = 1, part_cap = 1;
 };
 
 namespace {
@@ -1054,13 +1064,18 @@ template <class E, class = void> struct EpiF16 : std::false_type {};
 template <class E>
 struct EpiF16<E, std::void_t<decltype(E::kF16)>> : std::integral_constant<bool, E::kF16> {};
 
+// Kernel variant of a product: 0 = the default rule (persistent unless the functor asks
+// for the per-tile kernel or AFQ_TC_PERSISTENT=0), 1 = persistent, 2 = per-tile.  The
+// set-up autotuner (mixed_tune) picks 1 or 2 per product site by timing both.
 template <int BN, int ST, bool SPLIT, class Epi, int MINB = 1, int FMT = 1>
 cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
-                     cudaStream_t st) {
-  if constexpr (!Epi::kTile && !tc::EpiPerTile<Epi>::value) {
+                     cudaStream_t st, int variant = 0) {
+  if constexpr (!Epi::kTile) {
     constexpr int PST = SPLIT ? 2 : 4;
     constexpr int WG = tc::EpiStaged<Epi>::value ? 1 : 2;
-    if (tc_persistent() || tc::EpiStaged<Epi>::value) {
+    const bool persist = tc::EpiStaged<Epi>::value || variant == 1 ||
+                         (variant == 0 && tc_persistent() && !tc::EpiPerTile<Epi>::value);
+    if (persist) {
       if constexpr (tc::PCfg<BN, PST, FMT, SPLIT, Epi, WG>::kFits)
         return tc::launch_persistent<BN, PST, FMT, SPLIT, Epi, WG>(mp, g, e, err, st);
       else
@@ -1079,25 +1094,26 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
 // the other's main loop (used when the epilogue needs no shared-memory tile).
 template <int BN, bool LEAN, class Epi>
 cudaError_t run_prec(int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, int* err,
-                     cudaStream_t st) {
+                     cudaStream_t st, int variant) {
   if (prec == PREC_SPLIT16) {
     if constexpr (EpiF16<Epi>::value)
-      return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1), 0>(mp, g, e, err, st);
+      return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1), 0>(mp, g, e, err, st, variant);
     else
       return cudaErrorInvalidValue;
   }
-  if (prec == PREC_SPLIT) return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st);
-  return run_gemm<BN, (LEAN ? 2 : 4), false, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st);
+  if (prec == PREC_SPLIT)
+    return run_gemm<BN, (LEAN ? 1 : 2), true, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st, variant);
+  return run_gemm<BN, (LEAN ? 2 : 4), false, Epi, (LEAN ? 2 : 1)>(mp, g, e, err, st, variant);
 }
 
 template <bool LEAN = false, class Epi>
 cudaError_t run_bn(int bn, int prec, const tc::Maps& mp, const tc::GemmShape& g, const Epi& e,
-                   int* err, cudaStream_t st) {
+                   int* err, cudaStream_t st, int variant = 0) {
   switch (bn) {
-    case 64: return run_prec<64, LEAN>(prec, mp, g, e, err, st);
-    case 128: return run_prec<128, LEAN>(prec, mp, g, e, err, st);
-    case 192: return run_prec<192, LEAN>(prec, mp, g, e, err, st);
-    case 256: return run_prec<256, LEAN>(prec, mp, g, e, err, st);
+    case 64: return run_prec<64, LEAN>(prec, mp, g, e, err, st, variant);
+    case 128: return run_prec<128, LEAN>(prec, mp, g, e, err, st, variant);
+    case 192: return run_prec<192, LEAN>(prec, mp, g, e, err, st, variant);
+    case 256: return run_prec<256, LEAN>(prec, mp, g, e, err, st, variant);
   }
   return cudaErrorInvalidValue;
 }
@@ -1108,10 +1124,10 @@ cudaError_t run_prop(MixedState* m, int prec, const tc::Maps& mp, const tc::Gemm
   const int n2 = 2 * m->n;
   if (n2 % 32 == 0) {
     EpiPropPair ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
-    return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st);
+    return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st, m->tune[TS_PROP]);
   }
   EpiProp ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
-  return run_bn(m->bn_prop, prec, mp, g, ep, m->err, st);
+  return run_bn(m->bn_prop, prec, mp, g, ep, m->err, st, m->tune[TS_PROP]);
 }
 
 int pick_bn(int cols) {
@@ -1120,6 +1136,16 @@ int pick_bn(int cols) {
   if (cols <= 192) return 192;
   if (cols <= 256) return 256;
   return 0;
+}
+
+// sp slices of the vbias / Coulomb K (a multiple of 64 each; fewer when K is short)
+void set_splits(MixedState* m, int sp) {
+  const long long Kq = m->greal ? m->NAK : 2 * m->NAK;
+  sp = std::max(1, std::min(32, sp));
+  long long ks = (Kq + sp - 1) / sp;
+  ks = (ks + 63) / 64 * 64;
+  m->splits = (int)((Kq + ks - 1) / ks);
+  m->ksplit = (int)ks;
 }
 
 bool map2(tc::Maps& mp, const Op& a, uint64_t Ka, uint64_t ra, uint64_t ba, uint64_t lda,
@@ -1152,6 +1178,8 @@ void parse_prec(MixedState* m) {
 }  // namespace
 
 // ------------------------------------------------------------ public entry points
+static cudaError_t mixed_tune(MixedState* m, cudaStream_t st);
+
 cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* msg,
                          cudaStream_t st) {
   *out = nullptr;
@@ -1245,17 +1273,19 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
       m->LhX.scale = gx16 ? m->sLh : 1.0f;
     }
   }
-  // split K of the vbias / Coulomb products so the grid covers the GPU
+  // split K of the vbias / Coulomb products so the grid covers the GPU (about four tiles
+  // per SM); the tuner also tries half and twice as many slices
   {
-    const long long Kq = m->greal ? NAK : 2 * NAK;
     const int tiles = ((nc + 127) / 128) * ((2 * nw + 127) / 128);
-    int sp = std::max(1, std::min(16, (int)((4 * 148 + tiles - 1) / tiles)));
-    long long ks = (Kq + sp - 1) / sp;
-    ks = (ks + 63) / 64 * 64;
-    sp = (int)((Kq + ks - 1) / ks);
-    m->splits = sp;
-    m->ksplit = (int)ks;
-    A(malloc_track(m, &m->part, (size_t)sp * nc * 2 * nw));
+    set_splits(m, std::max(1, std::min(16, (int)((4 * 148 + tiles - 1) / tiles))));
+    m->splits0 = m->splits;
+    const int ks = m->ksplit;
+    const char* fs = getenv("AFQ_SPLITK");   // forced slice count
+    set_splits(m, std::max(2 * m->splits0, fs ? atoi(fs) : 0));
+    m->part_cap = m->splits;
+    m->splits = m->splits0;
+    m->ksplit = ks;
+    A(malloc_track(m, &m->part, (size_t)m->part_cap * nc * 2 * nw));
   }
   if (e != cudaSuccess) return bail(e, "allocation");
   A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
@@ -1375,6 +1405,7 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     }
   }
   if (!ok) return bail(cudaSuccess, "tensor map encoding failed");
+  if ((e = mixed_tune(m, st)) != cudaSuccess) return bail(e, "kernel tuning");
   *out = m;
   return cudaSuccess;
 }
@@ -1403,23 +1434,27 @@ int mixed_launches(const MixedState* m, int stage) {
   return 0;
 }
 
-cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
-  const int nc = m->nc, nw = m->nw, N = m->N;
-  pack_x_kernel<<<dim3((nc + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(X, nc, nw, m->Kv,
-                                                                             m->s_real, m->Xf);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+// V = X^T Spvn of every walker from the packed fields Xf
+static cudaError_t vhs_product(MixedState* m, cudaStream_t st) {
+  const int nw = m->nw, N = m->N;
   if (m->vsym) {
     tc::GemmShape g{2 * nw, m->npairs * 256, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0,
                     true};
     EpiVhsSym epi{m->Vf, nw, N, m->pairs};
-    static const bool lean = getenv("AFQ_VHS_LEAN") != nullptr;   // 2 CTAs/SM, 1-stage rings
-    if (lean) return run_bn<true>(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
-    return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
+    return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, m->tune[TS_VHS]);
   }
   tc::GemmShape g{2 * nw, N * N, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0, true};
   EpiVhs epi{m->Vf, nw, (long long)N * N};
-  return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st);
+  return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, m->tune[TS_VHS]);
+}
+
+cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
+  const int nc = m->nc, nw = m->nw;
+  pack_x_kernel<<<dim3((nc + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(X, nc, nw, m->Kv,
+                                                                             m->s_real, m->Xf);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return vhs_product(m, st);
 }
 
 cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st) {
@@ -1471,7 +1506,7 @@ static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, f
   tc::GemmShape g{nc, 2 * nw, (int)(m->greal ? m->NAK : 2 * m->NAK), m->splits, 128,
                   (nc + 127) / 128, false, false, m->ksplit};
   EpiPart ep{m->part, nc, 2 * nw, (long long)nc * 2 * nw};
-  cudaError_t e = run_bn(128, prec, mp, g, ep, m->err, st);
+  cudaError_t e = run_bn(128, prec, mp, g, ep, m->err, st, m->tune[TS_PART]);
   if (e != cudaSuccess) return e;
   const bool f16 = prec == PREC_SPLIT16;
   reduce_part_kernel<<<grid_for((long long)nc * nw), 256, 0, st>>>(
@@ -1501,23 +1536,19 @@ cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t 
   return splitk_product(m, m->m_ej, m->prec_ej, m->sLh, cvec, st);
 }
 
-// Exchange partial sums Kpart[w][s][block] of the first nsub walkers packed in Gc.
-cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
-                           cudaStream_t st) {
-  if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
-  const bool f16 = m->Gx.f16;
-  if (f16) gc_scale_kernel<<<nsub, 256, 0, st>>>(Gc, m->NAK, m->wscale);
-  pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(
-      Gc, nsub, m->n, m->N, Op{}, m->Gx, m->nw, m->greal, f16 ? m->wscale : nullptr);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+// Exchange product of the first nsub walkers packed in Gx: the staged persistent kernel
+// (per-row traces from TMEM) for the compiled walker widths, else the per-tile kernel.
+static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nblk,
+                                    cudaStream_t st) {
   const int n = m->n;
+  const bool f16 = m->Gx.f16;
   const float as = f16 ? m->sLh : 1.0f;
   const float* ws = f16 ? m->wscale : nullptr;
   tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
                   m->ex_mtiles, true, true, 0};
-  if (tc_persistent()) {
-    switch (2 * n) {   // staged exchange for the compiled walker widths
+  const int v = m->tune[2 * nsub > m->nw ? TS_EXF : TS_EXS];
+  if (v == 1 || (v == 0 && tc_persistent())) {
+    switch (2 * n) {
       case 32: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
                              EpiExchangeStaged<32>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
@@ -1528,9 +1559,23 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
                              EpiExchangeStaged<96>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
     }
+    if (v == 1) return cudaErrorInvalidValue;
   }
   EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws};
   return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g, ep, m->err, st);
+}
+
+// Exchange partial sums Kpart[w][s][block] of the first nsub walkers packed in Gc.
+cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
+                           cudaStream_t st) {
+  if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
+  const bool f16 = m->Gx.f16;
+  if (f16) gc_scale_kernel<<<nsub, 256, 0, st>>>(Gc, m->NAK, m->wscale);
+  pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(
+      Gc, nsub, m->n, m->N, Op{}, m->Gx, m->nw, m->greal, f16 ? m->wscale : nullptr);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return exchange_product(m, nsub, Kpart, nblk, st);
 }
 
 bool mixed_has_dm(const MixedState* m) { return m && m->T1 && m->bn_t1 && m->bn_gc; }
@@ -1547,7 +1592,8 @@ cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, i
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   {  // T1 (conjugated) of both spins: one 128-row tile per walker
     tc::GemmShape g{128, 4 * n, 2 * N, nw, 128, 1, true, false, 0};
-    if ((e = run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st)) != cudaSuccess)
+    if ((e = run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st,
+                    m->tune[TS_T1])) != cudaSuccess)
       return e;
   }
   if ((e = launch_lu(m->T1, n, 2 * nw, m->Tinv, Wd, info, 1, save_old, st)) != cudaSuccess ||
@@ -1570,6 +1616,253 @@ cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpar
   cudaError_t e = mixed_coulomb(m, Gc, cvec, st);
   if (e != cudaSuccess) return e;
   return mixed_exchange(m, Gc, m->nw, Kpart, nblk, st);
+}
+
+// ------------------------------------------------------------ kernel autotuning
+// Times the candidate kernels of each product site on the real shapes and keeps the
+// fastest: persistent or per-tile for every site, and for the split-K vbias / Coulomb
+// products also half, once and twice the default slice count.  The per-step operands are
+// zeroed first and every timed product writes scratch only (S, F, Vf, T1, part and the
+// temporaries below), so the walkers are untouched.  AFQ_TUNE=0 keeps the built-in rules,
+// AFQ_TUNE=1 / 2 (or AFQ_TC_PERSISTENT=0) forces the persistent / per-tile kernel wherever
+// it exists, with the default slice count; AFQ_SPLITK=<s> sets the slice count.
+// Choices are cached per shape for the process (every handle of one shape computes with
+// the same kernels and slice counts, so its results do not depend on timing noise) and,
+// with AFQ_TUNE_CACHE=<file>, across processes: the file holds one line per shape and is
+// read before timing and appended after it.
+namespace {
+struct TuneRec {
+  int tune[TS_N];
+  float ms[TS_N][2];
+  int splits;
+};
+std::mutex tune_mu;
+std::map<std::string, TuneRec>& tune_cache() {
+  static std::map<std::string, TuneRec> c;
+  return c;
+}
+std::string tune_key(const MixedState* m) {
+  char b[256];
+  snprintf(b, sizeof b, "N%d_n%d_nc%d_nw%d_o%d_g%d_p%d_s%d_v%d_x%d_t%d_q%d%d%d%d%d%d%d",
+           m->N, m->n, m->nc, m->nw, m->in.order, (int)m->greal, (int)m->preal, (int)m->s_real,
+           (int)m->vsym, m->in.Lh ? 1 : 0, mixed_has_dm(m) ? 1 : 0, m->prec_vhs, m->prec_p,
+           m->prec_v1, m->prec_vk, m->prec_vbias, m->prec_ej, m->prec_ek);
+  return b;
+}
+std::set<std::string>& tune_file_keys() {   // shapes present in the loaded file
+  static std::set<std::string> k;
+  return k;
+}
+void tune_load(const char* path) {
+  static std::string loaded;
+  if (!path || loaded == path) return;
+  loaded = path;
+  tune_file_keys().clear();
+  FILE* f = fopen(path, "r");
+  if (!f) return;
+  char key[256];
+  TuneRec r{};
+  while (fscanf(f, "%255s", key) == 1) {
+    bool ok = true;
+    for (int i = 0; i < TS_N && ok; i++)
+      ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
+    if (!ok || fscanf(f, "%d", &r.splits) != 1) break;
+    tune_cache()[key] = r;
+    tune_file_keys().insert(key);
+  }
+  fclose(f);
+}
+void tune_save(const char* path, const std::string& key, const TuneRec& r) {
+  if (!path || !tune_file_keys().insert(key).second) return;
+  FILE* f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s", key.c_str());
+  for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
+  fprintf(f, " %d\n", r.splits);
+  fclose(f);
+}
+}  // namespace
+
+static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
+  const char* env = getenv("AFQ_TUNE");
+  int force = env ? atoi(env) : -1;
+  if (force == 0) {
+    if (const char* fs = getenv("AFQ_SPLITK")) set_splits(m, std::max(1, atoi(fs)));
+    return cudaSuccess;
+  }
+  if (force < 0 && !tc_persistent()) force = 2;   // AFQ_TC_PERSISTENT=0: per-tile kernels
+  const char* fsk = getenv("AFQ_SPLITK");
+  const std::string key = tune_key(m) + "_f" + std::to_string(force) + "_k" +
+                          std::to_string(fsk ? atoi(fsk) : 0);
+  const char* cache_path = getenv("AFQ_TUNE_CACHE");
+  {
+    std::lock_guard<std::mutex> lk(tune_mu);
+    tune_load(cache_path);
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+      const TuneRec& r = it->second;
+      for (int i = 0; i < TS_N; i++) {
+        m->tune[i] = r.tune[i];
+        m->tune_ms[i][0] = r.ms[i][0];
+        m->tune_ms[i][1] = r.ms[i][1];
+      }
+      if (r.splits >= 1) {
+        set_splits(m, r.splits);
+        if (m->splits > m->part_cap) set_splits(m, m->splits0);
+      }
+      tune_save(cache_path, key, r);   // a shape timed before the file was named
+      return cudaSuccess;
+    }
+  }
+  const int N = m->N, n = m->n, nw = m->nw, nc = m->nc;
+  const long long NAK = m->NAK;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  auto zero = [&](const Op& o, size_t count) {
+    if (o.hi) A(cudaMemsetAsync(o.hi, 0, sizeof(*o.hi) * count, st));
+    if (o.lo) A(cudaMemsetAsync(o.lo, 0, sizeof(*o.lo) * count, st));
+  };
+  zero(m->Xf, (size_t)2 * nw * m->Kv);
+  zero(m->Vf, (size_t)nw * N * 2 * N);
+  zero(m->F[0], (size_t)nw * 4 * n * 2 * N);
+  zero(m->F[1], (size_t)nw * 4 * n * 2 * N);
+  zero(m->Gb, (size_t)2 * nw * 2 * NAK);
+  if (m->in.Lh) zero(m->Gx, (size_t)nw * 2 * NAK * 2);
+  A(cudaMemsetAsync(m->S, 0, sizeof(float2) * (size_t)nw * N * 2 * n, st));
+  A(cudaMemsetAsync(m->wscale, 0, sizeof(float) * nw, st));
+  z_t* out = nullptr;   // vbias-shaped result of the split-K products
+  z_t* kp = nullptr;    // exchange partial sums
+  A(cudaMallocAsync(&out, sizeof(z_t) * (size_t)nc * nw, st));
+  if (m->in.Lh) A(cudaMallocAsync(&kp, sizeof(z_t) * (size_t)nw * 2 * m->ex_mtiles, st));
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  A(cudaEventCreate(&t0));
+  A(cudaEventCreate(&t1));
+  A(cudaStreamSynchronize(st));
+  bool fatal = e != cudaSuccess;
+  // mean time of one call after a warm-up call; < 0 when the candidate does not launch
+  auto timed = [&](const std::function<cudaError_t()>& run) -> float {
+    if (fatal) return -1.0f;
+    if (run() != cudaSuccess) {
+      cudaGetLastError();
+      return -1.0f;
+    }
+    cudaEventRecord(t0, st);
+    for (int r = 0; r < 3; r++) run();
+    cudaEventRecord(t1, st);
+    float ms = -1.0f;
+    if (cudaEventSynchronize(t1) != cudaSuccess || cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {
+      fatal = true;
+      return -1.0f;
+    }
+    return ms / 3.0f;
+  };
+  auto pick = [&](int site, const std::function<cudaError_t()>& run) {
+    int best = 0;
+    for (int v = 1; v <= 2; v++) {
+      if (force > 0 && v != force) continue;
+      m->tune[site] = v;
+      const float t = timed(run);
+      m->tune_ms[site][v - 1] = t > 0.0f ? t : 0.0f;
+      if (t > 0.0f && (!best || t < m->tune_ms[site][best - 1])) best = v;
+    }
+    m->tune[site] = best;
+  };
+  pick(TS_VHS, [&] { return vhs_product(m, st); });
+  {
+    const int mt = (N + 127) / 128, n2 = 2 * n;
+    const int Kp = m->preal ? N : 2 * N;
+    const int order = m->in.order;
+    pick(TS_PROP, [&] {   // the chain: two P products and `order` V products
+      tc::GemmShape gp{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
+      tc::GemmShape gv{N, 2 * n2, 2 * N, nw, 128, mt, true, true, 0};
+      cudaError_t r = run_prop(m, m->prec_p, m->m_pw[0], gp, 0, 0, 0, nullptr,
+                               next_op(m->F[1], m->prec_v1), st);
+      for (int k = 1; k <= order && r == cudaSuccess; k++)
+        r = run_prop(m, k == 1 ? m->prec_v1 : m->prec_vk, m->m_v[0], gv, 1, k, 0, nullptr,
+                     next_op(m->F[1], m->prec_vk), st);
+      if (r == cudaSuccess)
+        r = run_prop(m, m->prec_p, m->m_pw[0], gp, 0, 0, 0, nullptr, next_op(m->F[1], m->prec_p),
+                     st);
+      return r;
+    });
+  }
+  {  // split-K slices x kernel
+    int bs = m->splits0, bv = 0;
+    float bt = 0.0f, bms[2] = {0.0f, 0.0f};
+    const char* fs = getenv("AFQ_SPLITK");
+    const int fsp = fs ? std::max(1, atoi(fs)) : 0;
+    const int cand[3] = {fsp ? fsp : m->splits0, std::max(1, m->splits0 / 2), 2 * m->splits0};
+    // forced kernels or AFQ_SPLITK: one slice count
+    for (int c = 0; c < (force > 0 || fsp ? 1 : 3); c++) {
+      set_splits(m, cand[c]);
+      if (m->splits > m->part_cap) continue;
+      pick(TS_PART, [&] { return splitk_product(m, m->m_vbias, m->prec_vbias, m->sSpT, out, st); });
+      const int v = m->tune[TS_PART];
+      if (v && (!bv || m->tune_ms[TS_PART][v - 1] < bt)) {
+        bv = v;
+        bs = m->splits;
+        bt = m->tune_ms[TS_PART][v - 1];
+        bms[0] = m->tune_ms[TS_PART][0];
+        bms[1] = m->tune_ms[TS_PART][1];
+      }
+    }
+    set_splits(m, bs);
+    m->tune[TS_PART] = bv;
+    m->tune_ms[TS_PART][0] = bms[0];
+    m->tune_ms[TS_PART][1] = bms[1];
+  }
+  if (m->in.Lh) {
+    const int nsub = std::max(1, nw / 8);
+    pick(TS_EXF, [&] { return exchange_product(m, nw, kp, m->ex_mtiles, st); });
+    pick(TS_EXS, [&] { return exchange_product(m, nsub, kp, m->ex_mtiles, st); });
+  }
+  if (mixed_has_dm(m)) {
+    pick(TS_T1, [&] {
+      tc::GemmShape g{128, 4 * n, 2 * N, nw, 128, 1, true, false, 0};
+      return run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st, m->tune[TS_T1]);
+    });
+  }
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  if (out) cudaFreeAsync(out, st);
+  if (kp) cudaFreeAsync(kp, st);
+  A(cudaMemsetAsync(m->err, 0, sizeof(int), st));
+  A(cudaStreamSynchronize(st));
+  if (fatal && e == cudaSuccess) e = cudaGetLastError();
+  if (fatal && e == cudaSuccess) e = cudaErrorUnknown;
+  if (e == cudaSuccess) {
+    TuneRec r{};
+    for (int i = 0; i < TS_N; i++) {
+      r.tune[i] = m->tune[i];
+      r.ms[i][0] = m->tune_ms[i][0];
+      r.ms[i][1] = m->tune_ms[i][1];
+    }
+    r.splits = m->splits;
+    std::lock_guard<std::mutex> lk(tune_mu);
+    tune_cache()[key] = r;
+    tune_save(cache_path, key, r);
+  }
+  if (getenv("AFQ_TUNE_VERBOSE"))
+    fprintf(stderr, "afq tune: vhs %d (%.3f %.3f) prop %d (%.3f %.3f) part %d x%d (%.3f %.3f) "
+            "exf %d (%.3f %.3f) exs %d (%.3f %.3f) t1 %d (%.3f %.3f) ms\n",
+            m->tune[TS_VHS], m->tune_ms[TS_VHS][0], m->tune_ms[TS_VHS][1], m->tune[TS_PROP],
+            m->tune_ms[TS_PROP][0], m->tune_ms[TS_PROP][1], m->tune[TS_PART], m->splits,
+            m->tune_ms[TS_PART][0], m->tune_ms[TS_PART][1], m->tune[TS_EXF],
+            m->tune_ms[TS_EXF][0], m->tune_ms[TS_EXF][1], m->tune[TS_EXS],
+            m->tune_ms[TS_EXS][0], m->tune_ms[TS_EXS][1], m->tune[TS_T1], m->tune_ms[TS_T1][0],
+            m->tune_ms[TS_T1][1]);
+  return e;
+}
+
+void mixed_tuning(const MixedState* m, int* choice, float* ms) {
+  for (int i = 0; i < TS_N; i++) {
+    if (choice) choice[i] = m ? m->tune[i] : 0;
+    if (ms) {
+      ms[2 * i] = m ? m->tune_ms[i][0] : 0.0f;
+      ms[2 * i + 1] = m ? m->tune_ms[i][1] : 0.0f;
+    }
+  }
+  if (choice) choice[TS_N] = m ? m->splits : 0;
 }
 
 }  // namespace afq

@@ -129,6 +129,16 @@ CONFIGS = {
                  energy_every=10, with_vakbl=False),
 }
 
+# heterogeneous batch: three systems of uneven size advanced together (AfqmcBatch)
+C5_SYSTEMS = [
+    Config(96, 12, 384, 0.10, 4, dt=0.005, nwalk=128, nsteps=300, northo=5, energy_every=10,
+           with_vakbl=False),
+    Config(200, 40, 800, 0.10, 5, dt=0.005, nwalk=256, nsteps=300, northo=5, energy_every=10,
+           with_vakbl=False),
+    Config(320, 64, 1280, 0.10, 6, dt=0.005, nwalk=384, nsteps=300, northo=5, energy_every=10,
+           with_vakbl=False),
+]
+
 
 def _sym_chol_coo(rng, N: int, nchol: int, density: float, complex_chol: bool,
                   sigma: float = 0.05):

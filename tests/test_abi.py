@@ -41,3 +41,16 @@ def test_status_strings_without_gpu():
     lib = load_library()
     assert lib.afq_status_string(0) == b"ok"
     assert lib.afq_status_string(6) == b"singular overlap matrix"
+
+
+def test_batch_rejects_bad_arguments_without_gpu():
+    """The multi-system batch checks its arguments before touching the device."""
+    import ctypes
+    from miniafqmc_b200.afqmc import load_library
+    lib = load_library()
+    out = ctypes.c_void_p()
+    assert lib.afq_batch_create(None, 1, ctypes.byref(out)) == 1      # AFQ_ERR_ARG
+    arr = (ctypes.c_void_p * 1)(None)
+    assert lib.afq_batch_create(arr, 1, ctypes.byref(out)) == 1
+    assert lib.afq_batch_substep(None, None, 0, 5) == 1
+    assert lib.afq_batch_synchronize(None) == 1

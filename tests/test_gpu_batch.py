@@ -1,0 +1,57 @@
+"""Heterogeneous multi-system batch (no reference counterpart): three systems of uneven
+NMO, electron count and nchol (the C5 shapes, fewer walkers) advanced by AfqmcBatch with
+one graph launch per substep give the same walkers, weights and energies as the same
+systems advanced one by one with afq_substep (the same kernels in the same order per
+system: equal to 1e-13 relative)."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+_SYS = {}
+
+
+def systems():
+    if not _SYS:
+        from miniafqmc_b200.synthetic import C5_SYSTEMS, make_system
+        for i, c in enumerate(C5_SYSTEMS):
+            cfg = dataclasses.replace(c, nwalk=(16, 32, 24)[i])
+            _SYS[i] = (cfg, make_system(cfg))
+    return [_SYS[i] for i in range(len(_SYS))]
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_matches_systems_alone(mixed):
+    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_FP64, AFQ_PREC_MIXED
+    prec = AFQ_PREC_MIXED if mixed else AFQ_PREC_FP64
+    sys_ = systems()
+    alone = [AfqmcSys(s, c.nwalk, precision=prec, use_vakbl=False) for c, s in sys_]
+    grouped = [AfqmcSys(s, c.nwalk, precision=prec, use_vakbl=False) for c, s in sys_]
+    seeds = [c.seed for c, _ in sys_]
+    batch = AfqmcBatch(grouped)
+    for e in alone + grouped:
+        e.calculate_mixed_density_matrix()
+    for st in range(7):   # includes the orthogonalisation at step 5
+        for e, sd in zip(alone, seeds):
+            e.substep(sd, st, 5, graph=True)
+        batch.substep(seeds, st, 5)
+    batch.synchronize()
+    for a, g in zip(alone, grouped):
+        Wa, Da = a.get_walkers()
+        Wg, Dg = g.get_walkers()
+        assert rel(Wg, Wa) < 1e-13 and rel(Dg, Da) < 1e-13
+        for e in (a, g):
+            e.calculate_mixed_density_matrix()
+        ea, eg = a.calculate_energy("chol"), g.calculate_energy("chol")
+        assert abs(eg - ea) <= 1e-13 * abs(ea)
+        assert np.all(np.isfinite(Dg[:, 1].real)) and np.all(Dg[:, 1].real >= 0)
+    batch.close()
+    for e in alone + grouped:
+        e.close()
+

@@ -1,0 +1,102 @@
+"""Kernel autotuning of the mixed-precision products (no reference counterpart).
+
+afq_set_hamiltonian times the persistent and the per-tile tensor-core kernel of each
+product site (and the split-K slice count of vbias / Coulomb) on the handle's shapes and
+keeps the fastest.  Both kernels run the same MMA sequence per tile, so forcing one or the
+other (AFQ_TUNE=1 / 2) gives the same density matrix, vbias, vHS and walkers to 1e-12
+relative (forcing a kernel also keeps the default slice count); the exchange trace is
+summed in another order by the staged epilogue (1e-5 relative on E_K).  The timed choice
+is cached per shape, and in AFQ_TUNE_CACHE when set."""
+import numpy as np
+import pytest
+
+from conftest import system
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def run_step(s, nw, walkers):
+    """One step of the stage sequence, returning the intermediate arrays."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    e = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=walkers)
+    e.calculate_mixed_density_matrix()
+    e.get_vbias()
+    out = {"Gc": e.copy_out("Gc"), "vbias": e.copy_out("vbias")}
+    e.sigma(3, 1)
+    e.get_vHS()
+    out["vHS"] = e.copy_out("vHS")
+    e.propagate()
+    out["W"] = e.get_walkers()[0]
+    e.calculate_mixed_density_matrix()
+    out["E"] = e.calculate_energy("chol")
+    out["parts"] = e.copy_out("energy_parts")
+    out["tuning"] = e.tuning()
+    e.close()
+    return out
+
+
+def walkers(s, nw, seed=0, amp=0.05):
+    rng = np.random.default_rng(seed)
+    W, Wd = s.initial_walkers(nw)
+    W = W + amp * (rng.normal(size=W.shape) + 1j * rng.normal(size=W.shape))
+    Wd[:, 1] = rng.uniform(0.5, 1.5, nw)
+    return W, Wd
+
+
+@pytest.mark.parametrize("name,kw,nw", [("C1", {}, 16), ("C2", dict(with_vakbl=False), 64)])
+def test_forced_kernels_agree(name, kw, nw, monkeypatch):
+    s = system(name, **kw)
+    wk = walkers(s, nw)
+    res = {}
+    for force in ("1", "2"):
+        monkeypatch.setenv("AFQ_TUNE", force)
+        res[force] = run_step(s, nw, wk)
+    a, b = res["1"], res["2"]
+    for site in ("vhs", "propagate", "splitk", "t1"):
+        assert a["tuning"][site]["kernel"] == 1 and b["tuning"][site]["kernel"] == 2
+        assert a["tuning"][site]["ms"][0] > 0 and b["tuning"][site]["ms"][1] > 0
+    # the per-tile exchange exists for every width, the staged persistent one for 2n in
+    # {32, 64, 96} only (C1: 2n = 32, C2: 2n = 64); other widths keep the built-in rule
+    assert b["tuning"]["exchange_subset"]["kernel"] == 2
+    assert a["tuning"]["exchange_subset"]["kernel"] == (1 if 2 * s.n in (32, 64, 96) else 0)
+    for k in ("Gc", "vbias", "vHS", "W"):
+        assert rel(a[k], b[k]) < 1e-12, k
+    assert rel(a["parts"][:, :2], b["parts"][:, :2]) < 1e-12
+    assert rel(a["parts"][:, 2], b["parts"][:, 2]) < 1e-5
+    assert abs(a["E"] - b["E"]) < 1e-5 * abs(b["E"])
+
+
+def test_timed_choice_cached_per_shape(tmp_path, monkeypatch):
+    """The timed choice is one of the candidates, matches a forced run's results, is
+    reused by a second handle of the same shape and is written to AFQ_TUNE_CACHE."""
+    path = tmp_path / "tune.txt"
+    monkeypatch.delenv("AFQ_TUNE", raising=False)
+    monkeypatch.setenv("AFQ_TUNE_CACHE", str(path))
+    s = system("C2", with_vakbl=False)
+    nw = 32
+    wk = walkers(s, nw, seed=1)
+    t1 = run_step(s, nw, wk)
+    t2 = run_step(s, nw, wk)
+    tun = t1["tuning"]
+    for site in ("vhs", "propagate", "splitk", "exchange_all", "exchange_subset", "t1"):
+        assert tun[site]["kernel"] in (1, 2)
+        k = tun[site]["kernel"]
+        assert tun[site]["ms"][k - 1] > 0
+    assert tun["splitk_slices"] >= 1
+    assert t2["tuning"] == tun
+    for k in ("Gc", "vbias", "vHS", "W", "parts"):
+        assert np.array_equal(t1[k], t2[k]), k
+    lines = [ln.split() for ln in path.read_text().splitlines() if ln.strip()]
+    assert len(lines) == 1 and lines[0][0].startswith("N128_n32_nc512_nw32_")
+    assert int(lines[0][-1]) == tun["splitk_slices"]
+    assert [int(lines[0][1 + 3 * i]) for i in range(6)] == [
+        tun[s_]["kernel"] for s_ in ("vhs", "propagate", "splitk", "exchange_all",
+                                     "exchange_subset", "t1")]
+    # the density matrix precedes the split-K products: equal to a forced run's
+    monkeypatch.setenv("AFQ_TUNE", "1" if tun["t1"]["kernel"] == 1 else "2")
+    f = run_step(s, nw, wk)
+    assert rel(t1["Gc"], f["Gc"]) < 1e-12
