@@ -178,8 +178,9 @@ def mixed_propagate_bytes(cfg, nw, order=6, preal=True):
     """HBM bytes one mixed-form propagation stage must move with its operand layouts:
     the FP64 walkers in and out, and per product the bf16 operands read once (hi, plus lo
     for the split products), the fp32 Taylor sum read and written, and the next bf16
-    operand written (hi and lo).  With a real Propg1 (preal) the P W and P S products
-    read B operands of K = N (separate Re / Im rows) instead of 2N."""
+    operand written (hi, plus lo when the next product is split).  With a real Propg1
+    (preal) the P W and P S products read B operands of K = N (separate Re / Im rows)
+    instead of 2N."""
     N, n = cfg.nmo, cfg.nel
     W64 = nw * N * 2 * n * 16            # FP64 walkers
     F = nw * 4 * n * 2 * N * 2           # one bf16 part of a B operand
@@ -191,7 +192,7 @@ def mixed_propagate_bytes(cfg, nw, order=6, preal=True):
     tot += 2 * Fp + S + 2 * F            # S = P W (split): B hi+lo in, S out, next B out
     for k in range(1, order + 1):
         sp = split["V1"] if k == 1 else split["Vk"]
-        nxt = 2 * Fp if k == order else 2 * F
+        nxt = 2 * Fp if k == order else (2 * F if split["Vk"] else F)
         tot += V * (2 if sp else 1) + F * (2 if sp else 1) + 2 * S + nxt
     tot += 2 * Fp + W64                  # W = P S (split)
     return float(tot)
@@ -288,7 +289,7 @@ class Form:
             self.eng.cv_configure(hidden=256, lr=1e-3, seed=cfg.seed, train_walker_steps=2000,
                                   subset_den=8)
         self.stream = torch.cuda.ExternalStream(self.eng.stream)
-        self.energies, self.sig2 = [], []
+        self.energies, self.sig2, self.cvvar = [], [], []
 
     def measure(self, record=True):
         from miniafqmc_b200 import driver
@@ -302,7 +303,9 @@ class Form:
             self.energies.append(E)
             s2 = float(np.sum(w * w * (el - E) ** 2) / np.sum(w) ** 2)
             if self.mode == "cv":   # plus the sampling variance of the subset correction
-                s2 += e.cv_stats()["subset_var"]
+                v = e.cv_stats()["subset_var"]
+                s2 += v
+                self.cvvar.append(v)
             self.sig2.append(s2)
         return E
 
@@ -463,6 +466,9 @@ def main():
             "speedup_vs_fp64_plain": T_6 / T_m,
             "energy": {"measurements": len(Em), "mean_E_form": float(Em.mean()),
                        "mean_E_fp64": float(E6.mean()), "abs_dE_Ha": float(abs(Em.mean() - E6.mean())),
+                       # standard deviation of the mean difference from the control variate's
+                       # subset sampling (independent subsets per measurement); 0 without it
+                       "dE_cv_sigma_Ha": float(np.sqrt(np.sum(head.cvvar)) / max(len(head.cvvar), 1)),
                        "max_abs_dE_per_measurement_Ha": float(np.max(np.abs(Em - E6))),
                        "err_per_wall_s": {"form": eps_m, "fp64": eps_6,
                                           "fp64_over_form": eps_6 / eps_m,
@@ -486,6 +492,7 @@ def main():
         emx = head.eng.calculate_energy("chol")
         same["mixed_exact_minus_fp64_Ha"] = emx - e64
         cmp["energy"]["same_walkers"] = same
+        cmp["fp64_plain"]["kernel_tuning"] = ref.eng.tuning()
         ref.eng.close()
 
     if rank != 0:
@@ -551,8 +558,7 @@ def main():
         line.update(cmp)
     if head.mode == "cv":
         line["control_variate"] = head.eng.cv_stats()
-    if args.form != "fp64":
-        line["config"]["kernel_tuning"] = head.eng.tuning()
+    line["config"]["kernel_tuning"] = head.eng.tuning()
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -198,14 +198,20 @@ afq_status afq_profile(afq_handle* h, int enable);
  * ([AFQ_NSTAGES] each, either may be NULL); reset != 0 clears the accumulators.
  * Launch counts include graph substeps. */
 afq_status afq_stage_times(afq_handle* h, double* ms, long long* launches, int reset);
-/* Kernel choices of the mixed-precision products, made when afq_set_hamiltonian times
- * the candidates on the handle's own shapes.  No counterpart in the reference (its
- * kernels have fixed launch shapes).  Sites, in order: vHS, propagation chain, split-K
- * vbias / Coulomb, exchange over all walkers, exchange over a 1/8 subset, T1 = W^T trial.
- * choice[7]: per site 0 (built-in rule), 1 (persistent kernel) or 2 (per-tile kernel),
- * then the split-K slice count; ms[12]: per site the timed milliseconds of candidates 1
- * and 2 (0 when not timed).  AFQ_TUNE=0 in the environment skips the timing, AFQ_TUNE=1
- * or 2 forces one kernel.  All zeros for an FP64 handle. */
+/* Kernel choices made when afq_set_hamiltonian times the candidates on the handle's own
+ * shapes.  No counterpart in the reference (its kernels have fixed launch shapes).
+ * choice[12]:
+ *   [0..5]  mixed form, per tensor-core product site (vHS, propagation chain, split-K
+ *           vbias / Coulomb, exchange over all walkers, exchange over a 1/8 subset,
+ *           T1 = W^T trial): 0 built-in rule, 1 persistent kernel, 2 per-tile kernel;
+ *   [6]     mixed form: split-K slice count;
+ *   [7..11] FP64 form: CTA shape of the vHS CSR product, ZGEMM tile shape of the
+ *           propagation chain, dense vbias, Coulomb and dense Vakbl products
+ *           (0 built-in rule, k > 0 the k-th listed shape).
+ * ms[24]: for mixed sites the timed milliseconds of candidates 1 and 2, for FP64 sites
+ * those of the chosen shape and of the rule (0 when not timed).  Sites of the other form
+ * read 0.  AFQ_TUNE=0 in the environment skips the timing, AFQ_TUNE=1 or 2 forces one
+ * tensor-core kernel. */
 afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */

@@ -276,18 +276,28 @@ class AfqmcSys:
                 "restandardisations": int(v[6]), "fallback": bool(v[7])}
 
     TUNE_SITES = ["vhs", "propagate", "splitk", "exchange_all", "exchange_subset", "t1"]
+    TUNE_SITES_FP64 = ["vhs_csr", "propagate_zgemm", "vbias_zgemm", "coulomb_zgemm",
+                       "vakbl_zgemm"]
 
     def tuning(self) -> dict:
-        """Kernel picked per mixed-precision product site at set-up (0 built-in rule,
-        1 persistent, 2 per-tile), the timed milliseconds of both candidates, and the
-        split-K slice count of the vbias / Coulomb products."""
-        c = np.zeros(len(self.TUNE_SITES) + 1, dtype=np.int32)
-        t = np.zeros(2 * len(self.TUNE_SITES))
+        """Kernels picked at set-up.  Mixed form: per tensor-core product site 0 (built-in
+        rule), 1 (persistent) or 2 (per-tile) with the timed milliseconds of both
+        candidates, and the split-K slice count.  FP64 form: per site the chosen CTA /
+        tile shape index (0 = rule) with the milliseconds of the chosen shape and of the
+        rule."""
+        ns, nf = len(self.TUNE_SITES), len(self.TUNE_SITES_FP64)
+        c = np.zeros(ns + 1 + nf, dtype=np.int32)
+        t = np.zeros(2 * (ns + nf))
         self._check(self.lib.afq_get_tuning(self.h, _p(c), _p(t)))
+        if self.precision != AFQ_PREC_MIXED:
+            return {k: {"shape": int(c[ns + 1 + i]),
+                        "ms": [round(float(t[2 * (ns + i)]), 4),
+                               round(float(t[2 * (ns + i) + 1]), 4)]}
+                    for i, k in enumerate(self.TUNE_SITES_FP64)}
         out = {k: {"kernel": int(c[i]), "ms": [round(float(t[2 * i]), 4),
                                                round(float(t[2 * i + 1]), 4)]}
                for i, k in enumerate(self.TUNE_SITES)}
-        out["splitk_slices"] = int(c[-1])
+        out["splitk_slices"] = int(c[ns])
         return out
 
     def substep(self, seed: int, step_tot: int, northo: int, graph: bool = True):

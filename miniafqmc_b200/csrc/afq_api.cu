@@ -4,6 +4,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <algorithm>
+#include <functional>
+#include <mutex>
+#include <map>
 #include <vector>
 
 #include "../../include/afqmc_b200.h"
@@ -47,6 +51,13 @@ struct afq_handle {
   z_t *Gcloc = nullptr, *cvec = nullptr, *Kpart = nullptr;
   int nblk = 0;
   double* parts = nullptr;
+
+  // FP64 form: ZGEMM tile shape per site (propagation, dense vbias, Coulomb, dense Vakbl)
+  // and CTA shape of the vHS CSR product, 0 = built-in rule (fp64_tune); timings in ms of
+  // the chosen shape and of the rule
+  enum { F64_VHS, F64_PROP, F64_VBIAS, F64_COUL, F64_VAKBL, F64_N };
+  int f64cfg[F64_N] = {0};
+  float f64ms[F64_N][2] = {};
 
   afq::MixedState* mixed = nullptr;
   afq::CvState* cv = nullptr;
@@ -230,7 +241,7 @@ cudaError_t body_vbias(afq_handle* h) {
   if (h->spT_dense) {
     ZGemmDesc g{h->nc, h->nw, (int)h->NAK, h->spT_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
     EpiStore e{h->vbias, h->nw, 0, zmk(0, 0), 0};
-    return zgemm_launch<true, true>(g, 1, e, h->st);
+    return zgemm_launch<true, true>(g, 1, e, h->st, h->f64cfg[afq_handle::F64_VBIAS]);
   }
   return launch_csr_gather(h->spT_ri, h->spT_ci, h->spT_v, h->Gc, h->NAK, h->nc, h->nw, h->vbias,
                            h->st);
@@ -244,7 +255,8 @@ cudaError_t body_sigma(afq_handle* h, int use_xraw) {
 cudaError_t body_vhs(afq_handle* h) {
   if (h->mixed) return afq::mixed_vhs(h->mixed, h->X, h->vHS, h->st);
   return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, h->N * h->N, h->nw,
-                                h->vHS, (long long)h->N * h->N, h->st);
+                                h->vHS, (long long)h->N * h->N, h->st,
+                                h->f64cfg[afq_handle::F64_VHS]);
 }
 
 cudaError_t body_propagate(afq_handle* h) {
@@ -252,24 +264,25 @@ cudaError_t body_propagate(afq_handle* h) {
   if (h->mixed) return afq::mixed_propagate(h->mixed, h->W, h->vHS, h->st);
   const int N = h->N, n2 = 2 * h->n, nw = h->nw;
   const long long sWN = (long long)N * n2, sV = (long long)N * N;
+  const int zc = h->f64cfg[afq_handle::F64_PROP];
   cudaError_t e;
   {  // S = P W, T1 = S
     ZGemmDesc g{N, n2, N, h->P, N, 0, h->W, n2, sWN, zmk(1, 0)};
     EpiDual ep{h->T1, h->S, n2, sWN};
-    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st)) != cudaSuccess) return e;
+    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st, zc)) != cudaSuccess) return e;
   }
   z_t* cur = h->T1;
   z_t* nxt = h->T2;
   for (int k = 1; k <= h->d.taylor_order; k++) {  // T = (i/k) V T; S += T
     ZGemmDesc g{N, n2, N, h->vHS, N, sV, cur, n2, sWN, zmk(0.0, 1.0 / (double)k)};
     EpiTaylor ep{nxt, h->S, n2, sWN};
-    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st)) != cudaSuccess) return e;
+    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st, zc)) != cudaSuccess) return e;
     std::swap(cur, nxt);
   }
   {  // W = P S
     ZGemmDesc g{N, n2, N, h->P, N, 0, h->S, n2, sWN, zmk(1, 0)};
     EpiStore ep{h->W, n2, sWN, zmk(0, 0), 0};
-    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st)) != cudaSuccess) return e;
+    if ((e = zgemm_launch<true, false>(g, nw, ep, h->st, zc)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
@@ -293,7 +306,9 @@ cudaError_t body_energy(afq_handle* h, int mode) {
     if (h->vk_dense) {
       ZGemmDesc g{nak, h->nw, nak, h->vk_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
       EpiStore ep{h->Gcloc, h->nw, 0, zmk(0, 0), 0};
-      if ((e = zgemm_launch<true, true>(g, 1, ep, h->st)) != cudaSuccess) return e;
+      if ((e = zgemm_launch<true, true>(g, 1, ep, h->st, h->f64cfg[afq_handle::F64_VAKBL])) !=
+          cudaSuccess)
+        return e;
     } else {
       if ((e = launch_csr_gather(h->vk_ri, h->vk_ci, h->vk_v, h->Gc, h->NAK, nak, h->nw, h->Gcloc,
                                  h->st)) != cudaSuccess)
@@ -310,7 +325,9 @@ cudaError_t body_energy(afq_handle* h, int mode) {
     } else {
       ZGemmDesc g{h->nc, h->nw, nak, h->Lh, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
       EpiStore ep{h->cvec, h->nw, 0, zmk(0, 0), 0};
-      if ((e = zgemm_launch<true, true>(g, 1, ep, h->st)) != cudaSuccess) return e;
+      if ((e = zgemm_launch<true, true>(g, 1, ep, h->st, h->f64cfg[afq_handle::F64_COUL])) !=
+          cudaSuccess)
+        return e;
       int nb = 0;
       if ((e = afq::launch_exchange(h->Lh, h->Gc, h->N, h->n, h->nc, h->nw, h->Kpart, &nb,
                                     h->st)) != cudaSuccess)
@@ -383,6 +400,146 @@ void drop_graphs(afq_handle* h) {
   if (h->g_plain) cudaGraphExecDestroy(h->g_plain);
   if (h->g_ortho) cudaGraphExecDestroy(h->g_ortho);
   h->g_plain = h->g_ortho = nullptr;
+}
+
+// FP64 form: times the tile shapes of its ZGEMM sites and the CTA shapes of the vHS CSR
+// product on the handle's shapes (per-step scratch zeroed, products written to scratch)
+// and keeps the fastest.  Every shape sums each output in the same order, so results do
+// not depend on the choice.  A candidate whose first call takes over 3x the best so far is
+// dropped after that call; calls over 20 ms are timed once.  Choices are cached per shape
+// for the process.  AFQ_TUNE=0 keeps the built-in rules.
+cudaError_t fp64_tune(afq_handle* h) {
+  const char* env = getenv("AFQ_TUNE");
+  if (env && atoi(env) == 0) return cudaSuccess;
+  static std::mutex mu;
+  static std::map<std::string, std::vector<float>> cache;
+  char key[160];
+  snprintf(key, sizeof key, "N%d_n%d_nc%d_nw%d_sp%lld_d%d%d_l%d_v%d", h->N, h->n, h->nc, h->nw,
+           h->sp_ri ? 1LL : 0LL, h->spT_dense ? 1 : 0, h->vk_dense ? 1 : 0, h->Lh ? 1 : 0,
+           h->sp_rv ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      for (int i = 0; i < afq_handle::F64_N; i++) {
+        h->f64cfg[i] = (int)it->second[3 * i];
+        h->f64ms[i][0] = it->second[3 * i + 1];
+        h->f64ms[i][1] = it->second[3 * i + 2];
+      }
+      return cudaSuccess;
+    }
+  }
+  const int N = h->N, n2 = 2 * h->n, nw = h->nw, nak = (int)h->NAK;
+  cudaError_t e = cudaSuccess;
+  auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+  A(cudaMemsetAsync(h->vHS, 0, sizeof(z_t) * (size_t)nw * N * N, h->st));
+  A(cudaMemsetAsync(h->T1, 0, sizeof(z_t) * (size_t)nw * N * n2, h->st));
+  A(cudaMemsetAsync(h->X, 0, sizeof(z_t) * (size_t)h->nc * nw, h->st));
+  A(cudaMemsetAsync(h->Gc, 0, sizeof(z_t) * (size_t)nw * nak, h->st));
+  cudaEvent_t ev[4] = {};
+  for (auto& x : ev) A(cudaEventCreate(&x));
+  A(cudaStreamSynchronize(h->st));
+  // median (or single) time of one call after a warm-up call; < 0 when it fails
+  auto timed = [&](const std::function<cudaError_t()>& run, float cap) -> float {
+    if (e != cudaSuccess) return -1.0f;
+    cudaEventRecord(ev[0], h->st);
+    if (run() != cudaSuccess) {
+      cudaGetLastError();
+      return -1.0f;
+    }
+    cudaEventRecord(ev[1], h->st);
+    float t0 = -1.0f;
+    if (cudaEventSynchronize(ev[1]) != cudaSuccess) {
+      e = cudaGetLastError();
+      return -1.0f;
+    }
+    cudaEventElapsedTime(&t0, ev[0], ev[1]);
+    if (t0 > cap) return t0;        // far slower than the best: not a contender
+    if (t0 > 20.0f) {               // long call: time it once more, alone
+      cudaEventRecord(ev[0], h->st);
+      run();
+      cudaEventRecord(ev[1], h->st);
+      cudaEventSynchronize(ev[1]);
+      cudaEventElapsedTime(&t0, ev[0], ev[1]);
+      return t0;
+    }
+    cudaEventRecord(ev[0], h->st);
+    for (int r = 0; r < 3; r++) {
+      run();
+      cudaEventRecord(ev[r + 1], h->st);
+    }
+    if (cudaEventSynchronize(ev[3]) != cudaSuccess) {
+      e = cudaGetLastError();
+      return -1.0f;
+    }
+    float t[3];
+    for (int r = 0; r < 3; r++) cudaEventElapsedTime(&t[r], ev[r], ev[r + 1]);
+    std::sort(t, t + 3);
+    return t[1];
+  };
+  auto pick = [&](int site, int ncfg, const std::function<cudaError_t(int)>& run) {
+    float best = -1.0f, rule = -1.0f;
+    int bc = 0;
+    for (int c = 0; c <= ncfg; c++) {
+      const float t = timed([&] { return run(c); }, best > 0.0f ? 3.0f * best : 1e30f);
+      if (c == 0) rule = t;
+      if (t > 0.0f && (best < 0.0f || t < best)) {
+        best = t;
+        bc = c;
+      }
+    }
+    h->f64cfg[site] = bc;
+    h->f64ms[site][0] = best > 0.0f ? best : 0.0f;
+    h->f64ms[site][1] = rule > 0.0f ? rule : 0.0f;
+  };
+  pick(afq_handle::F64_VHS, afq::kCsrWalkerCfgs, [&](int c) {
+    return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, N * N, nw, h->vHS,
+                                  (long long)N * N, h->st, c);
+  });
+  pick(afq_handle::F64_PROP, kZgCfgs, [&](int c) {   // T2 = (i/k) V T1 of every walker
+    ZGemmDesc g{N, n2, N, h->vHS, N, (long long)N * N, h->T1, n2, (long long)N * n2, zmk(0, 1)};
+    EpiStore ep{h->T2, n2, (long long)N * n2, zmk(0, 0), 0};
+    return zgemm_launch<true, false>(g, nw, ep, h->st, c);
+  });
+  if (h->spT_dense)
+    pick(afq_handle::F64_VBIAS, kZgCfgs, [&](int c) {
+      ZGemmDesc g{h->nc, nw, nak, h->spT_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+      EpiStore ep{h->vbias, nw, 0, zmk(0, 0), 0};
+      return zgemm_launch<true, true>(g, 1, ep, h->st, c);
+    });
+  if (h->Lh && h->cvec)
+    pick(afq_handle::F64_COUL, kZgCfgs, [&](int c) {
+      ZGemmDesc g{h->nc, nw, nak, h->Lh, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+      EpiStore ep{h->cvec, nw, 0, zmk(0, 0), 0};
+      return zgemm_launch<true, true>(g, 1, ep, h->st, c);
+    });
+  if (h->vk_dense && h->Gcloc)
+    pick(afq_handle::F64_VAKBL, kZgCfgs, [&](int c) {
+      ZGemmDesc g{nak, nw, nak, h->vk_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+      EpiStore ep{h->Gcloc, nw, 0, zmk(0, 0), 0};
+      return zgemm_launch<true, true>(g, 1, ep, h->st, c);
+    });
+  for (auto& x : ev)
+    if (x) cudaEventDestroy(x);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+  if (e != cudaSuccess) return e;
+  if (getenv("AFQ_TUNE_VERBOSE"))
+    fprintf(stderr, "afq tune fp64: vhs %s (%.3f, rule %.3f) prop %s (%.3f, %.3f) vbias %s "
+            "(%.3f, %.3f) coulomb %s (%.3f, %.3f) vakbl %s (%.3f, %.3f) ms\n",
+            afq::csr_walker_cfg_name(h->f64cfg[0]), h->f64ms[0][0], h->f64ms[0][1],
+            zgemm_cfg_name(h->f64cfg[1]), h->f64ms[1][0], h->f64ms[1][1],
+            zgemm_cfg_name(h->f64cfg[2]), h->f64ms[2][0], h->f64ms[2][1],
+            zgemm_cfg_name(h->f64cfg[3]), h->f64ms[3][0], h->f64ms[3][1],
+            zgemm_cfg_name(h->f64cfg[4]), h->f64ms[4][0], h->f64ms[4][1]);
+  std::vector<float> rec;
+  for (int i = 0; i < afq_handle::F64_N; i++) {
+    rec.push_back((float)h->f64cfg[i]);
+    rec.push_back(h->f64ms[i][0]);
+    rec.push_back(h->f64ms[i][1]);
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  cache[key] = rec;
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -554,6 +711,7 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
       h->nblk = nb;
     }
   }
+  if (!h->mixed) AFQ_CUDA(h, fp64_tune(h));
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
   h->have_ham = true;
   return AFQ_OK;
@@ -1001,6 +1159,13 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms) {
     if (choice) choice[i] = c[i];
   for (int i = 0; i < 2 * afq::TS_N; i++)
     if (ms) ms[i] = t[i];
+  for (int i = 0; i < afq_handle::F64_N; i++) {   // FP64-form sites follow
+    if (choice) choice[afq::TS_N + 1 + i] = h->f64cfg[i];
+    if (ms) {
+      ms[2 * afq::TS_N + 2 * i] = h->f64ms[i][0];
+      ms[2 * afq::TS_N + 2 * i + 1] = h->f64ms[i][1];
+    }
+  }
   return AFQ_OK;
 }
 

@@ -11,9 +11,13 @@ cudaError_t launch_dm(const z_t* W, const z_t* tw, int N, int n, int nw, z_t* Gc
                       int* info, int want_gc, int save_old, cudaStream_t st);
 cudaError_t launch_sigma(const z_t* vbias, z_t* X, double* xraw, z_t* hybridW, int nchol,
                          int nw, const DevScalars* sc, int use_xraw, cudaStream_t st);
+// CSR x walker-fast dense (vHS = Spvn X).  cfg 0 is the built-in CTA shape (16 rows x 64
+// walkers), 1..kCsrWalkerCfgs the shapes the set-up tuner times (csr_walker_cfg_name).
+constexpr int kCsrWalkerCfgs = 7;
 cudaError_t launch_csr_walker(const int* rowIndex, const int* cols, const z_t* zvals,
                               const double* rvals, const z_t* B, int nrows, int nw, z_t* out,
-                              long long out_ld, cudaStream_t st);
+                              long long out_ld, cudaStream_t st, int cfg = 0);
+const char* csr_walker_cfg_name(int cfg);
 cudaError_t launch_csr_gather(const int* rowIndex, const int* cols, const z_t* vals, const z_t* G,
                               long long ldg, int nrows, int nw, z_t* out, cudaStream_t st);
 cudaError_t launch_weights(z_t* Wd, const z_t* hybridW, int nw, double dt, DevScalars* sc,

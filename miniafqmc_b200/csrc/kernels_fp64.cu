@@ -293,21 +293,22 @@ cudaError_t launch_sigma(const z_t* vbias, z_t* X, double* xraw, z_t* hybridW, i
 // fastest (vHS = Spvn X, vHS.hpp:47-56).  A warp owns a row; its lanes own walkers;
 // the nonzeros of a row are fetched 32 at a time and broadcast with shuffles.  The CTA
 // stages its [rows x walkers] results in shared memory and writes them walker-major.
-constexpr int VHS_ROWS = 16;      // warps (rows) per CTA
-constexpr int VHS_WALK = 64;      // walkers per CTA (2 per lane)
-
-template <bool REALV>
-__global__ void __launch_bounds__(VHS_ROWS * 32)
+// ROWS warps (rows) per CTA, WPL walkers per lane (CTA covers 32 WPL walkers); the set-up
+// tuner picks the shape (every shape sums each output in CSR order: same results).
+template <bool REALV, int ROWS, int WPL>
+__global__ void __launch_bounds__(ROWS * 32)
 csr_walker_kernel(const int* __restrict__ rowIndex, const int* __restrict__ cols,
                   const z_t* __restrict__ zvals, const double* __restrict__ rvals,
                   const z_t* __restrict__ B, int nrows, int nw, z_t* __restrict__ out,
                   long long out_ld) {
-  __shared__ z_t tile[VHS_ROWS][VHS_WALK + 1];
+  constexpr int WALK = 32 * WPL;
+  __shared__ z_t tile[ROWS][WALK + 1];
   const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
-  const int r0 = blockIdx.x * VHS_ROWS, r = r0 + wy;
-  const int w0 = blockIdx.y * VHS_WALK;
-  const int wa = w0 + lane, wb = w0 + 32 + lane;
-  z_t acc0 = zmk(0, 0), acc1 = zmk(0, 0);
+  const int r0 = blockIdx.x * ROWS, r = r0 + wy;
+  const int w0 = blockIdx.y * WALK;
+  z_t acc[WPL];
+#pragma unroll
+  for (int j = 0; j < WPL; j++) acc[j] = zmk(0, 0);
   if (r < nrows) {
     const int beg = rowIndex[r], end = rowIndex[r + 1];
     for (int p0 = beg; p0 < end; p0 += 32) {
@@ -325,39 +326,67 @@ csr_walker_kernel(const int* __restrict__ rowIndex, const int* __restrict__ cols
         const z_t* br = B + (long long)c * nw;
         if (REALV) {
           const double v = __shfl_sync(0xffffffffu, myr, q);
-          if (wa < nw) zfma_r(acc0, v, br[wa]);
-          if (wb < nw) zfma_r(acc1, v, br[wb]);
+#pragma unroll
+          for (int j = 0; j < WPL; j++) {
+            const int w = w0 + 32 * j + lane;
+            if (w < nw) zfma_r(acc[j], v, br[w]);
+          }
         } else {
           z_t v;
           v.x = __shfl_sync(0xffffffffu, myv.x, q);
           v.y = __shfl_sync(0xffffffffu, myv.y, q);
-          if (wa < nw) zfma(acc0, v, br[wa]);
-          if (wb < nw) zfma(acc1, v, br[wb]);
+#pragma unroll
+          for (int j = 0; j < WPL; j++) {
+            const int w = w0 + 32 * j + lane;
+            if (w < nw) zfma(acc[j], v, br[w]);
+          }
         }
       }
     }
   }
-  tile[wy][lane] = acc0;
-  tile[wy][lane + 32] = acc1;
+#pragma unroll
+  for (int j = 0; j < WPL; j++) tile[wy][32 * j + lane] = acc[j];
   __syncthreads();
-  for (int e = threadIdx.x; e < VHS_ROWS * VHS_WALK; e += VHS_ROWS * 32) {
-    const int wl = e / VHS_ROWS, rr = e % VHS_ROWS;
+  for (int e = threadIdx.x; e < ROWS * WALK; e += ROWS * 32) {
+    const int wl = e / ROWS, rr = e % ROWS;
     const int w = w0 + wl, rw = r0 + rr;
     if (w < nw && rw < nrows) out[(long long)w * out_ld + rw] = tile[rr][wl];
   }
 }
 
-cudaError_t launch_csr_walker(const int* rowIndex, const int* cols, const z_t* zvals,
+template <int ROWS, int WPL>
+cudaError_t csr_walker_launch(const int* rowIndex, const int* cols, const z_t* zvals,
                               const double* rvals, const z_t* B, int nrows, int nw, z_t* out,
                               long long out_ld, cudaStream_t st) {
-  dim3 grid((nrows + VHS_ROWS - 1) / VHS_ROWS, (nw + VHS_WALK - 1) / VHS_WALK);
+  dim3 grid((nrows + ROWS - 1) / ROWS, (nw + 32 * WPL - 1) / (32 * WPL));
   if (rvals)
-    csr_walker_kernel<true><<<grid, VHS_ROWS * 32, 0, st>>>(rowIndex, cols, nullptr, rvals, B,
-                                                            nrows, nw, out, out_ld);
+    csr_walker_kernel<true, ROWS, WPL><<<grid, ROWS * 32, 0, st>>>(rowIndex, cols, nullptr, rvals,
+                                                                   B, nrows, nw, out, out_ld);
   else
-    csr_walker_kernel<false><<<grid, VHS_ROWS * 32, 0, st>>>(rowIndex, cols, zvals, nullptr, B,
-                                                             nrows, nw, out, out_ld);
+    csr_walker_kernel<false, ROWS, WPL><<<grid, ROWS * 32, 0, st>>>(rowIndex, cols, zvals, nullptr,
+                                                                    B, nrows, nw, out, out_ld);
   return cudaGetLastError();
+}
+
+const char* csr_walker_cfg_name(int cfg) {
+  static const char* names[kCsrWalkerCfgs + 1] = {"16x2", "16x2", "8x2", "4x2",
+                                                  "16x1", "8x4",  "4x4", "32x1"};
+  return cfg >= 0 && cfg <= kCsrWalkerCfgs ? names[cfg] : "?";
+}
+
+// cfg: 0 built-in (16 rows x 2 walkers per lane), 1..kCsrWalkerCfgs the shapes above
+cudaError_t launch_csr_walker(const int* rowIndex, const int* cols, const z_t* zvals,
+                              const double* rvals, const z_t* B, int nrows, int nw, z_t* out,
+                              long long out_ld, cudaStream_t st, int cfg) {
+  switch (cfg) {
+    case 2: return csr_walker_launch<8, 2>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+    case 3: return csr_walker_launch<4, 2>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+    case 4: return csr_walker_launch<16, 1>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+    case 5: return csr_walker_launch<8, 4>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+    case 6: return csr_walker_launch<4, 4>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+    case 7: return csr_walker_launch<32, 1>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+    default: return csr_walker_launch<16, 2>(rowIndex, cols, zvals, rvals, B, nrows, nw, out, out_ld, st);
+  }
 }
 
 // ============================================================ CSR x walker-major G

@@ -844,6 +844,12 @@ struct EpiPart {
   }
 };
 
+// Split-K partials with the accumulator promoted every PKB K slabs (persistent kernel).
+template <int PKB>
+struct EpiPartPromoted : EpiPart {
+  static constexpr int kPromoteKB = PKB;
+};
+
 // Propagation products: tile rows i (orbital), columns [Re C | Im C] over the 2n walker
 // columns.  mode 0: S = C (P W); mode 1: T = (i/k) C, S += T (Taylor term k; the last
 // term forms S); mode 2: W = C (P S).  Modes 0 and 1 write the next B operand.
@@ -1047,6 +1053,96 @@ struct EpiExchangeStaged {
   }
 };
 
+// Exchange from register-promoted accumulators (persistent kernel, two epilogue
+// warpgroups, each owning BN / 2 columns = whole walkers): the K sum of T is chunked every
+// PKB slabs and added in fp32 registers.  Per walker, thread (cv, a) then sums
+// T[a][b] T[b][a] over b from its own row (registers) and column a of its Cholesky block,
+// which passes through shared memory as the real, then the imaginary parts of half the
+// block's rows at a time (scratch of 128 / n blocks x n / 2 rows x (n + 1) floats).
+template <int TWO_N, int PKB>
+struct EpiExchangePromoted {
+  static constexpr bool kTile = false, kPair = false, kF16 = true, kRegs = true;
+  static constexpr int kPromoteKB = PKB;
+  static constexpr int NH = TWO_N / 2;       // n
+  static constexpr int BW = NH / 2;          // rows of a block staged per pass
+  static constexpr int GMAX = 128 / NH;      // Cholesky blocks of a tile
+  static constexpr int LD = NH + 1;          // conflict-free column reads (LD odd)
+  static constexpr int kScratchBytes = GMAX * BW * LD * 4;
+  int n, Gn, Gw, nc, nw, nblk;
+  z_t* Kpart;
+  float ascale;
+  const float* wscale;
+  template <int CPW>
+  AFQ_D void regs(int s, int mt, int nt, int row, const float (&acc)[CPW], float* scr,
+                  int wg) const {
+    if constexpr (CPW % TWO_N != 0) {
+      return;   // not launched: the host requires whole walkers per warpgroup
+    } else {
+      constexpr int WPG = CPW / TWO_N;
+      __shared__ double red[2][2][4][2];
+      const int lane = row & 31, warp = row >> 5;
+      const int ncv = min(Gn, nc - mt * Gn);
+      const bool act = row < ncv * NH;
+      const bool slot = row < GMAX * NH;
+      const int cv = row / NH, a = row - cv * NH;
+      const float* col = scr + cv * BW * LD + a;
+#pragma unroll
+      for (int q = 0; q < WPG; q++) {
+        const float* re = acc + q * TWO_N;
+        const float* im = re + NH;
+        float fr = 0.0f, fi = 0.0f;
+#pragma unroll
+        for (int part = 0; part < 2; part++) {   // real, then imaginary rows
+          const float* mine = part ? im : re;
+#pragma unroll
+          for (int rc = 0; rc < 2; rc++) {
+            const int b0 = rc * BW;
+            if (slot && a >= b0 && a < b0 + BW) {
+              float* dst = scr + (cv * BW + a - b0) * LD;
+#pragma unroll
+              for (int c = 0; c < NH; c++) dst[c] = mine[c];
+            }
+            tc::epi_bar_group(wg);
+            if (act) {
+#pragma unroll
+              for (int bb = 0; bb < BW; bb++) {
+                const float v = col[bb * LD];
+                if (part == 0) {
+                  fr = fmaf(re[b0 + bb], v, fr);
+                  fi = fmaf(im[b0 + bb], v, fi);
+                } else {
+                  fr = fmaf(-im[b0 + bb], v, fr);
+                  fi = fmaf(re[b0 + bb], v, fi);
+                }
+              }
+            }
+            tc::epi_bar_group(wg);
+          }
+        }
+        double sr = fr, si = fi;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          sr += __shfl_xor_sync(0xffffffffu, sr, o);
+          si += __shfl_xor_sync(0xffffffffu, si, o);
+        }
+        if (lane == 0) {
+          red[wg][q & 1][warp][0] = sr;
+          red[wg][q & 1][warp][1] = si;
+        }
+        tc::epi_bar_group(wg);
+        const int w = nt * Gw + wg * WPG + q;
+        if (row == 0 && w < nw) {
+          const double (*r)[2] = red[wg][q & 1];
+          const double u = 1.0 / ((double)ascale * (wscale ? (double)wscale[w] : 1.0));
+          Kpart[((long long)w * 2 + s) * nblk + mt] =
+              zmk((((r[0][0] + r[1][0]) + r[2][0]) + r[3][0]) * u * u,
+                  (((r[0][1] + r[1][1]) + r[2][1]) + r[3][1]) * u * u);
+        }
+      }
+    }
+  }
+};
+
 // ------------------------------------------------------------ dispatch helpers
 // The persistent kernel (double-buffered accumulator) runs every product whose epilogue
 // needs no shared-memory tile; AFQ_TC_PERSISTENT=0 selects the per-tile kernel instead.
@@ -1057,6 +1153,26 @@ bool tc_persistent() {
     on = (e && atoi(e) == 0) ? 0 : 1;
   }
   return on == 1;
+}
+
+// K slabs per promoted chunk: AFQ_PROMOTE="part=<k>,ex=<k>" (0 turns promotion off)
+enum { PROMOTE_PART, PROMOTE_EXCHANGE };
+int promote_kb(int which) {
+  static int kb[2] = {-1, -1};
+  if (kb[0] < 0) {
+    // C4 (NMO 384, 48+48 electrons, nchol 1536, 1024 walkers), same walkers as the FP64
+    // form: E_J error 2e-6 Ha with part=2; E_K -1.4e-5 Ha with ex=1 (5.9 ms per 128-walker
+    // subset), -2.7e-5 Ha with ex=2 (4.7 ms), -9.1e-5 Ha without promotion (4.4 ms)
+    kb[0] = 2;
+    kb[1] = 2;
+    if (const char* env = getenv("AFQ_PROMOTE")) {
+      const std::string s(env);
+      const size_t p = s.find("part="), q = s.find("ex=");
+      if (p != std::string::npos) kb[0] = atoi(s.c_str() + p + 5);
+      if (q != std::string::npos) kb[1] = atoi(s.c_str() + q + 3);
+    }
+  }
+  return kb[which];
 }
 
 // Functors that may consume fp16 split operands (kF16) get that variant compiled.
@@ -1073,7 +1189,8 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
   if constexpr (!Epi::kTile) {
     constexpr int PST = SPLIT ? 2 : 4;
     constexpr int WG = tc::EpiStaged<Epi>::value ? 1 : 2;
-    const bool persist = tc::EpiStaged<Epi>::value || variant == 1 ||
+    constexpr bool only_persistent = tc::EpiStaged<Epi>::value || tc::EpiPromote<Epi>::value > 0;
+    const bool persist = only_persistent || variant == 1 ||
                          (variant == 0 && tc_persistent() && !tc::EpiPerTile<Epi>::value);
     if (persist) {
       if constexpr (tc::PCfg<BN, PST, FMT, SPLIT, Epi, WG>::kFits)
@@ -1082,7 +1199,7 @@ cudaError_t run_gemm(const tc::Maps& mp, const tc::GemmShape& g, const Epi& e, i
         return cudaErrorInvalidValue;
     }
   }
-  if constexpr (tc::EpiStaged<Epi>::value) {
+  if constexpr (tc::EpiStaged<Epi>::value || tc::EpiPromote<Epi>::value > 0) {
     return cudaErrorInvalidValue;
   } else {
     return tc::launch<BN, ST, FMT, SPLIT, Epi, MINB>(mp, g, e, err, st);
@@ -1506,7 +1623,15 @@ static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, f
   tc::GemmShape g{nc, 2 * nw, (int)(m->greal ? m->NAK : 2 * m->NAK), m->splits, 128,
                   (nc + 127) / 128, false, false, m->ksplit};
   EpiPart ep{m->part, nc, 2 * nw, (long long)nc * 2 * nw};
-  cudaError_t e = run_bn(128, prec, mp, g, ep, m->err, st, m->tune[TS_PART]);
+  cudaError_t e;
+  const int pk = promote_kb(PROMOTE_PART);
+  if (pk && m->tune[TS_PART] == 2) return cudaErrorInvalidValue;   // promotion: persistent only
+  switch (pk) {   // chained K slabs in TMEM (0: whole slice)
+    case 1: e = run_bn(128, prec, mp, g, EpiPartPromoted<1>{ep}, m->err, st); break;
+    case 2: e = run_bn(128, prec, mp, g, EpiPartPromoted<2>{ep}, m->err, st); break;
+    case 4: e = run_bn(128, prec, mp, g, EpiPartPromoted<4>{ep}, m->err, st); break;
+    default: e = run_bn(128, prec, mp, g, ep, m->err, st, m->tune[TS_PART]);
+  }
   if (e != cudaSuccess) return e;
   const bool f16 = prec == PREC_SPLIT16;
   reduce_part_kernel<<<grid_for((long long)nc * nw), 256, 0, st>>>(
@@ -1547,6 +1672,22 @@ static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nbl
   tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
                   m->ex_mtiles, true, true, 0};
   const int v = m->tune[2 * nsub > m->nw ? TS_EXF : TS_EXS];
+  const int pk = promote_kb(PROMOTE_EXCHANGE);
+  if ((v == 1 || (v == 0 && tc_persistent())) && pk && (m->ex_bn / 2) % (2 * n) == 0) {
+    cudaError_t r = cudaErrorInvalidValue;
+#define AFQ_EXP(TN, PK)                                                                        \
+  case TN * 8 + PK:                                                                            \
+    r = run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,                                               \
+               EpiExchangePromoted<TN, PK>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws}, \
+               m->err, st);                                                                    \
+    break;
+    switch (2 * n * 8 + pk) {   // promoted exchange for the compiled walker widths
+      AFQ_EXP(32, 1) AFQ_EXP(32, 2) AFQ_EXP(64, 1) AFQ_EXP(64, 2) AFQ_EXP(96, 1) AFQ_EXP(96, 2)
+    }
+#undef AFQ_EXP
+    // invalid value: no such instance, or its shared memory does not fit (nothing launched)
+    if (r != cudaErrorInvalidValue) return r;
+  }
   if (v == 1 || (v == 0 && tc_persistent())) {
     switch (2 * n) {
       case 32: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
@@ -1693,7 +1834,9 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   if (force < 0 && !tc_persistent()) force = 2;   // AFQ_TC_PERSISTENT=0: per-tile kernels
   const char* fsk = getenv("AFQ_SPLITK");
   const std::string key = tune_key(m) + "_f" + std::to_string(force) + "_k" +
-                          std::to_string(fsk ? atoi(fsk) : 0);
+                          std::to_string(fsk ? atoi(fsk) : 0) + "_p" +
+                          std::to_string(promote_kb(PROMOTE_PART)) +
+                          std::to_string(promote_kb(PROMOTE_EXCHANGE));
   const char* cache_path = getenv("AFQ_TUNE_CACHE");
   {
     std::lock_guard<std::mutex> lk(tune_mu);
@@ -1734,33 +1877,51 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   z_t* kp = nullptr;    // exchange partial sums
   A(cudaMallocAsync(&out, sizeof(z_t) * (size_t)nc * nw, st));
   if (m->in.Lh) A(cudaMallocAsync(&kp, sizeof(z_t) * (size_t)nw * 2 * m->ex_mtiles, st));
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
-  A(cudaEventCreate(&t0));
-  A(cudaEventCreate(&t1));
   A(cudaStreamSynchronize(st));
   bool fatal = e != cudaSuccess;
-  // mean time of one call after a warm-up call; < 0 when the candidate does not launch
+  // median time of three calls after a warm-up call; < 0 when the candidate does not
+  // launch or a kernel raised a timeout flag (the candidate is then never chosen)
+  const bool verbose = getenv("AFQ_TUNE_VERBOSE") != nullptr;
+  cudaEvent_t ev[4] = {};
+  for (auto& x : ev) A(cudaEventCreate(&x));
   auto timed = [&](const std::function<cudaError_t()>& run) -> float {
     if (fatal) return -1.0f;
+    cudaMemsetAsync(m->err, 0, sizeof(int), st);
     if (run() != cudaSuccess) {
       cudaGetLastError();
       return -1.0f;
     }
-    cudaEventRecord(t0, st);
-    for (int r = 0; r < 3; r++) run();
-    cudaEventRecord(t1, st);
-    float ms = -1.0f;
-    if (cudaEventSynchronize(t1) != cudaSuccess || cudaEventElapsedTime(&ms, t0, t1) != cudaSuccess) {
+    cudaEventRecord(ev[0], st);
+    for (int r = 0; r < 3; r++) {
+      run();
+      cudaEventRecord(ev[r + 1], st);
+    }
+    float t[3] = {-1.0f, -1.0f, -1.0f};
+    int flags = 0;
+    if (cudaEventSynchronize(ev[3]) != cudaSuccess ||
+        cudaMemcpy(&flags, m->err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
       fatal = true;
       return -1.0f;
     }
-    return ms / 3.0f;
+    for (int r = 0; r < 3; r++) cudaEventElapsedTime(&t[r], ev[r], ev[r + 1]);
+    if (verbose)
+      fprintf(stderr, "afq tune:   %.4f %.4f %.4f ms, flags %d\n", t[0], t[1], t[2], flags);
+    if (flags) {
+      cudaMemsetAsync(m->err, 0, sizeof(int), st);
+      return -1.0f;
+    }
+    std::sort(t, t + 3);
+    return t[1];
   };
-  auto pick = [&](int site, const std::function<cudaError_t()>& run) {
+  // candidates: both kernels, or (only_persistent) the promoted persistent one, whose
+  // accuracy the per-tile kernel does not match
+  auto pick = [&](int site, const std::function<cudaError_t()>& run, bool only_persistent = false) {
     int best = 0;
     for (int v = 1; v <= 2; v++) {
       if (force > 0 && v != force) continue;
+      if (only_persistent && force <= 0 && v == 2) continue;
       m->tune[site] = v;
+      if (verbose) fprintf(stderr, "afq tune: site %d kernel %d slices %d\n", site, v, m->splits);
       const float t = timed(run);
       m->tune_ms[site][v - 1] = t > 0.0f ? t : 0.0f;
       if (t > 0.0f && (!best || t < m->tune_ms[site][best - 1])) best = v;
@@ -1813,8 +1974,10 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   }
   if (m->in.Lh) {
     const int nsub = std::max(1, nw / 8);
-    pick(TS_EXF, [&] { return exchange_product(m, nw, kp, m->ex_mtiles, st); });
-    pick(TS_EXS, [&] { return exchange_product(m, nsub, kp, m->ex_mtiles, st); });
+    const bool exp = promote_kb(PROMOTE_EXCHANGE) > 0 && (2 * n) % 32 == 0 && 2 * n <= 96 &&
+                     (m->ex_bn / 2) % (2 * n) == 0;
+    pick(TS_EXF, [&] { return exchange_product(m, nw, kp, m->ex_mtiles, st); }, exp);
+    pick(TS_EXS, [&] { return exchange_product(m, nsub, kp, m->ex_mtiles, st); }, exp);
   }
   if (mixed_has_dm(m)) {
     pick(TS_T1, [&] {
@@ -1822,8 +1985,8 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       return run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st, m->tune[TS_T1]);
     });
   }
-  if (t0) cudaEventDestroy(t0);
-  if (t1) cudaEventDestroy(t1);
+  for (auto& x : ev)
+    if (x) cudaEventDestroy(x);
   if (out) cudaFreeAsync(out, st);
   if (kp) cudaFreeAsync(kp, st);
   A(cudaMemsetAsync(m->err, 0, sizeof(int), st));

@@ -119,6 +119,59 @@ AFQ_D void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// acc[i] += column i of 32 consecutive fp32 TMEM columns of this thread's lane.  Load,
+// wait and adds sit in one asm block so the 32 loaded values die at once (a promoting
+// epilogue holds its whole accumulator in registers next to them).
+AFQ_D void tmem_ld32_add(uint32_t taddr, float* acc) {
+  asm volatile(
+      "{\n .reg .b32 t0, t1, t2, t3, t4, t5, t6, t7, t8, t9, t10, t11, t12, t13, t14, t15, t16, t17, t18, t19, t20, t21, t22, t23, t24, t25, t26, t27, t28, t29, t30, t31;\n"
+      " tcgen05.ld.sync.aligned.32x32b.x32.b32 {t0, t1, t2, t3, t4, t5, t6, t7, t8, t9, t10, t11, t12, t13, t14, t15, t16, t17, t18, t19, t20, t21, t22, t23, t24, t25, t26, t27, t28, t29, t30, t31}, [%32];\n"
+      " tcgen05.wait::ld.sync.aligned;\n"
+      " add.f32 %0, %0, t0;\n"
+      " add.f32 %1, %1, t1;\n"
+      " add.f32 %2, %2, t2;\n"
+      " add.f32 %3, %3, t3;\n"
+      " add.f32 %4, %4, t4;\n"
+      " add.f32 %5, %5, t5;\n"
+      " add.f32 %6, %6, t6;\n"
+      " add.f32 %7, %7, t7;\n"
+      " add.f32 %8, %8, t8;\n"
+      " add.f32 %9, %9, t9;\n"
+      " add.f32 %10, %10, t10;\n"
+      " add.f32 %11, %11, t11;\n"
+      " add.f32 %12, %12, t12;\n"
+      " add.f32 %13, %13, t13;\n"
+      " add.f32 %14, %14, t14;\n"
+      " add.f32 %15, %15, t15;\n"
+      " add.f32 %16, %16, t16;\n"
+      " add.f32 %17, %17, t17;\n"
+      " add.f32 %18, %18, t18;\n"
+      " add.f32 %19, %19, t19;\n"
+      " add.f32 %20, %20, t20;\n"
+      " add.f32 %21, %21, t21;\n"
+      " add.f32 %22, %22, t22;\n"
+      " add.f32 %23, %23, t23;\n"
+      " add.f32 %24, %24, t24;\n"
+      " add.f32 %25, %25, t25;\n"
+      " add.f32 %26, %26, t26;\n"
+      " add.f32 %27, %27, t27;\n"
+      " add.f32 %28, %28, t28;\n"
+      " add.f32 %29, %29, t29;\n"
+      " add.f32 %30, %30, t30;\n"
+      " add.f32 %31, %31, t31;\n"
+      "}\n"
+      : "+f"(acc[0]), "+f"(acc[1]), "+f"(acc[2]), "+f"(acc[3]),
+        "+f"(acc[4]), "+f"(acc[5]), "+f"(acc[6]), "+f"(acc[7]),
+        "+f"(acc[8]), "+f"(acc[9]), "+f"(acc[10]), "+f"(acc[11]),
+        "+f"(acc[12]), "+f"(acc[13]), "+f"(acc[14]), "+f"(acc[15]),
+        "+f"(acc[16]), "+f"(acc[17]), "+f"(acc[18]), "+f"(acc[19]),
+        "+f"(acc[20]), "+f"(acc[21]), "+f"(acc[22]), "+f"(acc[23]),
+        "+f"(acc[24]), "+f"(acc[25]), "+f"(acc[26]), "+f"(acc[27]),
+        "+f"(acc[28]), "+f"(acc[29]), "+f"(acc[30]), "+f"(acc[31])
+      : "r"(taddr)
+      : "memory");
+}
+
 // Shared-memory matrix descriptor: K-major operand tile written by TMA with
 // SWIZZLE_128B (rows of 128 bytes, 8-row groups 1024 bytes apart).
 AFQ_D uint64_t sdesc_k128(uint32_t saddr) {
@@ -172,6 +225,21 @@ struct EpiStaged<E, std::void_t<decltype(E::kStaged)>> : std::integral_constant<
 template <class E, class = void> struct EpiPerTile : std::false_type {};
 template <class E>
 struct EpiPerTile<E, std::void_t<decltype(E::kPerTile)>> : std::integral_constant<bool, E::kPerTile> {};
+// kPromoteKB functors (persistent kernel only): the MMA restarts the accumulator every
+// kPromoteKB K slabs and the epilogue warps add the chunks in registers with
+// round-to-nearest fp32 adds.  The tensor pipe rounds its fp32 accumulator toward zero on
+// every MMA, which biases long sums of like-signed terms; promotion bounds every chain in
+// TMEM to kPromoteKB slabs.  Warpgroup g then owns the contiguous columns
+// [g BN / EPI_WG, (g + 1) BN / EPI_WG) and gets them as one register array: row-wise
+// functors are called per 32-column chunk, kRegs functors once through
+//   epi.regs(batch, m_tile, n_tile, tile_row, acc, scratch, wg).
+template <class E, class = void> struct EpiPromote : std::integral_constant<int, 0> {};
+template <class E>
+struct EpiPromote<E, std::void_t<decltype(E::kPromoteKB)>>
+    : std::integral_constant<int, E::kPromoteKB> {};
+template <class E, class = void> struct EpiRegs : std::false_type {};
+template <class E>
+struct EpiRegs<E, std::void_t<decltype(E::kRegs)>> : std::integral_constant<bool, E::kRegs> {};
 template <class E, class = void> struct EpiScratch : std::integral_constant<int, 0> {};
 template <class E>
 struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
@@ -385,6 +453,9 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int WPROD = P::NEPI / 32, WMMA = WPROD + 1;
+  constexpr int PK = EpiPromote<Epi>::value;
+  static_assert(PK == 0 || !(Epi::kPair || EpiStaged<Epi>::value),
+                "promotion: row-wise or kRegs functors");
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
       mbar_init(&full[s], 1);
@@ -439,55 +510,108 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
     // the last fills of each stage land before the CTA can exit
     for (int q = max(0, g - STAGES); q < g; q++) mbar_wait(&full[q % STAGES], (q / STAGES) & 1);
   } else if (warp == WMMA && lane == 0) {
-    // ---- MMA issuer
+    // ---- MMA issuer: one accumulator buffer per tile, or per K chunk when promoting
     constexpr uint32_t ID = idesc(128, BN, FMT);
     int g = 0, li = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < total && ok; t += gridDim.x, li++) {
+    for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
       int z, mt, nt;
       sched.decode(t, z, mt, nt);
       const int kbase = k_split ? z * k_split : 0;
       const int klen = k_split ? min(k_split, K - kbase) : K;
       const int nk = (klen + C::BK - 1) / C::BK;
-      const int b = li & 1;
-      if (!mbar_wait(&acce[b], ((li >> 1) & 1) ^ 1)) {   // the epilogue released buffer b
-        atomicOr(err, ERR_TIMEOUT_MMA);
-        break;
-      }
-      tc_fence_after();
-      const uint32_t d = tmem + b * C::TMEM_COLS;
-      for (int kb = 0; kb < nk; kb++, g++) {
-        const int s = g % STAGES;
-        if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+      const int nch = PK ? (nk + PK - 1) / PK : 1;
+      for (int ch = 0; ch < nch && ok; ch++, li++) {
+        const int b = li & 1;
+        if (!mbar_wait(&acce[b], ((li >> 1) & 1) ^ 1)) {   // the epilogue released buffer b
           atomicOr(err, ERR_TIMEOUT_MMA);
           ok = false;
           break;
         }
         tc_fence_after();
-        const uint64_t ad = sdesc_k128(smem_u32(stA(s, 0)));
-        const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
-#pragma unroll
-        for (int k = 0; k < C::BK / C::UK; k++)
-          umma<FMT>(d, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
-        if (SPLIT) {
-          const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
-          const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
-#pragma unroll
-          for (int k = 0; k < C::BK / C::UK; k++) {
-            umma<FMT>(d, ad + 2 * k, bl + 2 * k, ID, 1u);
-            umma<FMT>(d, al + 2 * k, bd + 2 * k, ID, 1u);
+        const uint32_t d = tmem + b * C::TMEM_COLS;
+        const int kb0 = PK ? ch * PK : 0, kb1 = PK ? min(nk, kb0 + PK) : nk;
+        for (int kb = kb0; kb < kb1; kb++, g++) {
+          const int s = g % STAGES;
+          if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+            atomicOr(err, ERR_TIMEOUT_MMA);
+            ok = false;
+            break;
           }
+          tc_fence_after();
+          const uint64_t ad = sdesc_k128(smem_u32(stA(s, 0)));
+          const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
+#pragma unroll
+          for (int k = 0; k < C::BK / C::UK; k++)
+            umma<FMT>(d, ad + 2 * k, bd + 2 * k, ID, (kb != kb0 || k != 0) ? 1u : 0u);
+          if (SPLIT) {
+            const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
+            const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
+#pragma unroll
+            for (int k = 0; k < C::BK / C::UK; k++) {
+              umma<FMT>(d, ad + 2 * k, bl + 2 * k, ID, 1u);
+              umma<FMT>(d, al + 2 * k, bd + 2 * k, ID, 1u);
+            }
+          }
+          umma_commit(&empty[s]);
         }
-        umma_commit(&empty[s]);
+        if (!ok) break;
+        umma_commit(&accf[b]);
       }
-      if (!ok) break;
-      umma_commit(&accf[b]);
     }
     umma_commit(fin);   // fires once every MMA issued above has completed
     mbar_wait(fin, 0);
   }
 
-  if (warp < WPROD) {
+  if constexpr (PK > 0) {
+    if (warp < WPROD) {
+      // ---- promoting epilogue: warpgroup wg sums its columns over the K chunks
+      constexpr int CPW = BN / EPI_WG;
+      static_assert(CPW % 32 == 0, "promotion: whole 32-column chunks per warpgroup");
+      const int wg = warp >> 2, wq = warp & 3;
+      const int row = wq * 32 + lane;
+      float* scr = scratch + (size_t)wg * (EpiScratch<Epi>::value / 4);
+      float acc[CPW];
+      int li = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        int z, mt, nt;
+        sched.decode(t, z, mt, nt);
+        const int kbase = k_split ? z * k_split : 0;
+        const int klen = k_split ? min(k_split, K - kbase) : K;
+        const int nk = (klen + C::BK - 1) / C::BK;
+        const int nch = (nk + PK - 1) / PK;
+        for (int ch = 0; ch < nch; ch++, li++) {
+          const int b = li & 1;
+          if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
+            if (lane == 0) atomicOr(err, ERR_TIMEOUT_EPILOGUE);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t trow =
+              tmem + b * C::TMEM_COLS + ((uint32_t)(wq * 32) << 16) + (uint32_t)(wg * CPW);
+          if (ch == 0) {
+#pragma unroll
+            for (int j = 0; j < CPW / 32; j++) tmem_ld32(trow + j * 32, acc + j * 32);
+          } else {
+#pragma unroll
+            for (int j = 0; j < CPW / 32; j++) tmem_ld32_add(trow + j * 32, acc + j * 32);
+          }
+          tc_fence_before();
+          mbar_arrive(&acce[b]);
+        }
+        if (!ok) break;
+        if constexpr (EpiRegs<Epi>::value) {
+          epi.regs(z, mt, nt, row, acc, scr, wg);
+        } else {
+          const int m0 = mt * m_step, n0 = nt * BN;
+#pragma unroll
+          for (int j = 0; j < CPW / 32; j++) epi(z, row, m0 + row, n0 + wg * CPW + j * 32, acc + j * 32);
+        }
+      }
+    }
+  } else if (warp < WPROD) {
     // ---- epilogue: warpgroup wg takes chunks wg, wg + EPI_WG, ...; TMEM lane = tile row
     const int wg = warp >> 2, wq = warp & 3;
     const int row = wq * 32 + lane;

@@ -154,9 +154,21 @@ zgemm_kernel(ZGemmDesc d, Epi epi) {
     }
 }
 
-// Host-side launcher: picks the tile width from N and sets the dynamic shared memory.
+// Tile shapes (BM x BN, TM x TN per thread, 256 threads) a launch may use: 0 picks by N,
+// 1..kZgCfgs the entries of this list (the set-up tuner times them).  Every shape sums each
+// output over K in the same order, so the choice never changes a result.
+constexpr int kZgCfgs = 7;
+inline const char* zgemm_cfg_name(int cfg) {
+  static const char* names[kZgCfgs + 1] = {"rule",     "64x32/4x2", "64x64/4x4", "64x96/4x6",
+                                           "32x64/2x4", "32x96/2x6", "128x64/8x4", "32x32/2x2"};
+  return cfg >= 0 && cfg <= kZgCfgs ? names[cfg] : "?";
+}
+
+// Host-side launcher: tile shape `cfg` (0: picked from N), dynamic shared memory set once
+// per instantiation.
 template <bool A_KMAJ, bool B_KMAJ, class Epi>
-cudaError_t zgemm_launch(const ZGemmDesc& d, int batch, const Epi& epi, cudaStream_t st) {
+cudaError_t zgemm_launch(const ZGemmDesc& d, int batch, const Epi& epi, cudaStream_t st,
+                         int cfg = 0) {
   if (d.M <= 0 || d.N <= 0 || batch <= 0) return cudaSuccess;
 #define AFQ_ZG_CASE(BM_, BN_, TM_, TN_)                                                     \
   {                                                                                        \
@@ -172,6 +184,16 @@ cudaError_t zgemm_launch(const ZGemmDesc& d, int batch, const Epi& epi, cudaStre
     dim3 grid((d.N + BN_ - 1) / BN_, (d.M + BM_ - 1) / BM_, batch);                        \
     kern<<<grid, Cfg::NT, Cfg::SMEM, st>>>(d, epi);                                        \
     return cudaGetLastError();                                                             \
+  }
+  switch (cfg) {
+    case 1: AFQ_ZG_CASE(64, 32, 4, 2)
+    case 2: AFQ_ZG_CASE(64, 64, 4, 4)
+    case 3: AFQ_ZG_CASE(64, 96, 4, 6)
+    case 4: AFQ_ZG_CASE(32, 64, 2, 4)
+    case 5: AFQ_ZG_CASE(32, 96, 2, 6)
+    case 6: AFQ_ZG_CASE(128, 64, 8, 4)
+    case 7: AFQ_ZG_CASE(32, 32, 2, 2)
+    default: break;
   }
   if (d.N <= 32) AFQ_ZG_CASE(64, 32, 4, 2)
   if (d.N <= 64 || (d.N > 96 && d.N <= 128)) AFQ_ZG_CASE(64, 64, 4, 4)

@@ -4,8 +4,10 @@ afq_set_hamiltonian times the persistent and the per-tile tensor-core kernel of 
 product site (and the split-K slice count of vbias / Coulomb) on the handle's shapes and
 keeps the fastest.  Both kernels run the same MMA sequence per tile, so forcing one or the
 other (AFQ_TUNE=1 / 2) gives the same density matrix, vbias, vHS and walkers to 1e-12
-relative (forcing a kernel also keeps the default slice count); the exchange trace is
-summed in another order by the staged epilogue (1e-5 relative on E_K).  The timed choice
+relative (forcing a kernel also keeps the default slice count); the split-K products
+promote their accumulator every few K slabs and run on the persistent kernel only; the
+exchange of the per-tile kernel keeps one accumulation chain over K (1e-5 relative on
+E_K against the promoted persistent one).  The timed choice
 is cached per shape, and in AFQ_TUNE_CACHE when set."""
 import numpy as np
 import pytest
@@ -56,9 +58,12 @@ def test_forced_kernels_agree(name, kw, nw, monkeypatch):
         monkeypatch.setenv("AFQ_TUNE", force)
         res[force] = run_step(s, nw, wk)
     a, b = res["1"], res["2"]
-    for site in ("vhs", "propagate", "splitk", "t1"):
+    for site in ("vhs", "propagate", "t1"):
         assert a["tuning"][site]["kernel"] == 1 and b["tuning"][site]["kernel"] == 2
         assert a["tuning"][site]["ms"][0] > 0 and b["tuning"][site]["ms"][1] > 0
+    # the split-K products promote their accumulator: persistent kernel only (forcing the
+    # per-tile kernel leaves the built-in rule)
+    assert a["tuning"]["splitk"]["kernel"] == 1 and b["tuning"]["splitk"]["kernel"] == 0
     # the per-tile exchange exists for every width, the staged persistent one for 2n in
     # {32, 64, 96} only (C1: 2n = 32, C2: 2n = 64); other widths keep the built-in rule
     assert b["tuning"]["exchange_subset"]["kernel"] == 2
@@ -66,6 +71,8 @@ def test_forced_kernels_agree(name, kw, nw, monkeypatch):
     for k in ("Gc", "vbias", "vHS", "W"):
         assert rel(a[k], b[k]) < 1e-12, k
     assert rel(a["parts"][:, :2], b["parts"][:, :2]) < 1e-12
+    # E_K: promoted persistent exchange against the per-tile one (its accumulator chains
+    # over the whole K, so it carries the truncation bias, ~4e-6 relative at C4)
     assert rel(a["parts"][:, 2], b["parts"][:, 2]) < 1e-5
     assert abs(a["E"] - b["E"]) < 1e-5 * abs(b["E"])
 
@@ -100,3 +107,36 @@ def test_timed_choice_cached_per_shape(tmp_path, monkeypatch):
     monkeypatch.setenv("AFQ_TUNE", "1" if tun["t1"]["kernel"] == 1 else "2")
     f = run_step(s, nw, wk)
     assert rel(t1["Gc"], f["Gc"]) < 1e-12
+
+
+@pytest.mark.parametrize("kw", [{}, dict(density=0.3, nchol=128)])
+def test_fp64_shapes_do_not_change_results(kw, monkeypatch):
+    """FP64 form: the tuner's CTA / tile shapes (CSR vHS, ZGEMM propagation, dense vbias,
+    Coulomb and Vakbl) sum every output in the same order, so a tuned handle and one on
+    the built-in rules (AFQ_TUNE=0) give bit-identical walkers and energies."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64
+    s = system("C1", **kw)
+    nw = 16
+    wk = walkers(s, nw, seed=2)
+    out = {}
+    for tune in ("0", None):
+        if tune is None:
+            monkeypatch.delenv("AFQ_TUNE", raising=False)
+        else:
+            monkeypatch.setenv("AFQ_TUNE", tune)
+        e = AfqmcSys(s, nw, precision=AFQ_PREC_FP64, walkers=wk)
+        e.calculate_mixed_density_matrix()
+        for st in range(6):
+            e.substep(4, st, 5, graph=True)
+        e.calculate_mixed_density_matrix()
+        out[tune] = (e.get_walkers(), e.calculate_energy("chol"), e.calculate_energy("vakbl"),
+                     e.tuning())
+        e.close()
+    (W0, D0), ec0, ev0, t0 = out["0"]
+    (W1, D1), ec1, ev1, t1 = out[None]
+    assert all(v["shape"] == 0 for v in t0.values())
+    assert t1["vhs_csr"]["ms"][0] > 0 and t1["propagate_zgemm"]["ms"][0] > 0
+    if kw:   # dense SpvnT above the density threshold
+        assert t1["vbias_zgemm"]["ms"][0] > 0
+    assert np.array_equal(W0, W1) and np.array_equal(D0, D1)
+    assert ec0 == ec1 and ev0 == ev1
