@@ -51,7 +51,7 @@ METRIC = "walker-steps/s"
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=40)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--config", default="C4")
@@ -333,6 +333,9 @@ def timed(form, steps, start, torch, dist, world, profile=False, record=True):
     e0.record(form.stream)
     for st in range(start, start + steps):
         form.step(st, record=record, graph=not profile)   # stage events need op-by-op calls
+    # the control variate's online training runs on its own stream after each measurement;
+    # wait for it (afq_synchronize) so the region holds the last one too, then close it
+    e.synchronize()
     e1.record(form.stream)
     torch.cuda.nvtx.range_pop()
     e.synchronize()
@@ -348,12 +351,113 @@ def timed(form, steps, start, torch, dist, world, profile=False, record=True):
     return ms, wall, stages
 
 
+def run_c5(args, torch):
+    """Heterogeneous batch (three systems of uneven NMO, electron count and nchol, mixed
+    form, one control variate each): K substeps advanced as one CUDA-graph launch per
+    substep for all systems (AfqmcBatch), against the same systems each launching its own
+    substep graph on its own stream (independent) and one after another with a
+    synchronisation between systems (serial).  Energies every energy_every substeps.
+    Times are wall clock around device-synchronised loops (several streams)."""
+    from miniafqmc_b200.synthetic import C5_SYSTEMS, make_system
+    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_MIXED
+    from miniafqmc_b200 import driver
+    systems = [(c, make_system(c)) for c in C5_SYSTEMS]
+    nws = [c.nwalk for c, _ in systems]
+    seeds = [c.seed for c, _ in systems]
+
+    def fresh():
+        engs = []
+        for c, sy in systems:
+            e = AfqmcSys(sy, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False)
+            e.cv_configure(hidden=256, lr=1e-3, seed=c.seed, train_walker_steps=2000, subset_den=8)
+            e.calculate_mixed_density_matrix()
+            driver.energy(e, "cv", None)
+            engs.append(e)
+        return engs
+
+    def measure(engs):
+        return [driver.energy(e, "cv", None) for e in engs]
+
+    def warm(engs, step_fn):
+        st = 0
+        while st < args.warmup or any(not e.cv_stats()["active"] for e in engs) or \
+                st % args.energy_every:
+            step_fn(st)
+            st += 1
+            if st % args.energy_every == 0:
+                for e in engs:
+                    e.calculate_mixed_density_matrix()
+                measure(engs)
+        return st
+
+    def run(mode):
+        engs = fresh()
+        batch = AfqmcBatch(engs) if mode == "batch" else None
+
+        def step(st):
+            if batch is not None:
+                batch.substep(seeds, st, args.northo)
+                return
+            for e, sd in zip(engs, seeds):
+                e.substep(sd, st, args.northo, graph=True)
+                if mode == "serial":
+                    e.synchronize()
+
+        st0 = warm(engs, step)
+        if batch is not None:
+            batch.synchronize()
+        for e in engs:
+            e.synchronize()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for st in range(st0, st0 + args.steps):
+            step(st)
+            if (st + 1) % args.energy_every == 0:
+                for e in engs:
+                    e.calculate_mixed_density_matrix()
+                measure(engs)
+        if batch is not None:
+            batch.synchronize()
+        for e in engs:
+            e.synchronize()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        cv = [e.cv_stats() for e in engs]
+        tun = [e.tuning() for e in engs]
+        if batch is not None:
+            batch.close()
+        for e in engs:
+            e.close()
+        return sum(nws) * args.steps / wall, wall, cv, tun
+
+    res = {m: run(m) for m in ("batch", "independent", "serial")}
+    v, wall, cv, tun = res["batch"]
+    line = {
+        "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 split/plain tensor-core + f64 LU/QR/weights", "data": "synthetic",
+        "config": {"workload": "C5: three systems batched, (NMO 96, 12+12 e, nchol 384, "
+                               "128 walkers), (200, 40+40, 800, 256), (320, 64+64, 1280, 384), "
+                               "10% sparse Cholesky, mixed form, control variate per system",
+                   "energy_every": args.energy_every, "timing": "wall clock, device-synchronised",
+                   "kernel_tuning": tun},
+        "independent_streams": {"value": res["independent"][0], "unit": METRIC},
+        "serial": {"value": res["serial"][0], "unit": METRIC},
+        "control_variate": cv,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
         return
     import torch
+    if args.config == "C5":
+        run_c5(args, torch)
+        return
     import torch.distributed as dist
     from datetime import timedelta
     import dataclasses

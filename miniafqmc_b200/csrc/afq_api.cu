@@ -1199,6 +1199,7 @@ afq_status afq_get_stream(afq_handle* h, void** stream) {
 afq_status afq_synchronize(afq_handle* h) {
   if (!h) return AFQ_ERR_ARG;
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  if (h->cv) AFQ_CUDA(h, afq::cv_sync(h->cv));   // the estimator's online training
   if (h->mixed) {
     int flags = 0;
     AFQ_CUDA(h, afq::mixed_error(h->mixed, &flags));

@@ -18,8 +18,10 @@ cudaError_t mlp_set_params(Mlp* m, const float* host, cudaStream_t st);
 cudaError_t mlp_get_params(Mlp* m, float* host, cudaStream_t st);
 cudaError_t mlp_forward(Mlp* m, const float* x, int B, float* y, bool keep, cudaStream_t st);
 cudaError_t mlp_gradient(Mlp* m, const float* x, const float* t, int B, cudaStream_t st);
+// last_loss: host destination of the last step's loss (pinned when !sync_loss, then the
+// copy is left in flight on st).
 cudaError_t mlp_train(Mlp* m, const float* x, const float* t, int B, int iters, float lr,
-                      float* last_loss, cudaStream_t st);
+                      float* last_loss, cudaStream_t st, bool sync_loss = true);
 // Rescales the network so that it computes the same function of new input / output
 // coordinates: x_old = a * x_new + c (device arrays [nin]), y_new = alpha y_old + gamma.
 // Restarts the Adam moments.
@@ -57,12 +59,15 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
                       cudaStream_t st);
 void cv_destroy(CvState* s);
 // Runs one measurement; writes W_data[:,0] and the two weighted sums (sum Re(e) Re(w),
-// sum Re(w)) of the estimator.  Synchronises the stream.
+// sum Re(w)) of the estimator.  Synchronises the stream; the network's online training
+// steps are left running on the estimator's own stream (cv_sync waits for them).
 cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t st);
 // stats: [exact samples seen, subset size of the last measurement, last training loss,
 //         estimator active (0/1), measurements, sampling variance of the last estimate
 //         from the subset correction, re-standardisations, fallback to exact (0/1)]
-void cv_stats(const CvState* s, double* stats);
+void cv_stats(CvState* s, double* stats);
+// Waits for the online training left running after the last measurement.
+cudaError_t cv_sync(CvState* s);
 // Kernels launched by the last cv_energy call (training included).
 long long cv_launches(const CvState* s);
 // Surrogate exchange energy of every walker from the last measurement (host doubles).

@@ -58,6 +58,12 @@ struct CvState {
   double ht_var = 0.0;
   z_t* Q = nullptr;      // [2][n][N] linearised exchange, set at the first measurement
   bool have_q = false;
+  // online training runs on its own stream after the estimate, overlapping the next
+  // substeps; the next measurement (and any use of the network) waits for ev_trained
+  cudaStream_t tst = nullptr;
+  cudaEvent_t ev_ready = nullptr, ev_trained = nullptr;
+  float* h_loss = nullptr;   // pinned: loss of the last training step
+  bool pending = false;
   std::vector<void*> allocs;
 };
 
@@ -421,6 +427,10 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   if (e == cudaSuccess) e = cudaMemsetAsync(s->Q, 0, sizeof(z_t) * nak, st);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sums, sizeof(double) * 4);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_loss, sizeof(float));
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->tst, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_trained, cudaEventDisableTiming);
   if (e == cudaSuccess) e = mlp_create(CV_NIN, cfg.hidden, s->cap, cfg.seed, &s->mlp, st);
   if (e == cudaSuccess) {
     cv_proj_init_kernel<<<gridn((long long)CV_NPROJ * 2 * nchol, 256), 256, 0, st>>>(
@@ -438,14 +448,41 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
 
 void cv_destroy(CvState* s) {
   if (!s) return;
+  if (s->tst) cudaStreamSynchronize(s->tst);
   mlp_destroy(s->mlp);
+  if (s->h_loss) cudaFreeHost(s->h_loss);
+  if (s->ev_ready) cudaEventDestroy(s->ev_ready);
+  if (s->ev_trained) cudaEventDestroy(s->ev_trained);
+  if (s->tst) cudaStreamDestroy(s->tst);
   if (s->h_sub) cudaFreeHost(s->h_sub);
   if (s->h_sums) cudaFreeHost(s->h_sums);
   for (void* p : s->allocs) cudaFree(p);
   delete s;
 }
 
-void cv_stats(const CvState* s, double* o) {
+// Takes the loss of a finished online training (blocking: waits for it); a non-finite loss
+// switches the estimator off.
+static void cv_settle(CvState* s, bool block) {
+  if (!s->pending) return;
+  if (block) {
+    if (cudaEventSynchronize(s->ev_trained) != cudaSuccess) return;
+  } else if (cudaEventQuery(s->ev_trained) != cudaSuccess) {
+    return;
+  }
+  s->last_loss = *s->h_loss;
+  if (!std::isfinite(s->last_loss)) s->failed = true;
+  s->pending = false;
+}
+
+cudaError_t cv_sync(CvState* s) {
+  if (!s || !s->tst) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(s->tst);
+  cv_settle(s, true);
+  return e;
+}
+
+void cv_stats(CvState* s, double* o) {
+  cv_settle(s, false);
   o[0] = (double)s->seen;
   o[1] = (double)s->last_m;
   o[2] = (double)s->last_loss;
@@ -474,6 +511,10 @@ cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st) {
 cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t st) {
   const int nw = s->nw;
   cudaError_t e;
+  if (s->pending) {   // the network of the previous online training
+    if ((e = cudaStreamWaitEvent(st, s->ev_trained, 0)) != cudaSuccess) return e;
+    cv_settle(s, true);
+  }
   s->meas++;
   s->launches = 0;
   if (!s->have_q && in.Lh) {   // linearised exchange about the first measurement's mean G
@@ -548,29 +589,35 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   s->buf_n = std::min(s->cap, s->buf_n + m);
   s->seen += m;
   if (!s->failed && s->seen >= s->cfg.train_walker_steps) {
+    // training on the side stream, after this measurement's work on st
+    const cudaStream_t ts = s->tst;
+    if ((e = cudaEventRecord(s->ev_ready, st)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(ts, s->ev_ready, 0)) != cudaSuccess)
+      return e;
     const bool first = !s->trained;
-    if ((e = cv_restandardize(s, st)) != cudaSuccess) return e;
+    if ((e = cv_restandardize(s, ts)) != cudaSuccess) return e;
     s->trained = true;
-    cv_normalize_buffer_kernel<<<gridn((long long)s->buf_n * CV_NIN, 256), 256, 0, st>>>(
+    cv_normalize_buffer_kernel<<<gridn((long long)s->buf_n * CV_NIN, 256), 256, 0, ts>>>(
         s->raw_x, s->raw_t, s->buf_n, s->d_mu, s->d_sd, (float)s->mu_r, (float)s->sd_r, s->buf_x,
         s->buf_t);
     s->launches++;
     const int iters = first ? s->cfg.iters_warm : s->cfg.iters_online;
     const int bb = s->cfg.batch_online;
     if (first || bb <= 0 || s->buf_n <= bb) {   // full-buffer steps
-      if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, &s->last_loss,
-                         st)) != cudaSuccess)
+      if ((e = mlp_train(s->mlp, s->buf_x, s->buf_t, s->buf_n, iters, s->cfg.lr, s->h_loss, ts,
+                         false)) != cudaSuccess)
         return e;
     } else {   // online: each step on the next contiguous window of bb buffered samples
       for (int it = 0; it < iters; it++) {
         const long long off = ((s->meas * iters + it) * (long long)bb) % (s->buf_n - bb + 1);
         if ((e = mlp_train(s->mlp, s->buf_x + off * CV_NIN, s->buf_t + off, bb, 1, s->cfg.lr,
-                           it == iters - 1 ? &s->last_loss : nullptr, st)) != cudaSuccess)
+                           it == iters - 1 ? s->h_loss : nullptr, ts, false)) != cudaSuccess)
           return e;
       }
     }
     s->launches += 10LL * iters;
-    if (!std::isfinite(s->last_loss)) s->failed = true;
+    if ((e = cudaEventRecord(s->ev_trained, ts)) != cudaSuccess) return e;
+    s->pending = true;
   }
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
   const double* hs = s->h_sums;

@@ -462,7 +462,7 @@ cudaError_t mlp_gradient(Mlp* m, const float* x, const float* t, int B, cudaStre
 }
 
 cudaError_t mlp_train(Mlp* m, const float* x, const float* t, int B, int iters, float lr,
-                      float* last_loss, cudaStream_t st) {
+                      float* last_loss, cudaStream_t st, bool sync_loss) {
   cudaError_t e = cudaSuccess;
   for (int it = 0; it < iters && e == cudaSuccess; it++) {
     e = mlp_gradient(m, x, t, B, st);
@@ -475,7 +475,7 @@ cudaError_t mlp_train(Mlp* m, const float* x, const float* t, int B, int iters, 
   }
   if (e == cudaSuccess && last_loss) {
     e = cudaMemcpyAsync(last_loss, m->loss, sizeof(float), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && sync_loss) e = cudaStreamSynchronize(st);
   }
   return e;
 }

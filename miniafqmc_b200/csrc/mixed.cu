@@ -1669,8 +1669,10 @@ static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nbl
   const bool f16 = m->Gx.f16;
   const float as = f16 ? m->sLh : 1.0f;
   const float* ws = f16 ? m->wscale : nullptr;
+  // N tiles step by whole walker groups (Gw walkers of 2n columns): when no compiled tile
+  // width is a multiple of 2n the tile's last BN - Gw 2n columns are not used
   tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
-                  m->ex_mtiles, true, true, 0};
+                  m->ex_mtiles, true, true, 0, false, m->ex_Gw * 2 * n};
   const int v = m->tune[2 * nsub > m->nw ? TS_EXF : TS_EXS];
   const int pk = promote_kb(PROMOTE_EXCHANGE);
   if ((v == 1 || (v == 0 && tc_persistent())) && pk && (m->ex_bn / 2) % (2 * n) == 0) {

@@ -256,8 +256,8 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 //   lean ring's CTAs pair up on an SM).
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
 __global__ void __launch_bounds__(192, MINB)
-tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched, int b_batched,
-               int k_split, int m_fast, Epi epi, int* err) {
+tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step, int a_batched,
+               int b_batched, int k_split, int m_fast, Epi epi, int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -273,7 +273,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batch
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // m_fast: M tiles along grid x, so the CTAs that share a B tile run together
   const int mt = m_fast ? blockIdx.x : blockIdx.y, nt = m_fast ? blockIdx.y : blockIdx.x;
-  const int m0 = mt * m_step, n0 = nt * BN;
+  const int m0 = mt * m_step, n0 = nt * n_step;
   const int batch = blockIdx.z;
   // split-K: z selects the K range [z*k_split, (z+1)*k_split) of an unbatched product
   const int kbase = k_split ? batch * k_split : 0;
@@ -433,8 +433,9 @@ struct PCfg {
 
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG>
 __global__ void __launch_bounds__(128 * EPI_WG + 64, 1)
-tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, int a_batched,
-                          int b_batched, int k_split, TileSched sched, Epi epi, int* err) {
+tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
+                          int a_batched, int b_batched, int k_split, TileSched sched, Epi epi,
+                          int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT>;
   using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
   static_assert(!Epi::kTile, "tile epilogues reuse the operand ring: per-tile kernel only");
@@ -489,7 +490,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       const int klen = k_split ? min(k_split, K - kbase) : K;
       const int nk = (klen + C::BK - 1) / C::BK;
       const int za = (a_batched && !k_split) ? z : 0, zb = (b_batched && !k_split) ? z : 0;
-      const int m0 = mt * m_step, n0 = nt * BN;
+      const int m0 = mt * m_step, n0 = nt * n_step;
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g % STAGES;
         if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1)) {
@@ -605,7 +606,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
         if constexpr (EpiRegs<Epi>::value) {
           epi.regs(z, mt, nt, row, acc, scr, wg);
         } else {
-          const int m0 = mt * m_step, n0 = nt * BN;
+          const int m0 = mt * m_step, n0 = nt * n_step;
 #pragma unroll
           for (int j = 0; j < CPW / 32; j++) epi(z, row, m0 + row, n0 + wg * CPW + j * 32, acc + j * 32);
         }
@@ -626,7 +627,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       }
       tc_fence_after();
       const uint32_t trow = tmem + b * C::TMEM_COLS + ((uint32_t)(wq * 32) << 16);
-      const int m0 = mt * m_step, n0 = nt * BN;
+      const int m0 = mt * m_step, n0 = nt * n_step;
       float v[32];
       if constexpr (Epi::kPair) {
         const int Pw = epi.pair_stride();
@@ -689,6 +690,8 @@ struct GemmShape {
   bool a_batched, b_batched;
   int k_split;         // 0, or the K extent of each z slice (a multiple of the K slab)
   bool m_fast = false; // raster M tiles fastest (B tiles reused from L2 across M)
+  int n_step = 0;      // columns between consecutive N tiles (0: BN); a smaller step lets a
+                       // tile hold whole column groups that do not fill BN
 };
 
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
@@ -710,9 +713,10 @@ cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* er
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const unsigned ntiles = (g.N + BN - 1) / BN;
+  const int ns = g.n_step > 0 ? g.n_step : BN;
+  const unsigned ntiles = (g.N + ns - 1) / ns;
   dim3 grid(g.m_fast ? g.m_tiles : ntiles, g.m_fast ? ntiles : g.m_tiles, g.batch);
-  kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, g.a_batched, g.b_batched, g.k_split,
+  kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, ns, g.a_batched, g.b_batched, g.k_split,
                                     g.m_fast ? 1 : 0, epi, err);
   return cudaGetLastError();
 }
@@ -741,11 +745,12 @@ cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& e
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  TileSched sc{g.m_tiles, (g.N + BN - 1) / BN, g.batch, g.m_fast ? 1 : 0};
+  const int ns = g.n_step > 0 ? g.n_step : BN;
+  TileSched sc{g.m_tiles, (g.N + ns - 1) / ns, g.batch, g.m_fast ? 1 : 0};
   const int total = sc.total();
   if (total <= 0) return cudaSuccess;
   const int grid = total < sm_count() ? total : sm_count();
-  kern<<<grid, P::THREADS, P::SMEM, st>>>(maps, g.K, g.m_step, g.a_batched, g.b_batched,
+  kern<<<grid, P::THREADS, P::SMEM, st>>>(maps, g.K, g.m_step, ns, g.a_batched, g.b_batched,
                                           g.k_split, sc, epi, err);
   return cudaGetLastError();
 }

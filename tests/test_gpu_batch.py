@@ -55,3 +55,26 @@ def test_batch_matches_systems_alone(mixed):
     for e in alone + grouped:
         e.close()
 
+
+
+def test_c5_shapes_mixed_energy_matches_fp64():
+    """Mixed against FP64 energies on identical walkers for the C5 shapes: n = 12, 40
+    and 64 take exchange tiles whose walker width 2n does not fill the 256-column tile
+    (per-tile kernel), or a walker width of 128 (1e-4 relative on E_J and E_K)."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
+    rng = np.random.default_rng(3)
+    for cfg, s in systems():
+        nw = cfg.nwalk
+        W, Wd = s.initial_walkers(nw)
+        W = W + 0.05 * (rng.normal(size=W.shape) + 1j * rng.normal(size=W.shape))
+        parts = []
+        for prec in (AFQ_PREC_FP64, AFQ_PREC_MIXED):
+            e = AfqmcSys(s, nw, precision=prec, walkers=(W, Wd), use_vakbl=False)
+            e.calculate_mixed_density_matrix()
+            e.calculate_energy("chol")
+            parts.append(e.copy_out("energy_parts"))
+            e.close()
+        pd, pm = parts
+        ej = rel(pm[:, 1], pd[:, 1])
+        ek = rel(pm[:, 2], pd[:, 2])
+        assert ej < 1e-4 and ek < 1e-4, (cfg.nmo, cfg.nel, ej, ek)
