@@ -317,6 +317,24 @@ class Form:
             self.measure(record)
 
 
+def exact_trajectory(system, cfg, args, device, torch, substeps=20):
+    """The mixed form's deterministic energy error along a trajectory: fresh mixed (exact
+    Cholesky energy, no control variate) and FP64 walker sets driven by the same auxiliary
+    fields for `substeps` substeps, energies every energy_every substeps (untimed)."""
+    forms = [Form(system, cfg, args, f, device, None, torch) for f in ("mixed", "fp64")]
+    for f in forms:
+        f.measure(record=False)
+        for st in range(substeps):
+            f.step(st)
+    Em, E6 = np.array(forms[0].energies), np.array(forms[1].energies)
+    for f in forms:
+        f.eng.close()
+    return {"substeps": substeps, "measurements": int(len(Em)),
+            "abs_dE_of_means_Ha": float(abs(Em.mean() - E6.mean())),
+            "max_abs_dE_Ha": float(np.max(np.abs(Em - E6))),
+            "definition": "mixed form (exact exchange) minus FP64 form, same seeds and fields"}
+
+
 def timed(form, steps, start, torch, dist, world, profile=False, record=True):
     """Times `steps` substeps from step index `start`.  profile=False: CUDA-graph substeps
     (the headline); profile=True: op-by-op calls with per-stage events (the breakdown)."""
@@ -598,6 +616,8 @@ def main():
         cmp["energy"]["same_walkers"] = same
         cmp["fp64_plain"]["kernel_tuning"] = ref.eng.tuning()
         ref.eng.close()
+        if head.mode == "cv":
+            cmp["energy"]["exact_trajectory"] = exact_trajectory(s, cfg, args, local, torch)
 
     if rank != 0:
         if world > 1:

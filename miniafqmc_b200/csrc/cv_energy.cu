@@ -428,7 +428,11 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sums, sizeof(double) * 4);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_loss, sizeof(float));
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->tst, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {   // lowest priority: the step's own kernels go first
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    e = cudaStreamCreateWithPriority(&s->tst, cudaStreamNonBlocking, lo);
+  }
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_ready, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_trained, cudaEventDisableTiming);
   if (e == cudaSuccess) e = mlp_create(CV_NIN, cfg.hidden, s->cap, cfg.seed, &s->mlp, st);
