@@ -128,6 +128,16 @@ afq_status afq_update_weights(afq_handle* h);
  * afq_set_eshift(global_sum / global_nwalk). */
 afq_status afq_update_weights_partial(afq_handle* h, double* e4_sum);
 afq_status afq_get_eshift(afq_handle* h, double* eshift);
+/* Population control by the comb (systematic resampling).  No counterpart in the
+ * reference, which leaves branching out (miniafqmc_base.cpp:347).  With weights
+ * w_i = max(Re W_data[i][1], 0), total T and prefix sums C_i in walker order, copy j of
+ * nwalk takes the first walker with C_i > (j + u) T / nwalk and weight T / nwalk; the
+ * other W_data entries come with it.  u is one Philox4x32-10 uniform for (seed, step),
+ * drawn from a stream apart from the auxiliary fields', so a run restored from saved
+ * walkers (afq_set_walkers, afq_set_eshift) at the same seed and step repeats it.  Per
+ * handle: sharded walker sets comb their own walkers.  AFQ_ERR_STATE when no walker has
+ * positive weight.  Synchronous. */
+afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step);
 afq_status afq_set_eshift(afq_handle* h, double eshift);
 /* Places this handle's walkers at [offset, offset+nwalk) of an ensemble of nwalk_global
  * walkers, so that the Philox stream (indexed by the global walker) gives every shard
@@ -254,6 +264,20 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
                              int northo);
 /* Waits for the batch's work and reports any handle's tensor-core timeout flags. */
 afq_status afq_batch_synchronize(afq_batch* b);
+
+/* Half-rotation of the Cholesky tensor on the GPU: base::halfrotate_cholesky
+ * (rotate.hpp:69-169) computed on `device`.
+ *   SpvnT[c][s*naea*nmo + a*nmo + k] = sum_i trial_s(i, a) Spvn[i*nmo + k][c]
+ * with entries of |value| <= cutoff dropped (rotate.hpp:119,156), rows and columns in
+ * order.  Spvn: [nmo^2 x nchol] CSR (scaled by sqrt(dt)); trial [2][nmo][naea] as for
+ * afq_set_hamiltonian.  Writes *nnz; with rowIndex != NULL also rowIndex[nchol+1], and
+ * cols[nnz] / vals[2*nnz] when those are not NULL (call once without them to size the
+ * buffers).  Lhalf (optional): the dense [nchol][2][naea][nmo] values times lh_scale
+ * without the cutoff (lh_scale = 1/sqrt(dt) gives the unscaled factors afq_set_hamiltonian
+ * takes).  Allocates and frees device memory; synchronous. */
+afq_status afq_halfrotate(int device, const afq_csr_z* Spvn, int nmo, int naea, int nchol,
+                          const double* trial, double cutoff, double lh_scale, long long* nnz,
+                          int32_t* rowIndex, int32_t* cols, double* vals, double* Lhalf);
 
 /* Self-test of the tensor-core GEMM used by the mixed form (no reference counterpart):
  * C[b][m][n] = sum_k A[b][m][k] B[b][n][k] for host fp32 arrays, computed on the current

@@ -35,7 +35,7 @@ EXPORTS = [
     "afq_mlp_create", "afq_mlp_destroy", "afq_mlp_num_params", "afq_mlp_set_params",
     "afq_mlp_get_params", "afq_mlp_forward", "afq_mlp_gradient", "afq_mlp_train",
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
-    "afq_get_tuning",
+    "afq_get_tuning", "afq_halfrotate", "afq_population_control",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -98,6 +98,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_batch_create": ([P, I, P], I), "afq_batch_destroy": ([P], None),
         "afq_batch_substep": ([P, P, U64, I], I), "afq_batch_synchronize": ([P], I),
         "afq_get_tuning": ([P, P, P], I),
+        "afq_halfrotate": ([I, P, I, I, I, P, D, D, P, P, P, P, P], I),
+        "afq_population_control": ([P, U64, U64], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -275,6 +277,10 @@ class AfqmcSys:
                 "active": bool(v[3]), "measurements": int(v[4]), "subset_var": float(v[5]),
                 "restandardisations": int(v[6]), "fallback": bool(v[7])}
 
+    def population_control(self, seed: int, step: int):
+        """Comb resampling of the walkers (weights equalised, total weight kept)."""
+        self._check(self.lib.afq_population_control(self.h, seed, step))
+
     TUNE_SITES = ["vhs", "propagate", "splitk", "exchange_all", "exchange_subset", "t1"]
     TUNE_SITES_FP64 = ["vhs_csr", "propagate_zgemm", "vbias_zgemm", "coulomb_zgemm",
                        "vakbl_zgemm"]
@@ -334,6 +340,37 @@ class AfqmcSys:
         v = ctypes.c_void_p()
         self._check(self.lib.afq_get_stream(self.h, ctypes.byref(v)))
         return v.value or 0
+
+
+def halfrotate(system, cutoff: float = 1e-6, device: int = 0, dense: bool = False):
+    """GPU half-rotation of the system's Spvn with its trial (rotate.hpp:69-169): returns
+    the SpvnT CSR triple (rowIndex, cols, vals) and, with dense=True, the unscaled dense
+    factors Lh [nchol][2][n][N] as well."""
+    lib = load_library()
+    S = system.Spvn
+    ri = np.ascontiguousarray(S.rowIndex, dtype=np.int32)
+    ci = np.ascontiguousarray(S.cols, dtype=np.int32)
+    v = np.ascontiguousarray(S.vals, dtype=np.complex128)
+    keep = (ri, ci, v)
+    m = CsrZ(S.nrows, S.ncols, _p(ri), _p(ci), _p(v))
+    tr = np.ascontiguousarray(system.trial, dtype=np.complex128)
+    N, n, nc = system.N, system.n, system.nchol
+    nnz = ctypes.c_longlong()
+    scale = 1.0 / np.sqrt(system.cfg.dt)
+    args = (device, ctypes.byref(m), N, n, nc, _p(tr), cutoff, scale, ctypes.byref(nnz))
+    st = lib.afq_halfrotate(*args, None, None, None, None)
+    if st != 0:
+        raise AfqmcError(st, "afq_halfrotate (count) failed")
+    rowIndex = np.empty(nc + 1, np.int32)
+    cols = np.empty(nnz.value, np.int32)
+    vals = np.empty(nnz.value, np.complex128)
+    Lh = np.empty((nc, 2, n, N), np.complex128) if dense else None
+    st = lib.afq_halfrotate(*args, _p(rowIndex), _p(cols), _p(vals),
+                            _p(Lh) if dense else None)
+    if st != 0:
+        raise AfqmcError(st, "afq_halfrotate failed")
+    del keep
+    return (rowIndex, cols, vals, Lh) if dense else (rowIndex, cols, vals)
 
 
 class AfqmcBatch:

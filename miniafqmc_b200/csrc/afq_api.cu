@@ -59,6 +59,10 @@ struct afq_handle {
   int f64cfg[F64_N] = {0};
   float f64ms[F64_N][2] = {};
 
+  // population control scratch (allocated by the first afq_population_control)
+  double *comb_C = nullptr, *comb_w = nullptr;
+  int* comb_idx = nullptr;
+
   afq::MixedState* mixed = nullptr;
   afq::CvState* cv = nullptr;
   afq::CvConfig cv_cfg;
@@ -828,6 +832,28 @@ afq_status afq_update_weights_partial(afq_handle* h, double* e4_sum) {
   AFQ_CUDA(h, cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
   *e4_sum = h->h_sc->e4sum;
+  return AFQ_OK;
+}
+
+afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (h->capturing) return fail(h, AFQ_ERR_STATE, "population control inside a captured step");
+  cudaSetDevice(h->d.device);
+  if (!h->comb_C) {
+    AFQ_CUDA(h, dalloc(h, &h->comb_C, (size_t)h->nw));
+    AFQ_CUDA(h, dalloc(h, &h->comb_idx, (size_t)h->nw));
+    AFQ_CUDA(h, dalloc(h, &h->comb_w, 1));
+  }
+  // copies go through T2 (walkers) and T1 (walker data), per-step scratch of the propagation
+  double total = 0.0;
+  AFQ_CUDA(h, afq::launch_comb(h->W, h->Wd, h->nw, (long long)h->N * 2 * h->n,
+                               afq::comb_uniform(seed, step), h->comb_C, h->comb_idx,
+                               h->comb_w, h->T2, h->T1, &total, h->st));
+  if (!(total > 0.0))   // walkers untouched
+    return fail(h, AFQ_ERR_STATE, "population control: no walker has positive weight");
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  h->dm_cache = false;   // the walkers changed
   return AFQ_OK;
 }
 

@@ -54,3 +54,24 @@ def test_batch_rejects_bad_arguments_without_gpu():
     assert lib.afq_batch_create(arr, 1, ctypes.byref(out)) == 1
     assert lib.afq_batch_substep(None, None, 0, 5) == 1
     assert lib.afq_batch_synchronize(None) == 1
+
+
+def test_halfrotate_rejects_bad_arguments_without_gpu():
+    """The GPU half-rotation checks its arguments before selecting a device."""
+    import ctypes
+    import numpy as np
+    from miniafqmc_b200.afqmc import load_library, CsrZ
+    lib = load_library()
+    nnz = ctypes.c_longlong()
+    ri = np.zeros(5, np.int32)
+    m = CsrZ(4, 3, ri.ctypes.data, None, None)        # nmo = 2, nchol = 3, no nonzeros
+    tr = np.zeros(8)
+    ok = (0, ctypes.byref(m), 2, 1, 3, tr.ctypes.data, 1e-6, 1.0, ctypes.byref(nnz))
+    assert lib.afq_halfrotate(0, None, 2, 1, 3, tr.ctypes.data, 1e-6, 1.0, ctypes.byref(nnz),
+                              None, None, None, None) == 1
+    assert lib.afq_halfrotate(*ok[:2], 3, 1, 3, *ok[5:], None, None, None, None) == 1   # nrows
+    assert lib.afq_halfrotate(*ok[:6], -1.0, 1.0, ctypes.byref(nnz), None, None, None,
+                              None) == 1                                            # cutoff
+    cols = np.zeros(1, np.int32)
+    assert lib.afq_halfrotate(*ok, None, cols.ctypes.data, None, None) == 1        # no rowIndex
+
