@@ -57,9 +57,11 @@ typedef enum {
   AFQ_BUF_INFO = 6,         /* int32 [nwalk][2], nonzero = singular overlap matrix      */
   AFQ_BUF_ENERGY_PARTS = 7, /* double [nwalk][3] = (E1, EJ, EK) of the last Cholesky
                                energy evaluation                                         */
-  AFQ_BUF_CV_PRED = 8       /* double [nwalk] surrogate exchange energy of every walker
+  AFQ_BUF_CV_PRED = 8,      /* double [nwalk] surrogate exchange energy of every walker
                                from the last AFQ_ENERGY_CV measurement (0 before the
                                estimator is active)                                      */
+  AFQ_BUF_G_FULL = 9        /* [2*NMO*NMO][nwalk] full density matrix of the last
+                               afq_mixed_density_matrix_full                            */
 } afq_buffer;
 
 typedef struct {
@@ -113,6 +115,16 @@ afq_status afq_mixed_density_matrix(afq_handle* h);
 afq_status afq_overlaps(afq_handle* h, int save_old);
 /* base::get_vbias(SpvnT, Gc, vbias, true) (vbias.hpp:49-63). */
 afq_status afq_vbias(afq_handle* h);
+/* The reference's transposed_Spvn == false path (CLI `-t no`, miniafqmc_base.cpp:265-273;
+ * the flag's parsing is broken there, :120,138), FP64 form only:
+ * afqmc_sys::calculate_mixed_density_matrix(W, W_data, G, compact=false)
+ * (afqmc_sys.hpp:98-116, mixed_density_matrix.hpp:96-99) -> the full G [2][NMO][NMO] of
+ * every walker (AFQ_BUF_G_FULL) plus the compact Gc and overlaps;
+ * base::get_vbias(Spvn, G, vbias, false) (vbias.hpp:66-81) -> vbias = T(Spvn) G_alpha +
+ * T(Spvn) G_beta.  Needs about 32 NMO^2 nwalk bytes of device memory, allocated on first
+ * use. */
+afq_status afq_mixed_density_matrix_full(afq_handle* h);
+afq_status afq_vbias_full(afq_handle* h);
 /* Driver step 2 (miniafqmc_base.cpp:281-289) with x ~ N(0,1) from Philox4x32-10
  * keyed by seed, counter (pair index, step).  afq_sigma_from takes x from the host. */
 afq_status afq_sigma(afq_handle* h, uint64_t seed, uint64_t step);

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libafqmc_b200.so")
 AFQ_PREC_FP64, AFQ_PREC_MIXED = 0, 1
 AFQ_ENERGY_VAKBL, AFQ_ENERGY_CHOLESKY, AFQ_ENERGY_CV = 0, 1, 2
 BUFFERS = {"Gc": 0, "vbias": 1, "X": 2, "vHS": 3, "hybridW": 4, "xraw": 5, "info": 6,
-           "energy_parts": 7, "cv_pred": 8}
+           "energy_parts": 7, "cv_pred": 8, "G_full": 9}
 STATUS = {0: "AFQ_OK", 1: "AFQ_ERR_ARG", 2: "AFQ_ERR_STATE", 3: "AFQ_ERR_CUDA",
           4: "AFQ_ERR_OOM", 5: "AFQ_ERR_UNSUPPORTED", 6: "AFQ_ERR_SINGULAR"}
 
@@ -36,6 +36,7 @@ EXPORTS = [
     "afq_mlp_get_params", "afq_mlp_forward", "afq_mlp_gradient", "afq_mlp_train",
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
+    "afq_mixed_density_matrix_full", "afq_vbias_full",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -100,6 +101,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_get_tuning": ([P, P, P], I),
         "afq_halfrotate": ([I, P, I, I, I, P, D, D, P, P, P, P, P], I),
         "afq_population_control": ([P, U64, U64], I),
+        "afq_mixed_density_matrix_full": ([P], I), "afq_vbias_full": ([P], I),
     }
     for name, (args, res) in sigs.items():
         f = getattr(lib, name)
@@ -194,7 +196,7 @@ class AfqmcSys:
                   "X": ((nc, nw), np.complex128), "vHS": ((N * N, nw), np.complex128),
                   "hybridW": ((nw,), np.complex128), "xraw": ((nc, nw), np.float64),
                   "info": ((nw, 2), np.int32), "energy_parts": ((nw, 3), np.float64),
-                  "cv_pred": ((nw,), np.float64)}
+                  "cv_pred": ((nw,), np.float64), "G_full": ((2 * N * N, nw), np.complex128)}
         shape, dt = shapes[which]
         out = np.empty(shape, dt)
         self._check(self.lib.afq_copy_out(self.h, BUFFERS[which], _p(out)))
@@ -276,6 +278,14 @@ class AfqmcSys:
         return {"samples": int(v[0]), "subset": int(v[1]), "loss": float(v[2]),
                 "active": bool(v[3]), "measurements": int(v[4]), "subset_var": float(v[5]),
                 "restandardisations": int(v[6]), "fallback": bool(v[7])}
+
+    def calculate_mixed_density_matrix_full(self):
+        """Full density matrix G[2][N][N] of every walker (the reference's -t no path)."""
+        self._check(self.lib.afq_mixed_density_matrix_full(self.h))
+
+    def get_vbias_full(self):
+        """vbias = T(Spvn) G_alpha + T(Spvn) G_beta from the full density matrix."""
+        self._check(self.lib.afq_vbias_full(self.h))
 
     def population_control(self, seed: int, step: int):
         """Comb resampling of the walkers (weights equalised, total weight kept)."""

@@ -59,6 +59,11 @@ struct afq_handle {
   int f64cfg[F64_N] = {0};
   float f64ms[F64_N][2] = {};
 
+  // full-G path (transposed_Spvn == false): G [nw][2][N][N] walker-major, and T(Spvn) for
+  // both spins as one CSR [nchol x 2 N^2] (allocated by the first full-G call)
+  z_t* Gf = nullptr;
+  int *spf_ri = nullptr, *spf_ci = nullptr;
+  z_t* spf_v = nullptr;
   // population control scratch (allocated by the first afq_population_control)
   double *comb_C = nullptr, *comb_w = nullptr;
   int* comb_idx = nullptr;
@@ -769,6 +774,84 @@ afq_status afq_mixed_density_matrix(afq_handle* h) {
   return AFQ_OK;
 }
 
+// The reference's transposed_Spvn == false branch (miniafqmc_base.cpp:265-273): the
+// non-compact density matrix G_s = conj(A_s) T1^-1 T(W_s) (mixed_density_matrix.hpp:96-99),
+// formed here as trial_s Gc_s by a batched ZGEMM after the compact one (FP64 form).
+afq_status afq_mixed_density_matrix_full(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (h->mixed) return fail(h, AFQ_ERR_UNSUPPORTED, "full density matrix: FP64 form only");
+  const int N = h->N, n = h->n, nw = h->nw;
+  if (!h->Gf) AFQ_CUDA(h, dalloc(h, &h->Gf, (size_t)nw * 2 * N * N));
+  AFQ_CUDA(h, st_dm(h, 1, 0));
+  for (int sp = 0; sp < 2; sp++) {   // G_s[i][k] = sum_a trial_s[i][a] Gc_s[a][k]
+    ZGemmDesc g{N, N, n, h->tw + sp * n, 2 * n, 0, h->Gc + (size_t)sp * n * N, N, h->NAK,
+                zmk(1, 0)};
+    EpiStore ep{h->Gf + (size_t)sp * N * N, N, 2LL * N * N, zmk(0, 0), 0};
+    AFQ_CUDA(h, (zgemm_launch<true, false>(g, nw, ep, h->st)));
+  }
+  return AFQ_OK;
+}
+
+// base::get_vbias(Spvn, G, vbias, false) (vbias.hpp:66-81): vbias = T(Spvn) G_alpha +
+// T(Spvn) G_beta.  T(Spvn) of both spins is one CSR whose row c lists the alpha entries
+// (columns ik) then the beta ones (N^2 + ik), each in increasing ik: the gather sums every
+// vbias element in the order the reference's two scatter passes add it.
+afq_status afq_vbias_full(afq_handle* h) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (h->mixed) return fail(h, AFQ_ERR_UNSUPPORTED, "full-G vbias: FP64 form only");
+  if (!h->Gf) return fail(h, AFQ_ERR_STATE, "full density matrix not formed");
+  const long long N2 = (long long)h->N * h->N;
+  if (!h->spf_ri) {   // transpose once on the host from the device copy of Spvn
+    std::vector<int> ri(N2 + 1);
+    AFQ_CUDA(h, cudaMemcpy(ri.data(), h->sp_ri, sizeof(int) * (N2 + 1), cudaMemcpyDeviceToHost));
+    const long long nz = ri[N2];
+    std::vector<int> ci(nz);
+    std::vector<z_t> v(nz);
+    AFQ_CUDA(h, cudaMemcpy(ci.data(), h->sp_ci, sizeof(int) * nz, cudaMemcpyDeviceToHost));
+    if (h->sp_rv) {
+      std::vector<double> rv(nz);
+      AFQ_CUDA(h, cudaMemcpy(rv.data(), h->sp_rv, sizeof(double) * nz, cudaMemcpyDeviceToHost));
+      for (long long p = 0; p < nz; p++) v[p] = zmk(rv[p], 0.0);
+    } else {
+      AFQ_CUDA(h, cudaMemcpy(v.data(), h->sp_v, sizeof(z_t) * nz, cudaMemcpyDeviceToHost));
+    }
+    const int nc = h->nc;
+    std::vector<long long> cnt(nc + 1, 0);
+    for (long long p = 0; p < nz; p++) cnt[ci[p] + 1] += 2;
+    for (int c = 0; c < nc; c++) cnt[c + 1] += cnt[c];
+    if (cnt[nc] > 0x7fffffffLL) return fail(h, AFQ_ERR_UNSUPPORTED, "T(Spvn) exceeds int32");
+    std::vector<int> tri(nc + 1), tci(cnt[nc]);
+    std::vector<z_t> tv(cnt[nc]);
+    std::vector<long long> half(nc), pos(nc);
+    for (int c = 0; c < nc; c++) {
+      tri[c] = (int)cnt[c];
+      half[c] = (cnt[c + 1] - cnt[c]) / 2;
+      pos[c] = 0;
+    }
+    tri[nc] = (int)cnt[nc];
+    for (long long r = 0; r < N2; r++)   // rows in order: entries land in increasing ik
+      for (int p = ri[r]; p < ri[r + 1]; p++) {
+        const int c = ci[p];
+        const long long q = cnt[c] + pos[c]++;
+        tci[q] = (int)r;
+        tv[q] = v[p];
+        tci[q + half[c]] = (int)(N2 + r);
+        tv[q + half[c]] = v[p];
+      }
+    AFQ_CUDA(h, dalloc(h, &h->spf_ri, (size_t)nc + 1));
+    AFQ_CUDA(h, dalloc(h, &h->spf_ci, (size_t)cnt[nc]));
+    AFQ_CUDA(h, dalloc(h, &h->spf_v, (size_t)cnt[nc]));
+    AFQ_CUDA(h, cudaMemcpy(h->spf_ri, tri.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice));
+    AFQ_CUDA(h, cudaMemcpy(h->spf_ci, tci.data(), sizeof(int) * cnt[nc], cudaMemcpyHostToDevice));
+    AFQ_CUDA(h, cudaMemcpy(h->spf_v, tv.data(), sizeof(z_t) * cnt[nc], cudaMemcpyHostToDevice));
+  }
+  AFQ_CUDA(h, launch_csr_gather(h->spf_ri, h->spf_ci, h->spf_v, h->Gf, 2 * N2, h->nc, h->nw,
+                                h->vbias, h->st));
+  return AFQ_OK;
+}
+
 afq_status afq_overlaps(afq_handle* h, int save_old) {
   afq_status s = need_ready(h);
   if (s != AFQ_OK) return s;
@@ -1268,6 +1351,15 @@ afq_status afq_copy_out(afq_handle* h, int which, void* host) {
     case AFQ_BUF_XRAW: AFQ_CUDA(h, d2h(host, h->xraw, sizeof(double) * nc * nw)); break;
     case AFQ_BUF_INFO: AFQ_CUDA(h, d2h(host, h->info, sizeof(int) * nw * 2)); break;
     case AFQ_BUF_ENERGY_PARTS: AFQ_CUDA(h, d2h(host, h->parts, sizeof(double) * nw * 3)); break;
+    case AFQ_BUF_G_FULL: {
+      if (!h->Gf) return fail(h, AFQ_ERR_STATE, "full density matrix not formed");
+      std::vector<z_t> t(nw * 2 * N * N);
+      AFQ_CUDA(h, d2h(t.data(), h->Gf, sizeof(z_t) * t.size()));
+      z_t* dst = static_cast<z_t*>(host);
+      for (size_t w = 0; w < nw; w++)
+        for (size_t i = 0; i < 2 * N * N; i++) dst[i * nw + w] = t[w * 2 * N * N + i];
+      break;
+    }
     case AFQ_BUF_CV_PRED:
       if (!h->cv) {
         for (size_t w = 0; w < nw; w++) static_cast<double*>(host)[w] = 0.0;

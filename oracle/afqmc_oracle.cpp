@@ -160,6 +160,7 @@ struct orc_handle {
   CSR Spvn, SpvnT, Vakbl;
   std::vector<cd> P, haj, trial[2], Lh;
   std::vector<cd> W, Wd, Gc, vbias, X, vHS, hybridW;
+  std::vector<cd> G;         // full density matrix [2][N][N][nw] (transposed_Spvn == false)
   std::vector<double> xraw;
   std::vector<int> info;
   double Eshift = 0.0;
@@ -254,6 +255,7 @@ void orc_copy_out(const orc_handle* h, int which, void* dst) {
     case 4: std::memcpy(dst, h->hybridW.data(), sizeof(cd) * h->hybridW.size()); break;
     case 5: std::memcpy(dst, h->xraw.data(), sizeof(double) * h->xraw.size()); break;
     case 6: std::memcpy(dst, h->info.data(), sizeof(int) * h->info.size()); break;
+    case 7: std::memcpy(dst, h->G.data(), sizeof(cd) * h->G.size()); break;
   }
 }
 
@@ -308,6 +310,44 @@ void orc_mixed_density_matrix(orc_handle* h) {
       }
     }
   }
+}
+
+// afqmc_sys::calculate_mixed_density_matrix with compact=false (afqmc_sys.hpp:98-116),
+// the non-compact branch of base::MixedDensityMatrix (mixed_density_matrix.hpp:96-99):
+// T2 = T1^-1 T(W), C = conj(A) T2, stored as G_4D[s][i][k][w] with N_ = NMO.
+void orc_mixed_density_matrix_full(orc_handle* h) {
+  const int N = h->N, n = h->n, nw = h->nw;
+  h->G.assign((size_t)2 * N * N * nw, cd(0));
+#pragma omp parallel
+  {
+    std::vector<cd> T1((size_t)n * n), T2((size_t)n * N), DM((size_t)N * N),
+        work((size_t)64 * n);
+    std::vector<int> ipiv(n);
+#pragma omp for schedule(dynamic, 1)
+    for (int w = 0; w < nw; w++) {
+      for (int s = 0; s < 2; s++) {
+        const cd* Ws = h->W.data() + ((size_t)w * 2 + s) * N * n;
+        rm_gemm('T', 'N', n, n, N, cd(1), Ws, n, h->trial[s].data(), n, cd(0), T1.data(), n);
+        int info = 0;
+        cd ov = invert(T1.data(), n, ipiv.data(), work.data(), (int)work.size(), &info);
+        h->info[(size_t)w * 2 + s] = info;
+        rm_gemm('N', 'T', n, N, n, cd(1), T1.data(), n, Ws, n, cd(0), T2.data(), N);
+        rm_gemm('N', 'N', N, N, n, cd(1), h->trial[s].data(), n, T2.data(), N, cd(0), DM.data(), N);
+        h->Wd[(size_t)w * 8 + 2 + s] = ov;
+        for (int i = 0; i < N; i++)
+          for (int k = 0; k < N; k++)
+            h->G[(((size_t)s * N + i) * N + k) * nw + w] = DM[(size_t)i * N + k];
+      }
+    }
+  }
+}
+
+// base::get_vbias(Spvn, G, vbias, false) (vbias.hpp:66-81): vbias = T(Spvn) G_alpha, then
+// vbias += T(Spvn) G_beta.
+void orc_vbias_full(orc_handle* h) {
+  const size_t half = (size_t)h->N * h->N * h->nw;
+  csrmm_T(h->Spvn, h->nw, cd(1), h->G.data(), h->nw, cd(0), h->vbias.data(), h->nw);
+  csrmm_T(h->Spvn, h->nw, cd(1), h->G.data() + half, h->nw, cd(1), h->vbias.data(), h->nw);
 }
 
 // afqmc_sys::calculate_overlaps (afqmc_sys.hpp:136-144), base::Overlap

@@ -76,6 +76,8 @@ def load(fast: bool = False) -> ctypes.CDLL:
         "orc_mixed_density_matrix": ([P], None),
         "orc_overlaps": ([P, I], None),
         "orc_vbias": ([P], None),
+        "orc_mixed_density_matrix_full": ([P], None),
+        "orc_vbias_full": ([P], None),
         "orc_generate_x": ([P, U64, U64], None),
         "orc_sigma": ([P, U64, U64], None),
         "orc_sigma_from": ([P, P], None),
@@ -160,7 +162,7 @@ class Oracle:
         shapes = {"Gc": ((2 * n * N, nw), np.complex128, 0), "vbias": ((nc, nw), np.complex128, 1),
                   "X": ((nc, nw), np.complex128, 2), "vHS": ((N * N, nw), np.complex128, 3),
                   "hybridW": ((nw,), np.complex128, 4), "xraw": ((nc, nw), np.float64, 5),
-                  "info": ((nw, 2), np.int32, 6)}
+                  "info": ((nw, 2), np.int32, 6), "G_full": ((2 * N * N, nw), np.complex128, 7)}
         shape, dt, code = shapes[which]
         out = np.empty(shape, dt)
         self.lib.orc_copy_out(self.h, code, _p(out))
@@ -186,6 +188,14 @@ class Oracle:
 
     def get_vbias(self):
         self.lib.orc_vbias(self.h)
+
+    def calculate_mixed_density_matrix_full(self):
+        """Non-compact density matrix G[2][N][N][nw] (transposed_Spvn == false)."""
+        self.lib.orc_mixed_density_matrix_full(self.h)
+
+    def get_vbias_full(self):
+        """vbias = T(Spvn) G_alpha + T(Spvn) G_beta from the full density matrix."""
+        self.lib.orc_vbias_full(self.h)
 
     def sigma(self, seed: int, step: int):
         self.lib.orc_sigma(self.h, seed, step)
