@@ -703,6 +703,9 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
         for (int a = 0; a < n; a++) t[(size_t)i * 2 * n + s2 * n + a] = src[((size_t)s2 * N + i) * n + a];
     AFQ_CUDA(h, cudaMemcpy(h->tw, t.data(), sizeof(z_t) * t.size(), cudaMemcpyHostToDevice));
   }
+  // the uploads above are pageable cudaMemcpy calls, which may return before their DMA
+  // lands; the handle's stream does not wait for the legacy stream, so finish them here
+  AFQ_CUDA(h, cudaDeviceSynchronize());
   if (h->d.precision == AFQ_PREC_MIXED) {
     afq::MixedInit mi{};
     mi.N = N; mi.n = n; mi.nchol = nc; mi.nw = h->nw; mi.order = h->d.taylor_order;
@@ -843,9 +846,14 @@ afq_status afq_vbias_full(afq_handle* h) {
     AFQ_CUDA(h, dalloc(h, &h->spf_ri, (size_t)nc + 1));
     AFQ_CUDA(h, dalloc(h, &h->spf_ci, (size_t)cnt[nc]));
     AFQ_CUDA(h, dalloc(h, &h->spf_v, (size_t)cnt[nc]));
-    AFQ_CUDA(h, cudaMemcpy(h->spf_ri, tri.data(), sizeof(int) * (nc + 1), cudaMemcpyHostToDevice));
-    AFQ_CUDA(h, cudaMemcpy(h->spf_ci, tci.data(), sizeof(int) * cnt[nc], cudaMemcpyHostToDevice));
-    AFQ_CUDA(h, cudaMemcpy(h->spf_v, tv.data(), sizeof(z_t) * cnt[nc], cudaMemcpyHostToDevice));
+    // on the handle's (non-blocking) stream, so the gather below is ordered after them
+    AFQ_CUDA(h, cudaMemcpyAsync(h->spf_ri, tri.data(), sizeof(int) * (nc + 1),
+                                cudaMemcpyHostToDevice, h->st));
+    AFQ_CUDA(h, cudaMemcpyAsync(h->spf_ci, tci.data(), sizeof(int) * cnt[nc],
+                                cudaMemcpyHostToDevice, h->st));
+    AFQ_CUDA(h, cudaMemcpyAsync(h->spf_v, tv.data(), sizeof(z_t) * cnt[nc],
+                                cudaMemcpyHostToDevice, h->st));
+    AFQ_CUDA(h, cudaStreamSynchronize(h->st));   // before the host vectors go
   }
   AFQ_CUDA(h, launch_csr_gather(h->spf_ri, h->spf_ci, h->spf_v, h->Gf, 2 * N2, h->nc, h->nw,
                                 h->vbias, h->st));

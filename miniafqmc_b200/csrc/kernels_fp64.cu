@@ -5,6 +5,8 @@
 //   tw  [N][2n]       trial, same interleave
 //   Gc  [nw][2][n][N] per-walker compact density matrices (linear index s*n*N + a*N + k)
 //   vHS [nw][N][N], vbias / X / xraw [nchol][nw] (reference layout)
+#include <cstdlib>
+
 #include "afq_kernels.h"
 #include "afq_common.cuh"
 
@@ -631,6 +633,10 @@ cudaError_t launch_ortho(z_t* W, int N, int n, int nw, cudaStream_t st) {
 // (walker, spin); the n x n factors live in shared memory, W streams through it in
 // 32-row chunks.  A walker whose Gram matrix is not positive definite is left as is
 // and flagged in info.
+// One pass leaves W R^-1 orthonormal to about n eps kappa(W)^2; the second pass is
+// skipped when kappa_F = |R|_F |R^-1|_F (>= the 2-norm condition number) is at most 4n,
+// i.e. orthonormal to ~1e-11 or better.  Walkers re-orthogonalised every few steps meet
+// that bound; a run may force both passes with two_pass = 1.
 constexpr int CQ_KC = 32;
 
 size_t cholqr_smem_bytes(int n) {
@@ -638,7 +644,7 @@ size_t cholqr_smem_bytes(int n) {
 }
 
 __global__ void __launch_bounds__(256)
-ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
+ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info, int two_pass) {
   extern __shared__ __align__(16) unsigned char cq_smem[];
   const int w = blockIdx.x >> 1, s = blockIdx.x & 1;
   const int ld = n + 1;
@@ -646,6 +652,7 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
   z_t* Ri = G + n * ld;                          // R^-1
   z_t* buf = Ri + n * ld;                        // W chunk [KC][n+1]
   __shared__ int s_bad;
+  __shared__ z_t s_red[32];
   const long long ldw = 2 * n;
   z_t* B = W + (long long)w * N * ldw + s * n;
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -730,6 +737,19 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
       }
     }
     __syncthreads();
+    bool last = pass == 1;
+    if (pass == 0 && !two_pass) {   // |R|_F^2 and |R^-1|_F^2 over the upper triangles
+      double r2 = 0.0, q2 = 0.0;
+      for (int e = tid; e < n * n; e += nt) {
+        const int a = e / n, b = e % n;
+        if (b < a) continue;
+        const z_t g = G[a * ld + b], q = Ri[a * ld + b];
+        r2 += g.x * g.x + g.y * g.y;
+        q2 += q.x * q.x + q.y * q.y;
+      }
+      const z_t t = block_zsum(zmk(r2, q2), s_red);
+      last = t.x * t.y <= 16.0 * n * n;
+    }
     // ---- B <- B R^-1 in 32-row chunks: thread (tk, tb) owns rows k = tk + 16i (i < 2)
     // and columns b = tb + 16j (j < R); R^-1 is upper triangular (zeros below)
     for (int k0 = 0; k0 < N; k0 += CQ_KC) {
@@ -775,6 +795,7 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info) {
         }
       __syncthreads();
     }
+    if (last) break;
   }
   if (tid == 0) info[w * 2 + s] |= s_bad ? 2 : 0;
 }
@@ -792,7 +813,11 @@ cudaError_t launch_ortho_cholqr(z_t* W, int N, int n, int nw, int* info, cudaStr
     if (e != cudaSuccess) return e;
     attr = smem;
   }
-  ortho_cholqr_kernel<<<2 * nw, 256, smem, st>>>(W, N, n, info);
+  static const int two_pass = [] {
+    const char* e = getenv("AFQ_CHOLQR_PASSES");
+    return e && atoi(e) == 2 ? 1 : 0;
+  }();
+  ortho_cholqr_kernel<<<2 * nw, 256, smem, st>>>(W, N, n, info, two_pass);
   return cudaGetLastError();
 }
 

@@ -147,3 +147,26 @@ def test_fp16_split_g_products(monkeypatch):
     assert ev < 1e-4 and res["EJ"] < 1e-4 and res["EK"] < 1e-4 and res["E"] < 1e-5
     d.close()
     m.close()
+
+
+@pytest.mark.parametrize("spread", [0.0, 3.0])
+def test_cholqr_orthonormal_with_one_or_two_passes(spread):
+    """Mixed-form re-orthogonalisation: well-conditioned walkers take one Cholesky-QR
+    pass, ill-conditioned ones (columns scaled over three decades, kappa ~ 1e3) take two;
+    both end orthonormal to 1e-11 with the same column space as before."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    s = system("C1")
+    nw = 8
+    W, Wd = perturbed(s, nw, amp=0.05)
+    W = W * (10.0 ** (spread * np.arange(s.n) / s.n))[None, None, None, :]
+    m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=(W, Wd))
+    m.orthogonalize()
+    Wo = m.get_walkers()[0]
+    for w in range(nw):
+        for sp in range(2):
+            Q = Wo[w, sp]
+            assert np.max(np.abs(Q.conj().T @ Q - np.eye(s.n))) < 1e-11
+            # same column space: W = Q (Q^H W)
+            X = W[w, sp]
+            assert np.max(np.abs(Q @ (Q.conj().T @ X) - X)) < 1e-10 * np.max(np.abs(X))
+    m.close()
