@@ -516,8 +516,9 @@ lu_inv_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ W
 }
 
 // The same Gauss-Jordan (in-place exchange form, implicit izamax pivoting) with the matrix
-// in shared memory: 128 threads per matrix (warps on rows, lanes on columns), three
-// barriers per pivot; small register footprint, so five matrices share an SM.
+// in shared memory: 128 threads per matrix (warps on rows, lanes on columns), two
+// barriers per pivot (the searching warp also scales the pivot row); small register
+// footprint, so five matrices share an SM.
 constexpr int LUS_THREADS = 128;
 size_t lus_smem_bytes(int n) { return sizeof(z_t) * ((size_t)n * (n + 1) + 2 * n); }
 
@@ -566,21 +567,24 @@ lu_smem_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ 
         }
       }
     }
+    if (warp == 0) {   // the scaled pivot row, prepared by the searching warp
+      __syncwarp();
+      const int pp = s_p;
+      if (pp >= 0) {
+        const z_t inv = zrecip(T[pp * ld + j]);
+        for (int c = lane; c < n; c += 32) prow[c] = (c == j) ? inv : zmul(T[pp * ld + c], inv);
+      }
+    }
     __syncthreads();
     const int p = s_p;
     if (p < 0) { sing = 1; break; }   // uniform across the CTA
-    const z_t pv = s_pv;
-    if (tid == 0) det = zmul(det, pv);
-    const z_t inv = zrecip(pv);
-    for (int i = tid; i < n; i += LUS_THREADS) {
-      pcol[i] = T[i * ld + j];
-      prow[i] = (i == j) ? inv : zmul(T[p * ld + i], inv);
-    }
-    __syncthreads();
+    if (tid == 0) det = zmul(det, s_pv);
     // lanes own columns lane and lane + 32 (n <= 64): the pivot row's values stay in
-    // registers across the rows; each element is one load, four FMAs and one store
+    // registers across the rows; a row's factor is its own column-j entry, read before
+    // any lane of the warp writes the row; four rows per warp in flight
     const bool c0 = lane < n, c1 = lane + 32 < n;
     const z_t pr0 = c0 ? prow[lane] : zmk(0, 0), pr1 = c1 ? prow[lane + 32] : zmk(0, 0);
+#pragma unroll 4
     for (int i = warp; i < n; i += NWARP) {
       z_t* Ti = T + i * ld;
       if (i == p) {
@@ -588,16 +592,15 @@ lu_smem_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ 
         if (c1) Ti[lane + 32] = pr1;
         continue;
       }
-      const z_t f = pcol[i];
-      if (c0) {
-        const z_t b = (lane == j) ? zmk(0, 0) : Ti[lane];
-        Ti[lane] = zmk(fma(-f.x, pr0.x, fma(f.y, pr0.y, b.x)), fma(-f.x, pr0.y, fma(-f.y, pr0.x, b.y)));
-      }
-      if (c1) {
-        const z_t b = (lane + 32 == j) ? zmk(0, 0) : Ti[lane + 32];
+      const z_t f = Ti[j];
+      const z_t b0 = (c0 && lane != j) ? Ti[lane] : zmk(0, 0);
+      const z_t b1 = (c1 && lane + 32 != j) ? Ti[lane + 32] : zmk(0, 0);
+      __syncwarp();
+      if (c0)
+        Ti[lane] = zmk(fma(-f.x, pr0.x, fma(f.y, pr0.y, b0.x)), fma(-f.x, pr0.y, fma(-f.y, pr0.x, b0.y)));
+      if (c1)
         Ti[lane + 32] =
-            zmk(fma(-f.x, pr1.x, fma(f.y, pr1.y, b.x)), fma(-f.x, pr1.y, fma(-f.y, pr1.x, b.y)));
-      }
+            zmk(fma(-f.x, pr1.x, fma(f.y, pr1.y, b1.x)), fma(-f.x, pr1.y, fma(-f.y, pr1.x, b1.y)));
     }
     __syncthreads();
   }
