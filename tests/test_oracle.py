@@ -213,3 +213,53 @@ def test_bf16_rounding_matches_torch():
     x = np.random.default_rng(1).normal(size=10000).astype(np.float32) * 100
     ref = torch.from_numpy(x).bfloat16().float().numpy()
     np.testing.assert_array_equal(M.bf16(x), ref)
+
+
+@pytest.mark.parametrize("cplx", [False, True])
+def test_oracle_full_g_path_matches_numpy(cplx):
+    """The oracle's transposed_Spvn == false branch: G_s = trial_s T1^-1 W_s^T
+    (mixed_density_matrix.hpp:96-99) and vbias = T(Spvn) G_alpha + T(Spvn) G_beta
+    (vbias.hpp:66-81), against numpy; and equal to the compact path's vbias without the
+    half-rotation cutoff (SpvnT built from the same Spvn and trial)."""
+    s = tiny_system(complex_trial=cplx, complex_chol=cplx)
+    nw = 4
+    N, n = s.N, s.n
+    o = O.Oracle(s, nw)
+    W0, Wd0 = s.initial_walkers(nw)
+    rng = np.random.default_rng(5)
+    W0 = W0 + 0.05 * (rng.normal(size=W0.shape) + 1j * rng.normal(size=W0.shape))
+    o.set_walkers(W0, Wd0)
+    o.calculate_mixed_density_matrix_full()
+    G = np.zeros((2 * N * N, nw), np.complex128)
+    for w in range(nw):
+        for sp in range(2):
+            T1 = W0[w, sp].T @ s.trial[sp]
+            G[sp * N * N:(sp + 1) * N * N, w] = (s.trial[sp] @ np.linalg.inv(T1) @ W0[w, sp].T).ravel()
+    assert rel(o.copy_out("G_full"), G) < 1e-12
+    o.get_vbias_full()
+    Sp = s.Spvn.todense()
+    vb = Sp.T @ G[:N * N] + Sp.T @ G[N * N:]
+    assert rel(o.copy_out("vbias"), vb) < 1e-12
+    Gc, _ = np_dm(s, W0)
+    Lh = s.Lh.reshape(s.nchol, 2 * n * N) * np.sqrt(s.cfg.dt)   # no cutoff
+    assert rel(np.asarray(Lh @ Gc), vb) < 1e-12
+
+
+def test_comb_restatement_properties():
+    """The comb the GPU test restates: every copy's parent has positive weight, parents
+    appear in walker order, and walker i gets floor or ceil of nw w_i / T copies."""
+    from test_gpu_population import comb
+    rng = np.random.default_rng(2)
+    nw = 200
+    W = rng.normal(size=(nw, 2, 3, 2))
+    Wd = np.zeros((nw, 8), np.complex128)
+    Wd[:, 1] = rng.lognormal(0.0, 1.0, nw)
+    Wd[::5, 1] = 0.0
+    for seed, step in ((1, 0), (1, 1), (9, 77)):
+        Wn, Wdn, idx = comb(W, Wd, seed, step)
+        w = np.maximum(Wd[:, 1].real, 0)
+        assert np.all(w[idx] > 0) and np.all(np.diff(idx) >= 0)
+        counts = np.bincount(idx, minlength=nw)
+        expect = nw * w / w.sum()
+        assert np.all(counts >= np.floor(expect) - 1e-9) and np.all(counts <= np.ceil(expect) + 1e-9)
+        assert np.allclose(Wdn[:, 1].real, w.sum() / nw)
