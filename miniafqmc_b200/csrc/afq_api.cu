@@ -1117,6 +1117,9 @@ struct afq_batch {
   cudaStream_t st = nullptr;
   cudaEvent_t fork = nullptr, done = nullptr;
   std::vector<cudaEvent_t> pre, join;
+  // recorded by the graph at the end of each system's branch (external event nodes): a
+  // handle's later work waits for its own system only, not for the whole batch
+  std::vector<cudaEvent_t> sysdone;
   cudaGraphExec_t g[2] = {nullptr, nullptr};
   std::vector<std::vector<long long>> counts[2];   // per handle, per stage
 };
@@ -1127,6 +1130,8 @@ void batch_release(afq_batch* b) {
     if (g) cudaGraphExecDestroy(g);
   for (cudaEvent_t e : b->pre) cudaEventDestroy(e);
   for (cudaEvent_t e : b->join) cudaEventDestroy(e);
+  for (cudaEvent_t e : b->sysdone)
+    if (e) cudaEventDestroy(e);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->done) cudaEventDestroy(b->done);
   if (b->st) cudaStreamDestroy(b->st);
@@ -1154,9 +1159,11 @@ afq_status afq_batch_create(afq_handle* const* handles, int count, afq_batch** o
             cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) == cudaSuccess;
   b->pre.assign(count, nullptr);
   b->join.assign(count, nullptr);
+  b->sysdone.assign(count, nullptr);
   for (int i = 0; ok && i < count; i++)
     ok = cudaEventCreateWithFlags(&b->pre[i], cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+         cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&b->sysdone[i], cudaEventDisableTiming) == cudaSuccess;
   if (!ok) {
     batch_release(b);
     return AFQ_ERR_CUDA;
@@ -1205,6 +1212,8 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
       e = st_substep(h, ortho);
       h->launch_sink = nullptr;
       h->capturing = false;
+      if (e == cudaSuccess)
+        e = cudaEventRecordWithFlags(b->sysdone[i], h->st, cudaEventRecordExternal);
       if (e == cudaSuccess) e = cudaEventRecord(b->join[i], h->st);
       if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->join[i], 0);
     }
@@ -1222,7 +1231,7 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
     return AFQ_ERR_CUDA;
   for (int i = 0; i < n; i++) {   // later work on a handle's own stream follows the step
     afq_handle* h = b->hs[i];
-    AFQ_CUDA(h, cudaStreamWaitEvent(h->st, b->done, 0));
+    AFQ_CUDA(h, cudaStreamWaitEvent(h->st, b->sysdone[i], 0));
     for (int k = 0; k < AFQ_NSTAGES; k++) h->stage_launches[k] += b->counts[slot][i][k];
     h->host_step = step_tot + 1;
   }
