@@ -180,7 +180,8 @@ def mixed_propagate_bytes(cfg, nw, order=6, preal=True):
     for the split products), the fp32 Taylor sum read and written, and the next bf16
     operand written (hi, plus lo when the next product is split).  With a real Propg1
     (preal) the P W and P S products read B operands of K = N (separate Re / Im rows)
-    instead of 2N."""
+    instead of 2N.  The last product W = P S also writes the new walkers' T1 operand (rows
+    (re, -im), hi + lo) and their next P W operand, so the chain has no pack of W."""
     N, n = cfg.nmo, cfg.nel
     W64 = nw * N * 2 * n * 16            # FP64 walkers
     F = nw * 4 * n * 2 * N * 2           # one bf16 part of a B operand
@@ -188,13 +189,12 @@ def mixed_propagate_bytes(cfg, nw, order=6, preal=True):
     V = nw * N * 2 * N * 2               # one bf16 part of the V operand
     S = nw * N * 2 * n * 8               # fp32 Taylor sum
     split = {"P": True, "V1": True, "Vk": False}
-    tot = W64 + 2 * Fp                   # pack W
-    tot += 2 * Fp + S + 2 * F            # S = P W (split): B hi+lo in, S out, next B out
+    tot = 2 * Fp + S + 2 * F             # S = P W (split): B hi+lo in, S out, next B out
     for k in range(1, order + 1):
         sp = split["V1"] if k == 1 else split["Vk"]
         nxt = 2 * Fp if k == order else (2 * F if split["Vk"] else F)
         tot += V * (2 if sp else 1) + F * (2 if sp else 1) + 2 * S + nxt
-    tot += 2 * Fp + W64                  # W = P S (split)
+    tot += 2 * Fp + W64 + F + 2 * Fp     # W = P S (split), T1 operand, next P W operand
     return float(tot)
 
 

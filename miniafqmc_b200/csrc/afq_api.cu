@@ -304,7 +304,10 @@ cudaError_t body_weights(afq_handle* h, int update_eshift) {
 // reference); the mixed form uses CholeskyQR2, equal up to column signs.
 cudaError_t body_ortho(afq_handle* h) {
   h->dm_cache = false;
-  if (h->mixed) return afq::launch_ortho_cholqr(h->W, h->N, h->n, h->nw, h->info, h->st);
+  if (h->mixed) {   // then the packed operand forms of the new walkers
+    cudaError_t e = afq::launch_ortho_cholqr(h->W, h->N, h->n, h->nw, h->info, h->st);
+    return e == cudaSuccess ? afq::mixed_repack(h->mixed, h->W, h->st) : e;
+  }
   return afq::launch_ortho(h->W, h->N, h->n, h->nw, h->st);
 }
 
@@ -374,7 +377,8 @@ cudaError_t st_weights(afq_handle* h, int update_eshift) {
   return staged(h, AFQ_STAGE_WEIGHTS, 1, [&] { return body_weights(h, update_eshift); });
 }
 cudaError_t st_ortho(afq_handle* h) {
-  return staged(h, AFQ_STAGE_ORTHO, 1, [&] { return body_ortho(h); });
+  return staged(h, AFQ_STAGE_ORTHO, 1 + (h->mixed ? afq::mixed_repack_launches(h->mixed) : 0),
+                [&] { return body_ortho(h); });
 }
 cudaError_t st_energy(afq_handle* h, int mode) {
   int nl = mode == AFQ_ENERGY_VAKBL ? 3
@@ -745,6 +749,7 @@ afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data)
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
   h->have_walkers = true;
   h->dm_cache = false;
+  afq::mixed_invalidate(h->mixed);
   return AFQ_OK;
 }
 
@@ -945,6 +950,7 @@ afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step) {
     return fail(h, AFQ_ERR_STATE, "population control: no walker has positive weight");
   AFQ_CUDA(h, cudaStreamSynchronize(h->st));
   h->dm_cache = false;   // the walkers changed
+  afq::mixed_invalidate(h->mixed);
   return AFQ_OK;
 }
 
@@ -1078,8 +1084,10 @@ afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int nort
   if (seed != h->host_seed || step_tot != h->host_step)
     if ((s = set_scalars(h, seed, step_tot)) != AFQ_OK) return s;
   const bool ortho = step_tot > 0 && step_tot % (uint64_t)northo == 0;
-  // the captured substep starts with a density matrix formed from the cached T1^-1 (and
-  // ends with an overlap call that leaves it valid): refresh it first when it is stale
+  // the captured substep starts with a density matrix formed from the cached T1^-1 and the
+  // packed operand forms of the walkers (and leaves both valid at its end): refresh them
+  // first when they are stale
+  if (h->mixed) AFQ_CUDA(h, afq::mixed_ensure_packed(h->mixed, h->W, h->st));
   if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
   cudaGraphExec_t* slot = ortho ? &h->g_ortho : &h->g_plain;
   long long* counts = ortho ? h->g_ortho_launches : h->g_plain_launches;
@@ -1193,6 +1201,7 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
     if (h->profiling) return fail(h, AFQ_ERR_STATE, "stage profiling is on");
     if (seeds[i] != h->host_seed || step_tot != h->host_step)
       if ((s = set_scalars(h, seeds[i], step_tot)) != AFQ_OK) return s;
+    if (h->mixed) AFQ_CUDA(h, afq::mixed_ensure_packed(h->mixed, h->W, h->st));
     if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
     AFQ_CUDA(h, cudaEventRecord(b->pre[i], h->st));
     if (cudaStreamWaitEvent(b->st, b->pre[i], 0) != cudaSuccess) return AFQ_ERR_CUDA;

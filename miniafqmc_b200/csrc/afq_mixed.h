@@ -44,6 +44,13 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
 bool mixed_has_dm(const MixedState* m);
 cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, int want_gc,
                      int save_old, int cached, cudaStream_t st);
+// Packed operand forms of the walkers (the T1 and P W operands): the propagation
+// leaves them current; mixed_invalidate marks them stale after any other change of W,
+// mixed_repack forms them from W, mixed_ensure_packed does so only when they are stale.
+void mixed_invalidate(MixedState* m);
+cudaError_t mixed_repack(MixedState* m, const z_t* W, cudaStream_t st);
+cudaError_t mixed_ensure_packed(MixedState* m, const z_t* W, cudaStream_t st);
+int mixed_repack_launches(const MixedState* m);
 // Kernels one call of a stage issues (afq_stage numbering), for the launch counters.
 int mixed_launches(const MixedState* m, int stage);
 // Cholesky-vector blocks of the exchange partial sums (Kpart[nw][2][nblk]).

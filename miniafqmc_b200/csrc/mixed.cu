@@ -135,6 +135,14 @@ struct MixedState {
   float2* T1 = nullptr;        // [nw][2][n][n]
   int bn_t1 = 0, bn_gc = 0;
   tc::Maps m_t1, m_gc[2];
+  // packed forms of the current walkers written by the last propagation product (pair
+  // epilogue) or by mixed_repack: F2 = the next P W operand, F[fa_buf] = the T1 operand.
+  // `packed` is false after anything else changed W.  (The Gc operand Wn is packed by the
+  // density matrix: its row-strided stores cost the epilogue more than the pack kernel.)
+  Op F2;
+  tc::Maps m_pw2, m_t1_1;
+  bool packed = false;
+  int fa_buf = 0;
   // kernel of each product site (0 built-in rule, 1 persistent, 2 per-tile), chosen at
   // set-up by timing the candidates on the real shapes; part_cap = split-K slots allocated
   int tune[TS_N] = {};
@@ -953,6 +961,41 @@ struct EpiPropPair {
   }
 };
 
+// The last propagation product W = P S, written with the new walkers' packed forms
+// (pair layout as EpiPropPair): the layouts their next consumers read, as the pack kernels
+// form them from W, bit for bit (a float converted to double and back is unchanged).
+// FA = the T1 operand (rows (re, -im)); F2 = the next P W operand ((re | im) rows when
+// f2_real, else (re, -im) / (im, re) rows); lanes on consecutive orbitals i (coalesced).
+// A functor of its own, so that the seven other products per substep keep their short
+// epilogue (a longer one in the shared kernel slowed all of them).
+struct EpiPropPack {
+  static constexpr bool kTile = false, kPair = true;
+  int N, n2;
+  z_t* W;
+  Op FA, F2;
+  int f2_real;
+  AFQ_D int pair_stride() const { return n2; }
+  AFQ_D void pair(int w, int, int i, int j0, const float* cr, const float* ci) const {
+    if (i >= N) return;
+    const long long row = (long long)w * N * n2 + (long long)i * n2;    // W[w][i][.]
+    const long long base = (long long)w * 2 * n2 * 2 * N;
+#pragma unroll
+    for (int jj = 0; jj < 32; jj++) {
+      const int j = j0 + jj;
+      const float vr = cr[jj], vi = ci[jj];
+      W[row + j] = zmk(vr, vi);
+      put2(FA, base + (long long)j * 2 * N + 2 * i, vr, -vi);
+      if (f2_real) {
+        put1(F2, base + (long long)j * 2 * N + i, vr);
+        put1(F2, base + (long long)(n2 + j) * 2 * N + i, vi);
+      } else {
+        put2(F2, base + (long long)j * 2 * N + 2 * i, vr, -vi);
+        put2(F2, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
+      }
+    }
+  }
+};
+
 // Exchange: rows (cv, a), columns (wl, re|im, b); per (cv, wl) the trace of T^2 with
 // T[a][b] = tile[cv*n + a][wl*2n + b] + i tile[cv*n + a][wl*2n + n + b].
 struct EpiExchange {
@@ -1240,9 +1283,13 @@ cudaError_t run_bn(int bn, int prec, const tc::Maps& mp, const tc::GemmShape& g,
 
 // propagation product with the pair epilogue when 2n is a multiple of 32
 cudaError_t run_prop(MixedState* m, int prec, const tc::Maps& mp, const tc::GemmShape& g, int mode,
-                     int k, int last, z_t* W, const Op& F, cudaStream_t st) {
+                     int k, int last, z_t* W, const Op& F, cudaStream_t st, int fa_buf = -1) {
   const int n2 = 2 * m->n;
   if (n2 % 32 == 0) {
+    if (mode == 2 && fa_buf >= 0) {   // the new walkers' packed forms as well
+      EpiPropPack ep{m->N, n2, W, m->F[fa_buf], m->F2, (m->preal && m->in.order >= 1) ? 1 : 0};
+      return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st, m->tune[TS_PROP]);
+    }
     EpiPropPair ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
     return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st, m->tune[TS_PROP]);
   }
@@ -1339,6 +1386,7 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   A(malloc_track(m, &m->err, 1));
   A(malloc_track(m, &m->wscale, nw));
   A(malloc_track(m, &m->dmax, 2));
+  A(alloc_op(m, m->F2, (size_t)nw * 4 * n * 2 * N));
   if (init->trial) {
     A(alloc_op(m, m->TwB, (size_t)4 * n * 2 * N));
     A(alloc_op(m, m->Wn, (size_t)nw * N * 4 * n));
@@ -1484,6 +1532,10 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   const uint64_t vrows = m->vsym ? (uint64_t)m->npairs * 256 : (uint64_t)N * N;
   ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv);
   const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
+  {
+    const uint64_t Kp = m->preal ? N : 2 * N;
+    ok &= map2(m->m_pw2, m->Pf, Kp, N, 1, Kp, 0, m->F2, Kp, fr, nw, 2 * N, fsz, m->bn_prop);
+  }
   for (int i = 0; i < 2; i++) {
     const uint64_t Kp = m->preal ? N : 2 * N;
     ok &= map2(m->m_pw[i], m->Pf, Kp, N, 1, Kp, 0, m->F[i], Kp, fr, nw, 2 * N, fsz, m->bn_prop);
@@ -1517,6 +1569,8 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
     ok &= map2(m->m_t1, m->F[0], 2 * N, fr, nw, 2 * N, fsz, m->TwB, 2 * N, 4 * n, 1, 2 * N, 0,
                m->bn_t1);
+    ok &= map2(m->m_t1_1, m->F[1], 2 * N, fr, nw, 2 * N, fsz, m->TwB, 2 * N, 4 * n, 1, 2 * N, 0,
+               m->bn_t1);
     for (int sp = 0; sp < 2; sp++) {
       Op a{m->Wn.hi + 2 * n * sp, m->Wn.lo + 2 * n * sp};
       Op b{m->Tinv.hi + (size_t)sp * 2 * n * 2 * n, m->Tinv.lo + (size_t)sp * 2 * n * 2 * n};
@@ -1546,10 +1600,11 @@ int mixed_launches(const MixedState* m, int stage) {
   switch (stage) {
     case 1: return 3;                                  // pack, GEMM, reduce (vbias)
     case 3: return 2;                                  // pack, GEMM (vHS)
-    case 4: return 2 + m->in.order + 1;                // pack, P W, order terms, P S
+    // the walker packs drop out while the packed forms are current (m->packed at the call)
+    case 4: return (m->packed ? 1 : 2) + m->in.order + 1;   // [pack], P W, terms, P S
     case 8: return m->in.Lh ? 4 : 0;                   // pack, E_J GEMM, reduce, E_K GEMM
-    case 0: return 6;                                  // pack, T1, LU, pack, Gc x 2 (3 cached)
-    case 5: return 3;                                  // pack, T1, LU (overlaps)
+    case 0: return m->packed ? 5 : 6;                  // [pack], T1, LU, pack, Gc x 2
+    case 5: return m->packed ? 2 : 3;                  // [pack], T1, LU (overlaps)
   }
   return 0;
 }
@@ -1589,17 +1644,21 @@ static Op next_op(const Op& F, int prec) { return prec == PREC_SPLIT ? F : Op{F.
 cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) {
   const int N = m->N, n2 = 2 * m->n, nw = m->nw;
   const bool pr = m->preal && m->in.order >= 1;
-  pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0],
-                                                                               pr ? 2 : 1);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  const bool from_f2 = m->packed;   // the P W operand of these walkers is in F2 already
+  m->packed = false;
+  cudaError_t e;
+  if (!from_f2) {
+    pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(
+        W, N, n2, m->F[0], pr ? 2 : 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   const int mt = (N + 127) / 128;
   const int Kp = pr ? N : 2 * N;   // K of P W and P S
   int cur = 0;
   {  // S = P W
     tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
-    if ((e = run_prop(m, m->prec_p, m->m_pw[0], g, 0, 0, 0, nullptr, next_op(m->F[1], m->prec_v1),
-                      st)) != cudaSuccess)
+    if ((e = run_prop(m, m->prec_p, from_f2 ? m->m_pw2 : m->m_pw[0], g, 0, 0, 0, nullptr,
+                      next_op(m->F[1], m->prec_v1), st)) != cudaSuccess)
       return e;
     cur = 1;
   }
@@ -1613,11 +1672,50 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
       return e;
     cur ^= 1;
   }
-  {  // W = P S (with order 0 the B operand of S = P W is already in F[cur])
+  {  // W = P S (with order 0 the B operand of S = P W is already in F[cur]); the pair
+     // epilogue also writes the new walkers' packed forms (F[cur ^ 1] is free)
     tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
-    if ((e = run_prop(m, m->prec_p, m->m_pw[cur], g, 2, 0, 0, W, Op{}, st)) != cudaSuccess) return e;
+    if ((e = run_prop(m, m->prec_p, m->m_pw[cur], g, 2, 0, 0, W, Op{}, st, cur ^ 1)) !=
+        cudaSuccess)
+      return e;
+  }
+  if (n2 % 32 == 0 && m->Wn.hi) {   // pair epilogue, and a trial (the T1 product exists)
+    m->packed = true;
+    m->fa_buf = cur ^ 1;
   }
   return cudaSuccess;
+}
+
+void mixed_invalidate(MixedState* m) {
+  if (m) m->packed = false;
+}
+
+// The packed forms from W itself (after the orthogonalisation, or before a captured
+// substep that expects them): the same layouts the propagation epilogue writes.
+cudaError_t mixed_repack(MixedState* m, const z_t* W, cudaStream_t st) {
+  if (!m) return cudaSuccess;
+  const int N = m->N, n2 = 2 * m->n, nw = m->nw;
+  m->packed = false;
+  if (n2 % 32 || !m->Wn.hi) return cudaSuccess;   // no fused path: the consumers pack
+  const bool pr = m->preal && m->in.order >= 1;
+  const dim3 grid((N + 31) / 32, (n2 + 31) / 32, nw), blk(32, 8);
+  pack_w_kernel<<<grid, blk, 0, st>>>(W, N, n2, m->F2, pr ? 2 : 1);
+  pack_w_kernel<<<grid, blk, 0, st>>>(W, N, n2, m->F[0], 0);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    m->packed = true;
+    m->fa_buf = 0;
+  }
+  return e;
+}
+
+int mixed_repack_launches(const MixedState* m) {
+  return (m && 2 * m->n % 32 == 0 && m->Wn.hi) ? 2 : 0;
+}
+
+cudaError_t mixed_ensure_packed(MixedState* m, const z_t* W, cudaStream_t st) {
+  if (!m || m->packed) return cudaSuccess;
+  return mixed_repack(m, W, st);
 }
 
 static cudaError_t splitk_product(MixedState* m, const tc::Maps& mp, int prec, float ascale,
@@ -1733,19 +1831,23 @@ cudaError_t mixed_dm(MixedState* m, const z_t* W, z_t* Gc, z_t* Wd, int* info, i
   if (!mixed_has_dm(m)) return cudaErrorInvalidValue;
   const int N = m->N, n = m->n, n2 = 2 * n, nw = m->nw;
   cudaError_t e;
-  if (cached && want_gc) goto gc;
-  pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2, m->F[0], 0);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  {  // T1 (conjugated) of both spins: one 128-row tile per walker
+  if (!(cached && want_gc)) {
+    // T1 (conjugated) of both spins: one 128-row tile per walker; its A operand is packed
+    // unless the walkers' packed forms are current
+    if (!m->packed) {
+      pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(W, N, n2,
+                                                                                   m->F[0], 0);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    const tc::Maps& mt1 = (m->packed && m->fa_buf == 1) ? m->m_t1_1 : m->m_t1;
     tc::GemmShape g{128, 4 * n, 2 * N, nw, 128, 1, true, false, 0};
-    if ((e = run_bn(m->bn_t1, PREC_SPLIT, m->m_t1, g, EpiT1{m->T1, n}, m->err, st,
+    if ((e = run_bn(m->bn_t1, PREC_SPLIT, mt1, g, EpiT1{m->T1, n}, m->err, st,
                     m->tune[TS_T1])) != cudaSuccess)
       return e;
+    if ((e = launch_lu(m->T1, n, 2 * nw, m->Tinv, Wd, info, 1, save_old, st)) != cudaSuccess ||
+        !want_gc)
+      return e;
   }
-  if ((e = launch_lu(m->T1, n, 2 * nw, m->Tinv, Wd, info, 1, save_old, st)) != cudaSuccess ||
-      !want_gc)
-    return e;
-gc:
   pack_wn_kernel<<<grid_for((long long)nw * N * n2), 256, 0, st>>>(W, (long long)nw * N * n2, m->Wn);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   for (int sp = 0; sp < 2; sp++) {

@@ -170,3 +170,39 @@ def test_cholqr_orthonormal_with_one_or_two_passes(spread):
             X = W[w, sp]
             assert np.max(np.abs(Q @ (Q.conj().T @ X) - X)) < 1e-10 * np.max(np.abs(X))
     m.close()
+
+
+@pytest.mark.parametrize("name,kw,nw", [("C1", {}, 16), ("C2", dict(with_vakbl=False), 32)])
+def test_packed_forms_equal_packing_from_w(name, kw, nw):
+    """The last propagation product writes the new walkers' T1 and P W operands itself,
+    and the orthogonalisation repacks them; population control and set_walkers mark them
+    stale.  Overlaps, density matrix and the next propagation from those forms are bit for
+    bit the ones of a handle given the same walkers (which packs them from W)."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    s = system(name, **kw)
+    e = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=perturbed(s, nw, seed=4))
+
+    def step(x, k):
+        x.calculate_mixed_density_matrix()
+        x.get_vbias()
+        x.sigma(7, k)
+        x.get_vHS()
+        x.propagate()
+
+    step(e, 1)
+    for k, change in enumerate(("none", "ortho", "population")):
+        if change == "ortho":
+            e.orthogonalize()
+        elif change == "population":
+            e.population_control(11, k)
+        f = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=e.get_walkers())
+        for x in (e, f):
+            x.calculate_overlaps()
+        assert np.array_equal(e.get_walker_data(), f.get_walker_data()), change
+        for x in (e, f):
+            step(x, 2 + k)
+        assert np.array_equal(e.copy_out("Gc"), f.copy_out("Gc")), change
+        We, Wf = e.get_walkers(), f.get_walkers()
+        assert np.array_equal(We[0], Wf[0]) and np.array_equal(We[1], Wf[1]), change
+        f.close()
+    e.close()
