@@ -113,7 +113,9 @@ class Config:
                 f"_W{self.nwalk}_seed{self.seed}")
 
 
-# The workload table (see DESIGN.md for which test / bench line uses which).
+# The workload table: C1 and C2 are the parity-test cases, C3 (Spvn above the dense
+# threshold) and C4 run through `bench.py --config`, C4 is the bench's default workload and
+# C5 the heterogeneous batch.
 CONFIGS = {
     # small closed shell, every stage checked against the FP64 oracle
     "C1": Config(64, 16, 256, 0.10, 0, dt=0.005, nwalk=16, nsteps=20, northo=5,

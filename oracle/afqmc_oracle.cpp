@@ -3,8 +3,8 @@
 // TEST INFRASTRUCTURE ONLY.  This file restates, in plain C++, the algorithm of the
 // reference miniapp (QMCPACK miniAFQMC) for one walker ensemble, with the reference's
 // call granularity: a per-walker loop of small zgemm / zgetrf / zgetri / zgelqf / zunglq
-// calls and the serial CSR x dense loop of `mySPBLAS::csrmm`.  It is the checker the
-// GPU library is compared against and the timed CPU baseline; nothing in the product
+// calls and the serial CSR x dense loop of `mySPBLAS::csrmm`.  The GPU library's tests
+// compare against it and the bench times it as the CPU baseline; nothing in the product
 // links or calls it.
 //
 // BLAS/LAPACK are not part of the reference tree (it links any Fortran LAPACK,

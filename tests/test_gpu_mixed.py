@@ -4,7 +4,7 @@ Stage tolerances (relative to the largest magnitude of the quantity; overlaps re
 per walker):
   split bf16 (hi*hi + hi*lo + lo*hi) stages: 1e-4    plain bf16 stages: 2e-2
 Trajectory: per-step mixed energy within 1e-4 relative of the FP64 energy on the same
-auxiliary fields.  Measured errors are written to gpurun_out/mixed_errors.json."""
+auxiliary fields.  The measured errors are also written out as JSON (OUT)."""
 import json
 import os
 
