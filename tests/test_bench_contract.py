@@ -1,0 +1,86 @@
+"""The bench's JSON contract on the host (no GPU).
+
+The reference arm (`bench.py --impl reference`: the FP64 CPU restatement of the reference
+on the host cores) prints exactly one line with the contract's keys, and only rank 0
+prints it.  The roofline's algorithmic models have their closed forms: the propagation
+chain's HBM bytes (FP64 walkers out, each bf16 operand read once, the fp32 Taylor sum
+read and written, the new walkers' packed forms written by the last product) and the
+tensor-core FLOPs of the vHS stage."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+CONTRACT_KEYS = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better",
+                 "scaling", "vs_baseline", "dtype", "data", "config")
+
+
+def run_bench(args, env=None):
+    e = dict(os.environ)
+    e.update(env or {})
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT,
+                          capture_output=True, text=True, timeout=600, env=e)
+
+
+def test_reference_arm_prints_one_contract_line():
+    out = run_bench(["--impl", "reference", "--config", "C1", "--steps", "1", "--warmup", "3",
+                     "--cpu-walkers", "4"])
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in CONTRACT_KEYS:
+        assert k in d, k
+    assert d["impl"] == "reference" and d["metric"] == "walker-steps/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["steps"] == 1
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    assert d["cpu_baseline"]["cores"] >= 1 and "4 walkers" in d["cpu_baseline"]["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+    assert d["config"]["workload"].startswith("C1:")
+
+
+def test_reference_arm_other_ranks_print_nothing():
+    out = run_bench(["--impl", "reference", "--config", "C1", "--steps", "1", "--warmup", "3",
+                     "--cpu-walkers", "4"], env={"RANK": "1"})
+    assert out.returncode == 0 and out.stdout.strip() == ""
+
+
+def test_propagation_byte_model():
+    sys.path.insert(0, ROOT)
+    import bench
+    from miniafqmc_b200.synthetic import CONFIGS
+    cfg = CONFIGS["C4"]
+    N, n, nw = cfg.nmo, cfg.nel, 1024
+    W64 = nw * N * 2 * n * 16                  # FP64 walkers [nw][2][N][n]
+    F = nw * 4 * n * 2 * N * 2                 # one bf16 part of a complex-as-real B operand
+    Fp = F // 2                                # real Propg1: K = N
+    V = nw * N * 2 * N * 2                     # one bf16 part of the V operand
+    S = nw * N * 2 * n * 8                     # fp32 Taylor sum
+    pw = 2 * Fp + S + 2 * F                    # S = P W
+    t1 = 2 * V + 2 * F + 2 * S + F             # first Taylor term (split V and B)
+    tk = V + F + 2 * S + F                     # terms 2-5 (plain bf16)
+    t6 = V + F + 2 * S + 2 * Fp                # term 6 forms the P S operand
+    ps = 2 * Fp + W64 + F + 2 * Fp             # W = P S + T1 operand + next P W operand
+    want = pw + t1 + 4 * tk + t6 + ps
+    assert bench.mixed_propagate_bytes(cfg, nw) == pytest.approx(want, rel=1e-15)
+    assert want == pytest.approx(14.4955e9, rel=1e-4)
+    # every term scales with the walker count
+    assert bench.mixed_propagate_bytes(cfg, 2 * nw) == pytest.approx(2 * want, rel=1e-15)
+    # a complex Propg1: the four P-product operands (hi + lo each) have K = 2N
+    cplx = want + 4 * 2 * (F - Fp)
+    assert bench.mixed_propagate_bytes(cfg, nw, preal=False) == pytest.approx(cplx, rel=1e-15)
+
+
+def test_vhs_flop_model():
+    sys.path.insert(0, ROOT)
+    import bench
+    from miniafqmc_b200.synthetic import CONFIGS
+    cfg = CONFIGS["C4"]
+    N, nc, nw = cfg.nmo, cfg.nchol, 1024
+    # real Spvn x complex X over the N(N+1)/2 symmetric orbital pairs: 4 FLOP each
+    assert bench.mixed_stage_flops(cfg, nw, "vHS") == 4.0 * nw * (N * (N + 1) // 2) * nc
