@@ -4,10 +4,37 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+#include <cstddef>
+#include <mutex>
+
 #define AFQ_HD __host__ __device__ __forceinline__
 #define AFQ_D __device__ __forceinline__
 
 typedef double2 z_t;
+
+// Host: a kernel's one-time function attributes (dynamic shared memory size, carveout)
+// belong to the device current when they are set, and one process may drive handles on
+// several devices (afq_system_desc::device) from several threads.  ensure(bytes, set)
+// runs set(bytes) the first time a launch on the current device needs `bytes` or more,
+// under a lock, so the recorded size (and the attribute) only grows.  A device ordinal
+// outside the table runs set(bytes) every time.
+struct DeviceAttr {
+  static constexpr int kDevices = 64;
+  std::atomic<size_t> set_bytes[kDevices] = {};
+  std::mutex mu;
+  template <class F>
+  cudaError_t ensure(size_t bytes, F&& set) {
+    int d = -1;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kDevices) return set(bytes);
+    if (set_bytes[d].load(std::memory_order_acquire) >= bytes) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(mu);
+    if (set_bytes[d].load(std::memory_order_relaxed) >= bytes) return cudaSuccess;
+    const cudaError_t e = set(bytes);
+    if (e == cudaSuccess) set_bytes[d].store(bytes, std::memory_order_release);
+    return e;
+  }
+};
 
 AFQ_HD z_t zmk(double r, double i) { return make_double2(r, i); }
 AFQ_HD z_t zadd(z_t a, z_t b) { return make_double2(a.x + b.x, a.y + b.y); }

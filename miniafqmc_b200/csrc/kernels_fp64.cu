@@ -225,16 +225,16 @@ dm_kernel(const z_t* __restrict__ W, const z_t* __restrict__ tw, int N, int n,
 cudaError_t launch_dm(const z_t* W, const z_t* tw, int N, int n, int nw, z_t* Gc, z_t* Wd,
                       int* info, int want_gc, int save_old, cudaStream_t st) {
   size_t smem = dm_smem_bytes(n);
-  static size_t attr = 0;
-  if (smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e == cudaSuccess)   // several CTAs per SM need the full shared-memory carveout
-      e = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(smem, [](size_t b) {
+    cudaError_t r = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)b);
+    if (r == cudaSuccess)   // several CTAs per SM need the full shared-memory carveout
+      r = cudaFuncSetAttribute(dm_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    attr = smem;
-  }
+    return r;
+  });
+  if (e != cudaSuccess) return e;
   dm_kernel<<<2 * nw, DM_THREADS, smem, st>>>(W, tw, N, n, Gc, Wd, info, want_gc, save_old);
   return cudaGetLastError();
 }
@@ -803,16 +803,16 @@ ortho_cholqr_kernel(z_t* __restrict__ W, int N, int n, int* __restrict__ info, i
 cudaError_t launch_ortho_cholqr(z_t* W, int N, int n, int nw, int* info, cudaStream_t st) {
   if (n > 64) return cudaErrorInvalidValue;   // the register tiles cover n <= 64
   size_t smem = cholqr_smem_bytes(n);
-  static size_t attr = 0;
-  if (smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(ortho_cholqr_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(ortho_cholqr_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(smem, [](size_t b) {
+    cudaError_t r = cudaFuncSetAttribute(ortho_cholqr_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+    if (r == cudaSuccess)
+      r = cudaFuncSetAttribute(ortho_cholqr_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    attr = smem;
-  }
+    return r;
+  });
+  if (e != cudaSuccess) return e;
   static const int two_pass = [] {
     const char* e = getenv("AFQ_CHOLQR_PASSES");
     return e && atoi(e) == 2 ? 1 : 0;
@@ -928,13 +928,12 @@ cudaError_t launch_exchange(const z_t* Lh, const z_t* Gc, int N, int n, int ncho
   *nblk_out = nblk;
   if (!Kpart) return cudaSuccess;
   size_t smem = exch_smem_bytes();
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(exchange_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(smem, [](size_t b) {
+    return cudaFuncSetAttribute(exchange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)b);
+  });
+  if (e != cudaSuccess) return e;
   dim3 grid(nblk, (nw + Gw - 1) / Gw, 2);
   exchange_kernel<<<grid, EX_THREADS, smem, st>>>(Lh, Gc, N, n, nchol, nw, Gn, Gw, Kpart, nblk);
   return cudaGetLastError();

@@ -648,16 +648,16 @@ cudaError_t launch_lu(const float2* T1, int n, int nmat, Op Tinv, z_t* Wd, int* 
   static const bool regs = getenv("AFQ_LU_REGISTERS") != nullptr;
   if (!regs && n <= 64) {   // shared-memory form (default)
     const size_t smem = lus_smem_bytes(n);
-    static size_t attr = 0;
-    if (smem > attr) {   // and the full shared-memory carveout: five matrices per SM
-      cudaError_t e = cudaFuncSetAttribute(lu_smem_kernel,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(lu_smem_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+    static DeviceAttr attr;   // and the full shared-memory carveout: five matrices per SM
+    cudaError_t e = attr.ensure(smem, [](size_t b) {
+      cudaError_t r = cudaFuncSetAttribute(lu_smem_kernel,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+      if (r == cudaSuccess)
+        r = cudaFuncSetAttribute(lu_smem_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                  (int)cudaSharedmemCarveoutMaxShared);
-      if (e != cudaSuccess) return e;
-      attr = smem;
-    }
+      return r;
+    });
+    if (e != cudaSuccess) return e;
     lu_smem_kernel<<<nmat, LUS_THREADS, smem, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
     return cudaGetLastError();
   }
@@ -1193,32 +1193,31 @@ struct EpiExchangePromoted {
 // The persistent kernel (double-buffered accumulator) runs every product whose epilogue
 // needs no shared-memory tile; AFQ_TC_PERSISTENT=0 selects the per-tile kernel instead.
 bool tc_persistent() {
-  static int on = -1;
-  if (on < 0) {
+  static const bool on = [] {   // initialised once, thread-safe
     const char* e = getenv("AFQ_TC_PERSISTENT");
-    on = (e && atoi(e) == 0) ? 0 : 1;
-  }
-  return on == 1;
+    return !(e && atoi(e) == 0);
+  }();
+  return on;
 }
 
 // K slabs per promoted chunk: AFQ_PROMOTE="part=<k>,ex=<k>" (0 turns promotion off)
 enum { PROMOTE_PART, PROMOTE_EXCHANGE };
 int promote_kb(int which) {
-  static int kb[2] = {-1, -1};
-  if (kb[0] < 0) {
+  struct KB { int v[2]; };
+  static const KB kb = [] {   // initialised once, thread-safe
     // C4 (NMO 384, 48+48 electrons, nchol 1536, 1024 walkers), same walkers as the FP64
     // form: E_J error 2e-6 Ha with part=2; E_K -1.4e-5 Ha with ex=1 (5.9 ms per 128-walker
     // subset), -2.7e-5 Ha with ex=2 (4.7 ms), -9.1e-5 Ha without promotion (4.4 ms)
-    kb[0] = 2;
-    kb[1] = 2;
+    KB r{{2, 2}};
     if (const char* env = getenv("AFQ_PROMOTE")) {
       const std::string s(env);
       const size_t p = s.find("part="), q = s.find("ex=");
-      if (p != std::string::npos) kb[0] = atoi(s.c_str() + p + 5);
-      if (q != std::string::npos) kb[1] = atoi(s.c_str() + q + 3);
+      if (p != std::string::npos) r.v[0] = atoi(s.c_str() + p + 5);
+      if (q != std::string::npos) r.v[1] = atoi(s.c_str() + q + 3);
     }
-  }
-  return kb[which];
+    return r;
+  }();
+  return kb.v[which];
 }
 
 // Functors that may consume fp16 split operands (kF16) get that variant compiled.

@@ -703,16 +703,15 @@ cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* er
   static_assert(MINB * C::SMEM <= 228 * 1024 && MINB * C::TMEM_COLS <= 512,
                 "CTAs per SM exceed shared memory or TMEM");
   auto kern = tc_gemm_kernel<BN, STAGES, FMT, SPLIT, Epi, MINB>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)C::SMEM);
-    if (e == cudaSuccess && MINB > 1)
-      e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(C::SMEM, [kern](size_t b) {
+    cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+    if (r == cudaSuccess && MINB > 1)
+      r = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                                (int)cudaSharedmemCarveoutMaxShared);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+    return r;
+  });
+  if (e != cudaSuccess) return e;
   const int ns = g.n_step > 0 ? g.n_step : BN;
   const unsigned ntiles = (g.N + ns - 1) / ns;
   dim3 grid(g.m_fast ? g.m_tiles : ntiles, g.m_fast ? ntiles : g.m_tiles, g.batch);
@@ -722,13 +721,13 @@ cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* er
 }
 
 inline int sm_count() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
+  static const int n = [] {   // initialised once, thread-safe (every device is a B200)
+    int dev = 0, c = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
-      n = 148;
-  }
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || c <= 0)
+      c = 148;
+    return c;
+  }();
   return n;
 }
 
@@ -738,13 +737,11 @@ cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& e
   using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
   static_assert(P::kFits, "persistent configuration exceeds shared memory or TMEM");
   auto kern = tc_gemm_persistent_kernel<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)P::SMEM);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(P::SMEM, [kern](size_t b) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  });
+  if (e != cudaSuccess) return e;
   const int ns = g.n_step > 0 ? g.n_step : BN;
   TileSched sc{g.m_tiles, (g.N + ns - 1) / ns, g.batch, g.m_fast ? 1 : 0};
   const int total = sc.total();

@@ -174,13 +174,11 @@ cudaError_t zgemm_launch(const ZGemmDesc& d, int batch, const Epi& epi, cudaStre
   {                                                                                        \
     using Cfg = ZTileCfg<BM_, BN_, 16, TM_, TN_>;                                          \
     auto kern = zgemm_kernel<BM_, BN_, 16, TM_, TN_, A_KMAJ, B_KMAJ, Epi>;                 \
-    static bool attr_set = false;                                                          \
-    if (!attr_set) {                                                                       \
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                           (int)Cfg::SMEM);                                \
-      if (e != cudaSuccess) return e;                                                      \
-      attr_set = true;                                                                     \
-    }                                                                                      \
+    static DeviceAttr attr;                                                                \
+    const cudaError_t e = attr.ensure(Cfg::SMEM, [kern](size_t b) {                        \
+      return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b); \
+    });                                                                                    \
+    if (e != cudaSuccess) return e;                                                        \
     dim3 grid((d.N + BN_ - 1) / BN_, (d.M + BM_ - 1) / BM_, batch);                        \
     kern<<<grid, Cfg::NT, Cfg::SMEM, st>>>(d, epi);                                        \
     return cudaGetLastError();                                                             \
