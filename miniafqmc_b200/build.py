@@ -1,7 +1,8 @@
-"""Builds libafqmc_b200.so (sm_100a) in-tree with nvcc.
+"""Builds libafqmc_b200.so (sm_100a) in-tree with nvcc, then the driver program.
 
 The library is the product: every CUDA kernel and the C ABI of include/afqmc_b200.h.
-It is compiled for sm_100a only (`-gencode arch=compute_100a,code=sm_100a`)."""
+It is compiled for sm_100a only (`-gencode arch=compute_100a,code=sm_100a`).  The driver
+program `miniafqmc` (app/miniafqmc.cpp, g++) is the miniapp's main over that ABI."""
 from __future__ import annotations
 
 import glob
@@ -13,6 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libafqmc_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+DRIVER_SRC = os.path.join(HERE, "app", "miniafqmc.cpp")
+DRIVER = os.path.join(HERE, "miniafqmc")
+DRIVER_FLAGS = ["-O2", "-std=c++17", "-Wall"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -41,14 +45,34 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra=()) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [NVCC, *NVCC_FLAGS, *extra, "-I", os.path.join(HERE, "..", "include"),
-           *sources(), "-o", LIB]
+    if force or not up_to_date():
+        cmd = [NVCC, *NVCC_FLAGS, *extra, "-I", os.path.join(HERE, "..", "include"),
+               *sources(), "-o", LIB]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd)
+    build_driver(force=force, verbose=verbose)
+    return LIB
+
+
+def driver_command(lib_dir: str, out: str) -> list:
+    """g++ line of the driver program linked against libafqmc_b200.so in lib_dir."""
+    return ["g++", *DRIVER_FLAGS, "-I", os.path.join(HERE, "..", "include"), DRIVER_SRC,
+            "-L", lib_dir, "-lafqmc_b200", f"-Wl,-rpath,{lib_dir}", "-o", out]
+
+
+def build_driver(force: bool = False, verbose: bool = False) -> str:
+    """The miniapp's driver program over the C ABI (`miniafqmc_b200/miniafqmc`)."""
+    deps = [DRIVER_SRC, LIB, os.path.join(HERE, "..", "include", "afqmc_b200.h")]
+    if (not force and os.path.exists(DRIVER)
+            and all(os.path.getmtime(f) <= os.path.getmtime(DRIVER) for f in deps)):
+        return DRIVER
+    cmd = driver_command("$ORIGIN", DRIVER)
+    cmd[cmd.index("-L") + 1] = HERE
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.check_call(cmd)
-    return LIB
+    return DRIVER
 
 
 if __name__ == "__main__":

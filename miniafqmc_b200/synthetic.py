@@ -41,6 +41,7 @@ import scipy.linalg
 import scipy.sparse as sp
 
 HALFROTATE_CUTOFF = 1e-6  # rotate.hpp:69 default cutoff
+INPUT_MAGIC = b"AFQINP01"  # the driver binary's input file (System.write_input)
 
 
 @dataclasses.dataclass
@@ -262,6 +263,41 @@ class System:
         d[pr + "Spvn_vals_0"] = v
         return d
 
+    def write_input(self, path: str) -> None:
+        """The driver binary's input file (`miniafqmc_b200/miniafqmc -f path`): the
+        in-memory data `afqmc::Initialize` leaves behind (initialize_serial.hpp:89-221),
+        in place of the HDF5 file no library here can write.  Little-endian binary:
+
+          char[8]  "AFQINP01"
+          int32    nmo, naea, naeb, nchol
+          float64  dt                        (the time step Propg1 was formed with)
+          int32    has_vakbl
+          CSR      Spvn [nmo^2 x nchol], values scaled by sqrt(dt)
+          float64  Propg1 [nmo][nmo] complex
+          float64  haj [2 naea][nmo] complex
+          float64  trial [2][nmo][naea] complex  (conj(Wavefun))
+          CSR      Vakbl [2 naea nmo]^2      (when has_vakbl)
+
+        with CSR = int32 nrows, ncols; int64 nnz; int32 rowIndex[nrows+1];
+        int32 cols[nnz]; float64 vals[nnz] complex.  The driver half-rotates Spvn
+        itself, as the miniapp's main does (miniafqmc_base.cpp:181-185)."""
+        def csr(f, m: CSR):
+            f.write(np.array([m.nrows, m.ncols], "<i4").tobytes())
+            f.write(np.array([m.nnz], "<i8").tobytes())
+            f.write(np.ascontiguousarray(m.rowIndex, "<i4").tobytes())
+            f.write(np.ascontiguousarray(m.cols, "<i4").tobytes())
+            f.write(np.ascontiguousarray(m.vals, "<c16").tobytes())
+        with open(path, "wb") as f:
+            f.write(INPUT_MAGIC)
+            f.write(np.array([self.N, self.n, self.n, self.nchol], "<i4").tobytes())
+            f.write(np.array([self.cfg.dt], "<f8").tobytes())
+            f.write(np.array([1 if self.Vakbl is not None else 0], "<i4").tobytes())
+            csr(f, self.Spvn)
+            for a in (self.Propg1, self.haj, self.trial):
+                f.write(np.ascontiguousarray(a, "<c16").tobytes())
+            if self.Vakbl is not None:
+                csr(f, self.Vakbl)
+
     def initial_walkers(self, nwalk: int):
         """W[nw][2][N][n] = conj(trialwfn) and W_data with weight 1
         (miniafqmc_base.cpp:222-236)."""
@@ -270,6 +306,39 @@ class System:
         Wd = np.zeros((nwalk, 8), np.complex128)
         Wd[:, 1] = 1.0
         return W, Wd
+
+
+def read_input(path: str) -> dict:
+    """The arrays of a `System.write_input` file (the driver binary's input)."""
+    buf = open(path, "rb").read()
+    pos = 0
+
+    def take(dtype, count):
+        nonlocal pos
+        a = np.frombuffer(buf, dtype, count, pos)
+        pos += a.nbytes
+        return a
+
+    def csr():
+        nr, nc = (int(v) for v in take("<i4", 2))
+        nnz = int(take("<i8", 1)[0])
+        return CSR(nr, nc, take("<i4", nr + 1).copy(), take("<i4", nnz).copy(),
+                   take("<c16", nnz).copy())
+
+    if buf[:8] != INPUT_MAGIC:
+        raise ValueError(f"{path}: not a driver input file")
+    pos = 8
+    nmo, naea, naeb, nchol = (int(v) for v in take("<i4", 4))
+    dt = float(take("<f8", 1)[0])
+    has_vakbl = int(take("<i4", 1)[0])
+    d = {"nmo": nmo, "naea": naea, "naeb": naeb, "nchol": nchol, "dt": dt, "Spvn": csr()}
+    d["Propg1"] = take("<c16", nmo * nmo).reshape(nmo, nmo).copy()
+    d["haj"] = take("<c16", 2 * naea * nmo).reshape(2 * naea, nmo).copy()
+    d["trial"] = take("<c16", 2 * nmo * naea).reshape(2, nmo, naea).copy()
+    d["Vakbl"] = csr() if has_vakbl else None
+    if pos != len(buf):
+        raise ValueError(f"{path}: {len(buf) - pos} trailing bytes")
+    return d
 
 
 def make_system(cfg: Config, build_vakbl: bool | None = None) -> System:

@@ -1,0 +1,183 @@
+"""The miniapp's driver program (`miniafqmc_b200/miniafqmc`, a C++ restatement of
+src/miniapps/miniafqmc_base.cpp:93-360 over the C ABI).
+
+On the host: the program built against the FP64 oracle behind the same ABI
+(`oracle/abi_shim.cpp`) prints, step by step, the energies of the Python driver
+(`miniafqmc_b200.driver.run`) on the oracle, to 1e-10 relative (the program half-rotates
+Spvn itself, as the miniapp's main does, so SpvnT and the Cholesky factors are formed in a
+different order than the Python system's: the last digits differ).  Covered: the
+transposed path with the two-body energy, the Cholesky energy, the `-t no` full-G path,
+and the input and option errors of the product binary.  The product binary on a GPU:
+`test_zzz_driver_program_gpu.py`."""
+import glob
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, system
+
+INCLUDE = os.path.join(ROOT, "include")
+
+
+def scipy_openblas():
+    import scipy
+    libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__), "..", "scipy.libs",
+                                  "libscipy_openblas*.so"))
+    return os.path.realpath(libs[0]) if libs else None
+
+
+@pytest.fixture(scope="module")
+def oracle_driver(tmp_path_factory):
+    """The driver program linked against the oracle behind the C ABI."""
+    if scipy_openblas() is None:
+        pytest.skip("no scipy OpenBLAS library to resolve the oracle's LAPACK calls")
+    d = tmp_path_factory.mktemp("oracle_driver")
+    lib = str(d / "libafqmc_b200.so")
+    subprocess.check_call(["g++", "-O2", "-fopenmp", "-std=c++17", "-fPIC", "-shared",
+                           "-I", INCLUDE, os.path.join(ROOT, "oracle", "afqmc_oracle.cpp"),
+                           os.path.join(ROOT, "oracle", "abi_shim.cpp"), "-ldl", "-o", lib])
+    from miniafqmc_b200 import build
+    exe = str(d / "miniafqmc")
+    subprocess.check_call(build.driver_command(str(d), exe))
+    return exe
+
+
+@pytest.fixture(scope="module")
+def c1_input(tmp_path_factory):
+    s = system("C1")
+    path = str(tmp_path_factory.mktemp("c1") / "c1.bin")
+    s.write_input(path)
+    return s, path
+
+
+def run_program(exe, args, **kw):
+    env = dict(os.environ, AFQ_ORACLE_LAPACK=scipy_openblas() or "",
+               AFQ_ORACLE_LAPACK_PREFIX="scipy_", OMP_NUM_THREADS="4",
+               OPENBLAS_NUM_THREADS="1")
+    return subprocess.run([exe, *args], capture_output=True, text=True, timeout=900, env=env,
+                          **kw)
+
+
+def step_energies(stdout):
+    """The `step   Eav` lines after the `# Step   Energy` header."""
+    out, on = [], False
+    for ln in stdout.splitlines():
+        if ln.startswith("# Step"):
+            on = True
+            continue
+        m = re.match(r"^(\d+)\s+(\S+)$", ln.strip()) if on else None
+        if m:
+            out.append((int(m.group(1)), float(m.group(2))))
+        elif on and ln.strip() == "":
+            if out:
+                break
+    return out
+
+
+def python_energies(s, nwalk, nsteps, nsub, northo, seed, mode, full_g=False):
+    from oracle import oracle as O
+    o = O.Oracle(s, nwalk)
+    if not full_g:
+        from miniafqmc_b200 import driver
+        return driver.run(o, nsteps, nsub, northo, seed, energy_mode=mode,
+                          graph=False).energies[1:]
+    o.calculate_mixed_density_matrix()
+    energies, step_tot = [], 0
+    for _ in range(nsteps):
+        for _ in range(nsub):
+            o.calculate_mixed_density_matrix_full()
+            o.get_vbias_full()
+            o.sigma(seed, step_tot)
+            o.get_vHS()
+            o.propagate()
+            o.calculate_overlaps(save_old=True)
+            o.update_weights()
+            if step_tot > 0 and step_tot % northo == 0:
+                o.orthogonalize()
+                o.calculate_overlaps(save_old=False)
+            step_tot += 1
+        o.calculate_mixed_density_matrix()
+        energies.append(o.calculate_energy(mode))
+    return energies
+
+
+@pytest.mark.parametrize("flags,mode,full_g", [
+    ([], "vakbl", False),
+    (["-e", "chol", "-g"], "chol", False),
+    (["-t", "no"], "vakbl", True),
+])
+def test_program_on_the_oracle_matches_the_python_driver(oracle_driver, c1_input, flags,
+                                                         mode, full_g):
+    s, path = c1_input
+    nwalk, nsteps, nsub, northo, seed = 4, 3, 4, 5, 11
+    out = run_program(oracle_driver, ["-f", path, "-w", str(nwalk), "-i", str(nsteps), "-s",
+                                      str(nsub), "-o", str(northo), "-r", str(seed),
+                                      "-P", "17", *flags])
+    assert out.returncode == 0, out.stderr
+    got = step_energies(out.stdout)
+    assert [k for k, _ in got] == list(range(nsteps))
+    want = python_energies(s, nwalk, nsteps, nsub, northo, seed, mode, full_g)
+    for (_, e), w in zip(got, want):
+        assert abs(e - w) <= 1e-10 * abs(w), (e, w)
+    assert "    NMO: 64" in out.stdout and "    nwalk: 4" in out.stdout
+
+
+def test_input_file_round_trip(c1_input):
+    from miniafqmc_b200.synthetic import read_input
+    s, path = c1_input
+    d = read_input(path)
+    assert (d["nmo"], d["naea"], d["naeb"], d["nchol"], d["dt"]) == (s.N, s.n, s.n, s.nchol,
+                                                                      s.cfg.dt)
+    for k in ("rowIndex", "cols", "vals"):
+        assert np.array_equal(getattr(d["Spvn"], k), getattr(s.Spvn, k))
+        assert np.array_equal(getattr(d["Vakbl"], k), getattr(s.Vakbl, k))
+    for k in ("Propg1", "haj", "trial"):
+        assert np.array_equal(d[k], getattr(s, k))
+
+
+def product_binary():
+    """The driver program linked against the in-tree library (relinked when stale)."""
+    from miniafqmc_b200 import build
+    if os.path.exists(build.LIB):
+        return build.build_driver()
+    build.build()
+    return build.DRIVER
+
+
+def test_program_help_and_option_errors():
+    exe = product_binary()
+    h = subprocess.run([exe, "-h"], capture_output=True, text=True, timeout=60)
+    assert h.returncode == 1 and "-t                If set to no" in h.stdout
+    for bad in (["-p", "half"], ["-e", "none"], ["-w", "0"], ["-t", "no", "-p", "mixed"],
+                ["-x"]):
+        r = subprocess.run([exe, *bad], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 1 and "bad option" in r.stderr, bad
+
+
+def test_program_input_errors(tmp_path, c1_input):
+    exe = product_binary()
+    s, path = c1_input
+    blob = open(path, "rb").read()
+    cases = {
+        "missing": (str(tmp_path / "none.bin"), "cannot open"),
+        "magic": (b"NOTAFILE" + blob[8:], "not a driver input file"),
+        "truncated": (blob[: len(blob) // 2], "truncated"),
+        "trailing": (blob + b"\0" * 8, "trailing bytes"),
+    }
+    for name, (content, msg) in cases.items():
+        if isinstance(content, bytes):
+            p = tmp_path / f"{name}.bin"
+            p.write_bytes(content)
+            content = str(p)
+        r = subprocess.run([exe, "-f", content], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 1 and msg in r.stderr, (name, r.stderr)
+    # the two-body energy needs the two-body matrix
+    s2 = system("C2", with_vakbl=False)
+    p2 = str(tmp_path / "c2.bin")
+    s2.write_input(p2)
+    r = subprocess.run([exe, "-f", p2, "-e", "vakbl"], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode == 1 and "needs the two-body matrix" in r.stderr
