@@ -24,7 +24,10 @@
 // `-t no` dereferences a null optarg); the auxiliary fields come from the library's
 // Philox4x32-10 stream keyed by -r instead of mt19937; -p, -e, -g, -d, -T, -P choose the
 // numerical form, energy evaluation, graph substeps, device, Taylor order and printed
-// digits.  Errors print the library's message and exit with status 1.
+// digits; -c writes a checkpoint (walkers, W_data, Eshift, seed and step counters) after
+// the last step and -R resumes from one: the fields are counter-based, so a resumed run
+// repeats the uninterrupted one exactly (the reference has no checkpoint).  Errors print
+// the library's message and exit with status 1.
 #include <getopt.h>
 
 #include <chrono>
@@ -171,6 +174,72 @@ bool read_input(const std::string& path, Input& in, std::string* err) {
   return true;
 }
 
+// Checkpoint: everything a substep reads besides the Hamiltonian.  Little-endian binary:
+//   char[8] "AFQCKP01"; int32 nmo, naea, nwalk, precision; int64 steps, step_tot;
+//   uint64 seed; float64 eshift; float64 W[nwalk][2][nmo][naea] complex;
+//   float64 W_data[nwalk][8] complex.
+struct Checkpoint {
+  int32_t nmo = 0, naea = 0, nwalk = 0, precision = 0;
+  int64_t steps = 0, step_tot = 0;
+  uint64_t seed = 0;
+  double eshift = 0.0;
+  std::vector<double> W, Wd;
+};
+
+bool write_checkpoint(const std::string& path, const Checkpoint& c, std::string* err) {
+  std::ofstream f(path, std::ios::binary);
+  auto put = [&](const void* p, size_t bytes) {
+    f.write(static_cast<const char*>(p), (std::streamsize)bytes);
+  };
+  put("AFQCKP01", 8);
+  const int32_t dims[4] = {c.nmo, c.naea, c.nwalk, c.precision};
+  const int64_t steps[2] = {c.steps, c.step_tot};
+  put(dims, sizeof dims);
+  put(steps, sizeof steps);
+  put(&c.seed, sizeof c.seed);
+  put(&c.eshift, sizeof c.eshift);
+  put(c.W.data(), sizeof(double) * c.W.size());
+  put(c.Wd.data(), sizeof(double) * c.Wd.size());
+  f.close();
+  if (!f) *err = "cannot write " + path;
+  return (bool)f;
+}
+
+bool read_checkpoint(const std::string& path, Checkpoint& c, std::string* err) {
+  Reader r(path);
+  if (!r.ok()) {
+    *err = "cannot open " + path;
+    return false;
+  }
+  char magic[8];
+  int32_t dims[4];
+  int64_t steps[2];
+  if (!r.read(magic, 8) || std::memcmp(magic, "AFQCKP01", 8) != 0) {
+    *err = path + ": not a checkpoint file (magic AFQCKP01)";
+    return false;
+  }
+  if (!r.read(dims, 4) || !r.read(steps, 2) || !r.read(&c.seed, 1) || !r.read(&c.eshift, 1)) {
+    *err = path + ": truncated header";
+    return false;
+  }
+  c.nmo = dims[0];
+  c.naea = dims[1];
+  c.nwalk = dims[2];
+  c.precision = dims[3];
+  c.steps = steps[0];
+  c.step_tot = steps[1];
+  if (c.nmo <= 0 || c.naea <= 0 || c.nwalk <= 0 || c.steps < 0 || c.step_tot < 0) {
+    *err = path + ": bad header";
+    return false;
+  }
+  if (!r.vec(c.W, 4LL * c.nwalk * c.nmo * c.naea) || !r.vec(c.Wd, 16LL * c.nwalk) ||
+      r.left() != 0) {
+    *err = path + ": walker arrays do not match the header";
+    return false;
+  }
+  return true;
+}
+
 void print_help() {
   std::printf("miniafqmc - QMCPACK AFQMC miniapp on the B200 library\n\n");
   std::printf("Options:\n");
@@ -191,11 +260,13 @@ void print_help() {
   std::printf("-r                Seed of the auxiliary-field stream (default 11)\n");
   std::printf("-T                Taylor order of exp(vHS) (default 6)\n");
   std::printf("-P                Significant digits of the printed energies (default 6)\n");
+  std::printf("-c                Write a checkpoint file after the last step\n");
+  std::printf("-R                Resume from a checkpoint file (-i counts the steps before it)\n");
 }
 
 struct Options {
   int nsteps = 10, nsubsteps = 10, nwalk = 16, northo = 10;
-  std::string init_file = "afqmc.bin";
+  std::string init_file = "afqmc.bin", checkpoint_out, resume_from;
   bool transposed = true, verbose = false, graph = false;
   int precision = AFQ_PREC_FP64;
   int energy = -1;   // -1: vakbl when present, else chol
@@ -206,7 +277,7 @@ struct Options {
 // parse; returns 0 to run, 1 after -h (the reference's exit status), 2 on a bad flag
 int parse(int argc, char** argv, Options& o) {
   int opt;
-  while ((opt = getopt(argc, argv, "hvgt:i:s:w:o:f:p:e:d:r:T:P:")) != -1) {
+  while ((opt = getopt(argc, argv, "hvgt:i:s:w:o:f:p:e:d:r:T:P:c:R:")) != -1) {
     switch (opt) {
       case 'h': print_help(); return 1;
       case 'i': o.nsteps = std::atoi(optarg); break;
@@ -232,6 +303,8 @@ int parse(int argc, char** argv, Options& o) {
       case 'r': o.seed = std::strtoull(optarg, nullptr, 10); break;
       case 'T': o.taylor = std::atoi(optarg); break;
       case 'P': o.digits = std::atoi(optarg); break;
+      case 'c': o.checkpoint_out = optarg; break;
+      case 'R': o.resume_from = optarg; break;
       default: return 2;
     }
   }
@@ -267,6 +340,21 @@ int run(const Options& o) {
   }
   const int N = in.nmo, n = in.naea, nchol = in.nchol;
   const long long NAK = 2LL * n * N;
+  Checkpoint resume;
+  uint64_t seed = o.seed;
+  if (!o.resume_from.empty()) {
+    if (!read_checkpoint(o.resume_from, resume, &err)) {
+      std::cerr << " Error: resume: " << err << std::endl;
+      return 1;
+    }
+    if (resume.nmo != N || resume.naea != n || resume.nwalk != o.nwalk) {
+      std::cerr << " Error: resume: the checkpoint holds " << resume.nwalk << " walkers of NMO "
+                << resume.nmo << ", NAEA " << resume.naea << "; this run has " << o.nwalk
+                << " of NMO " << N << ", NAEA " << n << std::endl;
+      return 1;
+    }
+    seed = resume.seed;   // the fields continue the checkpointed stream
+  }
   const int energy = o.energy >= 0 ? o.energy
                                    : (in.has_vakbl ? AFQ_ENERGY_VAKBL : AFQ_ENERGY_CHOLESKY);
   if (energy == AFQ_ENERGY_VAKBL && !in.has_vakbl) {
@@ -331,7 +419,11 @@ int run(const Options& o) {
             << (energy == AFQ_ENERGY_VAKBL ? "vakbl" : energy == AFQ_ENERGY_CV ? "cv" : "chol")
             << "\n"
             << "    graph substeps: " << o.graph << "\n"
-            << "    device: " << o.device << std::endl;
+            << "    device: " << o.device << "\n"
+            << "    seed: " << seed << std::endl;
+  if (!o.resume_from.empty())
+    std::cout << "    resumed after step " << resume.steps - 1 << " (substep " << resume.step_tot
+              << ") from " << o.resume_from << std::endl;
 
   afq_system_desc desc{N, in.naea, in.naeb, nchol, o.nwalk, in.dt, o.taylor, o.precision,
                        o.device};
@@ -351,7 +443,7 @@ int run(const Options& o) {
   Lhalf.clear();
   Lhalf.shrink_to_fit();
   if (energy == AFQ_ENERGY_CV &&
-      !check(afq_cv_configure(h, 256, 1e-3, o.seed, 2000, 8), h, "afq_cv_configure"))
+      !check(afq_cv_configure(h, 256, 1e-3, seed, 2000, 8), h, "afq_cv_configure"))
     return 1;
 
   // walkers = conj(trial), weights 1 (miniafqmc_base.cpp:226-236)
@@ -365,7 +457,12 @@ int run(const Options& o) {
       }
       Wd[(size_t)w * 16 + 2] = 1.0;   // W_data[w][1] = 1
     }
-    if (!check(afq_set_walkers(h, W.data(), Wd.data()), h, "afq_set_walkers")) return 1;
+    const bool res = !o.resume_from.empty();
+    if (!check(afq_set_walkers(h, res ? resume.W.data() : W.data(),
+                               res ? resume.Wd.data() : Wd.data()),
+               h, "afq_set_walkers") ||
+        (res && !check(afq_set_eshift(h, resume.eshift), h, "afq_set_eshift")))
+      return 1;
   }
   if (!o.graph && !check(afq_profile(h, 1), h, "afq_profile")) return 1;
 
@@ -386,23 +483,24 @@ int run(const Options& o) {
   std::cout << "# Step   Energy   \n";
 
   const auto t0 = std::chrono::steady_clock::now();
-  for (int step = 0, step_tot = 0; step < o.nsteps; step++) {
+  int step = (int)resume.steps;
+  uint64_t step_tot = (uint64_t)resume.step_tot;
+  for (; step < o.nsteps; step++) {
     for (int sub = 0; sub < o.nsubsteps; sub++, step_tot++) {
       if (o.graph) {
-        if (!check(afq_substep(h, o.seed, (uint64_t)step_tot, o.northo), h, "substep"))
-          return 1;
+        if (!check(afq_substep(h, seed, step_tot, o.northo), h, "substep")) return 1;
         continue;
       }
       // 1. density matrix and bias potential; 2. X and hybrid weight; 3. vHS;
       // 4. propagation; 5. overlaps; 6. weights and Eshift (miniafqmc_base.cpp:255-328)
       if (!check(density_matrix(), h, "mixed density matrix") ||
           !check(o.transposed ? afq_vbias(h) : afq_vbias_full(h), h, "vbias") ||
-          !check(afq_sigma(h, o.seed, (uint64_t)step_tot), h, "sigma") ||
+          !check(afq_sigma(h, seed, step_tot), h, "sigma") ||
           !check(afq_vhs(h), h, "vHS") || !check(afq_propagate(h), h, "propagate") ||
           !check(afq_overlaps(h, 1), h, "overlaps") ||
           !check(afq_update_weights(h), h, "weights"))
         return 1;
-      if (step_tot > 0 && step_tot % o.northo == 0) {   // miniafqmc_base.cpp:330-337
+      if (step_tot > 0 && step_tot % (uint64_t)o.northo == 0) {   // miniafqmc_base.cpp:330-337
         if (!check(afq_orthogonalize(h), h, "orthogonalize") ||
             !check(afq_overlaps(h, 0), h, "overlaps"))
           return 1;
@@ -414,6 +512,25 @@ int run(const Options& o) {
     std::cout << step << "   " << Eav << "\n";
   }
   if (!check(afq_synchronize(h), h, "synchronize")) return 1;
+  if (!o.checkpoint_out.empty()) {
+    Checkpoint c;
+    c.nmo = N;
+    c.naea = n;
+    c.nwalk = o.nwalk;
+    c.precision = o.precision;
+    c.steps = step;
+    c.step_tot = (int64_t)step_tot;
+    c.seed = seed;
+    c.W.resize((size_t)4 * o.nwalk * N * n);
+    c.Wd.resize((size_t)16 * o.nwalk);
+    if (!check(afq_get_walkers(h, c.W.data(), c.Wd.data()), h, "afq_get_walkers") ||
+        !check(afq_get_eshift(h, &c.eshift), h, "afq_get_eshift"))
+      return 1;
+    if (!write_checkpoint(o.checkpoint_out, c, &err)) {
+      std::cerr << " Error: checkpoint: " << err << std::endl;
+      return 1;
+    }
+  }
   const double total_s =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 

@@ -33,7 +33,9 @@ void orc_set_vakbl(orc_handle* h, int nrows, int ncols, const int* ri, const int
 void orc_set_dense(orc_handle* h, const double* P, const double* haj, const double* trial,
                    const double* Lh);
 void orc_set_walkers(orc_handle* h, const double* W, const double* Wd);
+void orc_get_walkers(const orc_handle* h, double* W, double* Wd);
 double orc_get_eshift(const orc_handle* h);
+void orc_set_eshift(orc_handle* h, double e);
 void orc_mixed_density_matrix(orc_handle* h);
 void orc_mixed_density_matrix_full(orc_handle* h);
 void orc_vbias(orc_handle* h);
@@ -183,6 +185,18 @@ afq_status afq_cv_configure(afq_handle* h, int, double, uint64_t, long long, int
 afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data) {
   if (!h || !W || !W_data) return fail(h, AFQ_ERR_ARG, "null walkers");
   orc_set_walkers(h->o, W, W_data);
+  return AFQ_OK;
+}
+
+afq_status afq_get_walkers(afq_handle* h, double* W, double* W_data) {
+  if (!h) return AFQ_ERR_ARG;
+  orc_get_walkers(h->o, W, W_data);
+  return AFQ_OK;
+}
+
+afq_status afq_set_eshift(afq_handle* h, double eshift) {
+  if (!h) return AFQ_ERR_ARG;
+  orc_set_eshift(h->o, eshift);
   return AFQ_OK;
 }
 

@@ -7,7 +7,7 @@ On the host: the program built against the FP64 oracle behind the same ABI
 Spvn itself, as the miniapp's main does, so SpvnT and the Cholesky factors are formed in a
 different order than the Python system's: the last digits differ).  Covered: the
 transposed path with the two-body energy, the Cholesky energy, the `-t no` full-G path,
-and the input and option errors of the product binary.  The product binary on a GPU:
+checkpoint and exact resume, and the input and option errors of the product binary.  The product binary on a GPU:
 `test_zzz_driver_program_gpu.py`."""
 import glob
 import os
@@ -123,6 +123,35 @@ def test_program_on_the_oracle_matches_the_python_driver(oracle_driver, c1_input
     for (_, e), w in zip(got, want):
         assert abs(e - w) <= 1e-10 * abs(w), (e, w)
     assert "    NMO: 64" in out.stdout and "    nwalk: 4" in out.stdout
+
+
+@pytest.mark.parametrize("flags", [[], ["-g"]])
+def test_checkpoint_resume_repeats_the_uninterrupted_run(oracle_driver, c1_input, tmp_path,
+                                                         flags):
+    """-c after two of four steps, then -R: the resumed steps print the energies of the
+    run that was never interrupted, to the last digit (the fields are counter-based)."""
+    s, path = c1_input
+    base = ["-f", path, "-w", "4", "-s", "3", "-o", "4", "-r", "5", "-P", "17", *flags]
+    full = run_program(oracle_driver, base + ["-i", "4"])
+    assert full.returncode == 0, full.stderr
+    ck = str(tmp_path / "ck.bin")
+    first = run_program(oracle_driver, base + ["-i", "2", "-c", ck])
+    assert first.returncode == 0, first.stderr
+    # a different -r is ignored on resume: the checkpoint's seed continues the stream
+    rest = run_program(oracle_driver, base[:-4] + ["-r", "99", "-P", "17", *flags,
+                                                   "-i", "4", "-R", ck])
+    assert rest.returncode == 0, rest.stderr
+    want = step_energies(full.stdout)
+    assert step_energies(first.stdout) == want[:2]
+    assert step_energies(rest.stdout) == want[2:]
+    assert "resumed after step 1 (substep 6)" in rest.stdout
+    # the checkpoint must match the run
+    bad = run_program(oracle_driver, base + ["-i", "4", "-w", "8", "-R", ck])
+    assert bad.returncode == 1 and "the checkpoint holds 4 walkers" in bad.stderr
+    junk = tmp_path / "junk.bin"
+    junk.write_bytes(b"AFQCKP01" + b"\0" * 12)
+    bad = run_program(oracle_driver, base + ["-i", "4", "-R", str(junk)])
+    assert bad.returncode == 1 and "truncated header" in bad.stderr
 
 
 def test_input_file_round_trip(c1_input):
