@@ -10,6 +10,8 @@
 #include <map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/afqmc_b200.h"
 #include "afq_cv.h"
 #include "afq_kernels.h"
@@ -200,9 +202,35 @@ cudaError_t collect_stage_times(afq_handle* h) {
 
 // Runs one stage body, counting its kernel launches and, with profiling on (and outside
 // stream capture), bracketing it with CUDA events on the handle's stream.
+// NVTX range per stage call, in the library's own domain "afqmc_b200" (a profiler shows
+// the reference's stage names on the timeline; the caller's ranges in the default domain
+// keep their own stack).  Host-only and without effect unless a tool is attached.
+struct StageRange {
+  explicit StageRange(int stage) {
+    static nvtxDomainHandle_t dom = nvtxDomainCreateA("afqmc_b200");
+    static const char* const names[AFQ_NSTAGES] = {
+        "mixed density matrix", "bias potential", "sigma", "H-S potential", "propagation",
+        "overlap", "weights", "orthogonalization", "local energy"};
+    nvtxEventAttributes_t a{};
+    a.version = NVTX_VERSION;
+    a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+    a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+    a.message.ascii = (stage >= 0 && stage < AFQ_NSTAGES) ? names[stage] : "stage";
+    dom_ = dom;
+    nvtxDomainRangePushEx(dom_, &a);
+  }
+  ~StageRange() { nvtxDomainRangePop(dom_); }
+  StageRange(const StageRange&) = delete;
+  StageRange& operator=(const StageRange&) = delete;
+
+ private:
+  nvtxDomainHandle_t dom_;
+};
+
 template <class F>
 cudaError_t staged(afq_handle* h, int stage, int nlaunch, F&& body) {
   (h->launch_sink ? h->launch_sink : h->stage_launches)[stage] += nlaunch;
+  StageRange range(stage);
   if (!h->profiling || h->capturing) return body();
   if (h->nrec == 4096) {
     cudaError_t e = collect_stage_times(h);
