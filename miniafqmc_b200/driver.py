@@ -14,6 +14,10 @@ from __future__ import annotations
 import dataclasses
 from typing import Callable, Optional
 
+import numpy as np
+
+CHECKPOINT_MAGIC = b"AFQCKP01"
+
 
 @dataclasses.dataclass
 class Comm:
@@ -59,17 +63,61 @@ def substep(engine, seed: int, step_tot: int, northo: int, comm: Optional[Comm] 
         engine.calculate_overlaps(save_old=False)
 
 
+def write_checkpoint(path: str, engine, steps: int, step_tot: int, seed: int,
+                     precision: int = 0) -> None:
+    """Everything a substep reads besides the Hamiltonian, in the driver program's layout
+    (`miniafqmc_b200/app/miniafqmc.cpp`, so either driver resumes the other's runs):
+    "AFQCKP01"; int32 nmo, naea, nwalk, precision; int64 steps, step_tot; uint64 seed;
+    float64 eshift; complex128 W[nwalk][2][nmo][naea]; complex128 W_data[nwalk][8]."""
+    W, Wd = engine.get_walkers()
+    nwalk, _, nmo, naea = W.shape
+    with open(path, "wb") as f:
+        f.write(CHECKPOINT_MAGIC)
+        f.write(np.array([nmo, naea, nwalk, precision], "<i4").tobytes())
+        f.write(np.array([steps, step_tot], "<i8").tobytes())
+        f.write(np.array([seed], "<u8").tobytes())
+        f.write(np.array([engine.eshift], "<f8").tobytes())
+        f.write(np.ascontiguousarray(W, "<c16").tobytes())
+        f.write(np.ascontiguousarray(Wd, "<c16").tobytes())
+
+
+def read_checkpoint(path: str) -> dict:
+    buf = open(path, "rb").read()
+    if buf[:8] != CHECKPOINT_MAGIC or len(buf) < 48:
+        raise ValueError(f"{path}: not a checkpoint file")
+    nmo, naea, nwalk, precision = (int(v) for v in np.frombuffer(buf, "<i4", 4, 8))
+    steps, step_tot = (int(v) for v in np.frombuffer(buf, "<i8", 2, 24))
+    seed = int(np.frombuffer(buf, "<u8", 1, 40)[0])
+    eshift = float(np.frombuffer(buf, "<f8", 1, 48)[0])
+    nW, nD = nwalk * 2 * nmo * naea, nwalk * 8
+    if len(buf) != 56 + 16 * (nW + nD):
+        raise ValueError(f"{path}: walker arrays do not match the header")
+    W = np.frombuffer(buf, "<c16", nW, 56).reshape(nwalk, 2, nmo, naea).copy()
+    Wd = np.frombuffer(buf, "<c16", nD, 56 + 16 * nW).reshape(nwalk, 8).copy()
+    return {"nmo": nmo, "naea": naea, "nwalk": nwalk, "precision": precision,
+            "steps": steps, "step_tot": step_tot, "seed": seed, "eshift": eshift,
+            "W": W, "W_data": Wd}
+
+
 def run(engine, nsteps: int, nsubsteps: int, northo: int, seed: int,
         energy_mode: str = "auto", comm: Optional[Comm] = None, graph: bool = True,
-        on_energy: Optional[Callable] = None) -> RunResult:
+        on_energy: Optional[Callable] = None, resume: Optional[dict] = None,
+        checkpoint: Optional[str] = None) -> RunResult:
     """nsteps outer steps of nsubsteps propagation substeps, energy after each outer
-    step (miniafqmc_base.cpp:249-349); the initial DM + energy (:239-240) included."""
+    step (miniafqmc_base.cpp:249-349); the initial DM + energy (:239-240) included.
+    `resume` (a `read_checkpoint` dict) restores the walkers, Eshift, seed and step
+    counters and runs the steps from there up to nsteps; `checkpoint` writes one after
+    the last step (single-ensemble runs)."""
     if comm is not None:
         engine.set_walker_offset(comm.offset, comm.nwalk_global)
+    step0 = step_tot = 0
+    if resume is not None:
+        engine.set_walkers(resume["W"], resume["W_data"])
+        engine.eshift = resume["eshift"]
+        step0, step_tot, seed = resume["steps"], resume["step_tot"], resume["seed"]
     engine.calculate_mixed_density_matrix()
     energies = [energy(engine, energy_mode, comm)]
-    step_tot = 0
-    for step in range(nsteps):
+    for step in range(step0, nsteps):
         for _ in range(nsubsteps):
             substep(engine, seed, step_tot, northo, comm, graph)
             step_tot += 1
@@ -78,4 +126,6 @@ def run(engine, nsteps: int, nsubsteps: int, northo: int, seed: int,
         energies.append(e)
         if on_energy is not None:
             on_energy(step, e)
+    if checkpoint is not None:
+        write_checkpoint(checkpoint, engine, max(nsteps, step0), step_tot, seed)
     return RunResult(energies, nsteps, step_tot)

@@ -154,6 +154,43 @@ def test_checkpoint_resume_repeats_the_uninterrupted_run(oracle_driver, c1_input
     assert bad.returncode == 1 and "truncated header" in bad.stderr
 
 
+def test_python_driver_resume_and_checkpoints_shared_with_the_program(oracle_driver, c1_input,
+                                                                      tmp_path):
+    """driver.run writes and resumes the program's checkpoint layout: its own resumed steps
+    repeat its uninterrupted run exactly, and a checkpoint of either driver continues in
+    the other with the other's uninterrupted energies (1e-10: the two half-rotate Spvn in
+    different orders)."""
+    from miniafqmc_b200 import driver
+    from oracle import oracle as O
+    s, path = c1_input
+    nwalk, nsub, northo, seed = 4, 3, 4, 5
+    full = driver.run(O.Oracle(s, nwalk), 4, nsub, northo, seed, "vakbl", graph=False).energies
+    ck = str(tmp_path / "py.bin")
+    driver.run(O.Oracle(s, nwalk), 2, nsub, northo, seed, "vakbl", graph=False, checkpoint=ck)
+    r = driver.read_checkpoint(ck)
+    assert (r["steps"], r["step_tot"], r["seed"], r["nwalk"]) == (2, 2 * nsub, seed, nwalk)
+    rest = driver.run(O.Oracle(s, nwalk), 4, nsub, northo, 999, "vakbl", graph=False,
+                      resume=r).energies
+    assert rest[1:] == full[3:]
+    # the Python checkpoint continued by the program
+    base = ["-f", path, "-w", str(nwalk), "-s", str(nsub), "-o", str(northo), "-P", "17"]
+    out = run_program(oracle_driver, base + ["-i", "4", "-R", ck])
+    assert out.returncode == 0, out.stderr
+    got = step_energies(out.stdout)
+    assert [k for k, _ in got] == [2, 3]
+    for (_, e), w in zip(got, full[3:]):
+        assert abs(e - w) <= 1e-10 * abs(w)
+    # the program's checkpoint continued by the Python driver
+    ckc = str(tmp_path / "cpp.bin")
+    prog_full = run_program(oracle_driver, base + ["-r", str(seed), "-i", "4"])
+    first = run_program(oracle_driver, base + ["-r", str(seed), "-i", "2", "-c", ckc])
+    assert prog_full.returncode == 0 and first.returncode == 0
+    cont = driver.run(O.Oracle(s, nwalk), 4, nsub, northo, 0, "vakbl", graph=False,
+                      resume=driver.read_checkpoint(ckc)).energies[1:]
+    for (_, w), e in zip(step_energies(prog_full.stdout)[2:], cont):
+        assert abs(e - w) <= 1e-10 * abs(w)
+
+
 def test_input_file_round_trip(c1_input):
     from miniafqmc_b200.synthetic import read_input
     s, path = c1_input
