@@ -40,6 +40,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -570,5 +571,10 @@ int main(int argc, char** argv) {
     std::cerr << " Error: bad option (see -h)" << std::endl;
     return 1;
   }
-  return run(o);
+  try {
+    return run(o);
+  } catch (const std::bad_alloc&) {
+    std::cerr << " Error: out of host memory (input arrays or walkers too large)" << std::endl;
+    return 1;
+  }
 }
