@@ -63,16 +63,10 @@ class CsrZ(ctypes.Structure):
 _LIB = None
 
 
-def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
-    """Loads the CUDA library; raises if it has not been built."""
-    global _LIB
-    if _LIB is not None:
-        return _LIB
-    if not os.path.exists(path):
-        raise RuntimeError(f"{path} is missing: build it with `python -m miniafqmc_b200.build`")
-    lib = ctypes.CDLL(path)
+def signatures() -> dict:
+    """ctypes (argtypes, restype) of every entry point of include/afqmc_b200.h."""
     P, I, D, U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_uint64
-    sigs = {
+    return {
         "afq_create": ([P, P], I), "afq_destroy": ([P], None),
         "afq_status_string": ([I], ctypes.c_char_p), "afq_last_error": ([P], ctypes.c_char_p),
         "afq_set_hamiltonian": ([P, P, P, P, P, P, P, P], I),
@@ -103,7 +97,17 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "afq_population_control": ([P, U64, U64], I),
         "afq_mixed_density_matrix_full": ([P], I), "afq_vbias_full": ([P], I),
     }
-    for name, (args, res) in sigs.items():
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the CUDA library; raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m miniafqmc_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, (args, res) in signatures().items():
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = res

@@ -75,3 +75,52 @@ def test_halfrotate_rejects_bad_arguments_without_gpu():
     cols = np.zeros(1, np.int32)
     assert lib.afq_halfrotate(*ok, None, cols.ctypes.data, None, None) == 1        # no rowIndex
 
+
+
+def _header_prototypes():
+    """{name: (return type, [parameter types])} of the header's function declarations."""
+    import re
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+    out = {}
+    for m in re.finditer(r"([A-Za-z_][\w\s\*]*?)\b(afq_\w+)\s*\(([^()]*)\)\s*;", text):
+        ret, name, params = " ".join(m.group(1).split()), m.group(2), m.group(3).strip()
+        plist = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+        types = []
+        for p in plist:
+            words = p.replace("*", " * ").split()
+            if "*" in words:
+                types.append("*")
+            else:   # drop the parameter name
+                types.append(" ".join(w for w in words[:-1] if w != "const"))
+        out[name] = (ret.replace("typedef", "").strip(), types)
+    return out
+
+
+def test_python_signatures_match_header_prototypes():
+    """Every ctypes declaration has the header prototype's arity and type classes
+    (pointer / int or enum / uint64_t / long long / double / float)."""
+    import ctypes
+    from miniafqmc_b200.afqmc import signatures
+    protos = _header_prototypes()
+    enums = {"afq_status", "int", "afq_precision", "afq_energy_mode", "afq_buffer", "afq_stage"}
+
+    def cls_of(c):
+        if c in ("*",):
+            return ctypes.c_void_p
+        if c in enums:
+            return ctypes.c_int
+        return {"uint64_t": ctypes.c_uint64, "long long": ctypes.c_longlong,
+                "double": ctypes.c_double, "float": ctypes.c_float}[c]
+
+    sigs = signatures()
+    assert set(sigs) == set(protos)
+    for name, (args, res) in sigs.items():
+        ret, params = protos[name]
+        assert len(args) == len(params), name
+        for a, p in zip(args, params):
+            assert a == cls_of(p), (name, p, a)
+        want = {"void": None, "const char *": ctypes.c_char_p, "const char*": ctypes.c_char_p,
+                "afq_status": ctypes.c_int, "long long": ctypes.c_longlong}[ret]
+        assert res == want, (name, ret, res)
