@@ -124,3 +124,42 @@ def test_python_signatures_match_header_prototypes():
         want = {"void": None, "const char *": ctypes.c_char_p, "const char*": ctypes.c_char_p,
                 "afq_status": ctypes.c_int, "long long": ctypes.c_longlong}[ret]
         assert res == want, (name, ret, res)
+
+
+def _header_enum_values():
+    """{enumerator: value} of the header's enums (explicit values or running count)."""
+    import re
+    text = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    vals = {}
+    for body in re.findall(r"typedef\s+enum\s*\{(.*?)\}", text, flags=re.S):
+        nxt = 0
+        for item in body.split(","):
+            item = item.strip()
+            if not item:
+                continue
+            name, _, v = item.partition("=")
+            nxt = int(v.strip()) if v.strip() else nxt
+            vals[name.strip()] = nxt
+            nxt += 1
+    return vals
+
+
+def test_python_constants_match_header_enums():
+    """Precision, energy-mode, buffer and stage numbering of the Python binding equal the
+    header's enums."""
+    from miniafqmc_b200 import afqmc as A
+    e = _header_enum_values()
+    assert (A.AFQ_PREC_FP64, A.AFQ_PREC_MIXED) == (e["AFQ_PREC_FP64"], e["AFQ_PREC_MIXED"])
+    assert (A.AFQ_ENERGY_VAKBL, A.AFQ_ENERGY_CHOLESKY, A.AFQ_ENERGY_CV) == (
+        e["AFQ_ENERGY_VAKBL"], e["AFQ_ENERGY_CHOLESKY"], e["AFQ_ENERGY_CV"])
+    header_buf = {"Gc": "AFQ_BUF_GC", "vbias": "AFQ_BUF_VBIAS", "X": "AFQ_BUF_X",
+                  "vHS": "AFQ_BUF_VHS", "hybridW": "AFQ_BUF_HYBRIDW", "xraw": "AFQ_BUF_XRAW",
+                  "info": "AFQ_BUF_INFO", "energy_parts": "AFQ_BUF_ENERGY_PARTS",
+                  "cv_pred": "AFQ_BUF_CV_PRED", "G_full": "AFQ_BUF_G_FULL"}
+    assert set(A.BUFFERS) == set(header_buf)
+    for k, v in A.BUFFERS.items():
+        assert v == e[header_buf[k]], k
+    stages = ["AFQ_STAGE_DM", "AFQ_STAGE_VBIAS", "AFQ_STAGE_SIGMA", "AFQ_STAGE_VHS",
+              "AFQ_STAGE_PROPAGATE", "AFQ_STAGE_OVERLAP", "AFQ_STAGE_WEIGHTS",
+              "AFQ_STAGE_ORTHO", "AFQ_STAGE_ENERGY"]
+    assert [e[s] for s in stages] == list(range(len(A.STAGES))) and e["AFQ_NSTAGES"] == 9
