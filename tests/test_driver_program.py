@@ -154,6 +154,25 @@ def test_checkpoint_resume_repeats_the_uninterrupted_run(oracle_driver, c1_input
     assert bad.returncode == 1 and "truncated header" in bad.stderr
 
 
+def test_program_on_a_complex_system_without_the_two_body_matrix(oracle_driver, tmp_path):
+    """Complex trial and Cholesky vectors, no Vakbl in the input: the program defaults to
+    the Cholesky energy and passes only the half-rotated factors."""
+    import dataclasses
+    from conftest import tiny_system
+    s = dataclasses.replace(tiny_system(), Vakbl=None)
+    path = str(tmp_path / "tiny.bin")
+    s.write_input(path)
+    out = run_program(oracle_driver, ["-f", path, "-w", "3", "-i", "3", "-s", "3", "-o", "2",
+                                      "-r", "7", "-P", "17"])
+    assert out.returncode == 0, out.stderr
+    assert "    energy: chol" in out.stdout
+    got = step_energies(out.stdout)
+    want = python_energies(s, 3, 3, 3, 2, 7, "chol")
+    assert len(got) == 3
+    for (_, e), w in zip(got, want):
+        assert abs(e - w) <= 1e-10 * abs(w), (e, w)
+
+
 def test_python_driver_resume_and_checkpoints_shared_with_the_program(oracle_driver, c1_input,
                                                                       tmp_path):
     """driver.run writes and resumes the program's checkpoint layout: its own resumed steps
