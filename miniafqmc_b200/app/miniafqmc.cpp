@@ -553,6 +553,12 @@ int run(const Options& o) {
                                                       : kStageNames[s])
                 << std::right << std::setw(10) << ms[s] << std::setw(12) << launches[s] << "\n";
   }
+  {   // throughput of the timed loop (substeps and the per-step energies)
+    const double ws = (double)o.nwalk * (double)(step_tot - (uint64_t)resume.step_tot);
+    std::cout << "\n  walker-steps/s: " << (total_s > 0.0 ? ws / total_s : 0.0) << "  ("
+              << (uint64_t)(step_tot - (uint64_t)resume.step_tot) << " substeps of "
+              << o.nwalk << " walkers in " << total_s << " s)\n";
+  }
   if (o.verbose) {
     double eshift = 0.0;
     if (check(afq_get_eshift(h, &eshift), h, "Eshift"))

@@ -123,6 +123,7 @@ def test_program_on_the_oracle_matches_the_python_driver(oracle_driver, c1_input
     for (_, e), w in zip(got, want):
         assert abs(e - w) <= 1e-10 * abs(w), (e, w)
     assert "    NMO: 64" in out.stdout and "    nwalk: 4" in out.stdout
+    assert f"({nsteps * nsub} substeps of {nwalk} walkers in" in out.stdout
 
 
 @pytest.mark.parametrize("flags", [[], ["-g"]])
