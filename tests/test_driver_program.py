@@ -238,7 +238,7 @@ def test_program_help_and_option_errors():
     h = subprocess.run([exe, "-h"], capture_output=True, text=True, timeout=60)
     assert h.returncode == 1 and "-t                If set to no" in h.stdout
     for bad in (["-p", "half"], ["-e", "none"], ["-w", "0"], ["-t", "no", "-p", "mixed"],
-                ["-x"]):
+                ["-t", "no", "-g"], ["-x"]):
         r = subprocess.run([exe, *bad], capture_output=True, text=True, timeout=60)
         assert r.returncode == 1 and "bad option" in r.stderr, bad
 
