@@ -256,7 +256,7 @@ void print_help() {
   std::printf("-e                vakbl | chol | cv: local energy from the two-body matrix, "
               "the Cholesky factors, or the learned control variate (default vakbl when the "
               "input has it, else chol)\n");
-  std::printf("-g                Run each substep as one CUDA-graph launch\n");
+  std::printf("-g                Run each substep as one CUDA-graph launch (not with -t no)\n");
   std::printf("-d                CUDA device (default 0)\n");
   std::printf("-r                Seed of the auxiliary-field stream (default 11)\n");
   std::printf("-T                Taylor order of exp(vHS) (default 6)\n");
