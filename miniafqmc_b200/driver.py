@@ -107,7 +107,8 @@ def run(engine, nsteps: int, nsubsteps: int, northo: int, seed: int,
     step (miniafqmc_base.cpp:249-349); the initial DM + energy (:239-240) included.
     `resume` (a `read_checkpoint` dict) restores the walkers, Eshift, seed and step
     counters and runs the steps from there up to nsteps; `checkpoint` writes one after
-    the last step (single-ensemble runs)."""
+    the last step.  With `comm`, every rank checkpoints and resumes its own walker block
+    (one file per rank; Eshift is the ensemble's on every rank)."""
     if comm is not None:
         engine.set_walker_offset(comm.offset, comm.nwalk_global)
     step0 = step_tot = 0

@@ -1,7 +1,7 @@
 """Walker sharding across ranks (gloo, world size 2, CPU): the sharded driver with the
 oracle as engine reproduces the unsharded ensemble -- same auxiliary fields (global
 Philox indexing), same Eshift (all-reduced sum of Re W_data[:,4]) and same weighted
-energy (all-reduced sums)."""
+energy (all-reduced sums); per-rank checkpoints resume the sharded run exactly."""
 import os
 import socket
 
@@ -42,7 +42,15 @@ def _worker(rank, world, port, out_dir):
         comm = driver.Comm(rank * per, NW, allreduce)
         res = driver.run(eng, STEPS, SUB, NORTHO, SEED, comm=comm, graph=False)
         W, Wd = eng.get_walkers()
-        np.savez(os.path.join(out_dir, f"r{rank}.npz"), W=W, Wd=Wd, E=np.array(res.energies))
+        # the same run with a per-rank checkpoint after the first step, resumed by a new
+        # engine on every rank
+        ck = os.path.join(out_dir, f"ck{rank}.bin")
+        driver.run(O.Oracle(s, per), 1, SUB, NORTHO, SEED, comm=comm, graph=False,
+                   checkpoint=ck)
+        res2 = driver.run(O.Oracle(s, per), STEPS, SUB, NORTHO, 0, comm=comm, graph=False,
+                          resume=driver.read_checkpoint(ck))
+        np.savez(os.path.join(out_dir, f"r{rank}.npz"), W=W, Wd=Wd, E=np.array(res.energies),
+                 E_resumed=np.array(res2.energies))
     finally:
         dist.destroy_process_group()
 
@@ -65,3 +73,5 @@ def test_sharded_run_matches_single_ensemble(tmp_path):
     np.testing.assert_allclose(Wd, Wdr, rtol=1e-11, atol=1e-12)
     for p in parts:
         np.testing.assert_allclose(p["E"], res.energies, rtol=1e-12)
+        # per-rank checkpoints resume the sharded run: the steps after it repeat it
+        assert np.array_equal(p["E_resumed"][1:], p["E"][2:])
