@@ -24,7 +24,8 @@
 // `-t no` dereferences a null optarg); the auxiliary fields come from the library's
 // Philox4x32-10 stream keyed by -r instead of mt19937; -p, -e, -g, -d, -T, -P choose the
 // numerical form, energy evaluation, graph substeps, device, Taylor order and printed
-// digits; -c writes a checkpoint (walkers, W_data, Eshift, seed and step counters) after
+// digits; -b k combs the population after every k-th step (where the reference leaves
+// branching out, :347); -c writes a checkpoint (walkers, W_data, Eshift, seed and step counters) after
 // the last step and -R resumes from one: the fields are counter-based, so a resumed run
 // repeats the uninterrupted one exactly (the reference has no checkpoint).  Errors print
 // the library's message and exit with status 1.
@@ -263,6 +264,8 @@ void print_help() {
   std::printf("-P                Significant digits of the printed energies (default 6)\n");
   std::printf("-c                Write a checkpoint file after the last step\n");
   std::printf("-R                Resume from a checkpoint file (-i counts the steps before it)\n");
+  std::printf("-b                Population control (comb) after every b-th step (default 0: "
+              "none)\n");
 }
 
 struct Options {
@@ -271,14 +274,14 @@ struct Options {
   bool transposed = true, verbose = false, graph = false;
   int precision = AFQ_PREC_FP64;
   int energy = -1;   // -1: vakbl when present, else chol
-  int device = 0, taylor = 6, digits = 6;
+  int device = 0, taylor = 6, digits = 6, branch = 0;
   uint64_t seed = 11;
 };
 
 // parse; returns 0 to run, 1 after -h (the reference's exit status), 2 on a bad flag
 int parse(int argc, char** argv, Options& o) {
   int opt;
-  while ((opt = getopt(argc, argv, "hvgt:i:s:w:o:f:p:e:d:r:T:P:c:R:")) != -1) {
+  while ((opt = getopt(argc, argv, "hvgt:i:s:w:o:f:p:e:d:r:T:P:c:R:b:")) != -1) {
     switch (opt) {
       case 'h': print_help(); return 1;
       case 'i': o.nsteps = std::atoi(optarg); break;
@@ -306,11 +309,12 @@ int parse(int argc, char** argv, Options& o) {
       case 'P': o.digits = std::atoi(optarg); break;
       case 'c': o.checkpoint_out = optarg; break;
       case 'R': o.resume_from = optarg; break;
+      case 'b': o.branch = std::atoi(optarg); break;
       default: return 2;
     }
   }
   if (o.nsteps < 0 || o.nsubsteps < 0 || o.nwalk <= 0 || o.northo <= 0 || o.taylor < 0 ||
-      o.digits <= 0 || o.digits > 17)
+      o.digits <= 0 || o.digits > 17 || o.branch < 0)
     return 2;
   // the full-G path is FP64 only and op by op (a graph substep is the transposed path)
   if (!o.transposed && (o.precision != AFQ_PREC_FP64 || o.graph)) return 2;
@@ -421,6 +425,7 @@ int run(const Options& o) {
             << (energy == AFQ_ENERGY_VAKBL ? "vakbl" : energy == AFQ_ENERGY_CV ? "cv" : "chol")
             << "\n"
             << "    graph substeps: " << o.graph << "\n"
+            << "    population control every: " << o.branch << " steps\n"
             << "    device: " << o.device << "\n"
             << "    seed: " << seed << std::endl;
   if (!o.resume_from.empty())
@@ -512,6 +517,10 @@ int run(const Options& o) {
         !check(afq_energy(h, energy, &Eav), h, "energy"))
       return 1;
     std::cout << step << "   " << Eav << "\n";
+    // "Branching in real code would happen here" (miniafqmc_base.cpp:347)
+    if (o.branch > 0 && (step + 1) % o.branch == 0 &&
+        !check(afq_population_control(h, seed, step_tot), h, "population control"))
+      return 1;
   }
   if (!check(afq_synchronize(h), h, "synchronize")) return 1;
   if (!o.checkpoint_out.empty()) {

@@ -102,13 +102,16 @@ def read_checkpoint(path: str) -> dict:
 def run(engine, nsteps: int, nsubsteps: int, northo: int, seed: int,
         energy_mode: str = "auto", comm: Optional[Comm] = None, graph: bool = True,
         on_energy: Optional[Callable] = None, resume: Optional[dict] = None,
-        checkpoint: Optional[str] = None) -> RunResult:
+        checkpoint: Optional[str] = None, branch_every: int = 0) -> RunResult:
     """nsteps outer steps of nsubsteps propagation substeps, energy after each outer
     step (miniafqmc_base.cpp:249-349); the initial DM + energy (:239-240) included.
     `resume` (a `read_checkpoint` dict) restores the walkers, Eshift, seed and step
     counters and runs the steps from there up to nsteps; `checkpoint` writes one after
     the last step.  With `comm`, every rank checkpoints and resumes its own walker block
-    (one file per rank; Eshift is the ensemble's on every rank)."""
+    (one file per rank; Eshift is the ensemble's on every rank).  `branch_every` = k > 0
+    runs population control (the comb, `population_control(seed, step_tot)`) after every
+    k-th step's energy, where the miniapp marks that branching belongs
+    (miniafqmc_base.cpp:347); sharded walker sets comb their own block."""
     if comm is not None:
         engine.set_walker_offset(comm.offset, comm.nwalk_global)
     step0 = step_tot = 0
@@ -127,6 +130,8 @@ def run(engine, nsteps: int, nsubsteps: int, northo: int, seed: int,
         energies.append(e)
         if on_energy is not None:
             on_energy(step, e)
+        if branch_every > 0 and (step + 1) % branch_every == 0:
+            engine.population_control(seed, step_tot)
     if checkpoint is not None:
         write_checkpoint(checkpoint, engine, max(nsteps, step0), step_tot, seed)
     return RunResult(energies, nsteps, step_tot)

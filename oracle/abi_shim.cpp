@@ -11,6 +11,7 @@
 // zunglq_}.  Calls outside the subset are not defined here (the link fails).
 #include <dlfcn.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <string>
@@ -48,6 +49,7 @@ void orc_update_weights(orc_handle* h);
 void orc_orthogonalize(orc_handle* h);
 double orc_energy_vakbl(orc_handle* h);
 double orc_energy_chol(orc_handle* h, double* parts);
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out);
 long long orc_halfrotate(int N, int n, int nchol, const int* ri, const int* ci,
                          const double* vals, const double* trial_a, const double* trial_b,
                          double cutoff, int* out_rowIndex, int* out_cols, double* out_vals);
@@ -197,6 +199,47 @@ afq_status afq_get_walkers(afq_handle* h, double* W, double* W_data) {
 afq_status afq_set_eshift(afq_handle* h, double eshift) {
   if (!h) return AFQ_ERR_ARG;
   orc_set_eshift(h->o, eshift);
+  return AFQ_OK;
+}
+
+// The comb of afq_population_control (oracle.comb restated in C++): prefix sums of
+// max(Re w, 0) in walker order, copy j = first walker with C_i > (j + u) T / nw, weight
+// T / nw; u from Philox4x32-10 at counter (0, 0, step) with key seed ^ 0x9E3779B97F4A7C15.
+afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step) {
+  if (!h) return AFQ_ERR_ARG;
+  const int nw = h->d.nwalk;
+  const size_t per = (size_t)2 * h->d.nmo * h->d.naea * 2;   // doubles per walker
+  std::vector<double> W(per * nw), Wd((size_t)16 * nw);
+  orc_get_walkers(h->o, W.data(), Wd.data());
+  std::vector<double> C(nw);
+  double T = 0.0;
+  int last = -1;
+  for (int i = 0; i < nw; i++) {
+    const double w = std::max(Wd[(size_t)16 * i + 2], 0.0);
+    T += w;
+    C[i] = T;
+    if (w > 0.0) last = i;
+  }
+  if (last < 0) return fail(h, AFQ_ERR_STATE, "population control: no walker has positive weight");
+  const uint64_t key = seed ^ 0x9E3779B97F4A7C15ull;
+  const uint32_t ctr[4] = {0, 0, (uint32_t)step, (uint32_t)(step >> 32)};
+  const uint32_t k[2] = {(uint32_t)key, (uint32_t)(key >> 32)};
+  uint32_t r[4];
+  orc_philox(ctr, k, r);
+  const double u =
+      (double)((((uint64_t)(r[0] >> 5)) << 26) | (uint64_t)(r[1] >> 6)) * (1.0 / 9007199254740992.0);
+  std::vector<double> Wn(per * nw), Wdn((size_t)16 * nw);
+  for (int j = 0; j < nw; j++) {
+    const double t = ((double)j + u) * T / nw;
+    int i = (int)(std::upper_bound(C.begin(), C.end(), t) - C.begin());
+    if (i >= nw) i = last;
+    std::copy(W.begin() + per * i, W.begin() + per * (i + 1), Wn.begin() + per * j);
+    std::copy(Wd.begin() + 16 * (size_t)i, Wd.begin() + 16 * (size_t)(i + 1),
+              Wdn.begin() + 16 * (size_t)j);
+    Wdn[(size_t)16 * j + 2] = T / nw;
+    Wdn[(size_t)16 * j + 3] = 0.0;
+  }
+  orc_set_walkers(h->o, Wn.data(), Wdn.data());
   return AFQ_OK;
 }
 

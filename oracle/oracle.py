@@ -232,6 +232,12 @@ class Oracle:
     def orthogonalize(self):
         self.lib.orc_orthogonalize(self.h)
 
+    def population_control(self, seed: int, step: int):
+        """The comb on this walker set (`comb` below), as afq_population_control."""
+        W, Wd = self.get_walkers()
+        Wn, Wdn, _ = comb(W, Wd, seed, step)
+        self.set_walkers(Wn, Wdn)
+
     def calculate_energy(self, mode: str = "auto", parts: bool = False):
         if mode == "auto":
             mode = "vakbl" if self.sys.Vakbl is not None else "chol"
@@ -286,3 +292,36 @@ def halfrotate(system, cutoff: float = 1e-6):
     vals = np.empty(nnz, np.complex128)
     lib.orc_halfrotate(*args, _p(rowIndex), _p(cols), _p(vals))
     return rowIndex, cols, vals
+
+
+# Population control by the comb (no reference counterpart: the reference leaves branching
+# out, miniafqmc_base.cpp:347).  Weights w_i = max(Re W_data[i][1], 0), total T, prefix sums
+# C_i in walker order; copy j takes the first walker with C_i > (j + u) T / nw and weight
+# T / nw.  u is one Philox4x32-10 uniform for (seed, step) on a key apart from the fields'.
+COMB_KEY = 0x9E3779B97F4A7C15
+
+
+def comb_uniform(seed: int, step: int) -> float:
+    key = (seed ^ COMB_KEY) & 0xFFFFFFFFFFFFFFFF
+    c = philox([0, 0, step & 0xFFFFFFFF, step >> 32], [key & 0xFFFFFFFF, key >> 32])
+    c = [int(x) for x in c]
+    return float(((c[0] >> 5) << 26) | (c[1] >> 6)) * (1.0 / 9007199254740992.0)
+
+
+def comb(W: np.ndarray, Wd: np.ndarray, seed: int, step: int):
+    """(new walkers, new walker data, parent index of each copy)."""
+    nw = Wd.shape[0]
+    w = np.maximum(Wd[:, 1].real, 0.0)
+    if not np.any(w > 0):
+        raise ValueError("population control: no walker has positive weight")
+    C = np.cumsum(w)
+    T = C[-1]
+    u = comb_uniform(seed, step)
+    t = (np.arange(nw, dtype=np.float64) + u) * T / nw
+    idx = np.searchsorted(C, t, side="right")
+    last = int(np.nonzero(w > 0)[0][-1])
+    idx = np.where(idx < nw, idx, last)
+    Wn, Wdn = W[idx].copy(), Wd[idx].copy()
+    Wdn[:, 1] = T / nw
+    return Wn, Wdn, idx
+

@@ -7,7 +7,8 @@ On the host: the program built against the FP64 oracle behind the same ABI
 Spvn itself, as the miniapp's main does, so SpvnT and the Cholesky factors are formed in a
 different order than the Python system's: the last digits differ).  Covered: the
 transposed path with the two-body energy, the Cholesky energy, the `-t no` full-G path,
-checkpoint and exact resume, and the input and option errors of the product binary.  The product binary on a GPU:
+checkpoint and exact resume, population control, and the input and option errors of the
+product binary.  The product binary on a GPU:
 `test_zzz_driver_program_gpu.py`."""
 import glob
 import os
@@ -174,6 +175,30 @@ def test_program_on_a_complex_system_without_the_two_body_matrix(oracle_driver, 
         assert abs(e - w) <= 1e-10 * abs(w), (e, w)
 
 
+def test_population_control_in_both_drivers(oracle_driver, c1_input):
+    """-b 1 / branch_every=1: the comb after every step's energy, in the program (through
+    afq_population_control) and in the Python driver on the oracle, gives the same energies;
+    the combed run differs from the uncombed one."""
+    from miniafqmc_b200 import driver
+    from oracle import oracle as O
+    s, path = c1_input
+    nwalk, nsteps, nsub, northo, seed = 6, 4, 3, 4, 13
+    out = run_program(oracle_driver, ["-f", path, "-w", str(nwalk), "-i", str(nsteps), "-s",
+                                      str(nsub), "-o", str(northo), "-r", str(seed), "-P", "17",
+                                      "-b", "1"])
+    assert out.returncode == 0, out.stderr
+    got = [e for _, e in step_energies(out.stdout)]
+    want = driver.run(O.Oracle(s, nwalk), nsteps, nsub, northo, seed, "vakbl", graph=False,
+                      branch_every=1).energies[1:]
+    plain = driver.run(O.Oracle(s, nwalk), nsteps, nsub, northo, seed, "vakbl",
+                       graph=False).energies[1:]
+    assert len(got) == nsteps
+    for e, w in zip(got, want):
+        assert abs(e - w) <= 1e-10 * abs(w), (e, w)
+    assert got[0] == pytest.approx(plain[0], rel=1e-10)   # the first comb follows step 0
+    assert any(abs(a - b) > 1e-9 * abs(b) for a, b in zip(want[1:], plain[1:]))
+
+
 def test_python_driver_resume_and_checkpoints_shared_with_the_program(oracle_driver, c1_input,
                                                                       tmp_path):
     """driver.run writes and resumes the program's checkpoint layout: its own resumed steps
@@ -238,7 +263,7 @@ def test_program_help_and_option_errors():
     h = subprocess.run([exe, "-h"], capture_output=True, text=True, timeout=60)
     assert h.returncode == 1 and "-t                If set to no" in h.stdout
     for bad in (["-p", "half"], ["-e", "none"], ["-w", "0"], ["-t", "no", "-p", "mixed"],
-                ["-t", "no", "-g"], ["-x"]):
+                ["-t", "no", "-g"], ["-b", "-1"], ["-x"]):
         r = subprocess.run([exe, *bad], capture_output=True, text=True, timeout=60)
         assert r.returncode == 1 and "bad option" in r.stderr, bad
 

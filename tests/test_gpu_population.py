@@ -1,8 +1,8 @@
 """Population control by the comb and exact resume from saved walkers (no reference
 counterpart: the reference leaves branching out, miniafqmc_base.cpp:347).
 
-The comb is restated here in numpy (prefix sums in walker order, teeth at
-(j + u) T / nw, first walker with C_i > t) with the same Philox uniform, and the GPU copies
+The comb is restated in the oracle (`oracle.comb`: prefix sums in walker order, teeth at
+(j + u) T / nw, first walker with C_i > t, the same Philox uniform), and the GPU copies
 must equal it exactly.  Resume: a run stopped after five substeps, its walkers, walker
 data and Eshift saved and loaded into a fresh handle, continues bit for bit like the run
 that never stopped (same seed and step counter)."""
@@ -14,29 +14,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-COMB_KEY = 0x9E3779B97F4A7C15
-
-
-def comb_uniform(seed, step):
-    key = seed ^ COMB_KEY
-    c = O.philox([0, 0, step & 0xFFFFFFFF, step >> 32], [key & 0xFFFFFFFF, key >> 32])
-    c = [int(x) for x in c]
-    return float(((c[0] >> 5) << 26) | (c[1] >> 6)) * (1.0 / 9007199254740992.0)
-
-
-def comb(W, Wd, seed, step):
-    nw = Wd.shape[0]
-    w = np.maximum(Wd[:, 1].real, 0.0)
-    C = np.cumsum(w)
-    T = C[-1]
-    u = comb_uniform(seed, step)
-    t = (np.arange(nw, dtype=np.float64) + u) * T / nw
-    idx = np.searchsorted(C, t, side="right")
-    last = int(np.nonzero(w > 0)[0][-1])
-    idx = np.where(idx < nw, idx, last)
-    Wn, Wdn = W[idx].copy(), Wd[idx].copy()
-    Wdn[:, 1] = T / nw
-    return Wn, Wdn, idx
+comb = O.comb
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])

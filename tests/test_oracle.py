@@ -246,9 +246,9 @@ def test_oracle_full_g_path_matches_numpy(cplx):
 
 
 def test_comb_restatement_properties():
-    """The comb the GPU test restates: every copy's parent has positive weight, parents
+    """The oracle's comb (the GPU test's reference): every copy's parent has positive weight, parents
     appear in walker order, and walker i gets floor or ceil of nw w_i / T copies."""
-    from test_gpu_population import comb
+    from oracle.oracle import comb
     rng = np.random.default_rng(2)
     nw = 200
     W = rng.normal(size=(nw, 2, 3, 2))
