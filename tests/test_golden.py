@@ -1,7 +1,8 @@
 """Pins the oracle against the reference's own known-answer tests and the published
 Philox4x32-10 answers.  The reference cases come from tests/golden/reference_kats.json,
 extracted by tests/golden/make_golden.py from test_sparse_ops.cpp, sp_blas.hpp and
-ma_operations.hpp of the reference."""
+ma_operations.hpp of the reference; the CSR cases of the reference's generator
+(gensparse.py) are restated in the test."""
 import json
 import os
 
@@ -129,3 +130,45 @@ def test_normals_moments():
     assert abs(x.mean()) < 0.01
     assert abs(x.var() - 1.0) < 0.01
     assert np.all(np.isfinite(x))
+
+
+def _gensparse_cases():
+    """The four C = alpha A X + beta Y cases of the reference's generator
+    (src/Numerics/tests/gensparse.py:19-58: alpha 1, beta 2), restated.  The script itself
+    no longer runs on current scipy (dok_matrix.iteritems), so its answer formula
+    b = alpha*(A.dot(X)) + beta*Y (:65) is evaluated here in numpy."""
+    cases = []
+    A = np.eye(3)
+    cases.append((A, np.ones((3, 1)), np.ones((3, 1))))
+    A = np.eye(3)
+    A[1, 2] = 2.0
+    cases.append((A, np.arange(0, 6.0).reshape(3, 2), np.arange(0, 6.0).reshape(3, 2)))
+    A = np.eye(3)
+    A[1, 1] = 0.0
+    A[1, 2] = 1.0
+    cases.append((A, np.arange(0, 9.0).reshape(3, 3), np.arange(0, 9.0).reshape(3, 3)))
+    A = np.eye(2)
+    A[0, 1] = 1.0
+    cases.append((A, np.arange(0, 6.0).reshape(2, 3), np.arange(0, 6.0).reshape(2, 3)))
+    return cases
+
+
+@pytest.mark.parametrize("i", range(4))
+@pytest.mark.parametrize("cplx", [False, True])
+def test_gensparse_known_answers(i, cplx):
+    """The generator's cases through the csrmm restatement (its double and complex<double>
+    cases hold the same real values); cplx adds imaginary parts to the same pattern."""
+    A, X, Y = _gensparse_cases()[i]
+    if cplx:
+        A = A * (1.0 + 0.5j)
+        X = X - 0.25j * X
+        Y = Y + 1j
+    M, K = A.shape
+    ncolsB = X.shape[1]
+    entries = [(r, c, A[r, c]) for r in range(M) for c in range(K) if A[r, c] != 0]
+    csr = _csr(M, K, entries)
+    B = np.ascontiguousarray(X, np.complex128).reshape(-1)
+    C = np.ascontiguousarray(Y, np.complex128).reshape(-1).copy()
+    _csrmm("N", M, K, csr, B, ncolsB, 1.0, 2.0, C)
+    np.testing.assert_allclose(C.reshape(M, ncolsB), 1.0 * (A @ X) + 2.0 * Y, rtol=0,
+                               atol=1e-14)
