@@ -277,6 +277,11 @@ def test_program_input_errors(tmp_path, c1_input):
         "magic": (b"NOTAFILE" + blob[8:], "not a driver input file"),
         "truncated": (blob[: len(blob) // 2], "truncated"),
         "trailing": (blob + b"\0" * 8, "trailing bytes"),
+        # NAEB != NAEA: the reference reads closed shells only (initialize_serial.hpp:67-71)
+        "open_shell": (blob[:16] + np.array([s.n + 1], "<i4").tobytes() + blob[20:],
+                       "NAEA != NAEB"),
+        "bad_sizes": (blob[:8] + np.array([0], "<i4").tobytes() + blob[12:],
+                      "bad sizes in the header"),
     }
     for name, (content, msg) in cases.items():
         if isinstance(content, bytes):
