@@ -144,11 +144,12 @@ afq_status afq_get_eshift(afq_handle* h, double* eshift);
  * reference, which leaves branching out (miniafqmc_base.cpp:347).  With weights
  * w_i = max(Re W_data[i][1], 0), total T and prefix sums C_i in walker order, copy j of
  * nwalk takes the first walker with C_i > (j + u) T / nwalk and weight T / nwalk; the
- * other W_data entries come with it.  u is one Philox4x32-10 uniform for (seed, step),
- * drawn from a stream apart from the auxiliary fields', so a run restored from saved
- * walkers (afq_set_walkers, afq_set_eshift) at the same seed and step repeats it.  Per
- * handle: sharded walker sets comb their own walkers.  AFQ_ERR_STATE when no walker has
- * positive weight.  Synchronous. */
+ * other W_data entries come with it.  u is one Philox4x32-10 uniform for (seed, step,
+ * walker offset), drawn from a stream apart from the auxiliary fields', so a run restored
+ * from saved walkers (afq_set_walkers, afq_set_eshift) at the same seed and step repeats
+ * it.  Per handle: the blocks of a sharded ensemble (afq_set_walker_offset) comb their own
+ * walkers, each with the u of its offset, and keep their own total weight.  AFQ_ERR_STATE
+ * when no walker has positive weight.  Synchronous. */
 afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step);
 afq_status afq_set_eshift(afq_handle* h, double eshift);
 /* Places this handle's walkers at [offset, offset+nwalk) of an ensemble of nwalk_global
@@ -248,14 +249,18 @@ afq_status afq_copy_out(afq_handle* h, int which, void* host);
  *   Lh  [nchol][2][naea][nmo] complex, unscaled half-rotated factors (device memory)
  *   Gc  [nwalk][2][naea][nmo] complex, compact density matrices, walker-major (device)
  *   ek  [nwalk] complex output (device): EK_w = 1/2 sum_{s,n} tr(T T), T = Lh_s[n] Gc_s^T
+ * Lh, Gc and ek must be 16-byte aligned (the kernels move whole complex values);
+ * other pointers are rejected with AFQ_ERR_ARG before any device work.
  * Asynchronous on `stream` (a cudaStream_t, NULL for the default stream).  The partial
  * sums live in one file-scope device array of 2^18 complex values (4 MiB, held by every
  * GPU that loads the library until exit): calls with 2 * nwalk * ceil(nchol / (96 /
- * naea)) above that are rejected with AFQ_ERR_UNSUPPORTED (split the walkers into
- * batches); naea must be <= 96.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) with that device current; make that first call before
- * any stream capture.  All calls share the array, so calls that overlap on the GPU (on
- * different streams) race; serialise them. */
+ * naea)) above that, or with ceil(nwalk / (96 / naea)) above 65535, are rejected with
+ * AFQ_ERR_UNSUPPORTED (split the walkers into batches); naea must be <= 96.  The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current and keeps it for the life of the process; make that first call before
+ * any stream capture, and do not reset the device (cudaDeviceReset) after it, since the
+ * kept address would then be stale.  All calls share the array, so calls that overlap on
+ * the GPU (on different streams) race; serialise them. */
 afq_status afq_exchange_energy_noalloc(const double* Lh, const double* Gc, int nmo, int naea,
                                        int nchol, int nwalk, double* ek, void* stream);
 

@@ -23,6 +23,7 @@ using afq::launch_csr_gather;
 struct afq_handle {
   afq_system_desc d{};
   int N = 0, n = 0, nc = 0, nw = 0;
+  int walker_offset = 0;     // global index of walker 0 (afq_set_walker_offset)
   long long NAK = 0;
   cudaStream_t st = nullptr;
   std::string err;
@@ -972,7 +973,7 @@ afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step) {
   // copies go through T2 (walkers) and T1 (walker data), per-step scratch of the propagation
   double total = 0.0;
   AFQ_CUDA(h, afq::launch_comb(h->W, h->Wd, h->nw, (long long)h->N * 2 * h->n,
-                               afq::comb_uniform(seed, step), h->comb_C, h->comb_idx,
+                               afq::comb_uniform(seed, step, h->walker_offset), h->comb_C, h->comb_idx,
                                h->comb_w, h->T2, h->T1, &total, h->st));
   if (!(total > 0.0))   // walkers untouched
     return fail(h, AFQ_ERR_STATE, "population control: no walker has positive weight");
@@ -1007,6 +1008,7 @@ afq_status afq_set_walker_offset(afq_handle* h, int offset, int nwalk_global) {
   AFQ_CUDA(h, afq::launch_set_scalars(h->sc, seed, step, 0, 0.0, h->st, offset, nwalk_global));
   h->host_seed = seed;
   h->host_step = step;
+  h->walker_offset = offset;
   return AFQ_OK;
 }
 

@@ -34,11 +34,12 @@ cudaError_t launch_energy_reduce(const z_t* Gc, const z_t* haj, int nak, const z
                                  const z_t* cv, int nchol, const z_t* Kpart, int nblk, int nw,
                                  int mode, z_t* Wd, double* parts, cudaStream_t st);
 cudaError_t launch_eav(const z_t* Wd, int nw, DevScalars* sc, cudaStream_t st);
-// Population control by the comb (popcontrol.cu): u = comb_uniform(seed, step); C [nw],
+// Population control by the comb (popcontrol.cu): u = comb_uniform(seed, step, offset of
+// the handle's walker block); C [nw],
 // idx [nw], wnew [1] device scratch; Wscr / Wdscr hold the copies before they replace
 // W [nw][per] and W_data [nw][8].  Synchronises once to read the total weight (*total);
 // with no positive weight nothing is copied.
-double comb_uniform(unsigned long long seed, unsigned long long step);
+double comb_uniform(unsigned long long seed, unsigned long long step, int walker_offset);
 cudaError_t launch_comb(z_t* W, z_t* Wd, int nw, long long per, double u, double* C, int* idx,
                         double* wnew, z_t* Wscr, z_t* Wdscr, double* total, cudaStream_t st);
 

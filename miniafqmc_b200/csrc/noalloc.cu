@@ -6,6 +6,7 @@
 // start-up.  This entry point serves them: the caller passes device inputs and outputs,
 // and the partial sums the exchange kernel needs live in a fixed file-scope device
 // array instead of a per-handle buffer.
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/afqmc_b200.h"
@@ -41,11 +42,19 @@ extern "C" afq_status afq_exchange_energy_noalloc(const double* Lh, const double
                                                   void* stream) {
   if (!Lh || !Gc || !ek || nmo <= 0 || naea <= 0 || nchol <= 0 || nwalk <= 0)
     return AFQ_ERR_ARG;
+  // the exchange kernel reads Lh and Gc with 16-byte asynchronous copies and the finish
+  // kernel stores whole complex values: a buffer that is only 8-byte aligned (a view at an
+  // odd double offset) would fault on the device, so it is refused here
+  if ((reinterpret_cast<uintptr_t>(Lh) | reinterpret_cast<uintptr_t>(Gc) |
+       reinterpret_cast<uintptr_t>(ek)) & 15u)
+    return AFQ_ERR_ARG;
   if (naea > 96 || naea > nmo) return AFQ_ERR_UNSUPPORTED;
   int nblk = 0;
   afq::launch_exchange(nullptr, nullptr, nmo, naea, nchol, nwalk, nullptr, &nblk, nullptr);
   const long long used = 2LL * nwalk * nblk;
   if (used > kMaxExchangePartials) return AFQ_ERR_UNSUPPORTED;   // batch too large for scratch
+  // one CTA row per group of 96 / naea walkers: the grid's y extent is at most 65535
+  if ((nwalk + 96 / naea - 1) / (96 / naea) > 65535) return AFQ_ERR_UNSUPPORTED;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AFQ_ERR_CUDA;
   z_t* scratch = nullptr;

@@ -5,9 +5,12 @@
 // t_j = (j + u) T / nw for one uniform u in [0, 1) and picks the first walker with
 // C_i > t_j; every copy carries weight T / nw, so the total weight is unchanged and a
 // walker's expected number of copies is nw w_i / T.  u comes from Philox4x32-10 on the
-// counter (0, 0, step) with the key seed ^ kCombKey, a stream apart from the auxiliary
-// fields' (counter (pair, step), key seed), so a run resumed from saved walkers at the
-// same seed and step draws the same comb.
+// counter (walker offset, 0, step) with the key seed ^ kCombKey, a stream apart from the
+// auxiliary fields' (counter (pair, step), key seed), so a run resumed from saved walkers
+// at the same seed and step draws the same comb.  The walker offset is the global index
+// of the handle's first walker (0 unless the ensemble is sharded): the blocks of a
+// sharded ensemble comb independently, each with its own u, and keep their own total
+// weight (no weight moves between blocks).
 #include "afq_kernels.h"
 
 namespace afq {
@@ -71,9 +74,9 @@ __global__ void comb_gather_kernel(const z_t* __restrict__ W, const z_t* __restr
 
 }  // namespace
 
-double comb_uniform(unsigned long long seed, unsigned long long step) {
+double comb_uniform(unsigned long long seed, unsigned long long step, int walker_offset) {
   const unsigned long long key = seed ^ kCombKey;
-  uint32_t c[4] = {0u, 0u, (uint32_t)step, (uint32_t)(step >> 32)};
+  uint32_t c[4] = {(uint32_t)walker_offset, 0u, (uint32_t)step, (uint32_t)(step >> 32)};
   philox4x32_10(c, (uint32_t)key, (uint32_t)(key >> 32));
   return (double)(((uint64_t)(c[0] >> 5) << 26) | (c[1] >> 6)) * (1.0 / 9007199254740992.0);
 }

@@ -111,7 +111,9 @@ def run(engine, nsteps: int, nsubsteps: int, northo: int, seed: int,
     (one file per rank; Eshift is the ensemble's on every rank).  `branch_every` = k > 0
     runs population control (the comb, `population_control(seed, step_tot)`) after every
     k-th step's energy, where the miniapp marks that branching belongs
-    (miniafqmc_base.cpp:347); sharded walker sets comb their own block."""
+    (miniafqmc_base.cpp:347); sharded walker sets comb their own block, each with the
+    comb uniform of its walker offset, so the blocks resample independently and keep
+    their own total weight (this differs from one comb over the whole ensemble)."""
     if comm is not None:
         engine.set_walker_offset(comm.offset, comm.nwalk_global)
     step0 = step_tot = 0

@@ -170,6 +170,7 @@ class Oracle:
 
     def set_walker_offset(self, offset: int, nwalk_global: int):
         self.lib.orc_set_walker_offset(self.h, offset, nwalk_global)
+        self.walker_offset = offset
 
     @property
     def eshift(self) -> float:
@@ -235,7 +236,7 @@ class Oracle:
     def population_control(self, seed: int, step: int):
         """The comb on this walker set (`comb` below), as afq_population_control."""
         W, Wd = self.get_walkers()
-        Wn, Wdn, _ = comb(W, Wd, seed, step)
+        Wn, Wdn, _ = comb(W, Wd, seed, step, getattr(self, "walker_offset", 0))
         self.set_walkers(Wn, Wdn)
 
     def calculate_energy(self, mode: str = "auto", parts: bool = False):
@@ -297,18 +298,21 @@ def halfrotate(system, cutoff: float = 1e-6):
 # Population control by the comb (no reference counterpart: the reference leaves branching
 # out, miniafqmc_base.cpp:347).  Weights w_i = max(Re W_data[i][1], 0), total T, prefix sums
 # C_i in walker order; copy j takes the first walker with C_i > (j + u) T / nw and weight
-# T / nw.  u is one Philox4x32-10 uniform for (seed, step) on a key apart from the fields'.
+# T / nw.  u is one Philox4x32-10 uniform for (seed, step, walker offset) on a key apart
+# from the fields'; the blocks of a sharded ensemble comb on their own, each with the u of
+# its offset (the global index of its first walker).
 COMB_KEY = 0x9E3779B97F4A7C15
 
 
-def comb_uniform(seed: int, step: int) -> float:
+def comb_uniform(seed: int, step: int, offset: int = 0) -> float:
     key = (seed ^ COMB_KEY) & 0xFFFFFFFFFFFFFFFF
-    c = philox([0, 0, step & 0xFFFFFFFF, step >> 32], [key & 0xFFFFFFFF, key >> 32])
+    c = philox([offset & 0xFFFFFFFF, 0, step & 0xFFFFFFFF, step >> 32],
+               [key & 0xFFFFFFFF, key >> 32])
     c = [int(x) for x in c]
     return float(((c[0] >> 5) << 26) | (c[1] >> 6)) * (1.0 / 9007199254740992.0)
 
 
-def comb(W: np.ndarray, Wd: np.ndarray, seed: int, step: int):
+def comb(W: np.ndarray, Wd: np.ndarray, seed: int, step: int, offset: int = 0):
     """(new walkers, new walker data, parent index of each copy)."""
     nw = Wd.shape[0]
     w = np.maximum(Wd[:, 1].real, 0.0)
@@ -316,7 +320,7 @@ def comb(W: np.ndarray, Wd: np.ndarray, seed: int, step: int):
         raise ValueError("population control: no walker has positive weight")
     C = np.cumsum(w)
     T = C[-1]
-    u = comb_uniform(seed, step)
+    u = comb_uniform(seed, step, offset)
     t = (np.arange(nw, dtype=np.float64) + u) * T / nw
     idx = np.searchsorted(C, t, side="right")
     last = int(np.nonzero(w > 0)[0][-1])

@@ -43,6 +43,25 @@ def test_comb_matches_numpy(prec):
     e.close()
 
 
+def test_comb_of_a_sharded_block_uses_its_offset():
+    """A handle holding walkers [offset, offset + nw) of a larger ensemble combs its block
+    with the uniform of its offset (oracle.comb with offset=)."""
+    from miniafqmc_b200.afqmc import AfqmcSys
+    s = system("C1")
+    nw, off = 32, 32
+    rng = np.random.default_rng(12)
+    W, Wd = s.initial_walkers(nw)
+    Wd[:, 1] = rng.lognormal(0.0, 0.8, nw)
+    e = AfqmcSys(s, nw, walkers=(W, Wd))
+    e.set_walker_offset(off, 2 * nw)
+    W0, Wd0 = e.get_walkers()
+    e.population_control(7, 3)
+    Wexp, Wdexp, _ = comb(W0, Wd0, 7, 3, offset=off)
+    W1, Wd1 = e.get_walkers()
+    assert np.array_equal(W1, Wexp) and np.array_equal(Wd1, Wdexp)
+    e.close()
+
+
 def test_comb_rejects_dead_population():
     from miniafqmc_b200.afqmc import AfqmcSys, AfqmcError
     s = system("C1")

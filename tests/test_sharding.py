@@ -1,7 +1,9 @@
 """Walker sharding across ranks (gloo, world size 2, CPU): the sharded driver with the
 oracle as engine reproduces the unsharded ensemble -- same auxiliary fields (global
 Philox indexing), same Eshift (all-reduced sum of Re W_data[:,4]) and same weighted
-energy (all-reduced sums); per-rank checkpoints resume the sharded run exactly."""
+energy (all-reduced sums); per-rank checkpoints resume the sharded run exactly.
+Population control is per block: each rank combs its own walkers with the uniform of its
+walker offset (independent combs), and no weight moves between ranks."""
 import os
 import socket
 
@@ -49,8 +51,12 @@ def _worker(rank, world, port, out_dir):
                    checkpoint=ck)
         res2 = driver.run(O.Oracle(s, per), STEPS, SUB, NORTHO, 0, comm=comm, graph=False,
                           resume=driver.read_checkpoint(ck))
+        # one comb of this rank's block after the run
+        Wb, Wdb = eng.get_walkers()
+        eng.population_control(SEED, 99)
+        Wc, Wdc = eng.get_walkers()
         np.savez(os.path.join(out_dir, f"r{rank}.npz"), W=W, Wd=Wd, E=np.array(res.energies),
-                 E_resumed=np.array(res2.energies))
+                 E_resumed=np.array(res2.energies), Wb=Wb, Wdb=Wdb, Wc=Wc, Wdc=Wdc)
     finally:
         dist.destroy_process_group()
 
@@ -75,3 +81,11 @@ def test_sharded_run_matches_single_ensemble(tmp_path):
         np.testing.assert_allclose(p["E"], res.energies, rtol=1e-12)
         # per-rank checkpoints resume the sharded run: the steps after it repeat it
         assert np.array_equal(p["E_resumed"][1:], p["E"][2:])
+    # sharded population control: block r combs alone with the uniform of offset r * per
+    per = NW // world
+    for r, p in enumerate(parts):
+        We, Wde, _ = O.comb(p["Wb"], p["Wdb"], SEED, 99, offset=r * per)
+        assert np.array_equal(p["Wc"], We) and np.array_equal(p["Wdc"], Wde)
+        tot = np.maximum(p["Wdb"][:, 1].real, 0).sum()
+        assert abs(p["Wdc"][:, 1].real.sum() - tot) < 1e-12 * per * max(tot, 1.0)
+    assert O.comb_uniform(SEED, 99, 0) != O.comb_uniform(SEED, 99, per)

@@ -3,7 +3,9 @@ device memory (graph capture, pool-owning frameworks).  Its per-walker output mu
 the exchange part of the handle's Cholesky energy (afq_energy + AFQ_BUF_ENERGY_PARTS) to
 1e-10 relative -- the FP64 parity tolerance -- on two calls in a row, since every call
 reuses the same static scratch array.  Inputs and outputs are device buffers the test
-(the caller) allocates with torch; the entry point itself allocates nothing."""
+(the caller) allocates with torch; the entry point itself allocates nothing.  The
+argument checks (alignment, batch size) run on the host before any device work, so they
+are tested without a GPU."""
 import ctypes
 
 import numpy as np
@@ -11,10 +13,19 @@ import pytest
 
 from conftest import system
 
-pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 
+def _entry():
+    from miniafqmc_b200.afqmc import load_library
+    lib = load_library()
+    f = lib.afq_exchange_energy_noalloc
+    f.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 2
+    f.restype = ctypes.c_int
+    return f
+
+
+@pytest.mark.gpu
 def test_exchange_energy_noalloc_matches_handle_twice():
     import torch
     from miniafqmc_b200.afqmc import AfqmcSys, load_library
@@ -50,12 +61,19 @@ def test_exchange_energy_noalloc_matches_handle_twice():
 
 
 def test_exchange_energy_noalloc_rejects_oversized_batch():
-    from miniafqmc_b200.afqmc import load_library
-    lib = load_library()
-    lib.afq_exchange_energy_noalloc.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_int] * 4 + \
-        [ctypes.c_void_p] * 2
-    lib.afq_exchange_energy_noalloc.restype = ctypes.c_int
+    f = _entry()
     # 2 * 4096 walkers * 1536/2 blocks far exceeds the 2^18 partials of the static array
     dummy = ctypes.c_void_p(16)
-    st = lib.afq_exchange_energy_noalloc(dummy, dummy, 384, 48, 1536, 4096, dummy, None)
-    assert st == 5   # AFQ_ERR_UNSUPPORTED
+    assert f(dummy, dummy, 384, 48, 1536, 4096, dummy, None) == 5   # AFQ_ERR_UNSUPPORTED
+    # few partials but more than 65535 walker groups in the launch grid (naea > 48: one
+    # walker per group)
+    assert f(dummy, dummy, 96, 64, 1, 70000, dummy, None) == 5
+
+
+def test_exchange_energy_noalloc_rejects_misaligned_buffers():
+    """The kernels move 16-byte complex values: 8-byte aligned pointers are refused
+    before any device work (AFQ_ERR_ARG) instead of faulting on the GPU."""
+    f = _entry()
+    ok, odd = ctypes.c_void_p(4096), ctypes.c_void_p(4096 + 8)
+    for args in ((odd, ok, ok), (ok, odd, ok), (ok, ok, odd)):
+        assert f(args[0], args[1], 64, 16, 256, 16, args[2], None) == 1   # AFQ_ERR_ARG
