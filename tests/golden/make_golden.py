@@ -1,7 +1,8 @@
 """Extracts the reference's own known-answer tests into tests/golden/reference_kats.json.
 
-Run here, where the reference tree is mounted (its path is the first argument, default
-/root/reference).  The numbers are parsed out of the reference's test sources as text:
+Run where the reference tree is mounted, with its path as the only argument
+(`python tests/golden/make_golden.py <reference tree>`).  The numbers are parsed out of
+the reference's test sources as text:
 
   src/Numerics/tests/test_sparse_ops.cpp   CSR x vector / CSR x matrix cases (alpha, beta)
   src/Numerics/sp_blas.hpp  (_TEST_SP_BLAS)        4x4 csrmm 'N' and 'T'
@@ -17,7 +18,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+    sys.exit("usage: make_golden.py <path of the miniAFQMC reference tree>")
+REF = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 NUM = r"[-+]?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?"
