@@ -63,6 +63,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-walkers", type=int, default=0)
     p.add_argument("--walkers", type=int, default=0, help="walkers per GPU (default: config)")
+    p.add_argument("--acc-substeps", type=int, default=500,
+                   help="substeps of the energy-accuracy pass (0 skips it)")
+    p.add_argument("--acc-equil", type=int, default=100,
+                   help="equilibration substeps left out of the accuracy statistics")
     return p.parse_args()
 
 
@@ -198,6 +202,25 @@ def mixed_propagate_bytes(cfg, nw, order=6, preal=True):
     return float(tot)
 
 
+def prop_flops(cfg, nw, order=6):
+    """Algorithmic FLOPs of one propagation (a6): per walker (order + 2) N x N times N x 2n
+    complex products = 16 N^2 n complex multiply-adds at order 6, 8 FLOP each."""
+    return 8.0 * nw * (order + 2) * cfg.nmo * cfg.nmo * 2 * cfg.nel
+
+
+def prop_compulsory_bytes(cfg, nw, preal=True):
+    """HBM bytes a propagation cannot avoid in the mixed form's layouts: V (bf16 hi + lo,
+    read once for all Taylor terms), the packed P W operand in (hi + lo), the FP64 walkers
+    out and the two packed forms of the new walkers out (T1 operand and next P W operand,
+    hi + lo)."""
+    N, n = cfg.nmo, cfg.nel
+    V = 2 * N * 2 * N * 2                 # hi + lo of [N][2N] bf16
+    Fp = 4 * n * (N if preal else 2 * N) * 2   # one part of a P-product B operand
+    T1op = 2 * n * 2 * N * 2 * 2          # hi + lo of the T1 operand, rows (re, -im)
+    W64 = N * 2 * n * 16
+    return float(nw * (V + 2 * Fp + W64 + T1op + 2 * Fp))
+
+
 def mixed_stage_flops(cfg, nw, stage, real_ops=True, subset=None):
     """Algorithmic FLOPs of one call of a mixed-form tensor-core stage (complex x complex
     multiply-add = 8 FLOP, real x complex = 4).  vHS counts the N(N+1)/2 symmetric pairs
@@ -317,22 +340,84 @@ class Form:
             self.measure(record)
 
 
-def exact_trajectory(system, cfg, args, device, torch, substeps=20):
-    """The mixed form's deterministic energy error along a trajectory: fresh mixed (exact
-    Cholesky energy, no control variate) and FP64 walker sets driven by the same auxiliary
-    fields for `substeps` substeps, energies every energy_every substeps (untimed)."""
-    forms = [Form(system, cfg, args, f, device, None, torch) for f in ("mixed", "fp64")]
-    for f in forms:
+def blocking_sigma(x):
+    """Standard error of the mean of a correlated series by blocking (Flyvbjerg and
+    Petersen, J. Chem. Phys. 91, 461 (1989)): neighbouring values are averaged in pairs
+    level after level, the naive standard error of each level's blocks is computed, and
+    the largest over the levels that keep at least 8 blocks is returned -- the plateau
+    value, or a bound above it when the series is too short to reach the plateau.
+    Returns (sigma, per-level sigmas)."""
+    x = np.asarray(x, dtype=np.float64)
+    levels = []
+    while len(x) >= 8:
+        n = len(x)
+        levels.append(float(np.sqrt(np.var(x, ddof=1) / n)))
+        h = n // 2 * 2
+        x = 0.5 * (x[0:h:2] + x[1:h:2])
+    return (max(levels) if levels else float("nan")), levels
+
+
+def accuracy_pass(system, cfg, args, device, torch):
+    """Energy accuracy at the target run length, apart from the headline timing: three
+    walker sets start from the trial and take `acc_substeps` substeps (CUDA-graph
+    substeps) on the same Philox fields -- mixed precision with the control variate (the
+    headline form), mixed precision with exact exchange, and FP64 -- measuring the energy
+    every energy_every substeps.  The control variate trains on its first exact samples
+    inside the pass (its first measurements are exact on every walker).  Measurements of
+    the first `acc_equil` substeps (equilibration from the trial) are left out of the
+    statistics.  Per form: mean energy, its standard error by blocking and the device time
+    of the whole pass (CUDA events on the form's stream around all its substeps and
+    measurements).  |dE| of each mixed form against FP64 on the same fields with the
+    blocked standard error of the difference series, and the energy error per wall-second
+    sigma_E * sqrt(T) of each form."""
+    out = {"substeps": args.acc_substeps, "energy_every": args.energy_every,
+           "equilibration_substeps": args.acc_equil, "forms": {}}
+    series = {}
+    for name in ("mixed-cv", "mixed", "fp64"):
+        f = Form(system, cfg, args, name, device, None, torch)
+        e = f.eng
+        e.synchronize()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(f.stream)
         f.measure(record=False)
-        for st in range(substeps):
+        steps = []
+        for st in range(args.acc_substeps):
             f.step(st)
-    Em, E6 = np.array(forms[0].energies), np.array(forms[1].energies)
-    for f in forms:
-        f.eng.close()
-    return {"substeps": substeps, "measurements": int(len(Em)),
-            "abs_dE_of_means_Ha": float(abs(Em.mean() - E6.mean())),
-            "max_abs_dE_Ha": float(np.max(np.abs(Em - E6))),
-            "definition": "mixed form (exact exchange) minus FP64 form, same seeds and fields"}
+            if (st + 1) % args.energy_every == 0:
+                steps.append(st + 1)
+        e.synchronize()
+        e1.record(f.stream)
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) * 1e-3
+        keep = np.array(steps) > args.acc_equil
+        E = np.array(f.energies)[keep]
+        sig, lev = blocking_sigma(E)
+        series[name] = E
+        rec = {"mean_E": float(E.mean()), "sigma_E_blocked": sig,
+               "sigma_E_levels": [float(v) for v in lev], "device_s": secs,
+               "measurements": int(keep.sum()), "eps_Ha_sqrt_s": sig * float(np.sqrt(secs))}
+        if f.mode == "cv":   # sampling variance of the subset correction, per measurement
+            sv = np.array(f.cvvar)[keep]
+            rec["subset_sigma_per_measurement_Ha"] = float(np.sqrt(np.mean(sv)))
+            rec["control_variate"] = e.cv_stats()
+        out["forms"][name] = rec
+        e.close()
+    for name in ("mixed-cv", "mixed"):
+        d = series[name] - series["fp64"]
+        sd, _ = blocking_sigma(d)
+        out[f"dE_{name}_vs_fp64"] = {"abs_dE_Ha": float(abs(d.mean())), "sigma_Ha": sd,
+                                     "max_abs_per_measurement_Ha": float(np.max(np.abs(d)))}
+    fm, f6 = out["forms"]["mixed-cv"], out["forms"]["fp64"]
+    out["abs_dE_Ha"] = out["dE_mixed-cv_vs_fp64"]["abs_dE_Ha"]
+    out["abs_dE_sigma_Ha"] = out["dE_mixed-cv_vs_fp64"]["sigma_Ha"]
+    out["err_per_wall_s"] = {
+        "form": fm["eps_Ha_sqrt_s"], "fp64": f6["eps_Ha_sqrt_s"],
+        "fp64_over_form": f6["eps_Ha_sqrt_s"] / fm["eps_Ha_sqrt_s"],
+        "definition": "sigma_E * sqrt(T): sigma_E the blocked standard error of the mean "
+                      "energy over the pass after equilibration, T the device seconds of the "
+                      "whole pass (substeps and measurements) of that form"}
+    return out
 
 
 def timed(form, steps, start, torch, dist, world, profile=False, record=True):
@@ -576,28 +661,13 @@ def main():
         _, _, stages64 = timed(ref, min(args.steps, 5), nwarm + args.steps, torch, dist, world,
                                profile=True, record=False)
         stages64 = {k: (v[0] * args.steps / min(args.steps, 5), v[1]) for k, v in stages64.items()}
-        Em, E6 = np.array(head.energies), np.array(ref.energies)
         T_m, T_6 = ms * 1e-3, ms64 * 1e-3
-        sig_m = float(np.sqrt(np.mean(head.sig2) / len(head.sig2)))
-        sig_6 = float(np.sqrt(np.mean(ref.sig2) / len(ref.sig2)))
-        eps_m, eps_6 = sig_m * np.sqrt(T_m), sig_6 * np.sqrt(T_6)
         cmp = {
             "fp64_plain": {"value": nw * args.steps / T_6, "unit": METRIC,
                            "ms_per_step": ms64 / args.steps,
                            "stages_ms": {k: round(v[0], 3) for k, v in stages64.items()}},
             "speedup_vs_fp64_plain": T_6 / T_m,
-            "energy": {"measurements": len(Em), "mean_E_form": float(Em.mean()),
-                       "mean_E_fp64": float(E6.mean()), "abs_dE_Ha": float(abs(Em.mean() - E6.mean())),
-                       # standard deviation of the mean difference from the control variate's
-                       # subset sampling (independent subsets per measurement); 0 without it
-                       "dE_cv_sigma_Ha": float(np.sqrt(np.sum(head.cvvar)) / max(len(head.cvvar), 1)),
-                       "max_abs_dE_per_measurement_Ha": float(np.max(np.abs(Em - E6))),
-                       "err_per_wall_s": {"form": eps_m, "fp64": eps_6,
-                                          "fp64_over_form": eps_6 / eps_m,
-                                          "definition": "sigma_E * sqrt(timed seconds); sigma_E "
-                                          "from the weighted walker spread of each measurement "
-                                          "(plus the subset-correction variance for the control "
-                                          "variate), combined over the measurements"}},
+            "energy": {},
         }
         # the same walkers measured by both forms: the mixed form's deterministic energy
         # error against FP64, and the control-variate estimate against exact exchange
@@ -616,8 +686,8 @@ def main():
         cmp["energy"]["same_walkers"] = same
         cmp["fp64_plain"]["kernel_tuning"] = ref.eng.tuning()
         ref.eng.close()
-        if head.mode == "cv":
-            cmp["energy"]["exact_trajectory"] = exact_trajectory(s, cfg, args, local, torch)
+        if head.mode == "cv" and args.acc_substeps > 0:
+            cmp["energy"].update(accuracy_pass(s, cfg, args, local, torch))
 
     if rank != 0:
         if world > 1:
@@ -639,12 +709,32 @@ def main():
                 "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run "
                                "(no FP64 entry in MEASURED_PEAKS.json)"}
     elif dom == "propagate":
+        # algorithmic work and compulsory bytes of one substep's chain (8 launches): the
+        # stage's 16 N^2 n complex multiply-adds per walker, against the bytes it cannot
+        # avoid moving (V once, the P W operand in, W and its packed forms out); the larger
+        # of the two lower bounds on the time names the roof
         preal = bool(np.all(np.asarray(s.Propg1).imag == 0))
-        byt = mixed_propagate_bytes(cfg, nw, preal=preal) * args.steps
-        achieved = byt / (dom_ms * 1e-3) / 1e9
-        roof = {"kernel": "propagate (tcgen05 GEMM chain)", "bound": "hbm", "achieved": achieved,
-                "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                "peak_source": f"hbm_gbs, {src}"}
+        fl = prop_flops(cfg, nw) * args.steps
+        by = prop_compulsory_bytes(cfg, nw, preal) * args.steps
+        t_fl = fl / (peaks["bf16_tflops_sustained"] * 1e12)
+        t_by = by / (peaks["hbm_gbs"] * 1e9)
+        if t_fl >= t_by:
+            achieved = fl / (dom_ms * 1e-3) / 1e12
+            roof = {"kernel": "propagate (tcgen05 GEMM chain)", "bound": "tensor",
+                    "achieved": achieved, "peak": peaks["bf16_tflops_sustained"],
+                    "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops_sustained"],
+                    "peak_source": f"bf16_tflops_sustained, {src}"}
+        else:
+            achieved = by / (dom_ms * 1e-3) / 1e9
+            roof = {"kernel": "propagate (tcgen05 GEMM chain)", "bound": "hbm",
+                    "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"], "peak_source": f"hbm_gbs, {src}"}
+        roof["per_launch"] = "one substep's chain of 8 product launches"
+        roof["algorithmic"] = {
+            "flop_per_walker": prop_flops(cfg, 1), "bytes_per_walker": prop_compulsory_bytes(cfg, 1, preal),
+            "t_flop_ms": t_fl * 1e3 / args.steps, "t_byte_ms": t_by * 1e3 / args.steps,
+            "ms_measured": dom_ms / args.steps}
+        roof["traffic_model"] = mixed_propagate_bytes(cfg, nw, preal=preal)
     else:
         calls = {"DM": args.steps + args.steps // args.energy_every,
                  "energy": args.steps // args.energy_every}.get(dom, args.steps)
@@ -659,9 +749,13 @@ def main():
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"{args.config}:{args.form}:{dom}")
+        tj = json.load(open(tpath)).get(f"{args.config}:{args.form}:{dom}")
+        if tj is not None:   # DRAM bytes per launch unit, measured at a reduced walker count
+            traffic = tj * nw / json.load(open(tpath)).get("_walkers", nw)
     roof.update({"traffic": traffic, "stage_ms": dom_ms, "launches": dom_launch,
                  "avg_launch_ms": dom_ms / max(dom_launch, 1)})
+    if traffic is not None and dom == "propagate" and args.form != "fp64":
+        roof["traffic_over_compulsory"] = traffic / (roof["algorithmic"]["bytes_per_walker"] * nw)
 
     cpu = None
     if not args.no_cpu and world == 1:

@@ -1784,7 +1784,8 @@ static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nbl
                m->err, st);                                                                    \
     break;
     switch (2 * n * 8 + pk) {   // promoted exchange for the compiled walker widths
-      AFQ_EXP(32, 1) AFQ_EXP(32, 2) AFQ_EXP(64, 1) AFQ_EXP(64, 2) AFQ_EXP(96, 1) AFQ_EXP(96, 2)
+      AFQ_EXP(24, 1) AFQ_EXP(24, 2) AFQ_EXP(32, 1) AFQ_EXP(32, 2) AFQ_EXP(64, 1) AFQ_EXP(64, 2)
+      AFQ_EXP(96, 1) AFQ_EXP(96, 2) AFQ_EXP(128, 1) AFQ_EXP(128, 2)
     }
 #undef AFQ_EXP
     // invalid value: no such instance, or its shared memory does not fit (nothing launched)

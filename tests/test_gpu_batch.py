@@ -58,9 +58,10 @@ def test_batch_matches_systems_alone(mixed):
 
 
 def test_c5_shapes_mixed_energy_matches_fp64():
-    """Mixed against FP64 energies on identical walkers for the C5 shapes: n = 12, 40
-    and 64 take exchange tiles whose walker width 2n does not fill the 256-column tile
-    (per-tile kernel), or a walker width of 128 (1e-4 relative on E_J and E_K)."""
+    """Mixed against FP64 energies on identical walkers for the C5 shapes (n = 12, 40 and
+    64: exchange tiles of 8 walkers of 24 columns, 3 walkers of 80 columns in a 256-column
+    tile, 2 walkers of 128 columns): 1e-4 relative on every walker's E_J and E_K, and the
+    mean local energy within 1e-4 Ha."""
     from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
     rng = np.random.default_rng(3)
     for cfg, s in systems():
@@ -78,3 +79,5 @@ def test_c5_shapes_mixed_energy_matches_fp64():
         ej = rel(pm[:, 1], pd[:, 1])
         ek = rel(pm[:, 2], pd[:, 2])
         assert ej < 1e-4 and ek < 1e-4, (cfg.nmo, cfg.nel, ej, ek)
+        de = np.mean((pm[:, 0] + pm[:, 1] - pm[:, 2]) - (pd[:, 0] + pd[:, 1] - pd[:, 2]))
+        assert abs(de) < 1e-4, (cfg.nmo, cfg.nel, de)
