@@ -236,6 +236,16 @@ afq_status afq_stage_times(afq_handle* h, double* ms, long long* launches, int r
  * read 0.  AFQ_TUNE=0 in the environment skips the timing, AFQ_TUNE=1 or 2 forces one
  * tensor-core kernel. */
 afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms);
+/* FP64 form: which product the set-up tuner measured faster for each sparse operand.
+ * The reference multiplies its CSR matrices with one loop (sparse.hpp:166-180, called from
+ * vHS.hpp:47-56, vbias.hpp:49-63 and energy.hpp:89-97); here an operand whose density
+ * reaches 2% (and whose dense copy fits in 30% of free device memory) is also held as a
+ * dense row-major tile operand, both products are timed on the handle's shapes, and the
+ * slower operand is freed (Spvn keeps its CSR for the full-G path).  path[3], for Spvn
+ * (vHS), SpvnT (vbias) and Vakbl (energy): 1 dense-tile GEMM, 0 CSR, -1 operand absent or
+ * mixed form.  ms[6]: the best milliseconds of the CSR product and of the dense product
+ * per operand (0 when not timed).  With AFQ_TUNE=0 the rule is dense at >= 25% density. */
+afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */
 afq_status afq_get_stream(afq_handle* h, void** stream);

@@ -36,7 +36,7 @@ EXPORTS = [
     "afq_mlp_get_params", "afq_mlp_forward", "afq_mlp_gradient", "afq_mlp_train",
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
-    "afq_mixed_density_matrix_full", "afq_vbias_full",
+    "afq_mixed_density_matrix_full", "afq_vbias_full", "afq_get_sparse_paths",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -96,6 +96,7 @@ def signatures() -> dict:
         "afq_halfrotate": ([I, P, I, I, I, P, D, D, P, P, P, P, P], I),
         "afq_population_control": ([P, U64, U64], I),
         "afq_mixed_density_matrix_full": ([P], I), "afq_vbias_full": ([P], I),
+        "afq_get_sparse_paths": ([P, P, P], I),
     }
 
 
@@ -319,6 +320,20 @@ class AfqmcSys:
                for i, k in enumerate(self.TUNE_SITES)}
         out["splitk_slices"] = int(c[ns])
         return out
+
+    SPARSE_OPERANDS = ["Spvn", "SpvnT", "Vakbl"]
+
+    def sparse_paths(self) -> dict:
+        """FP64 form: per sparse operand the product the set-up tuner kept ("dense",
+        "csr", or None when absent) with the best milliseconds of the CSR and the dense
+        product (0 when not timed)."""
+        p = np.zeros(3, np.int32)
+        t = np.zeros(6)
+        self._check(self.lib.afq_get_sparse_paths(self.h, _p(p), _p(t)))
+        names = {1: "dense", 0: "csr", -1: None}
+        return {k: {"path": names[int(p[i])], "ms": [round(float(t[2 * i]), 4),
+                                                      round(float(t[2 * i + 1]), 4)]}
+                for i, k in enumerate(self.SPARSE_OPERANDS)}
 
     def substep(self, seed: int, step_tot: int, northo: int, graph: bool = True):
         """One substep of the driver loop (miniafqmc_base.cpp:251-337)."""

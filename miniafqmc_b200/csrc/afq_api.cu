@@ -61,6 +61,17 @@ struct afq_handle {
   enum { F64_VHS, F64_PROP, F64_VBIAS, F64_COUL, F64_VAKBL, F64_N };
   int f64cfg[F64_N] = {0};
   float f64ms[F64_N][2] = {};
+  // FP64 form: sparse operands (Spvn for vHS, SpvnT for vbias, Vakbl for the energy) keep
+  // the CSR arrays and, above kDenseCandidate density and within the memory budget, a
+  // dense row-major copy as well; the set-up tuner times both products and frees the
+  // slower operand.  sp_path: 1 dense-tile GEMM, 0 CSR, -1 operand absent; sp_ms: best
+  // milliseconds of the CSR and of the dense product (0 when not timed).
+  enum { SP_SPVN, SP_SPVNT, SP_VAKBL, SP_N };
+  int sp_path[SP_N] = {-1, -1, -1};
+  float sp_ms[SP_N][2] = {};
+  double sp_density[SP_N] = {};
+  z_t* sp_dense = nullptr;   // dense Spvn [N^2][nchol]
+  int vhsd_cfg = 0;          // ZGEMM tile shape of the dense vHS product
 
   // full-G path (transposed_Spvn == false): G [nw][2][N][N] walker-major, and T(Spvn) for
   // both spins as one CSR [nchol x 2 N^2] (allocated by the first full-G call)
@@ -102,7 +113,10 @@ struct afq_handle {
 
 namespace {
 
-const double kDenseThreshold = 0.25;  // CSR operand above this density is densified
+const double kDenseThreshold = 0.25;  // built-in rule: a CSR operand above this density is
+                                      // multiplied as a dense tile (the mixed form needs it)
+const double kDenseCandidate = 0.02;  // FP64 form: below this density the CSR product wins
+                                      // without timing; above it both paths are timed
 
 afq_status fail(afq_handle* h, afq_status s, const std::string& msg) {
   if (h) h->err = msg;
@@ -136,12 +150,36 @@ void dfree(afq_handle* h, void* p) {
     }
 }
 
-__global__ void csr_to_dense_kernel(const int* ri, const int* ci, const z_t* v, int nrows,
-                                    long long ncols, z_t* out) {
+// Scatters a CSR into a zeroed dense row-major matrix; rv (real values) replaces v when
+// non-null.
+__global__ void csr_to_dense_kernel(const int* ri, const int* ci, const z_t* v, const double* rv,
+                                    int nrows, long long ncols, z_t* out) {
   int r = blockIdx.x * blockDim.y + threadIdx.y;
   if (r >= nrows) return;
   for (int p = ri[r] + threadIdx.x; p < ri[r + 1]; p += blockDim.x)
-    out[(long long)r * ncols + ci[p]] = v[p];
+    out[(long long)r * ncols + ci[p]] = rv ? zmk(rv[p], 0.0) : v[p];
+}
+
+// Dense copy of a device CSR (rows x cols) into a new buffer, when the density reaches
+// kDenseCandidate and the copy takes at most 30% of the free device memory; else *dense
+// stays null.
+afq_status densify(afq_handle* h, const int* ri, const int* ci, const z_t* v, const double* rv,
+                   int nrows, long long ncols, double density, z_t** dense) {
+  *dense = nullptr;
+  if (density < kDenseCandidate) return AFQ_OK;
+  const size_t cnt = (size_t)nrows * (size_t)ncols;
+  size_t free_b = 0, total_b = 0;
+  AFQ_CUDA(h, cudaMemGetInfo(&free_b, &total_b));
+  if (sizeof(z_t) * cnt > free_b / 10 * 3) return AFQ_OK;
+  // the CSR arrays came up by pageable copies whose DMA may still be in flight
+  AFQ_CUDA(h, cudaDeviceSynchronize());
+  AFQ_CUDA(h, dalloc(h, dense, cnt));
+  AFQ_CUDA(h, cudaMemsetAsync(*dense, 0, sizeof(z_t) * cnt, h->st));
+  csr_to_dense_kernel<<<(nrows + 7) / 8, dim3(32, 8), 0, h->st>>>(ri, ci, v, rv, nrows, ncols,
+                                                                  *dense);
+  AFQ_CUDA(h, cudaGetLastError());
+  AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+  return AFQ_OK;
 }
 
 afq_status check_csr(afq_handle* h, const afq_csr_z* m, int nrows, int ncols, const char* name) {
@@ -160,10 +198,13 @@ afq_status check_csr(afq_handle* h, const afq_csr_z* m, int nrows, int ncols, co
   return AFQ_OK;
 }
 
-// Uploads a CSR; when dense_out is non-null and the density reaches the threshold, a
-// dense row-major copy is built on the device instead and the CSR arrays are released.
+// Uploads a CSR.  keep_both (FP64 form): a dense copy is added next to the CSR arrays
+// when densify allows one (the tuner keeps the faster).  Otherwise, when dense_out is
+// non-null and the density reaches kDenseThreshold, a dense row-major copy is built on
+// the device instead and the CSR arrays are released.
 afq_status upload_csr(afq_handle* h, const afq_csr_z* m, int** ri, int** ci, z_t** v,
-                      z_t** dense_out, bool allow_dense) {
+                      z_t** dense_out, bool allow_dense, bool keep_both = false,
+                      double* density = nullptr) {
   long long nnz = m->rowIndex[m->nrows];
   AFQ_CUDA(h, dalloc(h, ri, m->nrows + 1));
   AFQ_CUDA(h, dalloc(h, ci, nnz));
@@ -172,13 +213,18 @@ afq_status upload_csr(afq_handle* h, const afq_csr_z* m, int** ri, int** ci, z_t
   AFQ_CUDA(h, cudaMemcpy(*ci, m->cols, sizeof(int) * nnz, cudaMemcpyHostToDevice));
   AFQ_CUDA(h, cudaMemcpy(*v, m->vals, sizeof(z_t) * nnz, cudaMemcpyHostToDevice));
   double dens = (double)nnz / ((double)m->nrows * (double)m->ncols);
+  if (density) *density = dens;
   if (dense_out) *dense_out = nullptr;
+  if (keep_both && dense_out)
+    return densify(h, *ri, *ci, *v, nullptr, m->nrows, m->ncols, dens, dense_out);
   if (allow_dense && dense_out && dens >= kDenseThreshold) {
     size_t cnt = (size_t)m->nrows * m->ncols;
+    AFQ_CUDA(h, cudaDeviceSynchronize());   // pageable uploads above
     AFQ_CUDA(h, dalloc(h, dense_out, cnt));
     AFQ_CUDA(h, cudaMemsetAsync(*dense_out, 0, sizeof(z_t) * cnt, h->st));
-    csr_to_dense_kernel<<<(m->nrows + 7) / 8, dim3(32, 8), 0, h->st>>>(*ri, *ci, *v, m->nrows,
-                                                                       m->ncols, *dense_out);
+    csr_to_dense_kernel<<<(m->nrows + 7) / 8, dim3(32, 8), 0, h->st>>>(*ri, *ci, *v, nullptr,
+                                                                       m->nrows, m->ncols,
+                                                                       *dense_out);
     AFQ_CUDA(h, cudaGetLastError());
     AFQ_CUDA(h, cudaStreamSynchronize(h->st));
     dfree(h, *ri); dfree(h, *ci); dfree(h, *v);
@@ -290,8 +336,18 @@ cudaError_t body_sigma(afq_handle* h, int use_xraw) {
                            h->st);
 }
 
+// vHS^T [w][ik] = sum_c X[c][w] Spvn[ik][c] with the dense Spvn: one ZGEMM of M = nw,
+// N = NMO^2, K = nchol writing each walker's matrix row by row.
+cudaError_t dense_vhs(afq_handle* h, int cfg) {
+  const long long NN = (long long)h->N * h->N;
+  ZGemmDesc g{h->nw, (int)NN, h->nc, h->X, h->nw, 0, h->sp_dense, h->nc, 0, zmk(1, 0)};
+  EpiStore ep{h->vHS, NN, 0, zmk(0, 0), 0};
+  return zgemm_launch<false, true>(g, 1, ep, h->st, cfg);
+}
+
 cudaError_t body_vhs(afq_handle* h) {
   if (h->mixed) return afq::mixed_vhs(h->mixed, h->X, h->vHS, h->st);
+  if (h->sp_dense) return dense_vhs(h, h->vhsd_cfg);
   return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, h->N * h->N, h->nw,
                                 h->vHS, (long long)h->N * h->N, h->st,
                                 h->f64cfg[afq_handle::F64_VHS]);
@@ -450,24 +506,70 @@ void drop_graphs(afq_handle* h) {
 // not depend on the choice.  A candidate whose first call takes over 3x the best so far is
 // dropped after that call; calls over 20 ms are timed once.  Choices are cached per shape
 // for the process.  AFQ_TUNE=0 keeps the built-in rules.
+// Keeps one form of each sparse operand of the FP64 form: dense[op] keeps the dense copy
+// (and frees the CSR arrays of SpvnT / Vakbl; Spvn's CSR stays for the full-G path),
+// otherwise the dense copy is freed.
+void keep_paths(afq_handle* h, const int* dense) {
+  auto one = [&](int op, z_t** d, int** ri, int** ci, z_t** v, bool free_csr) {
+    if (h->sp_path[op] < 0) return;
+    if (dense[op] && *d) {
+      if (free_csr) {
+        dfree(h, *ri); dfree(h, *ci); dfree(h, *v);
+        *ri = nullptr; *ci = nullptr; *v = nullptr;
+      }
+      h->sp_path[op] = 1;
+    } else {
+      if (*d) dfree(h, *d);
+      *d = nullptr;
+      h->sp_path[op] = 0;
+    }
+  };
+  int *r0 = nullptr, *c0 = nullptr;
+  z_t* v0 = nullptr;
+  one(afq_handle::SP_SPVN, &h->sp_dense, &r0, &c0, &v0, false);
+  one(afq_handle::SP_SPVNT, &h->spT_dense, &h->spT_ri, &h->spT_ci, &h->spT_v, true);
+  one(afq_handle::SP_VAKBL, &h->vk_dense, &h->vk_ri, &h->vk_ci, &h->vk_v, true);
+}
+
+// FP64 form, built-in rule for the sparse operands: dense above kDenseThreshold.
+void rule_paths(afq_handle* h) {
+  int dense[afq_handle::SP_N];
+  for (int i = 0; i < afq_handle::SP_N; i++) dense[i] = h->sp_density[i] >= kDenseThreshold;
+  keep_paths(h, dense);
+}
+
 cudaError_t fp64_tune(afq_handle* h) {
   const char* env = getenv("AFQ_TUNE");
-  if (env && atoi(env) == 0) return cudaSuccess;
+  if (env && atoi(env) == 0) {
+    rule_paths(h);
+    return cudaSuccess;
+  }
   static std::mutex mu;
   static std::map<std::string, std::vector<float>> cache;
-  char key[160];
-  snprintf(key, sizeof key, "N%d_n%d_nc%d_nw%d_sp%lld_d%d%d_l%d_v%d", h->N, h->n, h->nc, h->nw,
-           h->sp_ri ? 1LL : 0LL, h->spT_dense ? 1 : 0, h->vk_dense ? 1 : 0, h->Lh ? 1 : 0,
-           h->sp_rv ? 1 : 0);
+  char key[200];
+  snprintf(key, sizeof key, "N%d_n%d_nc%d_nw%d_sp%lld_d%d%d%d_l%d_v%d_p%d%d%d", h->N, h->n, h->nc,
+           h->nw, h->sp_ri ? 1LL : 0LL, h->sp_dense ? 1 : 0, h->spT_dense ? 1 : 0,
+           h->vk_dense ? 1 : 0, h->Lh ? 1 : 0, h->sp_rv ? 1 : 0, h->sp_path[0], h->sp_path[1],
+           h->sp_path[2]);
   {
     std::lock_guard<std::mutex> lk(mu);
     auto it = cache.find(key);
     if (it != cache.end()) {
+      const std::vector<float>& c = it->second;
       for (int i = 0; i < afq_handle::F64_N; i++) {
-        h->f64cfg[i] = (int)it->second[3 * i];
-        h->f64ms[i][0] = it->second[3 * i + 1];
-        h->f64ms[i][1] = it->second[3 * i + 2];
+        h->f64cfg[i] = (int)c[3 * i];
+        h->f64ms[i][0] = c[3 * i + 1];
+        h->f64ms[i][1] = c[3 * i + 2];
       }
+      const size_t o = 3 * afq_handle::F64_N;
+      int dense[afq_handle::SP_N];
+      for (int i = 0; i < afq_handle::SP_N; i++) {
+        dense[i] = (int)c[o + 3 * i];
+        h->sp_ms[i][0] = c[o + 3 * i + 1];
+        h->sp_ms[i][1] = c[o + 3 * i + 2];
+      }
+      h->vhsd_cfg = (int)c[o + 3 * afq_handle::SP_N];
+      keep_paths(h, dense);
       return cudaSuccess;
     }
   }
@@ -519,48 +621,89 @@ cudaError_t fp64_tune(afq_handle* h) {
     std::sort(t, t + 3);
     return t[1];
   };
-  auto pick = [&](int site, int ncfg, const std::function<cudaError_t(int)>& run) {
-    float best = -1.0f, rule = -1.0f;
-    int bc = 0;
+  struct Best {
+    int cfg = 0;
+    float ms = -1.0f, rule = -1.0f;
+  };
+  auto fastest = [&](int ncfg, const std::function<cudaError_t(int)>& run) {
+    Best b;
     for (int c = 0; c <= ncfg; c++) {
-      const float t = timed([&] { return run(c); }, best > 0.0f ? 3.0f * best : 1e30f);
-      if (c == 0) rule = t;
-      if (t > 0.0f && (best < 0.0f || t < best)) {
-        best = t;
-        bc = c;
+      const float t = timed([&] { return run(c); }, b.ms > 0.0f ? 3.0f * b.ms : 1e30f);
+      if (c == 0) b.rule = t;
+      if (t > 0.0f && (b.ms < 0.0f || t < b.ms)) {
+        b.ms = t;
+        b.cfg = c;
       }
     }
-    h->f64cfg[site] = bc;
-    h->f64ms[site][0] = best > 0.0f ? best : 0.0f;
-    h->f64ms[site][1] = rule > 0.0f ? rule : 0.0f;
+    return b;
   };
-  pick(afq_handle::F64_VHS, afq::kCsrWalkerCfgs, [&](int c) {
-    return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, N * N, nw, h->vHS,
-                                  (long long)N * N, h->st, c);
-  });
+  auto pick = [&](int site, int ncfg, const std::function<cudaError_t(int)>& run) {
+    const Best b = fastest(ncfg, run);
+    h->f64cfg[site] = b.cfg;
+    h->f64ms[site][0] = b.ms > 0.0f ? b.ms : 0.0f;
+    h->f64ms[site][1] = b.rule > 0.0f ? b.rule : 0.0f;
+    return b;
+  };
+  // dense or CSR for each sparse operand: the faster of the two best shapes
+  int dense[afq_handle::SP_N] = {0, 0, 0};
+  auto choose = [&](int op, float t_csr, float t_dense) {
+    h->sp_ms[op][0] = t_csr > 0.0f ? t_csr : 0.0f;
+    h->sp_ms[op][1] = t_dense > 0.0f ? t_dense : 0.0f;
+    dense[op] = t_dense > 0.0f && (t_csr <= 0.0f || t_dense < t_csr);
+  };
+  {
+    const Best bc = pick(afq_handle::F64_VHS, afq::kCsrWalkerCfgs, [&](int c) {
+      return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, N * N, nw, h->vHS,
+                                    (long long)N * N, h->st, c);
+    });
+    Best bd;
+    if (h->sp_dense) {
+      bd = fastest(kZgCfgs, [&](int c) { return dense_vhs(h, c); });
+      h->vhsd_cfg = bd.cfg;
+    }
+    choose(afq_handle::SP_SPVN, bc.ms, bd.ms);
+  }
   pick(afq_handle::F64_PROP, kZgCfgs, [&](int c) {   // T2 = (i/k) V T1 of every walker
     ZGemmDesc g{N, n2, N, h->vHS, N, (long long)N * N, h->T1, n2, (long long)N * n2, zmk(0, 1)};
     EpiStore ep{h->T2, n2, (long long)N * n2, zmk(0, 0), 0};
     return zgemm_launch<true, false>(g, nw, ep, h->st, c);
   });
-  if (h->spT_dense)
-    pick(afq_handle::F64_VBIAS, kZgCfgs, [&](int c) {
-      ZGemmDesc g{h->nc, nw, nak, h->spT_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
-      EpiStore ep{h->vbias, nw, 0, zmk(0, 0), 0};
-      return zgemm_launch<true, true>(g, 1, ep, h->st, c);
-    });
+  if (h->sp_path[afq_handle::SP_SPVNT] >= 0) {
+    Best bd, bc;
+    if (h->spT_dense)
+      bd = pick(afq_handle::F64_VBIAS, kZgCfgs, [&](int c) {
+        ZGemmDesc g{h->nc, nw, nak, h->spT_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+        EpiStore ep{h->vbias, nw, 0, zmk(0, 0), 0};
+        return zgemm_launch<true, true>(g, 1, ep, h->st, c);
+      });
+    if (h->spT_ri)
+      bc = fastest(0, [&](int) {
+        return launch_csr_gather(h->spT_ri, h->spT_ci, h->spT_v, h->Gc, h->NAK, h->nc, nw,
+                                 h->vbias, h->st);
+      });
+    choose(afq_handle::SP_SPVNT, bc.ms, bd.ms);
+  }
   if (h->Lh && h->cvec)
     pick(afq_handle::F64_COUL, kZgCfgs, [&](int c) {
       ZGemmDesc g{h->nc, nw, nak, h->Lh, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
       EpiStore ep{h->cvec, nw, 0, zmk(0, 0), 0};
       return zgemm_launch<true, true>(g, 1, ep, h->st, c);
     });
-  if (h->vk_dense && h->Gcloc)
-    pick(afq_handle::F64_VAKBL, kZgCfgs, [&](int c) {
-      ZGemmDesc g{nak, nw, nak, h->vk_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
-      EpiStore ep{h->Gcloc, nw, 0, zmk(0, 0), 0};
-      return zgemm_launch<true, true>(g, 1, ep, h->st, c);
-    });
+  if (h->sp_path[afq_handle::SP_VAKBL] >= 0 && h->Gcloc) {
+    Best bd, bc;
+    if (h->vk_dense)
+      bd = pick(afq_handle::F64_VAKBL, kZgCfgs, [&](int c) {
+        ZGemmDesc g{nak, nw, nak, h->vk_dense, h->NAK, 0, h->Gc, h->NAK, 0, zmk(1, 0)};
+        EpiStore ep{h->Gcloc, nw, 0, zmk(0, 0), 0};
+        return zgemm_launch<true, true>(g, 1, ep, h->st, c);
+      });
+    if (h->vk_ri)
+      bc = fastest(0, [&](int) {
+        return launch_csr_gather(h->vk_ri, h->vk_ci, h->vk_v, h->Gc, h->NAK, nak, nw, h->Gcloc,
+                                 h->st);
+      });
+    choose(afq_handle::SP_VAKBL, bc.ms, bd.ms);
+  }
   for (auto& x : ev)
     if (x) cudaEventDestroy(x);
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
@@ -579,6 +722,13 @@ cudaError_t fp64_tune(afq_handle* h) {
     rec.push_back(h->f64ms[i][0]);
     rec.push_back(h->f64ms[i][1]);
   }
+  for (int i = 0; i < afq_handle::SP_N; i++) {
+    rec.push_back((float)dense[i]);
+    rec.push_back(h->sp_ms[i][0]);
+    rec.push_back(h->sp_ms[i][1]);
+  }
+  rec.push_back((float)h->vhsd_cfg);
+  keep_paths(h, dense);
   std::lock_guard<std::mutex> lk(mu);
   cache[key] = rec;
   return cudaSuccess;
@@ -694,6 +844,7 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
   if ((s = check_csr(h, SpvnT, nc, NAK, "SpvnT")) != AFQ_OK) return s;
   if (Vakbl && (s = check_csr(h, Vakbl, NAK, NAK, "Vakbl")) != AFQ_OK) return s;
   cudaSetDevice(h->d.device);
+  const bool mixed_form = h->d.precision == AFQ_PREC_MIXED;
   // Spvn: keep real values only when every imaginary part is zero
   {
     long long nnz = Spvn->rowIndex[N * N];
@@ -713,12 +864,24 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
       AFQ_CUDA(h, dalloc(h, &h->sp_v, nnz));
       AFQ_CUDA(h, cudaMemcpy(h->sp_v, Spvn->vals, sizeof(z_t) * nnz, cudaMemcpyHostToDevice));
     }
+    if (!mixed_form) {   // the dense-tile candidate of the vHS product
+      AFQ_CUDA(h, cudaDeviceSynchronize());
+      h->sp_path[afq_handle::SP_SPVN] = 0;
+      h->sp_density[afq_handle::SP_SPVN] = (double)nnz / ((double)N * N * nc);
+      if ((s = densify(h, h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, N * N, nc,
+                       h->sp_density[afq_handle::SP_SPVN], &h->sp_dense)) != AFQ_OK)
+        return s;
+    }
   }
-  if ((s = upload_csr(h, SpvnT, &h->spT_ri, &h->spT_ci, &h->spT_v, &h->spT_dense, true)) != AFQ_OK)
+  if ((s = upload_csr(h, SpvnT, &h->spT_ri, &h->spT_ci, &h->spT_v, &h->spT_dense, true,
+                      !mixed_form, &h->sp_density[afq_handle::SP_SPVNT])) != AFQ_OK)
     return s;
+  if (!mixed_form) h->sp_path[afq_handle::SP_SPVNT] = 0;
   if (Vakbl) {
-    if ((s = upload_csr(h, Vakbl, &h->vk_ri, &h->vk_ci, &h->vk_v, &h->vk_dense, true)) != AFQ_OK)
+    if ((s = upload_csr(h, Vakbl, &h->vk_ri, &h->vk_ci, &h->vk_v, &h->vk_dense, true,
+                        !mixed_form, &h->sp_density[afq_handle::SP_VAKBL])) != AFQ_OK)
       return s;
+    if (!mixed_form) h->sp_path[afq_handle::SP_VAKBL] = 0;
     AFQ_CUDA(h, dalloc(h, &h->Gcloc, (size_t)NAK * h->nw));
     h->have_vakbl = true;
   }
@@ -1329,6 +1492,18 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms) {
     if (ms) {
       ms[2 * afq::TS_N + 2 * i] = h->f64ms[i][0];
       ms[2 * afq::TS_N + 2 * i + 1] = h->f64ms[i][1];
+    }
+  }
+  return AFQ_OK;
+}
+
+afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms) {
+  if (!h || (!path && !ms)) return AFQ_ERR_ARG;
+  for (int i = 0; i < afq_handle::SP_N; i++) {
+    if (path) path[i] = h->sp_path[i];
+    if (ms) {
+      ms[2 * i] = h->sp_ms[i][0];
+      ms[2 * i + 1] = h->sp_ms[i][1];
     }
   }
   return AFQ_OK;

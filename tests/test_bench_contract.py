@@ -84,3 +84,38 @@ def test_vhs_flop_model():
     N, nc, nw = cfg.nmo, cfg.nchol, 1024
     # real Spvn x complex X over the N(N+1)/2 symmetric orbital pairs: 4 FLOP each
     assert bench.mixed_stage_flops(cfg, nw, "vHS") == 4.0 * nw * (N * (N + 1) // 2) * nc
+
+
+def test_propagation_roofline_models():
+    """Algorithmic work of one propagation: 16 N^2 n complex multiply-adds per walker at
+    Taylor order 6; compulsory bytes: V once (hi + lo), the packed P W operand in, the FP64
+    walkers and their two packed forms out.  At C4 the FLOP bound is the larger one."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from miniafqmc_b200.synthetic import CONFIGS
+    cfg = CONFIGS["C4"]
+    N, n = cfg.nmo, cfg.nel
+    assert bench.prop_flops(cfg, 1) == 8.0 * 16 * N * N * n
+    V, Fp, T1, W64 = 2 * N * 2 * N * 2, 4 * n * N * 2, 2 * n * 2 * N * 4, N * 2 * n * 16
+    assert bench.prop_compulsory_bytes(cfg, 1) == V + 2 * Fp + W64 + T1 + 2 * Fp
+    assert bench.prop_compulsory_bytes(cfg, 1) < bench.mixed_propagate_bytes(cfg, 1) / 5
+    assert bench.prop_flops(cfg, 1) / 1314.4e12 > bench.prop_compulsory_bytes(cfg, 1) / 6545.6e9
+
+
+def test_blocking_sigma():
+    """Blocking analysis (Flyvbjerg-Petersen): white noise gives the naive standard error;
+    an AR(1) series with correlation time tau gives about sqrt(2 tau) times more."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import numpy as np
+    rng = np.random.default_rng(1)
+    x = rng.normal(size=4096)
+    s, lev = bench.blocking_sigma(x)
+    assert len(lev) == 10 and abs(lev[0] - x.std(ddof=1) / 64) < 1e-12
+    assert 0.8 < s / lev[0] < 1.3
+    phi = 0.9                                  # tau_int = (1 + phi) / (1 - phi) / 2 = 9.5
+    y = np.zeros(8192)
+    for i in range(1, len(y)):
+        y[i] = phi * y[i - 1] + rng.normal()
+    s, lev = bench.blocking_sigma(y)
+    assert 3.0 < s / lev[0] < 5.5             # sqrt(2 tau_int) = 4.36

@@ -146,3 +146,21 @@ def test_sigma_from_host_buffer():
     assert rel(g.copy_out("X"), o.copy_out("X")) < TOL
     assert rel(g.copy_out("hybridW"), o.copy_out("hybridW")) < TOL
     g.close()
+
+
+@pytest.mark.parametrize("tune", ["0", "1"])
+def test_stages_dense_tile_spvn(tune, monkeypatch):
+    """Spvn at 30% density: the built-in rule (AFQ_TUNE=0) multiplies it as a dense tile
+    (vHS by ZGEMM over the densified operand), and the set-up tuner picks the faster of
+    the dense and CSR products; either way every stage equals the oracle's."""
+    from miniafqmc_b200.afqmc import AfqmcSys
+    monkeypatch.setenv("AFQ_TUNE", tune)
+    s = system("C1", density=0.3, nchol=128)
+    e = AfqmcSys(s, 16)
+    paths = e.sparse_paths()
+    e.close()
+    if tune == "0":
+        assert paths["Spvn"]["path"] == "dense" and paths["SpvnT"]["path"] == "dense"
+    else:
+        assert paths["Spvn"]["ms"][0] > 0 and paths["Spvn"]["ms"][1] > 0
+    check_stages(s, 16)

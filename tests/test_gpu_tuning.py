@@ -113,7 +113,9 @@ def test_timed_choice_cached_per_shape(tmp_path, monkeypatch):
 def test_fp64_shapes_do_not_change_results(kw, monkeypatch):
     """FP64 form: the tuner's CTA / tile shapes (CSR vHS, ZGEMM propagation, dense vbias,
     Coulomb and Vakbl) sum every output in the same order, so a tuned handle and one on
-    the built-in rules (AFQ_TUNE=0) give bit-identical walkers and energies."""
+    the built-in rules (AFQ_TUNE=0) give bit-identical walkers and energies when both
+    multiply each sparse operand the same way (dense tile or CSR); when the tuner measured
+    the other product faster for some operand, only the summation order differs (1e-12)."""
     from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64
     s = system("C1", **kw)
     nw = 16
@@ -130,13 +132,21 @@ def test_fp64_shapes_do_not_change_results(kw, monkeypatch):
             e.substep(4, st, 5, graph=True)
         e.calculate_mixed_density_matrix()
         out[tune] = (e.get_walkers(), e.calculate_energy("chol"), e.calculate_energy("vakbl"),
-                     e.tuning())
+                     e.tuning(), e.sparse_paths())
         e.close()
-    (W0, D0), ec0, ev0, t0 = out["0"]
-    (W1, D1), ec1, ev1, t1 = out[None]
+    (W0, D0), ec0, ev0, t0, p0 = out["0"]
+    (W1, D1), ec1, ev1, t1, p1 = out[None]
     assert all(v["shape"] == 0 for v in t0.values())
     assert t1["vhs_csr"]["ms"][0] > 0 and t1["propagate_zgemm"]["ms"][0] > 0
     if kw:   # dense SpvnT above the density threshold
         assert t1["vbias_zgemm"]["ms"][0] > 0
-    assert np.array_equal(W0, W1) and np.array_equal(D0, D1)
-    assert ec0 == ec1 and ev0 == ev1
+    # the rule: dense at 25% density and above
+    assert p0["Spvn"]["path"] == ("dense" if kw else "csr")
+    # the tuner timed both products of every operand dense enough for a dense copy
+    assert p1["SpvnT"]["ms"][0] > 0 and p1["SpvnT"]["ms"][1] > 0
+    if [v["path"] for v in p0.values()] == [v["path"] for v in p1.values()]:
+        assert np.array_equal(W0, W1) and np.array_equal(D0, D1)
+        assert ec0 == ec1 and ev0 == ev1
+    else:
+        assert rel(W1, W0) < 1e-12 and rel(D1, D0) < 1e-12
+        assert abs(ec1 - ec0) < 1e-12 * abs(ec0) and abs(ev1 - ev0) < 1e-12 * abs(ev0)
