@@ -172,6 +172,9 @@ afq_status afq_energy_sums(afq_handle* h, int mode, double* sums);
  * step_tot > 0 && step_tot % northo == 0.  Asynchronous. */
 afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int northo);
 
+/* Waits for the handle's work.  AFQ_ERR_CUDA when a tensor-core kernel's pipeline wait
+ * timed out since the last call (afq_set_tc_wait_limit); the flags are cleared once
+ * reported, so the next calls run normally. */
 afq_status afq_synchronize(afq_handle* h);
 
 /* Learned control variate for the exchange energy (no reference counterpart).  A
@@ -314,6 +317,15 @@ afq_status afq_halfrotate(int device, const afq_csr_z* Spvn, int nmo, int naea, 
  * warpgroups.  *kernel_err receives the kernel's timeout flags (0 when clean). */
 afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn, int mode,
                                 const float* A, const float* B, float* C, int* kernel_err);
+/* Bound, in SM clocks, of the tensor-core kernels' pipeline waits on `device` (no
+ * reference counterpart; the reference has no device code).  Each wait of a kernel's TMA
+ * producer, MMA issuer and epilogue gives up after this many clocks, sets a timeout flag
+ * (reported, then cleared, by afq_synchronize) and ends the kernel's work; the kernel still
+ * waits, with the default bound, for the copies and MMAs it has issued before it frees its
+ * tensor memory.  clocks <= 0 restores the default (2e9 clocks, about one second).  Meant
+ * for tests of the timeout path and for watchdogs; it applies to every handle on the
+ * device, so set it while no other work of this library runs there. */
+afq_status afq_set_tc_wait_limit(int device, long long clocks);
 
 #ifdef __cplusplus
 }

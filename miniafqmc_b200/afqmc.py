@@ -37,6 +37,7 @@ EXPORTS = [
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
     "afq_mixed_density_matrix_full", "afq_vbias_full", "afq_get_sparse_paths",
+    "afq_set_tc_wait_limit",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -97,6 +98,7 @@ def signatures() -> dict:
         "afq_population_control": ([P, U64, U64], I),
         "afq_mixed_density_matrix_full": ([P], I), "afq_vbias_full": ([P], I),
         "afq_get_sparse_paths": ([P, P, P], I),
+        "afq_set_tc_wait_limit": ([I, ctypes.c_longlong], I),
     }
 
 

@@ -36,6 +36,10 @@ struct CvConfig {
   int subset_den = 8;                     // exact exchange on nw / subset_den walkers
   int iters_warm = 200, iters_online = 20;
   int batch_online = 1024;                // samples per online Adam step (a window of the buffer)
+  // subset design: 0 = simple random sample of m walkers (inclusion m / nw); 1 = systematic
+  // sample of m teeth with probability proportional to the walker weight, over the walkers
+  // ordered by the surrogate's prediction (implicit stratification)
+  int sampling = 1;
 };
 
 struct CvState;

@@ -57,6 +57,9 @@ int mixed_launches(const MixedState* m, int stage);
 int mixed_nblk(const MixedState* m);
 // Timeout flags raised by the tensor-core kernels (0 when clean).
 cudaError_t mixed_error(MixedState* m, int* flags);
+// Work-wait bound of this module's tensor-core kernels on the current device (SM clocks;
+// <= 0 restores the default of about one second).
+cudaError_t mixed_set_wait_clocks(long long clocks);
 // Kernel choices: choice[TS_N + 1] (0 built-in rule, 1 persistent, 2 per-tile; the last
 // entry is the split-K slice count), ms[TS_N][2] the set-up timings (0 when not timed).
 void mixed_tuning(const MixedState* m, int* choice, float* ms);

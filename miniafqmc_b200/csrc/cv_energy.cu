@@ -6,12 +6,15 @@
 //     E_1 = Gc_w.haj, log|ovlp_a ovlp_b| and its phase, and the linearised exchange
 //     Q.Gc_w (Re, Im), Q = dE_K/dG at the first measurement's mean G;
 //   surrogate f_w = MLP(features) on every walker;
-//   exact exchange E_K on a seeded random subset S of m = ceil(nw / subset_den) walkers
-//     (all walkers until the first train_walker_steps exact samples are in);
-//   sum_w w_w eloc_w = sum_w w_w (E1 + EJ)_w - [sum_w w_w f_w + (nw/m) sum_{w in S} w_w (EK_w - f_w)]
-//     which is unbiased for the exact weighted energy (Horvitz-Thompson correction of the
-//     surrogate on a without-replacement sample with inclusion probability m/nw), whatever
-//     the network predicts;
+//   exact exchange E_K on a seeded subset S drawn with m = ceil(nw / subset_den) teeth
+//     (all walkers until the first train_walker_steps exact samples are in): by default a
+//     systematic sample with probability proportional to the walker weight over the
+//     walkers ordered by f, so walker w gets m w_w / T teeth on average (T = sum of the
+//     weights), and
+//       sum_w w_w eloc_w = sum_w w_w (E1 + EJ)_w - [sum_w w_w f_w + (T/m) sum_teeth (EK - f)]
+//     (AFQ_CV_SAMPLING=0: a simple random sample of m walkers and the correction
+//     (nw/m) sum_{w in S} w_w (EK_w - f_w));  either way unbiased for the exact weighted
+//     energy whatever the network predicts (Horvitz-Thompson);
 //   W_data[:,0] holds exact energies on S and E1 + EJ - f elsewhere;
 //   the exact (features, E_K) pairs of S enter a replay buffer of raw values and the
 //     network takes a few Adam steps on it -- after the estimate, so the estimate never
@@ -46,6 +49,10 @@ struct CvState {
   float *raw_x = nullptr, *raw_t = nullptr, *buf_x = nullptr, *buf_t = nullptr;
   double *e1ej = nullptr, *ek_sub = nullptr, *d_sums = nullptr, *h_sums = nullptr;
   int *d_sub = nullptr, *member = nullptr, *h_sub = nullptr;
+  // weight-proportional design: per member, its number of teeth and teeth * T / m
+  int *d_cnt = nullptr, *h_cnt = nullptr;
+  double *d_mult = nullptr, *h_mult = nullptr, *d_wt = nullptr, *h_wt = nullptr;
+  float* h_f = nullptr;
   z_t* Gc_sub = nullptr;
   int sub_cap = 0, cap = 0, buf_n = 0, buf_head = 0;
   // standardisation: features (mu, sd); targets E_K = ref + mu_r + sd_r * y
@@ -281,16 +288,26 @@ __global__ void cv_append_kernel(const float* __restrict__ feats, const int* __r
   }
 }
 
+// Re W_data[w][1] of every walker (the weights the subset design draws by).
+__global__ void cv_weights_kernel(const z_t* __restrict__ Wd, int nw, double* __restrict__ wt) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x)
+    wt[w] = Wd[(long long)w * 8 + 1].x;
+}
+
 // Assembles W_data[:,0] and the weighted sums of the estimator (one CTA, fixed order).
-// sums = [numerator, sum of weights, sum_S x, sum_S x^2] with x = w (E_K - f) on the
-// subset (the terms of the Horvitz-Thompson correction, for its sampling variance).
+// Simple random sample (mult == null): sums = [numerator, sum of weights, sum_S x,
+// sum_S x^2] with x = w (E_K - f) on the subset (the terms of the Horvitz-Thompson
+// correction, for its sampling variance).  Weight-proportional teeth (mult != null,
+// member i drawn cnt[i] times, mult[i] = cnt[i] T / m): the correction is
+// sum_S mult (E_K - f), and sums[2..3] = sum_S cnt r, sum_S cnt r^2 with r = E_K - f.
 __global__ void __launch_bounds__(1024)
 cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
                    const double* __restrict__ e1ej, const double* __restrict__ ek,
                    const float* __restrict__ fpred, double f0, double fs,
+                   const int* __restrict__ cnt, const double* __restrict__ mult,
                    z_t* __restrict__ Wd, double* __restrict__ sums) {
   __shared__ z_t red[32];
-  double A = 0.0, Bc = 0.0, Wt = 0.0, B2 = 0.0;
+  double A = 0.0, Bc = 0.0, Wt = 0.0, B2 = 0.0, Wt2 = 0.0;
   for (int w = threadIdx.x; w < nw; w += blockDim.x) {
     const double* p = e1ej + (long long)w * 4;
     const int i = member[w];
@@ -302,9 +319,15 @@ cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
     const double om = Wd[(long long)w * 8 + 1].x;
     if (active) {
       A += om * (p[0] + p[2] - f);
-      if (i >= 0) {
+      if (i >= 0 && mult) {
+        const double r = ek[2 * i] - f;
+        Bc += mult[i] * r;
+        Wt2 += cnt[i] * r;
+        B2 += cnt[i] * r * r;
+      } else if (i >= 0) {
         const double x = om * (ek[2 * i] - f);
         Bc += x;
+        Wt2 += x;
         B2 += x * x;
       }
     } else {
@@ -314,10 +337,11 @@ cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
   }
   const z_t ab = block_zsum(zmk(A, Bc), red);
   const z_t wt = block_zsum(zmk(Wt, B2), red);
+  const z_t s2 = block_zsum(zmk(Wt2, 0.0), red);
   if (threadIdx.x == 0) {
-    sums[0] = active ? ab.x - ((double)nw / (double)m) * ab.y : ab.x;
+    sums[0] = !active ? ab.x : mult ? ab.x - ab.y : ab.x - ((double)nw / (double)m) * ab.y;
     sums[1] = wt.x;
-    sums[2] = active ? ab.y : 0.0;
+    sums[2] = active ? s2.x : 0.0;
     sums[3] = active ? wt.y : 0.0;
   }
 }
@@ -335,6 +359,47 @@ void sample_subset(unsigned long long seed, long long meas, int nw, int m, int* 
   }
   std::sort(idx.begin(), idx.begin() + m);
   for (int i = 0; i < m; i++) out[i] = idx[i];
+}
+
+// Systematic sample with probability proportional to weight: the walkers are ordered by
+// their surrogate prediction f (ties by index), weights clipped at zero are summed in that
+// order (total T), and m teeth at (j + u) T / m pick the walkers whose cumulative weight
+// first exceeds them.  Walker w is expected to get m w / T teeth whatever u is, so
+// (T / m) sum over teeth of (E_K - f) is unbiased for sum_w w (E_K - f); ordering by f
+// stratifies the sample.  Writes the distinct members in increasing walker order with
+// their teeth counts and weights cnt T / m; returns how many there are (0: no weight).
+int sample_pps(unsigned long long seed, long long meas, int nw, int m, const float* f,
+               const double* w, int* out, int* cnt, double* mult, double* total) {
+  std::vector<int> order(nw);
+  for (int i = 0; i < nw; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return f[a] < f[b]; });
+  std::vector<double> C(nw);
+  double T = 0.0;
+  for (int i = 0; i < nw; i++) {
+    T += std::max(w[order[i]], 0.0);
+    C[i] = T;
+  }
+  *total = T;
+  if (!(T > 0.0)) return 0;
+  uint32_t c[4] = {0u, 0x50505331u, (uint32_t)meas, (uint32_t)(meas >> 32)};
+  philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+  const double u = (double)(((uint64_t)(c[0] >> 5) << 26) | (c[1] >> 6)) * (1.0 / 9007199254740992.0);
+  std::vector<int> teeth(nw, 0);
+  int i = 0;
+  for (int j = 0; j < m; j++) {
+    const double t = ((double)j + u) * T / m;
+    while (i < nw - 1 && !(C[i] > t)) i++;
+    teeth[order[i]]++;
+  }
+  int k = 0;
+  for (int v = 0; v < nw; v++)
+    if (teeth[v] > 0) {
+      out[k] = v;
+      cnt[k] = teeth[v];
+      mult[k] = teeth[v] * T / m;
+      k++;
+    }
+  return k;
 }
 
 // Scale of a column: its standard deviation, floored so constant columns (identical
@@ -399,6 +464,7 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   CvState* s = new CvState();
   s->cfg = cfg;
   if (const char* it = getenv("AFQ_CV_ITERS")) s->cfg.iters_online = std::max(1, atoi(it));
+  if (const char* sm = getenv("AFQ_CV_SAMPLING")) s->cfg.sampling = atoi(sm) == 0 ? 0 : 1;
   s->nw = nw; s->nc = nchol; s->nak = nak;
   s->sub_cap = (nw + cfg.subset_den - 1) / cfg.subset_den;
   s->cap = std::max(4096, nw);
@@ -422,11 +488,18 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   A(cmal(s, &s->d_sums, 4));
   A(cmal(s, &s->d_sub, nw));
   A(cmal(s, &s->member, nw));
+  A(cmal(s, &s->d_cnt, nw));
+  A(cmal(s, &s->d_mult, nw));
+  A(cmal(s, &s->d_wt, nw));
   A(cmal(s, &s->Gc_sub, (size_t)s->sub_cap * nak));
   A(cmal(s, &s->Q, (size_t)nak));
   if (e == cudaSuccess) e = cudaMemsetAsync(s->Q, 0, sizeof(z_t) * nak, st);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sums, sizeof(double) * 4);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_cnt, sizeof(int) * nw);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_mult, sizeof(double) * nw);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_wt, sizeof(double) * nw);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->h_f, sizeof(float) * nw);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_loss, sizeof(float));
   if (e == cudaSuccess) {   // lowest priority: the step's own kernels go first
     int lo = 0, hi = 0;
@@ -460,6 +533,10 @@ void cv_destroy(CvState* s) {
   if (s->tst) cudaStreamDestroy(s->tst);
   if (s->h_sub) cudaFreeHost(s->h_sub);
   if (s->h_sums) cudaFreeHost(s->h_sums);
+  if (s->h_cnt) cudaFreeHost(s->h_cnt);
+  if (s->h_mult) cudaFreeHost(s->h_mult);
+  if (s->h_wt) cudaFreeHost(s->h_wt);
+  if (s->h_f) cudaFreeHost(s->h_f);
   for (void* p : s->allocs) cudaFree(p);
   delete s;
 }
@@ -540,8 +617,37 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   s->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   s->active = s->trained && !s->failed;
-  const int m = s->active ? s->sub_cap : nw;
+  const int m_design = s->active ? s->sub_cap : nw;   // sample size, or teeth
   if (s->active) {
+    cv_normalize_kernel<<<gridn((long long)nw * CV_NIN, 256), 256, 0, st>>>(
+        s->feats, (long long)nw * CV_NIN, s->d_mu, s->d_sd, s->featn);
+    if ((e = mlp_forward(s->mlp, s->featn, nw, s->fpred, false, st)) != cudaSuccess) return e;
+    s->launches += 2;
+  }
+  bool pps = s->active && s->cfg.sampling == 1;
+  double total_w = 0.0;
+  int m = m_design;   // distinct walkers evaluated exactly
+  if (pps) {   // the design needs the predictions and weights on the host
+    cv_weights_kernel<<<gridn(nw, 256), 256, 0, st>>>(in.Wd, nw, s->d_wt);
+    s->launches++;
+    if ((e = cudaMemcpyAsync(s->h_f, s->fpred, sizeof(float) * nw, cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(s->h_wt, s->d_wt, sizeof(double) * nw, cudaMemcpyDeviceToHost, st)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+      return e;
+    m = sample_pps(s->cfg.seed, s->meas, nw, m_design, s->h_f, s->h_wt, s->h_sub, s->h_cnt,
+                   s->h_mult, &total_w);
+    if (m == 0) pps = false;   // no positive weight: fall back to the simple random sample
+  }
+  if (pps) {
+    if ((e = cudaMemcpyAsync(s->d_cnt, s->h_cnt, sizeof(int) * m, cudaMemcpyHostToDevice, st)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(s->d_mult, s->h_mult, sizeof(double) * m, cudaMemcpyHostToDevice,
+                             st)) != cudaSuccess)
+      return e;
+  } else if (s->active) {
+    m = m_design;
     sample_subset(s->cfg.seed, s->meas, nw, m, s->h_sub);
   } else {
     for (int i = 0; i < nw; i++) s->h_sub[i] = i;
@@ -550,12 +656,6 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   if ((e = cudaMemcpyAsync(s->d_sub, s->h_sub, sizeof(int) * m, cudaMemcpyHostToDevice, st)) !=
       cudaSuccess)
     return e;
-  if (s->active) {
-    cv_normalize_kernel<<<gridn((long long)nw * CV_NIN, 256), 256, 0, st>>>(
-        s->feats, (long long)nw * CV_NIN, s->d_mu, s->d_sd, s->featn);
-    if ((e = mlp_forward(s->mlp, s->featn, nw, s->fpred, false, st)) != cudaSuccess) return e;
-    s->launches += 2;
-  }
   // exact exchange on the subset
   const z_t* gsub = in.Gc;
   if (s->active) {
@@ -569,7 +669,9 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   if ((e = cudaMemsetAsync(s->member, 0xFF, sizeof(int) * nw, st)) != cudaSuccess) return e;
   cv_mark_kernel<<<gridn(m, 256), 256, 0, st>>>(s->d_sub, m, s->member);
   cv_assemble_kernel<<<1, 1024, 0, st>>>(nw, m, s->active ? 1 : 0, s->member, s->e1ej, s->ek_sub,
-                                          s->fpred, s->ref + s->mu_r, s->sd_r, in.Wd, s->d_sums);
+                                          s->fpred, s->ref + s->mu_r, s->sd_r,
+                                          pps ? s->d_cnt : nullptr, pps ? s->d_mult : nullptr,
+                                          in.Wd, s->d_sums);
   s->launches += 3;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if ((e = cudaMemcpyAsync(s->h_sums, s->d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost,
@@ -627,10 +729,16 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   const double* hs = s->h_sums;
   sums[0] = hs[0];
   sums[1] = hs[1];
-  // sampling variance of the weighted mean from the subset correction (without
-  // replacement): nw^2 (1 - m/nw) S_x^2 / m / (sum w)^2
+  // sampling variance of the weighted mean from the subset correction.  Simple random
+  // sample (without replacement): nw^2 (1 - m/nw) S_x^2 / m / (sum w)^2.  Weight-
+  // proportional teeth: the with-replacement bound (T / sum w)^2 S_r^2 / m over the m
+  // teeth (systematic sampling of an ordered population does at least as well)
   s->ht_var = 0.0;
-  if (s->active && m > 1 && hs[1] != 0.0) {
+  if (pps && m_design > 1 && hs[1] != 0.0) {
+    const double md = m_design;
+    const double S2 = (hs[3] - hs[2] * hs[2] / md) / (md - 1);
+    s->ht_var = (total_w / hs[1]) * (total_w / hs[1]) * std::max(S2, 0.0) / md;
+  } else if (s->active && m > 1 && hs[1] != 0.0) {
     const double S2 = (hs[3] - hs[2] * hs[2] / m) / (m - 1);
     s->ht_var = (double)nw * nw * (1.0 - (double)m / nw) * std::max(S2, 0.0) / m / (hs[1] * hs[1]);
   }

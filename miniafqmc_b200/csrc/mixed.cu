@@ -1591,9 +1591,15 @@ void mixed_destroy(MixedState* m) {
 
 int mixed_nblk(const MixedState* m) { return m ? m->ex_mtiles : 0; }
 
+// Timeout flags of the tensor-core kernels since the last call; reading clears them, so
+// one failed call does not condemn the calls after it.
 cudaError_t mixed_error(MixedState* m, int* flags) {
-  return cudaMemcpy(flags, m->err, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaError_t e = cudaMemcpy(flags, m->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && *flags) e = cudaMemset(m->err, 0, sizeof(int));
+  return e;
 }
+
+cudaError_t mixed_set_wait_clocks(long long clocks) { return tc::set_wait_clocks(clocks); }
 
 int mixed_launches(const MixedState* m, int stage) {
   switch (stage) {

@@ -13,7 +13,10 @@
 // (bf16x3), with tf32 parts ~21 bits (3xTF32).
 //
 // Every mbarrier wait is bounded (about one second of SM clocks); on timeout the CTA
-// records an error code in *err, skips its remaining work and still frees its TMEM.
+// records an error code in *err and skips its remaining work.  Before it frees its TMEM
+// and exits it drains its own asynchronous work -- the TMA fills it issued and the MMAs it
+// issued -- with waits that keep the one-second bound whatever the work waits' bound is
+// (g_tc_wait_clocks, which a test may lower to make the work waits run out).
 #pragma once
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -35,8 +38,13 @@ AFQ_D void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
-// Waits for the phase with the given parity to complete; false after ~1 s of clocks.
-AFQ_D bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bound of the work waits in SM clocks (default ~1 s at 1.96 GHz); one copy per
+// translation unit, set with the module's set_wait_clocks.  The drains use kDrainClocks.
+constexpr long long kDrainClocks = 2000000000LL;
+static __device__ long long g_tc_wait_clocks = kDrainClocks;
+
+// Waits for the phase with the given parity to complete; false after `limit` clocks.
+AFQ_D bool mbar_wait_for(uint64_t* bar, uint32_t parity, long long limit) {
   const uint32_t addr = smem_u32(bar);
   const long long t0 = clock64();
   while (true) {
@@ -48,8 +56,23 @@ AFQ_D bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > 2000000000LL) return false;
+    if (clock64() - t0 > limit) return false;
   }
+}
+// A work wait (bounded by g_tc_wait_clocks).
+AFQ_D bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, g_tc_wait_clocks);
+}
+// A drain of the CTA's own asynchronous copies or MMAs before it frees TMEM or exits.
+AFQ_D bool mbar_wait_drain(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, kDrainClocks);
+}
+
+// Host side: sets this translation unit's work-wait bound on the current device
+// (clocks <= 0 restores the default).
+inline cudaError_t set_wait_clocks(long long clocks) {
+  const long long v = clocks > 0 ? clocks : kDrainClocks;
+  return cudaMemcpyToSymbol(g_tc_wait_clocks, &v, sizeof(v));
 }
 AFQ_D void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -201,7 +224,7 @@ struct Cfg {
   static constexpr int PARTS = SPLIT ? 2 : 1;    // hi (and lo) parts of each operand
   static constexpr uint32_t STAGE_BYTES = PARTS * (A_BYTES + B_BYTES);
   static constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
-  static constexpr size_t SMEM = 1024 + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 1) + 16;
+  static constexpr size_t SMEM = 1024 + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 2) + 16;
   static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256, "UMMA N for M=128");
   static_assert(SMEM <= 227 * 1024, "shared memory");
 };
@@ -268,7 +291,8 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * C::STAGE_BYTES);
   uint64_t* empty = full + STAGES;
   uint64_t* done = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* fin = done + 1;          // the issuer's MMAs after it gave up
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // m_fast: M tiles along grid x, so the CTAs that share a B tile run together
@@ -286,6 +310,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
       mbar_init(&empty[s], 1);
     }
     mbar_init(done, 1);
+    mbar_init(fin, 1);
     fence_barrier_init();
   }
   if (warp == 0) {
@@ -300,6 +325,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
   if (warp == 4 && lane == 0) {
     // ---- TMA producer
     const int za = (a_batched && !k_split) ? batch : 0, zb = (b_batched && !k_split) ? batch : 0;
+    int issued = 0;
     for (int kb = 0; kb < nk; kb++) {
       const int kx = kbase + kb * C::BK;
       const int s = kb % STAGES;
@@ -315,7 +341,11 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
         tma_load_3d(stA(s, 1), &maps.a_lo, &full[s], kx, m0, za);
         tma_load_3d(stB(s, 1), &maps.b_lo, &full[s], kx, n0, zb);
       }
+      issued = kb + 1;
     }
+    // the last fills of each stage land before the CTA can exit
+    for (int q = max(0, issued - STAGES); q < issued; q++)
+      mbar_wait_drain(&full[q % STAGES], (q / STAGES) & 1);
   } else if (warp == 5 && lane == 0) {
     // ---- MMA issuer
     constexpr uint32_t ID = idesc(128, BN, FMT);
@@ -345,7 +375,11 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
       }
       umma_commit(&empty[s]);
     }
-    if (ok) umma_commit(done);
+    // every MMA issued above completes before the TMEM is freed: `done` releases the
+    // epilogue; after a timeout `fin` only drains (the epilogue gives up on its own)
+    uint64_t* last = ok ? done : fin;
+    umma_commit(last);
+    mbar_wait_drain(last, 0);
   }
 
   if (warp < 4) {
@@ -509,7 +543,8 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       }
     }
     // the last fills of each stage land before the CTA can exit
-    for (int q = max(0, g - STAGES); q < g; q++) mbar_wait(&full[q % STAGES], (q / STAGES) & 1);
+    for (int q = max(0, g - STAGES); q < g; q++)
+      mbar_wait_drain(&full[q % STAGES], (q / STAGES) & 1);
   } else if (warp == WMMA && lane == 0) {
     // ---- MMA issuer: one accumulator buffer per tile, or per K chunk when promoting
     constexpr uint32_t ID = idesc(128, BN, FMT);
@@ -561,7 +596,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       }
     }
     umma_commit(fin);   // fires once every MMA issued above has completed
-    mbar_wait(fin, 0);
+    mbar_wait_drain(fin, 0);
   }
 
   if constexpr (PK > 0) {

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../include/afqmc_b200.h"
+#include "afq_mixed.h"
 #include "tc_gemm.cuh"
 
 namespace {
@@ -91,4 +92,16 @@ extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int t
   cudaFree(dC);
   cudaFree(derr);
   return s;
+}
+
+extern "C" afq_status afq_set_tc_wait_limit(int device, long long clocks) {
+  int prev = 0;
+  if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess)
+    return AFQ_ERR_ARG;
+  // every module holding tensor-core kernels keeps its own copy of the bound
+  cudaError_t e = tc::set_wait_clocks(clocks);
+  if (e == cudaSuccess) e = afq::mixed_set_wait_clocks(clocks);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaSetDevice(prev);
+  return e == cudaSuccess ? AFQ_OK : AFQ_ERR_CUDA;
 }
