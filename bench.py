@@ -9,7 +9,9 @@ matrix, vbias, sigma, vHS, propagation, overlaps, weights; orthogonalisation eve
 local energy (miniafqmc_base.cpp:341-345).  The workload is the target system: NMO=384,
 48+48 electrons, nchol=1536 Cholesky vectors (20% nonzero), 1024 walkers per GPU,
 synthetic seeded inputs.  Multi-GPU runs shard walkers (weak scaling): each rank holds
-its own 1024 walkers and the per-step Eshift sum and the energy sums are all-reduced.
+its own 1024 walkers; the per-substep Eshift sum is all-reduced on the device (NCCL on the
+handle's stream between the two graph launches of afq_substep_begin / afq_substep_end) and
+the two energy sums on the host at each measurement.
 
 The headline form is mixed precision with the learned control variate (tensor-core
 contractions, FP64 LU/QR/weights, exact exchange on 1/8 of the walkers); at N=1 the plain
@@ -334,8 +336,8 @@ class Form:
 
     def step(self, st, record=True, graph=True):
         from miniafqmc_b200 import driver
-        driver.substep(self.eng, self.cfg.seed, st, self.args.northo, self.comm,
-                       graph=graph and self.comm is None)
+        # sharded runs keep graph substeps with the Eshift sum all-reduced on the device
+        driver.substep(self.eng, self.cfg.seed, st, self.args.northo, self.comm, graph=graph)
         if (st + 1) % self.args.energy_every == 0:
             self.measure(record)
 
@@ -583,7 +585,8 @@ def main():
             t = torch.tensor(vals, dtype=torch.float64, device="cuda")
             dist.all_reduce(t)
             return t.tolist()
-        comm = driver.Comm(rank * nw, world * nw, allreduce)
+        comm = driver.Comm(rank * nw, world * nw, allreduce,
+                           driver.nccl_allreduce_device(torch, dist))
 
     head = Form(s, cfg, args, args.form, local, comm, torch)
     head.measure(record=False)

@@ -171,6 +171,19 @@ afq_status afq_energy_sums(afq_handle* h, int mode, double* sums);
  * propagation, overlaps, weights, and orthogonalization + overlaps when
  * step_tot > 0 && step_tot % northo == 0.  Asynchronous. */
 afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int northo);
+/* The same substep for a walker-sharded ensemble (afq_set_walker_offset), in two CUDA-graph
+ * launches around the one coupling of the ranks (miniafqmc_base.cpp:317-327).  No
+ * reference counterpart: the reference runs one ensemble in one process.
+ * afq_substep_begin runs everything up to the weight update, which uses the current
+ * Eshift, and leaves this block's sum of Re W_data[:,4] in a device double owned by the
+ * handle, whose address it returns in *e4sum (valid in the handle's stream order).  The
+ * caller all-reduces (sums) that double in place across the ranks, ordered on the handle's
+ * stream (for example NCCL on afq_get_stream's stream).  afq_substep_end then sets
+ * Eshift = that sum / nwalk_global on the device and re-orthogonalises when
+ * step_tot > 0 && step_tot % northo == 0.  No host synchronisation; with one rank the
+ * result equals afq_substep bit for bit. */
+afq_status afq_substep_begin(afq_handle* h, uint64_t seed, uint64_t step_tot, double** e4sum);
+afq_status afq_substep_end(afq_handle* h, uint64_t step_tot, int northo);
 
 /* Waits for the handle's work.  AFQ_ERR_CUDA when a tensor-core kernel's pipeline wait
  * timed out since the last call (afq_set_tc_wait_limit); the flags are cleared once

@@ -37,7 +37,7 @@ EXPORTS = [
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
     "afq_mixed_density_matrix_full", "afq_vbias_full", "afq_get_sparse_paths",
-    "afq_set_tc_wait_limit",
+    "afq_set_tc_wait_limit", "afq_substep_begin", "afq_substep_end",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -99,6 +99,7 @@ def signatures() -> dict:
         "afq_mixed_density_matrix_full": ([P], I), "afq_vbias_full": ([P], I),
         "afq_get_sparse_paths": ([P, P, P], I),
         "afq_set_tc_wait_limit": ([I, ctypes.c_longlong], I),
+        "afq_substep_begin": ([P, U64, U64, P], I), "afq_substep_end": ([P, U64, I], I),
     }
 
 
@@ -352,6 +353,17 @@ class AfqmcSys:
         if step_tot > 0 and step_tot % northo == 0:
             self.orthogonalize()
             self.calculate_overlaps(save_old=False)
+
+    def substep_begin(self, seed: int, step_tot: int) -> int:
+        """First half of a walker-sharded substep (afq_substep_begin): returns the device
+        address of the double holding this block's sum of Re W_data[:,4], which the caller
+        all-reduces in place on the handle's stream before substep_end."""
+        p = ctypes.c_void_p()
+        self._check(self.lib.afq_substep_begin(self.h, seed, step_tot, ctypes.byref(p)))
+        return p.value
+
+    def substep_end(self, step_tot: int, northo: int):
+        self._check(self.lib.afq_substep_end(self.h, step_tot, northo))
 
     def synchronize(self):
         self._check(self.lib.afq_synchronize(self.h))

@@ -87,6 +87,12 @@ struct afq_handle {
   afq::CvConfig cv_cfg;
 
   cudaGraphExec_t g_plain = nullptr, g_ortho = nullptr;
+  // sharded substeps: everything up to the weight update (g_begin), the
+  // re-orthogonalisation and its overlaps (g_orth); the local sum of Re W_data[:,4] for the
+  // caller's all-reduce lives in e4buf
+  cudaGraphExec_t g_begin = nullptr, g_orth = nullptr;
+  long long g_begin_launches[AFQ_NSTAGES] = {0}, g_orth_launches[AFQ_NSTAGES] = {0};
+  double* e4buf = nullptr;
   // mixed form: the T1^-1 of the last overlap / density-matrix call matches the current
   // walkers (cleared by propagate, orthogonalise and set_walkers)
   bool dm_cache = false;
@@ -471,16 +477,20 @@ cudaError_t st_energy(afq_handle* h, int mode) {
   return staged(h, AFQ_STAGE_ENERGY, nl, [&] { return body_energy(h, mode); });
 }
 
-cudaError_t st_substep(afq_handle* h, bool ortho) {
+// One substep; part 0 = all of it, 1 = up to the weight update without the Eshift update
+// (sharded: the caller all-reduces the sum first), 2 = the re-orthogonalisation only.
+cudaError_t st_substep(afq_handle* h, bool ortho, int part = 0) {
   cudaError_t e;
-  if ((e = st_dm(h, 1, 0)) != cudaSuccess) return e;
-  if ((e = st_vbias(h)) != cudaSuccess) return e;
-  if ((e = st_sigma(h, 0)) != cudaSuccess) return e;
-  if ((e = st_vhs(h)) != cudaSuccess) return e;
-  if ((e = st_propagate(h)) != cudaSuccess) return e;
-  if ((e = st_dm(h, 0, 1)) != cudaSuccess) return e;
-  if ((e = st_weights(h, 1)) != cudaSuccess) return e;
-  if (ortho) {
+  if (part != 2) {
+    if ((e = st_dm(h, 1, 0)) != cudaSuccess) return e;
+    if ((e = st_vbias(h)) != cudaSuccess) return e;
+    if ((e = st_sigma(h, 0)) != cudaSuccess) return e;
+    if ((e = st_vhs(h)) != cudaSuccess) return e;
+    if ((e = st_propagate(h)) != cudaSuccess) return e;
+    if ((e = st_dm(h, 0, 1)) != cudaSuccess) return e;
+    if ((e = st_weights(h, part == 1 ? 0 : 1)) != cudaSuccess) return e;
+  }
+  if (ortho && part != 1) {
     if ((e = st_ortho(h)) != cudaSuccess) return e;
     if ((e = st_dm(h, 0, 0)) != cudaSuccess) return e;
   }
@@ -494,10 +504,38 @@ afq_status set_scalars(afq_handle* h, uint64_t seed, uint64_t step) {
   return AFQ_OK;
 }
 
+// Captures (once) and launches one substep graph: part as for st_substep.
+afq_status launch_substep_graph(afq_handle* h, cudaGraphExec_t* slot, long long* counts,
+                                bool ortho, int part) {
+  if (!*slot) {
+    cudaGraph_t g = nullptr;
+    AFQ_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
+    h->capturing = true;
+    for (int i = 0; i < AFQ_NSTAGES; i++) counts[i] = 0;
+    h->launch_sink = counts;
+    cudaError_t e = st_substep(h, ortho, part);
+    h->launch_sink = nullptr;
+    h->capturing = false;
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return fail(h, AFQ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+    }
+    AFQ_CUDA(h, e2);
+    e = cudaGraphInstantiate(slot, g, 0);
+    cudaGraphDestroy(g);
+    AFQ_CUDA(h, e);
+  }
+  AFQ_CUDA(h, cudaGraphLaunch(*slot, h->st));
+  for (int i = 0; i < AFQ_NSTAGES; i++) h->stage_launches[i] += counts[i];
+  return AFQ_OK;
+}
+
 void drop_graphs(afq_handle* h) {
-  if (h->g_plain) cudaGraphExecDestroy(h->g_plain);
-  if (h->g_ortho) cudaGraphExecDestroy(h->g_ortho);
-  h->g_plain = h->g_ortho = nullptr;
+  for (cudaGraphExec_t* g : {&h->g_plain, &h->g_ortho, &h->g_begin, &h->g_orth}) {
+    if (*g) cudaGraphExecDestroy(*g);
+    *g = nullptr;
+  }
 }
 
 // FP64 form: times the tile shapes of its ZGEMM sites and the CTA shapes of the vHS CSR
@@ -1282,30 +1320,41 @@ afq_status afq_substep(afq_handle* h, uint64_t seed, uint64_t step_tot, int nort
   // first when they are stale
   if (h->mixed) AFQ_CUDA(h, afq::mixed_ensure_packed(h->mixed, h->W, h->st));
   if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
-  cudaGraphExec_t* slot = ortho ? &h->g_ortho : &h->g_plain;
-  long long* counts = ortho ? h->g_ortho_launches : h->g_plain_launches;
-  if (!*slot) {
-    cudaGraph_t g = nullptr;
-    AFQ_CUDA(h, cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
-    h->capturing = true;
-    for (int i = 0; i < AFQ_NSTAGES; i++) counts[i] = 0;
-    h->launch_sink = counts;
-    cudaError_t e = st_substep(h, ortho);
-    h->launch_sink = nullptr;
-    h->capturing = false;
-    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
-    if (e != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      return fail(h, AFQ_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
-    }
-    AFQ_CUDA(h, e2);
-    e = cudaGraphInstantiate(slot, g, 0);
-    cudaGraphDestroy(g);
-    AFQ_CUDA(h, e);
-  }
-  AFQ_CUDA(h, cudaGraphLaunch(*slot, h->st));
-  for (int i = 0; i < AFQ_NSTAGES; i++) h->stage_launches[i] += counts[i];
+  if ((s = launch_substep_graph(h, ortho ? &h->g_ortho : &h->g_plain,
+                                 ortho ? h->g_ortho_launches : h->g_plain_launches, ortho, 0)) !=
+      AFQ_OK)
+    return s;
   h->host_step = step_tot + 1;
+  return AFQ_OK;
+}
+
+afq_status afq_substep_begin(afq_handle* h, uint64_t seed, uint64_t step_tot, double** e4sum) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (!e4sum) return fail(h, AFQ_ERR_ARG, "null e4sum");
+  if (seed != h->host_seed || step_tot != h->host_step)
+    if ((s = set_scalars(h, seed, step_tot)) != AFQ_OK) return s;
+  if (!h->e4buf) AFQ_CUDA(h, dalloc(h, &h->e4buf, 1));
+  if (h->mixed) AFQ_CUDA(h, afq::mixed_ensure_packed(h->mixed, h->W, h->st));
+  if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
+  if ((s = launch_substep_graph(h, &h->g_begin, h->g_begin_launches, false, 1)) != AFQ_OK)
+    return s;
+  AFQ_CUDA(h, afq::launch_e4sum_out(h->sc, h->e4buf, h->st));
+  *e4sum = h->e4buf;
+  h->host_step = step_tot + 1;
+  return AFQ_OK;
+}
+
+afq_status afq_substep_end(afq_handle* h, uint64_t step_tot, int northo) {
+  afq_status s = need_ready(h);
+  if (s != AFQ_OK) return s;
+  if (northo <= 0) return fail(h, AFQ_ERR_ARG, "northo must be positive");
+  if (!h->e4buf || h->host_step != step_tot + 1)
+    return fail(h, AFQ_ERR_STATE, "afq_substep_end without afq_substep_begin of that step");
+  AFQ_CUDA(h, afq::launch_eshift_from(h->sc, h->e4buf, h->nw, h->st));
+  h->stage_launches[AFQ_STAGE_WEIGHTS] += 1;
+  if (step_tot > 0 && step_tot % (uint64_t)northo == 0)
+    return launch_substep_graph(h, &h->g_orth, h->g_orth_launches, true, 2);
   return AFQ_OK;
 }
 

@@ -33,6 +33,8 @@ cudaError_t launch_exchange(const z_t* Lh, const z_t* Gc, int N, int n, int ncho
 cudaError_t launch_energy_reduce(const z_t* Gc, const z_t* haj, int nak, const z_t* Gcloc,
                                  const z_t* cv, int nchol, const z_t* Kpart, int nblk, int nw,
                                  int mode, z_t* Wd, double* parts, cudaStream_t st);
+cudaError_t launch_e4sum_out(const DevScalars* sc, double* out, cudaStream_t st);
+cudaError_t launch_eshift_from(DevScalars* sc, const double* total, int nw, cudaStream_t st);
 cudaError_t launch_eav(const z_t* Wd, int nw, DevScalars* sc, cudaStream_t st);
 // Population control by the comb (popcontrol.cu): u = comb_uniform(seed, step, offset of
 // the handle's walker block); C [nw],

@@ -463,6 +463,26 @@ cudaError_t launch_weights(z_t* Wd, const z_t* hybridW, int nw, double dt, DevSc
   return cudaGetLastError();
 }
 
+// Sharded substeps: the last weight update's local sum of Re W_data[:,4] into a device
+// double, and Eshift = (the ensemble's sum, all-reduced in place by the caller) / walkers
+// of the whole ensemble (miniafqmc_base.cpp:327).
+__global__ void e4sum_out_kernel(const DevScalars* __restrict__ sc, double* __restrict__ out) {
+  *out = sc->e4sum;
+}
+__global__ void eshift_from_kernel(DevScalars* __restrict__ sc, const double* __restrict__ total,
+                                   int nw) {
+  const long long ng = sc->nwalk_global > 0 ? sc->nwalk_global : nw;
+  sc->eshift = *total / (double)ng;
+}
+cudaError_t launch_e4sum_out(const DevScalars* sc, double* out, cudaStream_t st) {
+  e4sum_out_kernel<<<1, 1, 0, st>>>(sc, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_eshift_from(DevScalars* sc, const double* total, int nw, cudaStream_t st) {
+  eshift_from_kernel<<<1, 1, 0, st>>>(sc, total, nw);
+  return cudaGetLastError();
+}
+
 __global__ void set_scalars_kernel(DevScalars* sc, unsigned long long seed,
                                    unsigned long long step, int set_eshift, double eshift,
                                    int walker_offset, long long nwalk_global) {

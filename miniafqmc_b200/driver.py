@@ -22,10 +22,14 @@ CHECKPOINT_MAGIC = b"AFQCKP01"
 @dataclasses.dataclass
 class Comm:
     """Walker sharding: this rank holds walkers [offset, offset + nwalk_local) of
-    nwalk_global; allreduce(list[float]) -> list[float] sums across ranks."""
+    nwalk_global; allreduce(list[float]) -> list[float] sums across ranks.  Optional
+    allreduce_device(address, stream): sums one float64 at a device address in place
+    across ranks, ordered on the given CUDA stream (NCCL); with it, graph substeps of an
+    engine that has substep_begin / substep_end keep the Eshift coupling on the device."""
     offset: int
     nwalk_global: int
     allreduce: Callable
+    allreduce_device: Optional[Callable] = None
 
 
 @dataclasses.dataclass
@@ -33,6 +37,24 @@ class RunResult:
     energies: list
     steps: int
     substeps: int
+
+
+class _DeviceDouble:
+    """One float64 at a device address, seen through the CUDA array interface."""
+
+    def __init__(self, addr: int):
+        self.__cuda_array_interface__ = {"shape": (1,), "typestr": "<f8",
+                                         "data": (int(addr), False), "version": 3}
+
+
+def nccl_allreduce_device(torch, dist) -> Callable:
+    """Comm.allreduce_device over torch.distributed (NCCL): the double at `addr` becomes a
+    tensor view (no copy) and is summed across ranks on the engine's stream."""
+    def allreduce_device(addr: int, stream: int):
+        t = torch.as_tensor(_DeviceDouble(addr), device="cuda")
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            dist.all_reduce(t)
+    return allreduce_device
 
 
 def energy(engine, mode: str = "auto", comm: Optional[Comm] = None) -> float:
@@ -48,6 +70,11 @@ def substep(engine, seed: int, step_tot: int, northo: int, comm: Optional[Comm] 
             graph: bool = True):
     if comm is None:
         engine.substep(seed, step_tot, northo, graph=graph)
+        return
+    if graph and comm.allreduce_device is not None and hasattr(engine, "substep_begin"):
+        addr = engine.substep_begin(seed, step_tot)
+        comm.allreduce_device(addr, engine.stream)
+        engine.substep_end(step_tot, northo)
         return
     engine.calculate_mixed_density_matrix()
     engine.get_vbias()
