@@ -89,3 +89,55 @@ def test_sharded_run_matches_single_ensemble(tmp_path):
         tot = np.maximum(p["Wdb"][:, 1].real, 0).sum()
         assert abs(p["Wdc"][:, 1].real.sum() - tot) < 1e-12 * per * max(tot, 1.0)
     assert O.comb_uniform(SEED, 99, 0) != O.comb_uniform(SEED, 99, per)
+
+
+class _DeviceCoupledEngine:
+    """Stand-in engine with the split substep of a device-coupled sharded run: begin
+    leaves this block's e4 sum at an address, end sets Eshift from the summed value."""
+
+    def __init__(self, e4, nwg):
+        self.slots = {7: float(e4)}
+        self.nwg, self.eshift, self.stream = nwg, None, 0
+
+    def substep_begin(self, seed, step):
+        return 7
+
+    def substep_end(self, step, northo):
+        self.eshift = self.slots[7] / self.nwg
+
+
+def _coupled_worker(rank, world, port, out_dir):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        from miniafqmc_b200 import driver
+        eng = _DeviceCoupledEngine(10.0 * (rank + 1), 8)
+
+        def allreduce_device(addr, stream):   # gloo stand-in for the NCCL all-reduce
+            t = torch.tensor([eng.slots[addr]], dtype=torch.float64)
+            dist.all_reduce(t)
+            eng.slots[addr] = float(t.item())
+
+        def host(vals):
+            raise AssertionError("host all-reduce used")
+
+        comm = driver.Comm(rank * 4, 8, host, allreduce_device)
+        driver.substep(eng, 1, 0, 5, comm, graph=True)
+        np.save(os.path.join(out_dir, f"e{rank}.npy"), np.array([eng.eshift]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_device_coupled_substep_driver_logic(tmp_path):
+    """driver.substep with Comm.allreduce_device: begin, one in-place all-reduce of the
+    block sums, end; every rank ends with Eshift = (sum over ranks) / walkers."""
+    world = 2
+    mp.start_processes(_coupled_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    for r in range(world):
+        assert np.load(tmp_path / f"e{r}.npy")[0] == (10.0 + 20.0) / 8
