@@ -688,6 +688,7 @@ def main():
         same["mixed_exact_minus_fp64_Ha"] = emx - e64
         cmp["energy"]["same_walkers"] = same
         cmp["fp64_plain"]["kernel_tuning"] = ref.eng.tuning()
+        cmp["fp64_plain"]["sparse_paths"] = ref.eng.sparse_paths()
         ref.eng.close()
         if head.mode == "cv" and args.acc_substeps > 0:
             cmp["energy"].update(accuracy_pass(s, cfg, args, local, torch))
@@ -780,6 +781,8 @@ def main():
     if head.mode == "cv":
         line["control_variate"] = head.eng.cv_stats()
     line["config"]["kernel_tuning"] = head.eng.tuning()
+    if args.form == "fp64":
+        line["config"]["sparse_paths"] = head.eng.sparse_paths()
     print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
