@@ -40,6 +40,12 @@ struct CvConfig {
   // sample of m teeth with probability proportional to the walker weight, over the walkers
   // ordered by the surrogate's prediction (implicit stratification)
   int sampling = 1;
+  // linearised exchange: Q = dE_K/dG at the weighted-mean G of the first measurement, and
+  // again every q_refresh measurements (0: never again); features 36/37 are the linearised
+  // E_K(G_w) = E_K(Gm) + Q.(G_w - Gm) (Re relative to the first one, Im)
+  int q_refresh = 0;
+  // residual learning: the network predicts E_K minus feature 36 (the linearisation)
+  int residual = 0;
 };
 
 struct CvState;

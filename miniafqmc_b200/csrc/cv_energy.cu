@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "afq_cv.h"
+#include "zgemm_fp64.cuh"
 
 namespace afq {
 
@@ -63,8 +64,12 @@ struct CvState {
   int last_m = 0;
   float last_loss = 0.0f;
   double ht_var = 0.0;
-  z_t* Q = nullptr;      // [2][n][N] linearised exchange, set at the first measurement
+  z_t* Q = nullptr;      // [2][n][N] linearised exchange dE_K/dG at the mean G Gm
   bool have_q = false;
+  long long q_meas = 0;  // measurement of the last Q
+  // Q set-up scratch: Gm [2][n][N], Tq [2][nc][n][n], Qpart [nc][n][N]; qoff = Q.Gm / 2
+  z_t *Gm = nullptr, *Tq = nullptr, *Qpart = nullptr, *d_qoff = nullptr;
+  double lin_ref = 0.0;  // Re of the first linearisation's E_K(Gm)
   // online training runs on its own stream after the estimate, overlapping the next
   // substeps; the next measurement (and any use of the network) waits for ev_trained
   cudaStream_t tst = nullptr;
@@ -103,7 +108,8 @@ __global__ void __launch_bounds__(256)
 cv_features_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, long long nak,
                    const z_t* __restrict__ cvec, int nc, int nw, const z_t* __restrict__ Wd,
                    const float* __restrict__ R, const z_t* __restrict__ Q,
-                   float* __restrict__ feats, double* __restrict__ e1ej) {
+                   const z_t* __restrict__ qoff, double lin_ref, float* __restrict__ feats,
+                   double* __restrict__ e1ej) {
   __shared__ z_t red[8];
   __shared__ float proj[CV_NPROJ];
   const int w = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -141,8 +147,9 @@ cv_features_kernel(const z_t* __restrict__ Gc, const z_t* __restrict__ haj, long
     f[33] = (float)e1.x;
     f[34] = (float)log(fmax(hypot(ov.x, ov.y), 1e-300));
     f[35] = (float)atan2(ov.y, ov.x);
-    f[36] = (float)eq.x;
-    f[37] = (float)eq.y;
+    // linearised exchange E_K(Gm) + Q.(G_w - Gm) = Q.G_w - Q.Gm / 2 (E_K is quadratic)
+    f[36] = (float)(eq.x - qoff->x - lin_ref);
+    f[37] = (float)(eq.y - qoff->y);
     double* o = e1ej + (long long)w * 4;
     o[0] = e1.x; o[1] = e1.y; o[2] = 0.5 * ej.x; o[3] = 0.5 * ej.y;
   }
@@ -163,34 +170,25 @@ __global__ void cv_gmean_kernel(const z_t* __restrict__ Gc, long long nak, int n
     Gm[q] = zscale(s, wt != 0.0 ? 1.0 / wt : 0.0);
   }
 }
-// Tt[s][b][c][a] = sum_k Gm[s][b][k] Lh[c][s][a][k]  (T_c = Lh_c Gm^T, transposed)
-__global__ void cv_qt_kernel(const z_t* __restrict__ Lh, const z_t* __restrict__ Gm, int nc,
-                             int n, int N, z_t* __restrict__ Tt) {
-  const long long tot = 2LL * n * nc * n;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
+// Q[e] = sum over Cholesky vectors c of part[c][e] (fixed order).
+__global__ void cv_qsum_kernel(const z_t* __restrict__ part, int nc, long long per,
+                               z_t* __restrict__ Q) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < per;
        e += (long long)gridDim.x * blockDim.x) {
-    const long long a = e % n, c = (e / n) % nc, b = (e / ((long long)n * nc)) % n,
-                    s = e / ((long long)n * nc * n);
-    const z_t* g = Gm + (s * n + b) * N;
-    const z_t* l = Lh + ((c * 2 + s) * n + a) * N;
     z_t t = zmk(0, 0);
-    for (int k = 0; k < N; k++) zfma(t, g[k], l[k]);
-    Tt[e] = t;
+    for (int c = 0; c < nc; c++) t = zadd(t, part[(long long)c * per + e]);
+    Q[e] = t;
   }
 }
-// Q[s][b][k] = dE_K/dG[s][b][k] = sum_{c,a} T_c[b][a] Lh[c][s][a][k] (E_K = 1/2 sum tr(T T))
-__global__ void cv_q_kernel(const z_t* __restrict__ Lh, const z_t* __restrict__ Tt, int nc,
-                            int n, int N, z_t* __restrict__ Q) {
-  const long long tot = 2LL * n * N;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < tot;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long k = e % N, b = (e / N) % n, s = e / ((long long)n * N);
-    const z_t* t = Tt + (s * n + b) * (long long)nc * n;
-    z_t q = zmk(0, 0);
-    for (int c = 0; c < nc; c++)
-      for (int a = 0; a < n; a++) zfma(q, t[c * n + a], Lh[((long long)(c * 2 + s) * n + a) * N + k]);
-    Q[e] = q;
-  }
+// qoff = Q.Gm / 2 = E_K(Gm) (one CTA, fixed order).
+__global__ void __launch_bounds__(256)
+cv_qoff_kernel(const z_t* __restrict__ Q, const z_t* __restrict__ Gm, long long nak,
+               z_t* __restrict__ qoff) {
+  __shared__ z_t red[8];
+  z_t s = zmk(0, 0);
+  for (long long i = threadIdx.x; i < nak; i += blockDim.x) zfma(s, Q[i], Gm[i]);
+  s = block_zsum(s, red);
+  if (threadIdx.x == 0) *qoff = zscale(s, 0.5);
 }
 
 // Standardised, clipped features: out = clip((f - mu) / sd, +-CV_CLIP_X).
@@ -209,14 +207,16 @@ __global__ void cv_normalize_buffer_kernel(const float* __restrict__ rx,
                                            const float* __restrict__ rt, int n,
                                            const float* __restrict__ mu,
                                            const float* __restrict__ sd, float mu_r, float sd_r,
-                                           float* __restrict__ bx, float* __restrict__ bt) {
+                                           int residual, float* __restrict__ bx,
+                                           float* __restrict__ bt) {
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)n * CV_NIN;
        e += (long long)gridDim.x * blockDim.x) {
     const int q = (int)(e % CV_NIN);
     bx[e] = fminf(fmaxf((rx[e] - mu[q]) / sd[q], -CV_CLIP_X), CV_CLIP_X);
     if (q == 0) {
       const long long b = e / CV_NIN;
-      bt[b] = fminf(fmaxf((rt[b] - mu_r) / sd_r, -CV_CLIP_T), CV_CLIP_T);
+      const float t = rt[b] - (residual ? rx[b * CV_NIN + 36] : 0.0f);
+      bt[b] = fminf(fmaxf((t - mu_r) / sd_r, -CV_CLIP_T), CV_CLIP_T);
     }
   }
 }
@@ -225,11 +225,12 @@ __global__ void cv_normalize_buffer_kernel(const float* __restrict__ rx,
 // one CTA per column, two passes in double, fixed reduction order.
 __global__ void __launch_bounds__(256)
 cv_buffer_stats_kernel(const float* __restrict__ rx, const float* __restrict__ rt, int n,
-                       float* __restrict__ stat) {
+                       int residual, float* __restrict__ stat) {
   __shared__ z_t red[8];
   const int q = blockIdx.x;
   auto val = [&](int b) -> double {
-    return q < CV_NIN ? (double)rx[(long long)b * CV_NIN + q] : (double)rt[b];
+    if (q < CV_NIN) return (double)rx[(long long)b * CV_NIN + q];
+    return (double)rt[b] - (residual ? (double)rx[(long long)b * CV_NIN + 36] : 0.0);
   };
   double s = 0.0;
   for (int b = threadIdx.x; b < n; b += blockDim.x) s += val(b);
@@ -304,14 +305,18 @@ __global__ void __launch_bounds__(1024)
 cv_assemble_kernel(int nw, int m, int active, const int* __restrict__ member,
                    const double* __restrict__ e1ej, const double* __restrict__ ek,
                    const float* __restrict__ fpred, double f0, double fs,
-                   const int* __restrict__ cnt, const double* __restrict__ mult,
-                   z_t* __restrict__ Wd, double* __restrict__ sums) {
+                   const float* __restrict__ fbase, const int* __restrict__ cnt,
+                   const double* __restrict__ mult, z_t* __restrict__ Wd,
+                   double* __restrict__ sums) {
   __shared__ z_t red[32];
   double A = 0.0, Bc = 0.0, Wt = 0.0, B2 = 0.0, Wt2 = 0.0;
   for (int w = threadIdx.x; w < nw; w += blockDim.x) {
     const double* p = e1ej + (long long)w * 4;
     const int i = member[w];
-    const double f = active ? f0 + fs * (double)fpred[w] : 0.0;
+    // surrogate E_K: network output (plus the linearisation it was trained on top of)
+    const double f = active ? f0 + fs * (double)fpred[w] +
+                                  (fbase ? (double)fbase[(long long)w * CV_NIN] : 0.0)
+                            : 0.0;
     z_t e;
     if (i >= 0) e = zmk(p[0] + p[2] - ek[2 * i], p[1] + p[3] - ek[2 * i + 1]);
     else e = zmk(p[0] + p[2] - f, p[1] + p[3]);
@@ -409,7 +414,8 @@ float floor_sd(float sd, float mu) { return std::max(sd, 1e-6f * (fabsf(mu) + 1.
 // New buffer statistics; (re)standardises the network when they drifted.
 cudaError_t cv_restandardize(CvState* s, cudaStream_t st) {
   cudaError_t e;
-  cv_buffer_stats_kernel<<<CV_NIN + 1, 256, 0, st>>>(s->raw_x, s->raw_t, s->buf_n, s->d_stat);
+  cv_buffer_stats_kernel<<<CV_NIN + 1, 256, 0, st>>>(s->raw_x, s->raw_t, s->buf_n,
+                                                     s->cfg.residual, s->d_stat);
   s->launches++;
   float hs[2 * (CV_NIN + 1)];
   if ((e = cudaMemcpyAsync(hs, s->d_stat, sizeof(hs), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
@@ -455,6 +461,41 @@ cudaError_t cv_restandardize(CvState* s, cudaStream_t st) {
   return cudaStreamSynchronize(st);
 }
 
+// Q = dE_K/dG at the weighted-mean density matrix Gm, with batched FP64 ZGEMMs over the
+// Cholesky vectors c (E_K = 1/2 sum_c tr(T_c T_c), T_c = Lh_c Gm^T per spin):
+//   Tq[s][c][a][b] = sum_k Gm[s][a][k] Lh[c][s][b][k]   (= T_c[b][a])
+//   Qpart[c][b][k] = sum_a T_c[b][a] Lh[c][s][a][k],  Q[s][b][k] = sum_c Qpart[c][b][k]
+// and qoff = Q.Gm / 2 = E_K(Gm).  Scratch is allocated on the first call.
+cudaError_t cv_refresh_q(CvState* s, const CvInputs& in, cudaStream_t st) {
+  const int n = in.n, N = in.N, nc = s->nc;
+  cudaError_t e = cudaSuccess;
+  if (!s->Gm) {
+    auto A = [&](cudaError_t r) { if (e == cudaSuccess) e = r; };
+    A(cmal(s, &s->Gm, (size_t)s->nak));
+    A(cmal(s, &s->Tq, (size_t)2 * nc * n * n));
+    A(cmal(s, &s->Qpart, (size_t)nc * n * N));
+    if (e != cudaSuccess) return e;
+  }
+  cv_gmean_kernel<<<gridn(s->nak, 256), 256, 0, st>>>(in.Gc, s->nak, s->nw, in.Wd, s->Gm);
+  s->launches++;
+  for (int sp = 0; sp < 2; sp++) {
+    const long long so = (long long)sp * n * N;
+    ZGemmDesc g1{n, n, N, s->Gm + so, N, 0, in.Lh + so, N, 2LL * n * N, zmk(1, 0)};
+    EpiStore e1{s->Tq + (long long)sp * nc * n * n, n, (long long)n * n, zmk(0, 0), 0};
+    if ((e = zgemm_launch<true, true>(g1, nc, e1, st)) != cudaSuccess) return e;
+    ZGemmDesc g2{n, N, n, s->Tq + (long long)sp * nc * n * n, n, (long long)n * n, in.Lh + so, N,
+                 2LL * n * N, zmk(1, 0)};
+    EpiStore e2{s->Qpart, N, (long long)n * N, zmk(0, 0), 0};
+    if ((e = zgemm_launch<false, false>(g2, nc, e2, st)) != cudaSuccess) return e;
+    cv_qsum_kernel<<<gridn((long long)n * N, 256), 256, 0, st>>>(s->Qpart, nc, (long long)n * N,
+                                                                 s->Q + so);
+    s->launches += 3;
+  }
+  cv_qoff_kernel<<<1, 256, 0, st>>>(s->Q, s->Gm, s->nak, s->d_qoff);
+  s->launches++;
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvState** out,
@@ -465,6 +506,8 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   s->cfg = cfg;
   if (const char* it = getenv("AFQ_CV_ITERS")) s->cfg.iters_online = std::max(1, atoi(it));
   if (const char* sm = getenv("AFQ_CV_SAMPLING")) s->cfg.sampling = atoi(sm) == 0 ? 0 : 1;
+  if (const char* qr = getenv("AFQ_CV_QREFRESH")) s->cfg.q_refresh = std::max(0, atoi(qr));
+  if (const char* rs = getenv("AFQ_CV_RESIDUAL")) s->cfg.residual = atoi(rs) != 0;
   s->nw = nw; s->nc = nchol; s->nak = nak;
   s->sub_cap = (nw + cfg.subset_den - 1) / cfg.subset_den;
   s->cap = std::max(4096, nw);
@@ -493,7 +536,9 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   A(cmal(s, &s->d_wt, nw));
   A(cmal(s, &s->Gc_sub, (size_t)s->sub_cap * nak));
   A(cmal(s, &s->Q, (size_t)nak));
+  A(cmal(s, &s->d_qoff, 1));
   if (e == cudaSuccess) e = cudaMemsetAsync(s->Q, 0, sizeof(z_t) * nak, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_qoff, 0, sizeof(z_t), st);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sums, sizeof(double) * 4);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_cnt, sizeof(int) * nw);
@@ -577,15 +622,19 @@ void cv_stats(CvState* s, double* o) {
 long long cv_launches(const CvState* s) { return s->launches; }
 
 cudaError_t cv_predictions(CvState* s, double* host, cudaStream_t st) {
-  std::vector<float> f(s->nw, 0.0f);
+  std::vector<float> f(s->nw, 0.0f), x((size_t)s->nw * CV_NIN, 0.0f);
   if (s->active) {
     cudaError_t e = cudaMemcpyAsync(f.data(), s->fpred, sizeof(float) * s->nw,
                                     cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(x.data(), s->feats, sizeof(float) * x.size(), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
   }
   for (int w = 0; w < s->nw; w++)
-    host[w] = s->active ? s->ref + s->mu_r + s->sd_r * (double)f[w] : 0.0;
+    host[w] = s->active ? s->ref + s->mu_r + s->sd_r * (double)f[w] +
+                              (s->cfg.residual ? (double)x[(size_t)w * CV_NIN + 36] : 0.0)
+                        : 0.0;
   return cudaSuccess;
 }
 
@@ -598,22 +647,23 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   }
   s->meas++;
   s->launches = 0;
-  if (!s->have_q && in.Lh) {   // linearised exchange about the first measurement's mean G
-    z_t *Gm = nullptr, *Tt = nullptr;
-    const long long ntt = 2LL * in.n * s->nc * in.n;
-    if ((e = cudaMallocAsync(&Gm, sizeof(z_t) * s->nak, st)) != cudaSuccess) return e;
-    if ((e = cudaMallocAsync(&Tt, sizeof(z_t) * ntt, st)) != cudaSuccess) return e;
-    cv_gmean_kernel<<<gridn(s->nak, 256), 256, 0, st>>>(in.Gc, s->nak, nw, in.Wd, Gm);
-    cv_qt_kernel<<<gridn(ntt, 256), 256, 0, st>>>(in.Lh, Gm, s->nc, in.n, in.N, Tt);
-    cv_q_kernel<<<gridn(s->nak, 128), 128, 0, st>>>(in.Lh, Tt, s->nc, in.n, in.N, s->Q);
-    s->launches += 3;
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    cudaFreeAsync(Gm, st);
-    cudaFreeAsync(Tt, st);
+  // linearised exchange about the weighted-mean G: at the first measurement, then every
+  // q_refresh measurements
+  if (in.Lh && (!s->have_q || (s->cfg.q_refresh > 0 && s->meas - s->q_meas >= s->cfg.q_refresh))) {
+    if ((e = cv_refresh_q(s, in, st)) != cudaSuccess) return e;
+    if (!s->have_q) {   // the reference of feature 36: E_K at the first mean G
+      z_t q0;
+      if ((e = cudaMemcpyAsync(&q0, s->d_qoff, sizeof(q0), cudaMemcpyDeviceToHost, st)) !=
+              cudaSuccess ||
+          (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+      s->lin_ref = q0.x;
+    }
     s->have_q = true;
+    s->q_meas = s->meas;
   }
   cv_features_kernel<<<nw, 256, 0, st>>>(in.Gc, in.haj, s->nak, in.cvec, s->nc, nw, in.Wd, s->R,
-                                         s->Q, s->feats, s->e1ej);
+                                         s->Q, s->d_qoff, s->lin_ref, s->feats, s->e1ej);
   s->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   s->active = s->trained && !s->failed;
@@ -670,6 +720,7 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   cv_mark_kernel<<<gridn(m, 256), 256, 0, st>>>(s->d_sub, m, s->member);
   cv_assemble_kernel<<<1, 1024, 0, st>>>(nw, m, s->active ? 1 : 0, s->member, s->e1ej, s->ek_sub,
                                           s->fpred, s->ref + s->mu_r, s->sd_r,
+                                          s->cfg.residual ? s->feats + 36 : nullptr,
                                           pps ? s->d_cnt : nullptr, pps ? s->d_mult : nullptr,
                                           in.Wd, s->d_sums);
   s->launches += 3;
@@ -677,6 +728,12 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   if ((e = cudaMemcpyAsync(s->h_sums, s->d_sums, 4 * sizeof(double), cudaMemcpyDeviceToHost,
                            st)) != cudaSuccess)
     return e;
+  if (!s->have_ref && s->cfg.residual && s->have_q) {
+    // residual learning: targets relative to the first linearisation's E_K(Gm), the same
+    // reference feature 36 is relative to
+    s->ref = s->lin_ref;
+    s->have_ref = true;
+  }
   if (!s->have_ref) {
     // offset of the stored targets: the first walker's exact exchange energy
     double ek0[2];
@@ -704,8 +761,8 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
     if ((e = cv_restandardize(s, ts)) != cudaSuccess) return e;
     s->trained = true;
     cv_normalize_buffer_kernel<<<gridn((long long)s->buf_n * CV_NIN, 256), 256, 0, ts>>>(
-        s->raw_x, s->raw_t, s->buf_n, s->d_mu, s->d_sd, (float)s->mu_r, (float)s->sd_r, s->buf_x,
-        s->buf_t);
+        s->raw_x, s->raw_t, s->buf_n, s->d_mu, s->d_sd, (float)s->mu_r, (float)s->sd_r,
+        s->cfg.residual, s->buf_x, s->buf_t);
     s->launches++;
     const int iters = first ? s->cfg.iters_warm : s->cfg.iters_online;
     const int bb = s->cfg.batch_online;
