@@ -703,9 +703,13 @@ def main():
     peaks, src = measured_peaks()
     dom = max(stages, key=lambda k: stages[k][0])
     dom_ms, dom_launch = stages[dom]
+    # calls of each stage in the profiled pass (substeps nwarm + K .. nwarm + 2K - 1): the
+    # density matrix once per substep and once per measurement, the energy per measurement
+    p0 = nwarm + args.steps
+    nmeas = sum(1 for st in range(p0, p0 + args.steps) if (st + 1) % args.energy_every == 0)
+    stage_calls = {"DM": args.steps + nmeas, "energy": max(nmeas, 1)}
     if args.form == "fp64":
-        calls = {"DM": args.steps + args.steps // args.energy_every,
-                 "energy": args.steps // args.energy_every}.get(dom, args.steps)
+        calls = stage_calls.get(dom, args.steps)
         peak = fp64_peak_tflops(torch)
         achieved = fp64_stage_flops(cfg, nw, dom) * calls / (dom_ms * 1e-3) / 1e12
         roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": peak,
@@ -740,8 +744,7 @@ def main():
             "ms_measured": dom_ms / args.steps}
         roof["traffic_model"] = mixed_propagate_bytes(cfg, nw, preal=preal)
     else:
-        calls = {"DM": args.steps + args.steps // args.energy_every,
-                 "energy": args.steps // args.energy_every}.get(dom, args.steps)
+        calls = stage_calls.get(dom, args.steps)
         real_ops = bool(np.all(s.SpvnT.vals.imag == 0)) and (s.Lh is None or
                                                              bool(np.all(s.Lh.imag == 0)))
         sub = (nw + 7) // 8 if head.mode == "cv" else nw
