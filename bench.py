@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--form", default="mixed-cv", choices=["mixed-cv", "mixed", "fp64"])
     p.add_argument("--energy-every", type=int, default=5)
     p.add_argument("--northo", type=int, default=5)
+    p.add_argument("--branch", type=int, default=1,
+                   help="population control (comb) after every energy measurement (0: none, "
+                        "as in the reference miniapp)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -340,6 +343,8 @@ class Form:
         driver.substep(self.eng, self.cfg.seed, st, self.args.northo, self.comm, graph=graph)
         if (st + 1) % self.args.energy_every == 0:
             self.measure(record)
+            if self.args.branch:   # where the miniapp marks branching (miniafqmc_base.cpp:347)
+                self.eng.population_control(self.cfg.seed, st + 1)
 
 
 def blocking_sigma(x):
@@ -640,6 +645,8 @@ def main():
                 eng.calculate_overlaps()
             if (k + 1) % args.energy_every == 0:
                 head.measure(record=False)
+                if args.branch:
+                    eng.population_control(cfg.seed, st + 1)
             eng._check(eng.lib.afq_get_walkers(eng.h, None, ctypes.c_void_p(wdnp.ctypes.data)))
         eng.synchronize()
         t_e2e = time.perf_counter() - t0
