@@ -60,9 +60,9 @@ def parse():
     p.add_argument("--form", default="mixed-cv", choices=["mixed-cv", "mixed", "fp64"])
     p.add_argument("--energy-every", type=int, default=5)
     p.add_argument("--northo", type=int, default=5)
-    p.add_argument("--branch", type=int, default=1,
-                   help="population control (comb) after every energy measurement (0: none, "
-                        "as in the reference miniapp)")
+    p.add_argument("--branch", type=int, default=0,
+                   help="1: population control (comb) after every energy measurement (default "
+                        "0: none, as in the reference miniapp)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -376,12 +376,24 @@ def accuracy_pass(system, cfg, args, device, torch):
     of the whole pass (CUDA events on the form's stream around all its substeps and
     measurements).  |dE| of each mixed form against FP64 on the same fields with the
     blocked standard error of the difference series, and the energy error per wall-second
-    sigma_E * sqrt(T) of each form."""
+    sigma_E * sqrt(T) of each form.
+
+    The trajectories of different forms drift apart even on the same fields (the walker
+    dynamics amplifies any rounding difference), so the precision of the mixed form is
+    measured on identical walkers as well: at every measurement of the FP64 trajectory a
+    mixed-form handle with its own control variate takes a device copy of the FP64
+    walkers (afq_copy_walkers) and measures them with the control-variate estimator and
+    with exact exchange ("same_walkers": the mean difference from FP64, the standard error
+    of that mean, the largest single difference; the shadow's time is left out of the FP64
+    pass's device time)."""
     out = {"substeps": args.acc_substeps, "energy_every": args.energy_every,
            "equilibration_substeps": args.acc_equil, "forms": {}}
     series = {}
+    shadow_e = {"cv": [], "exact": []}
     for name in ("mixed-cv", "mixed", "fp64"):
         f = Form(system, cfg, args, name, device, None, torch)
+        shadow = Form(system, cfg, args, "mixed-cv", device, None, torch) if name == "fp64" else None
+        t_shadow = 0.0
         e = f.eng
         e.synchronize()
         torch.cuda.synchronize()
@@ -393,10 +405,22 @@ def accuracy_pass(system, cfg, args, device, torch):
             f.step(st)
             if (st + 1) % args.energy_every == 0:
                 steps.append(st + 1)
+                if shadow is not None:
+                    ts = time.perf_counter()
+                    se = shadow.eng
+                    se.copy_walkers_from(e)
+                    se.calculate_mixed_density_matrix()
+                    shadow_e["cv"].append(se.calculate_energy("cv"))
+                    shadow_e["exact"].append(se.calculate_energy("chol"))
+                    se.synchronize()
+                    t_shadow += time.perf_counter() - ts
         e.synchronize()
         e1.record(f.stream)
         torch.cuda.synchronize()
-        secs = e0.elapsed_time(e1) * 1e-3
+        secs = e0.elapsed_time(e1) * 1e-3 - t_shadow
+        if shadow is not None:
+            out["same_walkers_cv_stats"] = shadow.eng.cv_stats()
+            shadow.eng.close()
         keep = np.array(steps) > args.acc_equil
         E = np.array(f.energies)[keep]
         sig, lev = blocking_sigma(E)
@@ -415,6 +439,15 @@ def accuracy_pass(system, cfg, args, device, torch):
         sd, _ = blocking_sigma(d)
         out[f"dE_{name}_vs_fp64"] = {"abs_dE_Ha": float(abs(d.mean())), "sigma_Ha": sd,
                                      "max_abs_per_measurement_Ha": float(np.max(np.abs(d)))}
+    keep = np.array(steps) > args.acc_equil
+    same = {}
+    for k in ("cv", "exact"):
+        d = np.array(shadow_e[k])[keep] - series["fp64"]
+        same[k] = {"dE_Ha": float(d.mean()), "abs_dE_Ha": float(abs(d.mean())),
+                   "sigma_of_mean_Ha": float(d.std(ddof=1) / np.sqrt(len(d))),
+                   "rms_per_measurement_Ha": float(np.sqrt(np.mean(d ** 2))),
+                   "max_abs_per_measurement_Ha": float(np.max(np.abs(d)))}
+    out["same_walkers_along_fp64_trajectory"] = same
     fm, f6 = out["forms"]["mixed-cv"], out["forms"]["fp64"]
     out["abs_dE_Ha"] = out["dE_mixed-cv_vs_fp64"]["abs_dE_Ha"]
     out["abs_dE_sigma_Ha"] = out["dE_mixed-cv_vs_fp64"]["sigma_Ha"]
@@ -505,8 +538,9 @@ def run_c5(args, torch):
         batch = AfqmcBatch(engs) if mode == "batch" else None
 
         def step(st):
-            if batch is not None:
-                batch.substep(seeds, st, args.northo)
+            if batch is not None:   # one launch per measurement interval
+                if st % args.energy_every == 0:
+                    batch.substeps(seeds, st, args.energy_every, args.northo)
                 return
             for e, sd in zip(engs, seeds):
                 e.substep(sd, st, args.northo, graph=True)

@@ -105,6 +105,12 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
                                const afq_csr_z* Vakbl, const double* Lhalf);
 
 afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data);
+/* Copies the walkers and walker data of `src` into `dst` on the device (same NMO,
+ * electrons, walker count and device; the two may be of different numerical forms), after
+ * the work queued on src's stream.  No reference counterpart: it lets one form measure
+ * another form's walkers (for example the mixed form's energy on the FP64 trajectory)
+ * without a round trip through host memory.  Synchronous. */
+afq_status afq_copy_walkers(afq_handle* dst, afq_handle* src);
 afq_status afq_get_walkers(afq_handle* h, double* W, double* W_data);
 
 /* afqmc_sys::calculate_mixed_density_matrix(W, W_data, Gc, compact=true)
@@ -305,6 +311,12 @@ afq_status afq_batch_create(afq_handle* const* handles, int count, afq_batch** o
 void afq_batch_destroy(afq_batch* b);
 afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_tot,
                              int northo);
+/* nsub (1..64) substeps of every system in ONE graph launch: substeps step_tot ..
+ * step_tot + nsub - 1, each re-orthogonalising when its step_tot > 0 is a multiple of
+ * northo.  The systems join once per launch instead of once per substep (use the
+ * substeps between two energy measurements).  Equal to nsub afq_batch_substep calls. */
+afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step_tot, int nsub,
+                              int northo);
 /* Waits for the batch's work and reports any handle's tensor-core timeout flags. */
 afq_status afq_batch_synchronize(afq_batch* b);
 

@@ -37,7 +37,8 @@ EXPORTS = [
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
     "afq_mixed_density_matrix_full", "afq_vbias_full", "afq_get_sparse_paths",
-    "afq_set_tc_wait_limit", "afq_substep_begin", "afq_substep_end",
+    "afq_set_tc_wait_limit", "afq_substep_begin", "afq_substep_end", "afq_batch_substeps",
+    "afq_copy_walkers",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -100,6 +101,8 @@ def signatures() -> dict:
         "afq_get_sparse_paths": ([P, P, P], I),
         "afq_set_tc_wait_limit": ([I, ctypes.c_longlong], I),
         "afq_substep_begin": ([P, U64, U64, P], I), "afq_substep_end": ([P, U64, I], I),
+        "afq_batch_substeps": ([P, P, U64, I, I], I),
+        "afq_copy_walkers": ([P, P], I),
     }
 
 
@@ -192,6 +195,10 @@ class AfqmcSys:
         Wd = np.empty((self.nw, 8), np.complex128)
         self._check(self.lib.afq_get_walkers(self.h, _p(W), _p(Wd)))
         return W, Wd
+
+    def copy_walkers_from(self, other: "AfqmcSys"):
+        """This handle's walkers := other's (device to device, afq_copy_walkers)."""
+        self._check(self.lib.afq_copy_walkers(self.h, other.h))
 
     def get_walker_data(self):
         Wd = np.empty((self.nw, 8), np.complex128)
@@ -436,6 +443,13 @@ class AfqmcBatch:
         st = self.lib.afq_batch_substep(self.b, _p(sd), step_tot, northo)
         if st != 0:
             raise AfqmcError(st, "afq_batch_substep failed")
+
+    def substeps(self, seeds, step_tot: int, nsub: int, northo: int):
+        """nsub substeps of every system in one graph launch (afq_batch_substeps)."""
+        sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+        st = self.lib.afq_batch_substeps(self.b, _p(sd), step_tot, nsub, northo)
+        if st != 0:
+            raise AfqmcError(st, "afq_batch_substeps failed")
 
     def synchronize(self):
         st = self.lib.afq_batch_synchronize(self.b)

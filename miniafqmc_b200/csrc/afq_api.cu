@@ -1184,6 +1184,33 @@ afq_status afq_population_control(afq_handle* h, uint64_t seed, uint64_t step) {
   return AFQ_OK;
 }
 
+afq_status afq_copy_walkers(afq_handle* dst, afq_handle* src) {
+  if (!dst || !src || dst == src) return AFQ_ERR_ARG;
+  if (dst->N != src->N || dst->n != src->n || dst->nw != src->nw ||
+      dst->d.device != src->d.device)
+    return fail(dst, AFQ_ERR_ARG, "afq_copy_walkers: handles of different shapes or devices");
+  if (!src->have_walkers) return fail(dst, AFQ_ERR_STATE, "source has no walkers");
+  cudaSetDevice(dst->d.device);
+  // the copy is ordered after the source's work and before the destination's next work
+  cudaEvent_t ev = nullptr;
+  AFQ_CUDA(dst, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, src->st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(dst->st, ev, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dst->W, src->W, sizeof(z_t) * (size_t)dst->nw * dst->N * 2 * dst->n,
+                        cudaMemcpyDeviceToDevice, dst->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dst->Wd, src->Wd, sizeof(z_t) * (size_t)dst->nw * 8,
+                        cudaMemcpyDeviceToDevice, dst->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(dst->st);
+  cudaEventDestroy(ev);
+  AFQ_CUDA(dst, e);
+  dst->have_walkers = true;
+  dst->dm_cache = false;
+  afq::mixed_invalidate(dst->mixed);
+  return AFQ_OK;
+}
+
 afq_status afq_get_eshift(afq_handle* h, double* eshift) {
   if (!h || !eshift) return AFQ_ERR_ARG;
   AFQ_CUDA(h, cudaMemcpyAsync(h->h_sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->st));
@@ -1370,14 +1397,18 @@ struct afq_batch {
   // recorded by the graph at the end of each system's branch (external event nodes): a
   // handle's later work waits for its own system only, not for the whole batch
   std::vector<cudaEvent_t> sysdone;
-  cudaGraphExec_t g[2] = {nullptr, nullptr};
-  std::vector<std::vector<long long>> counts[2];   // per handle, per stage
+  // one graph per (substeps per launch, which of them re-orthogonalise)
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<std::vector<long long>> counts;   // per handle, per stage
+  };
+  std::map<std::pair<int, uint64_t>, Graph> g;
 };
 
 namespace {
 void batch_release(afq_batch* b) {
-  for (auto& g : b->g)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto& kv : b->g)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
   for (cudaEvent_t e : b->pre) cudaEventDestroy(e);
   for (cudaEvent_t e : b->join) cudaEventDestroy(e);
   for (cudaEvent_t e : b->sysdone)
@@ -1429,12 +1460,16 @@ void afq_batch_destroy(afq_batch* b) {
   batch_release(b);
 }
 
-afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_tot,
-                             int northo) {
-  if (!b || !seeds || northo <= 0) return AFQ_ERR_ARG;
+afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step_tot, int nsub,
+                              int northo) {
+  if (!b || !seeds || northo <= 0 || nsub < 1 || nsub > 64) return AFQ_ERR_ARG;
   cudaSetDevice(b->device);
   const int n = (int)b->hs.size();
-  const bool ortho = step_tot > 0 && step_tot % (uint64_t)northo == 0;
+  uint64_t omask = 0;   // substeps of this launch that re-orthogonalise
+  for (int k = 0; k < nsub; k++) {
+    const uint64_t t = step_tot + (uint64_t)k;
+    if (t > 0 && t % (uint64_t)northo == 0) omask |= 1ull << k;
+  }
   // per system: scalars of this step, a fresh T1^-1 for the graph's first density matrix
   for (int i = 0; i < n; i++) {
     afq_handle* h = b->hs[i];
@@ -1448,19 +1483,20 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
     AFQ_CUDA(h, cudaEventRecord(b->pre[i], h->st));
     if (cudaStreamWaitEvent(b->st, b->pre[i], 0) != cudaSuccess) return AFQ_ERR_CUDA;
   }
-  const int slot = ortho ? 1 : 0;
-  if (!b->g[slot]) {
-    // one graph: fork from the batch stream into every handle's stream, join back
+  afq_batch::Graph& gr = b->g[{nsub, omask}];
+  if (!gr.exec) {
+    // one graph: fork from the batch stream into every handle's stream, nsub substeps of
+    // each system as its branch, join back
     if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return AFQ_ERR_CUDA;
     cudaError_t e = cudaEventRecord(b->fork, b->st);
-    b->counts[slot].assign(n, std::vector<long long>(AFQ_NSTAGES, 0));
+    gr.counts.assign(n, std::vector<long long>(AFQ_NSTAGES, 0));
     for (int i = 0; i < n && e == cudaSuccess; i++) {
       afq_handle* h = b->hs[i];
       if ((e = cudaStreamWaitEvent(h->st, b->fork, 0)) != cudaSuccess) break;
       h->capturing = true;
-      h->launch_sink = b->counts[slot][i].data();
-      e = st_substep(h, ortho);
+      h->launch_sink = gr.counts[i].data();
+      for (int k = 0; k < nsub && e == cudaSuccess; k++) e = st_substep(h, (omask >> k) & 1);
       h->launch_sink = nullptr;
       h->capturing = false;
       if (e == cudaSuccess)
@@ -1471,22 +1507,27 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
     if (e == cudaSuccess) e = e2;
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->g[slot], g, 0);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&gr.exec, g, 0);
     if (g) cudaGraphDestroy(g);
     if (e != cudaSuccess) {
-      b->g[slot] = nullptr;
+      gr.exec = nullptr;
       return fail(b->hs[0], AFQ_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e));
     }
   }
-  if (cudaGraphLaunch(b->g[slot], b->st) != cudaSuccess || cudaEventRecord(b->done, b->st) != cudaSuccess)
+  if (cudaGraphLaunch(gr.exec, b->st) != cudaSuccess || cudaEventRecord(b->done, b->st) != cudaSuccess)
     return AFQ_ERR_CUDA;
   for (int i = 0; i < n; i++) {   // later work on a handle's own stream follows the step
     afq_handle* h = b->hs[i];
     AFQ_CUDA(h, cudaStreamWaitEvent(h->st, b->sysdone[i], 0));
-    for (int k = 0; k < AFQ_NSTAGES; k++) h->stage_launches[k] += b->counts[slot][i][k];
-    h->host_step = step_tot + 1;
+    for (int k = 0; k < AFQ_NSTAGES; k++) h->stage_launches[k] += gr.counts[i][k];
+    h->host_step = step_tot + (uint64_t)nsub;
   }
   return AFQ_OK;
+}
+
+afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_tot,
+                             int northo) {
+  return afq_batch_substeps(b, seeds, step_tot, 1, northo);
 }
 
 afq_status afq_batch_synchronize(afq_batch* b) {

@@ -26,8 +26,10 @@ def rel(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_batch_matches_systems_alone(mixed):
+@pytest.mark.parametrize("mixed,nsub", [(False, 1), (True, 1), (True, 5)])
+def test_batch_matches_systems_alone(mixed, nsub):
+    """nsub substeps per graph launch (nsub = 5: the launches cover substeps 0-4 and 5-9,
+    the second one re-orthogonalising in its first substep)."""
     from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_FP64, AFQ_PREC_MIXED
     prec = AFQ_PREC_MIXED if mixed else AFQ_PREC_FP64
     sys_ = systems()
@@ -37,10 +39,14 @@ def test_batch_matches_systems_alone(mixed):
     batch = AfqmcBatch(grouped)
     for e in alone + grouped:
         e.calculate_mixed_density_matrix()
-    for st in range(7):   # includes the orthogonalisation at step 5
+    nst = 7 if nsub == 1 else 10   # includes the orthogonalisation at step 5
+    for st in range(nst):
         for e, sd in zip(alone, seeds):
             e.substep(sd, st, 5, graph=True)
-        batch.substep(seeds, st, 5)
+        if nsub == 1:
+            batch.substep(seeds, st, 5)
+        elif st % nsub == 0:
+            batch.substeps(seeds, st, nsub, 5)
     batch.synchronize()
     for a, g in zip(alone, grouped):
         Wa, Da = a.get_walkers()

@@ -51,8 +51,15 @@ def test_mlp_training_reduces_loss():
     net.close()
 
 
-def test_cv_energy_unbiased_with_variance_gain():
+@pytest.mark.parametrize("opts", [{}, {"AFQ_CV_SAMPLING": "0"},
+                                  {"AFQ_CV_RESIDUAL": "1", "AFQ_CV_QREFRESH": "5"}])
+def test_cv_energy_unbiased_with_variance_gain(opts, monkeypatch):
+    """Default subset design (weight-proportional teeth over walkers ordered by the
+    surrogate), the simple random sample, and residual learning on a linearised exchange
+    refreshed every five measurements: all unbiased, all with a variance gain."""
     from miniafqmc_b200.afqmc import AfqmcSys
+    for k, v in opts.items():
+        monkeypatch.setenv(k, v)
     s = system("C1")
     nw = 256
     g = AfqmcSys(s, nw)

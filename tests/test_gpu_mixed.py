@@ -215,3 +215,31 @@ def test_packed_forms_equal_packing_from_w(name, kw, nw):
         assert np.array_equal(We[0], Wf[0]) and np.array_equal(We[1], Wf[1]), change
         f.close()
     e.close()
+
+
+def test_copy_walkers_between_forms():
+    """afq_copy_walkers: the mixed form measures the FP64 form's walkers after a device
+    copy (energy within the absolute 1e-4 Ha bar of the FP64 energy of the same walkers);
+    handles of another shape are refused."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcError, AFQ_PREC_FP64, AFQ_PREC_MIXED
+    s = system("C1")
+    nw = 16
+    d = AfqmcSys(s, nw, precision=AFQ_PREC_FP64)
+    m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED)
+    d.calculate_mixed_density_matrix()
+    for st in range(7):
+        d.substep(2, st, 5, graph=True)
+    m.copy_walkers_from(d)
+    assert np.array_equal(m.get_walkers()[0], d.get_walkers()[0])
+    assert np.array_equal(m.get_walker_data(), d.get_walker_data())
+    for e in (d, m):
+        e.calculate_mixed_density_matrix()
+    ed, em = d.calculate_energy("chol"), m.calculate_energy("chol")
+    assert abs(em - ed) < 1e-4
+    m.substep(2, 7, 5, graph=True)         # the copy leaves the mixed handle usable
+    assert np.all(np.isfinite(m.get_walker_data()))
+    other = AfqmcSys(s, 8, precision=AFQ_PREC_MIXED)
+    with pytest.raises(AfqmcError):
+        other.copy_walkers_from(d)
+    for e in (d, m, other):
+        e.close()
