@@ -268,6 +268,13 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms);
  * mixed form.  ms[6]: the best milliseconds of the CSR product and of the dense product
  * per operand (0 when not timed).  With AFQ_TUNE=0 the rule is dense at >= 25% density. */
 afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
+/* Mixed form: walkers per group of the propagation chain (no reference counterpart).  The
+ * chain's products (P W, the Taylor terms, P S) run group by group, so one group's Taylor
+ * sum, operands and V stay in L2 between its products; 0 = every product over all walkers
+ * at once.  The set-up tuner times 0, 32, 48, 64, 96 and 128 walkers (those below nwalk)
+ * and keeps the fastest; ms[6] (may be NULL) receives those times (0 when not timed).
+ * AFQ_PROP_GROUP=<walkers> in the environment forces one.  Results do not depend on it. */
+afq_status afq_get_prop_group(afq_handle* h, int* walkers, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */
 afq_status afq_get_stream(afq_handle* h, void** stream);

@@ -1587,6 +1587,15 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms) {
   return AFQ_OK;
 }
 
+afq_status afq_get_prop_group(afq_handle* h, int* walkers, double* ms) {
+  if (!h || !walkers) return AFQ_ERR_ARG;
+  float t[6] = {};
+  *walkers = h->mixed ? afq::mixed_prop_group(h->mixed, t) : 0;
+  if (ms)
+    for (int i = 0; i < 6; i++) ms[i] = t[i];
+  return AFQ_OK;
+}
+
 afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms) {
   if (!h || (!path && !ms)) return AFQ_ERR_ARG;
   for (int i = 0; i < afq_handle::SP_N; i++) {

@@ -62,6 +62,9 @@ cudaError_t mixed_error(MixedState* m, int* flags);
 cudaError_t mixed_set_wait_clocks(long long clocks);
 // Kernel choices: choice[TS_N + 1] (0 built-in rule, 1 persistent, 2 per-tile; the last
 // entry is the split-K slice count), ms[TS_N][2] the set-up timings (0 when not timed).
+// Walkers per group of the propagation chain picked at set-up (0: all walkers per
+// product) and, in ms[6], the timed chain for 0 (all), 32, 48, 64, 96 and 128 walkers.
+int mixed_prop_group(const MixedState* m, float* ms);
 void mixed_tuning(const MixedState* m, int* choice, float* ms);
 // FP64 copy of the V operand ([nw][N*N]), for copy-out.
 cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st);

@@ -147,6 +147,11 @@ struct MixedState {
   // set-up by timing the candidates on the real shapes; part_cap = split-K slots allocated
   int tune[TS_N] = {};
   float tune_ms[TS_N][2] = {};
+  // propagation chain run walker group by walker group (0: all walkers per product), so a
+  // group's Taylor sum, operands and V stay in L2 across its eight products; picked by the
+  // set-up tuner (prop_group_ms: the timed chain per candidate, 0 = all walkers first)
+  int prop_group = 0;
+  float prop_group_ms[6] = {};
   int splits0 = 1, part_cap = 1;
 };
 
@@ -1606,7 +1611,10 @@ int mixed_launches(const MixedState* m, int stage) {
     case 1: return 3;                                  // pack, GEMM, reduce (vbias)
     case 3: return 2;                                  // pack, GEMM (vHS)
     // the walker packs drop out while the packed forms are current (m->packed at the call)
-    case 4: return (m->packed ? 1 : 2) + m->in.order + 1;   // [pack], P W, terms, P S
+    case 4: {   // [pack], then per walker group P W, terms, P S
+      const int G = m->prop_group > 0 && m->prop_group < m->nw ? m->prop_group : m->nw;
+      return (m->packed ? 0 : 1) + ((m->nw + G - 1) / G) * (m->in.order + 2);
+    }
     case 8: return m->in.Lh ? 4 : 0;                   // pack, E_J GEMM, reduce, E_K GEMM
     case 0: return m->packed ? 5 : 6;                  // [pack], T1, LU, pack, Gc x 2
     case 5: return m->packed ? 2 : 3;                  // [pack], T1, LU (overlaps)
@@ -1659,30 +1667,40 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
   }
   const int mt = (N + 127) / 128;
   const int Kp = pr ? N : 2 * N;   // K of P W and P S
+  // walker groups: every product of the chain over one group before the next group (the
+  // same tiles and epilogues as one launch over all walkers, in another order)
+  const int G = m->prop_group > 0 && m->prop_group < nw ? m->prop_group : nw;
   int cur = 0;
-  {  // S = P W
-    tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
-    if ((e = run_prop(m, m->prec_p, from_f2 ? m->m_pw2 : m->m_pw[0], g, 0, 0, 0, nullptr,
-                      next_op(m->F[1], m->prec_v1), st)) != cudaSuccess)
-      return e;
-    cur = 1;
-  }
-  for (int k = 1; k <= m->in.order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
-    tc::GemmShape g{N, 2 * n2, 2 * N, nw, 128, mt, true, true, 0};
-    int prec = k == 1 ? m->prec_v1 : m->prec_vk;
-    const int nprec = k < m->in.order ? m->prec_vk : m->prec_p;   // precision of the next product
-    if ((e = run_prop(m, prec, m->m_v[cur], g, 1, k, k == m->in.order, nullptr,
-                      next_op(m->F[cur ^ 1], nprec),
-                      st)) != cudaSuccess)
-      return e;
-    cur ^= 1;
-  }
-  {  // W = P S (with order 0 the B operand of S = P W is already in F[cur]); the pair
-     // epilogue also writes the new walkers' packed forms (F[cur ^ 1] is free)
-    tc::GemmShape g{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
-    if ((e = run_prop(m, m->prec_p, m->m_pw[cur], g, 2, 0, 0, W, Op{}, st, cur ^ 1)) !=
-        cudaSuccess)
-      return e;
+  for (int z0 = 0; z0 < nw; z0 += G) {
+    const int gb = std::min(G, nw - z0);
+    cur = 0;
+    {  // S = P W
+      tc::GemmShape g{N, 2 * n2, Kp, gb, 128, mt, false, true, 0};
+      g.z0 = z0;
+      if ((e = run_prop(m, m->prec_p, from_f2 ? m->m_pw2 : m->m_pw[0], g, 0, 0, 0, nullptr,
+                        next_op(m->F[1], m->prec_v1), st)) != cudaSuccess)
+        return e;
+      cur = 1;
+    }
+    for (int k = 1; k <= m->in.order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
+      tc::GemmShape g{N, 2 * n2, 2 * N, gb, 128, mt, true, true, 0};
+      g.z0 = z0;
+      int prec = k == 1 ? m->prec_v1 : m->prec_vk;
+      const int nprec = k < m->in.order ? m->prec_vk : m->prec_p;   // precision of the next product
+      if ((e = run_prop(m, prec, m->m_v[cur], g, 1, k, k == m->in.order, nullptr,
+                        next_op(m->F[cur ^ 1], nprec),
+                        st)) != cudaSuccess)
+        return e;
+      cur ^= 1;
+    }
+    {  // W = P S (with order 0 the B operand of S = P W is already in F[cur]); the pair
+       // epilogue also writes the new walkers' packed forms (F[cur ^ 1] is free)
+      tc::GemmShape g{N, 2 * n2, Kp, gb, 128, mt, false, true, 0};
+      g.z0 = z0;
+      if ((e = run_prop(m, m->prec_p, m->m_pw[cur], g, 2, 0, 0, W, Op{}, st, cur ^ 1)) !=
+          cudaSuccess)
+        return e;
+    }
   }
   if (n2 % 32 == 0 && m->Wn.hi) {   // pair epilogue, and a trial (the T1 product exists)
     m->packed = true;
@@ -1889,6 +1907,7 @@ struct TuneRec {
   int tune[TS_N];
   float ms[TS_N][2];
   int splits;
+  int prop_group;
 };
 std::mutex tune_mu;
 std::map<std::string, TuneRec>& tune_cache() {
@@ -1920,7 +1939,7 @@ void tune_load(const char* path) {
     bool ok = true;
     for (int i = 0; i < TS_N && ok; i++)
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
-    if (!ok || fscanf(f, "%d", &r.splits) != 1) break;
+    if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
     tune_cache()[key] = r;
     tune_file_keys().insert(key);
   }
@@ -1932,7 +1951,7 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   if (!f) return;
   fprintf(f, "%s", key.c_str());
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
-  fprintf(f, " %d\n", r.splits);
+  fprintf(f, " %d %d\n", r.splits, r.prop_group);
   fclose(f);
 }
 }  // namespace
@@ -1946,7 +1965,9 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   }
   if (force < 0 && !tc_persistent()) force = 2;   // AFQ_TC_PERSISTENT=0: per-tile kernels
   const char* fsk = getenv("AFQ_SPLITK");
-  const std::string key = tune_key(m) + "_f" + std::to_string(force) + "_k" +
+  const char* fpg = getenv("AFQ_PROP_GROUP");
+  const std::string key = tune_key(m) + "_pg" + std::to_string(fpg ? atoi(fpg) : -1) + "_f" +
+                          std::to_string(force) + "_k" +
                           std::to_string(fsk ? atoi(fsk) : 0) + "_p" +
                           std::to_string(promote_kb(PROMOTE_PART)) +
                           std::to_string(promote_kb(PROMOTE_EXCHANGE));
@@ -1966,6 +1987,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
         set_splits(m, r.splits);
         if (m->splits > m->part_cap) set_splits(m, m->splits0);
       }
+      m->prop_group = r.prop_group;
       tune_save(cache_path, key, r);   // a shape timed before the file was named
       return cudaSuccess;
     }
@@ -2046,19 +2068,44 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     const int mt = (N + 127) / 128, n2 = 2 * n;
     const int Kp = m->preal ? N : 2 * N;
     const int order = m->in.order;
-    pick(TS_PROP, [&] {   // the chain: two P products and `order` V products
-      tc::GemmShape gp{N, 2 * n2, Kp, nw, 128, mt, false, true, 0};
-      tc::GemmShape gv{N, 2 * n2, 2 * N, nw, 128, mt, true, true, 0};
-      cudaError_t r = run_prop(m, m->prec_p, m->m_pw[0], gp, 0, 0, 0, nullptr,
-                               next_op(m->F[1], m->prec_v1), st);
-      for (int k = 1; k <= order && r == cudaSuccess; k++)
-        r = run_prop(m, k == 1 ? m->prec_v1 : m->prec_vk, m->m_v[0], gv, 1, k, 0, nullptr,
-                     next_op(m->F[1], m->prec_vk), st);
-      if (r == cudaSuccess)
-        r = run_prop(m, m->prec_p, m->m_pw[0], gp, 0, 0, 0, nullptr, next_op(m->F[1], m->prec_p),
-                     st);
+    int group = 0;   // walkers per group of the timed chain (0: all)
+    auto chain = [&] {   // the chain: two P products and `order` V products per group
+      const int G = group > 0 && group < nw ? group : nw;
+      cudaError_t r = cudaSuccess;
+      for (int z0 = 0; z0 < nw && r == cudaSuccess; z0 += G) {
+        const int gb = std::min(G, nw - z0);
+        tc::GemmShape gp{N, 2 * n2, Kp, gb, 128, mt, false, true, 0};
+        tc::GemmShape gv{N, 2 * n2, 2 * N, gb, 128, mt, true, true, 0};
+        gp.z0 = gv.z0 = z0;
+        r = run_prop(m, m->prec_p, m->m_pw[0], gp, 0, 0, 0, nullptr,
+                     next_op(m->F[1], m->prec_v1), st);
+        for (int k = 1; k <= order && r == cudaSuccess; k++)
+          r = run_prop(m, k == 1 ? m->prec_v1 : m->prec_vk, m->m_v[0], gv, 1, k, 0, nullptr,
+                       next_op(m->F[1], m->prec_vk), st);
+        if (r == cudaSuccess)
+          r = run_prop(m, m->prec_p, m->m_pw[0], gp, 0, 0, 0, nullptr,
+                       next_op(m->F[1], m->prec_p), st);
+      }
       return r;
-    });
+    };
+    pick(TS_PROP, chain);
+    // then the walker group of the chosen kernel: all walkers, or groups whose Taylor sum,
+    // operands and V fit in L2 together; AFQ_PROP_GROUP=<walkers> forces one
+    const char* fg = getenv("AFQ_PROP_GROUP");
+    const int cand[6] = {0, 32, 48, 64, 96, 128};
+    int best = 0;
+    float bt = 0.0f;
+    for (int c = 0; c < 6 && m->tune[TS_PROP]; c++) {
+      if (cand[c] >= nw || (fg && cand[c] != atoi(fg))) continue;
+      group = cand[c];
+      const float t = timed(chain);
+      m->prop_group_ms[c] = t > 0.0f ? t : 0.0f;
+      if (t > 0.0f && (bt == 0.0f || t < bt)) {
+        bt = t;
+        best = group;
+      }
+    }
+    m->prop_group = best;
   }
   {  // split-K slices x kernel
     int bs = m->splits0, bv = 0;
@@ -2087,8 +2134,11 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   }
   if (m->in.Lh) {
     const int nsub = std::max(1, nw / 8);
-    const bool exp = promote_kb(PROMOTE_EXCHANGE) > 0 && (2 * n) % 32 == 0 && 2 * n <= 96 &&
-                     (m->ex_bn / 2) % (2 * n) == 0;
+    // the promoted exchange instances (walker widths 24, 32, 64, 96, 128) run on the
+    // persistent kernel only: the tuner may not trade their accuracy for speed
+    const int w2 = 2 * n;
+    const bool exp = promote_kb(PROMOTE_EXCHANGE) > 0 && (w2 == 24 || w2 == 32 || w2 == 64 ||
+                     w2 == 96 || w2 == 128) && (m->ex_bn / 2) % w2 == 0;
     pick(TS_EXF, [&] { return exchange_product(m, nw, kp, m->ex_mtiles, st); }, exp);
     pick(TS_EXS, [&] { return exchange_product(m, nsub, kp, m->ex_mtiles, st); }, exp);
   }
@@ -2114,6 +2164,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       r.ms[i][1] = m->tune_ms[i][1];
     }
     r.splits = m->splits;
+    r.prop_group = m->prop_group;
     std::lock_guard<std::mutex> lk(tune_mu);
     tune_cache()[key] = r;
     tune_save(cache_path, key, r);
@@ -2128,6 +2179,12 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
             m->tune_ms[TS_EXS][0], m->tune_ms[TS_EXS][1], m->tune[TS_T1], m->tune_ms[TS_T1][0],
             m->tune_ms[TS_T1][1]);
   return e;
+}
+
+int mixed_prop_group(const MixedState* m, float* ms) {
+  if (ms)
+    for (int i = 0; i < 6; i++) ms[i] = m ? m->prop_group_ms[i] : 0.0f;
+  return m ? m->prop_group : 0;
 }
 
 void mixed_tuning(const MixedState* m, int* choice, float* ms) {

@@ -280,7 +280,7 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
 __global__ void __launch_bounds__(192, MINB)
 tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step, int a_batched,
-               int b_batched, int k_split, int m_fast, Epi epi, int* err) {
+               int b_batched, int k_split, int m_fast, int z0, Epi epi, int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -298,7 +298,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
   // m_fast: M tiles along grid x, so the CTAs that share a B tile run together
   const int mt = m_fast ? blockIdx.x : blockIdx.y, nt = m_fast ? blockIdx.y : blockIdx.x;
   const int m0 = mt * m_step, n0 = nt * n_step;
-  const int batch = blockIdx.z;
+  const int batch = z0 + blockIdx.z;
   // split-K: z selects the K range [z*k_split, (z+1)*k_split) of an unbatched product
   const int kbase = k_split ? batch * k_split : 0;
   const int klen = k_split ? min(k_split, K - kbase) : K;
@@ -439,10 +439,11 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
 // and the others follow at their next wait.
 struct TileSched {
   int m_tiles, n_tiles, nbatch, m_fast;
+  int z0 = 0;   // first batch index of the launch (a walker group of a larger batch)
   AFQ_HD int total() const { return m_tiles * n_tiles * nbatch; }
   AFQ_D void decode(int t, int& z, int& mt, int& nt) const {
     const int per = m_tiles * n_tiles;
-    z = t / per;
+    z = z0 + t / per;
     const int r = t - z * per;
     if (m_fast) {
       mt = r % m_tiles;
@@ -727,6 +728,8 @@ struct GemmShape {
   bool m_fast = false; // raster M tiles fastest (B tiles reused from L2 across M)
   int n_step = 0;      // columns between consecutive N tiles (0: BN); a smaller step lets a
                        // tile hold whole column groups that do not fill BN
+  int z0 = 0;          // first batch of the launch: batches z0 .. z0 + batch - 1 of operands
+                       // (and epilogue outputs) that hold more (no split-K)
 };
 
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
@@ -751,7 +754,7 @@ cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* er
   const unsigned ntiles = (g.N + ns - 1) / ns;
   dim3 grid(g.m_fast ? g.m_tiles : ntiles, g.m_fast ? ntiles : g.m_tiles, g.batch);
   kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, ns, g.a_batched, g.b_batched, g.k_split,
-                                    g.m_fast ? 1 : 0, epi, err);
+                                    g.m_fast ? 1 : 0, g.z0, epi, err);
   return cudaGetLastError();
 }
 
@@ -778,7 +781,7 @@ cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& e
   });
   if (e != cudaSuccess) return e;
   const int ns = g.n_step > 0 ? g.n_step : BN;
-  TileSched sc{g.m_tiles, (g.N + ns - 1) / ns, g.batch, g.m_fast ? 1 : 0};
+  TileSched sc{g.m_tiles, (g.N + ns - 1) / ns, g.batch, g.m_fast ? 1 : 0, g.z0};
   const int total = sc.total();
   if (total <= 0) return cudaSuccess;
   const int grid = total < sm_count() ? total : sm_count();

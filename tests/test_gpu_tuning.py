@@ -150,3 +150,25 @@ def test_fp64_shapes_do_not_change_results(kw, monkeypatch):
     else:
         assert rel(W1, W0) < 1e-12 and rel(D1, D0) < 1e-12
         assert abs(ec1 - ec0) < 1e-12 * abs(ec0) and abs(ev1 - ev0) < 1e-12 * abs(ev0)
+
+
+def test_grouped_propagation_chain_is_bit_identical(monkeypatch):
+    """The mixed propagation chain run walker group by walker group (AFQ_PROP_GROUP) gives
+    the walkers of the chain over all walkers at once, bit for bit (same tiles, same
+    epilogues, another launch order), through graph substeps with a re-orthogonalisation."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    s = system("C2", with_vakbl=False)
+    nw = 80
+    wk = walkers(s, nw, seed=6)
+    out = {}
+    for grp in ("0", "32"):
+        monkeypatch.setenv("AFQ_PROP_GROUP", grp)
+        e = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=wk, use_vakbl=False)
+        assert e.tuning()["propagate_walker_group"]["walkers"] == int(grp)
+        e.calculate_mixed_density_matrix()
+        for st in range(6):
+            e.substep(9, st, 5, graph=True)
+        out[grp] = e.get_walkers()
+        e.close()
+    assert np.array_equal(out["0"][0], out["32"][0])
+    assert np.array_equal(out["0"][1], out["32"][1])
