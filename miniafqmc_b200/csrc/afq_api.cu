@@ -70,7 +70,8 @@ struct afq_handle {
   int sp_path[SP_N] = {-1, -1, -1};
   float sp_ms[SP_N][2] = {};
   double sp_density[SP_N] = {};
-  z_t* sp_dense = nullptr;   // dense Spvn [N^2][nchol]
+  z_t* sp_dense = nullptr;   // dense Spvn [N^2][nchol] (complex values)
+  double* sp_dense_r = nullptr;   // the same when every value is real
   int vhsd_cfg = 0;          // ZGEMM tile shape of the dense vHS product
 
   // full-G path (transposed_Spvn == false): G [nw][2][N][N] walker-major, and T(Spvn) for
@@ -154,6 +155,15 @@ void dfree(afq_handle* h, void* p) {
       cudaFree(q);
       q = nullptr;
     }
+}
+
+// Scatters a real CSR into a zeroed dense row-major matrix of doubles.
+__global__ void csr_to_dense_real_kernel(const int* ri, const int* ci, const double* rv, int nrows,
+                                         long long ncols, double* out) {
+  int r = blockIdx.x * blockDim.y + threadIdx.y;
+  if (r >= nrows) return;
+  for (int p = ri[r] + threadIdx.x; p < ri[r + 1]; p += blockDim.x)
+    out[(long long)r * ncols + ci[p]] = rv[p];
 }
 
 // Scatters a CSR into a zeroed dense row-major matrix; rv (real values) replaces v when
@@ -343,17 +353,22 @@ cudaError_t body_sigma(afq_handle* h, int use_xraw) {
 }
 
 // vHS^T [w][ik] = sum_c X[c][w] Spvn[ik][c] with the dense Spvn: one ZGEMM of M = nw,
-// N = NMO^2, K = nchol writing each walker's matrix row by row.
+// N = NMO^2, K = nchol writing each walker's matrix row by row (real x complex
+// multiply-adds when Spvn is real).
 cudaError_t dense_vhs(afq_handle* h, int cfg) {
   const long long NN = (long long)h->N * h->N;
   ZGemmDesc g{h->nw, (int)NN, h->nc, h->X, h->nw, 0, h->sp_dense, h->nc, 0, zmk(1, 0)};
   EpiStore ep{h->vHS, NN, 0, zmk(0, 0), 0};
+  if (h->sp_dense_r) {
+    g.Br = h->sp_dense_r;
+    return zgemm_launch<false, true, EpiStore, true>(g, 1, ep, h->st, cfg);
+  }
   return zgemm_launch<false, true>(g, 1, ep, h->st, cfg);
 }
 
 cudaError_t body_vhs(afq_handle* h) {
   if (h->mixed) return afq::mixed_vhs(h->mixed, h->X, h->vHS, h->st);
-  if (h->sp_dense) return dense_vhs(h, h->vhsd_cfg);
+  if (h->sp_dense || h->sp_dense_r) return dense_vhs(h, h->vhsd_cfg);
   return afq::launch_csr_walker(h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, h->X, h->N * h->N, h->nw,
                                 h->vHS, (long long)h->N * h->N, h->st,
                                 h->f64cfg[afq_handle::F64_VHS]);
@@ -564,7 +579,19 @@ void keep_paths(afq_handle* h, const int* dense) {
   };
   int *r0 = nullptr, *c0 = nullptr;
   z_t* v0 = nullptr;
-  one(afq_handle::SP_SPVN, &h->sp_dense, &r0, &c0, &v0, false);
+  if (h->sp_dense_r) {   // real dense Spvn: the CSR stays either way
+    if (h->sp_path[afq_handle::SP_SPVN] >= 0) {
+      if (dense[afq_handle::SP_SPVN]) {
+        h->sp_path[afq_handle::SP_SPVN] = 1;
+      } else {
+        dfree(h, h->sp_dense_r);
+        h->sp_dense_r = nullptr;
+        h->sp_path[afq_handle::SP_SPVN] = 0;
+      }
+    }
+  } else {
+    one(afq_handle::SP_SPVN, &h->sp_dense, &r0, &c0, &v0, false);
+  }
   one(afq_handle::SP_SPVNT, &h->spT_dense, &h->spT_ri, &h->spT_ci, &h->spT_v, true);
   one(afq_handle::SP_VAKBL, &h->vk_dense, &h->vk_ri, &h->vk_ci, &h->vk_v, true);
 }
@@ -586,7 +613,7 @@ cudaError_t fp64_tune(afq_handle* h) {
   static std::map<std::string, std::vector<float>> cache;
   char key[200];
   snprintf(key, sizeof key, "N%d_n%d_nc%d_nw%d_sp%lld_d%d%d%d_l%d_v%d_p%d%d%d", h->N, h->n, h->nc,
-           h->nw, h->sp_ri ? 1LL : 0LL, h->sp_dense ? 1 : 0, h->spT_dense ? 1 : 0,
+           h->nw, h->sp_ri ? 1LL : 0LL, (h->sp_dense || h->sp_dense_r) ? 1 : 0, h->spT_dense ? 1 : 0,
            h->vk_dense ? 1 : 0, h->Lh ? 1 : 0, h->sp_rv ? 1 : 0, h->sp_path[0], h->sp_path[1],
            h->sp_path[2]);
   {
@@ -695,7 +722,7 @@ cudaError_t fp64_tune(afq_handle* h) {
                                     (long long)N * N, h->st, c);
     });
     Best bd;
-    if (h->sp_dense) {
+    if (h->sp_dense || h->sp_dense_r) {
       bd = fastest(kZgCfgs, [&](int c) { return dense_vhs(h, c); });
       h->vhsd_cfg = bd.cfg;
     }
@@ -906,9 +933,23 @@ afq_status afq_set_hamiltonian(afq_handle* h, const afq_csr_z* Spvn, const afq_c
       AFQ_CUDA(h, cudaDeviceSynchronize());
       h->sp_path[afq_handle::SP_SPVN] = 0;
       h->sp_density[afq_handle::SP_SPVN] = (double)nnz / ((double)N * N * nc);
-      if ((s = densify(h, h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, N * N, nc,
-                       h->sp_density[afq_handle::SP_SPVN], &h->sp_dense)) != AFQ_OK)
+      if (h->sp_rv) {   // real values: a dense operand of doubles (half the bytes)
+        size_t free_b = 0, total_b = 0;
+        const size_t cnt = (size_t)N * N * nc;
+        AFQ_CUDA(h, cudaMemGetInfo(&free_b, &total_b));
+        if (h->sp_density[afq_handle::SP_SPVN] >= kDenseCandidate &&
+            sizeof(double) * cnt <= free_b / 10 * 3) {
+          AFQ_CUDA(h, dalloc(h, &h->sp_dense_r, cnt));
+          AFQ_CUDA(h, cudaMemsetAsync(h->sp_dense_r, 0, sizeof(double) * cnt, h->st));
+          csr_to_dense_real_kernel<<<(N * N + 7) / 8, dim3(32, 8), 0, h->st>>>(
+              h->sp_ri, h->sp_ci, h->sp_rv, N * N, nc, h->sp_dense_r);
+          AFQ_CUDA(h, cudaGetLastError());
+          AFQ_CUDA(h, cudaStreamSynchronize(h->st));
+        }
+      } else if ((s = densify(h, h->sp_ri, h->sp_ci, h->sp_v, h->sp_rv, N * N, nc,
+                              h->sp_density[afq_handle::SP_SPVN], &h->sp_dense)) != AFQ_OK) {
         return s;
+      }
     }
   }
   if ((s = upload_csr(h, SpvnT, &h->spT_ri, &h->spT_ci, &h->spT_v, &h->spT_dense, true,

@@ -3,6 +3,7 @@
 // C(b)[m][n] = epilogue( alpha * sum_k A(b)(m,k) * B(b)(k,n) )
 //   A_KMAJ: A(m,k) = A[b*sA + m*lda + k]   else A(m,k) = A[b*sA + k*lda + m]
 //   B_KMAJ: B(k,n) = B[b*sB + n*ldb + k]   else B(k,n) = B[b*sB + k*ldb + n]
+//   B_REAL: B holds real doubles (ZGemmDesc::Br), each multiply-add a real x complex one
 //
 // sm_100a has no FP64 tensor-core kind for tcgen05 and its FP64 FMA rate equals its
 // FP64 MMA rate, so the FP64 form is a register-tiled CUDA-core GEMM: a BM x BN tile per
@@ -19,6 +20,7 @@ struct ZGemmDesc {
   const z_t* B;
   long long ldb, sB;
   z_t alpha;
+  const double* Br = nullptr;   // real B operand (B_REAL launches; B unused)
 };
 
 // ---------------------------------------------------------------- epilogues
@@ -65,7 +67,8 @@ struct ZTileCfg {
   static constexpr size_t SMEM = sizeof(z_t) * 2 * BK * (LDA_S + LDB_S);
 };
 
-template <int BM, int BN, int BK, int TM, int TN, bool A_KMAJ, bool B_KMAJ, class Epi>
+template <int BM, int BN, int BK, int TM, int TN, bool A_KMAJ, bool B_KMAJ, class Epi,
+          bool B_REAL = false>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 zgemm_kernel(ZGemmDesc d, Epi epi) {
   using Cfg = ZTileCfg<BM, BN, BK, TM, TN>;
@@ -78,7 +81,9 @@ zgemm_kernel(ZGemmDesc d, Epi epi) {
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const long long b = blockIdx.z;
   const z_t* A = d.A + b * d.sA;
-  const z_t* B = d.B + b * d.sB;
+  const z_t* B = B_REAL ? nullptr : d.B + b * d.sB;
+  const double* Br = B_REAL ? d.Br + b * d.sB : nullptr;
+  double* Bsr = reinterpret_cast<double*>(Bs);   // real B slabs (same row stride)
   const int M = d.M, N = d.N, K = d.K;
 
   auto load = [&](int stage, int k0) {
@@ -102,13 +107,14 @@ zgemm_kernel(ZGemmDesc d, Epi epi) {
       int n, k;
       if (B_KMAJ) { n = e / BK; k = e % BK; } else { k = e / BN; n = e % BN; }
       int gn = n0 + n, gk = k0 + k;
-      const z_t* src = B;
-      int bytes = 0;
-      if (gn < N && gk < K) {
-        src = B_KMAJ ? B + (long long)gn * d.ldb + gk : B + (long long)gk * d.ldb + gn;
-        bytes = 16;
+      const bool in = gn < N && gk < K;
+      const long long off = B_KMAJ ? (long long)gn * d.ldb + gk : (long long)gk * d.ldb + gn;
+      if constexpr (B_REAL) {
+        double* bsr = Bsr + stage * BK * LDB_S;
+        cp_async8(bsr + k * LDB_S + n, in ? Br + off : Br, in ? 8 : 0);
+      } else {
+        cp_async16(bs + k * LDB_S + n, in ? B + off : B, in ? 16 : 0);
       }
-      cp_async16(bs + k * LDB_S + n, src, bytes);
     }
     cp_async_commit();
   };
@@ -131,17 +137,32 @@ zgemm_kernel(ZGemmDesc d, Epi epi) {
     __syncthreads();
     const z_t* as = As + (kt & 1) * BK * LDA_S;
     const z_t* bs = Bs + (kt & 1) * BK * LDB_S;
+    const double* bsr = Bsr + (kt & 1) * BK * LDB_S;
 #pragma unroll
     for (int kk = 0; kk < BK; kk++) {
-      z_t a[TM], bb[TN];
+      z_t a[TM];
 #pragma unroll
       for (int i = 0; i < TM; i++) a[i] = as[kk * LDA_S + ty + i * NTY];
+      if constexpr (B_REAL) {
+        double bb[TN];
 #pragma unroll
-      for (int j = 0; j < TN; j++) bb[j] = bs[kk * LDB_S + tx + j * NTX];
+        for (int j = 0; j < TN; j++) bb[j] = bsr[kk * LDB_S + tx + j * NTX];
 #pragma unroll
-      for (int i = 0; i < TM; i++)
+        for (int i = 0; i < TM; i++)
 #pragma unroll
-        for (int j = 0; j < TN; j++) zfma(acc[i][j], a[i], bb[j]);
+          for (int j = 0; j < TN; j++) {
+            acc[i][j].x = fma(a[i].x, bb[j], acc[i][j].x);
+            acc[i][j].y = fma(a[i].y, bb[j], acc[i][j].y);
+          }
+      } else {
+        z_t bb[TN];
+#pragma unroll
+        for (int j = 0; j < TN; j++) bb[j] = bs[kk * LDB_S + tx + j * NTX];
+#pragma unroll
+        for (int i = 0; i < TM; i++)
+#pragma unroll
+          for (int j = 0; j < TN; j++) zfma(acc[i][j], a[i], bb[j]);
+      }
     }
     __syncthreads();
   }
@@ -166,14 +187,14 @@ inline const char* zgemm_cfg_name(int cfg) {
 
 // Host-side launcher: tile shape `cfg` (0: picked from N), dynamic shared memory set once
 // per instantiation.
-template <bool A_KMAJ, bool B_KMAJ, class Epi>
+template <bool A_KMAJ, bool B_KMAJ, class Epi, bool B_REAL = false>
 cudaError_t zgemm_launch(const ZGemmDesc& d, int batch, const Epi& epi, cudaStream_t st,
                          int cfg = 0) {
   if (d.M <= 0 || d.N <= 0 || batch <= 0) return cudaSuccess;
 #define AFQ_ZG_CASE(BM_, BN_, TM_, TN_)                                                     \
   {                                                                                        \
     using Cfg = ZTileCfg<BM_, BN_, 16, TM_, TN_>;                                          \
-    auto kern = zgemm_kernel<BM_, BN_, 16, TM_, TN_, A_KMAJ, B_KMAJ, Epi>;                 \
+    auto kern = zgemm_kernel<BM_, BN_, 16, TM_, TN_, A_KMAJ, B_KMAJ, Epi, B_REAL>;         \
     static DeviceAttr attr;                                                                \
     const cudaError_t e = attr.ensure(Cfg::SMEM, [kern](size_t b) {                        \
       return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b); \
