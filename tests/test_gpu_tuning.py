@@ -99,7 +99,8 @@ def test_timed_choice_cached_per_shape(tmp_path, monkeypatch):
         assert np.array_equal(t1[k], t2[k]), k
     lines = [ln.split() for ln in path.read_text().splitlines() if ln.strip()]
     assert len(lines) == 1 and lines[0][0].startswith("N128_n32_nc512_nw32_")
-    assert int(lines[0][-1]) == tun["splitk_slices"]
+    assert int(lines[0][-2]) == tun["splitk_slices"]
+    assert int(lines[0][-1]) == tun["propagate_walker_group"]["walkers"]
     assert [int(lines[0][1 + 3 * i]) for i in range(6)] == [
         tun[s_]["kernel"] for s_ in ("vhs", "propagate", "splitk", "exchange_all",
                                      "exchange_subset", "t1")]
@@ -155,8 +156,11 @@ def test_fp64_shapes_do_not_change_results(kw, monkeypatch):
 def test_grouped_propagation_chain_is_bit_identical(monkeypatch):
     """The mixed propagation chain run walker group by walker group (AFQ_PROP_GROUP) gives
     the walkers of the chain over all walkers at once, bit for bit (same tiles, same
-    epilogues, another launch order), through graph substeps with a re-orthogonalisation."""
+    epilogues, another launch order), through graph substeps with a re-orthogonalisation.
+    The split-K slice count, which sets the vbias summation order, is forced to one value
+    so the two handles' separate tuning runs cannot pick different ones."""
     from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    monkeypatch.setenv("AFQ_SPLITK", "2")
     s = system("C2", with_vakbl=False)
     nw = 80
     wk = walkers(s, nw, seed=6)
