@@ -122,7 +122,8 @@ afq_status afq_overlaps(afq_handle* h, int save_old);
 /* base::get_vbias(SpvnT, Gc, vbias, true) (vbias.hpp:49-63). */
 afq_status afq_vbias(afq_handle* h);
 /* The reference's transposed_Spvn == false path (CLI `-t no`, miniafqmc_base.cpp:265-273;
- * the flag's parsing is broken there, :120,138), FP64 form only:
+ * the flag's parsing is broken there, :120,138), in both forms (the mixed form's compact
+ * Gc comes from its tensor-core density matrix; the full G and the gather are FP64):
  * afqmc_sys::calculate_mixed_density_matrix(W, W_data, G, compact=false)
  * (afqmc_sys.hpp:98-116, mixed_density_matrix.hpp:96-99) -> the full G [2][NMO][NMO] of
  * every walker (AFQ_BUF_G_FULL) plus the compact Gc and overlaps;

@@ -316,8 +316,8 @@ int parse(int argc, char** argv, Options& o) {
   if (o.nsteps < 0 || o.nsubsteps < 0 || o.nwalk <= 0 || o.northo <= 0 || o.taylor < 0 ||
       o.digits <= 0 || o.digits > 17 || o.branch < 0)
     return 2;
-  // the full-G path is FP64 only and op by op (a graph substep is the transposed path)
-  if (!o.transposed && (o.precision != AFQ_PREC_FP64 || o.graph)) return 2;
+  // the full-G path runs op by op (a graph substep is the transposed path)
+  if (!o.transposed && o.graph) return 2;
   return 0;
 }
 

@@ -1059,7 +1059,8 @@ afq_status afq_mixed_density_matrix(afq_handle* h) {
 afq_status afq_mixed_density_matrix_full(afq_handle* h) {
   afq_status s = need_ready(h);
   if (s != AFQ_OK) return s;
-  if (h->mixed) return fail(h, AFQ_ERR_UNSUPPORTED, "full density matrix: FP64 form only");
+  // mixed form: the compact Gc comes from the tensor-core density matrix (stored in FP64);
+  // the full G and the T(Spvn) gather below run in FP64 in both forms
   const int N = h->N, n = h->n, nw = h->nw;
   if (!h->Gf) AFQ_CUDA(h, dalloc(h, &h->Gf, (size_t)nw * 2 * N * N));
   AFQ_CUDA(h, st_dm(h, 1, 0));
@@ -1079,7 +1080,6 @@ afq_status afq_mixed_density_matrix_full(afq_handle* h) {
 afq_status afq_vbias_full(afq_handle* h) {
   afq_status s = need_ready(h);
   if (s != AFQ_OK) return s;
-  if (h->mixed) return fail(h, AFQ_ERR_UNSUPPORTED, "full-G vbias: FP64 form only");
   if (!h->Gf) return fail(h, AFQ_ERR_STATE, "full density matrix not formed");
   const long long N2 = (long long)h->N * h->N;
   if (!h->spf_ri) {   // transpose once on the host from the device copy of Spvn

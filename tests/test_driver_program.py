@@ -262,7 +262,7 @@ def test_program_help_and_option_errors():
     exe = product_binary()
     h = subprocess.run([exe, "-h"], capture_output=True, text=True, timeout=60)
     assert h.returncode == 1 and "-t                If set to no" in h.stdout
-    for bad in (["-p", "half"], ["-e", "none"], ["-w", "0"], ["-t", "no", "-p", "mixed"],
+    for bad in (["-p", "half"], ["-e", "none"], ["-w", "0"],
                 ["-t", "no", "-g"], ["-b", "-1"], ["-x"]):
         r = subprocess.run([exe, *bad], capture_output=True, text=True, timeout=60)
         assert r.returncode == 1 and "bad option" in r.stderr, bad

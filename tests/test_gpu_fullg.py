@@ -43,14 +43,34 @@ def test_full_g_path_matches_oracle(make, nw):
     g.close()
 
 
-def test_full_g_path_rejects_mixed_form_and_order():
-    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcError, AFQ_PREC_MIXED
+def test_full_g_path_rejects_calls_out_of_order():
+    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcError
     s = system("C1")
     e = AfqmcSys(s, 16)
     with pytest.raises(AfqmcError):      # vbias before the full density matrix
         e.get_vbias_full()
     e.close()
-    m = AfqmcSys(s, 16, precision=AFQ_PREC_MIXED)
-    with pytest.raises(AfqmcError):
-        m.calculate_mixed_density_matrix_full()
+
+
+def test_full_g_path_mixed_form():
+    """The mixed form's -t no branch: full G from its tensor-core compact Gc (the FP64
+    full-G product and T(Spvn) gather on top), against the FP64 form's on the same walkers
+    (1e-4 relative, the split-bf16 tolerance of Gc), and a substep driven by that vbias."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
+    s = system("C1")
+    nw = 16
+    wk = perturbed(s, nw)
+    d = AfqmcSys(s, nw, precision=AFQ_PREC_FP64, walkers=wk)
+    m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=wk)
+    for e in (d, m):
+        e.calculate_mixed_density_matrix_full()
+        e.get_vbias_full()
+    assert rel(m.copy_out("G_full"), d.copy_out("G_full")) < 1e-4
+    assert rel(m.copy_out("vbias"), d.copy_out("vbias")) < 1e-4
+    for e in (d, m):
+        e.sigma(3, 0)
+        e.get_vHS()
+        e.propagate()
+    assert rel(m.get_walkers()[0], d.get_walkers()[0]) < 2e-2
+    d.close()
     m.close()
