@@ -269,13 +269,19 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms);
  * mixed form.  ms[6]: the best milliseconds of the CSR product and of the dense product
  * per operand (0 when not timed).  With AFQ_TUNE=0 the rule is dense at >= 25% density. */
 afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
-/* Mixed form: walkers per group of the propagation chain (no reference counterpart).  The
- * chain's products (P W, the Taylor terms, P S) run group by group, so one group's Taylor
- * sum, operands and V stay in L2 between its products; 0 = every product over all walkers
- * at once.  The set-up tuner times 0, 32, 48, 64, 96 and 128 walkers (those below nwalk)
- * and keeps the fastest; ms[6] (may be NULL) receives those times (0 when not timed).
- * AFQ_PROP_GROUP=<walkers> in the environment forces one.  Results do not depend on it. */
-afq_status afq_get_prop_group(afq_handle* h, int* walkers, double* ms);
+/* Mixed form: launch schedule the set-up tuner picked (no reference counterpart); 0s for
+ * the FP64 form.
+ * sched[0]: walkers per group of the propagation chain.  The chain's products (P W, the
+ *   Taylor terms, P S) run group by group, so one group's Taylor sum, operands and V can
+ *   stay in L2 between its products; 0 = every product over all walkers at once.  Timed:
+ *   0, 32, 48, 64, 96 and 128 walkers (those below nwalk) -> ms[0..5].  Results do not
+ *   depend on it.  AFQ_PROP_GROUP=<walkers> forces one.
+ * sched[1]: K slab of the vHS product in bytes, 128 (two 96 KB split stages) or 64 (four
+ *   48 KB stages, SWIZZLE_64B operand tiles).  Timed -> ms[6..7].  The slab sets the order
+ *   of the MMAs' fp32 accumulation, so it changes vHS in the last bits.  AFQ_VHS_SLAB=64 or
+ *   128 forces one; a forced kernel (AFQ_TUNE=1 or 2) keeps 128.
+ * ms[8] may be NULL; 0 where not timed. */
+afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */
 afq_status afq_get_stream(afq_handle* h, void** stream);
@@ -347,7 +353,8 @@ afq_status afq_halfrotate(int device, const afq_csr_z* Spvn, int nmo, int naea, 
  * device with bf16 operands (tf32 == 0, inputs rounded to nearest bf16) or tf32 operands,
  * fp32 accumulation, tile width bn in {64, 128, 192}; K must be a multiple of 8.
  * mode 0 = one CTA per tile, 1 / 2 = persistent kernel with one / two epilogue
- * warpgroups.  *kernel_err receives the kernel's timeout flags (0 when clean). */
+ * warpgroups, 3 / 4 = per-tile / persistent kernel with 64-byte K slabs (SWIZZLE_64B
+ * operand tiles).  *kernel_err receives the kernel's timeout flags (0 when clean). */
 afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn, int mode,
                                 const float* A, const float* B, float* C, int* kernel_err);
 /* Bound, in SM clocks, of the tensor-core kernels' pipeline waits on `device` (no

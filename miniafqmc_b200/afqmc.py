@@ -38,7 +38,7 @@ EXPORTS = [
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
     "afq_mixed_density_matrix_full", "afq_vbias_full", "afq_get_sparse_paths",
     "afq_set_tc_wait_limit", "afq_substep_begin", "afq_substep_end", "afq_batch_substeps",
-    "afq_copy_walkers", "afq_get_prop_group",
+    "afq_copy_walkers", "afq_get_schedule",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -102,7 +102,7 @@ def signatures() -> dict:
         "afq_set_tc_wait_limit": ([I, ctypes.c_longlong], I),
         "afq_substep_begin": ([P, U64, U64, P], I), "afq_substep_end": ([P, U64, I], I),
         "afq_batch_substeps": ([P, P, U64, I, I], I),
-        "afq_copy_walkers": ([P, P], I), "afq_get_prop_group": ([P, P, P], I),
+        "afq_copy_walkers": ([P, P], I), "afq_get_schedule": ([P, P, P], I),
     }
 
 
@@ -329,11 +329,14 @@ class AfqmcSys:
                                                round(float(t[2 * i + 1]), 4)]}
                for i, k in enumerate(self.TUNE_SITES)}
         out["splitk_slices"] = int(c[ns])
-        g = ctypes.c_int()
-        gm = np.zeros(6)
-        self._check(self.lib.afq_get_prop_group(self.h, ctypes.byref(g), _p(gm)))
-        out["propagate_walker_group"] = {"walkers": g.value,
-                                         "ms_all_32_48_64_96_128": [round(float(x), 4) for x in gm]}
+        sc = np.zeros(2, np.int32)
+        gm = np.zeros(8)
+        self._check(self.lib.afq_get_schedule(self.h, _p(sc), _p(gm)))
+        out["propagate_walker_group"] = {"walkers": int(sc[0]),
+                                         "ms_all_32_48_64_96_128": [round(float(x), 4)
+                                                                    for x in gm[:6]]}
+        out["vhs_k_slab"] = {"bytes": int(sc[1]),
+                             "ms_128_64": [round(float(x), 4) for x in gm[6:]]}
         return out
 
     SPARSE_OPERANDS = ["Spvn", "SpvnT", "Vakbl"]

@@ -1628,12 +1628,13 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms) {
   return AFQ_OK;
 }
 
-afq_status afq_get_prop_group(afq_handle* h, int* walkers, double* ms) {
-  if (!h || !walkers) return AFQ_ERR_ARG;
-  float t[6] = {};
-  *walkers = h->mixed ? afq::mixed_prop_group(h->mixed, t) : 0;
+afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms) {
+  if (!h || !sched) return AFQ_ERR_ARG;
+  float t[8] = {};
+  sched[0] = h->mixed ? afq::mixed_prop_group(h->mixed, t) : 0;
+  sched[1] = h->mixed ? afq::mixed_vhs_slab(h->mixed, t + 6) : 0;
   if (ms)
-    for (int i = 0; i < 6; i++) ms[i] = t[i];
+    for (int i = 0; i < 8; i++) ms[i] = t[i];
   return AFQ_OK;
 }
 

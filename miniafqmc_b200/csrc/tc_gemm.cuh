@@ -196,16 +196,20 @@ AFQ_D void tmem_ld32_add(uint32_t taddr, float* acc) {
 }
 
 // Shared-memory matrix descriptor: K-major operand tile written by TMA with
-// SWIZZLE_128B (rows of 128 bytes, 8-row groups 1024 bytes apart).
-AFQ_D uint64_t sdesc_k128(uint32_t saddr) {
+// SWIZZLE_128B (rows of 128 bytes, 8-row groups 1024 bytes apart) or, for SLAB = 64,
+// SWIZZLE_64B (rows of 64 bytes, 8-row groups 512 bytes apart).
+template <int SLAB = 128>
+AFQ_D uint64_t sdesc_k(uint32_t saddr) {
+  static_assert(SLAB == 128 || SLAB == 64, "K slab of 64 or 128 bytes");
   uint64_t d = 0;
   d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);   // start address
   d |= (uint64_t)1 << 16;                     // leading byte offset (unused when swizzled)
-  d |= (uint64_t)(1024 >> 4) << 32;           // stride byte offset: one 8-row group
+  d |= (uint64_t)(8 * SLAB >> 4) << 32;       // stride byte offset: one 8-row group
   d |= (uint64_t)1 << 46;                     // descriptor version for sm_100
-  d |= (uint64_t)2 << 61;                     // SWIZZLE_128B
+  d |= (uint64_t)(SLAB == 128 ? 2 : 4) << 61; // SWIZZLE_128B / SWIZZLE_64B
   return d;
 }
+AFQ_D uint64_t sdesc_k128(uint32_t saddr) { return sdesc_k<128>(saddr); }
 
 // Instruction descriptor: fp32 accumulator, A and B of the same format (0 = fp16,
 // 1 = bf16 for kind::f16; 2 = tf32 for kind::tf32), both K-major.
@@ -214,13 +218,13 @@ constexpr uint32_t idesc(int M, int N, int fmt) {
          ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-template <int BN, int STAGES, int FMT, bool SPLIT>
+template <int BN, int STAGES, int FMT, bool SPLIT, int SLAB = 128>
 struct Cfg {
   static constexpr int BM = 128;
   static constexpr int ELEM = FMT == 2 ? 4 : 2;
-  static constexpr int BK = 128 / ELEM;          // elements per 128-byte K slab
+  static constexpr int BK = SLAB / ELEM;         // elements per K slab (128 or 64 bytes)
   static constexpr int UK = 32 / ELEM;           // K of one tcgen05.mma
-  static constexpr uint32_t A_BYTES = BM * 128, B_BYTES = BN * 128;
+  static constexpr uint32_t A_BYTES = BM * SLAB, B_BYTES = BN * SLAB;
   static constexpr int PARTS = SPLIT ? 2 : 1;    // hi (and lo) parts of each operand
   static constexpr uint32_t STAGE_BYTES = PARTS * (A_BYTES + B_BYTES);
   static constexpr uint32_t TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
@@ -277,11 +281,11 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
 //   MINB = CTAs per SM the launch is compiled for (2 caps registers at 170 per thread so a
 //   lean ring's CTAs pair up on an SM).
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1, int SLAB = 128>
 __global__ void __launch_bounds__(192, MINB)
 tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step, int a_batched,
                int b_batched, int k_split, int m_fast, int z0, Epi epi, int* err) {
-  using C = Cfg<BN, STAGES, FMT, SPLIT>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -359,14 +363,14 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
         break;
       }
       tc_fence_after();
-      const uint64_t ad = sdesc_k128(smem_u32(stA(s, 0)));
-      const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
+      const uint64_t ad = sdesc_k<SLAB>(smem_u32(stA(s, 0)));
+      const uint64_t bd = sdesc_k<SLAB>(smem_u32(stB(s, 0)));
 #pragma unroll
       for (int k = 0; k < C::BK / C::UK; k++)   // advance 32 bytes along K per MMA
         umma<FMT>(tmem, ad + 2 * k, bd + 2 * k, ID, (kb | k) != 0);
       if (SPLIT) {
-        const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
-        const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
+        const uint64_t al = sdesc_k<SLAB>(smem_u32(stA(s, 1)));
+        const uint64_t bl = sdesc_k<SLAB>(smem_u32(stB(s, 1)));
 #pragma unroll
         for (int k = 0; k < C::BK / C::UK; k++) {
           umma<FMT>(tmem, ad + 2 * k, bl + 2 * k, ID, 1u);   // hi * lo
@@ -455,9 +459,9 @@ struct TileSched {
   }
 };
 
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG, int SLAB = 128>
 struct PCfg {
-  using C = Cfg<BN, STAGES, FMT, SPLIT>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   static constexpr int NEPI = 128 * EPI_WG, THREADS = NEPI + 64;
   static constexpr uint32_t ACC_COLS = 2 * C::TMEM_COLS;
   static constexpr size_t SCRATCH = (size_t)EpiScratch<Epi>::value * EPI_WG;
@@ -466,13 +470,13 @@ struct PCfg {
   static constexpr bool kFits = SMEM <= 227 * 1024 && ACC_COLS <= 512;
 };
 
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG, int SLAB = 128>
 __global__ void __launch_bounds__(128 * EPI_WG + 64, 1)
 tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
                           int a_batched, int b_batched, int k_split, TileSched sched, Epi epi,
                           int* err) {
-  using C = Cfg<BN, STAGES, FMT, SPLIT>;
-  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
+  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG, SLAB>;
   static_assert(!Epi::kTile, "tile epilogues reuse the operand ring: per-tile kernel only");
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -576,14 +580,14 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
             break;
           }
           tc_fence_after();
-          const uint64_t ad = sdesc_k128(smem_u32(stA(s, 0)));
-          const uint64_t bd = sdesc_k128(smem_u32(stB(s, 0)));
+          const uint64_t ad = sdesc_k<SLAB>(smem_u32(stA(s, 0)));
+          const uint64_t bd = sdesc_k<SLAB>(smem_u32(stB(s, 0)));
 #pragma unroll
           for (int k = 0; k < C::BK / C::UK; k++)
             umma<FMT>(d, ad + 2 * k, bd + 2 * k, ID, (kb != kb0 || k != 0) ? 1u : 0u);
           if (SPLIT) {
-            const uint64_t al = sdesc_k128(smem_u32(stA(s, 1)));
-            const uint64_t bl = sdesc_k128(smem_u32(stB(s, 1)));
+            const uint64_t al = sdesc_k<SLAB>(smem_u32(stA(s, 1)));
+            const uint64_t bl = sdesc_k<SLAB>(smem_u32(stB(s, 1)));
 #pragma unroll
             for (int k = 0; k < C::BK / C::UK; k++) {
               umma<FMT>(d, ad + 2 * k, bl + 2 * k, ID, 1u);
@@ -696,10 +700,11 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
 
 // ------------------------------------------------------------------ host side
 // Tensor map of a [batch][rows][K] K-major operand (rows strided by ld elements, batches
-// by sbatch elements), tiles of box_rows x 128 bytes, SWIZZLE_128B, zero fill outside.
+// by sbatch elements), tiles of box_rows x slab bytes (128: SWIZZLE_128B, 64:
+// SWIZZLE_64B), zero fill outside.
 inline CUresult make_kmajor_map(CUtensorMap* map, const void* base, bool fp32, uint64_t K,
                                 uint64_t rows, uint64_t batch, uint64_t ld, uint64_t sbatch,
-                                uint32_t box_rows) {
+                                uint32_t box_rows, uint32_t slab = 128) {
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     cudaDriverEntryPointQueryResult q;
@@ -711,11 +716,12 @@ inline CUresult make_kmajor_map(CUtensorMap* map, const void* base, bool fp32, u
   const uint32_t esz = fp32 ? 4 : 2;
   cuuint64_t dims[3] = {K, rows, batch};
   cuuint64_t strides[2] = {ld * esz, (batch > 1 ? sbatch : rows * ld) * esz};
-  cuuint32_t box[3] = {128 / esz, box_rows, 1};
+  cuuint32_t box[3] = {slab / esz, box_rows, 1};
   cuuint32_t es[3] = {1, 1, 1};
   return encode(map, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3,
                 const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                slab == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 }
 
@@ -732,15 +738,15 @@ struct GemmShape {
                        // (and epilogue outputs) that hold more (no split-K)
 };
 
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1, int SLAB = 128>
 cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
                    cudaStream_t st) {
-  using C = Cfg<BN, STAGES, FMT, SPLIT>;
+  using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
                 "tile epilogue needs the operand ring to hold the fp32 tile");
   static_assert(MINB * C::SMEM <= 228 * 1024 && MINB * C::TMEM_COLS <= 512,
                 "CTAs per SM exceed shared memory or TMEM");
-  auto kern = tc_gemm_kernel<BN, STAGES, FMT, SPLIT, Epi, MINB>;
+  auto kern = tc_gemm_kernel<BN, STAGES, FMT, SPLIT, Epi, MINB, SLAB>;
   static DeviceAttr attr;
   cudaError_t e = attr.ensure(C::SMEM, [kern](size_t b) {
     cudaError_t r = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
@@ -769,12 +775,12 @@ inline int sm_count() {
   return n;
 }
 
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG = 1>
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG = 1, int SLAB = 128>
 cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
                               cudaStream_t st) {
-  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
+  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG, SLAB>;
   static_assert(P::kFits, "persistent configuration exceeds shared memory or TMEM");
-  auto kern = tc_gemm_persistent_kernel<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
+  auto kern = tc_gemm_persistent_kernel<BN, STAGES, FMT, SPLIT, Epi, EPI_WG, SLAB>;
   static DeviceAttr attr;
   cudaError_t e = attr.ensure(P::SMEM, [kern](size_t b) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);

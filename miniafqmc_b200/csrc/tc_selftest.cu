@@ -28,14 +28,19 @@ template <int BN, bool TF32>
 cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, int batch,
                 int mode, int* derr, cudaStream_t st) {
   tc::Maps maps;
-  if (tc::make_kmajor_map(&maps.a, dA, TF32, K, M, batch, K, (uint64_t)M * K, 128) != CUDA_SUCCESS)
+  const uint32_t slab = mode >= 3 ? 64 : 128;   // modes 3 / 4: 64-byte K slabs
+  if (tc::make_kmajor_map(&maps.a, dA, TF32, K, M, batch, K, (uint64_t)M * K, 128, slab) !=
+      CUDA_SUCCESS)
     return cudaErrorInvalidValue;
-  if (tc::make_kmajor_map(&maps.b, dB, TF32, K, N, batch, K, (uint64_t)N * K, BN) != CUDA_SUCCESS)
+  if (tc::make_kmajor_map(&maps.b, dB, TF32, K, N, batch, K, (uint64_t)N * K, BN, slab) !=
+      CUDA_SUCCESS)
     return cudaErrorInvalidValue;
   maps.a_lo = maps.a;
   maps.b_lo = maps.b;
   tc::GemmShape g{M, N, K, batch, 128, (M + 127) / 128, true, true, 0};
   EpiStoreF32 epi{dC, M, N, (long long)M * N};
+  if (mode == 3) return tc::launch<BN, 4, (TF32 ? 2 : 1), false, EpiStoreF32, 1, 64>(maps, g, epi, derr, st);
+  if (mode == 4) return tc::launch_persistent<BN, 4, (TF32 ? 2 : 1), false, EpiStoreF32, 1, 64>(maps, g, epi, derr, st);
   if (mode == 1) return tc::launch_persistent<BN, 4, (TF32 ? 2 : 1), false, EpiStoreF32, 1>(maps, g, epi, derr, st);
   if (mode == 2) return tc::launch_persistent<BN, 4, (TF32 ? 2 : 1), false, EpiStoreF32, 2>(maps, g, epi, derr, st);
   return tc::launch<BN, 4, (TF32 ? 2 : 1), false>(maps, g, epi, derr, st);
@@ -46,7 +51,7 @@ cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, 
 extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn,
                                           int mode, const float* A, const float* B, float* C,
                                           int* kernel_err) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C || mode < 0 || mode > 2)
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C || mode < 0 || mode > 4)
     return AFQ_ERR_ARG;
   if (K % 8 != 0) return AFQ_ERR_UNSUPPORTED;   // 16-byte row strides for TMA
   const size_t na = (size_t)batch * M * K, nb = (size_t)batch * N * K, nc = (size_t)batch * M * N;

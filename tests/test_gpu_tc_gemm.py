@@ -38,7 +38,8 @@ def run(M, N, K, batch, tf32, bn, seed=0, mode=0):
 @pytest.mark.parametrize("shape", [(128, 128, 64, 1, 128), (300, 200, 768, 3, 128),
                                    (256, 192, 1024, 2, 192), (100, 64, 72, 1, 64),
                                    (384, 192, 768, 4, 192)])
-@pytest.mark.parametrize("mode", [0, 1, 2])   # per-tile, persistent x1 / x2 epilogue groups
+# per-tile, persistent x1 / x2 epilogue groups; per-tile and persistent with 64-byte K slabs
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4])
 def test_tc_gemm_matches_reference(shape, tf32, mode):
     M, N, K, batch, bn = shape
     C, ref = run(M, N, K, batch, tf32, bn, mode=mode)
