@@ -157,9 +157,11 @@ def test_grouped_propagation_chain_is_bit_identical(monkeypatch):
     """The mixed propagation chain run walker group by walker group (AFQ_PROP_GROUP) gives
     the walkers of the chain over all walkers at once, bit for bit (same tiles, same
     epilogues, another launch order), through graph substeps with a re-orthogonalisation.
-    The split-K slice count, which sets the vbias summation order, is forced to one value
-    so the two handles' separate tuning runs cannot pick different ones."""
+    The kernel of every product site and the split-K slice count are forced (AFQ_TUNE=1,
+    AFQ_SPLITK) so the two handles' separate tuning runs cannot pick different ones (other
+    kernel choices agree to 1e-12, not bit for bit)."""
     from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    monkeypatch.setenv("AFQ_TUNE", "1")
     monkeypatch.setenv("AFQ_SPLITK", "2")
     s = system("C2", with_vakbl=False)
     nw = 80
