@@ -276,11 +276,7 @@ afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
  *   stay in L2 between its products; 0 = every product over all walkers at once.  Timed:
  *   0, 32, 48, 64, 96 and 128 walkers (those below nwalk) -> ms[0..5].  Results do not
  *   depend on it.  AFQ_PROP_GROUP=<walkers> forces one.
- * sched[1]: K slab of the vHS product in bytes, 128 (two 96 KB split stages) or 64 (four
- *   48 KB stages, SWIZZLE_64B operand tiles).  Timed -> ms[6..7].  The slab sets the order
- *   of the MMAs' fp32 accumulation, so it changes vHS in the last bits.  AFQ_VHS_SLAB=64 or
- *   128 forces one; a forced kernel (AFQ_TUNE=1 or 2) keeps 128.
- * ms[8] may be NULL; 0 where not timed. */
+ * ms[6] may be NULL; 0 where not timed. */
 afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */

@@ -65,9 +65,6 @@ cudaError_t mixed_set_wait_clocks(long long clocks);
 // Walkers per group of the propagation chain picked at set-up (0: all walkers per
 // product) and, in ms[6], the timed chain for 0 (all), 32, 48, 64, 96 and 128 walkers.
 int mixed_prop_group(const MixedState* m, float* ms);
-// K slab in bytes of the vHS product picked at set-up (128 or 64) and, in ms[2], the timed
-// product for each (0 when not timed).
-int mixed_vhs_slab(const MixedState* m, float* ms);
 void mixed_tuning(const MixedState* m, int* choice, float* ms);
 // FP64 copy of the V operand ([nw][N*N]), for copy-out.
 cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st);

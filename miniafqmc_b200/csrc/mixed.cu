@@ -141,11 +141,6 @@ struct MixedState {
   // density matrix: its row-strided stores cost the epilogue more than the pack kernel.)
   Op F2;
   tc::Maps m_pw2, m_t1_1;
-  // vHS product with 64-byte K slabs (SWIZZLE_64B maps): a four-stage split ring in the
-  // shared memory of the two-stage 128-byte one; picked by the set-up tuner (vhs_slab)
-  tc::Maps m_vhs64;
-  int vhs_slab = 128;
-  float vhs_slab_ms[2] = {};
   bool packed = false;
   int fa_buf = 0;
   // kernel of each product site (0 built-in rule, 1 persistent, 2 per-tile), chosen at
@@ -1540,8 +1535,6 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   const int bnv = 256;
   const uint64_t vrows = m->vsym ? (uint64_t)m->npairs * 256 : (uint64_t)N * N;
   ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv);
-  ok &= map2(m->m_vhs64, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv,
-             64);
   const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
   {
     const uint64_t Kp = m->preal ? N : 2 * N;
@@ -1636,12 +1629,6 @@ static cudaError_t vhs_product(MixedState* m, cudaStream_t st) {
     tc::GemmShape g{2 * nw, m->npairs * 256, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0,
                     true};
     EpiVhsSym epi{m->Vf, nw, N, m->pairs};
-    if (m->vhs_slab == 64 && m->prec_vhs == PREC_SPLIT) {   // four 48 KB split stages
-      if (m->tune[TS_VHS] == 1)
-        return tc::launch_persistent<256, 4, 1, true, EpiVhsSym, 2, 64>(m->m_vhs64, g, epi,
-                                                                        m->err, st);
-      return tc::launch<256, 4, 1, true, EpiVhsSym, 1, 64>(m->m_vhs64, g, epi, m->err, st);
-    }
     return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, m->tune[TS_VHS]);
   }
   tc::GemmShape g{2 * nw, N * N, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0, true};
@@ -1921,7 +1908,6 @@ struct TuneRec {
   float ms[TS_N][2];
   int splits;
   int prop_group;
-  int vhs_slab;
 };
 std::mutex tune_mu;
 std::map<std::string, TuneRec>& tune_cache() {
@@ -1953,7 +1939,7 @@ void tune_load(const char* path) {
     bool ok = true;
     for (int i = 0; i < TS_N && ok; i++)
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
-    if (!ok || fscanf(f, "%d %d %d", &r.splits, &r.prop_group, &r.vhs_slab) != 3) break;
+    if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
     tune_cache()[key] = r;
     tune_file_keys().insert(key);
   }
@@ -1965,7 +1951,7 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   if (!f) return;
   fprintf(f, "%s", key.c_str());
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
-  fprintf(f, " %d %d %d\n", r.splits, r.prop_group, r.vhs_slab);
+  fprintf(f, " %d %d\n", r.splits, r.prop_group);
   fclose(f);
 }
 }  // namespace
@@ -1980,9 +1966,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   if (force < 0 && !tc_persistent()) force = 2;   // AFQ_TC_PERSISTENT=0: per-tile kernels
   const char* fsk = getenv("AFQ_SPLITK");
   const char* fpg = getenv("AFQ_PROP_GROUP");
-  const char* fvs = getenv("AFQ_VHS_SLAB");
-  const std::string key = tune_key(m) + "_pg" + std::to_string(fpg ? atoi(fpg) : -1) + "_vs" +
-                          std::to_string(fvs ? atoi(fvs) : 0) + "_f" +
+  const std::string key = tune_key(m) + "_pg" + std::to_string(fpg ? atoi(fpg) : -1) + "_f" +
                           std::to_string(force) + "_k" +
                           std::to_string(fsk ? atoi(fsk) : 0) + "_p" +
                           std::to_string(promote_kb(PROMOTE_PART)) +
@@ -2004,7 +1988,6 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
         if (m->splits > m->part_cap) set_splits(m, m->splits0);
       }
       m->prop_group = r.prop_group;
-      m->vhs_slab = r.vhs_slab == 64 ? 64 : 128;
       tune_save(cache_path, key, r);   // a shape timed before the file was named
       return cudaSuccess;
     }
@@ -2081,22 +2064,6 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     m->tune[site] = best;
   };
   pick(TS_VHS, [&] { return vhs_product(m, st); });
-  // then the K slab of the chosen vHS kernel (full tuning only: a forced kernel keeps the
-  // 128-byte slab, so forced runs stay comparable bit for bit); AFQ_VHS_SLAB=64|128 forces
-  if (m->vsym && m->prec_vhs == PREC_SPLIT && m->tune[TS_VHS] && force < 0) {
-    const char* fs = getenv("AFQ_VHS_SLAB");
-    float t[2] = {0.0f, 0.0f};
-    for (int i = 0; i < 2; i++) {
-      const int slab = i ? 64 : 128;
-      if (fs && atoi(fs) != slab) continue;
-      m->vhs_slab = slab;
-      const float ms = timed([&] { return vhs_product(m, st); });
-      t[i] = ms > 0.0f ? ms : 0.0f;
-    }
-    m->vhs_slab = (t[1] > 0.0f && (t[0] <= 0.0f || t[1] < t[0])) ? 64 : 128;
-    m->vhs_slab_ms[0] = t[0];
-    m->vhs_slab_ms[1] = t[1];
-  }
   {
     const int mt = (N + 127) / 128, n2 = 2 * n;
     const int Kp = m->preal ? N : 2 * N;
@@ -2198,7 +2165,6 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     }
     r.splits = m->splits;
     r.prop_group = m->prop_group;
-    r.vhs_slab = m->vhs_slab;
     std::lock_guard<std::mutex> lk(tune_mu);
     tune_cache()[key] = r;
     tune_save(cache_path, key, r);
@@ -2219,12 +2185,6 @@ int mixed_prop_group(const MixedState* m, float* ms) {
   if (ms)
     for (int i = 0; i < 6; i++) ms[i] = m ? m->prop_group_ms[i] : 0.0f;
   return m ? m->prop_group : 0;
-}
-
-int mixed_vhs_slab(const MixedState* m, float* ms) {
-  if (ms)
-    for (int i = 0; i < 2; i++) ms[i] = m ? m->vhs_slab_ms[i] : 0.0f;
-  return m ? m->vhs_slab : 0;
 }
 
 void mixed_tuning(const MixedState* m, int* choice, float* ms) {

@@ -447,8 +447,9 @@ struct TileSched {
   AFQ_HD int total() const { return m_tiles * n_tiles * nbatch; }
   AFQ_D void decode(int t, int& z, int& mt, int& nt) const {
     const int per = m_tiles * n_tiles;
-    z = z0 + t / per;
-    const int r = t - z * per;
+    const int zl = t / per;   // batch within the launch
+    const int r = t - zl * per;
+    z = z0 + zl;
     if (m_fast) {
       mt = r % m_tiles;
       nt = r / m_tiles;

@@ -243,34 +243,3 @@ def test_copy_walkers_between_forms():
         other.copy_walkers_from(d)
     for e in (d, m, other):
         e.close()
-
-
-def test_vhs_with_64_byte_k_slabs(monkeypatch):
-    """The vHS product with 64-byte K slabs (four SWIZZLE_64B split stages) against the
-    128-byte one (same products, another MMA accumulation order: 1e-6 relative) and the
-    FP64 form (the split-bf16 tolerance)."""
-    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
-    monkeypatch.delenv("AFQ_TUNE", raising=False)
-    s = system("C2", with_vakbl=False)
-    nw = 64
-    wk = perturbed(s, nw)
-    out = {}
-    for slab in ("128", "64"):
-        monkeypatch.setenv("AFQ_VHS_SLAB", slab)
-        m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=wk, use_vakbl=False)
-        assert m.tuning()["vhs_k_slab"]["bytes"] == int(slab)
-        m.calculate_mixed_density_matrix()
-        m.get_vbias()
-        m.sigma(3, 1)
-        m.get_vHS()
-        out[slab] = m.copy_out("vHS")
-        m.close()
-    d = AfqmcSys(s, nw, precision=AFQ_PREC_FP64, walkers=wk, use_vakbl=False)
-    d.calculate_mixed_density_matrix()
-    d.get_vbias()
-    d.sigma(3, 1)
-    d.get_vHS()
-    ref = d.copy_out("vHS")
-    d.close()
-    assert rel(out["64"], out["128"]) < 1e-6
-    assert rel(out["64"], ref) < 1e-4
