@@ -497,9 +497,10 @@ def timed(form, steps, start, torch, dist, world, profile=False, record=True):
 def run_c5(args, torch):
     """Heterogeneous batch (three systems of uneven NMO, electron count and nchol, mixed
     form, one control variate each): K substeps advanced as one CUDA-graph launch per
-    substep for all systems (AfqmcBatch), against the same systems each launching its own
-    substep graph on its own stream (independent) and one after another with a
-    synchronisation between systems (serial).  Energies every energy_every substeps.
+    substep for all systems (AfqmcBatch), against the fused batch (the vHS product and each
+    propagation product one launch over all systems' tiles), the same systems each
+    launching its own substep graph on its own stream (independent) and one after another
+    with a synchronisation between systems (serial).  Energies every energy_every substeps.
     Times are wall clock around device-synchronised loops (several streams)."""
     from miniafqmc_b200.synthetic import C5_SYSTEMS, make_system
     from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_MIXED
@@ -535,7 +536,9 @@ def run_c5(args, torch):
 
     def run(mode):
         engs = fresh()
-        batch = AfqmcBatch(engs) if mode == "batch" else None
+        batch = AfqmcBatch(engs) if mode in ("batch", "fused") else None
+        if mode == "fused":
+            batch.set_fused(True)
 
         def step(st):
             if batch is not None:   # one launch per measurement interval
@@ -574,7 +577,7 @@ def run_c5(args, torch):
             e.close()
         return sum(nws) * args.steps / wall, wall, cv, tun
 
-    res = {m: run(m) for m in ("batch", "independent", "serial")}
+    res = {m: run(m) for m in ("batch", "fused", "independent", "serial")}
     v, wall, cv, tun = res["batch"]
     line = {
         "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
@@ -586,6 +589,7 @@ def run_c5(args, torch):
                                "10% sparse Cholesky, mixed form, control variate per system",
                    "energy_every": args.energy_every, "timing": "wall clock, device-synchronised",
                    "kernel_tuning": tun},
+        "fused_batch": {"value": res["fused"][0], "unit": METRIC},
         "independent_streams": {"value": res["independent"][0], "unit": METRIC},
         "serial": {"value": res["serial"][0], "unit": METRIC},
         "control_variate": cv,

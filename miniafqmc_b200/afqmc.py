@@ -38,7 +38,7 @@ EXPORTS = [
     "afq_get_tuning", "afq_halfrotate", "afq_population_control",
     "afq_mixed_density_matrix_full", "afq_vbias_full", "afq_get_sparse_paths",
     "afq_set_tc_wait_limit", "afq_substep_begin", "afq_substep_end", "afq_batch_substeps",
-    "afq_copy_walkers", "afq_get_schedule",
+    "afq_copy_walkers", "afq_get_schedule", "afq_batch_set_fused",
 ]
 STAGES = ["DM", "vbias", "sigma", "vHS", "propagate", "overlap", "weights", "ortho", "energy"]
 
@@ -103,6 +103,7 @@ def signatures() -> dict:
         "afq_substep_begin": ([P, U64, U64, P], I), "afq_substep_end": ([P, U64, I], I),
         "afq_batch_substeps": ([P, P, U64, I, I], I),
         "afq_copy_walkers": ([P, P], I), "afq_get_schedule": ([P, P, P], I),
+        "afq_batch_set_fused": ([P, I], I),
     }
 
 
@@ -443,6 +444,14 @@ class AfqmcBatch:
         if st != 0:
             raise AfqmcError(st, "afq_batch_create failed")
         self.b = h
+
+    def set_fused(self, fused: bool = True):
+        """Fused batch (afq_batch_set_fused): the vHS product and each propagation product
+        as one launch over every system's tiles.  Raises AfqmcError when a system is not
+        in the mixed form or the systems' precisions, Taylor orders or vHS forms differ."""
+        st = self.lib.afq_batch_set_fused(self.b, 1 if fused else 0)
+        if st != 0:
+            raise AfqmcError(st, "afq_batch_set_fused failed")
 
     def substep(self, seeds, step_tot: int, northo: int):
         sd = np.ascontiguousarray(seeds, dtype=np.uint64)

@@ -1438,6 +1438,9 @@ struct afq_batch {
   // recorded by the graph at the end of each system's branch (external event nodes): a
   // handle's later work waits for its own system only, not for the whole batch
   std::vector<cudaEvent_t> sysdone;
+  // fused: the vHS product and the propagation chain of every system run as one launch
+  // each over all systems' tiles (mixed-form systems of matching precisions)
+  bool fused = false;
   // one graph per (substeps per launch, which of them re-orthogonalise)
   struct Graph {
     cudaGraphExec_t exec = nullptr;
@@ -1458,6 +1461,75 @@ void batch_release(afq_batch* b) {
   if (b->done) cudaEventDestroy(b->done);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
+}
+
+void count_launches(afq_handle* h, int stage, long long k) {
+  (h->launch_sink ? h->launch_sink : h->stage_launches)[stage] += k;
+}
+
+// One substep of every system of a fused batch.  Each system's stages up to sigma, and
+// from the overlaps on, run on its own stream; the vHS product and the eight products of
+// the propagation chain are joint launches on the batch stream (counted on the first
+// system), with the systems' streams joined before and forked after them.
+cudaError_t batch_substep_fused(afq_batch* b, bool ortho) {
+  const int n = (int)b->hs.size();
+  std::vector<afq::MixedState*> ms(n);
+  std::vector<z_t*> W(n);
+  for (int i = 0; i < n; i++) {
+    ms[i] = b->hs[i]->mixed;
+    W[i] = b->hs[i]->W;
+  }
+  auto join = [&]() {
+    for (int i = 0; i < n; i++) {
+      cudaError_t r = cudaEventRecord(b->pre[i], b->hs[i]->st);
+      if (r == cudaSuccess) r = cudaStreamWaitEvent(b->st, b->pre[i], 0);
+      if (r != cudaSuccess) return r;
+    }
+    return cudaSuccess;
+  };
+  auto fork = [&]() {
+    cudaError_t r = cudaEventRecord(b->fork, b->st);
+    for (int i = 0; i < n && r == cudaSuccess; i++) r = cudaStreamWaitEvent(b->hs[i]->st, b->fork, 0);
+    return r;
+  };
+  cudaError_t e;
+  for (afq_handle* h : b->hs) {
+    if ((e = st_dm(h, 1, 0)) != cudaSuccess || (e = st_vbias(h)) != cudaSuccess ||
+        (e = st_sigma(h, 0)) != cudaSuccess)
+      return e;
+    if ((e = staged(h, AFQ_STAGE_VHS, 1, [&] { return afq::mixed_vhs_pack(h->mixed, h->X, h->st); })) !=
+        cudaSuccess)
+      return e;
+  }
+  if ((e = join()) != cudaSuccess) return e;
+  count_launches(b->hs[0], AFQ_STAGE_VHS, 1);
+  if ((e = afq::mixed_vhs_multi(ms.data(), n, b->st)) != cudaSuccess) return e;
+  if ((e = fork()) != cudaSuccess) return e;
+  for (afq_handle* h : b->hs) {
+    h->dm_cache = false;
+    if ((e = staged(h, AFQ_STAGE_PROPAGATE, afq::mixed_prop_pack_launches(h->mixed),
+                    [&] { return afq::mixed_prop_pack(h->mixed, h->W, h->st); })) != cudaSuccess)
+      return e;
+  }
+  if ((e = join()) != cudaSuccess) return e;
+  count_launches(b->hs[0], AFQ_STAGE_PROPAGATE, b->hs[0]->d.taylor_order + 2);
+  if ((e = afq::mixed_prop_multi(ms.data(), W.data(), n, b->st)) != cudaSuccess) return e;
+  if ((e = fork()) != cudaSuccess) return e;
+  for (afq_handle* h : b->hs) {
+    if ((e = st_dm(h, 0, 1)) != cudaSuccess || (e = st_weights(h, 1)) != cudaSuccess) return e;
+    if (ortho && ((e = st_ortho(h)) != cudaSuccess || (e = st_dm(h, 0, 0)) != cudaSuccess))
+      return e;
+  }
+  return cudaSuccess;
+}
+
+bool batch_fusable(const afq_batch* b) {
+  std::vector<afq::MixedState*> ms;
+  for (afq_handle* h : b->hs) {
+    if (!h->mixed) return false;
+    ms.push_back(h->mixed);
+  }
+  return afq::mixed_multi_compatible(ms.data(), (int)ms.size());
 }
 }  // namespace
 
@@ -1519,7 +1591,10 @@ afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step
     if (h->profiling) return fail(h, AFQ_ERR_STATE, "stage profiling is on");
     if (seeds[i] != h->host_seed || step_tot != h->host_step)
       if ((s = set_scalars(h, seeds[i], step_tot)) != AFQ_OK) return s;
-    if (h->mixed) AFQ_CUDA(h, afq::mixed_ensure_packed(h->mixed, h->W, h->st));
+    // the fused chain starts from W itself: every capture and launch of its graph sees
+    // no packed forms
+    if (h->mixed && b->fused) afq::mixed_invalidate(h->mixed);
+    if (h->mixed && !b->fused) AFQ_CUDA(h, afq::mixed_ensure_packed(h->mixed, h->W, h->st));
     if (mixed_dm_on(h) && !h->dm_cache) AFQ_CUDA(h, st_dm(h, 0, 0));
     AFQ_CUDA(h, cudaEventRecord(b->pre[i], h->st));
     if (cudaStreamWaitEvent(b->st, b->pre[i], 0) != cudaSuccess) return AFQ_ERR_CUDA;
@@ -1532,7 +1607,26 @@ afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step
       return AFQ_ERR_CUDA;
     cudaError_t e = cudaEventRecord(b->fork, b->st);
     gr.counts.assign(n, std::vector<long long>(AFQ_NSTAGES, 0));
-    for (int i = 0; i < n && e == cudaSuccess; i++) {
+    if (b->fused) {
+      for (int i = 0; i < n && e == cudaSuccess; i++) {
+        afq_handle* h = b->hs[i];
+        e = cudaStreamWaitEvent(h->st, b->fork, 0);
+        h->capturing = true;
+        h->launch_sink = gr.counts[i].data();
+      }
+      for (int k = 0; k < nsub && e == cudaSuccess; k++)
+        e = batch_substep_fused(b, (omask >> k) & 1);
+      for (int i = 0; i < n; i++) {
+        afq_handle* h = b->hs[i];
+        h->launch_sink = nullptr;
+        h->capturing = false;
+        if (e == cudaSuccess)
+          e = cudaEventRecordWithFlags(b->sysdone[i], h->st, cudaEventRecordExternal);
+        if (e == cudaSuccess) e = cudaEventRecord(b->join[i], h->st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->st, b->join[i], 0);
+      }
+    }
+    for (int i = 0; i < n && e == cudaSuccess && !b->fused; i++) {
       afq_handle* h = b->hs[i];
       if ((e = cudaStreamWaitEvent(h->st, b->fork, 0)) != cudaSuccess) break;
       h->capturing = true;
@@ -1569,6 +1663,20 @@ afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step
 afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_tot,
                              int northo) {
   return afq_batch_substeps(b, seeds, step_tot, 1, northo);
+}
+
+afq_status afq_batch_set_fused(afq_batch* b, int fused) {
+  if (!b || (fused != 0 && fused != 1)) return AFQ_ERR_ARG;
+  if (fused && !batch_fusable(b)) return AFQ_ERR_UNSUPPORTED;
+  cudaSetDevice(b->device);
+  if (b->fused != (fused != 0)) {   // graphs of the other mode
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return AFQ_ERR_CUDA;
+    for (auto& kv : b->g)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    b->g.clear();
+    b->fused = fused != 0;
+  }
+  return AFQ_OK;
 }
 
 afq_status afq_batch_synchronize(afq_batch* b) {

@@ -66,6 +66,17 @@ cudaError_t mixed_set_wait_clocks(long long clocks);
 // product) and, in ms[6], the timed chain for 0 (all), 32, 48, 64, 96 and 128 walkers.
 int mixed_prop_group(const MixedState* m, float* ms);
 void mixed_tuning(const MixedState* m, int* choice, float* ms);
+// Heterogeneous batches: the vHS product and the propagation chain of n systems (n <= 4),
+// each product one launch over every system's tiles.  mixed_multi_compatible: the systems
+// share the precisions, Taylor order and vHS form.  mixed_vhs_pack / mixed_prop_pack
+// (on each system's stream, before the joint launches) pack X and, unless current, the
+// P W operand; mixed_prop_multi leaves no packed walker forms current.
+bool mixed_multi_compatible(MixedState* const* ms, int n);
+cudaError_t mixed_vhs_pack(MixedState* m, const z_t* X, cudaStream_t st);
+cudaError_t mixed_vhs_multi(MixedState* const* ms, int n, cudaStream_t st);
+cudaError_t mixed_prop_pack(MixedState* m, const z_t* W, cudaStream_t st);
+int mixed_prop_pack_launches(const MixedState* m);
+cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaStream_t st);
 // FP64 copy of the V operand ([nw][N*N]), for copy-out.
 cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st);
 

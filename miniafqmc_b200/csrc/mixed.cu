@@ -1636,11 +1636,15 @@ static cudaError_t vhs_product(MixedState* m, cudaStream_t st) {
   return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, m->tune[TS_VHS]);
 }
 
-cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
+cudaError_t mixed_vhs_pack(MixedState* m, const z_t* X, cudaStream_t st) {
   const int nc = m->nc, nw = m->nw;
   pack_x_kernel<<<dim3((nc + 31) / 32, (nw + 31) / 32), dim3(32, 8), 0, st>>>(X, nc, nw, m->Kv,
                                                                              m->s_real, m->Xf);
-  cudaError_t e = cudaGetLastError();
+  return cudaGetLastError();
+}
+
+cudaError_t mixed_vhs(MixedState* m, const z_t* X, z_t*, cudaStream_t st) {
+  cudaError_t e = mixed_vhs_pack(m, X, st);
   if (e != cudaSuccess) return e;
   return vhs_product(m, st);
 }
@@ -1711,6 +1715,160 @@ cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) 
 
 void mixed_invalidate(MixedState* m) {
   if (m) m->packed = false;
+}
+
+// ------------------------------------------------------------ heterogeneous batches
+// The vHS product and the eight products of the propagation chain of several systems,
+// each product one launch over the work list of every system's (walker, M tile, N tile)
+// tiles (tc::launch_multi, per-tile CTAs).  The systems share the precisions, the Taylor
+// order and the vHS form; the chain runs the tile epilogue (EpiProp) for every system, so
+// no system's packed walker forms survive it (the overlap stage packs its own operand).
+namespace {
+constexpr int kMultiMax = 4;
+
+template <class Epi>
+void multi_add(tc::MultiJob<Epi, kMultiMax>& job, int i, const tc::Maps& mp, const Epi& ep,
+               int K, int m_tiles, int n_tiles, int bn, int batch, int a_batched,
+               int b_batched, int& t) {
+  job.maps[i] = mp;
+  job.epi[i] = ep;
+  job.K[i] = K;
+  job.m_step[i] = 128;
+  job.n_step[i] = bn;
+  job.bn[i] = bn;
+  job.m_tiles[i] = m_tiles;
+  job.n_tiles[i] = n_tiles;
+  job.a_batched[i] = a_batched;
+  job.b_batched[i] = b_batched;
+  job.tile0[i] = t;
+  t += batch * m_tiles * n_tiles;
+}
+
+template <class Epi>
+cudaError_t multi_run(int prec, const tc::MultiJob<Epi, kMultiMax>& job, int* err,
+                      cudaStream_t st) {
+  if (prec == PREC_SPLIT) return tc::launch_multi<256, 2, 1, true, Epi, kMultiMax>(job, err, st);
+  if (prec == PREC_BF16) return tc::launch_multi<256, 4, 1, false, Epi, kMultiMax>(job, err, st);
+  return cudaErrorInvalidValue;
+}
+}  // namespace
+
+bool mixed_multi_compatible(MixedState* const* ms, int n) {
+  if (n < 1 || n > kMultiMax) return false;
+  for (int i = 0; i < n; i++) {
+    const MixedState* m = ms[i];
+    const MixedState* a = ms[0];
+    if (!m || m->prec_vhs != a->prec_vhs || m->prec_p != a->prec_p || m->prec_v1 != a->prec_v1 ||
+        m->prec_vk != a->prec_vk || m->in.order != a->in.order || m->vsym != a->vsym ||
+        m->bn_prop < 32 || m->bn_prop > 256 || 4 * m->n > m->bn_prop)
+      return false;
+    for (int p : {m->prec_vhs, m->prec_p, m->prec_v1, m->prec_vk})
+      if (p != PREC_SPLIT && p != PREC_BF16) return false;
+  }
+  return true;
+}
+
+cudaError_t mixed_vhs_multi(MixedState* const* ms, int n, cudaStream_t st) {
+  if (!mixed_multi_compatible(ms, n)) return cudaErrorInvalidValue;
+  int t = 0;
+  if (ms[0]->vsym) {
+    tc::MultiJob<EpiVhsSym, kMultiMax> job{};
+    for (int i = 0; i < n; i++) {
+      MixedState* m = ms[i];
+      multi_add(job, i, m->m_vhs, EpiVhsSym{m->Vf, m->nw, m->N, m->pairs}, m->Kv,
+                (2 * m->nw + 127) / 128, m->npairs, 256, 1, 0, 0, t);
+    }
+    job.tile0[n] = t;
+    job.np = n;
+    return multi_run(ms[0]->prec_vhs, job, ms[0]->err, st);
+  }
+  tc::MultiJob<EpiVhs, kMultiMax> job{};
+  for (int i = 0; i < n; i++) {
+    MixedState* m = ms[i];
+    const long long NN = (long long)m->N * m->N;
+    multi_add(job, i, m->m_vhs, EpiVhs{m->Vf, m->nw, NN}, m->Kv, (2 * m->nw + 127) / 128,
+              (int)((NN + 255) / 256), 256, 1, 0, 0, t);
+  }
+  job.tile0[n] = t;
+  job.np = n;
+  return multi_run(ms[0]->prec_vhs, job, ms[0]->err, st);
+}
+
+cudaError_t mixed_prop_pack(MixedState* m, const z_t* W, cudaStream_t st) {
+  if (m->packed) return cudaSuccess;   // the P W operand is in F2
+  const bool pr = m->preal && m->in.order >= 1;
+  pack_w_kernel<<<dim3((m->N + 31) / 32, (2 * m->n + 31) / 32, m->nw), dim3(32, 8), 0, st>>>(
+      W, m->N, 2 * m->n, m->F[0], pr ? 2 : 1);
+  return cudaGetLastError();
+}
+
+int mixed_prop_pack_launches(const MixedState* m) { return m->packed ? 0 : 1; }
+
+cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaStream_t st) {
+  if (!mixed_multi_compatible(ms, n)) return cudaErrorInvalidValue;
+  const int order = ms[0]->in.order;
+  bool from_f2[kMultiMax];
+  for (int i = 0; i < n; i++) {
+    from_f2[i] = ms[i]->packed;
+    ms[i]->packed = false;
+  }
+  auto shape = [&](const MixedState* m, int& mt, int& nt) {
+    mt = (m->N + 127) / 128;
+    nt = (4 * m->n + m->bn_prop - 1) / m->bn_prop;
+  };
+  cudaError_t e;
+  {  // S = P W
+    tc::MultiJob<EpiProp, kMultiMax> job{};
+    int t = 0;
+    for (int i = 0; i < n; i++) {
+      MixedState* m = ms[i];
+      const bool pr = m->preal && order >= 1;
+      int mt, nt;
+      shape(m, mt, nt);
+      EpiProp ep{0, 0, 0, m->N, 2 * m->n, m->S, nullptr, next_op(m->F[1], m->prec_v1), 0};
+      multi_add(job, i, from_f2[i] ? m->m_pw2 : m->m_pw[0], ep, pr ? m->N : 2 * m->N, mt, nt,
+                m->bn_prop, m->nw, 0, 1, t);
+    }
+    job.tile0[n] = t;
+    job.np = n;
+    if ((e = multi_run(ms[0]->prec_p, job, ms[0]->err, st)) != cudaSuccess) return e;
+  }
+  int cur = 1;
+  for (int k = 1; k <= order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
+    const int prec = k == 1 ? ms[0]->prec_v1 : ms[0]->prec_vk;
+    const int nprec = k < order ? ms[0]->prec_vk : ms[0]->prec_p;
+    tc::MultiJob<EpiProp, kMultiMax> job{};
+    int t = 0;
+    for (int i = 0; i < n; i++) {
+      MixedState* m = ms[i];
+      int mt, nt;
+      shape(m, mt, nt);
+      EpiProp ep{1, k, k == order ? 1 : 0, m->N, 2 * m->n, m->S, nullptr,
+                 next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0};
+      multi_add(job, i, m->m_v[cur], ep, 2 * m->N, mt, nt, m->bn_prop, m->nw, 1, 1, t);
+    }
+    job.tile0[n] = t;
+    job.np = n;
+    if ((e = multi_run(prec, job, ms[0]->err, st)) != cudaSuccess) return e;
+    cur ^= 1;
+  }
+  {  // W = P S
+    tc::MultiJob<EpiProp, kMultiMax> job{};
+    int t = 0;
+    for (int i = 0; i < n; i++) {
+      MixedState* m = ms[i];
+      const bool pr = m->preal && order >= 1;
+      int mt, nt;
+      shape(m, mt, nt);
+      EpiProp ep{2, 0, 0, m->N, 2 * m->n, m->S, W[i], Op{}, 0};
+      multi_add(job, i, m->m_pw[cur], ep, pr ? m->N : 2 * m->N, mt, nt, m->bn_prop, m->nw, 0, 1,
+                t);
+    }
+    job.tile0[n] = t;
+    job.np = n;
+    if ((e = multi_run(ms[0]->prec_p, job, ms[0]->err, st)) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // The packed forms from W itself (after the orthogonalisation, or before a captured

@@ -281,10 +281,12 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
 //   MINB = CTAs per SM the launch is compiled for (2 caps registers at 170 per thread so a
 //   lean ring's CTAs pair up on an SM).
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1, int SLAB = 128>
-__global__ void __launch_bounds__(192, MINB)
-tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step, int a_batched,
-               int b_batched, int k_split, int m_fast, int z0, Epi epi, int* err) {
+// The body of the per-tile kernels: one 128 x bn output tile (bn <= BN, a multiple of 16;
+// the B tensor map's box holds bn rows) of batch `batch`, K range [kbase, kbase + klen),
+// operand batches za / zb.  The shared-memory ring is laid out for BN.
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int SLAB>
+AFQ_D void gemm_tile(const Maps& maps, int mt, int nt, int m0, int n0, int batch, int za,
+                     int zb, int kbase, int klen, int bn, const Epi& epi, int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -299,14 +301,8 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // m_fast: M tiles along grid x, so the CTAs that share a B tile run together
-  const int mt = m_fast ? blockIdx.x : blockIdx.y, nt = m_fast ? blockIdx.y : blockIdx.x;
-  const int m0 = mt * m_step, n0 = nt * n_step;
-  const int batch = z0 + blockIdx.z;
-  // split-K: z selects the K range [z*k_split, (z+1)*k_split) of an unbatched product
-  const int kbase = k_split ? batch * k_split : 0;
-  const int klen = k_split ? min(k_split, K - kbase) : K;
   const int nk = (klen + C::BK - 1) / C::BK;
+  const uint32_t stage_bytes = C::PARTS * (C::A_BYTES + (uint32_t)bn * SLAB);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -328,7 +324,6 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
 
   if (warp == 4 && lane == 0) {
     // ---- TMA producer
-    const int za = (a_batched && !k_split) ? batch : 0, zb = (b_batched && !k_split) ? batch : 0;
     int issued = 0;
     for (int kb = 0; kb < nk; kb++) {
       const int kx = kbase + kb * C::BK;
@@ -338,7 +333,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
         atomicOr(err, ERR_TIMEOUT_PRODUCER);
         break;
       }
-      mbar_expect_tx(&full[s], C::STAGE_BYTES);
+      mbar_expect_tx(&full[s], stage_bytes);
       tma_load_3d(stA(s, 0), &maps.a, &full[s], kx, m0, za);
       tma_load_3d(stB(s, 0), &maps.b, &full[s], kx, n0, zb);
       if (SPLIT) {
@@ -352,7 +347,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
       mbar_wait_drain(&full[q % STAGES], (q / STAGES) & 1);
   } else if (warp == 5 && lane == 0) {
     // ---- MMA issuer
-    constexpr uint32_t ID = idesc(128, BN, FMT);
+    const uint32_t ID = idesc(128, bn, FMT);
     bool ok = true;
     for (int kb = 0; kb < nk; kb++) {
       const int s = kb % STAGES;
@@ -402,7 +397,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
         const int P = epi.pair_stride();
         float u[32];
 #pragma unroll 1
-        for (int c0 = 0; c0 < P && c0 + P < BN + 1; c0 += 32) {
+        for (int c0 = 0; c0 < P && c0 + P < bn + 1; c0 += 32) {
           tmem_ld32(trow + c0, v);
           tmem_ld32(trow + c0 + P, u);
           epi.pair(batch, row, m0 + row, c0, v, u);
@@ -411,7 +406,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
         // the operand ring is idle once `done` has fired: reuse it for the fp32 tile
         float* tile = reinterpret_cast<float*>(smem);
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 32) {
+        for (int c0 = 0; c0 < bn; c0 += 32) {
           tmem_ld32(trow + c0, v);
 #pragma unroll
           for (int i = 0; i < 32; i++) tile[row * (BN + 1) + c0 + i] = v[i];
@@ -420,7 +415,7 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
         epi.tile(batch, mt, nt, tile, BN + 1, threadIdx.x);
       } else {
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 32) {
+        for (int c0 = 0; c0 < bn; c0 += 32) {
           tmem_ld32(trow + c0, v);
           epi(batch, row, m0 + row, n0 + c0, v);
         }
@@ -430,6 +425,53 @@ tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tmem, C::TMEM_COLS);
+}
+
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1, int SLAB = 128>
+__global__ void __launch_bounds__(192, MINB)
+tc_gemm_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step, int a_batched,
+               int b_batched, int k_split, int m_fast, int z0, Epi epi, int* err) {
+  // m_fast: M tiles along grid x, so the CTAs that share a B tile run together
+  const int mt = m_fast ? blockIdx.x : blockIdx.y, nt = m_fast ? blockIdx.y : blockIdx.x;
+  const int batch = z0 + blockIdx.z;
+  // split-K: z selects the K range [z*k_split, (z+1)*k_split) of an unbatched product
+  const int kbase = k_split ? batch * k_split : 0;
+  const int klen = k_split ? min(k_split, K - kbase) : K;
+  const int za = (a_batched && !k_split) ? batch : 0, zb = (b_batched && !k_split) ? batch : 0;
+  gemm_tile<BN, STAGES, FMT, SPLIT, Epi, SLAB>(maps, mt, nt, mt * m_step, nt * n_step, batch, za,
+                                               zb, kbase, klen, BN, epi, err);
+}
+
+// Several independent batched products (one per problem: a system of a heterogeneous
+// batch) in one launch over a work list of (problem, batch, M tile, N tile): problem p
+// owns the CTAs [tile0[p], tile0[p + 1]) of the 1-D grid, batch-major then M tiles then N
+// tiles.  Each problem has its own tensor maps, K, row / column steps, tile width
+// bn[p] <= BN and epilogue functor; the template (ring depth, precision, epilogue type) is
+// shared.  No split-K.
+template <class Epi, int NP>
+struct MultiJob {
+  Maps maps[NP];
+  Epi epi[NP];
+  int K[NP], m_step[NP], n_step[NP], bn[NP], m_tiles[NP], n_tiles[NP];
+  int a_batched[NP], b_batched[NP];
+  int tile0[NP + 1];
+  int np;
+};
+
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int NP, int SLAB = 128>
+__global__ void __launch_bounds__(192, 1)
+tc_gemm_multi_kernel(const __grid_constant__ MultiJob<Epi, NP> job, int* err) {
+  const int t = blockIdx.x;
+  int p = 0;
+  while (p + 1 < job.np && t >= job.tile0[p + 1]) p++;
+  const int local = t - job.tile0[p];
+  const int per = job.m_tiles[p] * job.n_tiles[p];
+  const int batch = local / per, r = local - batch * per;
+  const int nt = r % job.n_tiles[p], mt = r / job.n_tiles[p];
+  gemm_tile<BN, STAGES, FMT, SPLIT, Epi, SLAB>(
+      job.maps[p], mt, nt, mt * job.m_step[p], nt * job.n_step[p], batch,
+      job.a_batched[p] ? batch : 0, job.b_batched[p] ? batch : 0, 0, job.K[p], job.bn[p],
+      job.epi[p], err);
 }
 
 // ------------------------------------------------------------------ persistent form
@@ -762,6 +804,33 @@ cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* er
   dim3 grid(g.m_fast ? g.m_tiles : ntiles, g.m_fast ? ntiles : g.m_tiles, g.batch);
   kern<<<grid, 192, C::SMEM, st>>>(maps, g.K, g.m_step, ns, g.a_batched, g.b_batched, g.k_split,
                                     g.m_fast ? 1 : 0, g.z0, epi, err);
+  return cudaGetLastError();
+}
+
+// One launch over the work list of job.np problems (job.tile0 filled by the caller: the
+// running sum of batch x m_tiles x n_tiles).  Tile widths must be multiples of 32 within BN.
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int NP, int SLAB = 128>
+cudaError_t launch_multi(const MultiJob<Epi, NP>& job, int* err, cudaStream_t st) {
+  using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
+  static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
+                "tile epilogue needs the operand ring to hold the fp32 tile");
+  static_assert(C::SMEM <= 227 * 1024 && C::TMEM_COLS <= 512, "shared memory or TMEM");
+  if (job.np < 1 || job.np > NP || job.tile0[0] != 0) return cudaErrorInvalidValue;
+  for (int p = 0; p < job.np; p++) {
+    if (job.bn[p] < 32 || job.bn[p] > BN || job.bn[p] % 32 || job.m_tiles[p] < 1 ||
+        job.n_tiles[p] < 1 || job.K[p] < 1 || job.tile0[p + 1] < job.tile0[p] ||
+        (job.tile0[p + 1] - job.tile0[p]) % (job.m_tiles[p] * job.n_tiles[p]))
+      return cudaErrorInvalidValue;
+  }
+  const int total = job.tile0[job.np];
+  if (total <= 0) return cudaSuccess;
+  auto kern = tc_gemm_multi_kernel<BN, STAGES, FMT, SPLIT, Epi, NP, SLAB>;
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(C::SMEM, [kern](size_t b) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  });
+  if (e != cudaSuccess) return e;
+  kern<<<total, 192, C::SMEM, st>>>(job, err);
   return cudaGetLastError();
 }
 

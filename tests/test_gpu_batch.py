@@ -62,6 +62,64 @@ def test_batch_matches_systems_alone(mixed, nsub):
         e.close()
 
 
+@pytest.mark.parametrize("nsub", [1, 5])
+def test_fused_batch_matches_systems_alone(nsub):
+    """Fused batch: the vHS product and each of the eight propagation products run as one
+    launch over the three systems' (walker, M tile, N tile) work list.  Every tile runs the
+    same MMA sequence and the same epilogue arithmetic as in a system's own launches (the
+    system with 2n = 128 takes the tile epilogue and the pack kernels instead of the paired
+    epilogue, which writes the same values), so the walkers, weights and energies equal
+    the systems advanced alone to 1e-13 relative, through a re-orthogonalisation."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_MIXED
+    sys_ = systems()
+    alone = [AfqmcSys(s, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False) for c, s in sys_]
+    grouped = [AfqmcSys(s, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False) for c, s in sys_]
+    seeds = [c.seed for c, _ in sys_]
+    batch = AfqmcBatch(grouped)
+    batch.set_fused(True)
+    for e in alone + grouped:
+        e.calculate_mixed_density_matrix()
+    for st in range(10):
+        for e, sd in zip(alone, seeds):
+            e.substep(sd, st, 5, graph=True)
+        if nsub == 1:
+            batch.substep(seeds, st, 5)
+        elif st % nsub == 0:
+            batch.substeps(seeds, st, nsub, 5)
+    batch.synchronize()
+    for a, g in zip(alone, grouped):
+        Wa, Da = a.get_walkers()
+        Wg, Dg = g.get_walkers()
+        assert rel(Wg, Wa) < 1e-13 and rel(Dg, Da) < 1e-13
+        for e in (a, g):
+            e.calculate_mixed_density_matrix()
+        ea, eg = a.calculate_energy("chol"), g.calculate_energy("chol")
+        assert abs(eg - ea) <= 1e-13 * abs(ea)
+    # back to the per-system branches: the next substeps still agree
+    batch.set_fused(False)
+    for e, sd in zip(alone, seeds):
+        e.substep(sd, 10, 5, graph=True)
+    batch.substep(seeds, 10, 5)
+    batch.synchronize()
+    for a, g in zip(alone, grouped):
+        assert rel(g.get_walkers()[0], a.get_walkers()[0]) < 1e-13
+    batch.close()
+    for e in alone + grouped:
+        e.close()
+
+
+def test_fused_batch_needs_mixed_systems():
+    from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AfqmcError, AFQ_PREC_FP64, AFQ_PREC_MIXED
+    (c0, s0), (c1, s1) = systems()[:2]
+    hs = [AfqmcSys(s0, c0.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False),
+          AfqmcSys(s1, c1.nwalk, precision=AFQ_PREC_FP64, use_vakbl=False)]
+    batch = AfqmcBatch(hs)
+    with pytest.raises(AfqmcError):
+        batch.set_fused(True)
+    batch.close()
+    for e in hs:
+        e.close()
+
 
 def test_c5_shapes_mixed_energy_matches_fp64():
     """Mixed against FP64 energies on identical walkers for the C5 shapes (n = 12, 40 and
