@@ -331,7 +331,7 @@ afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step
  * (P W, the Taylor terms, P S) run as ONE launch over the tiles of every system, a work
  * list of (system, walker, M tile, N tile) in one grid, instead of one launch per system;
  * the other stages stay per system on the systems' streams.  Needs every handle in the
- * mixed form with the same precisions, Taylor order and vHS form, at most 4 systems
+ * mixed form with the same precisions and Taylor order, at most 4 systems
  * (else AFQ_ERR_UNSUPPORTED; the batch stays unfused).  The chain then writes no packed
  * walker forms (the overlap stage packs its own operand), so a system with 2n a multiple
  * of 32 runs its chain with the tile epilogue instead of the paired one: its walkers

@@ -448,7 +448,7 @@ class AfqmcBatch:
     def set_fused(self, fused: bool = True):
         """Fused batch (afq_batch_set_fused): the vHS product and each propagation product
         as one launch over every system's tiles.  Raises AfqmcError when a system is not
-        in the mixed form or the systems' precisions, Taylor orders or vHS forms differ."""
+        in the mixed form or the systems' precisions or Taylor orders differ."""
         st = self.lib.afq_batch_set_fused(self.b, 1 if fused else 0)
         if st != 0:
             raise AfqmcError(st, "afq_batch_set_fused failed")

@@ -68,7 +68,7 @@ int mixed_prop_group(const MixedState* m, float* ms);
 void mixed_tuning(const MixedState* m, int* choice, float* ms);
 // Heterogeneous batches: the vHS product and the propagation chain of n systems (n <= 4),
 // each product one launch over every system's tiles.  mixed_multi_compatible: the systems
-// share the precisions, Taylor order and vHS form.  mixed_vhs_pack / mixed_prop_pack
+// share the precisions and the Taylor order.  mixed_vhs_pack / mixed_prop_pack
 // (on each system's stream, before the joint launches) pack X and, unless current, the
 // P W operand; mixed_prop_multi leaves no packed walker forms current.
 bool mixed_multi_compatible(MixedState* const* ms, int n);

@@ -1720,9 +1720,10 @@ void mixed_invalidate(MixedState* m) {
 // ------------------------------------------------------------ heterogeneous batches
 // The vHS product and the eight products of the propagation chain of several systems,
 // each product one launch over the work list of every system's (walker, M tile, N tile)
-// tiles (tc::launch_multi, per-tile CTAs).  The systems share the precisions, the Taylor
-// order and the vHS form; the chain runs the tile epilogue (EpiProp) for every system, so
-// no system's packed walker forms survive it (the overlap stage packs its own operand).
+// tiles (tc::launch_multi, per-tile CTAs).  The systems share the precisions and the
+// Taylor order (the vHS epilogue form is picked per system); the chain runs the tile
+// epilogue (EpiProp) for every system, so no system's packed walker forms survive it (the
+// overlap stage packs its own operand).
 namespace {
 constexpr int kMultiMax = 4;
 
@@ -1759,8 +1760,7 @@ bool mixed_multi_compatible(MixedState* const* ms, int n) {
     const MixedState* m = ms[i];
     const MixedState* a = ms[0];
     if (!m || m->prec_vhs != a->prec_vhs || m->prec_p != a->prec_p || m->prec_v1 != a->prec_v1 ||
-        m->prec_vk != a->prec_vk || m->in.order != a->in.order || m->vsym != a->vsym ||
-        m->bn_prop < 32 || m->bn_prop > 256 || 4 * m->n > m->bn_prop)
+        m->prec_vk != a->prec_vk || m->in.order != a->in.order || m->bn_prop < 32 || m->bn_prop > 256 || 4 * m->n > m->bn_prop)
       return false;
     for (int p : {m->prec_vhs, m->prec_p, m->prec_v1, m->prec_vk})
       if (p != PREC_SPLIT && p != PREC_BF16) return false;
@@ -1768,26 +1768,32 @@ bool mixed_multi_compatible(MixedState* const* ms, int n) {
   return true;
 }
 
+// vHS epilogue of either form (block pairs of symmetric L_n, or the full N^2 columns),
+// picked per system of a joint launch
+struct EpiVhsAny {
+  static constexpr bool kTile = false, kPair = false;
+  int sym;
+  EpiVhsSym s;
+  EpiVhs f;
+  AFQ_D void operator()(int b, int r, int m, int n0, const float* v) const {
+    if (sym)
+      s(b, r, m, n0, v);
+    else
+      f(b, r, m, n0, v);
+  }
+};
+
 cudaError_t mixed_vhs_multi(MixedState* const* ms, int n, cudaStream_t st) {
   if (!mixed_multi_compatible(ms, n)) return cudaErrorInvalidValue;
   int t = 0;
-  if (ms[0]->vsym) {
-    tc::MultiJob<EpiVhsSym, kMultiMax> job{};
-    for (int i = 0; i < n; i++) {
-      MixedState* m = ms[i];
-      multi_add(job, i, m->m_vhs, EpiVhsSym{m->Vf, m->nw, m->N, m->pairs}, m->Kv,
-                (2 * m->nw + 127) / 128, m->npairs, 256, 1, 0, 0, t);
-    }
-    job.tile0[n] = t;
-    job.np = n;
-    return multi_run(ms[0]->prec_vhs, job, ms[0]->err, st);
-  }
-  tc::MultiJob<EpiVhs, kMultiMax> job{};
+  tc::MultiJob<EpiVhsAny, kMultiMax> job{};
   for (int i = 0; i < n; i++) {
     MixedState* m = ms[i];
     const long long NN = (long long)m->N * m->N;
-    multi_add(job, i, m->m_vhs, EpiVhs{m->Vf, m->nw, NN}, m->Kv, (2 * m->nw + 127) / 128,
-              (int)((NN + 255) / 256), 256, 1, 0, 0, t);
+    EpiVhsAny ep{m->vsym ? 1 : 0, EpiVhsSym{m->Vf, m->nw, m->N, m->pairs},
+                 EpiVhs{m->Vf, m->nw, NN}};
+    const int ntiles = m->vsym ? m->npairs : (int)((NN + 255) / 256);
+    multi_add(job, i, m->m_vhs, ep, m->Kv, (2 * m->nw + 127) / 128, ntiles, 256, 1, 0, 0, t);
   }
   job.tile0[n] = t;
   job.np = n;
