@@ -536,9 +536,9 @@ def run_c5(args, torch):
 
     def run(mode):
         engs = fresh()
-        batch = AfqmcBatch(engs) if mode in ("batch", "fused") else None
-        if mode == "fused":
-            batch.set_fused(True)
+        batch = AfqmcBatch(engs) if mode.startswith(("batch", "fused")) else None
+        if mode.startswith("fused"):
+            batch.set_fused({"fused": 3, "fused_vhs": 1, "fused_chain": 2}[mode])
 
         def step(st):
             if batch is not None:   # one launch per measurement interval
@@ -577,7 +577,8 @@ def run_c5(args, torch):
             e.close()
         return sum(nws) * args.steps / wall, wall, cv, tun
 
-    res = {m: run(m) for m in ("batch", "fused", "independent", "serial")}
+    res = {m: run(m) for m in ("batch", "fused", "fused_vhs", "fused_chain", "independent",
+                               "serial")}
     v, wall, cv, tun = res["batch"]
     line = {
         "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
@@ -589,7 +590,8 @@ def run_c5(args, torch):
                                "10% sparse Cholesky, mixed form, control variate per system",
                    "energy_every": args.energy_every, "timing": "wall clock, device-synchronised",
                    "kernel_tuning": tun},
-        "fused_batch": {"value": res["fused"][0], "unit": METRIC},
+        "fused_batch": {"value": res["fused"][0], "unit": METRIC,
+                        "vhs_only": res["fused_vhs"][0], "chain_only": res["fused_chain"][0]},
         "independent_streams": {"value": res["independent"][0], "unit": METRIC},
         "serial": {"value": res["serial"][0], "unit": METRIC},
         "control_variate": cv,

@@ -327,17 +327,17 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
  * substeps between two energy measurements).  Equal to nsub afq_batch_substep calls. */
 afq_status afq_batch_substeps(afq_batch* b, const uint64_t* seeds, uint64_t step_tot, int nsub,
                               int northo);
-/* Fused batch (fused = 1): the vHS product and each of the propagation chain's products
- * (P W, the Taylor terms, P S) run as ONE launch over the tiles of every system, a work
- * list of (system, walker, M tile, N tile) in one grid, instead of one launch per system;
- * the other stages stay per system on the systems' streams.  Needs every handle in the
- * mixed form with the same precisions and Taylor order, at most 4 systems
- * (else AFQ_ERR_UNSUPPORTED; the batch stays unfused).  The chain then writes no packed
- * walker forms (the overlap stage packs its own operand), so a system with 2n a multiple
- * of 32 runs its chain with the tile epilogue instead of the paired one: its walkers
- * agree with the unfused batch to the mixed form's rounding, not bit for bit.  Tensor-core
- * timeouts of the joint launches are reported on the first handle.  fused = 0 restores
- * the per-system graph branches. */
+/* Fused batch: the vHS product (fused bit 1) and / or each of the propagation chain's
+ * products (P W, the Taylor terms, P S; bit 2) run as ONE launch over the tiles of every
+ * system, a work list of (system, walker, M tile, N tile) in one grid, instead of one
+ * launch per system; the other stages stay per system on the systems' streams.  Needs
+ * every handle in the mixed form with the same precisions and Taylor order, at most 4
+ * systems (else AFQ_ERR_UNSUPPORTED; the batch stays as it was).  Every tile runs the
+ * MMAs and epilogue arithmetic of the system's own launches, so results equal the
+ * unfused batch; the joint chain writes the walkers through the shared-memory tile
+ * epilogue and leaves no packed walker forms (the overlap stage packs its operand).
+ * Tensor-core timeouts of the joint launches are reported on the first handle.
+ * fused = 0 restores the per-system graph branches; fused = 3 joins both. */
 afq_status afq_batch_set_fused(afq_batch* b, int fused);
 /* Waits for the batch's work and reports any handle's tensor-core timeout flags. */
 afq_status afq_batch_synchronize(afq_batch* b);

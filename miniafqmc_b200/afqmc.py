@@ -445,11 +445,14 @@ class AfqmcBatch:
             raise AfqmcError(st, "afq_batch_create failed")
         self.b = h
 
-    def set_fused(self, fused: bool = True):
-        """Fused batch (afq_batch_set_fused): the vHS product and each propagation product
-        as one launch over every system's tiles.  Raises AfqmcError when a system is not
-        in the mixed form or the systems' precisions or Taylor orders differ."""
-        st = self.lib.afq_batch_set_fused(self.b, 1 if fused else 0)
+    def set_fused(self, fused=True):
+        """Fused batch (afq_batch_set_fused): True (3) runs the vHS product and each
+        propagation product as one launch over every system's tiles, 1 the vHS product
+        only, 2 the propagation chain only, False (0) neither.  Raises AfqmcError when a
+        system is not in the mixed form or the systems' precisions or Taylor orders
+        differ."""
+        mode = 3 if fused is True else 0 if fused is False else int(fused)
+        st = self.lib.afq_batch_set_fused(self.b, mode)
         if st != 0:
             raise AfqmcError(st, "afq_batch_set_fused failed")
 

@@ -1438,9 +1438,10 @@ struct afq_batch {
   // recorded by the graph at the end of each system's branch (external event nodes): a
   // handle's later work waits for its own system only, not for the whole batch
   std::vector<cudaEvent_t> sysdone;
-  // fused: the vHS product and the propagation chain of every system run as one launch
-  // each over all systems' tiles (mixed-form systems of matching precisions)
-  bool fused = false;
+  // fused: the vHS product (bit 1) and / or the propagation chain (bit 2) of every system
+  // run as one launch each over all systems' tiles (mixed-form systems of matching
+  // precisions); 0 = per-system graph branches
+  int fused = 0;
   // one graph per (substeps per launch, which of them re-orthogonalise)
   struct Graph {
     cudaGraphExec_t exec = nullptr;
@@ -1493,28 +1494,41 @@ cudaError_t batch_substep_fused(afq_batch* b, bool ortho) {
     return r;
   };
   cudaError_t e;
+  const bool jv = b->fused & 1, jp = b->fused & 2;
   for (afq_handle* h : b->hs) {
     if ((e = st_dm(h, 1, 0)) != cudaSuccess || (e = st_vbias(h)) != cudaSuccess ||
         (e = st_sigma(h, 0)) != cudaSuccess)
       return e;
-    if ((e = staged(h, AFQ_STAGE_VHS, 1, [&] { return afq::mixed_vhs_pack(h->mixed, h->X, h->st); })) !=
-        cudaSuccess)
+    if (!jv) {
+      if ((e = st_vhs(h)) != cudaSuccess) return e;
+    } else if ((e = staged(h, AFQ_STAGE_VHS, 1, [&] {
+                  return afq::mixed_vhs_pack(h->mixed, h->X, h->st);
+                })) != cudaSuccess) {
       return e;
+    }
   }
-  if ((e = join()) != cudaSuccess) return e;
-  count_launches(b->hs[0], AFQ_STAGE_VHS, 1);
-  if ((e = afq::mixed_vhs_multi(ms.data(), n, b->st)) != cudaSuccess) return e;
-  if ((e = fork()) != cudaSuccess) return e;
+  if (jv) {
+    if ((e = join()) != cudaSuccess) return e;
+    count_launches(b->hs[0], AFQ_STAGE_VHS, 1);
+    if ((e = afq::mixed_vhs_multi(ms.data(), n, b->st)) != cudaSuccess) return e;
+    if ((e = fork()) != cudaSuccess) return e;
+  }
   for (afq_handle* h : b->hs) {
+    if (!jp) {
+      if ((e = st_propagate(h)) != cudaSuccess) return e;
+      continue;
+    }
     h->dm_cache = false;
     if ((e = staged(h, AFQ_STAGE_PROPAGATE, afq::mixed_prop_pack_launches(h->mixed),
                     [&] { return afq::mixed_prop_pack(h->mixed, h->W, h->st); })) != cudaSuccess)
       return e;
   }
-  if ((e = join()) != cudaSuccess) return e;
-  count_launches(b->hs[0], AFQ_STAGE_PROPAGATE, b->hs[0]->d.taylor_order + 2);
-  if ((e = afq::mixed_prop_multi(ms.data(), W.data(), n, b->st)) != cudaSuccess) return e;
-  if ((e = fork()) != cudaSuccess) return e;
+  if (jp) {
+    if ((e = join()) != cudaSuccess) return e;
+    count_launches(b->hs[0], AFQ_STAGE_PROPAGATE, b->hs[0]->d.taylor_order + 2);
+    if ((e = afq::mixed_prop_multi(ms.data(), W.data(), n, b->st)) != cudaSuccess) return e;
+    if ((e = fork()) != cudaSuccess) return e;
+  }
   for (afq_handle* h : b->hs) {
     if ((e = st_dm(h, 0, 1)) != cudaSuccess || (e = st_weights(h, 1)) != cudaSuccess) return e;
     if (ortho && ((e = st_ortho(h)) != cudaSuccess || (e = st_dm(h, 0, 0)) != cudaSuccess))
@@ -1666,15 +1680,15 @@ afq_status afq_batch_substep(afq_batch* b, const uint64_t* seeds, uint64_t step_
 }
 
 afq_status afq_batch_set_fused(afq_batch* b, int fused) {
-  if (!b || (fused != 0 && fused != 1)) return AFQ_ERR_ARG;
+  if (!b || fused < 0 || fused > 3) return AFQ_ERR_ARG;
   if (fused && !batch_fusable(b)) return AFQ_ERR_UNSUPPORTED;
   cudaSetDevice(b->device);
-  if (b->fused != (fused != 0)) {   // graphs of the other mode
+  if (b->fused != fused) {   // graphs of another mode
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return AFQ_ERR_CUDA;
     for (auto& kv : b->g)
       if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     b->g.clear();
-    b->fused = fused != 0;
+    b->fused = fused;
   }
   return AFQ_OK;
 }

@@ -62,21 +62,22 @@ def test_batch_matches_systems_alone(mixed, nsub):
         e.close()
 
 
-@pytest.mark.parametrize("nsub", [1, 5])
-def test_fused_batch_matches_systems_alone(nsub):
+@pytest.mark.parametrize("mode,nsub", [(3, 1), (3, 5), (1, 5), (2, 5)])
+def test_fused_batch_matches_systems_alone(mode, nsub):
     """Fused batch: the vHS product and each of the eight propagation products run as one
     launch over the three systems' (walker, M tile, N tile) work list.  Every tile runs the
     same MMA sequence and the same epilogue arithmetic as in a system's own launches (the
     system with 2n = 128 takes the tile epilogue and the pack kernels instead of the paired
     epilogue, which writes the same values), so the walkers, weights and energies equal
-    the systems advanced alone to 1e-13 relative, through a re-orthogonalisation."""
+    the systems advanced alone to 1e-13 relative, through a re-orthogonalisation.  Modes:
+    3 both joint, 1 the vHS product only, 2 the chain only."""
     from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_MIXED
     sys_ = systems()
     alone = [AfqmcSys(s, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False) for c, s in sys_]
     grouped = [AfqmcSys(s, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False) for c, s in sys_]
     seeds = [c.seed for c, _ in sys_]
     batch = AfqmcBatch(grouped)
-    batch.set_fused(True)
+    batch.set_fused(mode)
     for e in alone + grouped:
         e.calculate_mixed_density_matrix()
     for st in range(10):
