@@ -966,6 +966,92 @@ struct EpiPropPair {
   }
 };
 
+// The propagation epilogue of EpiPropPair for any even 2n, through the persistent kernel's
+// staged interface: each thread owns one output row (orbital i of walker w) and takes
+// Re C (columns j) and Im C (columns n2 + j) 32 j at a time.  TMEM loads stay on 32-column
+// boundaries: when n2 is not a multiple of 32, the Im block [n2 + j0, n2 + j0 + 32) is
+// gathered from the aligned chunks that cover it through the thread's own shared-memory
+// row of 33 floats (written and read by that thread only).  Same arithmetic as
+// EpiPropPair, so the same values.
+struct EpiPropStaged {
+  static constexpr bool kTile = false, kPair = false, kStaged = true;
+  static constexpr int kScratchBytes = 128 * 33 * 4;
+  int mode, k, last, N, n2;
+  float2* S;
+  z_t* W;
+  Op F;
+  int real_next;
+  template <class LD>
+  AFQ_D void staged(int w, int mt, int, int row, LD& ld, float* scr, int) const {
+    const int i = mt * 128 + row;
+    float* my = scr + row * 33;
+    const long long wrow = (long long)w * N * n2 + (long long)i * n2;   // W[w][i][.]
+    const long long scol = (long long)w * N * n2 + i;                   // S[w][.][i]
+    const long long base = (long long)w * 2 * n2 * 2 * N;
+    const float inv = mode == 1 ? 1.0f / (float)k : 0.0f;
+#pragma unroll 1
+    for (int j0 = 0; j0 < n2; j0 += 32) {
+      float cr[32], ci[32];
+      ld(j0, cr);
+      const int need = min(32, n2 - j0);           // j in [j0, j0 + need)
+      const int c = n2 + j0, a0 = c & ~31, off = c - a0;
+      if (off == 0) {
+        ld(a0, ci);
+      } else {
+        float t[32];
+        ld(a0, t);
+#pragma unroll
+        for (int q = 0; q < 32; q++) my[q] = t[q];
+#pragma unroll
+        for (int jj = 0; jj < 32; jj++)
+          if (jj < 32 - off) ci[jj] = my[off + jj];
+        if (off + need > 32) {   // the block runs into the next aligned chunk
+          ld(a0 + 32, t);
+#pragma unroll
+          for (int q = 0; q < 32; q++) my[q] = t[q];
+#pragma unroll
+          for (int jj = 0; jj < 32; jj++)
+            if (jj >= 32 - off) ci[jj] = my[jj + off - 32];
+        }
+      }
+      if (i >= N) continue;
+      float2 sv[32];
+      if (mode == 1) {
+#pragma unroll
+        for (int jj = 0; jj < 32; jj++)
+          if (jj < need) sv[jj] = S[scol + (long long)(j0 + jj) * N];
+      }
+#pragma unroll
+      for (int jj = 0; jj < 32; jj++) {
+        if (jj >= need) continue;
+        const int j = j0 + jj;
+        float vr = cr[jj], vi = ci[jj];
+        if (mode == 0) {
+          S[scol + (long long)j * N] = make_float2(vr, vi);
+        } else if (mode == 1) {
+          const float tr = -vi * inv, ti = vr * inv;
+          float2 s = sv[jj];
+          s.x += tr;
+          s.y += ti;
+          S[scol + (long long)j * N] = s;
+          vr = last ? s.x : tr;
+          vi = last ? s.y : ti;
+        } else {
+          W[wrow + j] = zmk(vr, vi);
+          continue;
+        }
+        if (real_next) {
+          put1(F, base + (long long)j * 2 * N + i, vr);
+          put1(F, base + (long long)(n2 + j) * 2 * N + i, vi);
+          continue;
+        }
+        put2(F, base + (long long)j * 2 * N + 2 * i, vr, -vi);
+        put2(F, base + (long long)(n2 + j) * 2 * N + 2 * i, vi, vr);
+      }
+    }
+  }
+};
+
 // The last propagation product W = P S, written with the new walkers' packed forms
 // (pair layout as EpiPropPair): the layouts their next consumers read, as the pack kernels
 // form them from W, bit for bit (a float converted to double and back is unchanged).
@@ -1720,10 +1806,11 @@ void mixed_invalidate(MixedState* m) {
 // ------------------------------------------------------------ heterogeneous batches
 // The vHS product and the eight products of the propagation chain of several systems,
 // each product one launch over the work list of every system's (walker, M tile, N tile)
-// tiles (tc::launch_multi, per-tile CTAs).  The systems share the precisions and the
-// Taylor order (the vHS epilogue form is picked per system); the chain runs the tile
-// epilogue (EpiProp) for every system, so no system's packed walker forms survive it (the
-// overlap stage packs its own operand).
+// tiles: vHS on per-tile CTAs (tc::launch_multi), the chain on the persistent kernel
+// (tc::launch_persistent_multi, one epilogue warpgroup).  The systems share the precisions
+// and the Taylor order (the vHS epilogue form is picked per system); the chain runs
+// EpiPropStaged for every system and writes no packed walker forms (the overlap stage
+// packs its own operand).
 namespace {
 constexpr int kMultiMax = 4;
 
@@ -1750,6 +1837,34 @@ cudaError_t multi_run(int prec, const tc::MultiJob<Epi, kMultiMax>& job, int* er
                       cudaStream_t st) {
   if (prec == PREC_SPLIT) return tc::launch_multi<256, 2, 1, true, Epi, kMultiMax>(job, err, st);
   if (prec == PREC_BF16) return tc::launch_multi<256, 4, 1, false, Epi, kMultiMax>(job, err, st);
+  return cudaErrorInvalidValue;
+}
+
+// one propagation product of every system: persistent kernel, one epilogue warpgroup
+using PropJob = tc::PJob<EpiPropStaged, kMultiMax>;
+void prop_add(PropJob& job, int i, const tc::Maps& mp, const EpiPropStaged& ep, int K,
+              const MixedState* m, int a_batched, int& t) {
+  job.maps[i] = mp;
+  job.epi[i] = ep;
+  job.sched[i] = tc::TileSched{(m->N + 127) / 128, (4 * m->n + m->bn_prop - 1) / m->bn_prop,
+                               m->nw, 0, 0};
+  job.K[i] = K;
+  job.m_step[i] = 128;
+  job.n_step[i] = m->bn_prop;
+  job.a_batched[i] = a_batched;
+  job.b_batched[i] = 1;
+  job.k_split[i] = 0;
+  job.bn[i] = m->bn_prop;
+  job.tile0[i] = t;
+  t += job.sched[i].total();
+}
+cudaError_t prop_run(int prec, PropJob& job, int n, int t, int* err, cudaStream_t st) {
+  job.tile0[n] = t;
+  job.np = n;
+  if (prec == PREC_SPLIT)
+    return tc::launch_persistent_multi<256, 2, 1, true, EpiPropStaged, 1>(job, err, st);
+  if (prec == PREC_BF16)
+    return tc::launch_persistent_multi<256, 4, 1, false, EpiPropStaged, 1>(job, err, st);
   return cudaErrorInvalidValue;
 }
 }  // namespace
@@ -1818,61 +1933,43 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     from_f2[i] = ms[i]->packed;
     ms[i]->packed = false;
   }
-  auto shape = [&](const MixedState* m, int& mt, int& nt) {
-    mt = (m->N + 127) / 128;
-    nt = (4 * m->n + m->bn_prop - 1) / m->bn_prop;
-  };
   cudaError_t e;
   {  // S = P W
-    tc::MultiJob<EpiProp, kMultiMax> job{};
+    PropJob job{};
     int t = 0;
     for (int i = 0; i < n; i++) {
       MixedState* m = ms[i];
       const bool pr = m->preal && order >= 1;
-      int mt, nt;
-      shape(m, mt, nt);
-      EpiProp ep{0, 0, 0, m->N, 2 * m->n, m->S, nullptr, next_op(m->F[1], m->prec_v1), 0};
-      multi_add(job, i, from_f2[i] ? m->m_pw2 : m->m_pw[0], ep, pr ? m->N : 2 * m->N, mt, nt,
-                m->bn_prop, m->nw, 0, 1, t);
+      EpiPropStaged ep{0, 0, 0, m->N, 2 * m->n, m->S, nullptr, next_op(m->F[1], m->prec_v1), 0};
+      prop_add(job, i, from_f2[i] ? m->m_pw2 : m->m_pw[0], ep, pr ? m->N : 2 * m->N, m, 0, t);
     }
-    job.tile0[n] = t;
-    job.np = n;
-    if ((e = multi_run(ms[0]->prec_p, job, ms[0]->err, st)) != cudaSuccess) return e;
+    if ((e = prop_run(ms[0]->prec_p, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
   }
   int cur = 1;
   for (int k = 1; k <= order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
     const int prec = k == 1 ? ms[0]->prec_v1 : ms[0]->prec_vk;
     const int nprec = k < order ? ms[0]->prec_vk : ms[0]->prec_p;
-    tc::MultiJob<EpiProp, kMultiMax> job{};
+    PropJob job{};
     int t = 0;
     for (int i = 0; i < n; i++) {
       MixedState* m = ms[i];
-      int mt, nt;
-      shape(m, mt, nt);
-      EpiProp ep{1, k, k == order ? 1 : 0, m->N, 2 * m->n, m->S, nullptr,
-                 next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0};
-      multi_add(job, i, m->m_v[cur], ep, 2 * m->N, mt, nt, m->bn_prop, m->nw, 1, 1, t);
+      EpiPropStaged ep{1, k, k == order ? 1 : 0, m->N, 2 * m->n, m->S, nullptr,
+                       next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0};
+      prop_add(job, i, m->m_v[cur], ep, 2 * m->N, m, 1, t);
     }
-    job.tile0[n] = t;
-    job.np = n;
-    if ((e = multi_run(prec, job, ms[0]->err, st)) != cudaSuccess) return e;
+    if ((e = prop_run(prec, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
     cur ^= 1;
   }
   {  // W = P S
-    tc::MultiJob<EpiProp, kMultiMax> job{};
+    PropJob job{};
     int t = 0;
     for (int i = 0; i < n; i++) {
       MixedState* m = ms[i];
       const bool pr = m->preal && order >= 1;
-      int mt, nt;
-      shape(m, mt, nt);
-      EpiProp ep{2, 0, 0, m->N, 2 * m->n, m->S, W[i], Op{}, 0};
-      multi_add(job, i, m->m_pw[cur], ep, pr ? m->N : 2 * m->N, mt, nt, m->bn_prop, m->nw, 0, 1,
-                t);
+      EpiPropStaged ep{2, 0, 0, m->N, 2 * m->n, m->S, W[i], Op{}, 0};
+      prop_add(job, i, m->m_pw[cur], ep, pr ? m->N : 2 * m->N, m, 0, t);
     }
-    job.tile0[n] = t;
-    job.np = n;
-    if ((e = multi_run(ms[0]->prec_p, job, ms[0]->err, st)) != cudaSuccess) return e;
+    if ((e = prop_run(ms[0]->prec_p, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

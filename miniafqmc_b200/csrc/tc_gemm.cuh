@@ -513,11 +513,34 @@ struct PCfg {
   static constexpr bool kFits = SMEM <= 227 * 1024 && ACC_COLS <= 512;
 };
 
-template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG, int SLAB = 128>
+// Problems of a persistent launch: one (every single product), or several independent
+// batched products (the systems of a heterogeneous batch) walked as one tile list.
+// Problem p owns tiles [tile0[p], tile0[p + 1]), decoded by sched[p]; its tensor maps,
+// K, row / column steps, split-K extent, tile width bn[p] <= BN (a multiple of 32; BN for
+// promoting epilogues) and epilogue functor are its own.
+template <class Epi, int NP>
+struct PJob {
+  Maps maps[NP];
+  Epi epi[NP];
+  TileSched sched[NP];
+  int K[NP], m_step[NP], n_step[NP], a_batched[NP], b_batched[NP], k_split[NP], bn[NP];
+  int tile0[NP + 1];
+  int np;
+  // tile t -> problem p and its (batch z, M tile, N tile)
+  AFQ_D void locate(int t, int& p, int& z, int& mt, int& nt) const {
+    p = 0;
+    if constexpr (NP > 1) {
+      while (p + 1 < np && t >= tile0[p + 1]) p++;
+      t -= tile0[p];
+    }
+    sched[p].decode(t, z, mt, nt);
+  }
+};
+
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG, int SLAB = 128,
+          int NP = 1>
 __global__ void __launch_bounds__(128 * EPI_WG + 64, 1)
-tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, int n_step,
-                          int a_batched, int b_batched, int k_split, TileSched sched, Epi epi,
-                          int* err) {
+tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG, SLAB>;
   static_assert(!Epi::kTile, "tile epilogues reuse the operand ring: per-tile kernel only");
@@ -559,20 +582,28 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int total = sched.total();
+  const int total = job.tile0[job.np];
+  // K slabs of tile t's problem
+  auto kslabs = [&](int p, int z, int& kbase) {
+    const int ks = job.k_split[p];
+    kbase = ks ? z * ks : 0;
+    const int klen = ks ? min(ks, job.K[p] - kbase) : job.K[p];
+    return (klen + C::BK - 1) / C::BK;
+  };
 
   if (warp == WPROD && lane == 0) {
     // ---- TMA producer
     int g = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-      int z, mt, nt;
-      sched.decode(t, z, mt, nt);
-      const int kbase = k_split ? z * k_split : 0;
-      const int klen = k_split ? min(k_split, K - kbase) : K;
-      const int nk = (klen + C::BK - 1) / C::BK;
-      const int za = (a_batched && !k_split) ? z : 0, zb = (b_batched && !k_split) ? z : 0;
-      const int m0 = mt * m_step, n0 = nt * n_step;
+      int p, z, mt, nt, kbase;
+      job.locate(t, p, z, mt, nt);
+      const int nk = kslabs(p, z, kbase);
+      const int za = (job.a_batched[p] && !job.k_split[p]) ? z : 0;
+      const int zb = (job.b_batched[p] && !job.k_split[p]) ? z : 0;
+      const int m0 = mt * job.m_step[p], n0 = nt * job.n_step[p];
+      const Maps& maps = job.maps[p];
+      const uint32_t stage_bytes = C::PARTS * (C::A_BYTES + (uint32_t)job.bn[p] * SLAB);
       for (int kb = 0; kb < nk; kb++, g++) {
         const int s = g % STAGES;
         if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1)) {
@@ -581,7 +612,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
           break;
         }
         const int kx = kbase + kb * C::BK;
-        mbar_expect_tx(&full[s], C::STAGE_BYTES);
+        mbar_expect_tx(&full[s], stage_bytes);
         tma_load_3d(stA(s, 0), &maps.a, &full[s], kx, m0, za);
         tma_load_3d(stB(s, 0), &maps.b, &full[s], kx, n0, zb);
         if (SPLIT) {
@@ -595,15 +626,13 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       mbar_wait_drain(&full[q % STAGES], (q / STAGES) & 1);
   } else if (warp == WMMA && lane == 0) {
     // ---- MMA issuer: one accumulator buffer per tile, or per K chunk when promoting
-    constexpr uint32_t ID = idesc(128, BN, FMT);
     int g = 0, li = 0;
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-      int z, mt, nt;
-      sched.decode(t, z, mt, nt);
-      const int kbase = k_split ? z * k_split : 0;
-      const int klen = k_split ? min(k_split, K - kbase) : K;
-      const int nk = (klen + C::BK - 1) / C::BK;
+      int p, z, mt, nt, kbase;
+      job.locate(t, p, z, mt, nt);
+      const int nk = kslabs(p, z, kbase);
+      const uint32_t ID = idesc(128, job.bn[p], FMT);
       const int nch = PK ? (nk + PK - 1) / PK : 1;
       for (int ch = 0; ch < nch && ok; ch++, li++) {
         const int b = li & 1;
@@ -659,12 +688,11 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       int li = 0;
       bool ok = true;
       for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-        int z, mt, nt;
-        sched.decode(t, z, mt, nt);
-        const int kbase = k_split ? z * k_split : 0;
-        const int klen = k_split ? min(k_split, K - kbase) : K;
-        const int nk = (klen + C::BK - 1) / C::BK;
+        int p, z, mt, nt, kbase;
+        job.locate(t, p, z, mt, nt);
+        const int nk = kslabs(p, z, kbase);
         const int nch = (nk + PK - 1) / PK;
+        const Epi& epi = job.epi[p];
         for (int ch = 0; ch < nch; ch++, li++) {
           const int b = li & 1;
           if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
@@ -689,7 +717,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
         if constexpr (EpiRegs<Epi>::value) {
           epi.regs(z, mt, nt, row, acc, scr, wg);
         } else {
-          const int m0 = mt * m_step, n0 = nt * n_step;
+          const int m0 = mt * job.m_step[p], n0 = nt * job.n_step[p];
 #pragma unroll
           for (int j = 0; j < CPW / 32; j++) epi(z, row, m0 + row, n0 + wg * CPW + j * 32, acc + j * 32);
         }
@@ -701,8 +729,10 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
     const int row = wq * 32 + lane;
     int li = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, li++) {
-      int z, mt, nt;
-      sched.decode(t, z, mt, nt);
+      int p, z, mt, nt;
+      job.locate(t, p, z, mt, nt);
+      const Epi& epi = job.epi[p];
+      const int bn = job.bn[p];
       const int b = li & 1;
       if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
         if (lane == 0) atomicOr(err, ERR_TIMEOUT_EPILOGUE);
@@ -710,13 +740,13 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
       }
       tc_fence_after();
       const uint32_t trow = tmem + b * C::TMEM_COLS + ((uint32_t)(wq * 32) << 16);
-      const int m0 = mt * m_step, n0 = nt * n_step;
+      const int m0 = mt * job.m_step[p], n0 = nt * job.n_step[p];
       float v[32];
       if constexpr (Epi::kPair) {
         const int Pw = epi.pair_stride();
         float u[32];
 #pragma unroll 1
-        for (int c0 = wg * 32; c0 < Pw && c0 + Pw < BN + 1; c0 += 32 * EPI_WG) {
+        for (int c0 = wg * 32; c0 < Pw && c0 + Pw < bn + 1; c0 += 32 * EPI_WG) {
           tmem_ld32(trow + c0, v);
           tmem_ld32(trow + c0 + Pw, u);
           epi.pair(z, row, m0 + row, c0, v, u);
@@ -727,7 +757,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ Maps maps, int K, int m_step, 
         epi.staged(z, mt, nt, row, ld, scr, wg);
       } else {
 #pragma unroll 1
-        for (int c0 = wg * 32; c0 < BN; c0 += 32 * EPI_WG) {
+        for (int c0 = wg * 32; c0 < bn; c0 += 32 * EPI_WG) {
           tmem_ld32(trow + c0, v);
           epi(z, row, m0 + row, n0 + c0, v);
         }
@@ -857,12 +887,49 @@ cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& e
   });
   if (e != cudaSuccess) return e;
   const int ns = g.n_step > 0 ? g.n_step : BN;
-  TileSched sc{g.m_tiles, (g.N + ns - 1) / ns, g.batch, g.m_fast ? 1 : 0, g.z0};
-  const int total = sc.total();
+  PJob<Epi, 1> job;
+  job.maps[0] = maps;
+  job.epi[0] = epi;
+  job.sched[0] = TileSched{g.m_tiles, (g.N + ns - 1) / ns, g.batch, g.m_fast ? 1 : 0, g.z0};
+  job.K[0] = g.K;
+  job.m_step[0] = g.m_step;
+  job.n_step[0] = ns;
+  job.a_batched[0] = g.a_batched;
+  job.b_batched[0] = g.b_batched;
+  job.k_split[0] = g.k_split;
+  job.bn[0] = BN;
+  job.tile0[0] = 0;
+  job.tile0[1] = job.sched[0].total();
+  job.np = 1;
+  const int total = job.tile0[1];
   if (total <= 0) return cudaSuccess;
   const int grid = total < sm_count() ? total : sm_count();
-  kern<<<grid, P::THREADS, P::SMEM, st>>>(maps, g.K, g.m_step, ns, g.a_batched, g.b_batched,
-                                          g.k_split, sc, epi, err);
+  kern<<<grid, P::THREADS, P::SMEM, st>>>(job, err);
+  return cudaGetLastError();
+}
+
+// The persistent kernel over job.np <= NP problems (no promoting epilogue): tile0 and the
+// schedules filled by the caller; tile widths multiples of 32 within BN.
+template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG, int NP>
+cudaError_t launch_persistent_multi(const PJob<Epi, NP>& job, int* err, cudaStream_t st) {
+  using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG>;
+  static_assert(P::kFits, "persistent configuration exceeds shared memory or TMEM");
+  static_assert(EpiPromote<Epi>::value == 0, "promoting epilogues need the full tile width");
+  if (job.np < 1 || job.np > NP || job.tile0[0] != 0) return cudaErrorInvalidValue;
+  for (int p = 0; p < job.np; p++)
+    if (job.bn[p] < 32 || job.bn[p] > BN || job.bn[p] % 32 || job.K[p] < 1 ||
+        job.tile0[p + 1] - job.tile0[p] != job.sched[p].total())
+      return cudaErrorInvalidValue;
+  const int total = job.tile0[job.np];
+  if (total <= 0) return cudaSuccess;
+  auto kern = tc_gemm_persistent_kernel<BN, STAGES, FMT, SPLIT, Epi, EPI_WG, 128, NP>;
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(P::SMEM, [kern](size_t b) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  });
+  if (e != cudaSuccess) return e;
+  const int grid = total < sm_count() ? total : sm_count();
+  kern<<<grid, P::THREADS, P::SMEM, st>>>(job, err);
   return cudaGetLastError();
 }
 
