@@ -972,7 +972,8 @@ struct EpiPropPair {
 // boundaries: when n2 is not a multiple of 32, the Im block [n2 + j0, n2 + j0 + 32) is
 // gathered from the aligned chunks that cover it through the thread's own shared-memory
 // row of 33 floats (written and read by that thread only).  Same arithmetic as
-// EpiPropPair, so the same values.
+// EpiPropPair, so the same values.  With nwg epilogue warpgroups, warpgroup wg takes the
+// 32-column blocks wg, wg + nwg, ... of every row.
 struct EpiPropStaged {
   static constexpr bool kTile = false, kPair = false, kStaged = true;
   static constexpr int kScratchBytes = 128 * 33 * 4;
@@ -981,8 +982,9 @@ struct EpiPropStaged {
   z_t* W;
   Op F;
   int real_next;
+  int nwg;
   template <class LD>
-  AFQ_D void staged(int w, int mt, int, int row, LD& ld, float* scr, int) const {
+  AFQ_D void staged(int w, int mt, int, int row, LD& ld, float* scr, int wg) const {
     const int i = mt * 128 + row;
     float* my = scr + row * 33;
     const long long wrow = (long long)w * N * n2 + (long long)i * n2;   // W[w][i][.]
@@ -990,7 +992,7 @@ struct EpiPropStaged {
     const long long base = (long long)w * 2 * n2 * 2 * N;
     const float inv = mode == 1 ? 1.0f / (float)k : 0.0f;
 #pragma unroll 1
-    for (int j0 = 0; j0 < n2; j0 += 32) {
+    for (int j0 = 32 * wg; j0 < n2; j0 += 32 * nwg) {
       float cr[32], ci[32];
       ld(j0, cr);
       const int need = min(32, n2 - j0);           // j in [j0, j0 + need)
@@ -1807,7 +1809,7 @@ void mixed_invalidate(MixedState* m) {
 // The vHS product and the eight products of the propagation chain of several systems,
 // each product one launch over the work list of every system's (walker, M tile, N tile)
 // tiles: vHS on per-tile CTAs (tc::launch_multi), the chain on the persistent kernel
-// (tc::launch_persistent_multi, one epilogue warpgroup).  The systems share the precisions
+// (tc::launch_persistent_multi, two epilogue warpgroups).  The systems share the precisions
 // and the Taylor order (the vHS epilogue form is picked per system); the chain runs
 // EpiPropStaged for every system and writes no packed walker forms (the overlap stage
 // packs its own operand).
@@ -1840,7 +1842,8 @@ cudaError_t multi_run(int prec, const tc::MultiJob<Epi, kMultiMax>& job, int* er
   return cudaErrorInvalidValue;
 }
 
-// one propagation product of every system: persistent kernel, one epilogue warpgroup
+// one propagation product of every system: persistent kernel, two epilogue warpgroups
+constexpr int kPropWG = 2;
 using PropJob = tc::PJob<EpiPropStaged, kMultiMax>;
 void prop_add(PropJob& job, int i, const tc::Maps& mp, const EpiPropStaged& ep, int K,
               const MixedState* m, int a_batched, int& t) {
@@ -1862,9 +1865,9 @@ cudaError_t prop_run(int prec, PropJob& job, int n, int t, int* err, cudaStream_
   job.tile0[n] = t;
   job.np = n;
   if (prec == PREC_SPLIT)
-    return tc::launch_persistent_multi<256, 2, 1, true, EpiPropStaged, 1>(job, err, st);
+    return tc::launch_persistent_multi<256, 2, 1, true, EpiPropStaged, kPropWG>(job, err, st);
   if (prec == PREC_BF16)
-    return tc::launch_persistent_multi<256, 4, 1, false, EpiPropStaged, 1>(job, err, st);
+    return tc::launch_persistent_multi<256, 4, 1, false, EpiPropStaged, kPropWG>(job, err, st);
   return cudaErrorInvalidValue;
 }
 }  // namespace
@@ -1940,7 +1943,8 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     for (int i = 0; i < n; i++) {
       MixedState* m = ms[i];
       const bool pr = m->preal && order >= 1;
-      EpiPropStaged ep{0, 0, 0, m->N, 2 * m->n, m->S, nullptr, next_op(m->F[1], m->prec_v1), 0};
+      EpiPropStaged ep{0, 0, 0, m->N, 2 * m->n, m->S, nullptr, next_op(m->F[1], m->prec_v1), 0,
+                       kPropWG};
       prop_add(job, i, from_f2[i] ? m->m_pw2 : m->m_pw[0], ep, pr ? m->N : 2 * m->N, m, 0, t);
     }
     if ((e = prop_run(ms[0]->prec_p, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
@@ -1954,7 +1958,7 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     for (int i = 0; i < n; i++) {
       MixedState* m = ms[i];
       EpiPropStaged ep{1, k, k == order ? 1 : 0, m->N, 2 * m->n, m->S, nullptr,
-                       next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0};
+                       next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0, kPropWG};
       prop_add(job, i, m->m_v[cur], ep, 2 * m->N, m, 1, t);
     }
     if ((e = prop_run(prec, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
@@ -1966,7 +1970,7 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     for (int i = 0; i < n; i++) {
       MixedState* m = ms[i];
       const bool pr = m->preal && order >= 1;
-      EpiPropStaged ep{2, 0, 0, m->N, 2 * m->n, m->S, W[i], Op{}, 0};
+      EpiPropStaged ep{2, 0, 0, m->N, 2 * m->n, m->S, W[i], Op{}, 0, kPropWG};
       prop_add(job, i, m->m_pw[cur], ep, pr ? m->N : 2 * m->N, m, 0, t);
     }
     if ((e = prop_run(ms[0]->prec_p, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
