@@ -1905,8 +1905,11 @@ cudaError_t mixed_vhs_multi(MixedState* const* ms, int n, cudaStream_t st) {
   if (!mixed_multi_compatible(ms, n)) return cudaErrorInvalidValue;
   int t = 0;
   tc::MultiJob<EpiVhsAny, kMultiMax> job{};
+  int ord[kMultiMax];   // systems in decreasing K: long tiles first
+  for (int i = 0; i < n; i++) ord[i] = i;
+  std::sort(ord, ord + n, [&](int a, int b) { return ms[a]->Kv > ms[b]->Kv; });
   for (int i = 0; i < n; i++) {
-    MixedState* m = ms[i];
+    MixedState* m = ms[ord[i]];
     const long long NN = (long long)m->N * m->N;
     EpiVhsAny ep{m->vsym ? 1 : 0, EpiVhsSym{m->Vf, m->nw, m->N, m->pairs},
                  EpiVhs{m->Vf, m->nw, NN}};
@@ -1936,16 +1939,22 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     from_f2[i] = ms[i]->packed;
     ms[i]->packed = false;
   }
+  // systems in decreasing K (per-tile work): the persistent CTAs take the long tiles
+  // first and the short ones fill the tail
+  int ord[kMultiMax];
+  for (int i = 0; i < n; i++) ord[i] = i;
+  std::sort(ord, ord + n, [&](int a, int b) { return ms[a]->N > ms[b]->N; });
   cudaError_t e;
   {  // S = P W
     PropJob job{};
     int t = 0;
     for (int i = 0; i < n; i++) {
-      MixedState* m = ms[i];
+      MixedState* m = ms[ord[i]];
       const bool pr = m->preal && order >= 1;
       EpiPropStaged ep{0, 0, 0, m->N, 2 * m->n, m->S, nullptr, next_op(m->F[1], m->prec_v1), 0,
                        kPropWG};
-      prop_add(job, i, from_f2[i] ? m->m_pw2 : m->m_pw[0], ep, pr ? m->N : 2 * m->N, m, 0, t);
+      prop_add(job, i, from_f2[ord[i]] ? m->m_pw2 : m->m_pw[0], ep, pr ? m->N : 2 * m->N, m, 0,
+               t);
     }
     if ((e = prop_run(ms[0]->prec_p, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
   }
@@ -1956,7 +1965,7 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     PropJob job{};
     int t = 0;
     for (int i = 0; i < n; i++) {
-      MixedState* m = ms[i];
+      MixedState* m = ms[ord[i]];
       EpiPropStaged ep{1, k, k == order ? 1 : 0, m->N, 2 * m->n, m->S, nullptr,
                        next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0, kPropWG};
       prop_add(job, i, m->m_v[cur], ep, 2 * m->N, m, 1, t);
@@ -1968,9 +1977,9 @@ cudaError_t mixed_prop_multi(MixedState* const* ms, z_t* const* W, int n, cudaSt
     PropJob job{};
     int t = 0;
     for (int i = 0; i < n; i++) {
-      MixedState* m = ms[i];
+      MixedState* m = ms[ord[i]];
       const bool pr = m->preal && order >= 1;
-      EpiPropStaged ep{2, 0, 0, m->N, 2 * m->n, m->S, W[i], Op{}, 0, kPropWG};
+      EpiPropStaged ep{2, 0, 0, m->N, 2 * m->n, m->S, W[ord[i]], Op{}, 0, kPropWG};
       prop_add(job, i, m->m_pw[cur], ep, pr ? m->N : 2 * m->N, m, 0, t);
     }
     if ((e = prop_run(ms[0]->prec_p, job, n, t, ms[0]->err, st)) != cudaSuccess) return e;
