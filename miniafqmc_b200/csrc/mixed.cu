@@ -1373,7 +1373,20 @@ cudaError_t run_bn(int bn, int prec, const tc::Maps& mp, const tc::GemmShape& g,
   return cudaErrorInvalidValue;
 }
 
-// propagation product with the pair epilogue when 2n is a multiple of 32
+// the staged propagation epilogue on the persistent kernel, two epilogue warpgroups
+template <int BN>
+cudaError_t run_prop_staged(int prec, const tc::Maps& mp, const tc::GemmShape& g,
+                            const EpiPropStaged& ep, int* err, cudaStream_t st) {
+  if (prec == PREC_SPLIT)
+    return tc::launch_persistent<BN, 2, 1, true, EpiPropStaged, 2>(mp, g, ep, err, st);
+  if (prec == PREC_BF16)
+    return tc::launch_persistent<BN, 4, 1, false, EpiPropStaged, 2>(mp, g, ep, err, st);
+  return cudaErrorInvalidValue;
+}
+
+// propagation product with the pair epilogue when 2n is a multiple of 32; for any other
+// 2n the staged epilogue on the persistent kernel (kernel choice 0 or 1) or the
+// shared-memory tile epilogue on the per-tile kernel (choice 2): the same values
 cudaError_t run_prop(MixedState* m, int prec, const tc::Maps& mp, const tc::GemmShape& g, int mode,
                      int k, int last, z_t* W, const Op& F, cudaStream_t st, int fa_buf = -1) {
   const int n2 = 2 * m->n;
@@ -1384,6 +1397,16 @@ cudaError_t run_prop(MixedState* m, int prec, const tc::Maps& mp, const tc::Gemm
     }
     EpiPropPair ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
     return run_bn<true>(m->bn_prop, prec, mp, g, ep, m->err, st, m->tune[TS_PROP]);
+  }
+  if (m->tune[TS_PROP] != 2 && tc_persistent()) {
+    EpiPropStaged ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0, 2};
+    switch (m->bn_prop) {
+      case 64: return run_prop_staged<64>(prec, mp, g, ep, m->err, st);
+      case 128: return run_prop_staged<128>(prec, mp, g, ep, m->err, st);
+      case 192: return run_prop_staged<192>(prec, mp, g, ep, m->err, st);
+      case 256: return run_prop_staged<256>(prec, mp, g, ep, m->err, st);
+    }
+    return cudaErrorInvalidValue;
   }
   EpiProp ep{mode, k, last, m->N, n2, m->S, W, F, (last && m->preal) ? 1 : 0};
   return run_bn(m->bn_prop, prec, mp, g, ep, m->err, st, m->tune[TS_PROP]);

@@ -178,3 +178,23 @@ def test_grouped_propagation_chain_is_bit_identical(monkeypatch):
         e.close()
     assert np.array_equal(out["0"][0], out["32"][0])
     assert np.array_equal(out["0"][1], out["32"][1])
+
+
+def test_staged_propagation_epilogue_matches_tile_epilogue(monkeypatch):
+    """Walker width 2n = 24 (C5's smallest system, not a multiple of 32): the propagation
+    products with the staged epilogue on the persistent kernel (AFQ_TUNE=1; Im columns
+    gathered from 32-column-aligned TMEM loads) and with the shared-memory tile epilogue on
+    the per-tile kernel (AFQ_TUNE=2) do the same arithmetic: walkers to 1e-12 as for the
+    other forced-kernel pairs."""
+    import dataclasses
+    from miniafqmc_b200.synthetic import C5_SYSTEMS, make_system
+    cfg = dataclasses.replace(C5_SYSTEMS[0], nwalk=24)
+    s = make_system(cfg)
+    wk = walkers(s, cfg.nwalk, seed=7)
+    res = {}
+    for force in ("1", "2"):
+        monkeypatch.setenv("AFQ_TUNE", force)
+        res[force] = run_step(s, cfg.nwalk, wk)
+    a, b = res["1"], res["2"]
+    assert a["tuning"]["propagate"]["kernel"] == 1 and b["tuning"]["propagate"]["kernel"] == 2
+    assert rel(a["W"], b["W"]) < 1e-12
