@@ -2203,6 +2203,7 @@ namespace {
 struct TuneRec {
   int tune[TS_N];
   float ms[TS_N][2];
+  float group_ms[6];
   int splits;
   int prop_group;
 };
@@ -2236,6 +2237,7 @@ void tune_load(const char* path) {
     bool ok = true;
     for (int i = 0; i < TS_N && ok; i++)
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
+    for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.group_ms[i]) == 1;
     if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
     tune_cache()[key] = r;
     tune_file_keys().insert(key);
@@ -2248,6 +2250,7 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   if (!f) return;
   fprintf(f, "%s", key.c_str());
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
+  for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.group_ms[i]);
   fprintf(f, " %d %d\n", r.splits, r.prop_group);
   fclose(f);
 }
@@ -2285,6 +2288,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
         if (m->splits > m->part_cap) set_splits(m, m->splits0);
       }
       m->prop_group = r.prop_group;
+      for (int i = 0; i < 6; i++) m->prop_group_ms[i] = r.group_ms[i];
       tune_save(cache_path, key, r);   // a shape timed before the file was named
       return cudaSuccess;
     }
@@ -2462,6 +2466,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     }
     r.splits = m->splits;
     r.prop_group = m->prop_group;
+    for (int i = 0; i < 6; i++) r.group_ms[i] = m->prop_group_ms[i];
     std::lock_guard<std::mutex> lk(tune_mu);
     tune_cache()[key] = r;
     tune_save(cache_path, key, r);
