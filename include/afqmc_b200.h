@@ -359,10 +359,13 @@ afq_status afq_halfrotate(int device, const afq_csr_z* Spvn, int nmo, int naea, 
 /* Self-test of the tensor-core GEMM used by the mixed form (no reference counterpart):
  * C[b][m][n] = sum_k A[b][m][k] B[b][n][k] for host fp32 arrays, computed on the current
  * device with bf16 operands (tf32 == 0, inputs rounded to nearest bf16) or tf32 operands,
- * fp32 accumulation, tile width bn in {64, 128, 192}; K must be a multiple of 8.
+ * fp32 accumulation, tile width bn in {64, 128, 192, 256}; K must be a multiple of 8.
  * mode 0 = one CTA per tile, 1 / 2 = persistent kernel with one / two epilogue
  * warpgroups, 3 / 4 = per-tile / persistent kernel with 64-byte K slabs (SWIZZLE_64B
- * operand tiles).  *kernel_err receives the kernel's timeout flags (0 when clean). */
+ * operand tiles).  Split modes (bf16 only; hi = A rounded to bf16, lo = A - hi rounded,
+ * C = hi*hi + hi*lo + lo*hi): 5 / 6 = per-tile kernel with 128- / 64-byte K slabs,
+ * 7 / 8 = persistent kernel (two epilogue warpgroups) with 128- / 64-byte K slabs.
+ * *kernel_err receives the kernel's timeout flags (0 when clean). */
 afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn, int mode,
                                 const float* A, const float* B, float* C, int* kernel_err);
 /* Bound, in SM clocks, of the tensor-core kernels' pipeline waits on `device` (no

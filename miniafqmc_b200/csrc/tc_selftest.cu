@@ -24,6 +24,29 @@ struct EpiStoreF32 {
   }
 };
 
+// Split modes (bf16 hi + lo parts of both operands, hi*hi + hi*lo + lo*hi):
+// 5 / 6 = per-tile kernel with 128- / 64-byte K slabs, 7 / 8 = persistent kernel (two
+// epilogue warpgroups) with 128- / 64-byte K slabs.
+template <int BN>
+cudaError_t run_split(const void* dA, const void* dAl, const void* dB, const void* dBl,
+                      float* dC, int M, int N, int K, int batch, int mode, int* derr,
+                      cudaStream_t st) {
+  tc::Maps maps;
+  const uint32_t slab = (mode == 6 || mode == 8) ? 64 : 128;
+  const uint64_t sa = (uint64_t)M * K, sb = (uint64_t)N * K;
+  if (tc::make_kmajor_map(&maps.a, dA, false, K, M, batch, K, sa, 128, slab) != CUDA_SUCCESS ||
+      tc::make_kmajor_map(&maps.a_lo, dAl, false, K, M, batch, K, sa, 128, slab) != CUDA_SUCCESS ||
+      tc::make_kmajor_map(&maps.b, dB, false, K, N, batch, K, sb, BN, slab) != CUDA_SUCCESS ||
+      tc::make_kmajor_map(&maps.b_lo, dBl, false, K, N, batch, K, sb, BN, slab) != CUDA_SUCCESS)
+    return cudaErrorInvalidValue;
+  tc::GemmShape g{M, N, K, batch, 128, (M + 127) / 128, true, true, 0};
+  EpiStoreF32 epi{dC, M, N, (long long)M * N};
+  if (mode == 5) return tc::launch<BN, 2, 1, true, EpiStoreF32>(maps, g, epi, derr, st);
+  if (mode == 6) return tc::launch<BN, 4, 1, true, EpiStoreF32, 1, 64>(maps, g, epi, derr, st);
+  if (mode == 7) return tc::launch_persistent<BN, 2, 1, true, EpiStoreF32, 2>(maps, g, epi, derr, st);
+  return tc::launch_persistent<BN, 4, 1, true, EpiStoreF32, 2, 64>(maps, g, epi, derr, st);
+}
+
 template <int BN, bool TF32>
 cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, int batch,
                 int mode, int* derr, cudaStream_t st) {
@@ -51,11 +74,14 @@ cudaError_t run(const void* dA, const void* dB, float* dC, int M, int N, int K, 
 extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int tf32, int bn,
                                           int mode, const float* A, const float* B, float* C,
                                           int* kernel_err) {
-  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C || mode < 0 || mode > 4)
+  if (M <= 0 || N <= 0 || K <= 0 || batch <= 0 || !A || !B || !C || mode < 0 || mode > 8)
     return AFQ_ERR_ARG;
+  if (bn != 64 && bn != 128 && bn != 192 && bn != 256) return AFQ_ERR_ARG;
   if (K % 8 != 0) return AFQ_ERR_UNSUPPORTED;   // 16-byte row strides for TMA
+  const bool split = mode >= 5;
+  if (split && tf32) return AFQ_ERR_UNSUPPORTED;
   const size_t na = (size_t)batch * M * K, nb = (size_t)batch * N * K, nc = (size_t)batch * M * N;
-  void *dA = nullptr, *dB = nullptr;
+  void *dA = nullptr, *dB = nullptr, *dAl = nullptr, *dBl = nullptr;
   float* dC = nullptr;
   int* derr = nullptr;
   cudaStream_t st = nullptr;
@@ -66,21 +92,42 @@ extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int t
       cudaStreamCreate(&st) != cudaSuccess) {
     s = AFQ_ERR_OOM;
   }
+  if (s == AFQ_OK && split &&
+      (cudaMalloc(&dAl, na * 2) != cudaSuccess || cudaMalloc(&dBl, nb * 2) != cudaSuccess))
+    s = AFQ_ERR_OOM;
   if (s == AFQ_OK) {
     if (tf32) {
       cudaMemcpy(dA, A, na * 4, cudaMemcpyHostToDevice);
       cudaMemcpy(dB, B, nb * 4, cudaMemcpyHostToDevice);
     } else {
-      std::vector<__nv_bfloat16> ha(na), hb(nb);
-      for (size_t i = 0; i < na; i++) ha[i] = __float2bfloat16_rn(A[i]);
-      for (size_t i = 0; i < nb; i++) hb[i] = __float2bfloat16_rn(B[i]);
+      // hi = A rounded to bf16; the split modes also take lo = (A - hi) rounded to bf16
+      std::vector<__nv_bfloat16> ha(na), hb(nb), la(split ? na : 0), lb(split ? nb : 0);
+      for (size_t i = 0; i < na; i++) {
+        ha[i] = __float2bfloat16_rn(A[i]);
+        if (split) la[i] = __float2bfloat16_rn(A[i] - __bfloat162float(ha[i]));
+      }
+      for (size_t i = 0; i < nb; i++) {
+        hb[i] = __float2bfloat16_rn(B[i]);
+        if (split) lb[i] = __float2bfloat16_rn(B[i] - __bfloat162float(hb[i]));
+      }
       cudaMemcpy(dA, ha.data(), na * 2, cudaMemcpyHostToDevice);
       cudaMemcpy(dB, hb.data(), nb * 2, cudaMemcpyHostToDevice);
+      if (split) {
+        cudaMemcpy(dAl, la.data(), na * 2, cudaMemcpyHostToDevice);
+        cudaMemcpy(dBl, lb.data(), nb * 2, cudaMemcpyHostToDevice);
+      }
     }
     cudaMemset(dC, 0, nc * 4);
     cudaMemset(derr, 0, sizeof(int));
     cudaError_t e;
-    if (bn == 64) e = tf32 ? run<64, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
+    if (split) {
+      if (bn == 64) e = run_split<64>(dA, dAl, dB, dBl, dC, M, N, K, batch, mode, derr, st);
+      else if (bn == 192) e = run_split<192>(dA, dAl, dB, dBl, dC, M, N, K, batch, mode, derr, st);
+      else if (bn == 256) e = run_split<256>(dA, dAl, dB, dBl, dC, M, N, K, batch, mode, derr, st);
+      else e = run_split<128>(dA, dAl, dB, dBl, dC, M, N, K, batch, mode, derr, st);
+    } else if (bn == 256) e = tf32 ? run<256, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
+                                   : run<256, false>(dA, dB, dC, M, N, K, batch, mode, derr, st);
+    else if (bn == 64) e = tf32 ? run<64, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
                            : run<64, false>(dA, dB, dC, M, N, K, batch, mode, derr, st);
     else if (bn == 192) e = tf32 ? run<192, true>(dA, dB, dC, M, N, K, batch, mode, derr, st)
                                  : run<192, false>(dA, dB, dC, M, N, K, batch, mode, derr, st);
@@ -94,6 +141,8 @@ extern "C" afq_status afq_selftest_tc_gemm(int M, int N, int K, int batch, int t
   if (st) cudaStreamDestroy(st);
   cudaFree(dA);
   cudaFree(dB);
+  cudaFree(dAl);
+  cudaFree(dBl);
   cudaFree(dC);
   cudaFree(derr);
   return s;
