@@ -276,7 +276,12 @@ afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
  *   stay in L2 between its products; 0 = every product over all walkers at once.  Timed:
  *   0, 32, 48, 64, 96 and 128 walkers (those below nwalk) -> ms[0..5].  Results do not
  *   depend on it.  AFQ_PROP_GROUP=<walkers> forces one.
- * ms[6] may be NULL; 0 where not timed. */
+ * sched[1]: epilogue of the vHS product over symmetric block pairs: 0 = row-wise (each
+ *   lane writes its walker's entries, the mirrored block as 4-byte stores), 1 = through
+ *   the fp32 tile in shared memory on the per-tile kernel (direct and mirrored rows as
+ *   16-byte stores).  Same values.  Timed -> ms[6..7].  AFQ_VHS_EPI=0|1 forces one; a
+ *   forced kernel (AFQ_TUNE=1 or 2) keeps 0.
+ * ms[8] may be NULL; 0 where not timed. */
 afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */

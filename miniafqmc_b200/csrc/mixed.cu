@@ -141,6 +141,10 @@ struct MixedState {
   // density matrix: its row-strided stores cost the epilogue more than the pack kernel.)
   Op F2;
   tc::Maps m_pw2, m_t1_1;
+  // symmetric vHS epilogue: 0 row-wise (EpiVhsSym, the tuned kernel), 1 through the
+  // shared-memory tile (EpiVhsSymTile, per-tile kernel); picked by the set-up tuner
+  int vhs_epi = 0;
+  float vhs_epi_ms[2] = {};
   bool packed = false;
   int fa_buf = 0;
   // kernel of each product site (0 built-in rule, 1 persistent, 2 per-tile), chosen at
@@ -841,6 +845,65 @@ struct EpiVhsSym {
       const int j = jb * 16 + jj;
       put2(V, (vw + (long long)i * N + j) * 2, re, im);
       if (ib != jb) put2(V, (vw + (long long)j * N + i) * 2, re, im);
+    }
+  }
+};
+
+// EpiVhsSym through the fp32 tile in shared memory (per-tile kernel): the same values,
+// written as 16-byte vector stores of four complex entries.  Tile row r = 2 wl (Re) /
+// 2 wl + 1 (Im) of walker mt * 64 + wl, column q = ii * 16 + jj.  Items (walker, row of
+// the 16 x 16 block, quarter): V[i][jb*16 + 4 quarter ..] from row ii of the block and,
+// off the block diagonal, V[j][ib*16 + 4 quarter ..] from column jj (the mirror), so both
+// halves leave as contiguous 64-byte rows instead of the row-wise functor's
+// one-lane-per-walker 4-byte mirror stores.  Needs N % 4 == 0 (16-byte aligned rows).
+struct EpiVhsSymTile {
+  static constexpr bool kTile = true, kPair = false;
+  Op V;
+  int nw, N;
+  const int* pairs;
+  AFQ_D static void put4(const Op& o, long long idx, const float* re, const float* im) {
+    bf162 h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      h[e] = __floats2bfloat162_rn(re[e], im[e]);
+      const float2 hf = __bfloat1622float2(h[e]);
+      l[e] = __floats2bfloat162_rn(re[e] - hf.x, im[e] - hf.y);
+    }
+    *reinterpret_cast<uint4*>(o.hi + idx) = *reinterpret_cast<const uint4*>(h);
+    if (o.lo) *reinterpret_cast<uint4*>(o.lo + idx) = *reinterpret_cast<const uint4*>(l);
+  }
+  AFQ_D void tile(int, int mt, int nt, const float* t, int ld, int tid) const {
+    int tt = nt, ib = 0;   // tile -> block pair (ib, jb), ib <= jb, in row order
+    const int nb = N >> 4;
+    while (tt >= nb - ib) { tt -= nb - ib; ib++; }
+    const int jb = ib + tt;
+    const int nmir = ib != jb ? 2 : 1;
+    // items: (mirror, walker, block row, quarter), quarter fastest
+#pragma unroll 1
+    for (int it = tid; it < nmir * 64 * 16 * 4; it += 128) {
+      const int qt = it & 3, rr = (it >> 2) & 15, wl = (it >> 6) & 63, mir = it >> 12;
+      const int w = mt * 64 + wl;
+      if (w >= nw) continue;
+      const float* tr = t + (2 * wl) * ld;
+      const float* ti = tr + ld;
+      float re[4], im[4];
+      long long row;
+      if (!mir) {   // V[ib*16 + rr][jb*16 + 4 qt + e] = tile column rr*16 + 4 qt + e
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          re[e] = tr[rr * 16 + 4 * qt + e];
+          im[e] = ti[rr * 16 + 4 * qt + e];
+        }
+        row = (long long)w * N * N + (long long)(ib * 16 + rr) * N + jb * 16 + 4 * qt;
+      } else {      // V[jb*16 + rr][ib*16 + 4 qt + e] = tile column (4 qt + e)*16 + rr
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          re[e] = tr[(4 * qt + e) * 16 + rr];
+          im[e] = ti[(4 * qt + e) * 16 + rr];
+        }
+        row = (long long)w * N * N + (long long)(jb * 16 + rr) * N + ib * 16 + 4 * qt;
+      }
+      put4(V, row * 2, re, im);
     }
   }
 };
@@ -1739,6 +1802,10 @@ static cudaError_t vhs_product(MixedState* m, cudaStream_t st) {
   if (m->vsym) {
     tc::GemmShape g{2 * nw, m->npairs * 256, m->Kv, 1, 128, (2 * nw + 127) / 128, false, false, 0,
                     true};
+    if (m->vhs_epi == 1) {
+      EpiVhsSymTile epi{m->Vf, nw, N, m->pairs};
+      return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, 2);
+    }
     EpiVhsSym epi{m->Vf, nw, N, m->pairs};
     return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, m->tune[TS_VHS]);
   }
@@ -2204,6 +2271,8 @@ struct TuneRec {
   int tune[TS_N];
   float ms[TS_N][2];
   float group_ms[6];
+  int vhs_epi;
+  float vhs_epi_ms[2];
   int splits;
   int prop_group;
 };
@@ -2238,6 +2307,7 @@ void tune_load(const char* path) {
     for (int i = 0; i < TS_N && ok; i++)
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.group_ms[i]) == 1;
+    if (ok) ok = fscanf(f, "%d %f %f", &r.vhs_epi, &r.vhs_epi_ms[0], &r.vhs_epi_ms[1]) == 3;
     if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
     tune_cache()[key] = r;
     tune_file_keys().insert(key);
@@ -2251,6 +2321,7 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   fprintf(f, "%s", key.c_str());
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.group_ms[i]);
+  fprintf(f, " %d %.5f %.5f", r.vhs_epi, r.vhs_epi_ms[0], r.vhs_epi_ms[1]);
   fprintf(f, " %d %d\n", r.splits, r.prop_group);
   fclose(f);
 }
@@ -2266,7 +2337,9 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   if (force < 0 && !tc_persistent()) force = 2;   // AFQ_TC_PERSISTENT=0: per-tile kernels
   const char* fsk = getenv("AFQ_SPLITK");
   const char* fpg = getenv("AFQ_PROP_GROUP");
-  const std::string key = tune_key(m) + "_pg" + std::to_string(fpg ? atoi(fpg) : -1) + "_f" +
+  const char* fve = getenv("AFQ_VHS_EPI");
+  const std::string key = tune_key(m) + "_pg" + std::to_string(fpg ? atoi(fpg) : -1) + "_ve" +
+                          std::to_string(fve ? atoi(fve) : -1) + "_f" +
                           std::to_string(force) + "_k" +
                           std::to_string(fsk ? atoi(fsk) : 0) + "_p" +
                           std::to_string(promote_kb(PROMOTE_PART)) +
@@ -2289,6 +2362,9 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       }
       m->prop_group = r.prop_group;
       for (int i = 0; i < 6; i++) m->prop_group_ms[i] = r.group_ms[i];
+      m->vhs_epi = r.vhs_epi;
+      m->vhs_epi_ms[0] = r.vhs_epi_ms[0];
+      m->vhs_epi_ms[1] = r.vhs_epi_ms[1];
       tune_save(cache_path, key, r);   // a shape timed before the file was named
       return cudaSuccess;
     }
@@ -2365,6 +2441,21 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     m->tune[site] = best;
   };
   pick(TS_VHS, [&] { return vhs_product(m, st); });
+  // then the symmetric vHS epilogue: the tuned row-wise one against the shared-memory
+  // tile (full tuning only, so forced kernels stay comparable); AFQ_VHS_EPI=0|1 forces
+  if (m->vsym && m->tune[TS_VHS] && force < 0) {
+    const char* fe = getenv("AFQ_VHS_EPI");
+    float t[2] = {0.0f, 0.0f};
+    for (int v = 0; v < 2; v++) {
+      if (fe && atoi(fe) != v) continue;
+      m->vhs_epi = v;
+      const float ms = timed([&] { return vhs_product(m, st); });
+      t[v] = ms > 0.0f ? ms : 0.0f;
+    }
+    m->vhs_epi = (t[1] > 0.0f && (t[0] <= 0.0f || t[1] < t[0])) ? 1 : 0;
+    m->vhs_epi_ms[0] = t[0];
+    m->vhs_epi_ms[1] = t[1];
+  }
   {
     const int mt = (N + 127) / 128, n2 = 2 * n;
     const int Kp = m->preal ? N : 2 * N;
@@ -2467,6 +2558,9 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     r.splits = m->splits;
     r.prop_group = m->prop_group;
     for (int i = 0; i < 6; i++) r.group_ms[i] = m->prop_group_ms[i];
+    r.vhs_epi = m->vhs_epi;
+    r.vhs_epi_ms[0] = m->vhs_epi_ms[0];
+    r.vhs_epi_ms[1] = m->vhs_epi_ms[1];
     std::lock_guard<std::mutex> lk(tune_mu);
     tune_cache()[key] = r;
     tune_save(cache_path, key, r);
@@ -2481,6 +2575,12 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
             m->tune_ms[TS_EXS][0], m->tune_ms[TS_EXS][1], m->tune[TS_T1], m->tune_ms[TS_T1][0],
             m->tune_ms[TS_T1][1]);
   return e;
+}
+
+int mixed_vhs_epilogue(const MixedState* m, float* ms) {
+  if (ms)
+    for (int i = 0; i < 2; i++) ms[i] = m ? m->vhs_epi_ms[i] : 0.0f;
+  return m ? m->vhs_epi : 0;
 }
 
 int mixed_prop_group(const MixedState* m, float* ms) {

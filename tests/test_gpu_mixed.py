@@ -243,3 +243,27 @@ def test_copy_walkers_between_forms():
         other.copy_walkers_from(d)
     for e in (d, m, other):
         e.close()
+
+
+def test_vhs_tile_epilogue_matches_rowwise(monkeypatch):
+    """The symmetric vHS product's two epilogues -- row-wise (each lane its walker's
+    entries) and through the fp32 tile in shared memory (16-byte rows, mirrored block
+    included) -- write the same V bit for bit: the same MMAs and the same bf16 rounding.
+    80 walkers: the second M tile holds 16 walkers and 96 empty rows."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    monkeypatch.delenv("AFQ_TUNE", raising=False)
+    s = system("C2", with_vakbl=False)
+    nw = 80
+    wk = perturbed(s, nw)
+    out = {}
+    for ve in ("0", "1"):
+        monkeypatch.setenv("AFQ_VHS_EPI", ve)
+        m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=wk, use_vakbl=False)
+        assert m.tuning()["vhs_epilogue"]["tile"] == int(ve)
+        m.calculate_mixed_density_matrix()
+        m.get_vbias()
+        m.sigma(3, 1)
+        m.get_vHS()
+        out[ve] = m.copy_out("vHS")
+        m.close()
+    assert np.array_equal(out["0"], out["1"])
