@@ -286,7 +286,7 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 // operand batches za / zb.  The shared-memory ring is laid out for BN.
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int SLAB>
 AFQ_D void gemm_tile(const Maps& maps, int mt, int nt, int m0, int n0, int batch, int za,
-                     int zb, int kbase, int klen, int bn, const Epi& epi, int* err) {
+                     int zb, int kbase, int klen, int bn, const Epi epi, int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
@@ -583,6 +583,11 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const int total = job.tile0[job.np];
+  // one problem: the epilogue functor as a local copy, so the compiler knows the
+  // epilogue's global stores cannot change it (a reference into the parameter block makes
+  // it reload the fields after every store); several problems, and the staged functors
+  // (whose copies would spill beside their staging arrays): a reference
+  using EpiHold = std::conditional_t<NP == 1 && !EpiStaged<Epi>::value, const Epi, const Epi&>;
   // K slabs of tile t's problem
   auto kslabs = [&](int p, int z, int& kbase) {
     const int ks = job.k_split[p];
@@ -692,7 +697,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
         job.locate(t, p, z, mt, nt);
         const int nk = kslabs(p, z, kbase);
         const int nch = (nk + PK - 1) / PK;
-        const Epi& epi = job.epi[p];
+        EpiHold epi = job.epi[p];
         for (int ch = 0; ch < nch; ch++, li++) {
           const int b = li & 1;
           if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
@@ -731,7 +736,7 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
     for (int t = blockIdx.x; t < total; t += gridDim.x, li++) {
       int p, z, mt, nt;
       job.locate(t, p, z, mt, nt);
-      const Epi& epi = job.epi[p];
+      EpiHold epi = job.epi[p];
       const int bn = job.bn[p];
       const int b = li & 1;
       if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
