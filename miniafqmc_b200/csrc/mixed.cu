@@ -125,6 +125,10 @@ struct MixedState {
   int ex_Gn = 0, ex_Gw = 0, ex_bn = 0, ex_mtiles = 0;
   std::vector<void*> allocs;
   tc::Maps m_vhs, m_pw[2], m_v[2], m_vbias, m_ej, m_ek;
+  // walker width 2n = 80: the promoted exchange on 160-column tiles (two walkers, one
+  // epilogue warpgroup), with its own Gx map (160-row boxes)
+  tc::Maps m_ek80;
+  bool ex80 = false;
   // symmetric Cholesky vectors (L_n(i,k) = L_n(k,i)): the vHS product covers the 16 x 16
   // orbital blocks (ib <= jb) only and the epilogue mirrors them
   bool vsym = false;
@@ -1740,6 +1744,11 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
     m->ex_mtiles = (nc + m->ex_Gn - 1) / m->ex_Gn;
     ok &= map2(m->m_ek, m->LhX, Kx, (uint64_t)nc * n, 2, Kx, (uint64_t)nc * n * Kx, m->Gx, Kx,
                (uint64_t)nw * 2 * n, 2, Kx, (uint64_t)nw * 2 * n * Kx, m->ex_bn);
+    if (2 * n == 80) {
+      m->ex80 = map2(m->m_ek80, m->LhX, Kx, (uint64_t)nc * n, 2, Kx, (uint64_t)nc * n * Kx, m->Gx,
+                     Kx, (uint64_t)nw * 2 * n, 2, Kx, (uint64_t)nw * 2 * n * Kx, 160);
+      ok &= m->ex80;
+    }
   }
   if (init->trial && n <= 64) {
     m->bn_t1 = pick_bn(4 * n);
@@ -2149,6 +2158,22 @@ cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t 
   return splitk_product(m, m->m_ej, m->prec_ej, m->sLh, cvec, st);
 }
 
+// The promoted exchange for 2n = 80: 160-column tiles of two walkers, one epilogue
+// warpgroup holding all 160 accumulator columns (5 chunks of 32).
+template <int PK>
+static cudaError_t exchange80(MixedState* m, const tc::GemmShape& g, int nsub, z_t* Kpart,
+                              int nblk, float as, const float* ws, cudaStream_t st) {
+  using E = EpiExchangePromoted<80, PK>;
+  const E ep{m->n, m->ex_Gn, 2, m->nc, nsub, nblk, Kpart, as, ws};
+  tc::GemmShape g2 = g;
+  g2.n_step = 160;
+  if (m->prec_ek == PREC_SPLIT16)
+    return tc::launch_persistent<160, 2, 0, true, E, 1>(m->m_ek80, g2, ep, m->err, st);
+  if (m->prec_ek == PREC_SPLIT)
+    return tc::launch_persistent<160, 2, 1, true, E, 1>(m->m_ek80, g2, ep, m->err, st);
+  return tc::launch_persistent<160, 4, 1, false, E, 1>(m->m_ek80, g2, ep, m->err, st);
+}
+
 // Exchange product of the first nsub walkers packed in Gx: the staged persistent kernel
 // (per-row traces from TMEM) for the compiled walker widths, else the per-tile kernel.
 static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nblk,
@@ -2163,6 +2188,10 @@ static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nbl
                   m->ex_mtiles, true, true, 0, false, m->ex_Gw * 2 * n};
   const int v = m->tune[2 * nsub > m->nw ? TS_EXF : TS_EXS];
   const int pk = promote_kb(PROMOTE_EXCHANGE);
+  if ((v == 1 || (v == 0 && tc_persistent())) && pk && m->ex80) {
+    if (pk == 1) return exchange80<1>(m, g, nsub, Kpart, nblk, as, ws, st);
+    if (pk == 2) return exchange80<2>(m, g, nsub, Kpart, nblk, as, ws, st);
+  }
   if ((v == 1 || (v == 0 && tc_persistent())) && pk && (m->ex_bn / 2) % (2 * n) == 0) {
     cudaError_t r = cudaErrorInvalidValue;
 #define AFQ_EXP(TN, PK)                                                                        \
@@ -2526,11 +2555,14 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   }
   if (m->in.Lh) {
     const int nsub = std::max(1, nw / 8);
-    // the promoted exchange instances (walker widths 24, 32, 64, 96, 128) run on the
-    // persistent kernel only: the tuner may not trade their accuracy for speed
+    // the promoted exchange instances (walker widths 24, 32, 64, 96, 128, and 80 on its
+    // own 160-column tiles) run on the persistent kernel only: the tuner may not trade
+    // their accuracy for speed
     const int w2 = 2 * n;
-    const bool exp = promote_kb(PROMOTE_EXCHANGE) > 0 && (w2 == 24 || w2 == 32 || w2 == 64 ||
-                     w2 == 96 || w2 == 128) && (m->ex_bn / 2) % w2 == 0;
+    const int pke = promote_kb(PROMOTE_EXCHANGE);
+    const bool exp = (pke > 0 && (w2 == 24 || w2 == 32 || w2 == 64 || w2 == 96 || w2 == 128) &&
+                      (m->ex_bn / 2) % w2 == 0) ||
+                     ((pke == 1 || pke == 2) && m->ex80);
     pick(TS_EXF, [&] { return exchange_product(m, nw, kp, m->ex_mtiles, st); }, exp);
     pick(TS_EXS, [&] { return exchange_product(m, nsub, kp, m->ex_mtiles, st); }, exp);
   }

@@ -124,9 +124,10 @@ def test_fused_batch_needs_mixed_systems():
 
 def test_c5_shapes_mixed_energy_matches_fp64():
     """Mixed against FP64 energies on identical walkers for the C5 shapes (n = 12, 40 and
-    64: exchange tiles of 8 walkers of 24 columns, 3 walkers of 80 columns in a 256-column
-    tile, 2 walkers of 128 columns): 1e-4 relative on every walker's E_J and E_K, and the
-    mean local energy within 1e-4 Ha."""
+    64: promoted exchange tiles of 8 walkers of 24 columns, 2 walkers of 80 columns in a
+    160-column tile, 2 walkers of 128 columns): 1e-4 relative on every walker's E_J and E_K,
+    and the mean local energy within 1e-4 Ha.  Every width runs the promoted exchange (the
+    set-up tuner keeps it: exchange kernel 1)."""
     from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
     rng = np.random.default_rng(3)
     for cfg, s in systems():
@@ -139,6 +140,9 @@ def test_c5_shapes_mixed_energy_matches_fp64():
             e.calculate_mixed_density_matrix()
             e.calculate_energy("chol")
             parts.append(e.copy_out("energy_parts"))
+            if prec == AFQ_PREC_MIXED:
+                tun = e.tuning()
+                assert tun["exchange_all"]["kernel"] == 1, (cfg.nel, tun["exchange_all"])
             e.close()
         pd, pm = parts
         ej = rel(pm[:, 1], pd[:, 1])
