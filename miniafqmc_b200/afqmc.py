@@ -330,14 +330,17 @@ class AfqmcSys:
                                                round(float(t[2 * i + 1]), 4)]}
                for i, k in enumerate(self.TUNE_SITES)}
         out["splitk_slices"] = int(c[ns])
-        sc = np.zeros(2, np.int32)
-        gm = np.zeros(8)
+        sc = np.zeros(3, np.int32)
+        gm = np.zeros(12)
         self._check(self.lib.afq_get_schedule(self.h, _p(sc), _p(gm)))
         out["propagate_walker_group"] = {"walkers": int(sc[0]),
                                          "ms_all_32_48_64_96_128": [round(float(x), 4)
                                                                     for x in gm[:6]]}
         out["vhs_epilogue"] = {"tile": int(sc[1]),
                                "ms_rowwise_tile": [round(float(x), 4) for x in gm[6:8]]}
+        out["propagate_chain"] = {"wave": int(sc[2]),
+                                  "ms_launches_16_24_32": [round(float(x), 4)
+                                                           for x in gm[8:12]]}
         return out
 
     SPARSE_OPERANDS = ["Spvn", "SpvnT", "Vakbl"]

@@ -160,6 +160,12 @@ struct MixedState {
   // set-up tuner (prop_group_ms: the timed chain per candidate, 0 = all walkers first)
   int prop_group = 0;
   float prop_group_ms[6] = {};
+  // the propagation chain as one cooperative persistent launch per substep (2n a multiple
+  // of 32): per-walker dependency counters, walkers per wave (0: eight launches), timed by
+  // the set-up tuner (chain_ms: eight launches, waves of 16, 24 and 32 walkers)
+  unsigned* dep = nullptr;
+  int chain_wave = 0;
+  float chain_ms[4] = {};
   int splits0 = 1, part_cap = 1;
 };
 
@@ -1156,6 +1162,26 @@ struct EpiPropPack {
   }
 };
 
+// Epilogue of the fused propagation chain: EpiPropPair for P W and the Taylor terms,
+// EpiPropPack for the last product; the active functor is copied locally per call so its
+// fields stay in registers across the stores.
+struct EpiChain {
+  static constexpr bool kTile = false, kPair = true;
+  int pack;
+  EpiPropPair pr;
+  EpiPropPack pk;
+  AFQ_D int pair_stride() const { return pr.n2; }
+  AFQ_D void pair(int w, int r, int i, int j0, const float* cr, const float* ci) const {
+    if (pack) {
+      const EpiPropPack e = pk;
+      e.pair(w, r, i, j0, cr, ci);
+    } else {
+      const EpiPropPair e = pr;
+      e.pair(w, r, i, j0, cr, ci);
+    }
+  }
+};
+
 // Exchange: rows (cv, a), columns (wl, re|im, b); per (cv, wl) the trace of T^2 with
 // T[a][b] = tile[cv*n + a][wl*2n + b] + i tile[cv*n + a][wl*2n + n + b].
 struct EpiExchange {
@@ -1566,6 +1592,7 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   A(alloc_op(m, m->Gb, (size_t)2 * nw * 2 * NAK));
   A(malloc_track(m, &m->S, (size_t)nw * N * 2 * n));
   A(malloc_track(m, &m->err, 1));
+  if ((2 * n) % 32 == 0) A(malloc_track(m, &m->dep, (size_t)nw));   // fused chain counters
   A(malloc_track(m, &m->wscale, nw));
   A(malloc_track(m, &m->dmax, 2));
   A(alloc_op(m, m->F2, (size_t)nw * 4 * n * 2 * N));
@@ -1794,7 +1821,8 @@ int mixed_launches(const MixedState* m, int stage) {
     case 1: return 3;                                  // pack, GEMM, reduce (vbias)
     case 3: return 2;                                  // pack, GEMM (vHS)
     // the walker packs drop out while the packed forms are current (m->packed at the call)
-    case 4: {   // [pack], then per walker group P W, terms, P S
+    case 4: {   // [pack], then per walker group P W, terms, P S (one launch when fused)
+      if (m->chain_wave > 0) return (m->packed ? 0 : 1) + 1;
       const int G = m->prop_group > 0 && m->prop_group < m->nw ? m->prop_group : m->nw;
       return (m->packed ? 0 : 1) + ((m->nw + G - 1) / G) * (m->in.order + 2);
     }
@@ -1845,7 +1873,88 @@ cudaError_t mixed_unpack_vhs(MixedState* m, z_t* vHS, cudaStream_t st) {
 // B operand of the next product: the lo part only when that product runs split
 static Op next_op(const Op& F, int prec) { return prec == PREC_SPLIT ? F : Op{F.hi, nullptr}; }
 
+// The whole propagation chain as one cooperative persistent launch (tc::launch_chain):
+// P W, the Taylor terms and P S over walker waves of `wave` walkers, a product's tile of
+// walker w starting once every tile of the previous product of w has published; the same
+// tiles, MMA order and epilogue arithmetic as the eight launches, so the same walkers.
+// timing (W unused, may be null): no pack of W, and the last product writes S and an
+// operand (as the tuner's eight-launch timing does) instead of the walkers and their
+// packed forms.
+using ChainJob = tc::PJob<EpiChain, 8>;
+static cudaError_t propagate_chain(MixedState* m, z_t* W, int wave, bool timing,
+                                   cudaStream_t st) {
+  const int N = m->N, n2 = 2 * m->n, nw = m->nw, order = m->in.order;
+  if (n2 % 32 || !m->dep || order + 2 > 8 || wave < 1) return cudaErrorInvalidValue;
+  for (int p : {m->prec_p, m->prec_v1, m->prec_vk})
+    if (p != PREC_SPLIT && p != PREC_BF16) return cudaErrorInvalidValue;
+  const bool pr = m->preal && order >= 1;
+  const bool from_f2 = !timing && m->packed;   // the P W operand is in F2 already
+  if (!timing) m->packed = false;
+  cudaError_t e;
+  if (!from_f2 && !timing) {
+    pack_w_kernel<<<dim3((N + 31) / 32, (n2 + 31) / 32, nw), dim3(32, 8), 0, st>>>(
+        W, N, n2, m->F[0], pr ? 2 : 1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  ChainJob job{};
+  const int mt = (N + 127) / 128, ntl = (2 * n2 + m->bn_prop - 1) / m->bn_prop;
+  const int Kp = pr ? N : 2 * N;
+  auto add = [&](int p, const tc::Maps& mp, const EpiChain& ep, int K, int a_batched, int prec) {
+    job.maps[p] = mp;
+    job.epi[p] = ep;
+    job.sched[p] = tc::TileSched{mt, ntl, nw, 0, 0};
+    job.K[p] = K;
+    job.m_step[p] = 128;
+    job.n_step[p] = m->bn_prop;
+    job.a_batched[p] = a_batched;
+    job.b_batched[p] = 1;
+    job.k_split[p] = 0;
+    job.bn[p] = m->bn_prop;
+    job.split[p] = prec == PREC_SPLIT ? 1 : 0;
+  };
+  add(0, from_f2 ? m->m_pw2 : m->m_pw[0],
+      EpiChain{0, EpiPropPair{0, 0, 0, N, n2, m->S, W, next_op(m->F[1], m->prec_v1), 0}, {}}, Kp,
+      0, m->prec_p);
+  int cur = 1;
+  for (int k = 1; k <= order; k++) {  // T_k = (i/k) V T_{k-1}; S += T_k
+    const int prec = k == 1 ? m->prec_v1 : m->prec_vk;
+    const int nprec = k < order ? m->prec_vk : m->prec_p;
+    add(k, m->m_v[cur],
+        EpiChain{0, EpiPropPair{1, k, k == order ? 1 : 0, N, n2, m->S, W,
+                                next_op(m->F[cur ^ 1], nprec), (k == order && m->preal) ? 1 : 0},
+                 {}},
+        2 * N, 1, prec);
+    cur ^= 1;
+  }
+  if (timing)
+    add(order + 1, m->m_pw[cur],
+        EpiChain{0, EpiPropPair{0, 0, 0, N, n2, m->S, W, next_op(m->F[cur ^ 1], m->prec_p), 0}, {}},
+        Kp, 0, m->prec_p);
+  else   // W = P S with the new walkers' packed forms
+    add(order + 1, m->m_pw[cur],
+        EpiChain{1, {}, EpiPropPack{N, n2, W, m->F[cur ^ 1], m->F2, pr ? 1 : 0}}, Kp, 0,
+        m->prec_p);
+  job.np = order + 2;
+  job.dep = m->dep;
+  job.wave = wave;
+  job.nbatch = nw;
+  if ((e = cudaMemsetAsync(m->dep, 0, sizeof(unsigned) * nw, st)) != cudaSuccess) return e;
+  switch (m->bn_prop) {
+    case 64: e = tc::launch_chain<64, 2, 1, EpiChain, 2, 8>(job, m->err, st); break;
+    case 128: e = tc::launch_chain<128, 2, 1, EpiChain, 2, 8>(job, m->err, st); break;
+    case 192: e = tc::launch_chain<192, 2, 1, EpiChain, 2, 8>(job, m->err, st); break;
+    case 256: e = tc::launch_chain<256, 2, 1, EpiChain, 2, 8>(job, m->err, st); break;
+    default: e = cudaErrorInvalidValue;
+  }
+  if (e == cudaSuccess && !timing && m->Wn.hi) {
+    m->packed = true;
+    m->fa_buf = cur ^ 1;
+  }
+  return e;
+}
+
 cudaError_t mixed_propagate(MixedState* m, z_t* W, const z_t*, cudaStream_t st) {
+  if (m->chain_wave > 0) return propagate_chain(m, W, m->chain_wave, false, st);
   const int N = m->N, n2 = 2 * m->n, nw = m->nw;
   const bool pr = m->preal && m->in.order >= 1;
   const bool from_f2 = m->packed;   // the P W operand of these walkers is in F2 already
@@ -2302,6 +2411,8 @@ struct TuneRec {
   float group_ms[6];
   int vhs_epi;
   float vhs_epi_ms[2];
+  int chain_wave;
+  float chain_ms[4];
   int splits;
   int prop_group;
 };
@@ -2337,6 +2448,8 @@ void tune_load(const char* path) {
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.group_ms[i]) == 1;
     if (ok) ok = fscanf(f, "%d %f %f", &r.vhs_epi, &r.vhs_epi_ms[0], &r.vhs_epi_ms[1]) == 3;
+    if (ok) ok = fscanf(f, "%d", &r.chain_wave) == 1;
+    for (int i = 0; i < 4 && ok; i++) ok = fscanf(f, "%f", &r.chain_ms[i]) == 1;
     if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
     tune_cache()[key] = r;
     tune_file_keys().insert(key);
@@ -2351,6 +2464,8 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.group_ms[i]);
   fprintf(f, " %d %.5f %.5f", r.vhs_epi, r.vhs_epi_ms[0], r.vhs_epi_ms[1]);
+  fprintf(f, " %d %.5f %.5f %.5f %.5f", r.chain_wave, r.chain_ms[0], r.chain_ms[1],
+          r.chain_ms[2], r.chain_ms[3]);
   fprintf(f, " %d %d\n", r.splits, r.prop_group);
   fclose(f);
 }
@@ -2367,8 +2482,10 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   const char* fsk = getenv("AFQ_SPLITK");
   const char* fpg = getenv("AFQ_PROP_GROUP");
   const char* fve = getenv("AFQ_VHS_EPI");
+  const char* fch = getenv("AFQ_PROP_CHAIN");
   const std::string key = tune_key(m) + "_pg" + std::to_string(fpg ? atoi(fpg) : -1) + "_ve" +
-                          std::to_string(fve ? atoi(fve) : -1) + "_f" +
+                          std::to_string(fve ? atoi(fve) : -1) + "_ch" +
+                          std::to_string(fch ? atoi(fch) : -1) + "_f" +
                           std::to_string(force) + "_k" +
                           std::to_string(fsk ? atoi(fsk) : 0) + "_p" +
                           std::to_string(promote_kb(PROMOTE_PART)) +
@@ -2394,6 +2511,8 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       m->vhs_epi = r.vhs_epi;
       m->vhs_epi_ms[0] = r.vhs_epi_ms[0];
       m->vhs_epi_ms[1] = r.vhs_epi_ms[1];
+      m->chain_wave = m->dep ? r.chain_wave : 0;
+      for (int i = 0; i < 4; i++) m->chain_ms[i] = r.chain_ms[i];
       tune_save(cache_path, key, r);   // a shape timed before the file was named
       return cudaSuccess;
     }
@@ -2527,6 +2646,27 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       }
     }
     m->prop_group = best;
+    // then the whole chain as one cooperative launch (waves of 16, 24 or 32 walkers)
+    // against the eight launches of the chosen kernel over all walkers; AFQ_PROP_CHAIN=0
+    // keeps the eight launches, =<walkers> forces a wave
+    const char* fc = getenv("AFQ_PROP_CHAIN");
+    const int fcw = fc ? atoi(fc) : -1;
+    if (m->dep && m->prop_group == 0 && m->tune[TS_PROP] && fcw != 0) {
+      m->chain_ms[0] = m->prop_group_ms[0];
+      const int waves[3] = {16, 24, 32};
+      int bw = 0;
+      float bwt = m->chain_ms[0] > 0.0f && fcw < 0 ? m->chain_ms[0] : 0.0f;
+      for (int c = 0; c < 3; c++) {
+        if (fcw > 0 && waves[c] != fcw) continue;
+        const float t = timed([&] { return propagate_chain(m, nullptr, waves[c], true, st); });
+        m->chain_ms[c + 1] = t > 0.0f ? t : 0.0f;
+        if (t > 0.0f && (bwt == 0.0f || t < bwt)) {
+          bwt = t;
+          bw = waves[c];
+        }
+      }
+      m->chain_wave = bw;
+    }
   }
   {  // split-K slices x kernel
     int bs = m->splits0, bv = 0;
@@ -2593,6 +2733,8 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     r.vhs_epi = m->vhs_epi;
     r.vhs_epi_ms[0] = m->vhs_epi_ms[0];
     r.vhs_epi_ms[1] = m->vhs_epi_ms[1];
+    r.chain_wave = m->chain_wave;
+    for (int i = 0; i < 4; i++) r.chain_ms[i] = m->chain_ms[i];
     std::lock_guard<std::mutex> lk(tune_mu);
     tune_cache()[key] = r;
     tune_save(cache_path, key, r);
@@ -2607,6 +2749,12 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
             m->tune_ms[TS_EXS][0], m->tune_ms[TS_EXS][1], m->tune[TS_T1], m->tune_ms[TS_T1][0],
             m->tune_ms[TS_T1][1]);
   return e;
+}
+
+int mixed_prop_chain(const MixedState* m, float* ms) {
+  if (ms)
+    for (int i = 0; i < 4; i++) ms[i] = m ? m->chain_ms[i] : 0.0f;
+  return m ? m->chain_wave : 0;
 }
 
 int mixed_vhs_epilogue(const MixedState* m, float* ms) {

@@ -518,6 +518,17 @@ struct PCfg {
 // Problem p owns tiles [tile0[p], tile0[p + 1]), decoded by sched[p]; its tensor maps,
 // K, row / column steps, split-K extent, tile width bn[p] <= BN (a multiple of 32; BN for
 // promoting epilogues) and epilogue functor are its own.
+//
+// Chain launches (the kernel's CHAIN parameter): the problems are consecutive products of
+// one batched chain (problem p + 1 reads what problem p wrote for the same batch), all of
+// the same batch count and tiles per batch.  The tile list runs in pairs of walker waves
+// of `wave` batches, problems in order within a pair (wave a problem 0, wave b problem 0,
+// wave a problem 1, ...), so a wave's operands stay in L2 across its products and one
+// wave's tiles fill the wait for the other's.  A tile of problem p > 0 waits until
+// dep[z] >= p * dep_per (every tile of problem p - 1 of batch z has published: each
+// epilogue warp adds 1 per tile, so dep_per = tiles per batch x epilogue warps).  split[p] selects split or plain operands per
+// problem within the split-capacity ring: a plain tile puts two consecutive K slabs in
+// each stage (parts 0 and 1), so its MMAs run in the same K order as the plain ring's.
 template <class Epi, int NP>
 struct PJob {
   Maps maps[NP];
@@ -526,6 +537,10 @@ struct PJob {
   int K[NP], m_step[NP], n_step[NP], a_batched[NP], b_batched[NP], k_split[NP], bn[NP];
   int tile0[NP + 1];
   int np;
+  // chain launches only
+  int split[NP];
+  unsigned* dep;
+  int dep_per, wave, nbatch;
   // tile t -> problem p and its (batch z, M tile, N tile)
   AFQ_D void locate(int t, int& p, int& z, int& mt, int& nt) const {
     p = 0;
@@ -535,15 +550,70 @@ struct PJob {
     }
     sched[p].decode(t, z, mt, nt);
   }
+  // chain order: pairs of waves, problems in order within a pair
+  AFQ_D void locate_chain(int t, int& p, int& z, int& mt, int& nt) const {
+    const int per = sched[0].m_tiles * sched[0].n_tiles;
+    const int nfull = nbatch / wave, rem = nbatch - nfull * wave;
+    const int fpairs = nfull / 2;                      // pairs of two full waves
+    const int tp = np * 2 * wave * per;                // tiles of a full pair
+    int w0, za, zb;                                    // first wave, batches of waves a, b
+    if (t < fpairs * tp) {
+      const int q = t / tp;
+      t -= q * tp;
+      w0 = 2 * q;
+      za = zb = wave;
+    } else {
+      t -= fpairs * tp;
+      w0 = 2 * fpairs;
+      const bool a_full = w0 < nfull;
+      za = a_full ? wave : rem;
+      zb = a_full ? (w0 + 1 < nfull ? wave : rem) : 0;
+    }
+    const int pp = (za + zb) * per;                    // tiles of one problem in the pair
+    p = t / pp;
+    int r = t - p * pp;
+    int which = 0;
+    if (r >= za * per) {
+      r -= za * per;
+      which = 1;
+    }
+    const int zl = r / per, ti = r - zl * per;
+    z = (w0 + which) * wave + zl;
+    const TileSched& sc = sched[p];
+    if (sc.m_fast) {
+      mt = ti % sc.m_tiles;
+      nt = ti / sc.m_tiles;
+    } else {
+      nt = ti % sc.n_tiles;
+      mt = ti / sc.n_tiles;
+    }
+  }
 };
 
+// Chain dependency counters: the epilogue publishes a finished tile with a release add,
+// the waiting producer reads with acquire and then orders its TMA reads (async proxy)
+// after the data it now sees (generic proxy).
+AFQ_D unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+AFQ_D void red_release_gpu_add(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+AFQ_D void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int EPI_WG, int SLAB = 128,
-          int NP = 1>
+          int NP = 1, bool CHAIN = false>
 __global__ void __launch_bounds__(128 * EPI_WG + 64, 1)
 tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
   using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
   using P = PCfg<BN, STAGES, FMT, SPLIT, Epi, EPI_WG, SLAB>;
   static_assert(!Epi::kTile, "tile epilogues reuse the operand ring: per-tile kernel only");
+  static_assert(!CHAIN || (SPLIT && EpiPromote<Epi>::value == 0),
+                "chain launches: split-capacity ring, no promotion");
   extern __shared__ __align__(1024) uint8_t tc_smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -583,6 +653,19 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const int total = job.tile0[job.np];
+  auto where = [&](int t, int& p, int& z, int& mt, int& nt) {
+    if constexpr (CHAIN)
+      job.locate_chain(t, p, z, mt, nt);
+    else
+      job.locate(t, p, z, mt, nt);
+  };
+  // split operands for problem p (chain launches choose per problem)
+  auto split_of = [&](int p) {
+    if constexpr (CHAIN) return job.split[p] != 0;
+    else return SPLIT;
+  };
+  // stage fills of a tile: one K slab per stage, or two when a chain tile is plain
+  auto fills = [&](int nk, bool sp) { return (CHAIN && !sp) ? (nk + 1) / 2 : nk; };
   // one problem: the epilogue functor as a local copy, so the compiler knows the
   // epilogue's global stores cannot change it (a reference into the parameter block makes
   // it reload the fields after every store); several problems, and the staged functors
@@ -602,22 +685,52 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
       int p, z, mt, nt, kbase;
-      job.locate(t, p, z, mt, nt);
+      where(t, p, z, mt, nt);
       const int nk = kslabs(p, z, kbase);
       const int za = (job.a_batched[p] && !job.k_split[p]) ? z : 0;
       const int zb = (job.b_batched[p] && !job.k_split[p]) ? z : 0;
       const int m0 = mt * job.m_step[p], n0 = nt * job.n_step[p];
       const Maps& maps = job.maps[p];
-      const uint32_t stage_bytes = C::PARTS * (C::A_BYTES + (uint32_t)job.bn[p] * SLAB);
-      for (int kb = 0; kb < nk; kb++, g++) {
+      const bool sp = split_of(p);
+      const uint32_t part_bytes = C::A_BYTES + (uint32_t)job.bn[p] * SLAB;
+      if constexpr (CHAIN) {
+        if (p > 0) {   // every tile of problem p - 1 of batch z has published
+          const unsigned target = (unsigned)(p * job.dep_per);
+          const long long t0 = clock64();
+          while (ld_acquire_gpu(job.dep + z) < target) {
+            if (clock64() - t0 > g_tc_wait_clocks) {
+              ok = false;
+              break;
+            }
+          }
+          if (!ok) {
+            atomicOr(err, ERR_TIMEOUT_PRODUCER);
+            break;
+          }
+          fence_proxy_async_global();
+        }
+      }
+      const int nf = fills(nk, sp);
+      for (int f = 0; f < nf; f++, g++) {
         const int s = g % STAGES;
         if (!mbar_wait(&empty[s], ((g / STAGES) & 1) ^ 1)) {
           atomicOr(err, ERR_TIMEOUT_PRODUCER);
           ok = false;
           break;
         }
-        const int kx = kbase + kb * C::BK;
-        mbar_expect_tx(&full[s], stage_bytes);
+        if (CHAIN && !sp) {   // plain chain tile: K slabs 2f and 2f + 1 in parts 0 and 1
+          const int kb = 2 * f, two = kb + 1 < nk;
+          mbar_expect_tx(&full[s], part_bytes * (two ? 2u : 1u));
+          tma_load_3d(stA(s, 0), &maps.a, &full[s], kbase + kb * C::BK, m0, za);
+          tma_load_3d(stB(s, 0), &maps.b, &full[s], kbase + kb * C::BK, n0, zb);
+          if (two) {
+            tma_load_3d(stA(s, 1), &maps.a, &full[s], kbase + (kb + 1) * C::BK, m0, za);
+            tma_load_3d(stB(s, 1), &maps.b, &full[s], kbase + (kb + 1) * C::BK, n0, zb);
+          }
+          continue;
+        }
+        const int kx = kbase + f * C::BK;
+        mbar_expect_tx(&full[s], C::PARTS * part_bytes);
         tma_load_3d(stA(s, 0), &maps.a, &full[s], kx, m0, za);
         tma_load_3d(stB(s, 0), &maps.b, &full[s], kx, n0, zb);
         if (SPLIT) {
@@ -635,10 +748,44 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
     bool ok = true;
     for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
       int p, z, mt, nt, kbase;
-      job.locate(t, p, z, mt, nt);
+      where(t, p, z, mt, nt);
       const int nk = kslabs(p, z, kbase);
       const uint32_t ID = idesc(128, job.bn[p], FMT);
       const int nch = PK ? (nk + PK - 1) / PK : 1;
+      const bool sp = split_of(p);
+      if (CHAIN && !sp) {   // plain chain tile: two K slabs per stage, one accumulator
+        const int b = li & 1;
+        if (!mbar_wait(&acce[b], ((li >> 1) & 1) ^ 1)) {
+          atomicOr(err, ERR_TIMEOUT_MMA);
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem + b * C::TMEM_COLS;
+        const int nf = fills(nk, sp);
+        for (int f = 0; f < nf; f++, g++) {
+          const int s = g % STAGES;
+          if (!mbar_wait(&full[s], (g / STAGES) & 1)) {
+            atomicOr(err, ERR_TIMEOUT_MMA);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const int nparts = 2 * f + 1 < nk ? 2 : 1;
+          for (int part = 0; part < nparts; part++) {
+            const uint64_t ad = sdesc_k<SLAB>(smem_u32(stA(s, part)));
+            const uint64_t bd = sdesc_k<SLAB>(smem_u32(stB(s, part)));
+#pragma unroll
+            for (int k = 0; k < C::BK / C::UK; k++)
+              umma<FMT>(d, ad + 2 * k, bd + 2 * k, ID, (f != 0 || part != 0 || k != 0) ? 1u : 0u);
+          }
+          umma_commit(&empty[s]);
+        }
+        if (!ok) break;
+        umma_commit(&accf[b]);
+        li++;
+        continue;
+      }
       for (int ch = 0; ch < nch && ok; ch++, li++) {
         const int b = li & 1;
         if (!mbar_wait(&acce[b], ((li >> 1) & 1) ^ 1)) {   // the epilogue released buffer b
@@ -735,15 +882,21 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
     int li = 0;
     for (int t = blockIdx.x; t < total; t += gridDim.x, li++) {
       int p, z, mt, nt;
-      job.locate(t, p, z, mt, nt);
+      where(t, p, z, mt, nt);
       EpiHold epi = job.epi[p];
       const int bn = job.bn[p];
       const int b = li & 1;
-      if (!mbar_wait(&accf[b], (li >> 1) & 1)) {
+      bool got = mbar_wait(&accf[b], (li >> 1) & 1);
+      // chain launches publish per warp: the warp decides as one whether to go on
+      if constexpr (CHAIN) got = __all_sync(0xffffffffu, got);
+      if (!got) {
         if (lane == 0) atomicOr(err, ERR_TIMEOUT_EPILOGUE);
         break;
       }
       tc_fence_after();
+      if constexpr (CHAIN) {   // see what problem p - 1 published before reading its output
+        if (p > 0) (void)ld_acquire_gpu(job.dep + z);
+      }
       const uint32_t trow = tmem + b * C::TMEM_COLS + ((uint32_t)(wq * 32) << 16);
       const int m0 = mt * job.m_step[p], n0 = nt * job.n_step[p];
       float v[32];
@@ -769,6 +922,11 @@ tc_gemm_persistent_kernel(const __grid_constant__ PJob<Epi, NP> job, int* err) {
       }
       tc_fence_before();
       mbar_arrive(&acce[b]);
+      if constexpr (CHAIN) {   // publish: this warp's writes of the tile are done
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) red_release_gpu_add(job.dep + z, 1u);
+      }
     }
   }
   tc_fence_before();
@@ -911,6 +1069,51 @@ cudaError_t launch_persistent(const Maps& maps, const GemmShape& g, const Epi& e
   const int grid = total < sm_count() ? total : sm_count();
   kern<<<grid, P::THREADS, P::SMEM, st>>>(job, err);
   return cudaGetLastError();
+}
+
+// Chain launch: the persistent kernel over a dependency-ordered tile list (PJob chain
+// fields).  Its CTAs wait on one another's tiles, so the launch is cooperative: every CTA
+// is resident at once (one per SM at most), and no CTA waits on one that has not started.
+// Every problem: the same batch count and tiles per batch; job.dep zeroed by the caller
+// (nbatch counters) before the launch.
+template <int BN, int STAGES, int FMT, class Epi, int EPI_WG, int NP>
+cudaError_t launch_chain(PJob<Epi, NP>& job, int* err, cudaStream_t st) {
+  using P = PCfg<BN, STAGES, FMT, true, Epi, EPI_WG>;
+  static_assert(P::kFits, "persistent configuration exceeds shared memory or TMEM");
+  if (job.np < 1 || job.np > NP || job.wave < 1 || job.nbatch < 1 || !job.dep)
+    return cudaErrorInvalidValue;
+  const int per = job.sched[0].m_tiles * job.sched[0].n_tiles;
+  for (int p = 0; p < job.np; p++)
+    if (job.bn[p] < 32 || job.bn[p] > BN || job.bn[p] % 32 || job.K[p] < 1 || job.k_split[p] ||
+        job.sched[p].m_tiles * job.sched[p].n_tiles != per || job.sched[p].nbatch != job.nbatch ||
+        job.sched[p].z0 != 0)
+      return cudaErrorInvalidValue;
+  job.dep_per = per * 4 * EPI_WG;   // one publish per epilogue warp per tile
+  job.tile0[0] = 0;
+  job.tile0[job.np] = job.np * job.nbatch * per;
+  const int total = job.tile0[job.np];
+  auto kern = tc_gemm_persistent_kernel<BN, STAGES, FMT, true, Epi, EPI_WG, 128, NP, true>;
+  static DeviceAttr attr;
+  cudaError_t e = attr.ensure(P::SMEM, [kern](size_t b) {
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  });
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::THREADS, P::SMEM);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = total < sm_count() ? total : sm_count();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(P::THREADS);
+  cfg.dynamicSmemBytes = P::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, (const PJob<Epi, NP>)job, err);
 }
 
 // The persistent kernel over job.np <= NP problems (no promoting epilogue): tile0 and the

@@ -198,3 +198,30 @@ def test_staged_propagation_epilogue_matches_tile_epilogue(monkeypatch):
     a, b = res["1"], res["2"]
     assert a["tuning"]["propagate"]["kernel"] == 1 and b["tuning"]["propagate"]["kernel"] == 2
     assert rel(a["W"], b["W"]) < 1e-12
+
+
+@pytest.mark.parametrize("wave", ["24", "16"])
+def test_fused_propagation_chain_matches_eight_launches(wave, monkeypatch):
+    """The propagation chain as one cooperative persistent launch (walker waves, per-walker
+    dependency counters, plain products two K slabs per stage) runs the same tiles, MMA
+    order and epilogue arithmetic as the eight launches: walkers bit for bit through graph
+    substeps with a re-orthogonalisation.  80 walkers in waves of 24 (two full pairs'
+    worth of waves and a partial wave of 8) or 16 (five full waves)."""
+    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
+    monkeypatch.setenv("AFQ_TUNE", "1")
+    monkeypatch.setenv("AFQ_SPLITK", "2")
+    s = system("C2", with_vakbl=False)
+    nw = 80
+    wk = walkers(s, nw, seed=8)
+    out = {}
+    for ch in ("0", wave):
+        monkeypatch.setenv("AFQ_PROP_CHAIN", ch)
+        e = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=wk, use_vakbl=False)
+        assert e.tuning()["propagate_chain"]["wave"] == int(ch)
+        e.calculate_mixed_density_matrix()
+        for st in range(6):
+            e.substep(9, st, 5, graph=True)
+        out[ch] = e.get_walkers()
+        e.close()
+    assert np.array_equal(out["0"][0], out[wave][0])
+    assert np.array_equal(out["0"][1], out[wave][1])
