@@ -1170,7 +1170,7 @@ struct EpiChain {
   int pack;
   EpiPropPair pr;
   EpiPropPack pk;
-  AFQ_D int pair_stride() const { return pr.n2; }
+  AFQ_D int pair_stride() const { return pack ? pk.n2 : pr.n2; }
   AFQ_D void pair(int w, int r, int i, int j0, const float* cr, const float* ci) const {
     if (pack) {
       const EpiPropPack e = pk;
