@@ -286,9 +286,9 @@ afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
  *   launch whose tiles run in pairs of walker waves, product by product, a tile starting
  *   once every tile of the previous product of its walker is done, so a wave's V, Taylor
  *   sum and operands stay in L2 across the eight products.  Same values.  Timed -> ms[8]
- *   (eight launches), ms[9..11] (waves of 16, 24, 32).  AFQ_PROP_CHAIN=0 keeps the eight
- *   launches, =<walkers> forces a wave.
- * ms[12] may be NULL; 0 where not timed. */
+ *   (eight launches), ms[9..13] (waves of 16, 24, 32, 48, 64).  AFQ_PROP_CHAIN=0 keeps
+ *   the eight launches, =<walkers> forces a wave.
+ * ms[14] may be NULL; 0 where not timed. */
 afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */

@@ -331,7 +331,7 @@ class AfqmcSys:
                for i, k in enumerate(self.TUNE_SITES)}
         out["splitk_slices"] = int(c[ns])
         sc = np.zeros(3, np.int32)
-        gm = np.zeros(12)
+        gm = np.zeros(14)
         self._check(self.lib.afq_get_schedule(self.h, _p(sc), _p(gm)))
         out["propagate_walker_group"] = {"walkers": int(sc[0]),
                                          "ms_all_32_48_64_96_128": [round(float(x), 4)
@@ -339,8 +339,8 @@ class AfqmcSys:
         out["vhs_epilogue"] = {"tile": int(sc[1]),
                                "ms_rowwise_tile": [round(float(x), 4) for x in gm[6:8]]}
         out["propagate_chain"] = {"wave": int(sc[2]),
-                                  "ms_launches_16_24_32": [round(float(x), 4)
-                                                           for x in gm[8:12]]}
+                                  "ms_launches_16_24_32_48_64": [round(float(x), 4)
+                                                                 for x in gm[8:14]]}
         return out
 
     SPARSE_OPERANDS = ["Spvn", "SpvnT", "Vakbl"]

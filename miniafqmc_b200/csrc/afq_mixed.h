@@ -68,8 +68,8 @@ int mixed_prop_group(const MixedState* m, float* ms);
 // Symmetric vHS epilogue picked at set-up (0 row-wise, 1 through the shared-memory tile)
 // and, in ms[2], the timed product for each (0 when not timed).
 int mixed_vhs_epilogue(const MixedState* m, float* ms);
-// Walkers per wave of the fused propagation chain (0: eight launches) and, in ms[4], the
-// timed chain: eight launches, waves of 16, 24 and 32 walkers (0 when not timed).
+// Walkers per wave of the fused propagation chain (0: eight launches) and, in ms[6], the
+// timed chain: eight launches, waves of 16, 24, 32, 48 and 64 walkers (0 when not timed).
 int mixed_prop_chain(const MixedState* m, float* ms);
 void mixed_tuning(const MixedState* m, int* choice, float* ms);
 // Heterogeneous batches: the vHS product and the propagation chain of n systems (n <= 4),

@@ -165,7 +165,7 @@ struct MixedState {
   // the set-up tuner (chain_ms: eight launches, waves of 16, 24 and 32 walkers)
   unsigned* dep = nullptr;
   int chain_wave = 0;
-  float chain_ms[4] = {};
+  float chain_ms[6] = {};
   int splits0 = 1, part_cap = 1;
 };
 
@@ -2412,7 +2412,7 @@ struct TuneRec {
   int vhs_epi;
   float vhs_epi_ms[2];
   int chain_wave;
-  float chain_ms[4];
+  float chain_ms[6];
   int splits;
   int prop_group;
 };
@@ -2449,7 +2449,7 @@ void tune_load(const char* path) {
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.group_ms[i]) == 1;
     if (ok) ok = fscanf(f, "%d %f %f", &r.vhs_epi, &r.vhs_epi_ms[0], &r.vhs_epi_ms[1]) == 3;
     if (ok) ok = fscanf(f, "%d", &r.chain_wave) == 1;
-    for (int i = 0; i < 4 && ok; i++) ok = fscanf(f, "%f", &r.chain_ms[i]) == 1;
+    for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.chain_ms[i]) == 1;
     if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
     tune_cache()[key] = r;
     tune_file_keys().insert(key);
@@ -2464,8 +2464,8 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.group_ms[i]);
   fprintf(f, " %d %.5f %.5f", r.vhs_epi, r.vhs_epi_ms[0], r.vhs_epi_ms[1]);
-  fprintf(f, " %d %.5f %.5f %.5f %.5f", r.chain_wave, r.chain_ms[0], r.chain_ms[1],
-          r.chain_ms[2], r.chain_ms[3]);
+  fprintf(f, " %d", r.chain_wave);
+  for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.chain_ms[i]);
   fprintf(f, " %d %d\n", r.splits, r.prop_group);
   fclose(f);
 }
@@ -2512,7 +2512,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       m->vhs_epi_ms[0] = r.vhs_epi_ms[0];
       m->vhs_epi_ms[1] = r.vhs_epi_ms[1];
       m->chain_wave = m->dep ? r.chain_wave : 0;
-      for (int i = 0; i < 4; i++) m->chain_ms[i] = r.chain_ms[i];
+      for (int i = 0; i < 6; i++) m->chain_ms[i] = r.chain_ms[i];
       tune_save(cache_path, key, r);   // a shape timed before the file was named
       return cudaSuccess;
     }
@@ -2646,17 +2646,17 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       }
     }
     m->prop_group = best;
-    // then the whole chain as one cooperative launch (waves of 16, 24 or 32 walkers)
+    // then the whole chain as one cooperative launch (waves of 16, 24, 32, 48 or 64 walkers)
     // against the eight launches of the chosen kernel over all walkers; AFQ_PROP_CHAIN=0
     // keeps the eight launches, =<walkers> forces a wave
     const char* fc = getenv("AFQ_PROP_CHAIN");
     const int fcw = fc ? atoi(fc) : -1;
     if (m->dep && m->prop_group == 0 && m->tune[TS_PROP] && fcw != 0) {
       m->chain_ms[0] = m->prop_group_ms[0];
-      const int waves[3] = {16, 24, 32};
+      const int waves[5] = {16, 24, 32, 48, 64};
       int bw = 0;
       float bwt = m->chain_ms[0] > 0.0f && fcw < 0 ? m->chain_ms[0] : 0.0f;
-      for (int c = 0; c < 3; c++) {
+      for (int c = 0; c < 5; c++) {
         if (fcw > 0 && waves[c] != fcw) continue;
         const float t = timed([&] { return propagate_chain(m, nullptr, waves[c], true, st); });
         m->chain_ms[c + 1] = t > 0.0f ? t : 0.0f;
@@ -2734,7 +2734,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     r.vhs_epi_ms[0] = m->vhs_epi_ms[0];
     r.vhs_epi_ms[1] = m->vhs_epi_ms[1];
     r.chain_wave = m->chain_wave;
-    for (int i = 0; i < 4; i++) r.chain_ms[i] = m->chain_ms[i];
+    for (int i = 0; i < 6; i++) r.chain_ms[i] = m->chain_ms[i];
     std::lock_guard<std::mutex> lk(tune_mu);
     tune_cache()[key] = r;
     tune_save(cache_path, key, r);
@@ -2753,7 +2753,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
 
 int mixed_prop_chain(const MixedState* m, float* ms) {
   if (ms)
-    for (int i = 0; i < 4; i++) ms[i] = m ? m->chain_ms[i] : 0.0f;
+    for (int i = 0; i < 6; i++) ms[i] = m ? m->chain_ms[i] : 0.0f;
   return m ? m->chain_wave : 0;
 }
 
