@@ -662,132 +662,10 @@ lu_smem_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ 
   }
 }
 
-// The same Gauss-Jordan with one warp per matrix (a 32-thread CTA): the pivot search,
-// the scaled pivot row and the row updates are warp-synchronous, so no CTA barrier sits
-// in the 2n dependent pivot steps; the matrix lives in shared memory (n (n + 1) complex:
-// six 48 x 48 matrices per SM).  Same pivots (first maximum of |re| + |im| over the
-// unused rows) and the same operations per element as lu_smem_kernel: the same results.
-__global__ void __launch_bounds__(32)
-lu_warp_kernel(const float2* __restrict__ T1, int n, Op Tinv, z_t* __restrict__ Wd,
-               int* __restrict__ info, int want_inv, int save_old) {
-  extern __shared__ __align__(16) unsigned char luw_raw[];
-  __shared__ int pivrow[64], invp[64], used[64];
-  const int q = blockIdx.x, lane = threadIdx.x;
-  const int ld = n + 1, nn = n * n;
-  z_t* T = reinterpret_cast<z_t*>(luw_raw);
-  const float2* src = T1 + (long long)q * nn;
-  for (int e = lane; e < nn; e += 32) {
-    const float2 v = src[e];
-    T[(e / n) * ld + e % n] = zmk(v.x, v.y);
-  }
-  for (int i = lane; i < 64; i += 32) used[i] = 0;
-  __syncwarp();
-  z_t det = zmk(1.0, 0.0);
-  int sing = 0;
-  const bool c0 = lane < n, c1 = lane + 32 < n;
-  for (int j = 0; j < n; j++) {
-    // pivot: max |re| + |im| of column j over the unused rows, first one on ties
-    double best = -1.0;
-    int bi = n;
-    for (int i = lane; i < n; i += 32) {
-      if (used[i]) continue;
-      const double v = zabs1(T[i * ld + j]);
-      if (v > best) { best = v; bi = i; }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-    }
-    if (!(best > 0.0)) {   // uniform across the warp
-      sing = 1;
-      break;
-    }
-    const int p = bi;
-    const z_t pv = T[p * ld + j];
-    det = zmul(det, pv);
-    // the scaled pivot row (column j holds the reciprocal), kept in registers
-    const z_t inv = zrecip(pv);
-    const z_t pr0 = c0 ? ((lane == j) ? inv : zmul(T[p * ld + lane], inv)) : zmk(0, 0);
-    const z_t pr1 = c1 ? ((lane + 32 == j) ? inv : zmul(T[p * ld + lane + 32], inv)) : zmk(0, 0);
-    __syncwarp();
-    if (lane == 0) {
-      used[p] = 1;
-      pivrow[j] = p;
-    }
-    if (c0) T[p * ld + lane] = pr0;
-    if (c1) T[p * ld + lane + 32] = pr1;
-    // every other row: its factor is its own column-j entry, read before lane j writes it
-#pragma unroll 4
-    for (int i = 0; i < n; i++) {
-      if (i == p) continue;
-      z_t* Ti = T + i * ld;
-      const z_t f = Ti[j];
-      const z_t b0 = (c0 && lane != j) ? Ti[lane] : zmk(0, 0);
-      const z_t b1 = (c1 && lane + 32 != j) ? Ti[lane + 32] : zmk(0, 0);
-      __syncwarp();
-      if (c0)
-        Ti[lane] = zmk(fma(-f.x, pr0.x, fma(f.y, pr0.y, b0.x)), fma(-f.x, pr0.y, fma(-f.y, pr0.x, b0.y)));
-      if (c1)
-        Ti[lane + 32] =
-            zmk(fma(-f.x, pr1.x, fma(f.y, pr1.y, b1.x)), fma(-f.x, pr1.y, fma(-f.y, pr1.x, b1.y)));
-    }
-    __syncwarp();
-  }
-  if (sing) det = zmk(0, 0);
-  if (!sing) {   // sign of the row permutation; its inverse
-    int inv_cnt = 0;
-    for (int a = lane; a < n; a += 32)
-      for (int b = a + 1; b < n; b++) inv_cnt += pivrow[a] > pivrow[b];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) inv_cnt += __shfl_xor_sync(0xffffffffu, inv_cnt, o);
-    if (inv_cnt & 1) det = zmk(-det.x, -det.y);
-    for (int a = lane; a < n; a += 32) invp[pivrow[a]] = a;
-  }
-  __syncwarp();
-  if (want_inv) {
-    const long long base = (long long)q * 2 * n * 2 * n;
-    for (int e = lane; e < nn; e += 32) {
-      const int i = e / n, c = e % n;
-      const int ra = sing ? i : invp[i], cb = sing ? c : pivrow[c];
-      const z_t y = sing ? zmk(0, 0) : T[i * ld + c];
-      put2(Tinv, base + (2LL * ra) * 2 * n + 2 * cb, (float)y.x, (float)-y.y);
-      put2(Tinv, base + (2LL * ra + 1) * 2 * n + 2 * cb, (float)y.y, (float)y.x);
-    }
-  }
-  if (lane == 0) {
-    const int w = q >> 1, sp = q & 1;
-    z_t* d = Wd + (long long)w * 8;
-    if (save_old) {
-      if (sp == 0) d[5] = d[4];
-      d[6 + sp] = d[2 + sp];
-    }
-    d[2 + sp] = det;
-    info[q] = sing;
-  }
-}
-
 cudaError_t launch_lu(const float2* T1, int n, int nmat, Op Tinv, z_t* Wd, int* info, int want_inv,
                       int save_old, cudaStream_t st) {
   static const bool regs = getenv("AFQ_LU_REGISTERS") != nullptr;
-  const char* lk = getenv("AFQ_LU_KERNEL");   // "smem": four warps per matrix
-  if (!regs && n <= 64 && !(lk && std::string(lk) == "smem")) {   // one warp per matrix (default)
-    const size_t smem = sizeof(z_t) * (size_t)n * (n + 1);
-    static DeviceAttr attr;
-    cudaError_t e = attr.ensure(smem, [](size_t b) {
-      cudaError_t r = cudaFuncSetAttribute(lu_warp_kernel,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
-      if (r == cudaSuccess)
-        r = cudaFuncSetAttribute(lu_warp_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
-      return r;
-    });
-    if (e != cudaSuccess) return e;
-    lu_warp_kernel<<<nmat, 32, smem, st>>>(T1, n, Tinv, Wd, info, want_inv, save_old);
-    return cudaGetLastError();
-  }
-  if (!regs && n <= 64) {   // shared-memory form, four warps per matrix
+  if (!regs && n <= 64) {   // shared-memory form (default)
     const size_t smem = lus_smem_bytes(n);
     static DeviceAttr attr;   // and the full shared-memory carveout: five matrices per SM
     cudaError_t e = attr.ensure(smem, [](size_t b) {

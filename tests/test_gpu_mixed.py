@@ -268,28 +268,3 @@ def test_vhs_tile_epilogue_matches_rowwise(monkeypatch):
         m.close()
     assert np.array_equal(out["0"], out["1"])
 
-
-def test_warp_gauss_jordan_matches_shared_memory_one(monkeypatch):
-    """The one-warp-per-matrix Gauss-Jordan (default) and the four-warp shared-memory one
-    (AFQ_LU_KERNEL=smem) pick the same pivots and do the same operations per element: the
-    same overlaps, density matrices and walkers bit for bit through graph substeps with a
-    re-orthogonalisation.  C1 (n = 16) and C2 (n = 32)."""
-    from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_MIXED
-    for name, nw in (("C1", 16), ("C2", 40)):
-        s = system(name, with_vakbl=False)
-        wk = perturbed(s, nw, seed=5)
-        out = {}
-        for lk in ("smem", "warp"):
-            monkeypatch.setenv("AFQ_LU_KERNEL", lk)
-            m = AfqmcSys(s, nw, precision=AFQ_PREC_MIXED, walkers=wk, use_vakbl=False)
-            m.calculate_mixed_density_matrix()
-            gc = m.copy_out("Gc")
-            for st in range(6):
-                m.substep(4, st, 5, graph=True)
-            m.calculate_mixed_density_matrix()
-            out[lk] = (gc, m.get_walkers(), m.copy_out("Gc"))
-            m.close()
-        a, b = out["smem"], out["warp"]
-        assert np.array_equal(a[0], b[0]), name
-        assert np.array_equal(a[1][0], b[1][0]) and np.array_equal(a[1][1], b[1][1]), name
-        assert np.array_equal(a[2], b[2]), name
