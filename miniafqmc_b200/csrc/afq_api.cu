@@ -1490,7 +1490,8 @@ cudaError_t batch_substep_fused(afq_batch* b, bool ortho) {
   };
   auto fork = [&]() {
     cudaError_t r = cudaEventRecord(b->fork, b->st);
-    for (int i = 0; i < n && r == cudaSuccess; i++) r = cudaStreamWaitEvent(b->hs[i]->st, b->fork, 0);
+    for (int i = 0; i < n && r == cudaSuccess; i++)
+      r = cudaStreamWaitEvent(b->hs[i]->st, b->fork, 0);
     return r;
   };
   cudaError_t e;

@@ -2086,7 +2086,8 @@ bool mixed_multi_compatible(MixedState* const* ms, int n) {
     const MixedState* m = ms[i];
     const MixedState* a = ms[0];
     if (!m || m->prec_vhs != a->prec_vhs || m->prec_p != a->prec_p || m->prec_v1 != a->prec_v1 ||
-        m->prec_vk != a->prec_vk || m->in.order != a->in.order || m->bn_prop < 32 || m->bn_prop > 256 || 4 * m->n > m->bn_prop)
+        m->prec_vk != a->prec_vk || m->in.order != a->in.order || m->bn_prop < 32 ||
+        m->bn_prop > 256 || 4 * m->n > m->bn_prop)
       return false;
     for (int p : {m->prec_vhs, m->prec_p, m->prec_v1, m->prec_vk})
       if (p != PREC_SPLIT && p != PREC_BF16) return false;

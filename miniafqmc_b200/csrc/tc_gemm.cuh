@@ -281,9 +281,10 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
 //   MINB = CTAs per SM the launch is compiled for (2 caps registers at 170 per thread so a
 //   lean ring's CTAs pair up on an SM).
-// The body of the per-tile kernels: one 128 x bn output tile (bn <= BN, a multiple of 16;
-// the B tensor map's box holds bn rows) of batch `batch`, K range [kbase, kbase + klen),
-// operand batches za / zb.  The shared-memory ring is laid out for BN.
+// The body of the per-tile kernels: one 128 x bn output tile (bn <= BN, a multiple of 32:
+// the epilogues take 32-column chunks; the B tensor map's box holds bn rows) of batch
+// `batch`, K range [kbase, kbase + klen), operand batches za / zb.  The shared-memory ring
+// is laid out for BN.
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int SLAB>
 AFQ_D void gemm_tile(const Maps& maps, int mt, int nt, int m0, int n0, int batch, int za,
                      int zb, int kbase, int klen, int bn, const Epi epi, int* err) {
@@ -526,9 +527,10 @@ struct PCfg {
 // wave a problem 1, ...), so a wave's operands stay in L2 across its products and one
 // wave's tiles fill the wait for the other's.  A tile of problem p > 0 waits until
 // dep[z] >= p * dep_per (every tile of problem p - 1 of batch z has published: each
-// epilogue warp adds 1 per tile, so dep_per = tiles per batch x epilogue warps).  split[p] selects split or plain operands per
-// problem within the split-capacity ring: a plain tile puts two consecutive K slabs in
-// each stage (parts 0 and 1), so its MMAs run in the same K order as the plain ring's.
+// epilogue warp adds 1 per tile, so dep_per = tiles per batch x epilogue warps).
+// split[p] selects split or plain operands per problem within the split-capacity ring: a
+// plain tile puts two consecutive K slabs in each stage (parts 0 and 1), so its MMAs run
+// in the same K order as the plain ring's.
 template <class Epi, int NP>
 struct PJob {
   Maps maps[NP];
