@@ -146,9 +146,10 @@ struct MixedState {
   Op F2;
   tc::Maps m_pw2, m_t1_1;
   // symmetric vHS epilogue: 0 row-wise (EpiVhsSym, the tuned kernel), 1 through the
-  // shared-memory tile (EpiVhsSymTile, per-tile kernel); picked by the set-up tuner
+  // shared-memory tile (EpiVhsSymTile, per-tile kernel), 2 the same with two CTAs per SM
+  // (one stage each, the tile staged in halves); picked by the set-up tuner
   int vhs_epi = 0;
-  float vhs_epi_ms[2] = {};
+  float vhs_epi_ms[3] = {};
   bool packed = false;
   int fa_buf = 0;
   // kernel of each product site (0 built-in rule, 1 persistent, 2 per-tile), chosen at
@@ -867,7 +868,7 @@ struct EpiVhsSym {
 // halves leave as contiguous 64-byte rows instead of the row-wise functor's
 // one-lane-per-walker 4-byte mirror stores.  Needs N % 4 == 0 (16-byte aligned rows).
 struct EpiVhsSymTile {
-  static constexpr bool kTile = true, kPair = false;
+  static constexpr bool kTile = true, kPair = false, kHalfTile = true;
   Op V;
   int nw, N;
   const int* pairs;
@@ -882,16 +883,38 @@ struct EpiVhsSymTile {
     *reinterpret_cast<uint4*>(o.hi + idx) = *reinterpret_cast<const uint4*>(h);
     if (o.lo) *reinterpret_cast<uint4*>(o.lo + idx) = *reinterpret_cast<const uint4*>(l);
   }
-  AFQ_D void tile(int, int mt, int nt, const float* t, int ld, int tid) const {
+  AFQ_D void tile(int b, int mt, int nt, const float* t, int ld, int tid) const {
+    tile_part(b, mt, nt, t, ld, tid, 0, 256);
+  }
+  // the tile's columns [c_first, c_first + c_count) (whole block rows ii; c_count 128 or
+  // 256) staged in t: block rows ii of the direct half, quarters of the mirrored half
+  AFQ_D void tile_part(int, int mt, int nt, const float* t, int ld, int tid, int c_first,
+                       int c_count) const {
     int tt = nt, ib = 0;   // tile -> block pair (ib, jb), ib <= jb, in row order
     const int nb = N >> 4;
     while (tt >= nb - ib) { tt -= nb - ib; ib++; }
     const int jb = ib + tt;
-    const int nmir = ib != jb ? 2 : 1;
-    // items: (mirror, walker, block row, quarter), quarter fastest
+    const int r0 = c_first >> 4, nr = c_count >> 4;   // block rows ii in [r0, r0 + nr)
+    const int q0 = r0 >> 2, nq = nr >> 2;            // their quarters of the mirrored rows
+    const int per = 64 * nr * 4;                      // items of each half
+    const int nitems = ib != jb ? 2 * per : per;
+    // items: (walker, block row, quarter) of the direct half, then (walker, column jj,
+    // quarter) of the mirrored half; quarter fastest, so four consecutive threads write
+    // one 64-byte row
 #pragma unroll 1
-    for (int it = tid; it < nmir * 64 * 16 * 4; it += 128) {
-      const int qt = it & 3, rr = (it >> 2) & 15, wl = (it >> 6) & 63, mir = it >> 12;
+    for (int it = tid; it < nitems; it += 128) {
+      const bool mir = it >= per;
+      const int k = mir ? it - per : it;
+      int wl, rr, qt;
+      if (!mir) {
+        qt = k & 3;
+        rr = r0 + (k >> 2) % nr;
+        wl = (k >> 2) / nr;
+      } else {
+        qt = q0 + k % nq;
+        rr = (k / nq) & 15;
+        wl = k / (nq * 16);
+      }
       const int w = mt * 64 + wl;
       if (w >= nw) continue;
       const float* tr = t + (2 * wl) * ld;
@@ -901,15 +924,15 @@ struct EpiVhsSymTile {
       if (!mir) {   // V[ib*16 + rr][jb*16 + 4 qt + e] = tile column rr*16 + 4 qt + e
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-          re[e] = tr[rr * 16 + 4 * qt + e];
-          im[e] = ti[rr * 16 + 4 * qt + e];
+          re[e] = tr[rr * 16 + 4 * qt + e - c_first];
+          im[e] = ti[rr * 16 + 4 * qt + e - c_first];
         }
         row = (long long)w * N * N + (long long)(ib * 16 + rr) * N + jb * 16 + 4 * qt;
       } else {      // V[jb*16 + rr][ib*16 + 4 qt + e] = tile column (4 qt + e)*16 + rr
 #pragma unroll
         for (int e = 0; e < 4; e++) {
-          re[e] = tr[(4 * qt + e) * 16 + rr];
-          im[e] = ti[(4 * qt + e) * 16 + rr];
+          re[e] = tr[(4 * qt + e) * 16 + rr - c_first];
+          im[e] = ti[(4 * qt + e) * 16 + rr - c_first];
         }
         row = (long long)w * N * N + (long long)(jb * 16 + rr) * N + ib * 16 + 4 * qt;
       }
@@ -1843,6 +1866,14 @@ static cudaError_t vhs_product(MixedState* m, cudaStream_t st) {
       EpiVhsSymTile epi{m->Vf, nw, N, m->pairs};
       return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, 2);
     }
+    if (m->vhs_epi == 2) {   // two CTAs per SM: one overlaps the other's epilogue
+      EpiVhsSymTile epi{m->Vf, nw, N, m->pairs};
+      if (m->prec_vhs == PREC_SPLIT)
+        return tc::launch<256, 1, 1, true, EpiVhsSymTile, 2>(m->m_vhs, g, epi, m->err, st);
+      if (m->prec_vhs == PREC_BF16)
+        return tc::launch<256, 2, 1, false, EpiVhsSymTile, 2>(m->m_vhs, g, epi, m->err, st);
+      return cudaErrorInvalidValue;
+    }
     EpiVhsSym epi{m->Vf, nw, N, m->pairs};
     return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, m->tune[TS_VHS]);
   }
@@ -2411,7 +2442,7 @@ struct TuneRec {
   float ms[TS_N][2];
   float group_ms[6];
   int vhs_epi;
-  float vhs_epi_ms[2];
+  float vhs_epi_ms[3];
   int chain_wave;
   float chain_ms[6];
   int splits;
@@ -2448,7 +2479,9 @@ void tune_load(const char* path) {
     for (int i = 0; i < TS_N && ok; i++)
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.group_ms[i]) == 1;
-    if (ok) ok = fscanf(f, "%d %f %f", &r.vhs_epi, &r.vhs_epi_ms[0], &r.vhs_epi_ms[1]) == 3;
+    if (ok)
+      ok = fscanf(f, "%d %f %f %f", &r.vhs_epi, &r.vhs_epi_ms[0], &r.vhs_epi_ms[1],
+                  &r.vhs_epi_ms[2]) == 4;
     if (ok) ok = fscanf(f, "%d", &r.chain_wave) == 1;
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.chain_ms[i]) == 1;
     if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
@@ -2464,7 +2497,8 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   fprintf(f, "%s", key.c_str());
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.group_ms[i]);
-  fprintf(f, " %d %.5f %.5f", r.vhs_epi, r.vhs_epi_ms[0], r.vhs_epi_ms[1]);
+  fprintf(f, " %d %.5f %.5f %.5f", r.vhs_epi, r.vhs_epi_ms[0], r.vhs_epi_ms[1],
+          r.vhs_epi_ms[2]);
   fprintf(f, " %d", r.chain_wave);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.chain_ms[i]);
   fprintf(f, " %d %d\n", r.splits, r.prop_group);
@@ -2510,8 +2544,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       m->prop_group = r.prop_group;
       for (int i = 0; i < 6; i++) m->prop_group_ms[i] = r.group_ms[i];
       m->vhs_epi = r.vhs_epi;
-      m->vhs_epi_ms[0] = r.vhs_epi_ms[0];
-      m->vhs_epi_ms[1] = r.vhs_epi_ms[1];
+      for (int v = 0; v < 3; v++) m->vhs_epi_ms[v] = r.vhs_epi_ms[v];
       m->chain_wave = m->dep ? r.chain_wave : 0;
       for (int i = 0; i < 6; i++) m->chain_ms[i] = r.chain_ms[i];
       tune_save(cache_path, key, r);   // a shape timed before the file was named
@@ -2594,16 +2627,17 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   // tile (full tuning only, so forced kernels stay comparable); AFQ_VHS_EPI=0|1 forces
   if (m->vsym && m->tune[TS_VHS] && force < 0) {
     const char* fe = getenv("AFQ_VHS_EPI");
-    float t[2] = {0.0f, 0.0f};
-    for (int v = 0; v < 2; v++) {
+    float t[3] = {0.0f, 0.0f, 0.0f};
+    int bv = 0;
+    for (int v = 0; v < 3; v++) {
       if (fe && atoi(fe) != v) continue;
       m->vhs_epi = v;
       const float ms = timed([&] { return vhs_product(m, st); });
       t[v] = ms > 0.0f ? ms : 0.0f;
+      if (t[v] > 0.0f && (t[bv] <= 0.0f || t[v] < t[bv])) bv = v;
     }
-    m->vhs_epi = (t[1] > 0.0f && (t[0] <= 0.0f || t[1] < t[0])) ? 1 : 0;
-    m->vhs_epi_ms[0] = t[0];
-    m->vhs_epi_ms[1] = t[1];
+    m->vhs_epi = bv;
+    for (int v = 0; v < 3; v++) m->vhs_epi_ms[v] = t[v];
   }
   {
     const int mt = (N + 127) / 128, n2 = 2 * n;
@@ -2732,8 +2766,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     r.prop_group = m->prop_group;
     for (int i = 0; i < 6; i++) r.group_ms[i] = m->prop_group_ms[i];
     r.vhs_epi = m->vhs_epi;
-    r.vhs_epi_ms[0] = m->vhs_epi_ms[0];
-    r.vhs_epi_ms[1] = m->vhs_epi_ms[1];
+    for (int v = 0; v < 3; v++) r.vhs_epi_ms[v] = m->vhs_epi_ms[v];
     r.chain_wave = m->chain_wave;
     for (int i = 0; i < 6; i++) r.chain_ms[i] = m->chain_ms[i];
     std::lock_guard<std::mutex> lk(tune_mu);
@@ -2760,7 +2793,7 @@ int mixed_prop_chain(const MixedState* m, float* ms) {
 
 int mixed_vhs_epilogue(const MixedState* m, float* ms) {
   if (ms)
-    for (int i = 0; i < 2; i++) ms[i] = m ? m->vhs_epi_ms[i] : 0.0f;
+    for (int i = 0; i < 3; i++) ms[i] = m ? m->vhs_epi_ms[i] : 0.0f;
   return m ? m->vhs_epi : 0;
 }
 

@@ -281,6 +281,16 @@ struct EpiScratch<E, std::void_t<decltype(E::kScratchBytes)>>
 //   epi.tile(batch, m_tile, n_tile, tile, ld, tid)  with tid in [0, 128).
 //   MINB = CTAs per SM the launch is compiled for (2 caps registers at 170 per thread so a
 //   lean ring's CTAs pair up on an SM).
+// Whether the fp32 tile of a tile epilogue (128 rows x BN + 1 floats) fits the operand
+// ring; kHalfTile functors also run with half the columns staged at a time.
+template <int BN, int STAGES, uint32_t STAGE_BYTES>
+struct TileInRing
+    : std::integral_constant<bool, (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * STAGE_BYTES> {};
+template <class E, class = void> struct EpiHalfTile : std::false_type {};
+template <class E>
+struct EpiHalfTile<E, std::void_t<decltype(E::kHalfTile)>>
+    : std::integral_constant<bool, E::kHalfTile> {};
+
 // The body of the per-tile kernels: one 128 x bn output tile (bn <= BN, a multiple of 32:
 // the epilogues take 32-column chunks; the B tensor map's box holds bn rows) of batch
 // `batch`, K range [kbase, kbase + klen), operand batches za / zb.  The shared-memory ring
@@ -404,16 +414,34 @@ AFQ_D void gemm_tile(const Maps& maps, int mt, int nt, int m0, int n0, int batch
           epi.pair(batch, row, m0 + row, c0, v, u);
         }
       } else if constexpr (Epi::kTile) {
-        // the operand ring is idle once `done` has fired: reuse it for the fp32 tile
+        // the operand ring is idle once `done` has fired: reuse it for the fp32 tile, or,
+        // when the ring cannot hold it (kHalfTile functors), for one half of the columns
+        // at a time through epi.tile_part(..., first column, columns)
         float* tile = reinterpret_cast<float*>(smem);
+        if constexpr (TileInRing<BN, STAGES, C::STAGE_BYTES>::value) {
 #pragma unroll 1
-        for (int c0 = 0; c0 < bn; c0 += 32) {
-          tmem_ld32(trow + c0, v);
+          for (int c0 = 0; c0 < bn; c0 += 32) {
+            tmem_ld32(trow + c0, v);
 #pragma unroll
-          for (int i = 0; i < 32; i++) tile[row * (BN + 1) + c0 + i] = v[i];
+            for (int i = 0; i < 32; i++) tile[row * (BN + 1) + c0 + i] = v[i];
+          }
+          epi_bar();
+          epi.tile(batch, mt, nt, tile, BN + 1, threadIdx.x);
+        } else {
+          constexpr int TC = BN / 2;
+#pragma unroll 1
+          for (int h = 0; h < 2; h++) {
+            if (h) epi_bar();   // every thread is done with the first half
+#pragma unroll 1
+            for (int c0 = 0; c0 < TC; c0 += 32) {
+              tmem_ld32(trow + h * TC + c0, v);
+#pragma unroll
+              for (int i = 0; i < 32; i++) tile[row * (TC + 1) + c0 + i] = v[i];
+            }
+            epi_bar();
+            epi.tile_part(batch, mt, nt, tile, TC + 1, threadIdx.x, h * TC, TC);
+          }
         }
-        epi_bar();
-        epi.tile(batch, mt, nt, tile, BN + 1, threadIdx.x);
       } else {
 #pragma unroll 1
         for (int c0 = 0; c0 < bn; c0 += 32) {
@@ -980,8 +1008,10 @@ template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int MINB = 1, int 
 cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* err,
                    cudaStream_t st) {
   using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
-  static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
-                "tile epilogue needs the operand ring to hold the fp32 tile");
+  static_assert(!Epi::kTile || TileInRing<BN, STAGES, C::STAGE_BYTES>::value ||
+                    (EpiHalfTile<Epi>::value && BN % 64 == 0 &&
+                     (size_t)128 * (BN / 2 + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES),
+                "tile epilogue needs the operand ring to hold the fp32 tile (or half of it)");
   static_assert(MINB * C::SMEM <= 228 * 1024 && MINB * C::TMEM_COLS <= 512,
                 "CTAs per SM exceed shared memory or TMEM");
   auto kern = tc_gemm_kernel<BN, STAGES, FMT, SPLIT, Epi, MINB, SLAB>;
@@ -1007,8 +1037,10 @@ cudaError_t launch(const Maps& maps, const GemmShape& g, const Epi& epi, int* er
 template <int BN, int STAGES, int FMT, bool SPLIT, class Epi, int NP, int SLAB = 128>
 cudaError_t launch_multi(const MultiJob<Epi, NP>& job, int* err, cudaStream_t st) {
   using C = Cfg<BN, STAGES, FMT, SPLIT, SLAB>;
-  static_assert(!Epi::kTile || (size_t)128 * (BN + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES,
-                "tile epilogue needs the operand ring to hold the fp32 tile");
+  static_assert(!Epi::kTile || TileInRing<BN, STAGES, C::STAGE_BYTES>::value ||
+                    (EpiHalfTile<Epi>::value && BN % 64 == 0 &&
+                     (size_t)128 * (BN / 2 + 1) * 4 <= (size_t)STAGES * C::STAGE_BYTES),
+                "tile epilogue needs the operand ring to hold the fp32 tile (or half of it)");
   static_assert(C::SMEM <= 227 * 1024 && C::TMEM_COLS <= 512, "shared memory or TMEM");
   if (job.np < 1 || job.np > NP || job.tile0[0] != 0) return cudaErrorInvalidValue;
   for (int p = 0; p < job.np; p++) {
