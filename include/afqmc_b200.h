@@ -280,17 +280,18 @@ afq_status afq_get_sparse_paths(afq_handle* h, int* path, double* ms);
  *   lane writes its walker's entries, the mirrored block as 4-byte stores), 1 = through
  *   the fp32 tile in shared memory on the per-tile kernel (direct and mirrored rows as
  *   16-byte stores), 2 = the same with two CTAs per SM (one operand stage each, the tile
- *   staged in two halves), so one CTA's epilogue overlaps the other's main loop.  Same
- *   values.  Timed -> ms[6..8].  AFQ_VHS_EPI=0|1|2 forces one; a forced kernel
- *   (AFQ_TUNE=1 or 2) keeps 0.
+ *   staged in two halves), so one CTA's epilogue overlaps the other's main loop; the same
+ *   values.  3 = as 2 with two 48 KB stages of 64-byte K slabs (SWIZZLE_64B) per CTA: the
+ *   same products in another fp32 summation order (1e-6 relative).  Timed -> ms[6..9].
+ *   AFQ_VHS_EPI=0..3 forces one; a forced kernel (AFQ_TUNE=1 or 2) keeps 0.
  * sched[2]: walkers per wave of the fused propagation chain, 0 = eight launches per
  *   substep.  Fused (2n a multiple of 32): the whole chain is ONE cooperative persistent
  *   launch whose tiles run in pairs of walker waves, product by product, a tile starting
  *   once every tile of the previous product of its walker is done, so a wave's V, Taylor
- *   sum and operands stay in L2 across the eight products.  Same values.  Timed -> ms[9]
- *   (eight launches), ms[10..14] (waves of 16, 24, 32, 48, 64).  AFQ_PROP_CHAIN=0 keeps
+ *   sum and operands stay in L2 across the eight products.  Same values.  Timed -> ms[10]
+ *   (eight launches), ms[11..15] (waves of 16, 24, 32, 48, 64).  AFQ_PROP_CHAIN=0 keeps
  *   the eight launches, =<walkers> forces a wave.
- * ms[15] may be NULL; 0 where not timed. */
+ * ms[16] may be NULL; 0 where not timed. */
 afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work
  * or events against the library's. */

@@ -331,16 +331,17 @@ class AfqmcSys:
                for i, k in enumerate(self.TUNE_SITES)}
         out["splitk_slices"] = int(c[ns])
         sc = np.zeros(3, np.int32)
-        gm = np.zeros(15)
+        gm = np.zeros(16)
         self._check(self.lib.afq_get_schedule(self.h, _p(sc), _p(gm)))
         out["propagate_walker_group"] = {"walkers": int(sc[0]),
                                          "ms_all_32_48_64_96_128": [round(float(x), 4)
                                                                     for x in gm[:6]]}
         out["vhs_epilogue"] = {"tile": int(sc[1]),
-                               "ms_rowwise_tile_tile2": [round(float(x), 4) for x in gm[6:9]]}
+                               "ms_rowwise_tile_tile2_tile2slab64": [round(float(x), 4)
+                                                                     for x in gm[6:10]]}
         out["propagate_chain"] = {"wave": int(sc[2]),
                                   "ms_launches_16_24_32_48_64": [round(float(x), 4)
-                                                                 for x in gm[9:15]]}
+                                                                 for x in gm[10:16]]}
         return out
 
     SPARSE_OPERANDS = ["Spvn", "SpvnT", "Vakbl"]

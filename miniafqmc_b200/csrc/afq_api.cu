@@ -1753,12 +1753,12 @@ afq_status afq_get_tuning(afq_handle* h, int* choice, double* ms) {
 
 afq_status afq_get_schedule(afq_handle* h, int* sched, double* ms) {
   if (!h || !sched) return AFQ_ERR_ARG;
-  float t[15] = {};
+  float t[16] = {};
   sched[0] = h->mixed ? afq::mixed_prop_group(h->mixed, t) : 0;
   sched[1] = h->mixed ? afq::mixed_vhs_epilogue(h->mixed, t + 6) : 0;
-  sched[2] = h->mixed ? afq::mixed_prop_chain(h->mixed, t + 9) : 0;
+  sched[2] = h->mixed ? afq::mixed_prop_chain(h->mixed, t + 10) : 0;
   if (ms)
-    for (int i = 0; i < 15; i++) ms[i] = t[i];
+    for (int i = 0; i < 16; i++) ms[i] = t[i];
   return AFQ_OK;
 }
 

@@ -66,8 +66,8 @@ cudaError_t mixed_set_wait_clocks(long long clocks);
 // product) and, in ms[6], the timed chain for 0 (all), 32, 48, 64, 96 and 128 walkers.
 int mixed_prop_group(const MixedState* m, float* ms);
 // Symmetric vHS epilogue picked at set-up (0 row-wise, 1 through the shared-memory tile,
-// 2 the same with two CTAs per SM) and, in ms[3], the timed product for each (0 when not
-// timed).
+// 2 the same with two CTAs per SM, 3 as 2 with two 64-byte-slab stages per CTA) and, in
+// ms[4], the timed product for each (0 when not timed).
 int mixed_vhs_epilogue(const MixedState* m, float* ms);
 // Walkers per wave of the fused propagation chain (0: eight launches) and, in ms[6], the
 // timed chain: eight launches, waves of 16, 24, 32, 48 and 64 walkers (0 when not timed).

@@ -125,6 +125,7 @@ struct MixedState {
   int ex_Gn = 0, ex_Gw = 0, ex_bn = 0, ex_mtiles = 0;
   std::vector<void*> allocs;
   tc::Maps m_vhs, m_pw[2], m_v[2], m_vbias, m_ej, m_ek;
+  tc::Maps m_vhs64;   // vHS operands in 64-byte K slabs (SWIZZLE_64B), epilogue choice 3
   // walker width 2n = 80: the promoted exchange on 160-column tiles (two walkers, one
   // epilogue warpgroup), with its own Gx map (160-row boxes)
   tc::Maps m_ek80;
@@ -147,9 +148,10 @@ struct MixedState {
   tc::Maps m_pw2, m_t1_1;
   // symmetric vHS epilogue: 0 row-wise (EpiVhsSym, the tuned kernel), 1 through the
   // shared-memory tile (EpiVhsSymTile, per-tile kernel), 2 the same with two CTAs per SM
-  // (one stage each, the tile staged in halves); picked by the set-up tuner
+  // (one stage each, the tile staged in halves), 3 as 2 with two 64-byte-slab stages per
+  // CTA; picked by the set-up tuner
   int vhs_epi = 0;
-  float vhs_epi_ms[3] = {};
+  float vhs_epi_ms[4] = {};
   bool packed = false;
   int fa_buf = 0;
   // kernel of each product site (0 built-in rule, 1 persistent, 2 per-tile), chosen at
@@ -1763,6 +1765,8 @@ cudaError_t mixed_create(const MixedInit* init, MixedState** out, std::string* m
   const int bnv = 256;
   const uint64_t vrows = m->vsym ? (uint64_t)m->npairs * 256 : (uint64_t)N * N;
   ok &= map2(m->m_vhs, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv);
+  ok &= map2(m->m_vhs64, m->Xf, m->Kv, 2 * nw, 1, m->Kv, 0, m->Sd, m->Kv, vrows, 1, m->Kv, 0, bnv,
+             64);
   const uint64_t fr = 4 * n, fsz = (uint64_t)4 * n * 2 * N;
   {
     const uint64_t Kp = m->preal ? N : 2 * N;
@@ -1866,8 +1870,11 @@ static cudaError_t vhs_product(MixedState* m, cudaStream_t st) {
       EpiVhsSymTile epi{m->Vf, nw, N, m->pairs};
       return run_bn(256, m->prec_vhs, m->m_vhs, g, epi, m->err, st, 2);
     }
-    if (m->vhs_epi == 2) {   // two CTAs per SM: one overlaps the other's epilogue
+    if (m->vhs_epi == 2 || m->vhs_epi == 3) {   // two CTAs per SM: one overlaps the other's epilogue
       EpiVhsSymTile epi{m->Vf, nw, N, m->pairs};
+      if (m->vhs_epi == 3 && m->prec_vhs == PREC_SPLIT)   // two 48 KB stages of 64-byte slabs
+        return tc::launch<256, 2, 1, true, EpiVhsSymTile, 2, 64>(m->m_vhs64, g, epi, m->err, st);
+      if (m->vhs_epi == 3) return cudaErrorInvalidValue;
       if (m->prec_vhs == PREC_SPLIT)
         return tc::launch<256, 1, 1, true, EpiVhsSymTile, 2>(m->m_vhs, g, epi, m->err, st);
       if (m->prec_vhs == PREC_BF16)
@@ -2442,7 +2449,7 @@ struct TuneRec {
   float ms[TS_N][2];
   float group_ms[6];
   int vhs_epi;
-  float vhs_epi_ms[3];
+  float vhs_epi_ms[4];
   int chain_wave;
   float chain_ms[6];
   int splits;
@@ -2479,9 +2486,8 @@ void tune_load(const char* path) {
     for (int i = 0; i < TS_N && ok; i++)
       ok = fscanf(f, "%d %f %f", &r.tune[i], &r.ms[i][0], &r.ms[i][1]) == 3;
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.group_ms[i]) == 1;
-    if (ok)
-      ok = fscanf(f, "%d %f %f %f", &r.vhs_epi, &r.vhs_epi_ms[0], &r.vhs_epi_ms[1],
-                  &r.vhs_epi_ms[2]) == 4;
+    if (ok) ok = fscanf(f, "%d", &r.vhs_epi) == 1;
+    for (int i = 0; i < 4 && ok; i++) ok = fscanf(f, "%f", &r.vhs_epi_ms[i]) == 1;
     if (ok) ok = fscanf(f, "%d", &r.chain_wave) == 1;
     for (int i = 0; i < 6 && ok; i++) ok = fscanf(f, "%f", &r.chain_ms[i]) == 1;
     if (!ok || fscanf(f, "%d %d", &r.splits, &r.prop_group) != 2) break;
@@ -2497,8 +2503,8 @@ void tune_save(const char* path, const std::string& key, const TuneRec& r) {
   fprintf(f, "%s", key.c_str());
   for (int i = 0; i < TS_N; i++) fprintf(f, " %d %.5f %.5f", r.tune[i], r.ms[i][0], r.ms[i][1]);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.group_ms[i]);
-  fprintf(f, " %d %.5f %.5f %.5f", r.vhs_epi, r.vhs_epi_ms[0], r.vhs_epi_ms[1],
-          r.vhs_epi_ms[2]);
+  fprintf(f, " %d", r.vhs_epi);
+  for (int i = 0; i < 4; i++) fprintf(f, " %.5f", r.vhs_epi_ms[i]);
   fprintf(f, " %d", r.chain_wave);
   for (int i = 0; i < 6; i++) fprintf(f, " %.5f", r.chain_ms[i]);
   fprintf(f, " %d %d\n", r.splits, r.prop_group);
@@ -2544,7 +2550,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       m->prop_group = r.prop_group;
       for (int i = 0; i < 6; i++) m->prop_group_ms[i] = r.group_ms[i];
       m->vhs_epi = r.vhs_epi;
-      for (int v = 0; v < 3; v++) m->vhs_epi_ms[v] = r.vhs_epi_ms[v];
+      for (int v = 0; v < 4; v++) m->vhs_epi_ms[v] = r.vhs_epi_ms[v];
       m->chain_wave = m->dep ? r.chain_wave : 0;
       for (int i = 0; i < 6; i++) m->chain_ms[i] = r.chain_ms[i];
       tune_save(cache_path, key, r);   // a shape timed before the file was named
@@ -2627,9 +2633,9 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
   // tile (full tuning only, so forced kernels stay comparable); AFQ_VHS_EPI=0|1 forces
   if (m->vsym && m->tune[TS_VHS] && force < 0) {
     const char* fe = getenv("AFQ_VHS_EPI");
-    float t[3] = {0.0f, 0.0f, 0.0f};
+    float t[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     int bv = 0;
-    for (int v = 0; v < 3; v++) {
+    for (int v = 0; v < 4; v++) {
       if (fe && atoi(fe) != v) continue;
       m->vhs_epi = v;
       const float ms = timed([&] { return vhs_product(m, st); });
@@ -2637,7 +2643,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
       if (t[v] > 0.0f && (t[bv] <= 0.0f || t[v] < t[bv])) bv = v;
     }
     m->vhs_epi = bv;
-    for (int v = 0; v < 3; v++) m->vhs_epi_ms[v] = t[v];
+    for (int v = 0; v < 4; v++) m->vhs_epi_ms[v] = t[v];
   }
   {
     const int mt = (N + 127) / 128, n2 = 2 * n;
@@ -2766,7 +2772,7 @@ static cudaError_t mixed_tune(MixedState* m, cudaStream_t st) {
     r.prop_group = m->prop_group;
     for (int i = 0; i < 6; i++) r.group_ms[i] = m->prop_group_ms[i];
     r.vhs_epi = m->vhs_epi;
-    for (int v = 0; v < 3; v++) r.vhs_epi_ms[v] = m->vhs_epi_ms[v];
+    for (int v = 0; v < 4; v++) r.vhs_epi_ms[v] = m->vhs_epi_ms[v];
     r.chain_wave = m->chain_wave;
     for (int i = 0; i < 6; i++) r.chain_ms[i] = m->chain_ms[i];
     std::lock_guard<std::mutex> lk(tune_mu);
@@ -2793,7 +2799,7 @@ int mixed_prop_chain(const MixedState* m, float* ms) {
 
 int mixed_vhs_epilogue(const MixedState* m, float* ms) {
   if (ms)
-    for (int i = 0; i < 3; i++) ms[i] = m ? m->vhs_epi_ms[i] : 0.0f;
+    for (int i = 0; i < 4; i++) ms[i] = m ? m->vhs_epi_ms[i] : 0.0f;
   return m ? m->vhs_epi : 0;
 }
 
