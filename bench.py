@@ -64,6 +64,10 @@ def parse():
                    help="1: population control (comb) after every energy measurement (default "
                         "0: none, as in the reference miniapp)")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    p.add_argument("--cv-base", type=int, default=0,
+                   help="headline control variate: 0 = network on the step's features, 1 = "
+                        "plain-bf16 exchange of every walker as the surrogate's base with a "
+                        "learned residual (the accuracy pass measures both)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-walkers", type=int, default=0)
@@ -305,7 +309,7 @@ def run_reference(args):
 class Form:
     """One walker set in one numerical form, with its step loop."""
 
-    def __init__(self, system, cfg, args, form, device, comm, torch):
+    def __init__(self, system, cfg, args, form, device, comm, torch, cv_base=None):
         from miniafqmc_b200.afqmc import AfqmcSys, AFQ_PREC_FP64, AFQ_PREC_MIXED
         self.cfg, self.args, self.form, self.comm = cfg, args, form, comm
         prec = AFQ_PREC_FP64 if form == "fp64" else AFQ_PREC_MIXED
@@ -316,6 +320,9 @@ class Form:
         if self.mode == "cv":
             self.eng.cv_configure(hidden=256, lr=1e-3, seed=cfg.seed, train_walker_steps=2000,
                                   subset_den=8)
+            self.cv_base = args.cv_base if cv_base is None else cv_base
+            if self.cv_base:   # plain-bf16 exchange of every walker + learned residual
+                self.eng.cv_set_base(1)
         self.stream = torch.cuda.ExternalStream(self.eng.stream)
         self.energies, self.sig2, self.cvvar = [], [], []
 
@@ -365,10 +372,11 @@ def blocking_sigma(x):
 
 
 def accuracy_pass(system, cfg, args, device, torch):
-    """Energy accuracy at the target run length, apart from the headline timing: three
+    """Energy accuracy at the target run length, apart from the headline timing: four
     walker sets start from the trial and take `acc_substeps` substeps (CUDA-graph
     substeps) on the same Philox fields -- mixed precision with the control variate (the
-    headline form), mixed precision with exact exchange, and FP64 -- measuring the energy
+    headline form), the same with the other control-variate setting, mixed precision with
+    exact exchange, and FP64 -- measuring the energy
     every energy_every substeps.  The control variate trains on its first exact samples
     inside the pass (its first measurements are exact on every walker).  Measurements of
     the first `acc_equil` substeps (equilibration from the trial) are left out of the
@@ -385,14 +393,25 @@ def accuracy_pass(system, cfg, args, device, torch):
     walkers (afq_copy_walkers) and measures them with the control-variate estimator and
     with exact exchange ("same_walkers": the mean difference from FP64, the standard error
     of that mean, the largest single difference; the shadow's time is left out of the FP64
-    pass's device time)."""
+    pass's device time).  Both control-variate settings are measured: the headline's
+    (--cv-base) and the other one, as a fourth trajectory and a second shadow."""
     out = {"substeps": args.acc_substeps, "energy_every": args.energy_every,
            "equilibration_substeps": args.acc_equil, "forms": {}}
     series = {}
-    shadow_e = {"cv": [], "exact": []}
-    for name in ("mixed-cv", "mixed", "fp64"):
-        f = Form(system, cfg, args, name, device, None, torch)
-        shadow = Form(system, cfg, args, "mixed-cv", device, None, torch) if name == "fp64" else None
+    # control variates measured on the FP64 trajectory's walkers: the headline's, the other
+    # base setting's, and exact exchange
+    other = "cv_two_level" if not args.cv_base else "cv_features_only"
+    shadow_e = {"cv": [], other: [], "exact": []}
+    forms = [("mixed-cv", None), ("mixed-cv-other", 1 - args.cv_base), ("mixed", None),
+             ("fp64", None)]
+    for name, base in forms:
+        kind = "mixed-cv" if name.startswith("mixed-cv") else name
+        f = Form(system, cfg, args, kind, device, None, torch, cv_base=base)
+        shadows = {}
+        if name == "fp64":
+            shadows = {"cv": Form(system, cfg, args, "mixed-cv", device, None, torch),
+                       other: Form(system, cfg, args, "mixed-cv", device, None, torch,
+                                   cv_base=1 - args.cv_base)}
         t_shadow = 0.0
         e = f.eng
         e.synchronize()
@@ -405,26 +424,29 @@ def accuracy_pass(system, cfg, args, device, torch):
             f.step(st)
             if (st + 1) % args.energy_every == 0:
                 steps.append(st + 1)
-                if shadow is not None:
+                if shadows:
                     ts = time.perf_counter()
-                    se = shadow.eng
-                    se.copy_walkers_from(e)
-                    se.calculate_mixed_density_matrix()
-                    shadow_e["cv"].append(se.calculate_energy("cv"))
-                    shadow_e["exact"].append(se.calculate_energy("chol"))
-                    se.synchronize()
+                    for k, sh in shadows.items():
+                        se = sh.eng
+                        se.copy_walkers_from(e)
+                        se.calculate_mixed_density_matrix()
+                        shadow_e[k].append(se.calculate_energy("cv"))
+                        if k == "cv":
+                            shadow_e["exact"].append(se.calculate_energy("chol"))
+                        se.synchronize()
                     t_shadow += time.perf_counter() - ts
         e.synchronize()
         e1.record(f.stream)
         torch.cuda.synchronize()
         secs = e0.elapsed_time(e1) * 1e-3 - t_shadow
-        if shadow is not None:
-            out["same_walkers_cv_stats"] = shadow.eng.cv_stats()
-            shadow.eng.close()
+        for k, sh in shadows.items():
+            out["same_walkers_%s_stats" % k] = sh.eng.cv_stats()
+            sh.eng.close()
         keep = np.array(steps) > args.acc_equil
         E = np.array(f.energies)[keep]
         sig, lev = blocking_sigma(E)
-        series[name] = E
+        key = name if name != "mixed-cv-other" else "mixed-" + other.replace("_", "-")
+        series[key] = E
         rec = {"mean_E": float(E.mean()), "sigma_E_blocked": sig,
                "sigma_E_levels": [float(v) for v in lev], "device_s": secs,
                "measurements": int(keep.sum()), "eps_Ha_sqrt_s": sig * float(np.sqrt(secs))}
@@ -432,25 +454,52 @@ def accuracy_pass(system, cfg, args, device, torch):
             sv = np.array(f.cvvar)[keep]
             rec["subset_sigma_per_measurement_Ha"] = float(np.sqrt(np.mean(sv)))
             rec["control_variate"] = e.cv_stats()
-        out["forms"][name] = rec
+            rec["low_precision_base"] = bool(f.cv_base)
+        out["forms"][key] = rec
         e.close()
-    for name in ("mixed-cv", "mixed"):
+    for name in series:
+        if name == "fp64":
+            continue
         d = series[name] - series["fp64"]
         sd, _ = blocking_sigma(d)
         out[f"dE_{name}_vs_fp64"] = {"abs_dE_Ha": float(abs(d.mean())), "sigma_Ha": sd,
                                      "max_abs_per_measurement_Ha": float(np.max(np.abs(d)))}
     keep = np.array(steps) > args.acc_equil
     same = {}
-    for k in ("cv", "exact"):
+    for k in shadow_e:
         d = np.array(shadow_e[k])[keep] - series["fp64"]
         same[k] = {"dE_Ha": float(d.mean()), "abs_dE_Ha": float(abs(d.mean())),
                    "sigma_of_mean_Ha": float(d.std(ddof=1) / np.sqrt(len(d))),
+                   "sigma_of_mean_blocked_Ha": blocking_sigma(d)[0],
                    "rms_per_measurement_Ha": float(np.sqrt(np.mean(d ** 2))),
                    "max_abs_per_measurement_Ha": float(np.max(np.abs(d)))}
     out["same_walkers_along_fp64_trajectory"] = same
     fm, f6 = out["forms"]["mixed-cv"], out["forms"]["fp64"]
-    out["abs_dE_Ha"] = out["dE_mixed-cv_vs_fp64"]["abs_dE_Ha"]
-    out["abs_dE_sigma_Ha"] = out["dE_mixed-cv_vs_fp64"]["sigma_Ha"]
+    # |dE| of the headline form: its energy estimate minus FP64's on the same walkers
+    # (the FP64 trajectory's), averaged over the measurements, with the standard error of
+    # that mean.  Different forms' trajectories decorrelate within tens of substeps (any
+    # rounding difference is amplified through the force bias), so the trajectory means
+    # agree only within their statistical error: reported beside it with the z-score.
+    out["abs_dE_Ha"] = same["cv"]["abs_dE_Ha"]
+    out["abs_dE_sigma_Ha"] = max(same["cv"]["sigma_of_mean_Ha"],
+                                 same["cv"]["sigma_of_mean_blocked_Ha"])
+    out["abs_dE_definition"] = ("mean over the measurements after equilibration of "
+                                "(control-variate estimate - FP64 energy) on the FP64 "
+                                "trajectory's walkers; sigma = standard error of that mean "
+                                "(the larger of the naive and the blocked estimate)")
+    tr = out["dE_mixed-cv_vs_fp64"]
+    out["trajectory_dE_Ha"] = tr["abs_dE_Ha"]
+    out["trajectory_dE_sigma_Ha"] = tr["sigma_Ha"]
+    out["trajectory_dE_z"] = tr["abs_dE_Ha"] / tr["sigma_Ha"] if tr["sigma_Ha"] > 0 else None
+    # the expectation of the control-variate estimate is the mixed form's exact-exchange
+    # energy (the subset correction is unbiased): its deterministic error against FP64
+    out["abs_dE_deterministic_Ha"] = same["exact"]["abs_dE_Ha"]
+    fo = out["forms"]["mixed-" + other.replace("_", "-")]
+    out["other_control_variate"] = {
+        "form": other, "abs_dE_Ha": same[other]["abs_dE_Ha"],
+        "abs_dE_sigma_Ha": max(same[other]["sigma_of_mean_Ha"],
+                               same[other]["sigma_of_mean_blocked_Ha"]),
+        "device_s": fo["device_s"], "fp64_over_form": f6["eps_Ha_sqrt_s"] / fo["eps_Ha_sqrt_s"]}
     out["err_per_wall_s"] = {
         "form": fm["eps_Ha_sqrt_s"], "fp64": f6["eps_Ha_sqrt_s"],
         "fp64_over_form": f6["eps_Ha_sqrt_s"] / fm["eps_Ha_sqrt_s"],

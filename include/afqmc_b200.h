@@ -207,6 +207,16 @@ afq_status afq_synchronize(afq_handle* h);
  * training online on the exact samples.  Call after afq_set_hamiltonian with Lhalf. */
 afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
                             long long train_walker_steps, int subset_den);
+/* Two-level control variate (no reference counterpart): base = 1 makes the surrogate of
+ * each walker's exchange energy the exchange from one plain bf16 tensor-core product
+ * (the hi parts of the split operands; about a third of the exact product's work) on
+ * every walker, plus the network's prediction of the exact-minus-base residual -- the
+ * network's last two inputs carry the base in place of the linearised exchange.  The
+ * Horvitz-Thompson correction on the exact subset keeps the estimator unbiased either
+ * way; the base shrinks the residual the subset must correct, and with it the estimator's
+ * sampling noise.  base = 0 (the default): the network on the step's own features.
+ * Mixed form only (AFQ_ERR_UNSUPPORTED otherwise); restarts the control variate. */
+afq_status afq_cv_set_base(afq_handle* h, int base);
 /* stats[8] = exact samples so far, subset size of the last measurement, last training
  * loss (standardised units), estimator active (0/1), measurements, sampling variance
  * (Ha^2) that the subset correction adds to the last weighted mean energy,

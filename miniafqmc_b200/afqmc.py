@@ -31,7 +31,7 @@ EXPORTS = [
     "afq_update_weights", "afq_update_weights_partial", "afq_get_eshift", "afq_set_eshift",
     "afq_orthogonalize", "afq_energy", "afq_energy_sums", "afq_substep", "afq_synchronize",
     "afq_copy_out", "afq_set_walker_offset", "afq_profile", "afq_stage_times", "afq_get_stream",
-    "afq_selftest_tc_gemm", "afq_exchange_energy_noalloc", "afq_cv_configure", "afq_cv_stats",
+    "afq_selftest_tc_gemm", "afq_exchange_energy_noalloc", "afq_cv_configure", "afq_cv_set_base", "afq_cv_stats",
     "afq_mlp_create", "afq_mlp_destroy", "afq_mlp_num_params", "afq_mlp_set_params",
     "afq_mlp_get_params", "afq_mlp_forward", "afq_mlp_gradient", "afq_mlp_train",
     "afq_batch_create", "afq_batch_destroy", "afq_batch_substep", "afq_batch_synchronize",
@@ -86,6 +86,7 @@ def signatures() -> dict:
         "afq_selftest_tc_gemm": ([I, I, I, I, I, I, I, P, P, P, P], I),
         "afq_exchange_energy_noalloc": ([P, P, I, I, I, I, P, P], I),
         "afq_cv_configure": ([P, I, D, U64, ctypes.c_longlong, I], I),
+        "afq_cv_set_base": ([P, I], I),
         "afq_cv_stats": ([P, P], I),
         "afq_mlp_create": ([I, I, I, U64, P], I), "afq_mlp_destroy": ([P], None),
         "afq_mlp_num_params": ([P], ctypes.c_longlong), "afq_mlp_set_params": ([P, P], I),
@@ -287,6 +288,11 @@ class AfqmcSys:
         """Learned control variate for the exchange energy (used by mode "cv")."""
         self._check(self.lib.afq_cv_configure(self.h, hidden, lr, seed, train_walker_steps,
                                               subset_den))
+
+    def cv_set_base(self, base: int = 1):
+        """Two-level control variate: plain-bf16 exchange of every walker as the
+        surrogate's base, the network learning the exact-minus-base residual (mixed form)."""
+        self._check(self.lib.afq_cv_set_base(self.h, base))
 
     def cv_stats(self) -> dict:
         v = np.zeros(8)

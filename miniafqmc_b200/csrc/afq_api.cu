@@ -1311,6 +1311,10 @@ afq_status energy_cv(afq_handle* h, double* sums) {
     int nb = 0;
     return afq::launch_exchange(h->Lh, gsub, h->N, h->n, h->nc, m, kp, &nb, h->st);
   };
+  if (h->mixed && h->cv_cfg.base)
+    in.base_exchange = [h](const z_t* g, int m, z_t* kp) -> cudaError_t {
+      return afq::mixed_exchange_lowp(h->mixed, g, m, kp, h->nblk, h->st);
+    };
   cudaError_t e = staged(h, AFQ_STAGE_ENERGY, 0, [&]() -> cudaError_t {
     cudaError_t r;
     if (h->mixed) {
@@ -1719,6 +1723,18 @@ afq_status afq_cv_configure(afq_handle* h, int hidden, double lr, uint64_t seed,
   h->cv_cfg.seed = seed;
   h->cv_cfg.train_walker_steps = train_walker_steps;
   h->cv_cfg.subset_den = subset_den;
+  return AFQ_OK;
+}
+
+afq_status afq_cv_set_base(afq_handle* h, int base) {
+  if (!h || base < 0 || base > 1) return AFQ_ERR_ARG;
+  if (base && h->d.precision != AFQ_PREC_MIXED)
+    return fail(h, AFQ_ERR_UNSUPPORTED, "low-precision base: mixed form only");
+  if (h->cv) {
+    afq::cv_destroy(h->cv);
+    h->cv = nullptr;
+  }
+  h->cv_cfg.base = base;
   return AFQ_OK;
 }
 

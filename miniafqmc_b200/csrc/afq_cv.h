@@ -46,6 +46,10 @@ struct CvConfig {
   int q_refresh = 0;
   // residual learning: the network predicts E_K minus feature 36 (the linearisation)
   int residual = 0;
+  // low-precision base: the exchange of every walker from one plain bf16 tensor-core
+  // product (CvInputs::base_exchange) takes the place of the linearisation in features
+  // 36/37 and the network learns E_K minus it (residual learning on)
+  int base = 0;
 };
 
 struct CvState;
@@ -63,6 +67,9 @@ struct CvInputs {
   std::function<cudaError_t(const z_t*, int, z_t*)> exact_exchange;
   const z_t* Lh;        // [nchol][2][n][N] unscaled half-rotated factors (FP64)
   int n, N;
+  // base_exchange(Gc, nw, Kpart): low-precision exchange partial sums of every walker, in
+  // the layout of exact_exchange (empty: no low-precision base available)
+  std::function<cudaError_t(const z_t*, int, z_t*)> base_exchange;
 };
 
 cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvState** out,

@@ -37,6 +37,11 @@ cudaError_t mixed_energy_chol(MixedState* m, const z_t* Gc, z_t* cvec, z_t* Kpar
 cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t st);
 cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
                            cudaStream_t st);
+// The exchange partial sums in plain bf16 (hi parts of the split operands, one product):
+// the control variate's low-precision base.  cudaErrorNotSupported unless the exchange
+// runs on bf16 split operands.
+cudaError_t mixed_exchange_lowp(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
+                                cudaStream_t st);
 // Mixed density matrix: T1 = W^T tw in split bf16 on tensor cores, FP64 Gauss-Jordan for
 // det(T1) (-> W_data overlaps, info) and T1^-1, Gc = T1^-1 W^T on tensor cores.
 // want_gc == 0 computes the overlaps (and keeps T1^-1); cached != 0 forms Gc from the

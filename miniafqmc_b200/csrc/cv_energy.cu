@@ -4,7 +4,10 @@
 //   features of every walker from quantities the step already has: a fixed Gaussian
 //     projection (32 rows) of the Coulomb vector c_w = Lh Gc_w, E_J = 1/2 c_w.c_w,
 //     E_1 = Gc_w.haj, log|ovlp_a ovlp_b| and its phase, and the linearised exchange
-//     Q.Gc_w (Re, Im), Q = dE_K/dG at the first measurement's mean G;
+//     Q.Gc_w (Re, Im), Q = dE_K/dG at the first measurement's mean G -- or, with the
+//     low-precision base (cfg.base), in place of the linearisation the exchange of every
+//     walker from one plain bf16 tensor-core product, the network then learning the exact
+//     E_K minus that base (a two-level control variate: cheap exchange + learned residual);
 //   surrogate f_w = MLP(features) on every walker;
 //   exact exchange E_K on a seeded subset S drawn with m = ceil(nw / subset_den) teeth
 //     (all walkers until the first train_walker_steps exact samples are in): by default a
@@ -70,6 +73,8 @@ struct CvState {
   // Q set-up scratch: Gm [2][n][N], Tq [2][nc][n][n], Qpart [nc][n][N]; qoff = Q.Gm / 2
   z_t *Gm = nullptr, *Tq = nullptr, *Qpart = nullptr, *d_qoff = nullptr;
   double lin_ref = 0.0;  // Re of the first linearisation's E_K(Gm)
+  double* ek_base = nullptr;   // [nw][2] low-precision exchange of every walker (cfg.base)
+  float* fsort = nullptr;      // [nw] surrogate in the order the subset design sorts by
   // online training runs on its own stream after the estimate, overlapping the next
   // substeps; the next measurement (and any use of the network) waits for ev_trained
   cudaStream_t tst = nullptr;
@@ -269,6 +274,23 @@ cv_ek_kernel(const z_t* __restrict__ Kpart, int nblk, double* __restrict__ ek) {
     ek[2 * i] = 0.5 * s.x;
     ek[2 * i + 1] = 0.5 * s.y;
   }
+}
+
+// Features 36/37 from the low-precision exchange of every walker (relative to ref).
+__global__ void cv_base_feature_kernel(const double* __restrict__ ek, int nw, double ref,
+                                       float* __restrict__ feats) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
+    feats[(long long)w * CV_NIN + 36] = (float)(ek[2 * w] - ref);
+    feats[(long long)w * CV_NIN + 37] = (float)ek[2 * w + 1];
+  }
+}
+
+// The surrogate up to a constant: fs * network output (+ feature 36 it was trained on top
+// of), the key of the weight-proportional design's ordering.
+__global__ void cv_sortkey_kernel(const float* __restrict__ fpred, const float* __restrict__ fbase,
+                                  float fs, int nw, float* __restrict__ out) {
+  for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x)
+    out[w] = fs * fpred[w] + (fbase ? fbase[(long long)w * CV_NIN] : 0.0f);
 }
 
 __global__ void cv_mark_kernel(const int* __restrict__ sub, int m, int* __restrict__ member) {
@@ -508,6 +530,7 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   if (const char* sm = getenv("AFQ_CV_SAMPLING")) s->cfg.sampling = atoi(sm) == 0 ? 0 : 1;
   if (const char* qr = getenv("AFQ_CV_QREFRESH")) s->cfg.q_refresh = std::max(0, atoi(qr));
   if (const char* rs = getenv("AFQ_CV_RESIDUAL")) s->cfg.residual = atoi(rs) != 0;
+  if (s->cfg.base) s->cfg.residual = 1;
   s->nw = nw; s->nc = nchol; s->nak = nak;
   s->sub_cap = (nw + cfg.subset_den - 1) / cfg.subset_den;
   s->cap = std::max(4096, nw);
@@ -537,6 +560,8 @@ cudaError_t cv_create(const CvConfig& cfg, int nw, int nchol, long long nak, CvS
   A(cmal(s, &s->Gc_sub, (size_t)s->sub_cap * nak));
   A(cmal(s, &s->Q, (size_t)nak));
   A(cmal(s, &s->d_qoff, 1));
+  A(cmal(s, &s->ek_base, (size_t)nw * 2));
+  A(cmal(s, &s->fsort, nw));
   if (e == cudaSuccess) e = cudaMemsetAsync(s->Q, 0, sizeof(z_t) * nak, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->d_qoff, 0, sizeof(z_t), st);
   if (e == cudaSuccess) e = cudaMallocHost(&s->h_sub, sizeof(int) * nw);
@@ -647,9 +672,11 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   }
   s->meas++;
   s->launches = 0;
+  const bool base = s->cfg.base && in.base_exchange;
   // linearised exchange about the weighted-mean G: at the first measurement, then every
-  // q_refresh measurements
-  if (in.Lh && (!s->have_q || (s->cfg.q_refresh > 0 && s->meas - s->q_meas >= s->cfg.q_refresh))) {
+  // q_refresh measurements (not with the low-precision base, which takes its features)
+  if (!base && in.Lh &&
+      (!s->have_q || (s->cfg.q_refresh > 0 && s->meas - s->q_meas >= s->cfg.q_refresh))) {
     if ((e = cv_refresh_q(s, in, st)) != cudaSuccess) return e;
     if (!s->have_q) {   // the reference of feature 36: E_K at the first mean G
       z_t q0;
@@ -666,6 +693,24 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
                                          s->Q, s->d_qoff, s->lin_ref, s->feats, s->e1ej);
   s->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (base) {   // low-precision exchange of every walker -> features 36/37
+    if ((e = in.base_exchange(in.Gc, nw, in.Kpart)) != cudaSuccess) return e;
+    cv_ek_kernel<<<nw, 128, 0, st>>>(in.Kpart, in.nblk, s->ek_base);
+    s->launches += 3;
+    if (!s->have_q) {   // the reference of feature 36: the first walker's first value
+      double b0[2];
+      if ((e = cudaMemcpyAsync(b0, s->ek_base, sizeof(b0), cudaMemcpyDeviceToHost, st)) !=
+              cudaSuccess ||
+          (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return e;
+      s->lin_ref = b0[0];
+      s->have_q = true;
+      s->q_meas = s->meas;
+    }
+    cv_base_feature_kernel<<<gridn(nw, 256), 256, 0, st>>>(s->ek_base, nw, s->lin_ref, s->feats);
+    s->launches++;
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   s->active = s->trained && !s->failed;
   const int m_design = s->active ? s->sub_cap : nw;   // sample size, or teeth
   if (s->active) {
@@ -679,8 +724,10 @@ cudaError_t cv_energy(CvState* s, const CvInputs& in, double* sums, cudaStream_t
   int m = m_design;   // distinct walkers evaluated exactly
   if (pps) {   // the design needs the predictions and weights on the host
     cv_weights_kernel<<<gridn(nw, 256), 256, 0, st>>>(in.Wd, nw, s->d_wt);
-    s->launches++;
-    if ((e = cudaMemcpyAsync(s->h_f, s->fpred, sizeof(float) * nw, cudaMemcpyDeviceToHost, st)) !=
+    cv_sortkey_kernel<<<gridn(nw, 256), 256, 0, st>>>(
+        s->fpred, s->cfg.residual ? s->feats + 36 : nullptr, (float)s->sd_r, nw, s->fsort);
+    s->launches += 2;
+    if ((e = cudaMemcpyAsync(s->h_f, s->fsort, sizeof(float) * nw, cudaMemcpyDeviceToHost, st)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(s->h_wt, s->d_wt, sizeof(double) * nw, cudaMemcpyDeviceToHost, st)) !=
             cudaSuccess ||

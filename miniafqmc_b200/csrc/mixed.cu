@@ -2310,22 +2310,26 @@ cudaError_t mixed_coulomb(MixedState* m, const z_t* Gc, z_t* cvec, cudaStream_t 
 // warpgroup holding all 160 accumulator columns (5 chunks of 32).
 template <int PK>
 static cudaError_t exchange80(MixedState* m, const tc::GemmShape& g, int nsub, z_t* Kpart,
-                              int nblk, float as, const float* ws, cudaStream_t st) {
+                              int nblk, float as, const float* ws, int prec, cudaStream_t st) {
   using E = EpiExchangePromoted<80, PK>;
   const E ep{m->n, m->ex_Gn, 2, m->nc, nsub, nblk, Kpart, as, ws};
   tc::GemmShape g2 = g;
   g2.n_step = 160;
-  if (m->prec_ek == PREC_SPLIT16)
+  if (prec == PREC_SPLIT16)
     return tc::launch_persistent<160, 2, 0, true, E, 1>(m->m_ek80, g2, ep, m->err, st);
-  if (m->prec_ek == PREC_SPLIT)
+  if (prec == PREC_SPLIT)
     return tc::launch_persistent<160, 2, 1, true, E, 1>(m->m_ek80, g2, ep, m->err, st);
   return tc::launch_persistent<160, 4, 1, false, E, 1>(m->m_ek80, g2, ep, m->err, st);
 }
 
 // Exchange product of the first nsub walkers packed in Gx: the staged persistent kernel
 // (per-row traces from TMEM) for the compiled walker widths, else the per-tile kernel.
+// prec < 0: the exchange's own operand precision (m->prec_ek); PREC_BF16 with bf16 split
+// operands multiplies their hi parts only.  promote = false: no accumulator promotion (the
+// staged or per-tile epilogue).
 static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nblk,
-                                    cudaStream_t st) {
+                                    cudaStream_t st, int prec = -1, bool promote = true) {
+  if (prec < 0) prec = m->prec_ek;
   const int n = m->n;
   const bool f16 = m->Gx.f16;
   const float as = f16 ? m->sLh : 1.0f;
@@ -2335,16 +2339,16 @@ static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nbl
   tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
                   m->ex_mtiles, true, true, 0, false, m->ex_Gw * 2 * n};
   const int v = m->tune[2 * nsub > m->nw ? TS_EXF : TS_EXS];
-  const int pk = promote_kb(PROMOTE_EXCHANGE);
+  const int pk = promote ? promote_kb(PROMOTE_EXCHANGE) : 0;
   if ((v == 1 || (v == 0 && tc_persistent())) && pk && m->ex80) {
-    if (pk == 1) return exchange80<1>(m, g, nsub, Kpart, nblk, as, ws, st);
-    if (pk == 2) return exchange80<2>(m, g, nsub, Kpart, nblk, as, ws, st);
+    if (pk == 1) return exchange80<1>(m, g, nsub, Kpart, nblk, as, ws, prec, st);
+    if (pk == 2) return exchange80<2>(m, g, nsub, Kpart, nblk, as, ws, prec, st);
   }
   if ((v == 1 || (v == 0 && tc_persistent())) && pk && (m->ex_bn / 2) % (2 * n) == 0) {
     cudaError_t r = cudaErrorInvalidValue;
 #define AFQ_EXP(TN, PK)                                                                        \
   case TN * 8 + PK:                                                                            \
-    r = run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,                                               \
+    r = run_bn(m->ex_bn, prec, m->m_ek, g,                                               \
                EpiExchangePromoted<TN, PK>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws}, \
                m->err, st);                                                                    \
     break;
@@ -2358,20 +2362,20 @@ static cudaError_t exchange_product(MixedState* m, int nsub, z_t* Kpart, int nbl
   }
   if (v == 1 || (v == 0 && tc_persistent())) {
     switch (2 * n) {
-      case 32: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
+      case 32: return run_bn(m->ex_bn, prec, m->m_ek, g,
                              EpiExchangeStaged<32>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
-      case 64: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
+      case 64: return run_bn(m->ex_bn, prec, m->m_ek, g,
                              EpiExchangeStaged<64>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
-      case 96: return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g,
+      case 96: return run_bn(m->ex_bn, prec, m->m_ek, g,
                              EpiExchangeStaged<96>{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws},
                              m->err, st);
     }
-    if (v == 1) return cudaErrorInvalidValue;
+    if (v == 1 && promote) return cudaErrorInvalidValue;
   }
   EpiExchange ep{n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, as, ws};
-  return run_bn(m->ex_bn, m->prec_ek, m->m_ek, g, ep, m->err, st);
+  return run_bn(m->ex_bn, prec, m->m_ek, g, ep, m->err, st);
 }
 
 // Exchange partial sums Kpart[w][s][block] of the first nsub walkers packed in Gc.
@@ -2385,6 +2389,23 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return exchange_product(m, nsub, Kpart, nblk, st);
+}
+
+// The same exchange partial sums in plain bf16: the hi parts of the split operands, one
+// product instead of three (about 8 significant bits per operand).  Unsupported when the
+// exchange runs on fp16 split operands.
+cudaError_t mixed_exchange_lowp(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, int nblk,
+                                cudaStream_t st) {
+  if (!m->in.Lh || nsub > m->nw) return cudaErrorInvalidValue;
+  if (m->Gx.f16 || m->prec_ek != PREC_SPLIT) return cudaErrorNotSupported;
+  pack_gc_kernel<<<grid_for((long long)nsub * m->NAK), 256, 0, st>>>(
+      Gc, nsub, m->n, m->N, Op{}, m->Gx, m->nw, m->greal, nullptr);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // the base's fp32 sums over K need no promotion next to its bf16 operand rounding; the
+  // staged epilogue keeps up with the single product's shorter main loop
+  static const bool promote = getenv("AFQ_CV_BASE_PROMOTE") != nullptr;
+  return exchange_product(m, nsub, Kpart, nblk, st, PREC_BF16, promote);
 }
 
 bool mixed_has_dm(const MixedState* m) { return m && m->T1 && m->bn_t1 && m->bn_gc; }

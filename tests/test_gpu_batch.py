@@ -63,15 +63,19 @@ def test_batch_matches_systems_alone(mixed, nsub):
 
 
 @pytest.mark.parametrize("mode,nsub", [(3, 1), (3, 5), (1, 5), (2, 5)])
-def test_fused_batch_matches_systems_alone(mode, nsub):
+def test_fused_batch_matches_systems_alone(mode, nsub, monkeypatch):
     """Fused batch: the vHS product and each of the eight propagation products run as one
     launch over the three systems' (walker, M tile, N tile) work list.  Every tile runs the
     same MMA sequence and the same epilogue arithmetic as in a system's own launches (the
     system with 2n = 128 takes the tile epilogue and the pack kernels instead of the paired
     epilogue, which writes the same values), so the walkers, weights and energies equal
     the systems advanced alone to 1e-13 relative, through a re-orthogonalisation.  Modes:
-    3 both joint, 1 the vHS product only, 2 the chain only."""
+    3 both joint, 1 the vHS product only, 2 the chain only.  The joint vHS launch streams
+    128-byte K slabs; the set-up tuner may give a system alone the 64-byte-slab epilogue,
+    which adds the hi*lo and lo*hi products of every 32 K columns in another order, so the
+    systems alone are pinned to a 128-byte-slab epilogue here."""
     from miniafqmc_b200.afqmc import AfqmcSys, AfqmcBatch, AFQ_PREC_MIXED
+    monkeypatch.setenv("AFQ_VHS_EPI", "0")
     sys_ = systems()
     alone = [AfqmcSys(s, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False) for c, s in sys_]
     grouped = [AfqmcSys(s, c.nwalk, precision=AFQ_PREC_MIXED, use_vakbl=False) for c, s in sys_]
