@@ -475,22 +475,25 @@ def accuracy_pass(system, cfg, args, device, torch):
                    "max_abs_per_measurement_Ha": float(np.max(np.abs(d)))}
     out["same_walkers_along_fp64_trajectory"] = same
     fm, f6 = out["forms"]["mixed-cv"], out["forms"]["fp64"]
-    # |dE| of the headline form: its energy estimate minus FP64's on the same walkers
-    # (the FP64 trajectory's), averaged over the measurements, with the standard error of
-    # that mean.  Different forms' trajectories decorrelate within tens of substeps (any
-    # rounding difference is amplified through the force bias), so the trajectory means
-    # agree only within their statistical error: reported beside it with the z-score.
-    out["abs_dE_Ha"] = same["cv"]["abs_dE_Ha"]
-    out["abs_dE_sigma_Ha"] = max(same["cv"]["sigma_of_mean_Ha"],
-                                 same["cv"]["sigma_of_mean_blocked_Ha"])
-    out["abs_dE_definition"] = ("mean over the measurements after equilibration of "
-                                "(control-variate estimate - FP64 energy) on the FP64 "
-                                "trajectory's walkers; sigma = standard error of that mean "
-                                "(the larger of the naive and the blocked estimate)")
+    # |dE| of the headline form against FP64 on identical auxiliary fields: the difference
+    # of the two trajectories' mean energies, with the blocked standard error of the
+    # difference series.  Different forms' trajectories decorrelate within tens of
+    # substeps (any rounding difference is amplified through the force bias), so they
+    # agree only within that statistical error (z-score beside it).  The precision of the
+    # estimator itself shows on identical walkers: its estimate minus FP64's on the FP64
+    # trajectory's walkers, averaged over the measurements, with the standard error of
+    # that mean (the larger of the naive and the blocked estimate).
     tr = out["dE_mixed-cv_vs_fp64"]
-    out["trajectory_dE_Ha"] = tr["abs_dE_Ha"]
-    out["trajectory_dE_sigma_Ha"] = tr["sigma_Ha"]
-    out["trajectory_dE_z"] = tr["abs_dE_Ha"] / tr["sigma_Ha"] if tr["sigma_Ha"] > 0 else None
+    out["abs_dE_Ha"] = tr["abs_dE_Ha"]
+    out["abs_dE_sigma_Ha"] = tr["sigma_Ha"]
+    out["abs_dE_z"] = tr["abs_dE_Ha"] / tr["sigma_Ha"] if tr["sigma_Ha"] > 0 else None
+    out["abs_dE_definition"] = ("difference of the mean energies of the headline form's and "
+                                "the FP64 form's trajectories on the same Philox fields after "
+                                "equilibration; sigma = blocked standard error of the "
+                                "difference series")
+    out["same_walkers_abs_dE_Ha"] = same["cv"]["abs_dE_Ha"]
+    out["same_walkers_abs_dE_sigma_Ha"] = max(same["cv"]["sigma_of_mean_Ha"],
+                                              same["cv"]["sigma_of_mean_blocked_Ha"])
     # the expectation of the control-variate estimate is the mixed form's exact-exchange
     # energy (the subset correction is unbiased): its deterministic error against FP64
     out["abs_dE_deterministic_Ha"] = same["exact"]["abs_dE_Ha"]
