@@ -4,7 +4,9 @@ with the FP64 form on the absolute energy bar.
 FP64 form against the oracle, 1e-10 relative (max |gpu - oracle| / max |oracle|):
   C2 as run: NMO=128, 32+32 electrons, nchol=512 (5% nonzero), 256 walkers, CUDA-graph
     substeps, orthogonalisation every 5, energy every 2 substeps (20 substeps);
-  C3 and C4 on a walker subset: each walker's trajectory depends on the others only
+  C3, C4 and the three C5 systems (NMO 96 / 200 / 320, 12+12 / 40+40 / 64+64 electrons,
+    128 / 256 / 384 walkers) on a walker subset: each walker's trajectory depends on the
+    others only
     through the weights' energy shift (miniafqmc_base.cpp:317-327), so the GPU runs the
     whole ensemble (512 / 1024 walkers) and the oracle 16 of them, placed at their global
     index for the auxiliary fields (set_walker_offset); W, overlaps, the density matrix
@@ -60,10 +62,16 @@ def test_trajectory_C2_graph_vs_oracle():
     g.close()
 
 
-@pytest.mark.parametrize("name,off", [("C3", 256), ("C4", 512)])
+def c5_system(i):
+    from miniafqmc_b200.synthetic import C5_SYSTEMS, make_system
+    return make_system(C5_SYSTEMS[i])
+
+
+@pytest.mark.parametrize("name,off", [("C3", 256), ("C4", 512), ("C5-0", 64), ("C5-1", 128),
+                                      ("C5-2", 192)])
 def test_walker_subset_vs_oracle(name, off):
     from miniafqmc_b200.afqmc import AfqmcSys
-    s = system(name)
+    s = c5_system(int(name[3:])) if name.startswith("C5-") else system(name)
     cfg = s.cfg
     nw, k, seed, northo, nsub = cfg.nwalk, 16, cfg.seed, 5, 6
     g = AfqmcSys(s, nw, use_vakbl=False)
