@@ -254,9 +254,10 @@ void print_help() {
               "matrix to calculate bias potential (default yes).\n");
   std::printf("-v                Verbose output\n");
   std::printf("-p                fp64 | mixed: numerical form (default fp64)\n");
-  std::printf("-e                vakbl | chol | cv: local energy from the two-body matrix, "
-              "the Cholesky factors, or the learned control variate (default vakbl when the "
-              "input has it, else chol)\n");
+  std::printf("-e                vakbl | chol | cv | cv2: local energy from the two-body "
+              "matrix, the Cholesky factors, the learned control variate, or the two-level "
+              "control variate (plain-bf16 exchange of every walker + learned residual; "
+              "-p mixed) (default vakbl when the input has it, else chol)\n");
   std::printf("-g                Run each substep as one CUDA-graph launch (not with -t no)\n");
   std::printf("-d                CUDA device (default 0)\n");
   std::printf("-r                Seed of the auxiliary-field stream (default 11)\n");
@@ -274,6 +275,7 @@ struct Options {
   bool transposed = true, verbose = false, graph = false;
   int precision = AFQ_PREC_FP64;
   int energy = -1;   // -1: vakbl when present, else chol
+  int cv_base = 0;   // -e cv2: the control variate's low-precision base
   int device = 0, taylor = 6, digits = 6, branch = 0;
   uint64_t seed = 11;
 };
@@ -301,7 +303,10 @@ int parse(int argc, char** argv, Options& o) {
         if (!std::strcmp(optarg, "vakbl")) o.energy = AFQ_ENERGY_VAKBL;
         else if (!std::strcmp(optarg, "chol")) o.energy = AFQ_ENERGY_CHOLESKY;
         else if (!std::strcmp(optarg, "cv")) o.energy = AFQ_ENERGY_CV;
-        else return 2;
+        else if (!std::strcmp(optarg, "cv2")) {
+          o.energy = AFQ_ENERGY_CV;
+          o.cv_base = 1;
+        } else return 2;
         break;
       case 'd': o.device = std::atoi(optarg); break;
       case 'r': o.seed = std::strtoull(optarg, nullptr, 10); break;
@@ -422,7 +427,9 @@ int run(const Options& o) {
             << (in.has_vakbl ? in.Vakbl.nnz() / (double(n) * n * N * N * 4.0) : 0.0) << "\n"
             << "    precision: " << (o.precision == AFQ_PREC_MIXED ? "mixed" : "fp64") << "\n"
             << "    energy: "
-            << (energy == AFQ_ENERGY_VAKBL ? "vakbl" : energy == AFQ_ENERGY_CV ? "cv" : "chol")
+            << (energy == AFQ_ENERGY_VAKBL ? "vakbl"
+                : energy == AFQ_ENERGY_CV   ? (o.cv_base ? "cv2" : "cv")
+                                            : "chol")
             << "\n"
             << "    graph substeps: " << o.graph << "\n"
             << "    population control every: " << o.branch << " steps\n"
@@ -451,6 +458,9 @@ int run(const Options& o) {
   Lhalf.shrink_to_fit();
   if (energy == AFQ_ENERGY_CV &&
       !check(afq_cv_configure(h, 256, 1e-3, seed, 2000, 8), h, "afq_cv_configure"))
+    return 1;
+  if (energy == AFQ_ENERGY_CV && o.cv_base &&
+      !check(afq_cv_set_base(h, 1), h, "afq_cv_set_base"))
     return 1;
 
   // walkers = conj(trial), weights 1 (miniafqmc_base.cpp:226-236)

@@ -184,6 +184,10 @@ afq_status afq_cv_configure(afq_handle* h, int, double, uint64_t, long long, int
   return fail(h, AFQ_ERR_UNSUPPORTED, "no control variate in the oracle");
 }
 
+afq_status afq_cv_set_base(afq_handle* h, int) {
+  return fail(h, AFQ_ERR_UNSUPPORTED, "no control variate in the oracle");
+}
+
 afq_status afq_set_walkers(afq_handle* h, const double* W, const double* W_data) {
   if (!h || !W || !W_data) return fail(h, AFQ_ERR_ARG, "null walkers");
   orc_set_walkers(h->o, W, W_data);
