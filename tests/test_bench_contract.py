@@ -119,3 +119,91 @@ def test_blocking_sigma():
         y[i] = phi * y[i - 1] + rng.normal()
     s, lev = bench.blocking_sigma(y)
     assert 3.0 < s / lev[0] < 5.5             # sqrt(2 tau_int) = 4.36
+
+
+def test_accuracy_pass_report_structure(monkeypatch):
+    """The energy-accuracy pass's bookkeeping on the host, with a stand-in for the GPU
+    walker sets: four trajectories (both control-variate settings, exact exchange, FP64),
+    the two shadow estimators on the FP64 trajectory's walkers, and the keys of the
+    report (|dE| on identical fields with its z-score, the identical-walker figures, the
+    other setting's summary and the energy error per wall-second)."""
+    import types
+    import numpy as np
+    import bench
+
+    class FakeTorchEvent:
+        t = 0.0
+
+        def __init__(self, **kw):
+            self.t = 0.0
+
+        def record(self, stream=None):
+            FakeTorchEvent.t += 1.0
+            self.t = FakeTorchEvent.t
+
+        def elapsed_time(self, other):
+            return 1000.0 * (other.t - self.t)
+
+    torch = types.SimpleNamespace(cuda=types.SimpleNamespace(
+        Event=FakeTorchEvent, synchronize=lambda: None))
+
+    class FakeEng:
+        def __init__(self, name, base):
+            self.name, self.base, self.k = name, base, 0
+            self.rng = np.random.default_rng(hash((name, base)) % 2**32)
+
+        def synchronize(self):
+            pass
+
+        def copy_walkers_from(self, other):
+            self.k = other.k
+
+        def calculate_mixed_density_matrix(self):
+            pass
+
+        def calculate_energy(self, mode):
+            e = -300.0 + 0.1 * np.sin(self.k)
+            if mode == "cv":
+                e += (1e-5 if self.base else 1e-3) * self.rng.normal()
+            return float(e)
+
+        def cv_stats(self):
+            return {"subset_var": 1e-6, "active": True}
+
+        def close(self):
+            pass
+
+    class FakeForm:
+        def __init__(self, system, cfg, args, form, device, comm, torch, cv_base=None):
+            self.form = form
+            self.mode = "cv" if form == "mixed-cv" else "chol"
+            self.cv_base = args.cv_base if cv_base is None else cv_base
+            self.eng = FakeEng(form, self.cv_base)
+            self.stream = None
+            self.energies, self.cvvar = [], []
+
+        def measure(self, record=True):
+            E = self.eng.calculate_energy(self.mode)
+            if record:
+                self.energies.append(E)
+                if self.mode == "cv":
+                    self.cvvar.append(1e-6)
+            return E
+
+        def step(self, st, record=True, graph=True):
+            self.eng.k = st + 1
+            if (st + 1) % 5 == 0:
+                self.measure(record)
+
+    monkeypatch.setattr(bench, "Form", FakeForm)
+    args = types.SimpleNamespace(acc_substeps=100, acc_equil=20, energy_every=5, cv_base=0)
+    out = bench.accuracy_pass(None, None, args, 0, torch)
+    assert set(out["forms"]) == {"mixed-cv", "mixed-cv-two-level", "mixed", "fp64"}
+    assert set(out["same_walkers_along_fp64_trajectory"]) == {"cv", "cv_two_level", "exact"}
+    for k in ("abs_dE_Ha", "abs_dE_sigma_Ha", "abs_dE_z", "same_walkers_abs_dE_Ha",
+              "same_walkers_abs_dE_sigma_Ha", "abs_dE_deterministic_Ha"):
+        assert np.isfinite(out[k]), k
+    assert out["other_control_variate"]["form"] == "cv_two_level"
+    assert out["forms"]["mixed-cv-two-level"]["low_precision_base"] is True
+    assert out["err_per_wall_s"]["fp64_over_form"] > 0
+    json.dumps(out)
