@@ -86,6 +86,11 @@ def workload(cfg, args, nw):
                      f"dt={cfg.dt}, Taylor order {cfg.taylor_order}, ortho every {args.northo}, "
                      f"energy every {args.energy_every} substeps"),
         "form": args.form,
+        "control_variate": (None if args.form != "mixed-cv" else
+                            "two-level: plain-bf16 exchange of every walker + learned residual"
+                            if args.cv_base else
+                            "network on the step's features, exact exchange on 1/8 of the "
+                            "walkers"),
         "l2": "inputs larger than L2 (vHS, walkers, Spvn, SpvnT each > 126 MB); no flush",
         "seed": cfg.seed,
     }
