@@ -1256,12 +1256,16 @@ struct EpiExchangeStaged {
   z_t* Kpart;
   float ascale;           // scale of the Lh operand (1 for bf16)
   const float* wscale;    // per-walker scale of the G operand (null for bf16)
+  // epilogue warpgroups of the launch: warpgroup wg takes the tile's walkers wg, wg + nwg,
+  // ... (with two, each keeps to one half of `red`; consecutive walkers of a warpgroup
+  // reuse its half only after the barrier that follows the staging)
+  int nwg = 1;
   template <class Ld>
   AFQ_D void staged(int s, int mt, int nt, int row, Ld& ld, float* scr, int wg) const {
     __shared__ double red[2][4][2];
     const int lane = row & 31, warp = row >> 5;
     const int ncv = min(Gn, nc - mt * Gn);
-    for (int wl = 0; wl < Gw; wl++) {
+    for (int wl = wg; wl < Gw; wl += nwg) {
       float v[32];
 #pragma unroll
       for (int q = 0; q < TWO_N / 32; q++) {
@@ -2391,6 +2395,26 @@ cudaError_t mixed_exchange(MixedState* m, const z_t* Gc, int nsub, z_t* Kpart, i
   return exchange_product(m, nsub, Kpart, nblk, st);
 }
 
+// The low-precision base's product on the staged epilogue with two epilogue warpgroups
+// (one walker each at a time) and a 3-stage ring: the single product's main loop is a
+// third of the split product's, and one warpgroup's traces would set the pace (ncu at
+// C4 with 128 walkers: tensor pipe 27%, L2 32% with one warpgroup).  Walker widths with a
+// staged instance whose tiles hold an even number of walkers; invalid value otherwise
+// (nothing launched).
+template <int TWO_N, int BN>
+static cudaError_t exchange_base2(MixedState* m, const tc::GemmShape& g, int nsub, z_t* Kpart,
+                                  int nblk, cudaStream_t st) {
+  using E = EpiExchangeStaged<TWO_N>;
+  using P = tc::PCfg<BN, 3, 1, false, E, 2>;
+  if constexpr (P::kFits && BN % (2 * TWO_N) == 0) {
+    E ep{m->n, m->ex_Gn, m->ex_Gw, m->nc, nsub, nblk, Kpart, 1.0f, nullptr};
+    ep.nwg = 2;
+    return tc::launch_persistent<BN, 3, 1, false, E, 2>(m->m_ek, g, ep, m->err, st);
+  } else {
+    return cudaErrorInvalidValue;
+  }
+}
+
 // The same exchange partial sums in plain bf16: the hi parts of the split operands, one
 // product instead of three (about 8 significant bits per operand).  Unsupported when the
 // exchange runs on fp16 split operands.
@@ -2405,6 +2429,21 @@ cudaError_t mixed_exchange_lowp(MixedState* m, const z_t* Gc, int nsub, z_t* Kpa
   // the base's fp32 sums over K need no promotion next to its bf16 operand rounding; the
   // staged epilogue keeps up with the single product's shorter main loop
   static const bool promote = getenv("AFQ_CV_BASE_PROMOTE") != nullptr;
+  static const bool one_wg = getenv("AFQ_CV_BASE_WG1") != nullptr;
+  if (!promote && !one_wg && m->ex_bn == m->ex_Gw * 2 * m->n && m->ex_Gw % 2 == 0) {
+    const int n = m->n;
+    tc::GemmShape g{m->nc * n, nsub * 2 * n, m->greal ? m->N : 2 * m->N, 2, m->ex_Gn * n,
+                    m->ex_mtiles, true, true, 0, false, m->ex_Gw * 2 * n};
+    cudaError_t r = cudaErrorInvalidValue;
+    switch (2 * n * 1000 + m->ex_bn) {
+      case 96 * 1000 + 192: r = exchange_base2<96, 192>(m, g, nsub, Kpart, nblk, st); break;
+      case 64 * 1000 + 256: r = exchange_base2<64, 256>(m, g, nsub, Kpart, nblk, st); break;
+      case 64 * 1000 + 128: r = exchange_base2<64, 128>(m, g, nsub, Kpart, nblk, st); break;
+      case 32 * 1000 + 256: r = exchange_base2<32, 256>(m, g, nsub, Kpart, nblk, st); break;
+      case 32 * 1000 + 128: r = exchange_base2<32, 128>(m, g, nsub, Kpart, nblk, st); break;
+    }
+    if (r != cudaErrorInvalidValue) return r;
+  }
   return exchange_product(m, nsub, Kpart, nblk, st, PREC_BF16, promote);
 }
 
