@@ -56,6 +56,15 @@ def test_batch_rejects_bad_arguments_without_gpu():
     assert lib.afq_batch_synchronize(None) == 1
 
 
+def test_control_variate_calls_reject_bad_arguments_without_gpu():
+    """The control-variate set-up calls check their arguments before any device work."""
+    from miniafqmc_b200.afqmc import load_library
+    lib = load_library()
+    assert lib.afq_cv_configure(None, 256, 1e-3, 1, 2000, 8) == 1      # AFQ_ERR_ARG
+    assert lib.afq_cv_set_base(None, 1) == 1
+    assert lib.afq_cv_stats(None, None) == 1
+
+
 def test_halfrotate_rejects_bad_arguments_without_gpu():
     """The GPU half-rotation checks its arguments before selecting a device."""
     import ctypes
